@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""H|psi> throughput of the dft-zig plane-wave hot path on B200.
+
+Workload (one "step"): one Davidson block of H|psi> (nbands + 4 = 164 columns) at every k-point of
+the Si64 cell -- 2x2x2 conventional Si supercell with seeded N(0, 0.02 A) displacements, 30 Ry
+cutoff, 75^3 FFT box, 2x2x2 Monkhorst-Pack mesh (8 k-points, time-reversal folded), FP64.
+Synthetic inputs: seeded wavefunction coefficients; the species are synthetic GTH-form
+pseudopotentials (the reference ships none).
+
+  value   algorithmic HBM GB/s of the device-resident operator: columns x B_alg / device time,
+          B_alg = 2 n_pw s + 2 N s + 8 N / nb per column (s = 16 B; the shared-memory-resident
+          P = 1 form of the per-band byte count), inputs resident in HBM; the 1 GB of inputs and
+          outputs per step exceeds the 126 MB L2, so no flush is needed.
+  e2e     the same metric through the C ABI (dftcuda_apply_h_batch) from pinned host buffers:
+          host->device copy of every column and device->host copy of every result inside the timing.
+
+--impl reference times the CPU restatement of the reference's path (the oracle: numpy FFT + BLAS,
+k-points and columns spread over all host cores with one process each), rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+CELL, SEED, ECUT, KMESH, NBANDS = "si64", 1, 30.0, (2, 2, 2), 160
+NCOLS = NBANDS + 4  # Davidson block (lobpcg/serial.zig:78-82)
+S = 16  # bytes per FP64 complex
+
+
+def bytes_per_column(npw: int, N: int, nb: int) -> float:
+    return 2.0 * npw * S + 2.0 * N * S + 8.0 * N / nb
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f,
+                stderr=subprocess.DEVNULL,
+            )
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                p = [v.strip() for v in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax.append(float(p[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {
+            "sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": float(max(smax)) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload_inputs():
+    import dftzig_loader
+
+    dz = dftzig_loader.load()
+    import importlib
+
+    system = importlib.import_module("dftzig_b200.system")
+    c = system.crystal(CELL, SEED)
+    kpts = system.monkhorst_pack(KMESH)
+    dims = system.fft_box(ECUT, c.recip)
+    tables = [[system.radial_table(sp, i, ECUT) for i in range(len(sp.betas))] for sp in c.species]
+    vloc = system.local_potential(c, dims, ECUT)
+    ins = [system.kpoint_inputs(c, ECUT, k, dims=dims, local_r=vloc, tables=tables) for k, _ in kpts]
+    return dz, c, kpts, dims, ins
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    dz, c, kpts, dims, ins = workload_inputs()
+    N = dims[0] * dims[1] * dims[2]
+    ctxs = []
+    for inp in ins:
+        kc = dz.KpointContext(dims[0], dims[1], dims[2], inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart)
+        kc.set_vloc(inp.local_r)
+        kc.set_projectors([dz.SpeciesProjectors(l, d, p) for (l, d, p) in inp.species_phi], inp.atom_species, inp.positions)
+        ctxs.append(kc)
+    gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    xs, ys = [], []
+    for kc in ctxs:
+        x = torch.randn((NCOLS, kc.n), dtype=torch.complex128, device="cuda", generator=gen)
+        xs.append(x)
+        ys.append(torch.empty_like(x))
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    def step():
+        for kc, x, y in zip(ctxs, xs, ys):
+            kc.apply_hamiltonian_async(x, y, NCOLS, sptr)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    cols_per_step = NCOLS * len(ctxs)
+    algo_bytes_step = sum(NCOLS * bytes_per_column(kc.n, N, NCOLS) for kc in ctxs)
+
+    sampler = ClockSampler(local)
+    for kc in ctxs:
+        kc.set_profiling(True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    profs = [kc.profile() for kc in ctxs]
+    for kc in ctxs:
+        kc.set_profiling(False)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+
+    # e2e through the C ABI from pinned host memory
+    hx = [torch.from_numpy(x.cpu().numpy()).pin_memory() for x in xs]
+    hy = [torch.empty_like(h).pin_memory() for h in hx]
+
+    def e2e_step():
+        for kc, x, y in zip(ctxs, hx, hy):
+            kc.apply_hamiltonian_batched(x, y, kc.n, NCOLS)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    # check one column against the device-resident result
+    ok = bool(np.allclose(hy[0].numpy()[:2], ys[0][:2].cpu().numpy(), rtol=1e-12, atol=1e-12))
+
+    # roofline: the fused local operator (three passes) is the dominant work
+    tot = {k: sum(p[k] for p in profs) for k in profs[0]}
+    launches = int(tot["kernel_launches"])
+    local_ns = tot["apply_local_ns"]
+    npw_avg = float(np.mean([kc.n for kc in ctxs]))
+    local_bytes = cols_per_step * args.steps * (2.0 * npw_avg * S + 2.0 * N * S + 8.0 * N / NCOLS)
+    peak, peak_kind = load_peaks()
+    achieved = local_bytes / (local_ns * 1e-9) / 1e9 if local_ns else None
+    value = world * algo_bytes_step / (ms * 1e-3) / 1e9
+    e2e_value = world * algo_bytes_step / (e2e_ms * 1e-3) / 1e9
+    h2d = sum(x.numel() * 16 for x in hx)
+    kern = {
+        k: {"ms_per_step": tot[k] / 1e6 / args.steps, "share": tot[k] / max(tot["apply_h_ns"], 1)}
+        for k in ("local_plane_inv_ns", "local_xline_ns", "local_plane_fwd_ns", "nl_project_ns", "nl_dij_ns", "nl_backproject_ns")
+    }
+    line = {
+        "metric": "H|psi> HBM GB/s (algorithmic)",
+        "value": round(value, 2),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded wavefunctions; synthetic GTH-form Si pseudopotential)",
+        "config": {
+            "workload": "Si64 2x2x2 conventional, 30 Ry, 75^3 box, 2x2x2 MP (8 k), 164-column Davidson block, FP64 H|psi>",
+            "columns_per_step": cols_per_step,
+            "n_pw_mean": round(npw_avg, 1),
+            "bytes_per_column_alg": round(bytes_per_column(int(npw_avg), N, NCOLS)),
+            "l2": "inputs+outputs per step 1 GB > L2 (no flush needed)",
+            "parallelism": f"replicas x{world}",
+        },
+        "clocks": clocks,
+        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d, "timer": "host wall clock around synchronous C-ABI calls", "matches_device_result": ok},
+        "gpu_launches": launches,
+        "roofline": {
+            "kernel": "local H|psi>: k_plane_inv + k_xline + k_plane_fwd",
+            "bound": "hbm",
+            "achieved": round(achieved, 1) if achieved else None,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": round(achieved / peak, 4) if achieved else None,
+            "peak_source": peak_kind,
+            "traffic": None,
+        },
+        "kernels": kern,
+    }
+    if rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_baseline()
+    if world > 1:
+        dist.destroy_process_group()
+    for kc in ctxs:
+        kc.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU: the oracle (test infrastructure) timed as the reported baseline
+# ---------------------------------------------------------------------------------------------
+
+
+def _cpu_worker(task):
+    os.environ["OMP_NUM_THREADS"] = "1"
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    import numpy as _np
+
+    from oracle import cases
+
+    kfrac, ncols, seed = task
+    c = cases.make_cell(CELL, SEED)
+    kp = cases.make_kproblem(c, ECUT, kfrac)
+    rng = _np.random.default_rng(seed)
+    x = rng.normal(size=(ncols, kp.ctx.n)) + 1j * rng.normal(size=(ncols, kp.ctx.n))
+    t0 = time.perf_counter()
+    kp.ctx.apply_batch(x)
+    dt = time.perf_counter() - t0
+    return dt, ncols, kp.ctx.n, kp.grid.count
+
+
+def cpu_baseline(cols: int = 24):
+    """Single core: the oracle H|psi> on `cols` columns of the Gamma k-point."""
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        dt, nc, npw, N = pool.map(_cpu_worker, [((0.0, 0.0, 0.0), cols, 0)])[0]
+    v = nc * bytes_per_column(npw, N, NCOLS) / dt / 1e9
+    return {"value": round(v, 4), "unit": "GB/s", "cores": 1, "kind": "port", "sample": f"{nc} columns of H|psi> at Gamma (1 k-point), numpy oracle, {dt:.1f} s"}
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    from oracle import cases
+
+    c = cases.make_cell(CELL, SEED)
+    kpts = cases.monkhorst_pack(KMESH)
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    cols = 4  # columns per k-point per step: a bounded sample of the 164-column block
+    steps = max(1, args.steps)
+    with ctx.Pool(cores) as pool:
+        tasks = [(k, cols, i) for i, (k, _) in enumerate(kpts)]
+        for _ in range(min(args.warmup, 1)):
+            pool.map(_cpu_worker, tasks[:cores])
+        times = []
+        done_bytes = 0.0
+        for s in range(steps):
+            t0 = time.perf_counter()
+            res = pool.map(_cpu_worker, tasks)
+            dt = time.perf_counter() - t0
+            times.append(dt)
+            done_bytes += sum(nc * bytes_per_column(npw, N, NCOLS) for _, nc, npw, N in res)
+    total_t = sum(times)
+    v = done_bytes / total_t / 1e9
+    sample = f"{cols} of {NCOLS} columns at each of {len(kpts)} k-points per step, {cores} processes (numpy oracle; the reference binary needs Zig/FFTW/OpenBLAS, absent here)"
+    line = {
+        "impl": "reference",
+        "metric": "H|psi> HBM GB/s (algorithmic)",
+        "value": round(v, 4),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_t / steps * 1e3, 1),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "Si64 2x2x2 conventional, 30 Ry, 75^3 box, 2x2x2 MP (8 k), FP64 H|psi> (column sample)"},
+        "cpu_baseline": {"value": round(v, 4), "unit": "GB/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": round(v, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

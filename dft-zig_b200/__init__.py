@@ -1,0 +1,413 @@
+"""dft-zig B200 hot path: host-side mirror of the reference interfaces over libdftcuda.so.
+
+The CUDA work all happens in ``libdftcuda.so`` (built from ``csrc/`` by ``build.py``); this module only
+binds its C ABI (``include/dftcuda.h``) with ctypes and mirrors the reference's names:
+
+  KpointContext.apply_hamiltonian(_batched)  src/features/scf/apply.zig:643-658, 1584-1618
+  Options / hermitian_eigen_decomp_iterative src/features/linalg/lobpcg/common.zig:44-52,
+                                             src/features/linalg/iterative.zig:67-76
+  KpointContext.accumulate_band_density      src/features/scf/kpoint/density.zig:444-474
+  KpointContext.nonlocal_energies            src/features/scf/kpoint/density.zig:238-266
+  Fft3dPlan.forward / inverse                src/features/fft/fft.zig:224-263 (FFTW semantics)
+
+Errors raise exceptions named after the reference's Zig errors (InvalidMatrixSize, InvalidGrid,
+LapackFailure, ...).  There is no CPU fallback: without the built library, or without a CUDA
+device, every entry point raises.
+
+Arrays: numpy arrays are host memory (the call copies through the library's device buffers);
+torch CUDA tensors are passed as device pointers.  Blocks of vectors are ``(ncols, n)``
+complex128 C-contiguous arrays, i.e. the reference's column-major [n x ncols] layout.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdftcuda.so")
+
+# C-ABI symbols declared in include/dftcuda.h (checked by tests/test_abi.py).
+ABI_SYMBOLS = (
+    "dftcuda_status_string",
+    "dftcuda_last_error_message",
+    "dftcuda_device_count",
+    "dftcuda_kctx_create",
+    "dftcuda_kctx_destroy",
+    "dftcuda_kctx_npw",
+    "dftcuda_set_vloc",
+    "dftcuda_set_projectors",
+    "dftcuda_apply_h_batch",
+    "dftcuda_apply_h",
+    "dftcuda_apply_h_batch_async",
+    "dftcuda_nonlocal_energies",
+    "dftcuda_eig_solve",
+    "dftcuda_accumulate_density",
+    "dftcuda_fft_plan_create",
+    "dftcuda_fft_plan_destroy",
+    "dftcuda_fft3d",
+    "dftcuda_kctx_set_profiling",
+    "dftcuda_kctx_get_profile",
+)
+
+PRECISION_FP64 = 0
+PRECISION_FP32 = 1
+
+
+class DftCudaError(RuntimeError):
+    status = -5
+
+
+class InvalidMatrixSize(DftCudaError):
+    status = -1
+
+
+class InvalidGrid(DftCudaError):
+    status = -2
+
+
+class LapackFailure(DftCudaError):
+    status = -3
+
+
+class OutOfMemory(DftCudaError):
+    status = -4
+
+
+class CudaError(DftCudaError):
+    status = -5
+
+
+class InvalidArgument(DftCudaError):
+    status = -6
+
+
+class Unsupported(DftCudaError):
+    status = -7
+
+
+class Timeout(DftCudaError):
+    status = -8
+
+
+_ERRORS = {c.status: c for c in (InvalidMatrixSize, InvalidGrid, LapackFailure, OutOfMemory, CudaError, InvalidArgument, Unsupported, Timeout)}
+
+
+class _Species(ct.Structure):
+    _fields_ = [
+        ("beta_count", ct.c_size_t),
+        ("l_list", ct.POINTER(ct.c_int32)),
+        ("dij", ct.POINTER(ct.c_double)),
+        ("m_total", ct.c_size_t),
+        ("phi", ct.POINTER(ct.c_double)),
+    ]
+
+
+class _EigOpts(ct.Structure):
+    _fields_ = [
+        ("max_iter", ct.c_size_t),
+        ("tol", ct.c_double),
+        ("max_subspace", ct.c_size_t),
+        ("block_size", ct.c_size_t),
+        ("init_diagonal", ct.c_int),
+    ]
+
+
+class _EigInfo(ct.Structure):
+    _fields_ = [
+        ("iterations", ct.c_size_t),
+        ("h_applies", ct.c_size_t),
+        ("converged", ct.c_int),
+        ("max_residual", ct.c_double),
+    ]
+
+
+PROFILE_FIELDS = (
+    "apply_h_ns",
+    "apply_local_ns",
+    "apply_nonlocal_ns",
+    "density_ns",
+    "subspace_ns",
+    "apply_h_calls",
+    "apply_h_columns",
+    "local_plane_inv_ns",
+    "local_xline_ns",
+    "local_plane_fwd_ns",
+    "local_plane_inv_launches",
+    "local_xline_launches",
+    "local_plane_fwd_launches",
+    "nl_project_ns",
+    "nl_dij_ns",
+    "nl_backproject_ns",
+    "kernel_launches",
+)
+
+
+class _Profile(ct.Structure):
+    _fields_ = [(f, ct.c_uint64) for f in PROFILE_FIELDS]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ct.CDLL:
+    """Load libdftcuda.so; raises when it has not been built (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libdftcuda.so not built at {path}; run __graft_entry__.build()")
+    lib = ct.CDLL(path)
+    vp, sz, dp, ip = ct.c_void_p, ct.c_size_t, ct.c_void_p, ct.c_int
+    lib.dftcuda_status_string.restype = ct.c_char_p
+    lib.dftcuda_status_string.argtypes = [ip]
+    lib.dftcuda_last_error_message.restype = ct.c_char_p
+    lib.dftcuda_device_count.restype = ip
+    lib.dftcuda_kctx_create.argtypes = [ct.POINTER(vp), ip, ip, ip, ct.c_double, sz, vp, vp, vp, ip]
+    lib.dftcuda_kctx_destroy.argtypes = [vp]
+    lib.dftcuda_kctx_npw.argtypes = [vp]
+    lib.dftcuda_kctx_npw.restype = sz
+    lib.dftcuda_set_vloc.argtypes = [vp, dp]
+    lib.dftcuda_set_projectors.argtypes = [vp, sz, ct.POINTER(_Species), sz, vp, vp]
+    lib.dftcuda_apply_h_batch.argtypes = [vp, dp, dp, sz, sz]
+    lib.dftcuda_apply_h.argtypes = [vp, dp, dp, sz]
+    lib.dftcuda_apply_h_batch_async.argtypes = [vp, dp, dp, sz, vp]
+    lib.dftcuda_nonlocal_energies.argtypes = [vp, dp, sz, sz, dp]
+    lib.dftcuda_eig_solve.argtypes = [vp, dp, sz, ct.POINTER(_EigOpts), dp, sz, dp, dp, ct.POINTER(_EigInfo)]
+    lib.dftcuda_accumulate_density.argtypes = [vp, dp, sz, sz, dp, dp]
+    lib.dftcuda_fft_plan_create.argtypes = [ct.POINTER(vp), ip, ip, ip]
+    lib.dftcuda_fft_plan_destroy.argtypes = [vp]
+    lib.dftcuda_fft3d.argtypes = [vp, dp, ip]
+    lib.dftcuda_kctx_set_profiling.argtypes = [vp, ip]
+    lib.dftcuda_kctx_get_profile.argtypes = [vp, ct.POINTER(_Profile)]
+    _lib = lib
+    return lib
+
+
+def _check(status: int):
+    if status == 0:
+        return
+    lib = load_library()
+    msg = lib.dftcuda_last_error_message().decode(errors="replace")
+    cls = _ERRORS.get(status, DftCudaError)
+    raise cls(f"{lib.dftcuda_status_string(status).decode()}: {msg}")
+
+
+def _require_device():
+    if load_library().dftcuda_device_count() < 1:
+        raise CudaError("no CUDA device visible to libdftcuda")
+
+
+def _ptr(a):
+    """Raw pointer of a numpy array (host) or a torch tensor (host or CUDA)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensors must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+@dataclass
+class Options:
+    """lobpcg/common.zig:44-52."""
+
+    max_iter: int = 40
+    tol: float = 1e-6
+    max_subspace: int = 0
+    block_size: int = 0
+    init_diagonal: bool = False
+    init_vectors: Optional[np.ndarray] = None
+    init_vectors_cols: int = 0
+
+
+@dataclass
+class EigenDecomp:
+    """linalg.zig:69-79 plus the solver's run statistics."""
+
+    values: np.ndarray
+    vectors: np.ndarray  # (nbands, n)
+    n: int
+    iterations: int = 0
+    h_applies: int = 0
+    converged: bool = True
+    max_residual: float = 0.0
+
+
+@dataclass
+class SpeciesProjectors:
+    """A NonlocalSpecies (scf/nonlocal_context.zig:9-41): l per radial projector, radial D_ij (Ry)
+    and phi[m_total, n_pw] = 4 pi R(|k+G|) Y_lm(k+G)."""
+
+    l_list: list
+    dij: np.ndarray
+    phi: np.ndarray
+
+
+class KpointContext:
+    """One k-point's H|psi> operator on the GPU (ApplyContext + KpointApplyCache of apply.zig:45-169)."""
+
+    def __init__(self, nx, ny, nz, volume, hkl, kinetic, gcart, precision=PRECISION_FP64):
+        lib = load_library()
+        _require_device()
+        self._lib = lib
+        self.hkl = np.ascontiguousarray(hkl, dtype=np.int32)
+        self.kinetic = np.ascontiguousarray(kinetic, dtype=np.float64)
+        self.gcart = np.ascontiguousarray(gcart, dtype=np.float64)
+        self.n = int(self.kinetic.size)
+        self.dims = (int(nx), int(ny), int(nz))
+        self.volume = float(volume)
+        self.precision = precision
+        h = ct.c_void_p()
+        _check(lib.dftcuda_kctx_create(ct.byref(h), nx, ny, nz, float(volume), self.n, _ptr(self.hkl), _ptr(self.kinetic), _ptr(self.gcart), precision))
+        self._h = h
+
+    @classmethod
+    def from_basis(cls, grid_dims, volume, basis, precision=PRECISION_FP64):
+        return cls(grid_dims[0], grid_dims[1], grid_dims[2], volume, basis.hkl, basis.kinetic, basis.cart, precision)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.dftcuda_kctx_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_vloc(self, local_r):
+        a = local_r if hasattr(local_r, "data_ptr") else np.ascontiguousarray(local_r, dtype=np.float64)
+        _check(self._lib.dftcuda_set_vloc(self._h, _ptr(a)))
+
+    def set_projectors(self, species, atom_species, atom_pos):
+        """species: list[SpeciesProjectors]; atom_species[natom] index; atom_pos[natom,3] Cartesian bohr."""
+        keep = []
+        arr = (_Species * max(len(species), 1))()
+        for i, sp in enumerate(species):
+            l = np.ascontiguousarray(sp.l_list, dtype=np.int32)
+            d = np.ascontiguousarray(sp.dij, dtype=np.float64)
+            phi = np.ascontiguousarray(sp.phi, dtype=np.float64)
+            keep += [l, d, phi]
+            arr[i].beta_count = l.size
+            arr[i].l_list = l.ctypes.data_as(ct.POINTER(ct.c_int32))
+            arr[i].dij = d.ctypes.data_as(ct.POINTER(ct.c_double))
+            arr[i].m_total = phi.shape[0] if phi.ndim == 2 else 0
+            arr[i].phi = phi.ctypes.data_as(ct.POINTER(ct.c_double))
+        asp = np.ascontiguousarray(atom_species, dtype=np.int32)
+        apos = np.ascontiguousarray(atom_pos, dtype=np.float64)
+        _check(self._lib.dftcuda_set_projectors(self._h, len(species), arr, asp.size, _ptr(asp), _ptr(apos)))
+
+    # Operator.apply / apply_batch -------------------------------------------------------------
+    def apply_hamiltonian_batched(self, x_batch, y_batch=None, n=None, ncols=None):
+        if isinstance(x_batch, np.ndarray):
+            x_batch = np.ascontiguousarray(x_batch, dtype=np.complex128)
+            ncols = x_batch.size // self.n if ncols is None else ncols
+            if y_batch is None:
+                y_batch = np.empty_like(x_batch)
+        n = self.n if n is None else n
+        if ncols is None:
+            ncols = x_batch.numel() // self.n
+        _check(self._lib.dftcuda_apply_h_batch(self._h, _ptr(x_batch), _ptr(y_batch), n, ncols))
+        return y_batch
+
+    def apply_hamiltonian(self, x, y=None):
+        x = np.ascontiguousarray(x, dtype=np.complex128)
+        y = np.empty_like(x) if y is None else y
+        _check(self._lib.dftcuda_apply_h(self._h, _ptr(x), _ptr(y), x.size))
+        return y
+
+    def apply_hamiltonian_async(self, x_dev, y_dev, ncols, stream=None):
+        """Device tensors only, no host synchronisation (the device-resident bench path)."""
+        _check(self._lib.dftcuda_apply_h_batch_async(self._h, _ptr(x_dev), _ptr(y_dev), ncols, stream))
+
+    def set_profiling(self, enable: bool = True):
+        """Start (and clear) or stop the device-time ScfProfile counters of this context."""
+        _check(self._lib.dftcuda_kctx_set_profiling(self._h, 1 if enable else 0))
+
+    def profile(self) -> dict:
+        p = _Profile()
+        _check(self._lib.dftcuda_kctx_get_profile(self._h, ct.byref(p)))
+        return {f: int(getattr(p, f)) for f in PROFILE_FIELDS}
+
+    def nonlocal_energies(self, psi):
+        psi = np.ascontiguousarray(psi, dtype=np.complex128).reshape(-1, self.n)
+        e = np.empty(psi.shape[0])
+        _check(self._lib.dftcuda_nonlocal_energies(self._h, _ptr(psi), self.n, psi.shape[0], _ptr(e)))
+        return e
+
+    def accumulate_band_density(self, vectors, weights, rho):
+        """rho (N, FFT order x fastest) += sum_b weights_b |psi_b(r)|^2 / Omega."""
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        if isinstance(vectors, np.ndarray):
+            vectors = np.ascontiguousarray(vectors, dtype=np.complex128).reshape(-1, self.n)
+        _check(self._lib.dftcuda_accumulate_density(self._h, _ptr(vectors), self.n, w.size, _ptr(w), _ptr(rho)))
+        return rho
+
+    def hermitian_eigen_decomp_iterative(self, diag, nbands, opts: Options = Options()) -> EigenDecomp:
+        """iterative.zig:67-76 -> lobpcg_serial.solve with this context as the Operator."""
+        diag = np.ascontiguousarray(diag, dtype=np.float64)
+        if diag.size != self.n:
+            raise InvalidMatrixSize("diag length != n")
+        o = _EigOpts(opts.max_iter, opts.tol, opts.max_subspace, opts.block_size, 1 if opts.init_diagonal else 0)
+        init = None
+        icols = 0
+        if opts.init_vectors is not None:
+            init = np.ascontiguousarray(opts.init_vectors, dtype=np.complex128).reshape(-1, self.n)
+            icols = opts.init_vectors_cols or init.shape[0]
+        vals = np.empty(nbands)
+        vecs = np.empty((nbands, self.n), dtype=np.complex128)
+        info = _EigInfo()
+        _check(self._lib.dftcuda_eig_solve(self._h, _ptr(diag), nbands, ct.byref(o), _ptr(init), icols, _ptr(vals), _ptr(vecs), ct.byref(info)))
+        return EigenDecomp(vals, vecs, self.n, info.iterations, info.h_applies, bool(info.converged), info.max_residual)
+
+
+class Fft3dPlan:
+    """Fft3dPlan with the fftw backend's semantics (fft.zig:44-263, fftw_fft.zig:141-166)."""
+
+    def __init__(self, nx, ny, nz):
+        lib = load_library()
+        _require_device()
+        self._lib = lib
+        self.nx, self.ny, self.nz = nx, ny, nz
+        h = ct.c_void_p()
+        _check(lib.dftcuda_fft_plan_create(ct.byref(h), nx, ny, nz))
+        self._h = h
+
+    def forward(self, data):
+        _check(self._lib.dftcuda_fft3d(self._h, _ptr(data), -1))
+        return data
+
+    def inverse(self, data):
+        _check(self._lib.dftcuda_fft3d(self._h, _ptr(data), 1))
+        return data
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.dftcuda_fft_plan_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,642 @@
+// Block-Davidson ("LOBPCG") eigensolver on the device: src/features/linalg/lobpcg/serial.zig:55-307.
+//
+// Device data: V, W = H V (max_subspace columns), Ritz vectors, residuals.  The host keeps only the
+// control flow of the reference loop (iteration count, which bands are added, restart), reading
+// back nbands eigenvalues and residual norms per iteration.
+//
+// Steps and their reference counterparts:
+//  * random start: the reference's LCG (common.zig:287-319) evaluated in closed form per element
+//    (s_k = a^k s0 + sum_{j<k} a^j mod 2^64), so the device draws exactly the reference's numbers;
+//  * T = V^H W, Hermitised (common.zig:231-259): FP64 complex GEMM + k_hermitize;
+//  * small eigenproblem (zheev, common.zig:440-508): cyclic two-sided complex Jacobi in one CTA,
+//    eigenvalues ascending;
+//  * Ritz vectors V C, W C and residuals r_b = W c_b - lambda_b V c_b with norms (serial.zig:201-227);
+//  * new directions: r_b / (diag - lambda_b) clamped at |den| >= 1e-8 (common.zig:214-226), then
+//    modified Gram-Schmidt against V with a drop when the remaining norm is < 1e-8
+//    (common.zig:263-284, serial.zig:250-262).  The device does this for the whole block at once:
+//    project out V twice, then a Cholesky of the new block's Gram matrix taken column by column in
+//    the reference's order, dropping a column when its Cholesky pivot (= the MGS norm) is < 1e-8,
+//    and a second Cholesky pass for orthogonality (CholQR2).  This spans exactly the vectors MGS
+//    keeps, in the same order; only rounding differs.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "kctx.cuh"
+
+namespace dftcuda {
+
+static const uint64_t kLcgA = 6364136223846793005ULL;
+
+// Affine map s -> A s + C applied k times for the step s -> a s + 1.
+__host__ __device__ inline void lcg_jump(uint64_t k, uint64_t& A, uint64_t& C) {
+  uint64_t ra = 1, rc = 0;  // accumulated map
+  uint64_t ba = kLcgA, bc = 1;  // map for 2^i steps
+  while (k) {
+    if (k & 1) {  // r <- b o r
+      rc = ba * rc + bc;
+      ra = ba * ra;
+    }
+    bc = ba * bc + bc;
+    ba = ba * ba;
+    k >>= 1;
+  }
+  A = ra;
+  C = rc;
+}
+
+// V[col][i] = (u(2e+1) - 0.5, u(2e+2) - 0.5), e = col*n + i, u(k) = (s_k >> 11) / 2^53.
+__global__ void k_lcg_fill(double2* __restrict__ V, long count, uint64_t s0) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= count) return;
+  uint64_t A, C;
+  lcg_jump((uint64_t)(2 * e + 1), A, C);
+  const uint64_t s1 = A * s0 + C;
+  const uint64_t s2 = kLcgA * s1 + 1;
+  const double re = (double)(s1 >> 11) / 9007199254740992.0 - 0.5;
+  const double im = (double)(s2 >> 11) / 9007199254740992.0 - 0.5;
+  V[e] = make_double2(re, im);
+}
+
+__global__ void k_hermitize(double2* T, int m) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= (long)m * m) return;
+  const int i = (int)(idx % m), j = (int)(idx / m);
+  if (i > j) return;
+  if (i == j) {
+    T[i + (long)j * m].y = 0.0;
+    return;
+  }
+  const double2 a = T[i + (long)j * m], b = T[j + (long)i * m];
+  const double re = 0.5 * (a.x + b.x), im = 0.5 * (a.y - b.y);
+  T[i + (long)j * m] = make_double2(re, im);
+  T[j + (long)i * m] = make_double2(re, -im);
+}
+
+// Cyclic two-sided Jacobi for a Hermitian m x m matrix (column-major), one CTA.  Each round applies
+// m/2 disjoint rotations chosen by the circle method.  Writes ascending eigenvalues and the
+// matching eigenvectors (columns of E).  status: 0 ok, 1 not converged.
+__global__ void __launch_bounds__(1024) k_jacobi(double2* __restrict__ A, double2* __restrict__ U,
+                                                 double* __restrict__ evals, double2* __restrict__ E, int m,
+                                                 int max_sweeps, double rel_tol, int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int m2 = m + (m & 1);
+  const int npair = m2 / 2;
+  int2* pq = reinterpret_cast<int2*>(smraw);
+  double* pc = reinterpret_cast<double*>(smraw + sizeof(int2) * npair);
+  double* ps = pc + npair;
+  double2* pe = reinterpret_cast<double2*>(ps + npair);  // e^{-i phi}
+  __shared__ double red[1024];
+  __shared__ int conv;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (long i = tid; i < (long)m * m; i += nt) {
+    const int r = (int)(i % m), c = (int)(i / m);
+    U[i] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+  }
+  __syncthreads();
+  int sweep = 0;
+  for (; sweep <= max_sweeps; ++sweep) {
+    double off = 0.0, tot = 0.0;
+    for (long i = tid; i < (long)m * m; i += nt) {
+      const int r = (int)(i % m), c = (int)(i / m);
+      const double2 v = A[i];
+      const double a2 = v.x * v.x + v.y * v.y;
+      tot += a2;
+      if (r != c) off += a2;
+    }
+    red[tid] = off;
+    __syncthreads();
+    for (int w = nt / 2; w > 0; w >>= 1) {
+      if (tid < w) red[tid] += red[tid + w];
+      __syncthreads();
+    }
+    const double off_s = red[0];
+    __syncthreads();
+    red[tid] = tot;
+    __syncthreads();
+    for (int w = nt / 2; w > 0; w >>= 1) {
+      if (tid < w) red[tid] += red[tid + w];
+      __syncthreads();
+    }
+    const double tot_s = red[0];
+    if (tid == 0) conv = (off_s <= rel_tol * rel_tol * tot_s) || tot_s == 0.0;
+    __syncthreads();
+    if (conv || sweep == max_sweeps) break;
+    for (int rnd = 0; rnd < m2 - 1; ++rnd) {
+      for (int k = tid; k < npair; k += nt) {
+        int p, q;
+        if (k == 0) {
+          p = rnd;
+          q = m2 - 1;
+        } else {
+          p = (rnd + k) % (m2 - 1);
+          q = (rnd - k + (m2 - 1)) % (m2 - 1);
+        }
+        if (p > q) { const int t = p; p = q; q = t; }
+        pq[k] = make_int2(p, q);
+        double c = 1.0, s = 0.0;
+        double2 e = make_double2(1.0, 0.0);
+        if (q < m) {
+          const double app = A[p + (long)p * m].x, aqq = A[q + (long)q * m].x;
+          const double2 apq = A[p + (long)q * m];
+          const double b = hypot(apq.x, apq.y);
+          if (b > 1e-300) {
+            e = make_double2(apq.x / b, -apq.y / b);  // e^{-i phi}
+            const double zeta = (aqq - app) / (2.0 * b);
+            const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+            c = 1.0 / sqrt(1.0 + t * t);
+            s = t * c;
+          }
+        }
+        pc[k] = c;
+        ps[k] = s;
+        pe[k] = e;
+      }
+      __syncthreads();
+      // A <- A G and U <- U G (columns p, q)
+      for (long i = tid; i < (long)m * npair; i += nt) {
+        const int k = (int)(i / m), r = (int)(i - (long)k * m);
+        const int2 ij = pq[k];
+        if (ij.y >= m || ps[k] == 0.0) continue;
+        const double c = pc[k], s = ps[k];
+        const double2 e = pe[k];
+        double2* ap = A + r + (long)ij.x * m;
+        double2* aq = A + r + (long)ij.y * m;
+        const double2 x = *ap, y = *aq;
+        const double2 ey = cmul(e, y);
+        *ap = make_double2(c * x.x - s * ey.x, c * x.y - s * ey.y);
+        *aq = make_double2(s * x.x + c * ey.x, s * x.y + c * ey.y);
+        double2* up = U + r + (long)ij.x * m;
+        double2* uq = U + r + (long)ij.y * m;
+        const double2 ux = *up, uy = *uq;
+        const double2 euy = cmul(e, uy);
+        *up = make_double2(c * ux.x - s * euy.x, c * ux.y - s * euy.y);
+        *uq = make_double2(s * ux.x + c * euy.x, s * ux.y + c * euy.y);
+      }
+      __syncthreads();
+      // A <- G^H A (rows p, q)
+      for (long i = tid; i < (long)m * npair; i += nt) {
+        const int k = (int)(i / m), col = (int)(i - (long)k * m);
+        const int2 ij = pq[k];
+        if (ij.y >= m || ps[k] == 0.0) continue;
+        const double c = pc[k], s = ps[k];
+        const double2 ec = cconj(pe[k]);  // e^{+i phi}
+        double2* ap = A + ij.x + (long)col * m;
+        double2* aq = A + ij.y + (long)col * m;
+        const double2 x = *ap, y = *aq;
+        const double2 ey = cmul(ec, y);
+        *ap = make_double2(c * x.x - s * ey.x, c * x.y - s * ey.y);
+        *aq = make_double2(s * x.x + c * ey.x, s * x.y + c * ey.y);
+      }
+      __syncthreads();
+      for (int k = tid; k < npair; k += nt) {
+        const int2 ij = pq[k];
+        if (ij.y >= m || ps[k] == 0.0) continue;
+        A[ij.x + (long)ij.y * m] = make_double2(0.0, 0.0);
+        A[ij.y + (long)ij.x * m] = make_double2(0.0, 0.0);
+        A[ij.x + (long)ij.x * m].y = 0.0;
+        A[ij.y + (long)ij.y * m].y = 0.0;
+      }
+      __syncthreads();
+    }
+  }
+  if (tid == 0) *status = conv ? 0 : 1;
+  // rank sort (ascending, ties by index) and gather eigenvectors
+  for (int i = tid; i < m; i += nt) {
+    const double di = A[i + (long)i * m].x;
+    int rank = 0;
+    for (int j = 0; j < m; ++j) {
+      const double dj = A[j + (long)j * m].x;
+      rank += (dj < di) || (dj == di && j < i);
+    }
+    evals[rank] = di;
+    for (int r = 0; r < m; ++r) E[r + (long)rank * m] = U[r + (long)i * m];
+  }
+}
+
+// res[b] -= lambda_b ritz[b]; norms[b] = ||res[b]||   (serial.zig:218-227)
+__global__ void k_residual(double2* __restrict__ res, const double2* __restrict__ ritz, const double* __restrict__ lam,
+                           long n, double* __restrict__ norms) {
+  const int b = blockIdx.x;
+  const double l = lam[b];
+  double2* r = res + (long)b * n;
+  const double2* x = ritz + (long)b * n;
+  double s = 0.0;
+  for (long i = threadIdx.x; i < n; i += blockDim.x) {
+    double2 v = r[i];
+    const double2 xv = x[i];
+    v.x -= l * xv.x;
+    v.y -= l * xv.y;
+    r[i] = v;
+    s += v.x * v.x + v.y * v.y;
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) norms[b] = sqrt(red[0]);
+}
+
+// Q[j] = res[band[j]] / (diag - lambda[band[j]]), |den| clamped to 1e-8 keeping its sign (common.zig:214-226)
+__global__ void k_precondition(double2* __restrict__ Q, const double2* __restrict__ res, const double* __restrict__ diag,
+                               const double* __restrict__ lam, const int* __restrict__ band, int k, long n) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= (long)k * n) return;
+  const int j = (int)(idx / n);
+  const long i = idx - (long)j * n;
+  const int b = band[j];
+  double den = diag[i] - lam[b];
+  if (fabs(den) < 1e-8) den = den >= 0.0 ? 1e-8 : -1e-8;
+  const double inv = 1.0 / den;
+  const double2 v = res[(long)b * n + i];
+  Q[idx] = make_double2(v.x * inv, v.y * inv);
+}
+
+// Left-looking Cholesky of the k x k Gram matrix G (column-major) in column order, dropping column j
+// when its pivot sqrt(d) < drop (the MGS norm test).  Produces Z (k x kk, column-major, ld k) with
+// Q Z = the orthonormalised kept columns, kept[0..kk) and *kk_out.
+__global__ void __launch_bounds__(512) k_chol_drop(const double2* __restrict__ G, int k, double drop,
+                                                   double2* __restrict__ R, double2* __restrict__ Z,
+                                                   int* __restrict__ kept, int* __restrict__ kk_out) {
+  // R: k x k workspace, row j holds R[j][l] for kept j (row-major, ld k).
+  __shared__ int s_kept[1024];
+  __shared__ int s_nk;
+  __shared__ double s_piv;
+  __shared__ double red[512];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (tid == 0) s_nk = 0;
+  __syncthreads();
+  for (int j = 0; j < k; ++j) {
+    const int nk = s_nk;
+    // d = G[j][j] - sum_{i kept} |R[i][j]|^2
+    double part = 0.0;
+    for (int t = tid; t < nk; t += nt) {
+      const double2 r = R[(long)s_kept[t] * k + j];
+      part += r.x * r.x + r.y * r.y;
+    }
+    red[tid] = part;
+    __syncthreads();
+    for (int w = nt / 2; w > 0; w >>= 1) {
+      if (tid < w) red[tid] += red[tid + w];
+      __syncthreads();
+    }
+    if (tid == 0) {
+      const double d = G[j + (long)j * k].x - red[0];
+      s_piv = (d > 0.0) ? sqrt(d) : 0.0;
+    }
+    __syncthreads();
+    const double piv = s_piv;
+    if (piv < drop) {
+      __syncthreads();
+      continue;
+    }
+    // R[j][l] = (G[j][l] - sum_{i kept} conj(R[i][j]) R[i][l]) / piv for l > j; R[j][j] = piv
+    for (int l = j + 1 + tid; l < k; l += nt) {
+      double2 s = G[j + (long)l * k];
+      for (int t = 0; t < nk; ++t) {
+        const int i = s_kept[t];
+        const double2 a = R[(long)i * k + j], b = R[(long)i * k + l];
+        s.x -= a.x * b.x + a.y * b.y;
+        s.y -= a.x * b.y - a.y * b.x;
+      }
+      R[(long)j * k + l] = make_double2(s.x / piv, s.y / piv);
+    }
+    if (tid == 0) {
+      R[(long)j * k + j] = make_double2(piv, 0.0);
+      s_kept[nk] = j;
+      s_nk = nk + 1;
+    }
+    __syncthreads();
+  }
+  const int kk = s_nk;
+  // Z[:, c] solves Rk z = e_c over the kept rows/cols (upper triangular back substitution);
+  // rows of dropped columns stay zero.
+  for (long i = tid; i < (long)k * kk; i += nt) Z[i] = make_double2(0.0, 0.0);
+  __syncthreads();
+  for (int c = tid; c < kk; c += nt) {
+    // unknowns z_t for kept index t = c down to 0
+    double2* zc = Z + (long)c * k;
+    for (int t = c; t >= 0; --t) {
+      const int i = s_kept[t];
+      double2 s = make_double2(t == c ? 1.0 : 0.0, 0.0);
+      for (int u = t + 1; u <= c; ++u) {
+        const int ju = s_kept[u];
+        const double2 r = R[(long)i * k + ju];
+        const double2 z = zc[ju];
+        s.x -= r.x * z.x - r.y * z.y;
+        s.y -= r.x * z.y + r.y * z.x;
+      }
+      const double d = R[(long)i * k + i].x;
+      zc[i] = make_double2(s.x / d, s.y / d);
+    }
+  }
+  for (int t = tid; t < kk; t += nt) kept[t] = s_kept[t];
+  if (tid == 0) *kk_out = kk;
+}
+
+// ------------------------------------------------------------------------------------------
+
+struct KCtxImpl {
+  size_t n = 0, max_sub = 0, nb = 0, kmax = 0;
+  double2 *V = nullptr, *W = nullptr, *ritz = nullptr, *res = nullptr, *Q = nullptr, *Q2 = nullptr;
+  double2 *T = nullptr, *U = nullptr, *E = nullptr, *H = nullptr, *G = nullptr, *R = nullptr, *Z = nullptr;
+  double *evals = nullptr, *norms = nullptr, *diag = nullptr;
+  int *band = nullptr, *kept = nullptr, *status = nullptr;
+  double2* ws = nullptr;
+  size_t ws_elems = 0;
+  void* all = nullptr;
+};
+
+void eig_destroy(KCtxImpl* e) {
+  if (!e) return;
+  if (e->all) cudaFree(e->all);
+  if (e->ws) cudaFree(e->ws);
+  delete e;
+}
+
+static int eig_alloc(dftcuda_kctx* c, size_t n, size_t max_sub, size_t nb) {
+  KCtxImpl* e = c->eig;
+  const size_t kmax = max_sub;
+  if (e && e->n == n && e->max_sub >= max_sub && e->nb >= nb) return DFTCUDA_OK;
+  eig_destroy(e);
+  e = c->eig = new KCtxImpl();
+  e->n = n; e->max_sub = max_sub; e->nb = nb; e->kmax = kmax;
+  const size_t ms2 = max_sub * max_sub;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { const size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
+  const size_t oV = take(sizeof(double2) * n * max_sub), oW = take(sizeof(double2) * n * max_sub);
+  const size_t oRi = take(sizeof(double2) * n * nb), oRe = take(sizeof(double2) * n * nb);
+  const size_t oQ = take(sizeof(double2) * n * kmax), oQ2 = take(sizeof(double2) * n * kmax);
+  const size_t oT = take(sizeof(double2) * ms2), oU = take(sizeof(double2) * ms2), oE = take(sizeof(double2) * ms2);
+  const size_t oH = take(sizeof(double2) * ms2), oG = take(sizeof(double2) * ms2), oR = take(sizeof(double2) * ms2);
+  const size_t oZ = take(sizeof(double2) * ms2);
+  const size_t oev = take(sizeof(double) * max_sub), onr = take(sizeof(double) * nb), odg = take(sizeof(double) * n);
+  const size_t obd = take(sizeof(int) * kmax), okp = take(sizeof(int) * kmax), ost = take(sizeof(int) * 4);
+  if (cudaMalloc(&e->all, off) != cudaSuccess) {
+    eig_destroy(e);
+    c->eig = nullptr;
+    return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "eigensolver workspace");
+  }
+  char* b = (char*)e->all;
+  e->V = (double2*)(b + oV); e->W = (double2*)(b + oW); e->ritz = (double2*)(b + oRi); e->res = (double2*)(b + oRe);
+  e->Q = (double2*)(b + oQ); e->Q2 = (double2*)(b + oQ2); e->T = (double2*)(b + oT); e->U = (double2*)(b + oU);
+  e->E = (double2*)(b + oE); e->H = (double2*)(b + oH); e->G = (double2*)(b + oG); e->R = (double2*)(b + oR);
+  e->Z = (double2*)(b + oZ); e->evals = (double*)(b + oev); e->norms = (double*)(b + onr); e->diag = (double*)(b + odg);
+  e->band = (int*)(b + obd); e->kept = (int*)(b + okp); e->status = (int*)(b + ost);
+  size_t need = 0;
+  const int ms = (int)max_sub;
+  need = std::max(need, zgemm_workspace_elems(ms, ms, (int)n));
+  need = std::max(need, zgemm_workspace_elems((int)nb, (int)n, ms));
+  need = std::max(need, zgemm_workspace_elems(ms, (int)kmax, (int)n));
+  need = std::max(need, zgemm_workspace_elems((int)kmax, (int)n, ms));
+  need = std::max(need, zgemm_workspace_elems((int)kmax, (int)kmax, (int)n));
+  if (need) {
+    if (cudaMalloc(&e->ws, need * sizeof(double2)) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "eig gemm ws");
+    e->ws_elems = need;
+  }
+  return DFTCUDA_OK;
+}
+
+// Gram products on blocks stored as rows of length n ("vector blocks", column-major [n x cols]).
+// out[i + j*ldo] = sum_g conj(X[i][g]) Y[j][g]
+static int gram(KCtxImpl* e, const double2* X, int mx, const double2* Y, int my, double2* out, int ldo, cudaStream_t s) {
+  GemmArgs g{};
+  g.M = mx; g.N = my; g.K = (int)e->n;
+  g.A = X; g.lda = (long)e->n; g.a_kc = true; g.conj_a = true;
+  g.B = Y; g.ldb = (long)e->n; g.b_kc = true; g.conj_b = false;
+  g.O = out; g.ldo_r = 1; g.ldo_c = ldo;
+  g.alpha = 1.0; g.beta = 0.0;
+  return zgemm(g, s, e->ws, e->ws_elems);
+}
+
+// Out[j][g] = alpha * sum_i X[i][g] C[i + j*ldc] + beta * Out[j][g]
+static int combine(KCtxImpl* e, const double2* X, int mx, const double2* C, int ldc, int ncols, double2* out,
+                   double alpha, double beta, cudaStream_t s) {
+  GemmArgs g{};
+  g.M = ncols; g.N = (int)e->n; g.K = mx;
+  g.A = C; g.lda = ldc; g.a_kc = true; g.conj_a = false;
+  g.B = X; g.ldb = (long)e->n; g.b_kc = false; g.conj_b = false;
+  g.O = out; g.ldo_r = (long)e->n; g.ldo_c = 1;
+  g.alpha = alpha; g.beta = beta;
+  return zgemm(g, s, e->ws, e->ws_elems);
+}
+
+// Orthonormalise the k vectors in Q against V[0:m] and among themselves (in order), writing the kept
+// vectors to dst.  Returns the number kept in *kk and their indices (into Q) in kept_host.
+static int block_orthonormalize(dftcuda_kctx* c, int m, double2* Q, int k, double2* dst, int* kk,
+                                std::vector<int>& kept_host, cudaStream_t s) {
+  KCtxImpl* e = c->eig;
+  if (k > 1024) return fail(DFTCUDA_ERR_UNSUPPORTED, "block_orthonormalize: more than 1024 new vectors");
+  for (int pass = 0; pass < 2 && m > 0; ++pass) {
+    DFT_TRY(gram(e, e->V, m, Q, k, e->H, m, s));
+    DFT_TRY(combine(e, e->V, m, e->H, m, k, Q, -1.0, 1.0, s));
+  }
+  DFT_TRY(gram(e, Q, k, Q, k, e->G, k, s));
+  k_chol_drop<<<1, 512, 0, s>>>(e->G, k, 1e-8, e->R, e->Z, e->kept, e->status + 1); count_launch();
+  int h_kk = 0;
+  DFT_CUDA_TRY(cudaMemcpyAsync(&h_kk, e->status + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  kept_host.assign(h_kk, 0);
+  if (h_kk > 0) {
+    DFT_CUDA_TRY(cudaMemcpyAsync(kept_host.data(), e->kept, sizeof(int) * h_kk, cudaMemcpyDeviceToHost, s));
+    DFT_TRY(combine(e, Q, k, e->Z, k, h_kk, e->Q2, 1.0, 0.0, s));
+    // second pass (CholQR2) without drops
+    if (m > 0) {
+      DFT_TRY(gram(e, e->V, m, e->Q2, h_kk, e->H, m, s));
+      DFT_TRY(combine(e, e->V, m, e->H, m, h_kk, e->Q2, -1.0, 1.0, s));
+    }
+    DFT_TRY(gram(e, e->Q2, h_kk, e->Q2, h_kk, e->G, h_kk, s));
+    k_chol_drop<<<1, 512, 0, s>>>(e->G, h_kk, 0.0, e->R, e->Z, e->kept, e->status + 2); count_launch();
+    DFT_TRY(combine(e, e->Q2, h_kk, e->Z, h_kk, h_kk, dst, 1.0, 0.0, s));
+    DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  *kk = h_kk;
+  return DFTCUDA_OK;
+}
+
+static int small_eig(KCtxImpl* e, int m, cudaStream_t s) {
+  const int m2 = m + (m & 1);
+  const size_t smem = (sizeof(int2) + 2 * sizeof(double) + sizeof(double2)) * (size_t)(m2 / 2);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    attr = true;
+  }
+  k_jacobi<<<1, 1024, smem, s>>>(e->T, e->U, e->evals, e->E, m, 60, 1e-14, e->status); count_launch();
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}
+
+// orthonormalize_all (common.zig:298-312) for V[0:m]: block Gram-Schmidt; columns that drop are
+// replaced by fresh LCG vectors (the reference's retry) and the block is redone, at most 3 times.
+static int orthonormalize_all(dftcuda_kctx* c, int m, uint64_t& seed, cudaStream_t s) {
+  KCtxImpl* e = c->eig;
+  const long n = (long)e->n;
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    DFT_CUDA_TRY(cudaMemcpyAsync(e->Q, e->V, sizeof(double2) * n * m, cudaMemcpyDeviceToDevice, s));
+    int kk = 0;
+    std::vector<int> kept;
+    DFT_TRY(block_orthonormalize(c, 0, e->Q, m, e->V, &kk, kept, s));
+    if (kk == m) return DFTCUDA_OK;
+    if (attempt == 3) break;
+    // Put kept vectors back in their slots, refill dropped slots with random vectors.
+    std::vector<char> ok(m, 0);
+    for (int t = 0; t < kk; ++t) ok[kept[t]] = 1;
+    DFT_CUDA_TRY(cudaMemcpyAsync(e->Q2, e->V, sizeof(double2) * n * kk, cudaMemcpyDeviceToDevice, s));
+    for (int t = 0; t < kk; ++t)
+      DFT_CUDA_TRY(cudaMemcpyAsync(e->V + (long)kept[t] * n, e->Q2 + (long)t * n, sizeof(double2) * n,
+                                   cudaMemcpyDeviceToDevice, s));
+    for (int j = 0; j < m; ++j) {
+      if (ok[j]) continue;
+      k_lcg_fill<<<ceil_div(n, 256), 256, 0, s>>>(e->V + (long)j * n, n, seed); count_launch();
+      uint64_t A, C;
+      lcg_jump(2 * (uint64_t)n, A, C);
+      seed = A * seed + C;
+    }
+  }
+  return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "orthonormalize_all: could not build an orthonormal block");
+}
+
+}  // namespace dftcuda
+
+using namespace dftcuda;
+
+extern "C" int dftcuda_eig_solve(dftcuda_kctx* c, const double* diag, size_t nbands, const dftcuda_eig_opts* opts_in,
+                                 const double* init_vecs, size_t init_cols, double* values_out, double* vectors_out,
+                                 dftcuda_eig_info* info) {
+  if (!c || !diag || (nbands && (!values_out || !vectors_out)))
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "eig_solve: null argument");
+  dftcuda_eig_opts opts{40, 1e-6, 0, 0, 0};
+  if (opts_in) opts = *opts_in;
+  const size_t n = c->npw;
+  if (info) *info = dftcuda_eig_info{0, 0, 1, 0.0};
+  if (nbands == 0 || n == 0) return DFTCUDA_OK;
+  const size_t max_sub = opts.max_subspace == 0 ? std::min(n, 4 * nbands + 8)
+                                                : std::min(n, std::max(opts.max_subspace, nbands));
+  const size_t block = opts.block_size == 0 ? std::min(max_sub, nbands + 4)
+                                            : std::min(max_sub, std::max(opts.block_size, nbands));
+  if (nbands > max_sub) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "eig_solve: nbands exceeds the basis size");
+  if (max_sub > 2048) return fail(DFTCUDA_ERR_UNSUPPORTED, "eig_solve: max_subspace above 2048");
+  cudaStream_t s = c->stream;
+  DFT_TRY(eig_alloc(c, n, max_sub, nbands));
+  KCtxImpl* e = c->eig;
+  const long ln = (long)n;
+  // diagonal
+  if (is_device_pointer(diag))
+    DFT_CUDA_TRY(cudaMemcpyAsync(e->diag, diag, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  else
+    DFT_CUDA_TRY(cudaMemcpyAsync(e->diag, diag, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  uint64_t seed = 0x6f3d3cbeULL;
+  size_t m = block;
+  size_t icols = 0;
+  if (init_vecs) icols = std::min(m, init_cols == 0 ? nbands : init_cols);
+  if (opts.init_diagonal) {
+    std::vector<double> hd(n);
+    DFT_CUDA_TRY(cudaMemcpyAsync(hd.data(), e->diag, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    DFT_CUDA_TRY(cudaStreamSynchronize(s));
+    std::vector<size_t> order(n);
+    for (size_t i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return hd[a] < hd[b]; });
+    DFT_CUDA_TRY(cudaMemsetAsync(e->V, 0, sizeof(double2) * n * m, s));
+    const double2 one = make_double2(1.0, 0.0);
+    for (size_t col = 0; col < m; ++col)
+      DFT_CUDA_TRY(cudaMemcpyAsync(e->V + col * n + order[col], &one, sizeof(double2), cudaMemcpyHostToDevice, s));
+    DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  } else {
+    k_lcg_fill<<<ceil_div(n * m, 256), 256, 0, s>>>(e->V, (long)(n * m), seed); count_launch();
+    uint64_t A, C;
+    lcg_jump(2 * (uint64_t)(n * m), A, C);
+    seed = A * seed + C;
+  }
+  if (icols) {
+    const bool dv = is_device_pointer(init_vecs);
+    DFT_CUDA_TRY(cudaMemcpyAsync(e->V, init_vecs, sizeof(double2) * n * icols,
+                                 dv ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  }
+  DFT_TRY(orthonormalize_all(c, (int)m, seed, s));
+  DFT_TRY(kctx_apply_h_dev(c, e->V, e->W, m, s));
+  size_t applies = m;
+  std::vector<double> h_ev(nbands), h_nr(nbands);
+  std::vector<int> cand;
+  size_t it = 0;
+  bool converged = false;
+  double max_res = 0.0;
+  for (; it < opts.max_iter; ++it) {
+    const int mi = (int)m;
+    ProfScope ps_sub(c, P_SUBSPACE, s);
+    DFT_TRY(gram(e, e->V, mi, e->W, mi, e->T, mi, s));
+    k_hermitize<<<ceil_div((size_t)mi * mi, 256), 256, 0, s>>>(e->T, mi); count_launch();
+    DFT_TRY(small_eig(e, mi, s));
+    DFT_TRY(combine(e, e->V, mi, e->E, mi, (int)nbands, e->ritz, 1.0, 0.0, s));
+    DFT_TRY(combine(e, e->W, mi, e->E, mi, (int)nbands, e->res, 1.0, 0.0, s));
+    k_residual<<<(unsigned)nbands, 256, 0, s>>>(e->res, e->ritz, e->evals, ln, e->norms); count_launch();
+    int jst = 0;
+    DFT_CUDA_TRY(cudaMemcpyAsync(h_ev.data(), e->evals, sizeof(double) * nbands, cudaMemcpyDeviceToHost, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(h_nr.data(), e->norms, sizeof(double) * nbands, cudaMemcpyDeviceToHost, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(&jst, e->status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    DFT_CUDA_TRY(cudaStreamSynchronize(s));
+    if (jst != 0) return fail(DFTCUDA_ERR_EIGENSOLVER_FAILURE, "eig_solve: subspace Jacobi did not converge");
+    max_res = 0.0;
+    for (size_t b = 0; b < nbands; ++b) max_res = std::max(max_res, h_nr[b]);
+    if (max_res < opts.tol) {
+      converged = true;
+      ++it;
+      break;
+    }
+    // Candidates in band order with ||r_b|| >= tol (serial.zig:242-264).
+    cand.clear();
+    for (size_t b = 0; b < nbands; ++b)
+      if (!(h_nr[b] < opts.tol)) cand.push_back((int)b);
+    size_t added = 0, next = 0;
+    while (m + added < max_sub && next < cand.size()) {
+      const size_t take = std::min(max_sub - (m + added), cand.size() - next);
+      DFT_CUDA_TRY(cudaMemcpyAsync(e->band, cand.data() + next, sizeof(int) * take, cudaMemcpyHostToDevice, s));
+      k_precondition<<<ceil_div(take * n, 256), 256, 0, s>>>(e->Q, e->res, e->diag, e->evals, e->band, (int)take, ln); count_launch();
+      // Orthonormalise against V[0:m+added]; the kept vectors land at V[m+added ...].
+      int kk = 0;
+      std::vector<int> kept;
+      DFT_TRY(block_orthonormalize(c, (int)(m + added), e->Q, (int)take, e->V + (m + added) * n, &kk, kept, s));
+      added += kk;
+      next += take;
+    }
+    if (added == 0) {
+      converged = true;
+      ++it;
+      break;
+    }
+    if (m + added >= max_sub) {
+      // Restart (serial.zig:285-293).  The reference also applies H to the vectors it is about to
+      // discard; that product is never read, so it is skipped here.
+      ps_sub.stop();
+      DFT_CUDA_TRY(cudaMemcpyAsync(e->V, e->ritz, sizeof(double2) * n * nbands, cudaMemcpyDeviceToDevice, s));
+      m = nbands;
+      DFT_TRY(orthonormalize_all(c, (int)m, seed, s));
+      DFT_TRY(kctx_apply_h_dev(c, e->V, e->W, m, s));
+      applies += m;
+      continue;
+    }
+    ps_sub.stop();
+    DFT_TRY(kctx_apply_h_dev(c, e->V + m * n, e->W + m * n, added, s));
+    applies += added;
+    m += added;
+  }
+  // values: last eigenvalues; vectors: last Ritz vectors (serial.zig:298-306)
+  if (is_device_pointer(values_out))
+    DFT_CUDA_TRY(cudaMemcpyAsync(values_out, e->evals, sizeof(double) * nbands, cudaMemcpyDeviceToDevice, s));
+  else
+    std::memcpy(values_out, h_ev.data(), sizeof(double) * nbands);
+  DFT_CUDA_TRY(cudaMemcpyAsync(vectors_out, e->ritz, sizeof(double2) * n * nbands,
+                               is_device_pointer(vectors_out) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+  DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  if (info) {
+    info->iterations = it;
+    info->h_applies = applies;
+    info->converged = converged ? 1 : 0;
+    info->max_residual = max_res;
+  }
+  return DFTCUDA_OK;
+}

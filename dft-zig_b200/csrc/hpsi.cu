@@ -1,0 +1,754 @@
+// H|psi> for one k-point: kinetic + local potential through sphere-pruned 3D FFTs + Kleinman-Bylander
+// nonlocal projectors, and the band density.  Replaces src/features/scf/apply.zig:577-1618 and
+// src/features/scf/kpoint/density.zig:444-474.
+//
+// Local potential, three passes per column block (the reference's scatter_fft -> inverse FFT ->
+// x V(r) -> forward FFT -> gather_fft, apply.zig:811-880):
+//  1. k_plane_inv   one CTA per (active x-frequency plane, column): scatter that plane's plane
+//                   waves into a shared-memory (z, y) plane at digit-reversed positions, inverse
+//                   DIT FFT along z then y, store the plane.  Planes whose x-frequency holds no
+//                   plane wave are never touched (about half the box for a 4x-ecut grid).
+//  2. k_xline       one CTA per run of (z, y) lines: gather the active planes into x pencils,
+//                   inverse DIT along x, multiply by V(r), forward DIF along x, keep only the active
+//                   x-frequencies.
+//  3. k_plane_fwd   forward DIF along y then z, gather the plane waves scaled by 1/N and add the
+//                   kinetic term |k+G|^2 x_G.
+// The net scaling equals the reference's (xN on scatter, 1/N in the inverse, 1/N on gather).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "kctx.cuh"
+
+namespace dftcuda {
+
+template <typename T>
+__global__ void __launch_bounds__(512) k_plane_inv(const double2* __restrict__ x, long npw, cplx<T>* __restrict__ W,
+                                                   int n_act, const int* __restrict__ plane_off,
+                                                   const int* __restrict__ pw_idx, const int* __restrict__ pw_spos,
+                                                   Fft1d py, Fft1d pz, int ny, int nz) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* S = reinterpret_cast<C*>(smraw);
+  const int slot = blockIdx.x;
+  const long b = blockIdx.y;
+  const int P = ny * nz;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) S[i] = mk<C>(0.0, 0.0);
+  __syncthreads();
+  const double2* xb = x + b * npw;
+  const int j1 = plane_off[slot + 1];
+  for (int j = plane_off[slot] + threadIdx.x; j < j1; j += blockDim.x) {
+    const double2 c = __ldg(xb + pw_idx[j]);
+    S[pw_spos[j]] = mk<C>(c.x, c.y);
+  }
+  __syncthreads();
+  fft_lines<T, true>(S, pz, ny, 1, ny, (T)1, true);   // along z, columns are lines
+  fft_lines<T, true>(S, py, 1, ny, nz, (T)1, false);  // along y, rows are lines
+  C* Wp = W + (b * n_act + slot) * (long)P;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) Wp[i] = S[i];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_xline(cplx<T>* __restrict__ W, int n_act, const int* __restrict__ slot_xpos,
+                                               const T* __restrict__ Vt, Fft1d px, int P, int ncols, int J,
+                                               int cols_per_cta) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int nx = px.n;
+  C* tile = reinterpret_cast<C*>(smraw);                 // [nx][J]
+  T* vt = reinterpret_cast<T*>(smraw + sizeof(C) * nx * J);  // [nx][J]
+  const int j0 = blockIdx.x * J;
+  const int nj = min(J, P - j0);
+  const int c0 = blockIdx.y * cols_per_cta;
+  const int c1 = min(ncols, c0 + cols_per_cta);
+  for (int i = threadIdx.x; i < nx * J; i += blockDim.x) {
+    const int xx = i / J, l = i - xx * J;
+    vt[i] = (l < nj) ? __ldg(Vt + (long)xx * P + j0 + l) : (T)0;
+  }
+  for (int c = c0; c < c1; ++c) {
+    for (int i = threadIdx.x; i < nx * J; i += blockDim.x) tile[i] = mk<C>(0.0, 0.0);
+    __syncthreads();
+    const C* Wc = W + (long)c * n_act * P + j0;
+    for (int i = threadIdx.x; i < n_act * J; i += blockDim.x) {
+      const int s = i / J, l = i - s * J;
+      if (l < nj) tile[slot_xpos[s] * J + l] = Wc[(long)s * P + l];
+    }
+    __syncthreads();
+    fft_lines<T, true>(tile, px, J, 1, J, (T)1, true);
+    for (int i = threadIdx.x; i < nx * J; i += blockDim.x) tile[i] = cscale(tile[i], vt[i]);
+    __syncthreads();
+    fft_lines<T, false>(tile, px, J, 1, J, (T)-1, true);
+    C* Wo = W + (long)c * n_act * P + j0;
+    for (int i = threadIdx.x; i < n_act * J; i += blockDim.x) {
+      const int s = i / J, l = i - s * J;
+      if (l < nj) Wo[(long)s * P + l] = tile[slot_xpos[s] * J + l];
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(512) k_plane_fwd(const cplx<T>* __restrict__ W, int n_act,
+                                                   const int* __restrict__ plane_off, const int* __restrict__ pw_idx,
+                                                   const int* __restrict__ pw_spos, Fft1d py, Fft1d pz, int ny,
+                                                   int nz, const double2* __restrict__ x, double2* __restrict__ y,
+                                                   long npw, const double* __restrict__ kinetic, double invN) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* S = reinterpret_cast<C*>(smraw);
+  const int slot = blockIdx.x;
+  const long b = blockIdx.y;
+  const int P = ny * nz;
+  const C* Wp = W + (b * n_act + slot) * (long)P;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) S[i] = Wp[i];
+  __syncthreads();
+  fft_lines<T, false>(S, py, 1, ny, nz, (T)-1, false);
+  fft_lines<T, false>(S, pz, ny, 1, ny, (T)-1, true);
+  const int j1 = plane_off[slot + 1];
+  for (int j = plane_off[slot] + threadIdx.x; j < j1; j += blockDim.x) {
+    const int g = pw_idx[j];
+    const C v = S[pw_spos[j]];
+    const double2 xv = __ldg(x + b * npw + g);
+    const double kin = __ldg(kinetic + g);
+    double2 out;
+    out.x = kin * xv.x + (double)v.x * invN;
+    out.y = kin * xv.y + (double)v.y * invN;
+    y[b * npw + g] = out;
+  }
+}
+
+// Density: inverse transform only, then rho(x, j) += sum_b w_b |psi_b|^2 / Omega over the column block.
+template <typename T>
+__global__ void __launch_bounds__(256) k_xline_density(const cplx<T>* __restrict__ W, int n_act,
+                                                       const int* __restrict__ slot_xpos, Fft1d px, int P, int ncols,
+                                                       int J, const double* __restrict__ w, double inv_vol,
+                                                       double* __restrict__ rho) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int nx = px.n;
+  C* tile = reinterpret_cast<C*>(smraw);                             // [nx][J]
+  double* acc = reinterpret_cast<double*>(smraw + sizeof(C) * nx * J);  // [nx][J]
+  const int j0 = blockIdx.x * J;
+  const int nj = min(J, P - j0);
+  for (int i = threadIdx.x; i < nx * J; i += blockDim.x) acc[i] = 0.0;
+  for (int c = 0; c < ncols; ++c) {
+    for (int i = threadIdx.x; i < nx * J; i += blockDim.x) tile[i] = mk<C>(0.0, 0.0);
+    __syncthreads();
+    const C* Wc = W + (long)c * n_act * P + j0;
+    for (int i = threadIdx.x; i < n_act * J; i += blockDim.x) {
+      const int s = i / J, l = i - s * J;
+      if (l < nj) tile[slot_xpos[s] * J + l] = Wc[(long)s * P + l];
+    }
+    __syncthreads();
+    fft_lines<T, true>(tile, px, J, 1, J, (T)1, true);
+    const double wc = __ldg(w + c) * inv_vol;
+    for (int i = threadIdx.x; i < nx * J; i += blockDim.x) {
+      const C v = tile[i];
+      acc[i] += wc * ((double)v.x * (double)v.x + (double)v.y * (double)v.y);
+    }
+    __syncthreads();
+  }
+  // rho is x-fastest: rho[x + nx*j] with j = z*ny + y
+  for (int i = threadIdx.x; i < nx * J; i += blockDim.x) {
+    const int l = i / nx, xx = i - l * nx;
+    if (l < nj) rho[(long)(j0 + l) * nx + xx] += acc[xx * J + l];
+  }
+}
+
+// P[p][g] = phi_m(g) * exp(i G_g . tau_a) for the projectors of one atom (apply.zig:883-896, 1118-1140).
+__global__ void k_build_projectors(double2* __restrict__ P, const double* __restrict__ phi, int mt, long npw,
+                                   const double* __restrict__ gcart, double tx, double ty, double tz) {
+  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (g >= npw) return;
+  const double arg = gcart[3 * g] * tx + gcart[3 * g + 1] * ty + gcart[3 * g + 2] * tz;
+  double s, c;
+  sincos(arg, &s, &c);
+  for (int m = 0; m < mt; ++m) {
+    const double f = phi[(long)m * npw + g];
+    P[(long)m * npw + g] = make_double2(f * c, f * s);
+  }
+}
+
+// coef2[p][c] = sum_j D_atom[p - off][j] * coef[off + j][c]  (apply.zig:1186-1275)
+__global__ void k_apply_dij(const double2* __restrict__ coef, double2* __restrict__ coef2, const double* __restrict__ D,
+                            const int* __restrict__ proj_off, const int* __restrict__ proj_mt, int maxm, int nproj,
+                            int ncols) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)nproj * ncols) return;
+  const int p = (int)(i / ncols), c = (int)(i - (long)p * ncols);
+  const int off = proj_off[p], mt = proj_mt[p];
+  double2 acc = make_double2(0.0, 0.0);
+  for (int j = 0; j < mt; ++j) {
+    const double d = D[(long)p * maxm + j];
+    if (d == 0.0) continue;
+    const double2 v = coef[(long)(off + j) * ncols + c];
+    acc.x += d * v.x;
+    acc.y += d * v.y;
+  }
+  coef2[(long)p * ncols + c] = acc;
+}
+
+// e[c] = Re sum_p conj(coef[p][c]) coef2[p][c] / Omega  (kpoint/density.zig:145-165)
+__global__ void k_nl_energy(const double2* __restrict__ coef, const double2* __restrict__ coef2, int nproj, int ncols,
+                            double inv_vol, double* __restrict__ e) {
+  const int c = blockIdx.x;
+  double s = 0.0;
+  for (int p = threadIdx.x; p < nproj; p += blockDim.x) {
+    const double2 a = coef[(long)p * ncols + c], b = coef2[(long)p * ncols + c];
+    s += a.x * b.x + a.y * b.y;
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) e[c] = red[0] * inv_vol;
+}
+
+__global__ void k_transpose_vloc(const double* __restrict__ v, double* __restrict__ vt, float* __restrict__ vt32, int nx,
+                                 int ny, int nz) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long N = (long)nx * ny * nz;
+  if (i >= N) return;
+  // i = x + nx*(y + ny*z)  ->  vt[x][z][y]
+  const int xx = (int)(i % nx);
+  const long r = i / nx;
+  const int yy = (int)(r % ny);
+  const int zz = (int)(r / ny);
+  const long o = (long)xx * ny * nz + (long)zz * ny + yy;
+  vt[o] = v[i];
+  vt32[o] = (float)v[i];
+}
+
+// ------------------------------------------------------------------------------------------
+
+static const size_t kSmemMax = 227 * 1024;
+
+template <typename T>
+static void set_smem_attrs() {
+  static bool done = false;
+  if (done) return;
+  cudaFuncSetAttribute(k_plane_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax);
+  cudaFuncSetAttribute(k_plane_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax);
+  cudaFuncSetAttribute(k_xline<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax);
+  cudaFuncSetAttribute(k_xline_density<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax);
+  done = true;
+}
+
+static int line_tile(int nx) { return nx > 64 ? 16 : 32; }
+
+template <typename T>
+static size_t box_bytes_per_col(const dftcuda_kctx* c) {
+  return sizeof(cplx<T>) * (size_t)c->n_act * c->P;
+}
+
+static size_t chunk_cols(const dftcuda_kctx* c, size_t ncols) {
+  const size_t per = (c->precision == DFTCUDA_PRECISION_FP32 ? sizeof(float2) : sizeof(double2)) * (size_t)c->n_act * c->P;
+  size_t ch = (size_t)std::max(1.0, c->w_budget_bytes / (double)per);
+  return std::min(ch, std::max<size_t>(ncols, 1));
+}
+
+static int ensure_box(dftcuda_kctx* c, size_t cols) {
+  if (cols <= c->box_cols) return DFTCUDA_OK;
+  if (c->d_box) cudaFree(c->d_box);
+  c->d_box = nullptr;
+  c->box_cols = 0;
+  const size_t bytes = sizeof(double2) * (size_t)c->n_act * c->P * cols;
+  if (cudaMalloc(&c->d_box, bytes) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "box workspace");
+  c->box_cols = cols;
+  return DFTCUDA_OK;
+}
+
+template <typename T>
+static int local_block(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols, cudaStream_t s) {
+  set_smem_attrs<T>();
+  cplx<T>* W = reinterpret_cast<cplx<T>*>(c->d_box);
+  const size_t smem_plane = sizeof(cplx<T>) * (size_t)c->P;
+  if (smem_plane > kSmemMax) return fail(DFTCUDA_ERR_UNSUPPORTED, "y-z plane does not fit shared memory");
+  dim3 gp(c->n_act, (unsigned)ncols);
+  {
+    ProfScope ps(c, P_PLANE_INV, s);
+    k_plane_inv<T><<<gp, 512, smem_plane, s>>>(x, (long)c->npw, W, c->n_act, c->d_plane_off, c->d_pw_idx, c->d_pw_spos,
+                                               c->fy.dev, c->fz.dev, c->ny, c->nz); count_launch();
+  }
+  const int J = line_tile(c->nx);
+  const int cpc = 4;
+  dim3 gx(ceil_div(c->P, J), ceil_div(ncols, cpc));
+  const size_t smem_x = (sizeof(cplx<T>) + sizeof(T)) * (size_t)c->nx * J;
+  const T* vt = std::is_same<T, double>::value ? (const T*)c->d_vt : (const T*)c->d_vt32;
+  {
+    ProfScope ps(c, P_XLINE, s);
+    k_xline<T><<<gx, 256, smem_x, s>>>(W, c->n_act, c->d_slot_xpos, vt, c->fx.dev, c->P, (int)ncols, J, cpc); count_launch();
+  }
+  {
+    ProfScope ps(c, P_PLANE_FWD, s);
+    k_plane_fwd<T><<<gp, 512, smem_plane, s>>>(W, c->n_act, c->d_plane_off, c->d_pw_idx, c->d_pw_spos, c->fy.dev,
+                                               c->fz.dev, c->ny, c->nz, x, y, (long)c->npw, c->d_kinetic,
+                                               1.0 / (double)c->N); count_launch();
+  }
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}
+
+int kctx_ensure_coef(dftcuda_kctx* c, size_t cols) {
+  if (c->nl.nproj == 0) return DFTCUDA_OK;
+  if (cols > c->coef_cols) {
+    if (c->d_coef) cudaFree(c->d_coef);
+    if (c->d_coef2) cudaFree(c->d_coef2);
+    c->d_coef = c->d_coef2 = nullptr;
+    c->coef_cols = 0;
+    const size_t b = sizeof(double2) * (size_t)c->nl.nproj * cols;
+    if (cudaMalloc(&c->d_coef, b) != cudaSuccess || cudaMalloc(&c->d_coef2, b) != cudaSuccess)
+      return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "projector coefficients");
+    c->coef_cols = cols;
+  }
+  const size_t need = std::max(zgemm_workspace_elems(c->nl.nproj, (int)cols, (int)c->npw),
+                               zgemm_workspace_elems((int)cols, (int)c->npw, c->nl.nproj));
+  if (need > c->gemm_ws_elems) {
+    if (c->d_gemm_ws) cudaFree(c->d_gemm_ws);
+    c->d_gemm_ws = nullptr;
+    c->gemm_ws_elems = 0;
+    if (cudaMalloc(&c->d_gemm_ws, need * sizeof(double2)) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "gemm workspace");
+    c->gemm_ws_elems = need;
+  }
+  return DFTCUDA_OK;
+}
+
+// d_coef[p][c] = sum_g P[p][g] x[c][g]   (batch_project_coeffs, apply.zig:1143-1183)
+int kctx_project(dftcuda_kctx* c, const double2* x, size_t ncols, cudaStream_t s) {
+  GemmArgs g{};
+  g.M = c->nl.nproj; g.N = (int)ncols; g.K = (int)c->npw;
+  g.A = c->nl.P; g.lda = (long)c->npw; g.a_kc = true; g.conj_a = false;
+  g.B = x; g.ldb = (long)c->npw; g.b_kc = true; g.conj_b = false;
+  g.O = c->d_coef; g.ldo_r = (long)ncols; g.ldo_c = 1;
+  g.alpha = 1.0; g.beta = 0.0;
+  return zgemm(g, s, c->d_gemm_ws, c->gemm_ws_elems);
+}
+
+static int nonlocal_block(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols, cudaStream_t s) {
+  {
+    ProfScope ps(c, P_NL_PROJECT, s);
+    DFT_TRY(kctx_project(c, x, ncols, s));
+  }
+  {
+    ProfScope ps(c, P_NL_DIJ, s);
+    const long tot = (long)c->nl.nproj * ncols;
+    k_apply_dij<<<ceil_div(tot, 256), 256, 0, s>>>(c->d_coef, c->d_coef2, c->nl.D, c->nl.proj_off, c->nl.proj_mt,
+                                                   c->nl.maxm, c->nl.nproj, (int)ncols); count_launch();
+  }
+  // y[c][g] += (1/Omega) sum_p coef2[p][c] conj(P[p][g])   (apply.zig:1278-1336)
+  ProfScope ps(c, P_NL_BACK, s);
+  GemmArgs g{};
+  g.M = (int)ncols; g.N = (int)c->npw; g.K = c->nl.nproj;
+  g.A = c->d_coef2; g.lda = (long)ncols; g.a_kc = false; g.conj_a = false;
+  g.B = c->nl.P; g.ldb = (long)c->npw; g.b_kc = false; g.conj_b = true;
+  g.O = y; g.ldo_r = (long)c->npw; g.ldo_c = 1;
+  g.alpha = 1.0 / c->volume; g.beta = 1.0;
+  return zgemm(g, s, c->d_gemm_ws, c->gemm_ws_elems);
+}
+
+int kctx_apply_h_dev(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols, cudaStream_t s) {
+  if (!c->has_vloc) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "apply_h: local potential not set (dftcuda_set_vloc)");
+  if (ncols == 0) return DFTCUDA_OK;
+  if (c->prof.on) {
+    c->prof.calls += 1;
+    c->prof.columns += ncols;
+  }
+  const size_t ch = chunk_cols(c, ncols);
+  DFT_TRY(ensure_box(c, ch));
+  for (size_t c0 = 0; c0 < ncols; c0 += ch) {
+    const size_t nc = std::min(ch, ncols - c0);
+    const double2* xc = x + c0 * c->npw;
+    double2* yc = y + c0 * c->npw;
+    if (c->precision == DFTCUDA_PRECISION_FP32)
+      DFT_TRY(local_block<float>(c, xc, yc, nc, s));
+    else
+      DFT_TRY(local_block<double>(c, xc, yc, nc, s));
+  }
+  if (c->nl.nproj > 0) {
+    const size_t nch = std::min<size_t>(ncols, 256);
+    DFT_TRY(kctx_ensure_coef(c, nch));
+    for (size_t c0 = 0; c0 < ncols; c0 += nch) {
+      const size_t nc = std::min(nch, ncols - c0);
+      DFT_TRY(nonlocal_block(c, x + c0 * c->npw, y + c0 * c->npw, nc, s));
+    }
+  }
+  return DFTCUDA_OK;
+}
+
+template <typename T>
+static int density_block(dftcuda_kctx* c, const double2* x, size_t ncols, const double* w, double* rho, cudaStream_t s) {
+  set_smem_attrs<T>();
+  ProfScope ps(c, P_DENSITY, s);
+  cplx<T>* W = reinterpret_cast<cplx<T>*>(c->d_box);
+  const size_t smem_plane = sizeof(cplx<T>) * (size_t)c->P;
+  dim3 gp(c->n_act, (unsigned)ncols);
+  k_plane_inv<T><<<gp, 512, smem_plane, s>>>(x, (long)c->npw, W, c->n_act, c->d_plane_off, c->d_pw_idx, c->d_pw_spos,
+                                             c->fy.dev, c->fz.dev, c->ny, c->nz); count_launch();
+  const int J = line_tile(c->nx);
+  const size_t smem_x = (sizeof(cplx<T>) + sizeof(double)) * (size_t)c->nx * J;
+  k_xline_density<T><<<ceil_div(c->P, J), 256, smem_x, s>>>(W, c->n_act, c->d_slot_xpos, c->fx.dev, c->P, (int)ncols, J,
+                                                            w, 1.0 / c->volume, rho); count_launch();
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}
+
+int kctx_density_dev(dftcuda_kctx* c, const double2* vecs, size_t nbands, const double* w_dev, double* rho_dev,
+                     cudaStream_t s) {
+  if (nbands == 0) return DFTCUDA_OK;
+  const size_t ch = chunk_cols(c, nbands);
+  DFT_TRY(ensure_box(c, ch));
+  for (size_t c0 = 0; c0 < nbands; c0 += ch) {
+    const size_t nc = std::min(ch, nbands - c0);
+    if (c->precision == DFTCUDA_PRECISION_FP32)
+      DFT_TRY(density_block<float>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
+    else
+      DFT_TRY(density_block<double>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
+  }
+  return DFTCUDA_OK;
+}
+
+int kctx_stage(dftcuda_kctx* c, size_t cols) {
+  if (cols <= c->stage_cols) return DFTCUDA_OK;
+  if (c->d_x) cudaFree(c->d_x);
+  if (c->d_y) cudaFree(c->d_y);
+  c->d_x = c->d_y = nullptr;
+  c->stage_cols = 0;
+  const size_t b = sizeof(double2) * c->npw * cols;
+  if (cudaMalloc(&c->d_x, b) != cudaSuccess || cudaMalloc(&c->d_y, b) != cudaSuccess)
+    return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "staging buffers");
+  c->stage_cols = cols;
+  return DFTCUDA_OK;
+}
+
+}  // namespace dftcuda
+
+using namespace dftcuda;
+
+// ------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------
+
+static void free_nonlocal(dftcuda_kctx* c) {
+  if (c->nl.P) cudaFree(c->nl.P);
+  if (c->nl.D) cudaFree(c->nl.D);
+  if (c->nl.proj_off) cudaFree(c->nl.proj_off);
+  if (c->nl.proj_mt) cudaFree(c->nl.proj_mt);
+  c->nl = NonlocalDev{};
+}
+
+extern "C" int dftcuda_kctx_destroy(dftcuda_kctx* c) {
+  if (!c) return DFTCUDA_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  eig_destroy(c->eig);
+  c->prof.destroy();
+  free_nonlocal(c);
+  void* ptrs[] = {c->d_plane_off, c->d_pw_idx, c->d_pw_spos, c->d_slot_xpos, c->d_kinetic, c->d_gcart, c->d_vt,
+                  c->d_vt32, c->d_box, c->d_coef, c->d_coef2, c->d_gemm_ws, c->d_x, c->d_y, c->d_rho, c->d_w};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  c->fx.destroy(); c->fy.destroy(); c->fz.destroy();
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_kctx_create(dftcuda_kctx** out, int nx, int ny, int nz, double volume, size_t n_pw,
+                                   const int32_t* hkl, const double* kinetic, const double* gcart, int precision) {
+  if (!out) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "kctx_create: out is null");
+  *out = nullptr;
+  if (nx <= 0 || ny <= 0 || nz <= 0 || !(volume > 0.0) || n_pw == 0 || !hkl || !kinetic || !gcart)
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "kctx_create: bad arguments");
+  if (precision != DFTCUDA_PRECISION_FP64 && precision != DFTCUDA_PRECISION_FP32)
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "kctx_create: unknown precision");
+  // Miller index range check, same rule as PwGridMap.init (pw_grid_map.zig:27-35).
+  const int min_h = -(nx / 2), min_k = -(ny / 2), min_l = -(nz / 2);
+  for (size_t i = 0; i < n_pw; ++i) {
+    const int h = hkl[3 * i] - min_h, k = hkl[3 * i + 1] - min_k, l = hkl[3 * i + 2] - min_l;
+    if (h < 0 || k < 0 || l < 0 || h >= nx || k >= ny || l >= nz)
+      return fail(DFTCUDA_ERR_INVALID_GRID, "kctx_create: Miller index outside the FFT box");
+  }
+  auto* c = new dftcuda_kctx();
+  c->nx = nx; c->ny = ny; c->nz = nz;
+  c->N = (long)nx * ny * nz;
+  c->P = ny * nz;
+  c->volume = volume;
+  c->npw = n_pw;
+  c->precision = precision;
+  int s;
+  if ((s = c->fx.create(nx)) || (s = c->fy.create(ny)) || (s = c->fz.create(nz))) {
+    dftcuda_kctx_destroy(c);
+    return s;
+  }
+  if ((size_t)c->P * sizeof(double2) > kSmemMax && precision == DFTCUDA_PRECISION_FP64) {
+    dftcuda_kctx_destroy(c);
+    return fail(DFTCUDA_ERR_UNSUPPORTED, "kctx_create: ny*nz plane exceeds shared memory for FP64");
+  }
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    dftcuda_kctx_destroy(c);
+    return fail(DFTCUDA_ERR_CUDA, "kctx_create: stream");
+  }
+  // Group plane waves by x-frequency plane.
+  std::vector<int> slot_of_x(nx, -1), xs;
+  std::vector<int> xpos(n_pw);
+  for (size_t i = 0; i < n_pw; ++i) {
+    const int x = ((hkl[3 * i] % nx) + nx) % nx;
+    xpos[i] = x;
+    if (slot_of_x[x] < 0) { slot_of_x[x] = 0; xs.push_back(x); }
+  }
+  std::sort(xs.begin(), xs.end());
+  for (size_t sidx = 0; sidx < xs.size(); ++sidx) slot_of_x[xs[sidx]] = (int)sidx;
+  c->n_act = (int)xs.size();
+  std::vector<int> cnt(c->n_act + 1, 0);
+  for (size_t i = 0; i < n_pw; ++i) cnt[slot_of_x[xpos[i]] + 1]++;
+  for (int sidx = 0; sidx < c->n_act; ++sidx) cnt[sidx + 1] += cnt[sidx];
+  std::vector<int> fill(cnt.begin(), cnt.end() - 1), pw_idx(n_pw), pw_spos(n_pw);
+  for (size_t i = 0; i < n_pw; ++i) {
+    const int sidx = slot_of_x[xpos[i]];
+    const int j = fill[sidx]++;
+    const int y = ((hkl[3 * i + 1] % ny) + ny) % ny, z = ((hkl[3 * i + 2] % nz) + nz) % nz;
+    pw_idx[j] = (int)i;
+    pw_spos[j] = c->fz.pinv[z] * ny + c->fy.pinv[y];
+  }
+  std::vector<int> slot_xpos(c->n_act);
+  for (int sidx = 0; sidx < c->n_act; ++sidx) slot_xpos[sidx] = c->fx.pinv[xs[sidx]];
+  c->h_kinetic.assign(kinetic, kinetic + n_pw);
+  bool ok = cudaMalloc(&c->d_plane_off, sizeof(int) * (c->n_act + 1)) == cudaSuccess &&
+            cudaMalloc(&c->d_pw_idx, sizeof(int) * n_pw) == cudaSuccess &&
+            cudaMalloc(&c->d_pw_spos, sizeof(int) * n_pw) == cudaSuccess &&
+            cudaMalloc(&c->d_slot_xpos, sizeof(int) * c->n_act) == cudaSuccess &&
+            cudaMalloc(&c->d_kinetic, sizeof(double) * n_pw) == cudaSuccess &&
+            cudaMalloc(&c->d_gcart, sizeof(double) * 3 * n_pw) == cudaSuccess &&
+            cudaMalloc(&c->d_vt, sizeof(double) * c->N) == cudaSuccess &&
+            cudaMalloc(&c->d_vt32, sizeof(float) * c->N) == cudaSuccess;
+  if (!ok) {
+    dftcuda_kctx_destroy(c);
+    return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "kctx_create: device tables");
+  }
+  cudaMemcpy(c->d_plane_off, cnt.data(), sizeof(int) * (c->n_act + 1), cudaMemcpyHostToDevice);
+  cudaMemcpy(c->d_pw_idx, pw_idx.data(), sizeof(int) * n_pw, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->d_pw_spos, pw_spos.data(), sizeof(int) * n_pw, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->d_slot_xpos, slot_xpos.data(), sizeof(int) * c->n_act, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->d_kinetic, kinetic, sizeof(double) * n_pw, cudaMemcpyHostToDevice);
+  if (cudaMemcpy(c->d_gcart, gcart, sizeof(double) * 3 * n_pw, cudaMemcpyHostToDevice) != cudaSuccess) {
+    dftcuda_kctx_destroy(c);
+    return fail(DFTCUDA_ERR_CUDA, "kctx_create: upload");
+  }
+  *out = c;
+  return DFTCUDA_OK;
+}
+
+extern "C" size_t dftcuda_kctx_npw(const dftcuda_kctx* c) { return c ? c->npw : 0; }
+
+extern "C" int dftcuda_set_vloc(dftcuda_kctx* c, const double* v) {
+  if (!c || !v) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_vloc: null argument");
+  double* dv = nullptr;
+  const bool dev = is_device_pointer(v);
+  if (!dev) {
+    if (cudaMalloc(&dv, sizeof(double) * c->N) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_vloc staging");
+    DFT_CUDA_TRY(cudaMemcpyAsync(dv, v, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+  }
+  k_transpose_vloc<<<ceil_div(c->N, 256), 256, 0, c->stream>>>(dev ? v : dv, c->d_vt, c->d_vt32, c->nx, c->ny, c->nz); count_launch();
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (dv) cudaFree(dv);
+  if (e != cudaSuccess) return fail(DFTCUDA_ERR_CUDA, std::string("set_vloc: ") + cudaGetErrorString(e));
+  c->has_vloc = true;
+  return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const dftcuda_species* species, size_t n_atoms,
+                                      const int32_t* atom_species, const double* atom_pos) {
+  if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_projectors: null context");
+  cudaStreamSynchronize(c->stream);
+  free_nonlocal(c);
+  if (n_species == 0 || n_atoms == 0) return DFTCUDA_OK;
+  if (!species || !atom_species || !atom_pos) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_projectors: null array");
+  // Projector order follows apply.zig:1454-1482: species in order, then that species' atoms in order.
+  int nproj = 0, maxm = 0;
+  for (size_t s = 0; s < n_species; ++s) {
+    const dftcuda_species& sp = species[s];
+    size_t mt = 0;
+    for (size_t b = 0; b < sp.beta_count; ++b) {
+      if (sp.l_list[b] < 0) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_projectors: negative l");
+      mt += 2 * sp.l_list[b] + 1;
+    }
+    if (mt != sp.m_total) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "set_projectors: m_total does not match l_list");
+    if (sp.m_total > 0 && !sp.phi) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_projectors: phi is null");
+    maxm = std::max(maxm, (int)sp.m_total);
+    for (size_t a = 0; a < n_atoms; ++a)
+      if ((size_t)atom_species[a] == s) nproj += (int)sp.m_total;
+  }
+  for (size_t a = 0; a < n_atoms; ++a)
+    if (atom_species[a] < 0 || (size_t)atom_species[a] >= n_species)
+      return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_projectors: atom species index out of range");
+  if (nproj == 0) return DFTCUDA_OK;
+  NonlocalDev& nl = c->nl;
+  nl.nproj = nproj;
+  nl.maxm = maxm;
+  std::vector<double> D((size_t)nproj * maxm, 0.0);
+  std::vector<int> poff(nproj), pmt(nproj);
+  if (cudaMalloc(&nl.P, sizeof(double2) * (size_t)nproj * c->npw) != cudaSuccess) {
+    free_nonlocal(c);
+    return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_projectors: projector matrix");
+  }
+  double* dphi = nullptr;
+  int p = 0;
+  for (size_t s = 0; s < n_species; ++s) {
+    const dftcuda_species& sp = species[s];
+    const int mt = (int)sp.m_total;
+    if (mt == 0) continue;
+    // expanded D (radial form: same-l blocks, m-diagonal), apply.zig:1186-1226
+    std::vector<int> moff(sp.beta_count);
+    int acc = 0;
+    for (size_t b = 0; b < sp.beta_count; ++b) { moff[b] = acc; acc += 2 * sp.l_list[b] + 1; }
+    std::vector<double> dm((size_t)mt * mt, 0.0);
+    for (size_t b = 0; b < sp.beta_count; ++b)
+      for (size_t j = 0; j < sp.beta_count; ++j) {
+        if (sp.l_list[b] != sp.l_list[j]) continue;
+        const double d = sp.dij[b * sp.beta_count + j];
+        for (int mi = 0; mi < 2 * sp.l_list[b] + 1; ++mi) dm[(size_t)(moff[b] + mi) * mt + moff[j] + mi] = d;
+      }
+    if (cudaMalloc(&dphi, sizeof(double) * (size_t)mt * c->npw) != cudaSuccess) {
+      free_nonlocal(c);
+      return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_projectors: phi");
+    }
+    cudaMemcpy(dphi, sp.phi, sizeof(double) * (size_t)mt * c->npw, cudaMemcpyHostToDevice);
+    for (size_t a = 0; a < n_atoms; ++a) {
+      if ((size_t)atom_species[a] != s) continue;
+      k_build_projectors<<<ceil_div(c->npw, 256), 256, 0, c->stream>>>(nl.P + (size_t)p * c->npw, dphi, mt, (long)c->npw,
+                                                                      c->d_gcart, atom_pos[3 * a], atom_pos[3 * a + 1],
+                                                                      atom_pos[3 * a + 2]); count_launch();
+      for (int i = 0; i < mt; ++i) {
+        poff[p + i] = p;
+        pmt[p + i] = mt;
+        for (int j = 0; j < mt; ++j) D[(size_t)(p + i) * maxm + j] = dm[(size_t)i * mt + j];
+      }
+      p += mt;
+    }
+    cudaStreamSynchronize(c->stream);
+    cudaFree(dphi);
+    dphi = nullptr;
+  }
+  bool ok = cudaMalloc(&nl.D, sizeof(double) * D.size()) == cudaSuccess &&
+            cudaMalloc(&nl.proj_off, sizeof(int) * nproj) == cudaSuccess &&
+            cudaMalloc(&nl.proj_mt, sizeof(int) * nproj) == cudaSuccess;
+  if (!ok) {
+    free_nonlocal(c);
+    return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_projectors: tables");
+  }
+  cudaMemcpy(nl.D, D.data(), sizeof(double) * D.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(nl.proj_off, poff.data(), sizeof(int) * nproj, cudaMemcpyHostToDevice);
+  cudaMemcpy(nl.proj_mt, pmt.data(), sizeof(int) * nproj, cudaMemcpyHostToDevice);
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_apply_h_batch_async(dftcuda_kctx* c, const double* x, double* y, size_t ncols, void* stream) {
+  if (!c || (!x && ncols) || (!y && ncols)) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "apply_h_batch_async: null argument");
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  return kctx_apply_h_dev(c, (const double2*)x, (double2*)y, ncols, s);
+}
+
+extern "C" int dftcuda_apply_h_batch(dftcuda_kctx* c, const double* x, double* y, size_t n, size_t ncols) {
+  if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "apply_h_batch: null context");
+  if (n != c->npw) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "apply_h_batch: n != n_pw");  // apply.zig:1591
+  if (ncols == 0) return DFTCUDA_OK;
+  if (!x || !y) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "apply_h_batch: null buffer");
+  const bool dx = is_device_pointer(x), dy = is_device_pointer(y);
+  const size_t bytes = sizeof(double2) * n * ncols;
+  const double2* xd = (const double2*)x;
+  double2* yd = (double2*)y;
+  if (!dx || !dy) DFT_TRY(kctx_stage(c, ncols));
+  if (!dx) {
+    DFT_CUDA_TRY(cudaMemcpyAsync(c->d_x, x, bytes, cudaMemcpyHostToDevice, c->stream));
+    xd = c->d_x;
+  }
+  if (!dy) yd = c->d_y;
+  DFT_TRY(kctx_apply_h_dev(c, xd, yd, ncols, c->stream));
+  if (!dy) DFT_CUDA_TRY(cudaMemcpyAsync(y, yd, bytes, cudaMemcpyDeviceToHost, c->stream));
+  DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_apply_h(dftcuda_kctx* c, const double* x, double* y, size_t n) {
+  return dftcuda_apply_h_batch(c, x, y, n, 1);
+}
+
+extern "C" int dftcuda_nonlocal_energies(dftcuda_kctx* c, const double* psi, size_t n, size_t nbands, double* e_out) {
+  if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_energies: null context");
+  if (n != c->npw) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "nonlocal_energies: n != n_pw");
+  if (nbands == 0) return DFTCUDA_OK;
+  if (!psi || !e_out) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_energies: null buffer");
+  const bool dp = is_device_pointer(psi), de = is_device_pointer(e_out);
+  if (c->nl.nproj == 0) {
+    if (de) DFT_CUDA_TRY(cudaMemset(e_out, 0, sizeof(double) * nbands));
+    else std::memset(e_out, 0, sizeof(double) * nbands);
+    return DFTCUDA_OK;
+  }
+  const double2* pd = (const double2*)psi;
+  DFT_TRY(kctx_stage(c, nbands));
+  if (!dp) {
+    DFT_CUDA_TRY(cudaMemcpyAsync(c->d_x, psi, sizeof(double2) * n * nbands, cudaMemcpyHostToDevice, c->stream));
+    pd = c->d_x;
+  }
+  double* ed = de ? e_out : (double*)c->d_y;
+  const size_t nch = std::min<size_t>(nbands, 256);
+  DFT_TRY(kctx_ensure_coef(c, nch));
+  for (size_t c0 = 0; c0 < nbands; c0 += nch) {
+    const size_t nc = std::min(nch, nbands - c0);
+    DFT_TRY(kctx_project(c, pd + c0 * n, nc, c->stream));
+    const long tot = (long)c->nl.nproj * nc;
+    k_apply_dij<<<ceil_div(tot, 256), 256, 0, c->stream>>>(c->d_coef, c->d_coef2, c->nl.D, c->nl.proj_off, c->nl.proj_mt,
+                                                          c->nl.maxm, c->nl.nproj, (int)nc); count_launch();
+    k_nl_energy<<<(unsigned)nc, 256, 0, c->stream>>>(c->d_coef, c->d_coef2, c->nl.nproj, (int)nc, 1.0 / c->volume, ed + c0); count_launch();
+  }
+  if (!de) DFT_CUDA_TRY(cudaMemcpyAsync(e_out, ed, sizeof(double) * nbands, cudaMemcpyDeviceToHost, c->stream));
+  DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_accumulate_density(dftcuda_kctx* c, const double* vectors, size_t n, size_t nbands,
+                                          const double* weights, double* rho) {
+  if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "accumulate_density: null context");
+  if (n != c->npw) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "accumulate_density: n != n_pw");
+  if (nbands == 0) return DFTCUDA_OK;
+  if (!vectors || !weights || !rho) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "accumulate_density: null buffer");
+  // Keep only bands with a positive weight (kpoint/density.zig:104-107, 386-388).
+  std::vector<double> hw(nbands);
+  if (is_device_pointer(weights))
+    DFT_CUDA_TRY(cudaMemcpy(hw.data(), weights, sizeof(double) * nbands, cudaMemcpyDeviceToHost));
+  else
+    std::memcpy(hw.data(), weights, sizeof(double) * nbands);
+  std::vector<size_t> keep;
+  for (size_t b = 0; b < nbands; ++b)
+    if (hw[b] > 0.0) keep.push_back(b);
+  if (keep.empty()) return DFTCUDA_OK;
+  const bool dv = is_device_pointer(vectors), dr = is_device_pointer(rho);
+  DFT_TRY(kctx_stage(c, keep.size()));
+  // Pack the kept bands contiguously into the staging buffer.
+  const size_t colb = sizeof(double2) * n;
+  for (size_t i = 0; i < keep.size(); ++i)
+    DFT_CUDA_TRY(cudaMemcpyAsync(c->d_x + i * n, vectors + 2 * keep[i] * n, colb,
+                                 dv ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
+  std::vector<double> kw(keep.size());
+  for (size_t i = 0; i < keep.size(); ++i) kw[i] = hw[keep[i]];
+  if (keep.size() > c->w_cap) {
+    if (c->d_w) cudaFree(c->d_w);
+    if (cudaMalloc(&c->d_w, sizeof(double) * keep.size()) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "weights");
+    c->w_cap = keep.size();
+  }
+  DFT_CUDA_TRY(cudaMemcpyAsync(c->d_w, kw.data(), sizeof(double) * kw.size(), cudaMemcpyHostToDevice, c->stream));
+  double* rd = rho;
+  if (!dr) {
+    if (!c->d_rho && cudaMalloc(&c->d_rho, sizeof(double) * c->N) != cudaSuccess)
+      return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "rho staging");
+    DFT_CUDA_TRY(cudaMemcpyAsync(c->d_rho, rho, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+    rd = c->d_rho;
+  }
+  DFT_TRY(kctx_density_dev(c, c->d_x, keep.size(), c->d_w, rd, c->stream));
+  if (!dr) DFT_CUDA_TRY(cudaMemcpyAsync(rho, rd, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
+  DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return DFTCUDA_OK;
+}

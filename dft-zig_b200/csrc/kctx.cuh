@@ -1,0 +1,139 @@
+// Per-k-point context shared by the H|psi>, density and eigensolver translation units.
+#pragma once
+
+#include <vector>
+
+#include "fft_core.cuh"
+
+namespace dftcuda {
+
+// Complex GEMM over strided operands (zgemm.cu):
+//   out(r, c) = alpha * sum_k opA(A(r, k)) * opB(B(c, k)) + beta * out(r, c)
+//   A(r, k) = a_kc ? A[r*lda + k] : A[k*lda + r]      B(c, k) = b_kc ? B[c*ldb + k] : B[k*ldb + c]
+//   out(r, c) = O[r*ldo_r + c*ldo_c];  conj_a / conj_b conjugate the operand.
+struct GemmArgs {
+  int M, N, K;
+  const double2* A; long lda; bool a_kc; bool conj_a;
+  const double2* B; long ldb; bool b_kc; bool conj_b;
+  double2* O; long ldo_r; long ldo_c;
+  double alpha, beta;
+};
+int zgemm(const GemmArgs& g, cudaStream_t s, double2* workspace, size_t workspace_elems);
+size_t zgemm_workspace_elems(int M, int N, int K);
+
+struct NonlocalDev {
+  int nproj = 0;                 // sum over atoms of m_total(species)
+  double2* P = nullptr;          // [nproj][npw] phi_m(g) exp(i G_g . tau_a)
+  double* D = nullptr;           // per-projector row: D[(p)*maxm + j] = D_atom[p-off][j], j < mt(atom)
+  int* proj_off = nullptr;       // [nproj] first projector of the atom owning p
+  int* proj_mt = nullptr;        // [nproj] m_total of that atom
+  int maxm = 0;
+};
+
+struct KCtxImpl;
+
+// Device-time profiler (CUDA events on the launch stream), ScfProfile's counters.
+enum ProfCat { P_PLANE_INV = 0, P_XLINE, P_PLANE_FWD, P_NL_PROJECT, P_NL_DIJ, P_NL_BACK, P_DENSITY, P_SUBSPACE, P_NCAT };
+
+struct Profiler {
+  struct Ev { int cat; cudaEvent_t a, b; };
+  bool on = false;
+  std::vector<Ev> pending;
+  std::vector<cudaEvent_t> pool;
+  double ns[P_NCAT] = {};
+  uint64_t launches[P_NCAT] = {};
+  uint64_t calls = 0, columns = 0;
+  cudaEvent_t take();
+  void resolve();
+  void clear();
+  void destroy();
+};
+
+}  // namespace dftcuda
+
+struct dftcuda_kctx {
+  int nx, ny, nz;
+  long N;        // nx*ny*nz
+  int P;         // ny*nz, points per x-plane
+  double volume;
+  size_t npw;
+  int precision;
+  cudaStream_t stream = nullptr;
+  dftcuda::Fft1dPlan fx, fy, fz;
+
+  // G-sphere grouped by active x-plane ("slot").
+  int n_act = 0;
+  int* d_plane_off = nullptr;  // [n_act+1]
+  int* d_pw_idx = nullptr;     // [npw] basis index, grouped by slot
+  int* d_pw_spos = nullptr;    // [npw] pinv_z(z)*ny + pinv_y(y)
+  int* d_slot_xpos = nullptr;  // [n_act] pinv_x(x) of each slot
+  double* d_kinetic = nullptr;
+  double* d_gcart = nullptr;   // [npw*3]
+  std::vector<double> h_kinetic;
+
+  // Local potential transposed to [x][z][y]; FP32 copy for the FP32 passes.
+  double* d_vt = nullptr;
+  float* d_vt32 = nullptr;
+  bool has_vloc = false;
+
+  // Box workspace for a chunk of columns: [chunk][n_act][P] complex.
+  void* d_box = nullptr;
+  size_t box_cols = 0;
+
+  dftcuda::NonlocalDev nl;
+  double2* d_coef = nullptr;   // [nproj][cols] projector coefficients
+  double2* d_coef2 = nullptr;
+  size_t coef_cols = 0;
+  double2* d_gemm_ws = nullptr;
+  size_t gemm_ws_elems = 0;
+
+  // Staging for host pointers.
+  double2* d_x = nullptr;
+  double2* d_y = nullptr;
+  size_t stage_cols = 0;
+  double* d_rho = nullptr;
+  double* d_w = nullptr;
+  size_t w_cap = 0;
+
+  dftcuda::Profiler prof;
+
+  // Eigensolver workspace (eig.cu).
+  dftcuda::KCtxImpl* eig = nullptr;
+  double w_budget_bytes = 96.0 * 1024 * 1024;  // box workspace target (stays L2-resident)
+};
+
+namespace dftcuda {
+
+int kctx_apply_h_dev(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols, cudaStream_t s);
+int kctx_project(dftcuda_kctx* c, const double2* x, size_t ncols, cudaStream_t s);  // d_coef = P x
+int kctx_ensure_coef(dftcuda_kctx* c, size_t cols);
+int kctx_stage(dftcuda_kctx* c, size_t cols);
+int kctx_density_dev(dftcuda_kctx* c, const double2* vecs, size_t nbands, const double* w_dev, double* rho_dev,
+                     cudaStream_t s);
+void eig_destroy(KCtxImpl* e);
+
+// Times the launches between construction and destruction under category `cat` when profiling is on.
+struct ProfScope {
+  dftcuda_kctx* c;
+  int cat;
+  cudaStream_t s;
+  cudaEvent_t a = nullptr;
+  uint64_t l0 = 0;
+  ProfScope(dftcuda_kctx* c_, int cat_, cudaStream_t s_) : c(c_), cat(cat_), s(s_) {
+    if (!c->prof.on) return;
+    a = c->prof.take();
+    cudaEventRecord(a, s);
+    l0 = launches_total();
+  }
+  void stop() {
+    if (!a) return;
+    cudaEvent_t b = c->prof.take();
+    cudaEventRecord(b, s);
+    c->prof.pending.push_back({cat, a, b});
+    c->prof.launches[cat] += launches_total() - l0;
+    a = nullptr;
+  }
+  ~ProfScope() { stop(); }
+};
+
+}  // namespace dftcuda

@@ -1,0 +1,179 @@
+// FP64 complex GEMM over strided operands, used for the Kleinman-Bylander projections
+// (apply.zig:1143-1183, 1278-1336) and the Rayleigh-Ritz contractions V^H W and V C
+// (lobpcg/common.zig:113-143, 231-259).  B200 has no FP64 tcgen05 kind, so the FP64 path runs on
+// the FP64 FMA pipe: 64x64 output tiles per 256-thread CTA, 4x4 complex outputs per thread,
+// K staged through shared memory in slices of 16, and split-K with a deterministic second-pass
+// reduction when the output has too few tiles to fill the 148 SMs.
+#include <algorithm>
+
+#include "kctx.cuh"
+
+namespace dftcuda {
+
+constexpr int BM = 64, BN = 64, BK = 16;
+
+template <bool AKC, bool BKC, bool CJA, bool CJB>
+__global__ void __launch_bounds__(256) k_zgemm(int M, int N, int K, const double2* __restrict__ A, long lda,
+                                               const double2* __restrict__ B, long ldb, double2* __restrict__ O,
+                                               long ldo_r, long ldo_c, double alpha, double beta, int kps,
+                                               double2* __restrict__ part) {
+  __shared__ double2 As[BK][BM + 1];
+  __shared__ double2 Bs[BK][BN + 1];
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
+  const int r0 = blockIdx.y * BM, c0 = blockIdx.x * BN;
+  const int kbeg = blockIdx.z * kps;
+  const int kend = min(K, kbeg + kps);
+  double2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
+
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = tid + 256 * q;
+      int r, kk;
+      if (AKC) { kk = i % BK; r = i / BK; } else { r = i % BM; kk = i / BM; }
+      const int gr = r0 + r, gk = k0 + kk;
+      double2 v = make_double2(0.0, 0.0);
+      if (gr < M && gk < kend) v = AKC ? A[(long)gr * lda + gk] : A[(long)gk * lda + gr];
+      if (CJA) v.y = -v.y;
+      As[kk][r] = v;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = tid + 256 * q;
+      int cc, kk;
+      if (BKC) { kk = i % BK; cc = i / BK; } else { cc = i % BN; kk = i / BN; }
+      const int gc = c0 + cc, gk = k0 + kk;
+      double2 v = make_double2(0.0, 0.0);
+      if (gc < N && gk < kend) v = BKC ? B[(long)gc * ldb + gk] : B[(long)gk * ldb + gc];
+      if (CJB) v.y = -v.y;
+      Bs[kk][cc] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      double2 a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc[i][j].x = fma(a[i].x, b[j].x, acc[i][j].x);
+          acc[i][j].x = fma(-a[i].y, b[j].y, acc[i][j].x);
+          acc[i][j].y = fma(a[i].x, b[j].y, acc[i][j].y);
+          acc[i][j].y = fma(a[i].y, b[j].x, acc[i][j].y);
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = r0 + ty + 16 * i, c = c0 + tx + 16 * j;
+      if (r >= M || c >= N) continue;
+      if (part) {
+        part[((long)blockIdx.z * M + r) * N + c] = acc[i][j];
+      } else {
+        double2* o = O + (long)r * ldo_r + (long)c * ldo_c;
+        double2 v;
+        v.x = alpha * acc[i][j].x;
+        v.y = alpha * acc[i][j].y;
+        if (beta != 0.0) {
+          const double2 old = *o;
+          v.x += beta * old.x;
+          v.y += beta * old.y;
+        }
+        *o = v;
+      }
+    }
+}
+
+__global__ void k_zgemm_reduce(int M, int N, int splits, const double2* __restrict__ part, double2* __restrict__ O,
+                               long ldo_r, long ldo_c, double alpha, double beta) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)M * N) return;
+  const int r = (int)(i / N), c = (int)(i - (long)r * N);
+  double2 s = make_double2(0.0, 0.0);
+  for (int z = 0; z < splits; ++z) {
+    const double2 v = part[(long)z * M * N + i];
+    s.x += v.x;
+    s.y += v.y;
+  }
+  double2* o = O + (long)r * ldo_r + (long)c * ldo_c;
+  double2 v = make_double2(alpha * s.x, alpha * s.y);
+  if (beta != 0.0) {
+    const double2 old = *o;
+    v.x += beta * old.x;
+    v.y += beta * old.y;
+  }
+  *o = v;
+}
+
+static int pick_splits(int M, int N, int K) {
+  const long tiles = (long)ceil_div(M, BM) * ceil_div(N, BN);
+  const long target = 2 * 148;
+  if (tiles >= target || K < 4 * BK * 8) return 1;
+  int s = (int)std::min<long>((target + tiles - 1) / tiles, K / (BK * 8));
+  return std::max(1, std::min(s, 64));
+}
+
+size_t zgemm_workspace_elems(int M, int N, int K) {
+  const int s = pick_splits(M, N, K);
+  return s > 1 ? (size_t)s * M * N : 0;
+}
+
+template <bool AKC, bool BKC, bool CJA, bool CJB>
+static void launch(const GemmArgs& g, dim3 grid, int kps, double2* part, cudaStream_t s) {
+  k_zgemm<AKC, BKC, CJA, CJB><<<grid, 256, 0, s>>>(g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r, g.ldo_c, g.alpha,
+                                                   g.beta, kps, part); count_launch();
+}
+
+int zgemm(const GemmArgs& g, cudaStream_t s, double2* ws, size_t ws_elems) {
+  if (g.M <= 0 || g.N <= 0) return DFTCUDA_OK;
+  if (g.K <= 0) {
+    // out = beta * out
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "zgemm: K must be positive");
+  }
+  int splits = pick_splits(g.M, g.N, g.K);
+  if (splits > 1 && (size_t)splits * g.M * g.N > ws_elems) splits = 1;
+  int kps = (g.K + splits - 1) / splits;
+  kps = ((kps + BK - 1) / BK) * BK;
+  splits = (g.K + kps - 1) / kps;
+  dim3 grid(ceil_div(g.N, BN), ceil_div(g.M, BM), splits);
+  double2* part = splits > 1 ? ws : nullptr;
+  const int key = (g.a_kc ? 8 : 0) | (g.b_kc ? 4 : 0) | (g.conj_a ? 2 : 0) | (g.conj_b ? 1 : 0);
+  switch (key) {
+    case 0: launch<false, false, false, false>(g, grid, kps, part, s); break;
+    case 1: launch<false, false, false, true>(g, grid, kps, part, s); break;
+    case 2: launch<false, false, true, false>(g, grid, kps, part, s); break;
+    case 3: launch<false, false, true, true>(g, grid, kps, part, s); break;
+    case 4: launch<false, true, false, false>(g, grid, kps, part, s); break;
+    case 5: launch<false, true, false, true>(g, grid, kps, part, s); break;
+    case 6: launch<false, true, true, false>(g, grid, kps, part, s); break;
+    case 7: launch<false, true, true, true>(g, grid, kps, part, s); break;
+    case 8: launch<true, false, false, false>(g, grid, kps, part, s); break;
+    case 9: launch<true, false, false, true>(g, grid, kps, part, s); break;
+    case 10: launch<true, false, true, false>(g, grid, kps, part, s); break;
+    case 11: launch<true, false, true, true>(g, grid, kps, part, s); break;
+    case 12: launch<true, true, false, false>(g, grid, kps, part, s); break;
+    case 13: launch<true, true, false, true>(g, grid, kps, part, s); break;
+    case 14: launch<true, true, true, false>(g, grid, kps, part, s); break;
+    default: launch<true, true, true, true>(g, grid, kps, part, s); break;
+  }
+  if (part) {
+    const long tot = (long)g.M * g.N;
+    k_zgemm_reduce<<<ceil_div(tot, 256), 256, 0, s>>>(g.M, g.N, splits, part, g.O, g.ldo_r, g.ldo_c, g.alpha, g.beta); count_launch();
+  }
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}
+
+}  // namespace dftcuda

@@ -1,0 +1,306 @@
+"""Host-side inputs of the hot path: cells, plane-wave basis, FFT box, projector tables, V_loc(r).
+
+In the reference these come from the SCF driver that calls the path (outside its scope):
+  plane_wave/basis.zig:26-74            G-sphere per k (h outer, l inner; |k+G|^2 <= ecut)
+  scf/pw_grid.zig:54-72, fft/sizing.zig auto FFT box (next 2,3,5-smooth >= 2 ceil(2 sqrt(ecut)/|b|) + 1)
+  pseudopotential/nonlocal.zig:8-338    radial projector tables (ctrap weights, j_l, 2048-point table)
+  scf/nonlocal_context.zig:387-549      phi = 4 pi R(|k+G|) Y_lm(k+G)
+  scf/potential.zig:320-334             V(r) = Re N IFFT(V(G))
+This module builds them with vectorised numpy for the benchmark and SCF workloads.  The synthetic
+species use the Goedecker-Teter-Hutter functional form with builder-chosen parameters (the
+reference ships no pseudopotential files); they are not a published pseudopotential.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+BOHR_PER_ANGSTROM = 1.0 / 0.529177210903
+
+# Builder-chosen GTH-form parameters (energies in Hartree): Z, r_loc, C1, C2 and per channel
+# (l, r_l, h matrix).
+SPECIES_PARAMS = {
+    "Si": dict(z=4.0, rloc=0.45, c1=-6.9, c2=0.0, chans=[(0, 0.42, [[5.8, -1.6], [-1.6, 2.1]]), (1, 0.49, [[2.6]])]),
+    "Al": dict(z=3.0, rloc=0.46, c1=-8.4, c2=0.0, chans=[(0, 0.46, [[5.2, -1.3], [-1.3, 1.8]]), (1, 0.54, [[2.1]])]),
+    "Ge": dict(z=4.0, rloc=0.54, c1=0.0, c2=0.0, chans=[(0, 0.42, [[7.0, -2.0], [-2.0, 2.6]]), (1, 0.56, [[2.5]])]),
+}
+
+DIAMOND8 = np.array(
+    [[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0], [0.25, 0.25, 0.25], [0.25, 0.75, 0.75], [0.75, 0.25, 0.75], [0.75, 0.75, 0.25]]
+)
+FCC4 = np.array([[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0]])
+
+
+@dataclass
+class SpeciesData:
+    """UPF-shaped arrays of one species."""
+
+    name: str
+    z_val: float
+    r: np.ndarray
+    rab: np.ndarray
+    betas: list  # (l, r*beta(r))
+    dij: np.ndarray  # Ry
+    params: dict = field(default_factory=dict)
+
+
+def log_mesh(zmesh=14.0, xmin=-7.0, dx=0.0125, rmax=10.0):
+    n = int((math.log(zmesh * rmax) - xmin) / dx) + 1
+    r = np.exp(xmin + np.arange(n) * dx) / zmesh
+    return r, r * dx
+
+
+def species(name: str) -> SpeciesData:
+    p = SPECIES_PARAMS[name]
+    r, rab = log_mesh()
+    betas, blocks = [], []
+    for l, rl, h in p["chans"]:
+        h = np.asarray(h, float)
+        for i in range(1, h.shape[0] + 1):
+            e = l + (4.0 * i - 1.0) / 2.0
+            proj = math.sqrt(2.0) * r ** (l + 2 * (i - 1)) * np.exp(-(r * r) / (2 * rl * rl)) / (rl**e * math.sqrt(math.gamma(e)))
+            betas.append((l, r * proj))
+        blocks.append(h)
+    nb = len(betas)
+    dij = np.zeros((nb, nb))
+    o = 0
+    for h in blocks:
+        k = h.shape[0]
+        dij[o : o + k, o : o + k] = 2.0 * h
+        o += k
+    return SpeciesData(name, p["z"], r, rab, betas, dij, p)
+
+
+@dataclass
+class Crystal:
+    cell: np.ndarray  # bohr, rows
+    species: list  # [SpeciesData]
+    atom_species: np.ndarray  # int
+    positions: np.ndarray  # bohr, Cartesian [natom,3]
+
+    @property
+    def recip(self):
+        a1, a2, a3 = self.cell
+        v = float(np.dot(a1, np.cross(a2, a3)))
+        return 2.0 * math.pi / v * np.array([np.cross(a2, a3), np.cross(a3, a1), np.cross(a1, a2)])
+
+    @property
+    def volume(self):
+        return abs(float(np.linalg.det(self.cell)))
+
+    @property
+    def nelec(self):
+        return float(sum(self.species[s].z_val for s in self.atom_species))
+
+
+def crystal(name: str, seed: int = 1) -> Crystal:
+    """The benchmark cells (same constructions and seeds as the parity tests)."""
+    si = species("Si")
+    if name == "si2":
+        h = 5.431 * BOHR_PER_ANGSTROM / 2.0
+        cell = np.array([[0.0, h, h], [h, 0.0, h], [h, h, 0.0]])
+        return Crystal(cell, [si], np.zeros(2, int), np.array([[0.0, 0.0, 0.0], [h / 2, h / 2, h / 2]]))
+    if name in ("si8", "si64", "si216"):
+        reps, sigma = {"si8": (1, 0.0), "si64": (2, 0.02), "si216": (3, 0.05)}[name]
+        a = 5.431 * BOHR_PER_ANGSTROM
+        shifts = np.array([[i, j, k] for i in range(reps) for j in range(reps) for k in range(reps)], float)
+        pos = ((shifts[:, None, :] + DIAMOND8[None, :, :]).reshape(-1, 3)) * a
+        rng = np.random.default_rng(seed)
+        if sigma > 0:
+            pos = pos + rng.normal(0.0, sigma * BOHR_PER_ANGSTROM, size=pos.shape)
+        return Crystal(np.eye(3) * a * reps, [si], np.zeros(len(pos), int), pos)
+    if name == "al4":
+        rng = np.random.default_rng(seed)
+        e = rng.uniform(-0.01, 0.01, size=(3, 3))
+        e = 0.5 * (e + e.T)
+        cell = (np.eye(3) * 4.05 * BOHR_PER_ANGSTROM) @ (np.eye(3) + e)
+        return Crystal(cell, [species("Al")], np.zeros(4, int), FCC4 @ cell)
+    if name == "sige8":
+        rng = np.random.default_rng(seed)
+        x = rng.uniform(0.0, 1.0)
+        a = (5.43 + 0.23 * x) * BOHR_PER_ANGSTROM
+        e = rng.uniform(-0.02, 0.02, size=(3, 3))
+        e = 0.5 * (e + e.T)
+        cell = (np.eye(3) * a) @ (np.eye(3) + e)
+        occ = rng.uniform(0.0, 1.0, size=8) < x
+        return Crystal(cell, [si, species("Ge")], occ.astype(int), DIAMOND8 @ cell)
+    raise KeyError(name)
+
+
+def _smooth235(n):
+    m = n
+    for p in (2, 3, 5):
+        while m % p == 0:
+            m //= p
+    return m == 1
+
+
+def fft_box(ecut: float, recip: np.ndarray):
+    out = []
+    for i in range(3):
+        n = max(int(math.ceil(2.0 * math.sqrt(ecut) / float(np.linalg.norm(recip[i])))) * 2 + 1, 3)
+        while not _smooth235(n):
+            n += 1
+        out.append(n)
+    return tuple(out)
+
+
+@dataclass
+class PwBasis:
+    hkl: np.ndarray
+    gcart: np.ndarray
+    kpg: np.ndarray
+    kinetic: np.ndarray
+
+    @property
+    def n(self):
+        return int(self.kinetic.size)
+
+
+def basis(recip: np.ndarray, ecut: float, k_frac) -> PwBasis:
+    k = np.asarray(k_frac, float) @ recip
+    nmax = int(math.ceil(math.sqrt(ecut) / min(np.linalg.norm(recip, axis=1)))) + 1
+    r = np.arange(-nmax, nmax + 1)
+    hkl = np.stack(np.meshgrid(r, r, r, indexing="ij"), axis=-1).reshape(-1, 3)
+    g = (recip[0] * hkl[:, :1] + recip[1] * hkl[:, 1:2]) + recip[2] * hkl[:, 2:3]
+    kpg = k + g
+    kin = kpg[:, 0] ** 2 + kpg[:, 1] ** 2 + kpg[:, 2] ** 2
+    sel = kin <= ecut
+    return PwBasis(hkl[sel].astype(np.int32), g[sel], kpg[sel], kin[sel])
+
+
+def _sph_jl(l: int, x: np.ndarray) -> np.ndarray:
+    out = np.empty_like(x)
+    small = np.abs(x) < 1e-6
+    xs, xb = x[small], x[~small]
+    if l == 0:
+        out[small] = 1.0 - xs**2 / 6.0 + xs**4 / 120.0
+        out[~small] = np.sin(xb) / xb
+    elif l == 1:
+        out[small] = xs / 3.0 - xs**3 / 30.0
+        out[~small] = np.sin(xb) / (xb * xb) - np.cos(xb) / xb
+    else:
+        raise NotImplementedError("synthetic species carry l <= 1 projectors")
+    return out
+
+
+def radial_table(sp: SpeciesData, b: int, ecut: float, npts: int = 2048) -> tuple:
+    """Uniform table of R_b(q) = sum_i r_i (r beta)_i j_l(q r_i) rab_i w_i over [0, 1.5 sqrt(2 ecut)]."""
+    l, beta = sp.betas[b]
+    gmax = 1.5 * math.sqrt(2.0 * ecut)
+    dq = gmax / (npts - 1)
+    q = dq * np.arange(npts)
+    n = sp.r.size
+    w = np.ones(n)
+    if n >= 10:
+        cw = np.array([23.75, 95.10, 55.20, 79.30, 70.65]) / 72.0
+        w[:5] = cw
+        w[-5:] = cw[::-1]
+    f = sp.r * beta * sp.rab * w
+    vals = np.cumsum(_sph_jl(l, np.outer(q, sp.r)) * f[None, :], axis=1)[:, -1]
+    return vals, gmax, dq
+
+
+def _interp(table, g):
+    vals, gmax, dq = table
+    x = g / dq
+    i = np.floor(x).astype(np.int64)
+    t = x - i
+    out = np.zeros_like(g)
+    inside = (g > 0) & (g < gmax)
+    last = inside & (i + 1 >= vals.size)
+    mid = inside & ~last
+    out[mid] = vals[i[mid]] * (1 - t[mid]) + vals[i[mid] + 1] * t[mid]
+    out[last] = vals[-1]
+    out[g <= 0] = vals[0]
+    return out
+
+
+def _ylm(l, m, v):
+    r = np.sqrt((v * v).sum(axis=1))
+    zero = r < math.sqrt(1e-30)
+    u = v / np.where(zero, 1.0, r)[:, None]
+    if l == 0:
+        return np.full(len(v), 1.0 / math.sqrt(4 * math.pi))
+    c = math.sqrt(3.0 / (4 * math.pi))
+    y = c * u[:, {-1: 1, 0: 2, 1: 0}[m]]
+    return np.where(zero, 0.0, y)
+
+
+def projectors(sp: SpeciesData, kpg: np.ndarray, tables) -> np.ndarray:
+    """phi[m_total, n_pw] for one species."""
+    g = np.sqrt((kpg * kpg).sum(axis=1))
+    rows = []
+    for b, (l, _) in enumerate(sp.betas):
+        rad = _interp(tables[b], g)
+        for mi in range(2 * l + 1):
+            rows.append(4.0 * math.pi * rad * _ylm(l, mi - l, kpg))
+    return np.array(rows)
+
+
+def local_potential(c: Crystal, dims, ecut: float) -> np.ndarray:
+    """V(r) (Ry) on the x-fastest box from the analytic GTH local form factors, |G|^2 <= 4 ecut, V(0) = 0."""
+    nx, ny, nz = dims
+    f = [np.fft.fftfreq(n, 1.0 / n) for n in dims]
+    hz, hy, hx = np.meshgrid(f[2], f[1], f[0], indexing="ij")
+    gv = np.stack([hx.ravel(), hy.ravel(), hz.ravel()], axis=1) @ c.recip
+    g2 = (gv * gv).sum(axis=1)
+    vg = np.zeros(g2.size, complex)
+    for s, sp in enumerate(c.species):
+        p = sp.params
+        rl = p["rloc"]
+        e = np.exp(-0.5 * g2 * rl * rl)
+        safe = np.where(g2 > 1e-12, g2, 1.0)
+        ff = np.where(g2 > 1e-12, (-4 * math.pi * p["z"] / safe * e + math.sqrt(8 * math.pi**3) * rl**3 * e * (p["c1"] + p["c2"] * (3 - g2 * rl * rl))), 0.0)
+        sf = np.zeros(g2.size, complex)
+        for a in np.where(c.atom_species == s)[0]:
+            sf += np.exp(-1j * (gv @ c.positions[a]))
+        vg += sf * 2.0 * ff / c.volume
+    vg[g2 > 4 * ecut] = 0.0
+    n = nx * ny * nz
+    return np.fft.ifftn(vg.reshape(nz, ny, nx) * n).real.ravel().copy()
+
+
+@dataclass
+class KpointInputs:
+    dims: tuple
+    volume: float
+    basis: PwBasis
+    local_r: np.ndarray
+    species_phi: list  # per species: (l_list, dij, phi)
+    atom_species: np.ndarray
+    positions: np.ndarray
+
+
+def kpoint_inputs(c: Crystal, ecut: float, k_frac, dims=None, local_r=None, tables=None) -> KpointInputs:
+    dims = dims or fft_box(ecut, c.recip)
+    b = basis(c.recip, ecut, k_frac)
+    if tables is None:
+        tables = [[radial_table(sp, i, ecut) for i in range(len(sp.betas))] for sp in c.species]
+    sph = [([l for l, _ in sp.betas], sp.dij, projectors(sp, b.kpg, tables[s])) for s, sp in enumerate(c.species)]
+    if local_r is None:
+        local_r = local_potential(c, dims, ecut)
+    return KpointInputs(dims, c.volume, b, local_r, sph, c.atom_species, c.positions)
+
+
+def monkhorst_pack(mesh):
+    """Gamma-centred MP mesh, k and -k folded (time reversal).  [(k_frac, weight)]."""
+    n1, n2, n3 = mesh
+    pts = {}
+    order = []
+    for i in range(n1):
+        for j in range(n2):
+            for k in range(n3):
+                key = (i, j, k)
+                neg = ((-i) % n1, (-j) % n2, (-k) % n3)
+                if neg in pts:
+                    pts[neg][1] += 1
+                else:
+                    f = np.array([i / n1, j / n2, k / n3])
+                    f = np.where(f > 0.5, f - 1.0, f)
+                    pts[key] = [f, 1]
+                    order.append(key)
+    tot = n1 * n2 * n3
+    return [(pts[key][0], pts[key][1] / tot) for key in order]

@@ -1,0 +1,180 @@
+/*
+ * libdftcuda — B200 (sm_100a) implementation of dft-zig's plane-wave SCF hot path:
+ * H|psi>, the block-Davidson ("LOBPCG") eigensolver's subspace algebra and the
+ * band-density accumulation, behind a plain C ABI.
+ *
+ * Conventions shared with the reference:
+ *  - complex numbers are interleaved {re, im} doubles (src/features/math/complex.zig:3-6);
+ *  - blocks of vectors are column-major [n x ncols] (src/features/linalg/lobpcg/common.zig:16-24);
+ *  - FFT boxes are indexed x + nx*(y + ny*z) (src/lib/fft/fftw_fft.zig:91-113);
+ *  - energies are Rydberg, lengths bohr.
+ *
+ * Pointer arguments marked "host or device" may point to host memory (pageable or
+ * pinned) or to device memory of the current CUDA device; the library detects which
+ * and copies through its own device buffers when needed.  Every call returns an int
+ * status: DFTCUDA_OK (0) or one of the negative codes below, which map one-to-one onto
+ * the reference's Zig error set.  All calls are synchronous with respect to the host
+ * unless named *_async.
+ */
+#ifndef DFTCUDA_H
+#define DFTCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Zig error each one maps to, in the reference's error sets. */
+#define DFTCUDA_OK 0
+#define DFTCUDA_ERR_INVALID_MATRIX_SIZE (-1) /* error.InvalidMatrixSize (apply.zig:580, serial.zig:73) */
+#define DFTCUDA_ERR_INVALID_GRID (-2)        /* error.InvalidGrid (pw_grid_map.zig:27-35)             */
+#define DFTCUDA_ERR_EIGENSOLVER_FAILURE (-3) /* error.LapackFailure (lobpcg/common.zig:466,491)       */
+#define DFTCUDA_ERR_OUT_OF_MEMORY (-4)       /* error.OutOfMemory                                     */
+#define DFTCUDA_ERR_CUDA (-5)                /* CUDA runtime failure (no reference counterpart)       */
+#define DFTCUDA_ERR_INVALID_ARGUMENT (-6)    /* null handle / inconsistent sizes                      */
+#define DFTCUDA_ERR_UNSUPPORTED (-7)         /* FFT length with a prime factor other than 2, 3, 5     */
+#define DFTCUDA_ERR_TIMEOUT (-8)             /* a bounded device wait gave up (no reference counterpart) */
+
+/* Arithmetic of the local-potential FFT passes of one k-point context. */
+#define DFTCUDA_PRECISION_FP64 0
+#define DFTCUDA_PRECISION_FP32 1
+
+typedef struct dftcuda_kctx dftcuda_kctx;
+typedef struct dftcuda_fft_plan dftcuda_fft_plan;
+
+/* Human-readable name of a status code, and the message of the last failure on this thread. */
+const char* dftcuda_status_string(int status);
+const char* dftcuda_last_error_message(void);
+
+/* Number of CUDA devices visible (0 on a host without a GPU; never fails). */
+int dftcuda_device_count(void);
+
+/* ------------------------------------------------------------------------------------------
+ * Per-k-point context: replaces the ApplyContext + KpointApplyCache pair
+ * (src/features/scf/apply.zig:45-169, 554-573) and PwGridMap (src/features/scf/pw_grid_map.zig:8-56).
+ *
+ * hkl[n_pw*3]   Miller indices of the G-sphere in basis order (plane_wave/basis.zig:26-74)
+ * kinetic[n_pw] |k+G|^2 (Ry) = the kinetic diagonal (apply.zig:589-592)
+ * gcart[n_pw*3] Cartesian G (bohr^-1), used for the atom phases exp(i G.tau) (apply.zig:883-896)
+ * The FFT box (nx, ny, nz) must hold every Miller index (else DFTCUDA_ERR_INVALID_GRID) and each
+ * extent must be 2,3,5-smooth and <= 128 (else DFTCUDA_ERR_UNSUPPORTED).
+ * All host pointers; the context keeps device copies.  One context per k-point; each owns a
+ * CUDA stream, so contexts run independently like the reference's per-thread ApplyContexts.
+ * ------------------------------------------------------------------------------------------ */
+int dftcuda_kctx_create(dftcuda_kctx** out, int nx, int ny, int nz, double volume, size_t n_pw,
+                        const int32_t* hkl, const double* kinetic, const double* gcart, int precision);
+int dftcuda_kctx_destroy(dftcuda_kctx* ctx);
+size_t dftcuda_kctx_npw(const dftcuda_kctx* ctx);
+
+/* Real local potential V(r) on the FFT box (N doubles, x fastest): the local_r argument of
+ * ApplyContext.init (apply.zig:235-300), built by build_local_potential_real (scf/potential.zig:320-334).
+ * Host or device pointer. */
+int dftcuda_set_vloc(dftcuda_kctx* ctx, const double* local_r);
+
+/* Kleinman-Bylander projectors of one species (NonlocalSpecies, scf/nonlocal_context.zig:9-41). */
+typedef struct dftcuda_species {
+  size_t beta_count;     /* number of radial projectors                                         */
+  const int32_t* l_list; /* [beta_count] angular momentum of each projector                      */
+  const double* dij;     /* [beta_count*beta_count] row-major D_ij (Ry), radial form             */
+  size_t m_total;        /* sum over projectors of 2l+1                                          */
+  const double* phi;     /* [m_total*n_pw] row-major phi = 4 pi R(|k+G|) Y_lm(k+G) (nonlocal_context.zig:524-549) */
+} dftcuda_species;
+
+/* Installs the nonlocal part: species[n_species], atom_species[n_atoms] (index into species),
+ * atom_pos[n_atoms*3] Cartesian bohr.  Passing n_species == 0 removes it.  Host pointers. */
+int dftcuda_set_projectors(dftcuda_kctx* ctx, size_t n_species, const dftcuda_species* species, size_t n_atoms,
+                           const int32_t* atom_species, const double* atom_pos);
+
+/* y = H x for ncols columns: Operator.apply_batch = apply_hamiltonian_batched (apply.zig:1584-1618).
+ * x, y: [n x ncols] column-major complex128, host or device.  n must equal n_pw. */
+int dftcuda_apply_h_batch(dftcuda_kctx* ctx, const double* x, double* y, size_t n, size_t ncols);
+/* Single column: Operator.apply = apply_hamiltonian (apply.zig:643-658). */
+int dftcuda_apply_h(dftcuda_kctx* ctx, const double* x, double* y, size_t n);
+/* Device pointers only, enqueued on `stream` (a cudaStream_t; NULL = the context's stream),
+ * no host synchronisation. */
+int dftcuda_apply_h_batch_async(dftcuda_kctx* ctx, const double* x_dev, double* y_dev, size_t ncols, void* stream);
+
+/* Re <psi_b|V_nl|psi_b> for nbands columns (kpoint/density.zig:145-165, 238-266). Host or device. */
+int dftcuda_nonlocal_energies(dftcuda_kctx* ctx, const double* psi, size_t n, size_t nbands, double* e_out);
+
+/* ------------------------------------------------------------------------------------------
+ * Eigensolver: lobpcg_serial.solve (src/features/linalg/lobpcg/serial.zig:55-307) with
+ * Options (lobpcg/common.zig:44-52).  The whole Davidson loop runs on the device; H is the
+ * context's operator.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct dftcuda_eig_opts {
+  size_t max_iter;      /* default 40 */
+  double tol;           /* default 1e-6 */
+  size_t max_subspace;  /* 0 = min(n, 4*nbands+8) */
+  size_t block_size;    /* 0 = min(max_subspace, nbands+4) */
+  int init_diagonal;    /* bool */
+} dftcuda_eig_opts;
+
+typedef struct dftcuda_eig_info {
+  size_t iterations;    /* Davidson iterations run */
+  size_t h_applies;     /* columns passed through H */
+  int converged;        /* 1 when max residual < tol or no vector could be added */
+  double max_residual;  /* at the last iteration */
+} dftcuda_eig_info;
+
+/* diag[n] is the preconditioner diagonal (kinetic |k+G|^2, kpoint/solve.zig:362-367).
+ * init_vecs: optional [n x init_cols] warm start (KpointCache, kpoint/data.zig:7-46), NULL for none.
+ * values_out[nbands], vectors_out[n x nbands]; all host or device.  info may be NULL. */
+int dftcuda_eig_solve(dftcuda_kctx* ctx, const double* diag, size_t nbands, const dftcuda_eig_opts* opts,
+                      const double* init_vecs, size_t init_cols, double* values_out, double* vectors_out,
+                      dftcuda_eig_info* info);
+
+/* ------------------------------------------------------------------------------------------
+ * Band density: rho(r) += sum_b weight_b |psi_b(r)|^2 / Omega
+ * (accumulate_band_density_fft, kpoint/density.zig:444-474; weights w_k*occ*2 as in :98-112).
+ * vectors [n x nbands], weights[nbands] (bands with weight <= 0 are skipped), rho[N] on the FFT
+ * box (x fastest) is ADDED to.  Host or device pointers.
+ * ------------------------------------------------------------------------------------------ */
+int dftcuda_accumulate_density(dftcuda_kctx* ctx, const double* vectors, size_t n, size_t nbands,
+                               const double* weights, double* rho);
+
+/* ------------------------------------------------------------------------------------------
+ * Profiling: the ScfProfile counters (src/features/scf/logging.zig:114-131) measured on the device
+ * with CUDA events on the context's launch stream.  The fused local-potential passes replace the
+ * reference's scatter / ifft / vmul / fft / gather sub-timers with the three pass timers below.
+ * set_profiling(1) clears and starts the counters; get_profile synchronises the context's stream.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct dftcuda_profile {
+  uint64_t apply_h_ns;          /* all H|psi> kernels                                              */
+  uint64_t apply_local_ns;      /* local potential + kinetic (the three passes)                    */
+  uint64_t apply_nonlocal_ns;   /* projector GEMMs and D_ij                                        */
+  uint64_t density_ns;          /* band-density kernels                                            */
+  uint64_t subspace_ns;         /* eigensolver kernels outside H: V^H W, Jacobi, V C, Gram-Schmidt */
+  uint64_t apply_h_calls;       /* block applications of H                                         */
+  uint64_t apply_h_columns;     /* columns through H                                               */
+  uint64_t local_plane_inv_ns;  /* scatter + inverse FFT along z and y                             */
+  uint64_t local_xline_ns;      /* inverse x FFT, x V(r), forward x FFT                            */
+  uint64_t local_plane_fwd_ns;  /* forward FFT along y and z, gather x 1/N, + kinetic              */
+  uint64_t local_plane_inv_launches;
+  uint64_t local_xline_launches;
+  uint64_t local_plane_fwd_launches;
+  uint64_t nl_project_ns;       /* <beta|psi> GEMM                                                 */
+  uint64_t nl_dij_ns;           /* D_ij                                                            */
+  uint64_t nl_backproject_ns;   /* sum |beta> D <beta|psi> GEMM                                    */
+  uint64_t kernel_launches;     /* libdftcuda kernels launched on this context while profiling     */
+} dftcuda_profile;
+
+int dftcuda_kctx_set_profiling(dftcuda_kctx* ctx, int enable);
+int dftcuda_kctx_get_profile(dftcuda_kctx* ctx, dftcuda_profile* out);
+
+/* ------------------------------------------------------------------------------------------
+ * Standalone 3D FFT with the FFTW backend's semantics: in place, forward e^{-i} unnormalised,
+ * inverse e^{+i} scaled by 1/N (Fft3dPlan.forward/inverse, features/fft/fft.zig:224-263;
+ * fftw_fft.zig:141-166).  direction: -1 forward, +1 inverse.  data: N complex128, host or device.
+ * ------------------------------------------------------------------------------------------ */
+int dftcuda_fft_plan_create(dftcuda_fft_plan** out, int nx, int ny, int nz);
+int dftcuda_fft_plan_destroy(dftcuda_fft_plan* plan);
+int dftcuda_fft3d(dftcuda_fft_plan* plan, double* data, int direction);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DFTCUDA_H */

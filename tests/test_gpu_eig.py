@@ -1,0 +1,87 @@
+"""Device Davidson eigensolver (lobpcg_serial.solve) against the golden KATs and the oracle.
+
+Eigenvalue tolerance 1e-7 Ry (the plain-FP64 parity bar), with the solver run at tol 1e-9."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import lobpcg
+from tests.helpers import kproblem, make_context
+
+pytestmark = pytest.mark.gpu
+
+
+def _diag_context(dz, diag):
+    """A context whose H is diag(values): kinetic = diag, V(r) = 0, no projectors."""
+    n = len(diag)
+    hkl = np.array([[i, 0, 0] for i in range(n)], dtype=np.int32)
+    kc = dz.KpointContext(8, 4, 4, 1.0, hkl, np.asarray(diag, float), np.zeros((n, 3)))
+    kc.set_vloc(np.zeros(8 * 4 * 4))
+    return kc
+
+
+@pytest.mark.parametrize("case", range(2))
+def test_lobpcg_diagonal_kats(dz, case):
+    with open(os.path.join(os.path.dirname(__file__), "golden", "lobpcg_diag.json")) as f:
+        doc = json.load(f)["cases"][case]
+    kc = _diag_context(dz, doc["diag"])
+    r = kc.hermitian_eigen_decomp_iterative(np.array(doc["diag"]), doc["nbands"], dz.Options(max_iter=doc["max_iter"], tol=doc["tol"]))
+    assert np.abs(r.values - np.array(doc["expected"])).max() < doc["atol"]
+    kc.close()
+
+
+@pytest.mark.parametrize("k", [(0.0, 0.0, 0.0), (0.25, 0.125, 0.0), (0.5, 0.25, 0.75)])
+def test_si2_eigenvalues_match_oracle(dz, k):
+    kp = kproblem("si2", 20.0, k)
+    kc = make_context(dz, kp)
+    diag = kp.ctx.basis.kinetic
+    opts = dict(max_iter=200, tol=1e-9)
+    r = kc.hermitian_eigen_decomp_iterative(diag, 8, dz.Options(**opts))
+    ref = lobpcg.solve(lobpcg.Operator(kp.ctx.n, kp.ctx.apply_batch), diag, 8, lobpcg.Options(**opts))
+    dense = np.linalg.eigvalsh(kp.ctx.dense_hamiltonian())[:8]
+    assert r.converged
+    assert np.abs(r.values - ref.values).max() < 1e-7
+    assert np.abs(r.values - dense).max() < 1e-7
+    # Ritz vectors are eigenvectors: ||H v - lambda v|| small, orthonormal
+    hv = kp.ctx.apply_batch(r.vectors)
+    res = np.linalg.norm(hv - r.values[:, None] * r.vectors, axis=1)
+    assert res.max() < 1e-8
+    assert np.abs(r.vectors.conj() @ r.vectors.T - np.eye(8)).max() < 1e-10
+    kc.close()
+
+
+def test_init_diagonal_and_warm_start(dz):
+    kp = kproblem("si2", 20.0, (0.25, 0.25, 0.0))
+    kc = make_context(dz, kp)
+    diag = kp.ctx.basis.kinetic
+    dense = np.linalg.eigvalsh(kp.ctx.dense_hamiltonian())[:8]
+    r = kc.hermitian_eigen_decomp_iterative(diag, 8, dz.Options(max_iter=200, tol=1e-9, init_diagonal=True))
+    assert np.abs(r.values - dense).max() < 1e-7
+    # warm start from converged vectors converges at once
+    r2 = kc.hermitian_eigen_decomp_iterative(diag, 8, dz.Options(max_iter=200, tol=1e-8, init_vectors=r.vectors))
+    assert np.abs(r2.values - dense).max() < 1e-7
+    assert r2.iterations <= 3
+    kc.close()
+
+
+def test_al4_twelve_bands_with_restarts(dz):
+    kp = kproblem("al4", 25.0, (0.125, 0.25, 0.375))
+    kc = make_context(dz, kp)
+    diag = kp.ctx.basis.kinetic
+    r = kc.hermitian_eigen_decomp_iterative(diag, 12, dz.Options(max_iter=300, tol=1e-9, max_subspace=32))
+    dense = np.linalg.eigvalsh(kp.ctx.dense_hamiltonian())[:12]
+    assert r.converged
+    assert np.abs(r.values - dense).max() < 1e-7
+    kc.close()
+
+
+def test_not_converged_returns_best_estimate(dz):
+    """serial.zig:298-306: no error when max_iter runs out; the last Ritz values come back."""
+    kp = kproblem("si2", 20.0)
+    kc = make_context(dz, kp)
+    r = kc.hermitian_eigen_decomp_iterative(kp.ctx.basis.kinetic, 8, dz.Options(max_iter=1, tol=1e-12))
+    assert not r.converged and r.iterations == 1
+    assert np.all(np.isfinite(r.values))
+    kc.close()

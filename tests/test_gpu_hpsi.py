@@ -1,0 +1,128 @@
+"""H|psi> on the GPU (through the C ABI) against the oracle's restatement of apply.zig.
+
+Tolerances: FP64 path max relative error 1e-11 (FFT round-off only); FP32 FFT passes 5e-5."""
+import numpy as np
+import pytest
+
+from oracle import fft as offt
+from tests.helpers import kproblem, make_context, random_block, rel_err
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    ("si2", 20.0, (0.25, 0.125, 0.0)),
+    ("si2", 20.0, (0.0, 0.0, 0.0)),
+    ("al4", 25.0, (0.1, 0.2, 0.3)),
+    ("sige8", 20.0, (0.25, 0.25, 0.25)),
+    ("si8", 20.0, (0.5, 0.0, 0.0)),
+]
+
+
+@pytest.mark.parametrize("name,ecut,k", CASES)
+def test_apply_batched_fp64(dz, name, ecut, k):
+    kp = kproblem(name, ecut, k)
+    kc = make_context(dz, kp)
+    x = random_block(kp.ctx.n, 7, 11)
+    y = kc.apply_hamiltonian_batched(x)
+    ref = kp.ctx.apply_batch(x)
+    assert rel_err(y, ref) < 1e-11
+    # single-column Operator.apply agrees with the batch
+    y1 = kc.apply_hamiltonian(x[3])
+    assert rel_err(y1, ref[3]) < 1e-11
+    kc.close()
+
+
+def test_apply_batched_si64_full_box(dz):
+    """Si64 2x2x2 supercell, 30 Ry, 75^3 box, 64 atoms of projectors."""
+    kp = kproblem("si64", 30.0)
+    kc = make_context(dz, kp)
+    x = random_block(kp.ctx.n, 3, 5)
+    assert rel_err(kc.apply_hamiltonian_batched(x), kp.ctx.apply_batch(x)) < 1e-11
+    kc.close()
+
+
+def test_apply_many_columns_chunked(dz):
+    """More columns than one box-workspace chunk holds."""
+    kp = kproblem("si8", 20.0)
+    kc = make_context(dz, kp)
+    kc_budget_cols = 70
+    x = random_block(kp.ctx.n, kc_budget_cols, 2)
+    y = kc.apply_hamiltonian_batched(x)
+    ref = kp.ctx.apply_batch(x)
+    assert rel_err(y, ref) < 1e-11
+    kc.close()
+
+
+@pytest.mark.parametrize("name,ecut,k", CASES[:3])
+def test_apply_batched_fp32_passes(dz, name, ecut, k):
+    kp = kproblem(name, ecut, k)
+    kc = make_context(dz, kp, precision=dz.PRECISION_FP32)
+    x = random_block(kp.ctx.n, 5, 3)
+    assert rel_err(kc.apply_hamiltonian_batched(x), kp.ctx.apply_batch(x)) < 5e-5
+    kc.close()
+
+
+def test_device_pointer_path_matches_host(dz):
+    import torch
+
+    kp = kproblem("si2", 20.0, (0.25, 0.0, 0.0))
+    kc = make_context(dz, kp)
+    x = random_block(kp.ctx.n, 4, 9)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.empty_like(xd)
+    kc.apply_hamiltonian_batched(xd, yd, kp.ctx.n, 4)
+    assert rel_err(yd.cpu().numpy(), kc.apply_hamiltonian_batched(x)) < 1e-14
+    kc.close()
+
+
+def test_nonlocal_energies(dz):
+    kp = kproblem("si8", 20.0, (0.25, 0.0, 0.0))
+    kc = make_context(dz, kp)
+    x = random_block(kp.ctx.n, 4, 4)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    e = kc.nonlocal_energies(x)
+    ref = np.array([kp.ctx.nonlocal_energy(v) for v in x])
+    assert np.abs(e - ref).max() < 1e-11 * max(1.0, np.abs(ref).max())
+    kc.close()
+
+
+def test_local_potential_kat_through_abi(dz):
+    """src/tests.zig:872-973 on the full 4^3 box through the C ABI: V psi = V_G for psi = delta(G=0)."""
+    import os
+
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "local_potential_kat.npz"))
+    nx, ny, nz = (int(v) for v in d["dims"])
+    N = nx * ny * nz
+    # the full box as a basis, in FFT order: Miller index of position i is index_to_freq
+    def freq(i, n):
+        return i if i <= (n - 1) // 2 else i - n
+
+    hkl = np.array([[freq(x, nx), freq(y, ny), freq(z, nz)] for z in range(nz) for y in range(ny) for x in range(nx)], dtype=np.int32)
+    kc = dz.KpointContext(nx, ny, nz, 1.0, hkl, np.zeros(N), np.zeros((N, 3)))
+    local_r = offt.fft3d_inverse(d["v1"] * N, nx, ny, nz).real.copy()
+    kc.set_vloc(local_r)
+    out = kc.apply_hamiltonian(d["psi1"])
+    assert np.abs(out[:5] - d["expected1"][:5]).max() < float(d["tol"])
+    assert np.abs(out - d["expected1"]).max() < float(d["tol"])
+    kc.close()
+
+
+def test_errors_map_to_reference(dz):
+    kp = kproblem("si2", 20.0)
+    kc = make_context(dz, kp)
+    with pytest.raises(dz.InvalidMatrixSize):
+        kc.apply_hamiltonian_batched(np.zeros((2, kp.ctx.n + 1), np.complex128), n=kp.ctx.n + 1, ncols=2)
+    kc.close()
+    b = kp.ctx.basis
+    with pytest.raises(dz.InvalidGrid):
+        dz.KpointContext(6, 6, 6, kp.grid.volume, b.hkl, b.kinetic, b.cart)
+    with pytest.raises(dz.Unsupported):
+        dz.KpointContext(21, 20, 20, kp.grid.volume, b.hkl, b.kinetic, b.cart)
+
+
+def test_zero_columns_is_a_noop(dz):
+    kp = kproblem("si2", 20.0)
+    kc = make_context(dz, kp)
+    y = kc.apply_hamiltonian_batched(np.zeros((0, kp.ctx.n), np.complex128), ncols=0)
+    assert y.shape == (0, kp.ctx.n)
+    kc.close()

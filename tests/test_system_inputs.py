@@ -1,0 +1,36 @@
+"""The package's host-side inputs (dft-zig_b200/system.py) equal the oracle's restatement."""
+import importlib
+
+import numpy as np
+import pytest
+
+from oracle import cases
+
+import dftzig_loader
+
+dftzig_loader.load()
+system = importlib.import_module("dftzig_b200.system")
+
+
+@pytest.mark.parametrize("name,ecut,k", [("si2", 20.0, (0.25, 0.125, 0.0)), ("al4", 25.0, (0.1, 0.2, 0.3)), ("sige8", 20.0, (0.0, 0.5, 0.25))])
+def test_inputs_match_oracle(name, ecut, k):
+    c = system.crystal(name, 1)
+    inp = system.kpoint_inputs(c, ecut, k)
+    kp = cases.make_kproblem(cases.make_cell(name, 1), ecut, k)
+    assert inp.dims == (kp.grid.nx, kp.grid.ny, kp.grid.nz)
+    b = kp.ctx.basis
+    assert (inp.basis.hkl == b.hkl).all()
+    assert np.array_equal(inp.basis.kinetic, b.kinetic)
+    assert np.allclose(inp.positions, np.array([a.position for a in kp.ctx.atoms]), atol=0, rtol=0)
+    assert np.abs(inp.local_r - kp.ctx.local_r).max() < 1e-12 * np.abs(kp.ctx.local_r).max()
+    for (l, d, phi), ns in zip(inp.species_phi, kp.ctx.nl):
+        assert list(l) == list(ns.l_list)
+        assert np.array_equal(d, ns.dij)
+        assert np.abs(phi - ns.phi).max() < 1e-12 * np.abs(ns.phi).max()
+
+
+def test_monkhorst_pack_weights():
+    k = system.monkhorst_pack((2, 2, 2))
+    assert len(k) == 8 and abs(sum(w for _, w in k) - 1.0) < 1e-15
+    k4 = system.monkhorst_pack((4, 4, 4))
+    assert abs(sum(w for _, w in k4) - 1.0) < 1e-15 and len(k4) == 36
