@@ -165,7 +165,10 @@ def run_ours(args):
         x = torch.randn((NCOLS, kc.n), dtype=torch.complex128, device="cuda", generator=gen)
         xs.append(x)
         ys.append(torch.empty_like(x))
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: the legacy default stream's handle is 0, which the C ABI reads as
+    # "use the context's own stream".
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
 
     def step():
@@ -313,7 +316,7 @@ def _cpu_worker(task):
     return dt, ncols, kp.ctx.n, kp.grid.count
 
 
-def cpu_baseline(cols: int = 24):
+def cpu_baseline(cols: int = 160):
     """Single core: the oracle H|psi> on `cols` columns of the Gamma k-point."""
     import multiprocessing as mp
 

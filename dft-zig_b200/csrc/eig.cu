@@ -83,10 +83,11 @@ __global__ void __launch_bounds__(1024) k_jacobi(double2* __restrict__ A, double
   extern __shared__ __align__(16) unsigned char smraw[];
   const int m2 = m + (m & 1);
   const int npair = m2 / 2;
-  int2* pq = reinterpret_cast<int2*>(smraw);
-  double* pc = reinterpret_cast<double*>(smraw + sizeof(int2) * npair);
+  // 16-byte members first so every array stays aligned for any npair.
+  double2* pe = reinterpret_cast<double2*>(smraw);  // e^{-i phi}
+  double* pc = reinterpret_cast<double*>(smraw + sizeof(double2) * npair);
   double* ps = pc + npair;
-  double2* pe = reinterpret_cast<double2*>(ps + npair);  // e^{-i phi}
+  int2* pq = reinterpret_cast<int2*>(ps + npair);
   __shared__ double red[1024];
   __shared__ int conv;
   const int tid = threadIdx.x, nt = blockDim.x;

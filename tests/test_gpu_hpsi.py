@@ -33,10 +33,11 @@ def test_apply_batched_fp64(dz, name, ecut, k):
 
 
 def test_apply_batched_si64_full_box(dz):
-    """Si64 2x2x2 supercell, 30 Ry, 75^3 box, 64 atoms of projectors."""
+    """Si64 2x2x2 supercell, 30 Ry, 75^3 box, 64 atoms of projectors; 36 columns span two
+    box-workspace chunks."""
     kp = kproblem("si64", 30.0)
     kc = make_context(dz, kp)
-    x = random_block(kp.ctx.n, 3, 5)
+    x = random_block(kp.ctx.n, 36, 5)
     assert rel_err(kc.apply_hamiltonian_batched(x), kp.ctx.apply_batch(x)) < 1e-11
     kc.close()
 
