@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--profile-case", action="store_true", help="small single-k case for ncu captures: Gamma, 32 columns, 2 applications")
     return ap.parse_args()
 
 
@@ -377,8 +378,39 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_case():
+    """One k-point (Gamma) of the benchmark cell, 32 columns, H|psi> twice: a few hundred MB on the
+    device, for ncu captures of single kernels."""
+    import torch
+
+    dz, c, kpts, dims, _ = None, None, None, None, None
+    import dftzig_loader
+
+    dz = dftzig_loader.load()
+    import importlib
+
+    system = importlib.import_module("dftzig_b200.system")
+    c = system.crystal(CELL, SEED)
+    dims = system.fft_box(ECUT, c.recip)
+    inp = system.kpoint_inputs(c, ECUT, (0.0, 0.0, 0.0), dims=dims)
+    kc = dz.KpointContext(dims[0], dims[1], dims[2], inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart)
+    kc.set_vloc(inp.local_r)
+    kc.set_projectors([dz.SpeciesProjectors(l, d, p) for (l, d, p) in inp.species_phi], inp.atom_species, inp.positions)
+    x = torch.randn((32, kc.n), dtype=torch.complex128, device="cuda")
+    y = torch.empty_like(x)
+    s = torch.cuda.Stream()
+    for _ in range(2):
+        kc.apply_hamiltonian_async(x, y, 32, s.cuda_stream)
+    torch.cuda.synchronize()
+    kc.close()
+    print("profile case done", flush=True)
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        run_profile_case()
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

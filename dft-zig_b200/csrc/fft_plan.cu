@@ -71,9 +71,12 @@ int Fft1dPlan::create(int n) {
   const size_t b64 = tw.size() * sizeof(double2), b32 = tw.size() * sizeof(float2), bp = n * sizeof(int);
   DFT_CUDA_TRY(cudaMalloc(&d_buf, b64 + b32 + bp + 64));
   char* base = (char*)d_buf;
+  // A pageable-host cudaMemcpy may return before its DMA lands, and kernels on non-blocking streams
+  // do not wait for the legacy stream; synchronise the device before the tables are used.
   DFT_CUDA_TRY(cudaMemcpy(base, tw.data(), b64, cudaMemcpyHostToDevice));
   DFT_CUDA_TRY(cudaMemcpy(base + b64, tw32.data(), b32, cudaMemcpyHostToDevice));
   DFT_CUDA_TRY(cudaMemcpy(base + b64 + b32, pinv.data(), bp, cudaMemcpyHostToDevice));
+  DFT_CUDA_TRY(cudaDeviceSynchronize());
   dev.tw64 = (const double2*)base;
   dev.tw32 = (const float2*)(base + b64);
   dev.pinv = (const int*)(base + b64 + b32);

@@ -527,12 +527,17 @@ extern "C" int dftcuda_kctx_create(dftcuda_kctx** out, int nx, int ny, int nz, d
     dftcuda_kctx_destroy(c);
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "kctx_create: device tables");
   }
-  cudaMemcpy(c->d_plane_off, cnt.data(), sizeof(int) * (c->n_act + 1), cudaMemcpyHostToDevice);
-  cudaMemcpy(c->d_pw_idx, pw_idx.data(), sizeof(int) * n_pw, cudaMemcpyHostToDevice);
-  cudaMemcpy(c->d_pw_spos, pw_spos.data(), sizeof(int) * n_pw, cudaMemcpyHostToDevice);
-  cudaMemcpy(c->d_slot_xpos, slot_xpos.data(), sizeof(int) * c->n_act, cudaMemcpyHostToDevice);
-  cudaMemcpy(c->d_kinetic, kinetic, sizeof(double) * n_pw, cudaMemcpyHostToDevice);
-  if (cudaMemcpy(c->d_gcart, gcart, sizeof(double) * 3 * n_pw, cudaMemcpyHostToDevice) != cudaSuccess) {
+  // Uploads are ordered on the context's own stream: kernels on that (non-blocking) stream do not
+  // wait for the legacy default stream, where a plain cudaMemcpy from pageable memory may still be
+  // in flight when it returns.
+  cudaStream_t st = c->stream;
+  cudaMemcpyAsync(c->d_plane_off, cnt.data(), sizeof(int) * (c->n_act + 1), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(c->d_pw_idx, pw_idx.data(), sizeof(int) * n_pw, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(c->d_pw_spos, pw_spos.data(), sizeof(int) * n_pw, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(c->d_slot_xpos, slot_xpos.data(), sizeof(int) * c->n_act, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(c->d_kinetic, kinetic, sizeof(double) * n_pw, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(c->d_gcart, gcart, sizeof(double) * 3 * n_pw, cudaMemcpyHostToDevice, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) {
     dftcuda_kctx_destroy(c);
     return fail(DFTCUDA_ERR_CUDA, "kctx_create: upload");
   }
@@ -614,7 +619,7 @@ extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const d
       free_nonlocal(c);
       return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_projectors: phi");
     }
-    cudaMemcpy(dphi, sp.phi, sizeof(double) * (size_t)mt * c->npw, cudaMemcpyHostToDevice);
+    cudaMemcpyAsync(dphi, sp.phi, sizeof(double) * (size_t)mt * c->npw, cudaMemcpyHostToDevice, c->stream);
     for (size_t a = 0; a < n_atoms; ++a) {
       if ((size_t)atom_species[a] != s) continue;
       k_build_projectors<<<ceil_div(c->npw, 256), 256, 0, c->stream>>>(nl.P + (size_t)p * c->npw, dphi, mt, (long)c->npw,
@@ -638,9 +643,10 @@ extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const d
     free_nonlocal(c);
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_projectors: tables");
   }
-  cudaMemcpy(nl.D, D.data(), sizeof(double) * D.size(), cudaMemcpyHostToDevice);
-  cudaMemcpy(nl.proj_off, poff.data(), sizeof(int) * nproj, cudaMemcpyHostToDevice);
-  cudaMemcpy(nl.proj_mt, pmt.data(), sizeof(int) * nproj, cudaMemcpyHostToDevice);
+  cudaMemcpyAsync(nl.D, D.data(), sizeof(double) * D.size(), cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(nl.proj_off, poff.data(), sizeof(int) * nproj, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(nl.proj_mt, pmt.data(), sizeof(int) * nproj, cudaMemcpyHostToDevice, c->stream);
+  DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
   DFT_CUDA_TRY(cudaGetLastError());
   return DFTCUDA_OK;
 }
@@ -683,7 +689,10 @@ extern "C" int dftcuda_nonlocal_energies(dftcuda_kctx* c, const double* psi, siz
   if (!psi || !e_out) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_energies: null buffer");
   const bool dp = is_device_pointer(psi), de = is_device_pointer(e_out);
   if (c->nl.nproj == 0) {
-    if (de) DFT_CUDA_TRY(cudaMemset(e_out, 0, sizeof(double) * nbands));
+    if (de) {
+      DFT_CUDA_TRY(cudaMemsetAsync(e_out, 0, sizeof(double) * nbands, c->stream));
+      DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    }
     else std::memset(e_out, 0, sizeof(double) * nbands);
     return DFTCUDA_OK;
   }
@@ -717,9 +726,10 @@ extern "C" int dftcuda_accumulate_density(dftcuda_kctx* c, const double* vectors
   if (!vectors || !weights || !rho) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "accumulate_density: null buffer");
   // Keep only bands with a positive weight (kpoint/density.zig:104-107, 386-388).
   std::vector<double> hw(nbands);
-  if (is_device_pointer(weights))
-    DFT_CUDA_TRY(cudaMemcpy(hw.data(), weights, sizeof(double) * nbands, cudaMemcpyDeviceToHost));
-  else
+  if (is_device_pointer(weights)) {
+    DFT_CUDA_TRY(cudaMemcpyAsync(hw.data(), weights, sizeof(double) * nbands, cudaMemcpyDeviceToHost, c->stream));
+    DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  } else
     std::memcpy(hw.data(), weights, sizeof(double) * nbands);
   std::vector<size_t> keep;
   for (size_t b = 0; b < nbands; ++b)
@@ -752,3 +762,4 @@ extern "C" int dftcuda_accumulate_density(dftcuda_kctx* c, const double* vectors
   DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return DFTCUDA_OK;
 }
+
