@@ -51,6 +51,7 @@ ABI_SYMBOLS = (
     "dftcuda_fft3d",
     "dftcuda_kctx_set_profiling",
     "dftcuda_kctx_get_profile",
+    "dftcuda_accumulate_density_noalloc",
 )
 
 PRECISION_FP64 = 0
@@ -183,6 +184,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.dftcuda_fft3d.argtypes = [vp, dp, ip]
     lib.dftcuda_kctx_set_profiling.argtypes = [vp, ip]
     lib.dftcuda_kctx_get_profile.argtypes = [vp, ct.POINTER(_Profile)]
+    lib.dftcuda_accumulate_density_noalloc.argtypes = [vp, dp, sz, sz, dp, dp]
     _lib = lib
     return lib
 
@@ -362,6 +364,14 @@ class KpointContext:
             vectors = np.ascontiguousarray(vectors, dtype=np.complex128).reshape(-1, self.n)
         _check(self._lib.dftcuda_accumulate_density(self._h, _ptr(vectors), self.n, w.size, _ptr(w), _ptr(rho)))
         return rho
+
+    def accumulate_band_density_noalloc(self, vectors_dev, weights_dev, rho_dev, nbands=None):
+        """Same result as accumulate_band_density for device tensors, without any device allocation
+        (for callers that cannot allocate: the library uses a fixed 48 MiB scratch array in its
+        device image instead).  Calls that overlap on the GPU share that array and race."""
+        nb = weights_dev.numel() if nbands is None else nbands
+        _check(self._lib.dftcuda_accumulate_density_noalloc(self._h, _ptr(vectors_dev), self.n, nb, _ptr(weights_dev), _ptr(rho_dev)))
+        return rho_dev
 
     def hermitian_eigen_decomp_iterative(self, diag, nbands, opts: Options = Options()) -> EigenDecomp:
         """iterative.zig:67-76 -> lobpcg_serial.solve with this context as the Operator."""

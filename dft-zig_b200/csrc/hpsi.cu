@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "kctx.cuh"
 
@@ -763,3 +764,97 @@ extern "C" int dftcuda_accumulate_density(dftcuda_kctx* c, const double* vectors
   return DFTCUDA_OK;
 }
 
+// ------------------------------------------------------------------------------------------
+// Band density for callers that cannot allocate device memory (a framework that owns all device
+// allocations through its own pool, or a loop that must not take the device-wide synchronisation an
+// allocation can cause).  The scratch lives in a fixed array of the library's device image instead
+// of a cudaMalloc'd buffer: the first kNoAllocMaxBands doubles hold the clamped weights, the rest
+// holds the y-z planes of as many columns at a time as fit.  Nothing in it has to start at zero:
+// each call writes every part of the scratch it later reads (k_plane_inv writes whole planes).
+// The array keeps the last call's contents, and all calls share it, so calls that overlap on the GPU
+// race.
+// ------------------------------------------------------------------------------------------
+namespace dftcuda {
+
+constexpr size_t kNoAllocScratchBytes = DFTCUDA_NOALLOC_SCRATCH_BYTES;
+constexpr size_t kNoAllocMaxBands = DFTCUDA_NOALLOC_MAX_BANDS;
+constexpr size_t kNoAllocWeightBytes = kNoAllocMaxBands * sizeof(double);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch for the current device, looked up once per device.  In host
+// code the array's name is only a host-side stand-in, so kernels always receive this address.
+static int noalloc_scratch(unsigned char** out) {
+  static std::mutex mu;
+  static void* addr[128] = {};
+  int dev = 0;
+  DFT_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return fail(DFTCUDA_ERR_UNSUPPORTED, "accumulate_density_noalloc: device ordinal above 127");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(DFTCUDA_ERR_CUDA, std::string("accumulate_density_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    addr[dev] = p;
+  }
+  *out = static_cast<unsigned char*>(addr[dev]);
+  return DFTCUDA_OK;
+}
+
+// w_out[b] = max(w[b], 0): a band with weight <= 0 contributes nothing (kpoint/density.zig:104-107).
+__global__ void k_nonneg_weights(const double* __restrict__ w, double* __restrict__ w_out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) w_out[i] = w[i] > 0.0 ? w[i] : 0.0;
+}
+
+template <typename T>
+static int density_noalloc(dftcuda_kctx* c, const double2* x, size_t nbands, const double* w, double* rho,
+                           unsigned char* scratch, cudaStream_t s) {
+  set_smem_attrs<T>();
+  double* ws = reinterpret_cast<double*>(scratch);
+  cplx<T>* W = reinterpret_cast<cplx<T>*>(scratch + kNoAllocWeightBytes);
+  const size_t per_col = sizeof(cplx<T>) * (size_t)c->n_act * c->P;
+  const size_t cols = (kNoAllocScratchBytes - kNoAllocWeightBytes) / per_col;
+  if (cols == 0)
+    return fail(DFTCUDA_ERR_UNSUPPORTED, "accumulate_density_noalloc: one column's planes (" + std::to_string(per_col) +
+                                             " bytes) exceed the fixed scratch of " + std::to_string(kNoAllocScratchBytes) + " bytes");
+  k_nonneg_weights<<<ceil_div(nbands, 256), 256, 0, s>>>(w, ws, (int)nbands); count_launch();
+  const size_t smem_plane = sizeof(cplx<T>) * (size_t)c->P;
+  const int J = line_tile(c->nx);
+  const size_t smem_x = (sizeof(cplx<T>) + sizeof(double)) * (size_t)c->nx * J;
+  for (size_t c0 = 0; c0 < nbands; c0 += cols) {
+    const size_t nc = std::min(cols, nbands - c0);
+    dim3 gp(c->n_act, (unsigned)nc);
+    k_plane_inv<T><<<gp, 512, smem_plane, s>>>(x + c0 * c->npw, (long)c->npw, W, c->n_act, c->d_plane_off, c->d_pw_idx,
+                                               c->d_pw_spos, c->fy.dev, c->fz.dev, c->ny, c->nz); count_launch();
+    k_xline_density<T><<<ceil_div(c->P, J), 256, smem_x, s>>>(W, c->n_act, c->d_slot_xpos, c->fx.dev, c->P, (int)nc, J,
+                                                              ws + c0, 1.0 / c->volume, rho); count_launch();
+  }
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}
+
+}  // namespace dftcuda
+
+extern "C" int dftcuda_accumulate_density_noalloc(dftcuda_kctx* c, const double* vectors, size_t n, size_t nbands,
+                                                  const double* weights, double* rho) {
+  if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "accumulate_density_noalloc: null context");
+  if (n != c->npw) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "accumulate_density_noalloc: n != n_pw");
+  if (nbands == 0) return DFTCUDA_OK;
+  if (nbands > kNoAllocMaxBands)
+    return fail(DFTCUDA_ERR_UNSUPPORTED, "accumulate_density_noalloc: nbands " + std::to_string(nbands) +
+                                             " exceeds DFTCUDA_NOALLOC_MAX_BANDS (" + std::to_string(kNoAllocMaxBands) + ")");
+  if (!vectors || !weights || !rho) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "accumulate_density_noalloc: null buffer");
+  if (!is_device_pointer(vectors) || !is_device_pointer(weights) || !is_device_pointer(rho))
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "accumulate_density_noalloc: vectors, weights and rho must be device pointers");
+  unsigned char* scratch = nullptr;
+  DFT_TRY(noalloc_scratch(&scratch));
+  const double2* x = reinterpret_cast<const double2*>(vectors);
+  if (c->precision == DFTCUDA_PRECISION_FP32)
+    DFT_TRY(density_noalloc<float>(c, x, nbands, weights, rho, scratch, c->stream));
+  else
+    DFT_TRY(density_noalloc<double>(c, x, nbands, weights, rho, scratch, c->stream));
+  DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return DFTCUDA_OK;
+}

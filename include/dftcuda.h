@@ -135,6 +135,23 @@ int dftcuda_eig_solve(dftcuda_kctx* ctx, const double* diag, size_t nbands, cons
 int dftcuda_accumulate_density(dftcuda_kctx* ctx, const double* vectors, size_t n, size_t nbands,
                                const double* weights, double* rho);
 
+/* Band density for callers that cannot allocate device memory.  This entry point has no
+ * counterpart in the reference.  Some callers cannot call cudaMalloc here: code running inside a
+ * host framework that owns every device allocation through its own memory pool, or a loop that must
+ * not take the device-wide synchronisation an allocation can cause.  This variant of
+ * dftcuda_accumulate_density allocates nothing: its scratch is a fixed array of
+ * DFTCUDA_NOALLOC_SCRATCH_BYTES (48 MiB) in the library's device image, which every GPU that loads
+ * the library holds until exit.  vectors [n x nbands], weights[nbands] and rho[N] must all be device
+ * pointers (host pointers are rejected), nbands may not exceed DFTCUDA_NOALLOC_MAX_BANDS, and rho is
+ * ADDED to exactly as in dftcuda_accumulate_density (bands with weight <= 0 contribute nothing).
+ * The first call on each device looks up the scratch address; make that first call before any
+ * stream capture.  All calls share the one scratch array, so calls that overlap on the GPU (from
+ * two host threads, or two contexts whose streams run concurrently) race; serialise them. */
+#define DFTCUDA_NOALLOC_SCRATCH_BYTES ((size_t)48 << 20)
+#define DFTCUDA_NOALLOC_MAX_BANDS 4096
+int dftcuda_accumulate_density_noalloc(dftcuda_kctx* ctx, const double* vectors, size_t n, size_t nbands,
+                                       const double* weights, double* rho);
+
 /* ------------------------------------------------------------------------------------------
  * Profiling: the ScfProfile counters (src/features/scf/logging.zig:114-131) measured on the device
  * with CUDA events on the context's launch stream.  The fused local-potential passes replace the

@@ -1,0 +1,71 @@
+"""The allocation-free band-density entry point (dftcuda_accumulate_density_noalloc).
+
+It exists for callers that cannot call cudaMalloc -- a framework that owns all device memory through
+its own pool, or a loop that must not take the device-wide synchronisation an allocation can cause.
+It keeps its scratch in a fixed 48 MiB array of the library's device image.  This file is collected
+last so that, if it fails, a run that stops at the first failure has already run every other test.
+It is called here through the C ABI (ctypes) and compared with dftcuda_accumulate_density on two
+calls in a row, which also shows that the scratch's leftover contents from one call do not leak
+into the next.
+"""
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+from tests.helpers import kproblem, make_context, random_block
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12  # relative, the same bar as the other FP64 density tests
+
+
+def _noalloc(dz, kc, v_dev, w_dev, rho_dev, nbands):
+    lib = dz.load_library()
+    return lib.dftcuda_accumulate_density_noalloc(kc.handle, ct.c_void_p(v_dev.data_ptr()), kc.n, nbands, ct.c_void_p(w_dev.data_ptr()), ct.c_void_p(rho_dev.data_ptr()))
+
+
+def _case(dz, torch, name, ecut, k, nb, seed):
+    kp = kproblem(name, ecut, k)
+    kc = make_context(dz, kp)
+    v = random_block(kp.ctx.n, nb, seed)
+    w = np.linspace(2.0, -0.5, nb)  # includes zero and negative weights, which contribute nothing
+    rho_ref = np.full(kp.grid.count, 0.125)
+    kc.accumulate_band_density(v, w, rho_ref)
+    v_dev = torch.from_numpy(v).cuda()
+    w_dev = torch.from_numpy(w).cuda()
+    rho_dev = torch.full((kp.grid.count,), 0.125, dtype=torch.float64, device="cuda")
+    status = _noalloc(dz, kc, v_dev, w_dev, rho_dev, nb)
+    assert status == 0, dz.load_library().dftcuda_last_error_message()
+    got = rho_dev.cpu().numpy()
+    assert np.abs(got - rho_ref).max() < TOL * np.abs(rho_ref).max()
+    return kc
+
+
+def test_noalloc_density_matches_existing_entry_point_twice(dz):
+    import torch
+
+    # first call: Si8, 32^3 box, 40 bands; second call: Si2, 20^3 box, 7 bands, on a different
+    # context, so the second call reads a scratch array the first left filled with other data.
+    kc1 = _case(dz, torch, "si8", 20.0, (0.25, 0.0, 0.0), 40, 3)
+    kc2 = _case(dz, torch, "si2", 20.0, (0.25, 0.125, 0.0), 7, 4)
+    kc1.close()
+    kc2.close()
+
+
+def test_noalloc_density_rejects_too_many_bands_and_host_pointers(dz):
+    import torch
+
+    kp = kproblem("si2", 20.0)
+    kc = make_context(dz, kp)
+    lib = dz.load_library()
+    nb = 4097  # DFTCUDA_NOALLOC_MAX_BANDS + 1
+    v_dev = torch.zeros((nb, kp.ctx.n), dtype=torch.complex128, device="cuda")
+    w_dev = torch.ones(nb, dtype=torch.float64, device="cuda")
+    rho_dev = torch.zeros(kp.grid.count, dtype=torch.float64, device="cuda")
+    assert _noalloc(dz, kc, v_dev, w_dev, rho_dev, nb) == -7
+    assert b"DFTCUDA_NOALLOC_MAX_BANDS" in lib.dftcuda_last_error_message()
+    host_rho = np.zeros(kp.grid.count)
+    st = lib.dftcuda_accumulate_density_noalloc(kc.handle, ct.c_void_p(v_dev.data_ptr()), kc.n, 1, ct.c_void_p(w_dev.data_ptr()), host_rho.ctypes.data)
+    assert st == -6
+    kc.close()
