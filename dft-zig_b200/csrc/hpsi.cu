@@ -16,8 +16,10 @@
 // The net scaling equals the reference's (xN on scatter, 1/N in the inverse, 1/N on gather).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <string>
 
 #include "kctx.cuh"
 
@@ -363,10 +365,17 @@ int kctx_apply_h_dev(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols
     const size_t nc = std::min(ch, ncols - c0);
     const double2* xc = x + c0 * c->npw;
     double2* yc = y + c0 * c->npw;
-    if (c->precision == DFTCUDA_PRECISION_FP32)
-      DFT_TRY(local_block<float>(c, xc, yc, nc, s));
-    else
-      DFT_TRY(local_block<double>(c, xc, yc, nc, s));
+    if (c->precision == DFTCUDA_PRECISION_FP32) {
+      if (c->fast32)
+        DFT_TRY(local_block4<float>(c, xc, yc, nc, s));
+      else
+        DFT_TRY(local_block<float>(c, xc, yc, nc, s));
+    } else {
+      if (c->fast64)
+        DFT_TRY(local_block4<double>(c, xc, yc, nc, s));
+      else
+        DFT_TRY(local_block<double>(c, xc, yc, nc, s));
+    }
   }
   if (c->nl.nproj > 0) {
     const size_t nch = std::min<size_t>(ncols, 256);
@@ -403,10 +412,17 @@ int kctx_density_dev(dftcuda_kctx* c, const double2* vecs, size_t nbands, const 
   DFT_TRY(ensure_box(c, ch));
   for (size_t c0 = 0; c0 < nbands; c0 += ch) {
     const size_t nc = std::min(ch, nbands - c0);
-    if (c->precision == DFTCUDA_PRECISION_FP32)
-      DFT_TRY(density_block<float>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
-    else
-      DFT_TRY(density_block<double>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
+    if (c->precision == DFTCUDA_PRECISION_FP32) {
+      if (c->fast32)
+        DFT_TRY(density_block4<float>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
+      else
+        DFT_TRY(density_block<float>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
+    } else {
+      if (c->fast64)
+        DFT_TRY(density_block4<double>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
+      else
+        DFT_TRY(density_block<double>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
+    }
   }
   return DFTCUDA_OK;
 }
@@ -447,7 +463,9 @@ extern "C" int dftcuda_kctx_destroy(dftcuda_kctx* c) {
   c->prof.destroy();
   free_nonlocal(c);
   void* ptrs[] = {c->d_plane_off, c->d_pw_idx, c->d_pw_spos, c->d_slot_xpos, c->d_kinetic, c->d_gcart, c->d_vt,
-                  c->d_vt32, c->d_box, c->d_coef, c->d_coef2, c->d_gemm_ws, c->d_x, c->d_y, c->d_rho, c->d_w};
+                  c->d_vt32, c->d_box, c->d_coef, c->d_coef2, c->d_gemm_ws, c->d_x, c->d_y, c->d_rho, c->d_w,
+                  c->d_pwmap, c->d_stick_off, c->d_stick_y, c->d_slot_of_x, c->d_tw4x64, c->d_tw4x32,
+                  c->d_tw4p64, c->d_tw4p32};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   c->fx.destroy(); c->fy.destroy(); c->fz.destroy();
@@ -541,6 +559,14 @@ extern "C" int dftcuda_kctx_create(dftcuda_kctx** out, int nx, int ny, int nz, d
   if (cudaStreamSynchronize(st) != cudaSuccess) {
     dftcuda_kctx_destroy(c);
     return fail(DFTCUDA_ERR_CUDA, "kctx_create: upload");
+  }
+  // The four-step register-FFT passes, unless DFTCUDA_FFT_PATH=generic asks for the stage-by-stage ones.
+  const char* path = std::getenv("DFTCUDA_FFT_PATH");
+  if (!(path && std::string(path) == "generic")) {
+    if ((s = kctx_setup_fast_path(c, slot_of_x, xpos, hkl)) != DFTCUDA_OK) {
+      dftcuda_kctx_destroy(c);
+      return s;
+    }
   }
   *out = c;
   return DFTCUDA_OK;

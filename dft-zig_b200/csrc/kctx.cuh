@@ -71,6 +71,17 @@ struct dftcuda_kctx {
   double* d_gcart = nullptr;   // [npw*3]
   std::vector<double> h_kinetic;
 
+  // Four-step path tables (local4.cu): used when fast64 / fast32 is set for the precision.
+  bool fast64 = false, fast32 = false;
+  int* d_pwmap = nullptr;      // [n_act][nz][ny] plane-wave index or -1
+  int* d_stick_off = nullptr;  // [n_act+1]
+  int* d_stick_y = nullptr;    // y of each stick, per slot, ascending
+  int* d_slot_of_x = nullptr;  // [nx] slot of each x frequency or -1
+  void* d_tw4x64 = nullptr;
+  void* d_tw4x32 = nullptr;
+  void* d_tw4p64 = nullptr;
+  void* d_tw4p32 = nullptr;
+
   // Local potential transposed to [x][z][y]; FP32 copy for the FP32 passes.
   double* d_vt = nullptr;
   float* d_vt32 = nullptr;
@@ -111,6 +122,14 @@ int kctx_stage(dftcuda_kctx* c, size_t cols);
 int kctx_density_dev(dftcuda_kctx* c, const double2* vecs, size_t nbands, const double* w_dev, double* rho_dev,
                      cudaStream_t s);
 void eig_destroy(KCtxImpl* e);
+
+// Four-step register-FFT path (local4.cu).
+bool kctx_fast_path_ok(const dftcuda_kctx* c, int precision);
+int kctx_setup_fast_path(dftcuda_kctx* c, const std::vector<int>& slot_of_x, const std::vector<int>& xpos,
+                         const int32_t* hkl);
+template <typename T> int local_block4(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols, cudaStream_t s);
+template <typename T>
+int density_block4(dftcuda_kctx* c, const double2* x, size_t ncols, const double* w, double* rho, cudaStream_t s);
 
 // Times the launches between construction and destruction under category `cat` when profiling is on.
 struct ProfScope {

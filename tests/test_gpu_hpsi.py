@@ -127,3 +127,27 @@ def test_zero_columns_is_a_noop(dz):
     y = kc.apply_hamiltonian_batched(np.zeros((0, kp.ctx.n), np.complex128), ncols=0)
     assert y.shape == (0, kp.ctx.n)
     kc.close()
+
+
+@pytest.mark.parametrize("path", ["generic", "four_step"])
+@pytest.mark.parametrize("name,ecut,k,prec", [("si2", 20.0, (0.25, 0.125, 0.0), 0), ("sige8", 20.0, (0.25, 0.25, 0.25), 0), ("al4", 25.0, (0.1, 0.2, 0.3), 1)])
+def test_both_fft_paths_match_oracle(dz, monkeypatch, path, name, ecut, k, prec):
+    """The four-step register-FFT passes and the stage-by-stage passes (DFTCUDA_FFT_PATH=generic)
+    give the oracle's H|psi> and density."""
+    from oracle import density as odens
+
+    if path == "generic":
+        monkeypatch.setenv("DFTCUDA_FFT_PATH", "generic")
+    else:
+        monkeypatch.delenv("DFTCUDA_FFT_PATH", raising=False)
+    kp = kproblem(name, ecut, k)
+    kc = make_context(dz, kp, precision=prec)
+    x = random_block(kp.ctx.n, 6, 21)
+    tol = 1e-11 if prec == 0 else 5e-5
+    assert rel_err(kc.apply_hamiltonian_batched(x), kp.ctx.apply_batch(x)) < tol
+    w = np.array([2.0, 1.0, 0.5, 0.25, 0.0, 1.5])
+    rho = np.zeros(kp.grid.count)
+    kc.accumulate_band_density(x, w, rho)
+    ref = odens.accumulate_density(kp.grid, kp.ctx.map, x, w, 1.0 / kp.grid.volume)
+    assert rel_err(rho, ref) < (1e-12 if prec == 0 else 5e-5)
+    kc.close()
