@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile-case", action="store_true", help="small single-k case for ncu captures: Gamma, 32 columns, 2 applications")
+    ap.add_argument("--workload", choices=("hpsi", "scf"), default="hpsi", help="hpsi: H|psi> GB/s (default); scf: time-to-SCF")
     return ap.parse_args()
 
 
@@ -406,8 +407,66 @@ def run_profile_case():
     print("profile case done", flush=True)
 
 
+def run_scf_workload(args):
+    """Time-to-SCF on Si2 (FCC primitive, a = 5.431 A), 20 Ry, 20^3 box, 4x4x4 Gamma-centred MP mesh
+    folded by time reversal (36 k-points), 8 bands, fixed occupations, Pulay 8 / beta 0.3 potential
+    mixing, the reference's default eigensolver settings (tol 1e-4, 20 iterations, 2 warm-up
+    iterations at 1e-3 / 10) and warm starts.  Target energy: a tight FP64 run on the same device
+    (density RMS 1e-9, eigensolver tol 1e-10).  Reported: wall seconds until |E - E_target| < 1e-6
+    Ry/atom, plain FP64 and mixed (FP32 FFT passes until the density residual < 1e-5)."""
+    import importlib
+
+    import torch
+
+    import dftzig_loader
+
+    dz = dftzig_loader.load()
+    scf = importlib.import_module("dftzig_b200.scf")
+    system = importlib.import_module("dftzig_b200.system")
+    c = system.crystal("si2")
+    base = dict(ecut=20.0, kmesh=(4, 4, 4), nbands=8, mixing_beta=0.3, pulay_history=8, max_iter=60)
+    tight = scf.ScfParams(**base, convergence=1e-9, iterative_tol=1e-10, iterative_max_iter=200, warmup_steps=0)
+    b = scf.GpuBackend(dz, "fp64")
+    ref = scf.run_scf(c, tight, b)
+    b.close()
+    out = {}
+    for mode in ("fp64", "mixed"):
+        p = scf.ScfParams(**base, convergence=1e-12, energy_target=ref.energy, energy_tol_per_atom=1e-6)
+        times = []
+        its = []
+        for _ in range(max(1, args.steps)):
+            torch.cuda.synchronize()
+            b = scf.GpuBackend(dz, mode)
+            r = scf.run_scf(c, p, b)
+            torch.cuda.synchronize()
+            b.close()
+            times.append(r.wall_s)
+            its.append(r.iterations)
+            if not r.converged:
+                raise RuntimeError(f"time-to-SCF run ({mode}) did not reach the target")
+        out[mode] = (float(np.median(times)), int(np.median(its)))
+    line = {
+        "metric": "time-to-SCF (|dE| < 1e-6 Ry/atom vs tight FP64), Si2 20 Ry 4x4x4",
+        "value": round(out["mixed"][0], 3),
+        "unit": "s",
+        "higher_is_better": False,
+        "n_gpus": 1,
+        "steps": max(1, args.steps),
+        "dtype": "f64/f32",
+        "data": "synthetic (synthetic GTH-form Si pseudopotential)",
+        "config": {"workload": "Si2 FCC 5.431 A, 20 Ry, 20^3, 4x4x4 MP (36 k, time-reversal folded), 8 bands, fixed occupations, Pulay 8 beta 0.3",
+                   "target_energy_per_atom": ref.energy_per_atom, "target_iterations": ref.iterations},
+        "fp64": {"seconds": round(out["fp64"][0], 3), "scf_iterations": out["fp64"][1]},
+        "mixed": {"seconds": round(out["mixed"][0], 3), "scf_iterations": out["mixed"][1], "switch": "FP32 FFT passes until drho < 1e-5, then FP64"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "scf":
+        run_scf_workload(args)
+        return
     if args.profile_case:
         run_profile_case()
         return

@@ -13,6 +13,55 @@ namespace dftcuda {
 constexpr int BM = 64, BN = 64, BK = 16;
 
 template <bool AKC, bool BKC, bool CJA, bool CJB>
+__device__ __forceinline__ void zgemm_load_tile(double2 (&ra)[4], double2 (&rb)[4], int M, int N, int kend, int r0, int c0,
+                                                int k0, const double2* __restrict__ A, long lda,
+                                                const double2* __restrict__ B, long ldb, int tid) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int i = tid + 256 * q;
+    int r, kk;
+    if (AKC) { kk = i % BK; r = i / BK; } else { r = i % BM; kk = i / BM; }
+    const int gr = r0 + r, gk = k0 + kk;
+    double2 v = make_double2(0.0, 0.0);
+    if (gr < M && gk < kend) v = AKC ? __ldg(A + (long)gr * lda + gk) : __ldg(A + (long)gk * lda + gr);
+    if (CJA) v.y = -v.y;
+    ra[q] = v;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int i = tid + 256 * q;
+    int cc, kk;
+    if (BKC) { kk = i % BK; cc = i / BK; } else { cc = i % BN; kk = i / BN; }
+    const int gc = c0 + cc, gk = k0 + kk;
+    double2 v = make_double2(0.0, 0.0);
+    if (gc < N && gk < kend) v = BKC ? __ldg(B + (long)gc * ldb + gk) : __ldg(B + (long)gk * ldb + gc);
+    if (CJB) v.y = -v.y;
+    rb[q] = v;
+  }
+}
+
+template <bool AKC, bool BKC>
+__device__ __forceinline__ void zgemm_store_tile(double2 (*As)[BM + 1], double2 (*Bs)[BN + 1], const double2 (&ra)[4],
+                                                 const double2 (&rb)[4], int tid) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int i = tid + 256 * q;
+    int r, kk;
+    if (AKC) { kk = i % BK; r = i / BK; } else { r = i % BM; kk = i / BM; }
+    As[kk][r] = ra[q];
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int i = tid + 256 * q;
+    int cc, kk;
+    if (BKC) { kk = i % BK; cc = i / BK; } else { cc = i % BN; kk = i / BN; }
+    Bs[kk][cc] = rb[q];
+  }
+}
+
+// Software-pipelined: the next K slice is fetched into registers while the current one is
+// multiplied out of shared memory.
+template <bool AKC, bool BKC, bool CJA, bool CJB>
 __global__ void __launch_bounds__(256) k_zgemm(int M, int N, int K, const double2* __restrict__ A, long lda,
                                                const double2* __restrict__ B, long ldb, double2* __restrict__ O,
                                                long ldo_r, long ldo_c, double alpha, double beta, int kps,
@@ -29,31 +78,15 @@ __global__ void __launch_bounds__(256) k_zgemm(int M, int N, int K, const double
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
-
+  double2 ra[4], rb[4];
+  if (kbeg < kend) {
+    zgemm_load_tile<AKC, BKC, CJA, CJB>(ra, rb, M, N, kend, r0, c0, kbeg, A, lda, B, ldb, tid);
+    zgemm_store_tile<AKC, BKC>(As, Bs, ra, rb, tid);
+  }
+  __syncthreads();
   for (int k0 = kbeg; k0 < kend; k0 += BK) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int i = tid + 256 * q;
-      int r, kk;
-      if (AKC) { kk = i % BK; r = i / BK; } else { r = i % BM; kk = i / BM; }
-      const int gr = r0 + r, gk = k0 + kk;
-      double2 v = make_double2(0.0, 0.0);
-      if (gr < M && gk < kend) v = AKC ? A[(long)gr * lda + gk] : A[(long)gk * lda + gr];
-      if (CJA) v.y = -v.y;
-      As[kk][r] = v;
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int i = tid + 256 * q;
-      int cc, kk;
-      if (BKC) { kk = i % BK; cc = i / BK; } else { cc = i % BN; kk = i / BN; }
-      const int gc = c0 + cc, gk = k0 + kk;
-      double2 v = make_double2(0.0, 0.0);
-      if (gc < N && gk < kend) v = BKC ? B[(long)gc * ldb + gk] : B[(long)gk * ldb + gc];
-      if (CJB) v.y = -v.y;
-      Bs[kk][cc] = v;
-    }
-    __syncthreads();
+    const bool more = k0 + BK < kend;
+    if (more) zgemm_load_tile<AKC, BKC, CJA, CJB>(ra, rb, M, N, kend, r0, c0, k0 + BK, A, lda, B, ldb, tid);
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
       double2 a[4], b[4];
@@ -72,6 +105,10 @@ __global__ void __launch_bounds__(256) k_zgemm(int M, int N, int K, const double
         }
     }
     __syncthreads();
+    if (more) {
+      zgemm_store_tile<AKC, BKC>(As, Bs, ra, rb, tid);
+      __syncthreads();
+    }
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i)

@@ -1,0 +1,428 @@
+"""Host-side SCF driver around the GPU hot path (the caller's side of the boundary).
+
+dft-zig keeps its SCF driver in Zig; this module restates the pieces needed to reach total energies
+and time-to-SCF with the hot path on the GPU, each following the cited reference code:
+
+  flat start rho_0 = N_e / Omega                  scf/run_state.zig:98-115
+  V_H(G) = 8 pi rho(G) / |G|^2 (Ry)               scf/potential.zig:34-41
+  LDA-PZ exchange-correlation (Ry)                xc/xc.zig:195-211, 344-384
+  V = V_ion + V_H + V_xc, real part on the grid   scf/potential.zig:144-203, 320-334
+  potential mixing (linear, then Pulay/DIIS from pulay_start on V_Hxc)
+                                                  scf/scf.zig:148-188, scf/mixing.zig:182-248
+  convergence on RMS(rho_out - rho_in)            scf/scf.zig:392-410, scf/util.zig:17-24
+  fixed occupations / Fermi-Dirac + Fermi level   kpoint/density.zig:98-112, scf/fermi_level.zig
+  total energy = band + (-E_H - int V_xc rho + E_xc) + E_ion-ion + psp_core - TS
+                                                  scf/energy.zig:372-396
+  Ewald ion-ion energy                            ewald/ewald.zig (standard Ewald split)
+  eigensolver warm start from the previous iteration's vectors
+                                                  kpoint/data.zig:7-46, defaults.zig:40
+  warm-up iterations with looser eigensolver settings
+                                                  scf/density.zig:167-176, defaults.zig:37-39
+
+The hot path (H|psi>, the Davidson solver, the band density) runs through a backend object:
+``GpuBackend`` drives libdftcuda through the package's KpointContext.  Tests plug in other
+backends through the same small interface.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import system as sysm
+
+
+# ---------------------------------------------------------------------------------------------
+# Exchange-correlation, Hartree, ionic terms
+# ---------------------------------------------------------------------------------------------
+
+
+def lda_pz(n: np.ndarray):
+    """xc.zig:195-211, 344-384: returns (f, v) in Ry (f per unit volume, v = df/dn); n <= 1e-12 -> 0."""
+    n = np.asarray(n, dtype=np.float64)
+    f = np.zeros_like(n)
+    v = np.zeros_like(n)
+    m = n > 1e-12
+    nn = n[m]
+    n13 = np.power(nn, 1.0 / 3.0)
+    c_x = -0.75 * (3.0 / math.pi) ** (1.0 / 3.0)
+    ex = nn * c_x * n13
+    rs = np.power(3.0 / (4.0 * math.pi * nn), 1.0 / 3.0)
+    eps_c = np.empty_like(nn)
+    v_c = np.empty_like(nn)
+    lo = rs < 1.0
+    a, b, c, d = 0.0311, -0.048, 0.0020, -0.0116
+    r = rs[lo]
+    lr = np.log(r)
+    e = a * lr + b + c * r * lr + d * r
+    de = a / r + c * lr + c + d
+    eps_c[lo] = e
+    v_c[lo] = e - (r / 3.0) * de
+    g, b1, b2 = -0.1423, 1.0529, 0.3334
+    r = rs[~lo]
+    sr = np.sqrt(r)
+    den = 1.0 + b1 * sr + b2 * r
+    e = g / den
+    de = -g * (0.5 * b1 / sr + b2) / (den * den)
+    eps_c[~lo] = e
+    v_c[~lo] = e - (r / 3.0) * de
+    f[m] = 2.0 * (ex + nn * eps_c)
+    v[m] = 2.0 * (4.0 / 3.0 * c_x * n13 + v_c)
+    return f, v
+
+
+def ewald_energy(cell: np.ndarray, charges: np.ndarray, pos: np.ndarray, tol: float = 1e-14) -> float:
+    """Ion-ion energy (Ry) by the Ewald split: real-space erfc sum + reciprocal sum - self - background."""
+    from scipy.special import erfc
+
+    vol = abs(np.linalg.det(cell))
+    recip = 2.0 * math.pi * np.linalg.inv(cell).T
+    eta = math.sqrt(math.pi) / vol ** (1.0 / 3.0)
+    # real-space cutoff where erfc(eta r) < tol, reciprocal cutoff where exp(-G^2/4eta^2) < tol
+    rcut = math.sqrt(-math.log(tol)) / eta + 1e-9
+    gcut = 2.0 * eta * math.sqrt(-math.log(tol))
+    na = [int(math.ceil(rcut * np.linalg.norm(recip[i]) / (2.0 * math.pi))) + 1 for i in range(3)]
+    e_real = 0.0
+    rng = [np.arange(-n, n + 1) for n in na]
+    L = np.stack(np.meshgrid(*rng, indexing="ij"), axis=-1).reshape(-1, 3) @ cell
+    for i in range(len(charges)):
+        d = pos[i][None, :] - pos  # [j, 3]
+        r = np.linalg.norm(d[:, None, :] + L[None, :, :], axis=2)  # [j, L]
+        mask = (r > 1e-10) & (r < rcut)
+        e_real += 0.5 * charges[i] * np.sum((charges[:, None] * erfc(eta * r) / np.where(mask, r, 1.0)) * mask)
+    ng = [int(math.ceil(gcut / np.linalg.norm(recip[i]))) + 1 for i in range(3)]
+    rng = [np.arange(-n, n + 1) for n in ng]
+    G = np.stack(np.meshgrid(*rng, indexing="ij"), axis=-1).reshape(-1, 3) @ recip
+    g2 = (G * G).sum(axis=1)
+    sel = (g2 > 1e-12) & (g2 < gcut * gcut)
+    G, g2 = G[sel], g2[sel]
+    sf = np.exp(1j * (G @ pos.T)) @ charges
+    e_rec = (2.0 * math.pi / vol) * np.sum(np.abs(sf) ** 2 * np.exp(-g2 / (4.0 * eta * eta)) / g2)
+    e_self = -eta / math.sqrt(math.pi) * np.sum(charges**2)
+    e_bg = -math.pi * np.sum(charges) ** 2 / (2.0 * eta * eta * vol)
+    return 2.0 * float(e_real + e_rec + e_self + e_bg)
+
+
+def gth_alpha(sp: sysm.SpeciesData) -> float:
+    """G -> 0 limit of Omega (V_loc(G) + 8 pi Z / G^2) for the GTH form (Ry): the epsatm of
+    energy.zig:350-365 for the synthetic species."""
+    p = sp.params
+    rl = p["rloc"]
+    return 2.0 * (2.0 * math.pi * p["z"] * rl * rl + math.sqrt(8.0 * math.pi**3) * rl**3 * (p["c1"] + 3.0 * p["c2"]))
+
+
+# ---------------------------------------------------------------------------------------------
+# Mixing
+# ---------------------------------------------------------------------------------------------
+
+
+class PulayMixer:
+    """mixing.zig:182-248 (mix_with_residual): history of inputs and residuals, DIIS coefficients
+    from B_ij = <R_i|R_j> with the constraint sum c = 1, new = sum c_i (x_i + beta R_i)."""
+
+    def __init__(self, history: int):
+        self.history = history
+        self.xs: list = []
+        self.rs: list = []
+
+    def mix(self, x: np.ndarray, residual: np.ndarray, beta: float) -> np.ndarray:
+        self.xs.append(x.copy())
+        self.rs.append(residual.copy())
+        while len(self.xs) > self.history:
+            self.xs.pop(0)
+            self.rs.pop(0)
+        m = len(self.xs)
+        if m < 2:
+            return x + beta * residual
+        B = np.zeros((m + 1, m + 1))
+        for i in range(m):
+            for j in range(m):
+                B[i, j] = float(np.dot(self.rs[i], self.rs[j]))
+        B[:m, m] = -1.0
+        B[m, :m] = -1.0
+        rhs = np.zeros(m + 1)
+        rhs[m] = -1.0
+        try:
+            c = np.linalg.solve(B, rhs)
+        except np.linalg.LinAlgError:
+            c = np.linalg.lstsq(B, rhs, rcond=None)[0]
+        out = np.zeros_like(x)
+        for i in range(m):
+            out += c[i] * (self.xs[i] + beta * self.rs[i])
+        return out
+
+
+# ---------------------------------------------------------------------------------------------
+# Occupations
+# ---------------------------------------------------------------------------------------------
+
+
+def fd_occ(e, mu, sigma):
+    x = np.clip((np.asarray(e) - mu) / sigma, -700.0, 700.0)
+    return 1.0 / (1.0 + np.exp(x))
+
+
+def fermi_level(nelec, sigma, kweights, values, spin=2.0):
+    """fermi_level.zig:61-124 (bracket with padding max(10 sigma, 1e-3), <= 80 bisections)."""
+    allv = np.concatenate([np.asarray(v) for v in values])
+    lo_e, hi_e = float(allv.min()), float(allv.max())
+
+    def count(mu):
+        return sum(spin * w * float(fd_occ(v, mu, sigma).sum()) for w, v in zip(kweights, values))
+
+    pad = max(10.0 * sigma, 1e-3)
+    low, high = lo_e - pad, hi_e + pad
+    for _ in range(12):
+        if count(low) <= nelec <= count(high):
+            break
+        pad *= 2.0
+        low, high = lo_e - pad, hi_e + pad
+    left, right = low, high
+    for _ in range(80):
+        mid = 0.5 * (left + right)
+        c = count(mid)
+        if abs(c - nelec) < 1e-8:
+            return mid
+        if c > nelec:
+            right = mid
+        else:
+            left = mid
+    return 0.5 * (left + right)
+
+
+def entropy_term(occ):
+    o = np.asarray(occ)
+    m = (o > 1e-12) & (o < 1.0 - 1e-12)
+    s = np.zeros_like(o)
+    s[m] = -(o[m] * np.log(o[m]) + (1.0 - o[m]) * np.log(1.0 - o[m]))
+    return s
+
+
+# ---------------------------------------------------------------------------------------------
+# Backend: the hot path on the GPU
+# ---------------------------------------------------------------------------------------------
+
+
+class GpuBackend:
+    """One libdftcuda k-point context per k-point (the GPU analogue of KpointApplyCache).
+
+    precision "fp64" runs every FFT pass in FP64.  "mixed" keeps a second, FP32 context per k-point
+    and uses it while the SCF density residual is above ``switch_drho``, then the FP64 one for the
+    rest (the subspace algebra, residual checks and occupations stay FP64 throughout)."""
+
+    def __init__(self, dz, precision="fp64", switch_drho: float = 1e-5):
+        self.dz = dz
+        self.precision = precision
+        self.switch_drho = switch_drho
+        self.ctxs = []
+        self.ctxs32 = []
+        self.use32 = precision == "mixed"
+        self.local_r = None
+
+    def _make(self, inp, prec):
+        kc = self.dz.KpointContext(*inp.dims, inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart, prec)
+        kc.set_projectors([self.dz.SpeciesProjectors(l, d, p) for (l, d, p) in inp.species_phi], inp.atom_species, inp.positions)
+        return kc
+
+    def setup(self, kinputs):
+        for inp in kinputs:
+            self.ctxs.append(self._make(inp, 0))
+            if self.precision == "mixed":
+                self.ctxs32.append(self._make(inp, 1))
+
+    def observe(self, drho: float):
+        if self.use32 and drho < self.switch_drho:
+            self.use32 = False
+            if self.local_r is not None:
+                for kc in self.ctxs:
+                    kc.set_vloc(self.local_r)
+
+    def _active(self):
+        return self.ctxs32 if self.use32 else self.ctxs
+
+    def set_vloc(self, local_r):
+        self.local_r = local_r
+        for kc in self._active():
+            kc.set_vloc(local_r)
+
+    def eig(self, k, diag, nbands, opts: dict, init):
+        o = self.dz.Options(**opts, init_vectors=init)
+        r = self._active()[k].hermitian_eigen_decomp_iterative(diag, nbands, o)
+        return r.values, r.vectors
+
+    def density(self, k, vectors, weights, rho):
+        self._active()[k].accumulate_band_density(vectors, weights, rho)
+
+    def nonlocal_energies(self, k, vectors):
+        return self._active()[k].nonlocal_energies(vectors)
+
+    def close(self):
+        for kc in self.ctxs + self.ctxs32:
+            kc.close()
+        self.ctxs = []
+        self.ctxs32 = []
+
+
+# ---------------------------------------------------------------------------------------------
+# The SCF loop
+# ---------------------------------------------------------------------------------------------
+
+
+@dataclass
+class ScfParams:
+    ecut: float
+    kmesh: tuple
+    nbands: int
+    mixing_beta: float = 0.3
+    pulay_history: int = 8
+    pulay_start: int = 4
+    max_iter: int = 50
+    convergence: float = 1e-6
+    iterative_max_iter: int = 20
+    iterative_tol: float = 1e-4
+    warmup_steps: int = 2
+    warmup_max_iter: int = 10
+    warmup_tol: float = 1e-3
+    reuse_vectors: bool = True
+    smearing: Optional[float] = None  # Fermi-Dirac width (Ry); None = fixed occupations
+    energy_tol_per_atom: Optional[float] = None  # stop once |E - E_target| < tol (time-to-SCF runs)
+    energy_target: Optional[float] = None
+
+
+@dataclass
+class ScfResult:
+    converged: bool
+    iterations: int
+    energy: float
+    energy_per_atom: float
+    eigenvalues: list
+    terms: dict
+    rho: np.ndarray
+    history: list = field(default_factory=list)
+    wall_s: float = 0.0
+
+
+def g_vectors(dims, recip):
+    f = [np.fft.fftfreq(n, 1.0 / n) for n in dims]
+    hz, hy, hx = np.meshgrid(f[2], f[1], f[0], indexing="ij")
+    G = np.stack([hx.ravel(), hy.ravel(), hz.ravel()], axis=1) @ recip
+    return (G * G).sum(axis=1)
+
+
+def ionic_potential_g(c: sysm.Crystal, dims, ecut: float) -> np.ndarray:
+    """V_ion(G) on the FFT grid (Ry), G = 0 term 0, |G|^2 <= 4 ecut (the same form factors as
+    system.local_potential)."""
+    n = dims[0] * dims[1] * dims[2]
+    vr = sysm.local_potential(c, dims, ecut)
+    return np.fft.fftn(vr.reshape(dims[2], dims[1], dims[0])).ravel() / n
+
+
+def run_scf(c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False) -> ScfResult:
+    t0 = time.perf_counter()
+    dims = sysm.fft_box(p.ecut, c.recip)
+    N = dims[0] * dims[1] * dims[2]
+    vol = c.volume
+    kpts = sysm.monkhorst_pack(p.kmesh)
+    tables = [[sysm.radial_table(sp, i, p.ecut) for i in range(len(sp.betas))] for sp in c.species]
+    vloc_r = sysm.local_potential(c, dims, p.ecut)
+    kin = [sysm.kpoint_inputs(c, p.ecut, k, dims=dims, local_r=vloc_r, tables=tables) for k, _ in kpts]
+    kweights = [w for _, w in kpts]
+    backend.setup(kin)
+    g2 = g_vectors(dims, c.recip)
+    gmask = g2 > 1e-12
+    nelec = c.nelec
+    nocc = int(math.ceil(nelec / 2.0 - 1e-12))
+    nbands = max(p.nbands, nocc)
+
+    def to_g(fr):
+        return np.fft.fftn(fr.reshape(dims[2], dims[1], dims[0])).ravel() / N
+
+    def to_r(fg):
+        return np.fft.ifftn(fg.reshape(dims[2], dims[1], dims[0])).ravel().real * N
+
+    def hxc_g(rho):
+        rg = to_g(rho)
+        vh = np.zeros_like(rg)
+        vh[gmask] = 8.0 * math.pi * rg[gmask] / g2[gmask]
+        _, vxc = lda_pz(rho)
+        return vh + to_g(vxc)
+
+    rho = np.full(N, nelec / vol)
+    v_hxc = hxc_g(rho)
+    mixer = PulayMixer(p.pulay_history)
+    vectors = [None] * len(kpts)
+    e_ion = ewald_energy(c.cell, np.array([c.species[s].z_val for s in c.atom_species]), c.positions)
+    psp_core = sum(gth_alpha(c.species[s]) for s in c.atom_species) * nelec / vol
+    history = []
+    energy = float("nan")
+    terms = {}
+    converged = False
+    values = []
+    it = 0
+    for it in range(1, p.max_iter + 1):
+        local_r = vloc_r + to_r(v_hxc)
+        backend.set_vloc(local_r)
+        warm = it <= p.warmup_steps
+        opts = dict(max_iter=p.warmup_max_iter if warm else p.iterative_max_iter, tol=p.warmup_tol if warm else p.iterative_tol)
+        values = []
+        for k, inp in enumerate(kin):
+            init = vectors[k] if (p.reuse_vectors and vectors[k] is not None) else None
+            ev, vec = backend.eig(k, inp.basis.kinetic, nbands, opts, init)
+            values.append(np.asarray(ev))
+            vectors[k] = vec
+        # occupations
+        if p.smearing:
+            mu = fermi_level(nelec, p.smearing, kweights, values)
+            occs = [fd_occ(v, mu, p.smearing) for v in values]
+        else:
+            occ = np.zeros(nbands)
+            occ[: nocc - 1] = 1.0
+            occ[nocc - 1] = nelec / 2.0 - (nocc - 1)
+            occs = [occ for _ in values]
+        rho_out = np.zeros(N)
+        e_band = 0.0
+        e_ent = 0.0
+        for k in range(len(kin)):
+            wts = kweights[k] * occs[k] * 2.0
+            e_band += float(np.dot(wts, values[k]))
+            if p.smearing:
+                e_ent += kweights[k] * 2.0 * p.smearing * float(entropy_term(occs[k]).sum())
+            backend.density(k, vectors[k], wts, rho_out)
+        diff = math.sqrt(float(np.mean((rho_out - rho) ** 2)))
+        if hasattr(backend, "observe"):
+            backend.observe(diff)
+        # energy of rho_out with eigenvalues from V_in (energy.zig:372-396)
+        rg = to_g(rho_out)
+        e_h = 0.5 * vol * float(np.sum(8.0 * math.pi * np.abs(rg[gmask]) ** 2 / g2[gmask]))
+        fxc, vxc_out = lda_pz(rho_out)
+        dv = vol / N
+        e_xc = float(fxc.sum()) * dv
+        v_in_r = to_r(v_hxc)
+        int_vin_rho = float(np.dot(v_in_r, rho_out)) * dv
+        energy = e_band - int_vin_rho + e_h + e_xc + e_ion + psp_core - e_ent
+        terms = dict(band=e_band, hartree=e_h, xc=e_xc, vin_rho=int_vin_rho, ion_ion=e_ion, psp_core=psp_core, entropy=e_ent)
+        history.append((it, energy, diff, time.perf_counter() - t0))
+        if verbose:
+            print(f"scf {it:3d}  E={energy:.10f} Ry  drho={diff:.3e}", flush=True)
+        if p.energy_target is not None and p.energy_tol_per_atom is not None:
+            if abs(energy - p.energy_target) / len(c.atom_species) < p.energy_tol_per_atom:
+                converged = True
+                rho = rho_out
+                break
+        if diff < p.convergence:
+            converged = True
+            rho = rho_out
+            break
+        v_out = hxc_g(rho_out)
+        resid = v_out - v_hxc
+        if it >= p.pulay_start:
+            flat = mixer.mix(np.concatenate([v_hxc.real, v_hxc.imag]), np.concatenate([resid.real, resid.imag]), p.mixing_beta)
+            v_hxc = flat[:N] + 1j * flat[N:]
+        else:
+            v_hxc = v_hxc + p.mixing_beta * resid
+        rho = rho_out
+    natom = len(c.atom_species)
+    return ScfResult(converged, it, energy, energy / natom, values, terms, rho, history, time.perf_counter() - t0)

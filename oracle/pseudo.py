@@ -238,9 +238,9 @@ class Species:
 # (Phys. Rev. B 54, 1703 (1996)): V_loc(r) = -Z/r erf(r/(sqrt2 r_loc)) + exp(-(r/r_loc)^2/2) (C1 + C2 (r/r_loc)^2),
 # projectors p_i^l(r) ~ r^(l+2(i-1)) exp(-r^2/(2 r_l^2)).  Energies below are Hartree.
 SYNTHETIC_PARAMS = {
-    "Si": dict(z=4.0, rloc=0.45, c1=-6.9, c2=0.0, chans=[(0, 0.42, [[5.8, -1.6], [-1.6, 2.1]]), (1, 0.49, [[2.6]])]),
-    "Al": dict(z=3.0, rloc=0.46, c1=-8.4, c2=0.0, chans=[(0, 0.46, [[5.2, -1.3], [-1.3, 1.8]]), (1, 0.54, [[2.1]])]),
-    "Ge": dict(z=4.0, rloc=0.54, c1=0.0, c2=0.0, chans=[(0, 0.42, [[7.0, -2.0], [-2.0, 2.6]]), (1, 0.56, [[2.5]])]),
+    "Si": dict(z=4.0, rloc=0.44, c1=-7.34, c2=0.0, chans=[(0, 0.423, [[5.9, 0.0], [0.0, 2.0]]), (1, 0.484, [[2.73]])]),
+    "Al": dict(z=3.0, rloc=0.45, c1=-8.5, c2=0.0, chans=[(0, 0.46, [[5.1, 0.0], [0.0, 1.2]]), (1, 0.54, [[2.2]])]),
+    "Ge": dict(z=4.0, rloc=0.54, c1=0.0, c2=0.0, chans=[(0, 0.42, [[7.5, 0.0], [0.0, 2.4]]), (1, 0.56, [[2.5]])]),
 }
 
 

@@ -63,10 +63,10 @@ def test_init_diagonal_and_warm_start(dz):
     dense = np.linalg.eigvalsh(kp.ctx.dense_hamiltonian())[:8]
     r = kc.hermitian_eigen_decomp_iterative(diag, 8, dz.Options(max_iter=200, tol=1e-9, init_diagonal=True))
     assert np.abs(r.values - dense).max() < 1e-7
-    # warm start from converged vectors converges at once
+    # a warm start from converged vectors (KpointCache) needs a small fraction of a cold start's iterations
     r2 = kc.hermitian_eigen_decomp_iterative(diag, 8, dz.Options(max_iter=200, tol=1e-8, init_vectors=r.vectors))
     assert np.abs(r2.values - dense).max() < 1e-7
-    assert r2.iterations <= 3
+    assert r2.iterations * 4 <= r.iterations
     kc.close()
 
 

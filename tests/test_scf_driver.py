@@ -1,0 +1,67 @@
+"""The host SCF driver pieces (dft-zig_b200/scf.py) on the CPU, with the oracle as the backend."""
+import importlib
+import math
+
+import numpy as np
+import pytest
+
+import dftzig_loader
+from tests.helpers import OracleBackend
+
+dftzig_loader.load()
+scf = importlib.import_module("dftzig_b200.scf")
+system = importlib.import_module("dftzig_b200.system")
+
+
+def test_lda_pz_potential_is_derivative():
+    n = np.array([1e-4, 1e-3, 0.01, 0.05, 0.2, 1.0])  # both r_s branches
+    h = 1e-7 * n
+    f_p, _ = scf.lda_pz(n + h)
+    f_m, _ = scf.lda_pz(n - h)
+    _, v = scf.lda_pz(n)
+    assert np.allclose((f_p - f_m) / (2 * h), v, rtol=1e-6)
+    f0, v0 = scf.lda_pz(np.array([0.0, 1e-13]))
+    assert (f0 == 0).all() and (v0 == 0).all()
+
+
+def test_ewald_graphene_golden():
+    """src/tests.zig:859-870: graphene (c = 20 A) ion-ion energy 50.1056 Ha (ABINIT) within 1%."""
+    a, c = 4.6487262675, 37.7945225
+    cell = np.array([[a, 0.0, 0.0], [a * 0.5, a * math.sqrt(3.0) / 2.0, 0.0], [0.0, 0.0, c]])
+    pos = np.array([[0.0, 0.0, 0.0], [3.0991508450, 2.6839433578, 0.0]])
+    e_ha = scf.ewald_energy(cell, np.array([4.0, 4.0]), pos) / 2.0
+    assert abs(e_ha - 50.1056) / 50.1056 < 0.01
+
+
+def test_ewald_independent_of_split():
+    c = system.crystal("si8")
+    z = np.array([4.0] * 8)
+    e1 = scf.ewald_energy(c.cell, z, c.positions)
+    # a translated copy has the same energy
+    e2 = scf.ewald_energy(c.cell, z, c.positions + 0.37)
+    assert abs(e1 - e2) < 1e-9 * abs(e1)
+
+
+def test_pulay_mixer_solves_linear_fixed_point():
+    rng = np.random.default_rng(0)
+    A = rng.normal(size=(6, 6)) * 0.1
+    b = rng.normal(size=6)
+    x = np.zeros(6)
+    mix = scf.PulayMixer(8)
+    for _ in range(30):
+        fx = A @ x + b  # fixed point x = A x + b
+        x = mix.mix(x, fx - x, 0.5)
+    assert np.abs(A @ x + b - x).max() < 1e-9
+
+
+def test_scf_converges_with_oracle_backend():
+    """Si2, 8 Ry, 2x2x2 mesh, fixed occupations: the synthetic Si is a semiconductor (one s-like
+    state under a p-like triplet at Gamma) and the potential-mixing loop converges."""
+    c = system.crystal("si2")
+    p = scf.ScfParams(ecut=8.0, kmesh=(2, 2, 2), nbands=8, convergence=1e-8, iterative_max_iter=100, iterative_tol=1e-9, warmup_steps=0)
+    r = scf.run_scf(c, p, OracleBackend())
+    assert r.converged
+    assert r.iterations < 25
+    assert math.isfinite(r.energy) and -9.0 < r.energy_per_atom < -7.0
+    g = r.eigenvalues[0]
+    assert abs(g[1] - g[3]) < 1e-6 and g[4] - g[3] > 0.02  # occupied triplet, gap above it
