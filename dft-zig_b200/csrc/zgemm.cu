@@ -12,20 +12,28 @@ namespace dftcuda {
 
 constexpr int BM = 64, BN = 64, BK = 16;
 
-template <bool AKC, bool BKC, bool CJA, bool CJB>
-__device__ __forceinline__ void zgemm_load_tile(double2 (&ra)[4], double2 (&rb)[4], int M, int N, int kend, int r0, int c0,
-                                                int k0, const double2* __restrict__ A, long lda,
-                                                const double2* __restrict__ B, long ldb, int tid) {
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = pred ? 16 : 0;  // 0 source bytes: the 16 destination bytes are zero-filled
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// One BK-deep slice of A and B into shared memory with cp.async (4 x 16 B per thread each).
+template <bool AKC, bool BKC>
+__device__ __forceinline__ void zgemm_fetch(double2 (*As)[BM + 1], double2 (*Bs)[BN + 1], int M, int N, int kend, int r0,
+                                            int c0, int k0, const double2* __restrict__ A, long lda,
+                                            const double2* __restrict__ B, long ldb, int tid) {
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const int i = tid + 256 * q;
     int r, kk;
     if (AKC) { kk = i % BK; r = i / BK; } else { r = i % BM; kk = i / BM; }
     const int gr = r0 + r, gk = k0 + kk;
-    double2 v = make_double2(0.0, 0.0);
-    if (gr < M && gk < kend) v = AKC ? __ldg(A + (long)gr * lda + gk) : __ldg(A + (long)gk * lda + gr);
-    if (CJA) v.y = -v.y;
-    ra[q] = v;
+    const bool ok = gr < M && gk < kend;
+    const double2* src = ok ? (AKC ? A + (long)gr * lda + gk : A + (long)gk * lda + gr) : A;
+    cp_async16(&As[kk][r], src, ok);
   }
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
@@ -33,67 +41,54 @@ __device__ __forceinline__ void zgemm_load_tile(double2 (&ra)[4], double2 (&rb)[
     int cc, kk;
     if (BKC) { kk = i % BK; cc = i / BK; } else { cc = i % BN; kk = i / BN; }
     const int gc = c0 + cc, gk = k0 + kk;
-    double2 v = make_double2(0.0, 0.0);
-    if (gc < N && gk < kend) v = BKC ? __ldg(B + (long)gc * ldb + gk) : __ldg(B + (long)gk * ldb + gc);
-    if (CJB) v.y = -v.y;
-    rb[q] = v;
+    const bool ok = gc < N && gk < kend;
+    const double2* src = ok ? (BKC ? B + (long)gc * ldb + gk : B + (long)gk * ldb + gc) : B;
+    cp_async16(&Bs[kk][cc], src, ok);
   }
+  cp_async_commit();
 }
 
-template <bool AKC, bool BKC>
-__device__ __forceinline__ void zgemm_store_tile(double2 (*As)[BM + 1], double2 (*Bs)[BN + 1], const double2 (&ra)[4],
-                                                 const double2 (&rb)[4], int tid) {
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int i = tid + 256 * q;
-    int r, kk;
-    if (AKC) { kk = i % BK; r = i / BK; } else { r = i % BM; kk = i / BM; }
-    As[kk][r] = ra[q];
-  }
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int i = tid + 256 * q;
-    int cc, kk;
-    if (BKC) { kk = i % BK; cc = i / BK; } else { cc = i % BN; kk = i / BN; }
-    Bs[kk][cc] = rb[q];
-  }
-}
-
-// Software-pipelined: the next K slice is fetched into registers while the current one is
-// multiplied out of shared memory.
+// Double-buffered: the next K slice streams into the other shared-memory buffer with cp.async
+// while the current one is multiplied; conjugation is applied as the operands leave shared memory.
+// At most 128 registers per thread so two CTAs share an SM.
 template <bool AKC, bool BKC, bool CJA, bool CJB>
-__global__ void __launch_bounds__(256) k_zgemm(int M, int N, int K, const double2* __restrict__ A, long lda,
-                                               const double2* __restrict__ B, long ldb, double2* __restrict__ O,
-                                               long ldo_r, long ldo_c, double alpha, double beta, int kps,
-                                               double2* __restrict__ part) {
-  __shared__ double2 As[BK][BM + 1];
-  __shared__ double2 Bs[BK][BN + 1];
+__global__ void __launch_bounds__(256, 2) k_zgemm(int M, int N, int K, const double2* __restrict__ A, long lda,
+                                                  const double2* __restrict__ B, long ldb, double2* __restrict__ O,
+                                                  long ldo_r, long ldo_c, double alpha, double beta, int kps,
+                                                  double2* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char zsm[];
+  double2(*As)[BK][BM + 1] = reinterpret_cast<double2(*)[BK][BM + 1]>(zsm);
+  double2(*Bs)[BK][BN + 1] = reinterpret_cast<double2(*)[BK][BN + 1]>(zsm + 2 * sizeof(double2) * BK * (BM + 1));
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
   const int r0 = blockIdx.y * BM, c0 = blockIdx.x * BN;
   const int kbeg = blockIdx.z * kps;
   const int kend = min(K, kbeg + kps);
+  const double sa = CJA ? -1.0 : 1.0, sb = CJB ? -1.0 : 1.0;
   double2 acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
-  double2 ra[4], rb[4];
-  if (kbeg < kend) {
-    zgemm_load_tile<AKC, BKC, CJA, CJB>(ra, rb, M, N, kend, r0, c0, kbeg, A, lda, B, ldb, tid);
-    zgemm_store_tile<AKC, BKC>(As, Bs, ra, rb, tid);
-  }
-  __syncthreads();
+  if (kbeg < kend) zgemm_fetch<AKC, BKC>(As[0], Bs[0], M, N, kend, r0, c0, kbeg, A, lda, B, ldb, tid);
+  int buf = 0;
   for (int k0 = kbeg; k0 < kend; k0 += BK) {
-    const bool more = k0 + BK < kend;
-    if (more) zgemm_load_tile<AKC, BKC, CJA, CJB>(ra, rb, M, N, kend, r0, c0, k0 + BK, A, lda, B, ldb, tid);
+    cp_async_wait_all();
+    __syncthreads();
+    if (k0 + BK < kend) zgemm_fetch<AKC, BKC>(As[buf ^ 1], Bs[buf ^ 1], M, N, kend, r0, c0, k0 + BK, A, lda, B, ldb, tid);
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
       double2 a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+      for (int i = 0; i < 4; ++i) {
+        a[i] = As[buf][kk][ty + 16 * i];
+        a[i].y *= sa;
+      }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+      for (int j = 0; j < 4; ++j) {
+        b[j] = Bs[buf][kk][tx + 16 * j];
+        b[j].y *= sb;
+      }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -104,11 +99,7 @@ __global__ void __launch_bounds__(256) k_zgemm(int M, int N, int K, const double
           acc[i][j].y = fma(a[i].y, b[j].x, acc[i][j].y);
         }
     }
-    __syncthreads();
-    if (more) {
-      zgemm_store_tile<AKC, BKC>(As, Bs, ra, rb, tid);
-      __syncthreads();
-    }
+    buf ^= 1;
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i)
@@ -133,6 +124,8 @@ __global__ void __launch_bounds__(256) k_zgemm(int M, int N, int K, const double
     }
 }
 
+static const size_t kZgemmSmem = 2 * sizeof(double2) * BK * (BM + 1) + 2 * sizeof(double2) * BK * (BN + 1);
+
 __global__ void k_zgemm_reduce(int M, int N, int splits, const double2* __restrict__ part, double2* __restrict__ O,
                                long ldo_r, long ldo_c, double alpha, double beta) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -154,12 +147,24 @@ __global__ void k_zgemm_reduce(int M, int N, int splits, const double2* __restri
   *o = v;
 }
 
+// Split K so that tiles x splits fills whole waves of 2 CTAs per SM on 148 SMs.
 static int pick_splits(int M, int N, int K) {
   const long tiles = (long)ceil_div(M, BM) * ceil_div(N, BN);
-  const long target = 2 * 148;
-  if (tiles >= target || K < 4 * BK * 8) return 1;
-  int s = (int)std::min<long>((target + tiles - 1) / tiles, K / (BK * 8));
-  return std::max(1, std::min(s, 64));
+  const long wave = 2 * 148;
+  if (tiles >= wave || K < 4 * BK * 8) return 1;
+  const long maxs = std::max<long>(1, K / (BK * 64));  // at least 64 K slices per split
+  long best = 1;
+  double best_eff = 0.0;
+  for (long sp = 1; sp <= std::min<long>(maxs, 64); ++sp) {
+    const long ctas = tiles * sp;
+    const double eff = (double)ctas / (double)(((ctas + wave - 1) / wave) * wave);  // wave fill
+    const double score = eff * std::min(1.0, (double)ctas / wave);
+    if (score > best_eff + 1e-9) {
+      best_eff = score;
+      best = sp;
+    }
+  }
+  return (int)best;
 }
 
 size_t zgemm_workspace_elems(int M, int N, int K) {
@@ -169,7 +174,12 @@ size_t zgemm_workspace_elems(int M, int N, int K) {
 
 template <bool AKC, bool BKC, bool CJA, bool CJB>
 static void launch(const GemmArgs& g, dim3 grid, int kps, double2* part, cudaStream_t s) {
-  k_zgemm<AKC, BKC, CJA, CJB><<<grid, 256, 0, s>>>(g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r, g.ldo_c, g.alpha,
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_zgemm<AKC, BKC, CJA, CJB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kZgemmSmem);
+    attr = true;
+  }
+  k_zgemm<AKC, BKC, CJA, CJB><<<grid, 256, kZgemmSmem, s>>>(g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r, g.ldo_c, g.alpha,
                                                    g.beta, kps, part); count_launch();
 }
 
