@@ -56,6 +56,7 @@ ABI_SYMBOLS = (
 
 PRECISION_FP64 = 0
 PRECISION_FP32 = 1
+PRECISION_TF32 = 2  # FP32 FFT passes + tcgen05 TF32 projector GEMMs
 
 
 class DftCudaError(RuntimeError):

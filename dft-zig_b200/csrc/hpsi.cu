@@ -248,7 +248,7 @@ static size_t box_bytes_per_col(const dftcuda_kctx* c) {
 }
 
 static size_t chunk_cols(const dftcuda_kctx* c, size_t ncols) {
-  const size_t per = (c->precision == DFTCUDA_PRECISION_FP32 ? sizeof(float2) : sizeof(double2)) * (size_t)c->n_act * c->P;
+  const size_t per = (c->precision != DFTCUDA_PRECISION_FP64 ? sizeof(float2) : sizeof(double2)) * (size_t)c->n_act * c->P;
   size_t ch = (size_t)std::max(1.0, c->w_budget_bytes / (double)per);
   return std::min(ch, std::max<size_t>(ncols, 1));
 }
@@ -307,8 +307,17 @@ int kctx_ensure_coef(dftcuda_kctx* c, size_t cols) {
       return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "projector coefficients");
     c->coef_cols = cols;
   }
-  const size_t need = std::max(zgemm_workspace_elems(c->nl.nproj, (int)cols, (int)c->npw),
-                               zgemm_workspace_elems((int)cols, (int)c->npw, c->nl.nproj));
+  size_t need = std::max(zgemm_workspace_elems(c->nl.nproj, (int)cols, (int)c->npw),
+                         zgemm_workspace_elems((int)cols, (int)c->npw, c->nl.nproj));
+  if (c->precision == DFTCUDA_PRECISION_TF32) {
+    need = std::max(need, cgemm_tf32_workspace_elems(c->nl.nproj, (int)cols, (int)c->npw));
+    need = std::max(need, cgemm_tf32_workspace_elems((int)cols, (int)c->npw, c->nl.nproj));
+    if (!c->d_err) {
+      if (cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "error flag");
+      DFT_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+      DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    }
+  }
   if (need > c->gemm_ws_elems) {
     if (c->d_gemm_ws) cudaFree(c->d_gemm_ws);
     c->d_gemm_ws = nullptr;
@@ -327,6 +336,7 @@ int kctx_project(dftcuda_kctx* c, const double2* x, size_t ncols, cudaStream_t s
   g.B = x; g.ldb = (long)c->npw; g.b_kc = true; g.conj_b = false;
   g.O = c->d_coef; g.ldo_r = (long)ncols; g.ldo_c = 1;
   g.alpha = 1.0; g.beta = 0.0;
+  if (c->precision == DFTCUDA_PRECISION_TF32) return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err);
   return zgemm(g, s, c->d_gemm_ws, c->gemm_ws_elems);
 }
 
@@ -349,6 +359,7 @@ static int nonlocal_block(dftcuda_kctx* c, const double2* x, double2* y, size_t 
   g.B = c->nl.P; g.ldb = (long)c->npw; g.b_kc = false; g.conj_b = true;
   g.O = y; g.ldo_r = (long)c->npw; g.ldo_c = 1;
   g.alpha = 1.0 / c->volume; g.beta = 1.0;
+  if (c->precision == DFTCUDA_PRECISION_TF32) return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err);
   return zgemm(g, s, c->d_gemm_ws, c->gemm_ws_elems);
 }
 
@@ -365,7 +376,7 @@ int kctx_apply_h_dev(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols
     const size_t nc = std::min(ch, ncols - c0);
     const double2* xc = x + c0 * c->npw;
     double2* yc = y + c0 * c->npw;
-    if (c->precision == DFTCUDA_PRECISION_FP32) {
+    if (c->precision != DFTCUDA_PRECISION_FP64) {
       if (c->fast32)
         DFT_TRY(local_block4<float>(c, xc, yc, nc, s));
       else
@@ -412,7 +423,7 @@ int kctx_density_dev(dftcuda_kctx* c, const double2* vecs, size_t nbands, const 
   DFT_TRY(ensure_box(c, ch));
   for (size_t c0 = 0; c0 < nbands; c0 += ch) {
     const size_t nc = std::min(ch, nbands - c0);
-    if (c->precision == DFTCUDA_PRECISION_FP32) {
+    if (c->precision != DFTCUDA_PRECISION_FP64) {
       if (c->fast32)
         DFT_TRY(density_block4<float>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
       else
@@ -425,6 +436,18 @@ int kctx_density_dev(dftcuda_kctx* c, const double2* vecs, size_t nbands, const 
     }
   }
   return DFTCUDA_OK;
+}
+
+// Turns the device error flag of the bounded waits into DFTCUDA_ERR_TIMEOUT (and clears it).
+int kctx_check_error(dftcuda_kctx* c) {
+  if (!c->d_err) return DFTCUDA_OK;
+  int h = 0;
+  DFT_CUDA_TRY(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (h == 0) return DFTCUDA_OK;
+  DFT_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+  DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return fail(DFTCUDA_ERR_TIMEOUT, "tensor-core GEMM: a bounded mbarrier wait gave up");
 }
 
 int kctx_stage(dftcuda_kctx* c, size_t cols) {
@@ -465,7 +488,7 @@ extern "C" int dftcuda_kctx_destroy(dftcuda_kctx* c) {
   void* ptrs[] = {c->d_plane_off, c->d_pw_idx, c->d_pw_spos, c->d_slot_xpos, c->d_kinetic, c->d_gcart, c->d_vt,
                   c->d_vt32, c->d_box, c->d_coef, c->d_coef2, c->d_gemm_ws, c->d_x, c->d_y, c->d_rho, c->d_w,
                   c->d_pwmap, c->d_stick_off, c->d_stick_y, c->d_slot_of_x, c->d_tw4x64, c->d_tw4x32,
-                  c->d_tw4p64, c->d_tw4p32};
+                  c->d_tw4p64, c->d_tw4p32, c->d_err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   c->fx.destroy(); c->fy.destroy(); c->fz.destroy();
@@ -480,7 +503,7 @@ extern "C" int dftcuda_kctx_create(dftcuda_kctx** out, int nx, int ny, int nz, d
   *out = nullptr;
   if (nx <= 0 || ny <= 0 || nz <= 0 || !(volume > 0.0) || n_pw == 0 || !hkl || !kinetic || !gcart)
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "kctx_create: bad arguments");
-  if (precision != DFTCUDA_PRECISION_FP64 && precision != DFTCUDA_PRECISION_FP32)
+  if (precision != DFTCUDA_PRECISION_FP64 && precision != DFTCUDA_PRECISION_FP32 && precision != DFTCUDA_PRECISION_TF32)
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "kctx_create: unknown precision");
   // Miller index range check, same rule as PwGridMap.init (pw_grid_map.zig:27-35).
   const int min_h = -(nx / 2), min_k = -(ny / 2), min_l = -(nz / 2);
@@ -702,6 +725,7 @@ extern "C" int dftcuda_apply_h_batch(dftcuda_kctx* c, const double* x, double* y
   DFT_TRY(kctx_apply_h_dev(c, xd, yd, ncols, c->stream));
   if (!dy) DFT_CUDA_TRY(cudaMemcpyAsync(y, yd, bytes, cudaMemcpyDeviceToHost, c->stream));
   DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  DFT_TRY(kctx_check_error(c));
   return DFTCUDA_OK;
 }
 

@@ -20,6 +20,10 @@ struct GemmArgs {
 };
 int zgemm(const GemmArgs& g, cudaStream_t s, double2* workspace, size_t workspace_elems);
 size_t zgemm_workspace_elems(int M, int N, int K);
+// The same contraction on the tensor cores (tc_gemm.cu): TF32 inputs, FP32 accumulation.  err_dev
+// receives 1 if a bounded wait gave up.
+int cgemm_tf32(const GemmArgs& g, cudaStream_t s, double2* workspace, size_t workspace_elems, int* err_dev);
+size_t cgemm_tf32_workspace_elems(int M, int N, int K);
 
 struct NonlocalDev {
   int nproj = 0;                 // sum over atoms of m_total(species)
@@ -97,6 +101,7 @@ struct dftcuda_kctx {
   size_t coef_cols = 0;
   double2* d_gemm_ws = nullptr;
   size_t gemm_ws_elems = 0;
+  int* d_err = nullptr;  // device error flag of the bounded waits (TF32 tensor-core GEMMs)
 
   // Staging for host pointers.
   double2* d_x = nullptr;
@@ -119,6 +124,7 @@ int kctx_apply_h_dev(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols
 int kctx_project(dftcuda_kctx* c, const double2* x, size_t ncols, cudaStream_t s);  // d_coef = P x
 int kctx_ensure_coef(dftcuda_kctx* c, size_t cols);
 int kctx_stage(dftcuda_kctx* c, size_t cols);
+int kctx_check_error(dftcuda_kctx* c);
 int kctx_density_dev(dftcuda_kctx* c, const double2* vecs, size_t nbands, const double* w_dev, double* rho_dev,
                      cudaStream_t s);
 void eig_destroy(KCtxImpl* e);

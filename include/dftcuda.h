@@ -37,9 +37,15 @@ extern "C" {
 #define DFTCUDA_ERR_UNSUPPORTED (-7)         /* FFT length with a prime factor other than 2, 3, 5     */
 #define DFTCUDA_ERR_TIMEOUT (-8)             /* a bounded device wait gave up (no reference counterpart) */
 
-/* Arithmetic of the local-potential FFT passes of one k-point context. */
+/* Arithmetic of one k-point context's H|psi>:
+ *  FP64  every pass in FP64;
+ *  FP32  local-potential FFT passes in FP32, projector GEMMs in FP64;
+ *  TF32  FFT passes in FP32 and the projector GEMMs on the tensor cores (tcgen05 kind::tf32, FP32
+ *        accumulation in TMEM).
+ * Wavefunctions are FP64 at the boundary in every mode; the eigensolver's subspace algebra is FP64. */
 #define DFTCUDA_PRECISION_FP64 0
 #define DFTCUDA_PRECISION_FP32 1
+#define DFTCUDA_PRECISION_TF32 2
 
 typedef struct dftcuda_kctx dftcuda_kctx;
 typedef struct dftcuda_fft_plan dftcuda_fft_plan;
