@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile-case", action="store_true", help="small single-k case for ncu captures: Gamma, 32 columns, 2 applications")
     ap.add_argument("--workload", choices=("hpsi", "scf"), default="hpsi", help="hpsi: H|psi> GB/s (default); scf: time-to-SCF")
+    ap.add_argument("--precision", choices=("fp64", "fp32", "tf32"), default="fp64", help="context precision of --profile-case")
     return ap.parse_args()
 
 
@@ -249,6 +250,33 @@ def run_ours(args):
         k: {"ms_per_step": tot[k] / 1e6 / args.steps, "share": tot[k] / max(tot["apply_h_ns"], 1)}
         for k in ("local_plane_inv_ns", "local_xline_ns", "local_plane_fwd_ns", "nl_project_ns", "nl_dij_ns", "nl_backproject_ns")
     }
+    # The same workload with the FP32 FFT passes (FP64 projector GEMMs) and in TF32 mode (FP32 FFT
+    # passes + tcgen05 TF32 projector GEMMs): device time per step, the same algorithmic byte count.
+    variants = {}
+    for label, prec in (("fp32_fft", dz.PRECISION_FP32), ("tf32", dz.PRECISION_TF32)):
+        vctx = []
+        for inp in ins:
+            kc = dz.KpointContext(dims[0], dims[1], dims[2], inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart, prec)
+            kc.set_vloc(inp.local_r)
+            kc.set_projectors([dz.SpeciesProjectors(l, d, p) for (l, d, p) in inp.species_phi], inp.atom_species, inp.positions)
+            vctx.append(kc)
+        for _ in range(3):
+            for kc, x, y in zip(vctx, xs, ys):
+                kc.apply_hamiltonian_async(x, y, NCOLS, sptr)
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            for kc, x, y in zip(vctx, xs, ys):
+                kc.apply_hamiltonian_async(x, y, NCOLS, sptr)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        vms = f0.elapsed_time(f1) / args.steps
+        variants[label] = {"ms_per_step": round(vms, 3), "value": round(world * algo_bytes_step / (vms * 1e-3) / 1e9, 1), "unit": "GB/s"}
+        for kc in vctx:
+            kc.close()
+
     line = {
         "metric": "H|psi> HBM GB/s (algorithmic)",
         "value": round(value, 2),
@@ -284,6 +312,7 @@ def run_ours(args):
             "traffic": None,
         },
         "kernels": kern,
+        "variants": variants,
     }
     if rank == 0 and world == 1:
         line["cpu_baseline"] = cpu_baseline()
@@ -389,7 +418,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_profile_case():
+def run_profile_case(precision: str = "fp64"):
     """One k-point (Gamma) of the benchmark cell, 32 columns, H|psi> twice: a few hundred MB on the
     device, for ncu captures of single kernels."""
     import torch
@@ -404,7 +433,8 @@ def run_profile_case():
     c = system.crystal(CELL, SEED)
     dims = system.fft_box(ECUT, c.recip)
     inp = system.kpoint_inputs(c, ECUT, (0.0, 0.0, 0.0), dims=dims)
-    kc = dz.KpointContext(dims[0], dims[1], dims[2], inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart)
+    prec = {"fp64": dz.PRECISION_FP64, "fp32": dz.PRECISION_FP32, "tf32": dz.PRECISION_TF32}[precision]
+    kc = dz.KpointContext(dims[0], dims[1], dims[2], inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart, prec)
     kc.set_vloc(inp.local_r)
     kc.set_projectors([dz.SpeciesProjectors(l, d, p) for (l, d, p) in inp.species_phi], inp.atom_species, inp.positions)
     x = torch.randn((32, kc.n), dtype=torch.complex128, device="cuda")
@@ -478,7 +508,7 @@ def main():
         run_scf_workload(args)
         return
     if args.profile_case:
-        run_profile_case()
+        run_profile_case(args.precision)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -52,11 +52,13 @@ ABI_SYMBOLS = (
     "dftcuda_kctx_set_profiling",
     "dftcuda_kctx_get_profile",
     "dftcuda_accumulate_density_noalloc",
+    "dftcuda_hermitian_eigen_decomp",
 )
 
 PRECISION_FP64 = 0
 PRECISION_FP32 = 1
-PRECISION_TF32 = 2  # FP32 FFT passes + tcgen05 TF32 projector GEMMs
+PRECISION_TF32 = 2  # FP32 FFT passes + tcgen05 TF32 projector GEMMs (~1e-3)
+PRECISION_TF32X3 = 3  # FP32 FFT passes + split (3xTF32) tensor-core GEMMs (~1e-6)
 
 
 class DftCudaError(RuntimeError):
@@ -186,6 +188,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.dftcuda_kctx_set_profiling.argtypes = [vp, ip]
     lib.dftcuda_kctx_get_profile.argtypes = [vp, ct.POINTER(_Profile)]
     lib.dftcuda_accumulate_density_noalloc.argtypes = [vp, dp, sz, sz, dp, dp]
+    lib.dftcuda_hermitian_eigen_decomp.argtypes = [sz, dp, sz, dp, dp]
     _lib = lib
     return lib
 
@@ -390,6 +393,24 @@ class KpointContext:
         info = _EigInfo()
         _check(self._lib.dftcuda_eig_solve(self._h, _ptr(diag), nbands, ct.byref(o), _ptr(init), icols, _ptr(vals), _ptr(vecs), ct.byref(info)))
         return EigenDecomp(vals, vecs, self.n, info.iterations, info.h_applies, bool(info.converged), info.max_residual)
+
+
+def hermitian_eigen_decomp(a, nev: Optional[int] = None) -> EigenDecomp:
+    """linalg.hermitian_eigen_decomp (linalg/linalg.zig:141-151) on the GPU: the nev lowest
+    eigenpairs (all when nev is None) of the Hermitian matrix a[i, j]; only its upper triangle
+    (i <= j) is read, as zheev 'U' does.  vectors has shape (nev, n), one eigenvector per row."""
+    lib = load_library()
+    _require_device()
+    a = np.asarray(a, dtype=np.complex128)
+    if a.ndim != 2 or a.shape[0] != a.shape[1]:
+        raise InvalidMatrixSize("hermitian_eigen_decomp: square matrix expected")
+    n = a.shape[0]
+    k = n if nev is None else int(nev)
+    colmajor = np.ascontiguousarray(a.T)  # memory order a[i + j n] = a[i, j]
+    vals = np.empty(k, dtype=np.float64)
+    vecs = np.empty((k, n), dtype=np.complex128)
+    _check(lib.dftcuda_hermitian_eigen_decomp(n, _ptr(colmajor), k, _ptr(vals), _ptr(vecs)))
+    return EigenDecomp(vals, vecs, n)
 
 
 class Fft3dPlan:

@@ -7,9 +7,9 @@
 // Steps and their reference counterparts:
 //  * random start: the reference's LCG (common.zig:287-319) evaluated in closed form per element
 //    (s_k = a^k s0 + sum_{j<k} a^j mod 2^64), so the device draws exactly the reference's numbers;
-//  * T = V^H W, Hermitised (common.zig:231-259): FP64 complex GEMM + k_hermitize;
-//  * small eigenproblem (zheev, common.zig:440-508): cyclic two-sided complex Jacobi in one CTA,
-//    eigenvalues ascending;
+//  * T = V^H W, Hermitised (common.zig:231-259): FP64 complex GEMM on the new columns only + k_gram_finish;
+//  * small eigenproblem (zheev, common.zig:440-508): cyclic two-sided complex Jacobi in one CTA
+//    below 96 columns, the tridiagonal solver of heev.cu (lowest nbands pairs) from there on;
 //  * Ritz vectors V C, W C and residuals r_b = W c_b - lambda_b V c_b with norms (serial.zig:201-227);
 //  * new directions: r_b / (diag - lambda_b) clamped at |den| >= 1e-8 (common.zig:214-226), then
 //    modified Gram-Schmidt against V with a drop when the remaining norm is < 1e-8
@@ -20,6 +20,7 @@
 //    keeps, in the same order; only rounding differs.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -59,19 +60,35 @@ __global__ void k_lcg_fill(double2* __restrict__ V, long count, uint64_t s0) {
   V[e] = make_double2(re, im);
 }
 
-__global__ void k_hermitize(double2* T, int m) {
+// Rayleigh-Ritz matrix from the persistent Gram store Tk (leading dimension ld).  Columns
+// [m_old, m) of Tk hold the fresh products V[0:m]^H W[m_old:m]; the rows [m_old, m) to their left
+// are the conjugate mirror (H is Hermitian, so V_new^H W_old = (V_old^H W_new)^H), and the new
+// diagonal block is hermitised as (T + T^H) / 2 (common.zig:231-259).  Writes T (ld m).
+__global__ void k_gram_finish(const double2* __restrict__ Tk, long ld, int m_old, int m, double2* __restrict__ T) {
   const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (idx >= (long)m * m) return;
   const int i = (int)(idx % m), j = (int)(idx / m);
-  if (i > j) return;
-  if (i == j) {
-    T[i + (long)j * m].y = 0.0;
-    return;
+  double2 v;
+  if (j < m_old && i < m_old) {
+    v = Tk[i + j * ld];
+  } else if (i < m_old) {
+    v = Tk[i + j * ld];
+  } else if (j < m_old) {
+    v = cconj(Tk[j + i * ld]);
+  } else if (i == j) {
+    v = make_double2(Tk[i + j * ld].x, 0.0);
+  } else {
+    const double2 a = Tk[i + j * ld], b = Tk[j + i * ld];
+    v = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
   }
-  const double2 a = T[i + (long)j * m], b = T[j + (long)i * m];
-  const double re = 0.5 * (a.x + b.x), im = 0.5 * (a.y - b.y);
-  T[i + (long)j * m] = make_double2(re, im);
-  T[j + (long)i * m] = make_double2(re, -im);
+  T[idx] = v;
+}
+
+__global__ void k_gram_store(const double2* __restrict__ T, int m, double2* __restrict__ Tk, long ld) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= (long)m * m) return;
+  const int i = (int)(idx % m), j = (int)(idx / m);
+  Tk[i + j * ld] = T[idx];
 }
 
 // Cyclic two-sided Jacobi for a Hermitian m x m matrix (column-major), one CTA.  Each round applies
@@ -344,18 +361,24 @@ __global__ void __launch_bounds__(512) k_chol_drop(const double2* __restrict__ G
 struct KCtxImpl {
   size_t n = 0, max_sub = 0, nb = 0, kmax = 0;
   double2 *V = nullptr, *W = nullptr, *ritz = nullptr, *res = nullptr, *Q = nullptr, *Q2 = nullptr;
+  double2 *Tk = nullptr;  // persistent Rayleigh-Ritz matrix, leading dimension max_sub
   double2 *T = nullptr, *U = nullptr, *E = nullptr, *H = nullptr, *G = nullptr, *R = nullptr, *Z = nullptr;
   double *evals = nullptr, *norms = nullptr, *diag = nullptr;
   int *band = nullptr, *kept = nullptr, *status = nullptr;
   double2* ws = nullptr;
   size_t ws_elems = 0;
   void* all = nullptr;
+  void* heev_mem = nullptr;
+  HeevWork hw;
+  bool rr_tc = false;  // Rayleigh-Ritz products on the tensor cores (3xTF32), TF32/TF32X3 contexts
+  int* err = nullptr;  // the context's tensor-core error flag
 };
 
 void eig_destroy(KCtxImpl* e) {
   if (!e) return;
   if (e->all) cudaFree(e->all);
   if (e->ws) cudaFree(e->ws);
+  if (e->heev_mem) cudaFree(e->heev_mem);
   delete e;
 }
 
@@ -374,7 +397,7 @@ static int eig_alloc(dftcuda_kctx* c, size_t n, size_t max_sub, size_t nb) {
   const size_t oQ = take(sizeof(double2) * n * kmax), oQ2 = take(sizeof(double2) * n * kmax);
   const size_t oT = take(sizeof(double2) * ms2), oU = take(sizeof(double2) * ms2), oE = take(sizeof(double2) * ms2);
   const size_t oH = take(sizeof(double2) * ms2), oG = take(sizeof(double2) * ms2), oR = take(sizeof(double2) * ms2);
-  const size_t oZ = take(sizeof(double2) * ms2);
+  const size_t oZ = take(sizeof(double2) * ms2), oTk = take(sizeof(double2) * ms2);
   const size_t oev = take(sizeof(double) * max_sub), onr = take(sizeof(double) * nb), odg = take(sizeof(double) * n);
   const size_t obd = take(sizeof(int) * kmax), okp = take(sizeof(int) * kmax), ost = take(sizeof(int) * 4);
   if (cudaMalloc(&e->all, off) != cudaSuccess) {
@@ -386,7 +409,7 @@ static int eig_alloc(dftcuda_kctx* c, size_t n, size_t max_sub, size_t nb) {
   e->V = (double2*)(b + oV); e->W = (double2*)(b + oW); e->ritz = (double2*)(b + oRi); e->res = (double2*)(b + oRe);
   e->Q = (double2*)(b + oQ); e->Q2 = (double2*)(b + oQ2); e->T = (double2*)(b + oT); e->U = (double2*)(b + oU);
   e->E = (double2*)(b + oE); e->H = (double2*)(b + oH); e->G = (double2*)(b + oG); e->R = (double2*)(b + oR);
-  e->Z = (double2*)(b + oZ); e->evals = (double*)(b + oev); e->norms = (double*)(b + onr); e->diag = (double*)(b + odg);
+  e->Z = (double2*)(b + oZ); e->Tk = (double2*)(b + oTk); e->evals = (double*)(b + oev); e->norms = (double*)(b + onr); e->diag = (double*)(b + odg);
   e->band = (int*)(b + obd); e->kept = (int*)(b + okp); e->status = (int*)(b + ost);
   size_t need = 0;
   const int ms = (int)max_sub;
@@ -395,35 +418,46 @@ static int eig_alloc(dftcuda_kctx* c, size_t n, size_t max_sub, size_t nb) {
   need = std::max(need, zgemm_workspace_elems(ms, (int)kmax, (int)n));
   need = std::max(need, zgemm_workspace_elems((int)kmax, (int)n, ms));
   need = std::max(need, zgemm_workspace_elems((int)kmax, (int)kmax, (int)n));
+  need = std::max(need, cgemm_tf32_workspace_elems(ms, ms, (int)n));
+  need = std::max(need, cgemm_tf32_workspace_elems((int)nb, (int)n, ms));
   if (need) {
     if (cudaMalloc(&e->ws, need * sizeof(double2)) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "eig gemm ws");
     e->ws_elems = need;
   }
+  if (cudaMalloc(&e->heev_mem, heev_work_bytes(ms, (int)nb)) != cudaSuccess)
+    return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "eig heev ws");
+  heev_bind(e->hw, e->heev_mem, ms, (int)nb);
   return DFTCUDA_OK;
 }
 
 // Gram products on blocks stored as rows of length n ("vector blocks", column-major [n x cols]).
 // out[i + j*ldo] = sum_g conj(X[i][g]) Y[j][g]
-static int gram(KCtxImpl* e, const double2* X, int mx, const double2* Y, int my, double2* out, int ldo, cudaStream_t s) {
+static int gemm_dispatch(KCtxImpl* e, const GemmArgs& g, bool rr, cudaStream_t s) {
+  if (rr && e->rr_tc) return cgemm_tf32(g, s, e->ws, e->ws_elems, e->err, true);
+  return zgemm(g, s, e->ws, e->ws_elems);
+}
+
+static int gram(KCtxImpl* e, const double2* X, int mx, const double2* Y, int my, double2* out, int ldo, cudaStream_t s,
+                bool rr = false) {
   GemmArgs g{};
   g.M = mx; g.N = my; g.K = (int)e->n;
   g.A = X; g.lda = (long)e->n; g.a_kc = true; g.conj_a = true;
   g.B = Y; g.ldb = (long)e->n; g.b_kc = true; g.conj_b = false;
   g.O = out; g.ldo_r = 1; g.ldo_c = ldo;
   g.alpha = 1.0; g.beta = 0.0;
-  return zgemm(g, s, e->ws, e->ws_elems);
+  return gemm_dispatch(e, g, rr, s);
 }
 
 // Out[j][g] = alpha * sum_i X[i][g] C[i + j*ldc] + beta * Out[j][g]
 static int combine(KCtxImpl* e, const double2* X, int mx, const double2* C, int ldc, int ncols, double2* out,
-                   double alpha, double beta, cudaStream_t s) {
+                   double alpha, double beta, cudaStream_t s, bool rr = false) {
   GemmArgs g{};
   g.M = ncols; g.N = (int)e->n; g.K = mx;
   g.A = C; g.lda = ldc; g.a_kc = true; g.conj_a = false;
   g.B = X; g.ldb = (long)e->n; g.b_kc = false; g.conj_b = false;
   g.O = out; g.ldo_r = (long)e->n; g.ldo_c = 1;
   g.alpha = alpha; g.beta = beta;
-  return zgemm(g, s, e->ws, e->ws_elems);
+  return gemm_dispatch(e, g, rr, s);
 }
 
 // Orthonormalise the k vectors in Q against V[0:m] and among themselves (in order), writing the kept
@@ -459,7 +493,14 @@ static int block_orthonormalize(dftcuda_kctx* c, int m, double2* Q, int k, doubl
   return DFTCUDA_OK;
 }
 
-static int small_eig(KCtxImpl* e, int m, cudaStream_t s) {
+// Subspace sizes from which the tridiagonal solver replaces the one-CTA Jacobi sweeps (whose cost
+// grows as m^3 on a single SM).  DFTCUDA_SUBSPACE_EIG=jacobi|tridiag forces either.
+constexpr int kTridiagMinM = 96;
+
+static int small_eig(KCtxImpl* e, int m, int nev, cudaStream_t s) {
+  const char* force = std::getenv("DFTCUDA_SUBSPACE_EIG");
+  const bool tri = force ? (std::strcmp(force, "tridiag") == 0) : (m >= kTridiagMinM);
+  if (tri) return heev_lowest(e->T, m, nev, e->evals, e->E, m, e->hw, e->status, s);
   const int m2 = m + (m & 1);
   const size_t smem = (sizeof(int2) + 2 * sizeof(double) + sizeof(double2)) * (size_t)(m2 / 2);
   static bool attr = false;
@@ -525,6 +566,12 @@ extern "C" int dftcuda_eig_solve(dftcuda_kctx* c, const double* diag, size_t nba
   cudaStream_t s = c->stream;
   DFT_TRY(eig_alloc(c, n, max_sub, nbands));
   KCtxImpl* e = c->eig;
+  e->rr_tc = precision_uses_tc(c->precision);
+  if (e->rr_tc && !c->d_err) {
+    DFT_CUDA_TRY(cudaMalloc(&c->d_err, sizeof(int)));
+    DFT_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+  }
+  e->err = c->d_err;
   const long ln = (long)n;
   // diagonal
   if (is_device_pointer(diag))
@@ -566,21 +613,31 @@ extern "C" int dftcuda_eig_solve(dftcuda_kctx* c, const double* diag, size_t nba
   size_t it = 0;
   bool converged = false;
   double max_res = 0.0;
+  // Columns of the Rayleigh-Ritz matrix still valid for the current V, W: only products with the
+  // columns added since the last iteration are formed (8 n m added flops instead of the full
+  // rebuild's 8 n m^2, serial.zig:170).  DFTCUDA_GRAM=full rebuilds every iteration.
+  const char* gram_mode = std::getenv("DFTCUDA_GRAM");
+  const bool gram_full = gram_mode && std::strcmp(gram_mode, "full") == 0;
+  size_t t_valid = 0;
+  const long ldt = (long)max_sub;
   for (; it < opts.max_iter; ++it) {
     const int mi = (int)m;
     ProfScope ps_sub(c, P_SUBSPACE, s);
-    DFT_TRY(gram(e, e->V, mi, e->W, mi, e->T, mi, s));
-    k_hermitize<<<ceil_div((size_t)mi * mi, 256), 256, 0, s>>>(e->T, mi); count_launch();
-    DFT_TRY(small_eig(e, mi, s));
-    DFT_TRY(combine(e, e->V, mi, e->E, mi, (int)nbands, e->ritz, 1.0, 0.0, s));
-    DFT_TRY(combine(e, e->W, mi, e->E, mi, (int)nbands, e->res, 1.0, 0.0, s));
+    const int m_old = gram_full ? 0 : (int)t_valid;
+    DFT_TRY(gram(e, e->V, mi, e->W + (size_t)m_old * n, mi - m_old, e->Tk + (size_t)m_old * ldt, (int)ldt, s, true));
+    k_gram_finish<<<ceil_div((size_t)mi * mi, 256), 256, 0, s>>>(e->Tk, ldt, m_old, mi, e->T); count_launch();
+    k_gram_store<<<ceil_div((size_t)mi * mi, 256), 256, 0, s>>>(e->T, mi, e->Tk, ldt); count_launch();
+    t_valid = m;
+    DFT_TRY(small_eig(e, mi, (int)nbands, s));
+    DFT_TRY(combine(e, e->V, mi, e->E, mi, (int)nbands, e->ritz, 1.0, 0.0, s, true));
+    DFT_TRY(combine(e, e->W, mi, e->E, mi, (int)nbands, e->res, 1.0, 0.0, s, true));
     k_residual<<<(unsigned)nbands, 256, 0, s>>>(e->res, e->ritz, e->evals, ln, e->norms); count_launch();
     int jst = 0;
     DFT_CUDA_TRY(cudaMemcpyAsync(h_ev.data(), e->evals, sizeof(double) * nbands, cudaMemcpyDeviceToHost, s));
     DFT_CUDA_TRY(cudaMemcpyAsync(h_nr.data(), e->norms, sizeof(double) * nbands, cudaMemcpyDeviceToHost, s));
     DFT_CUDA_TRY(cudaMemcpyAsync(&jst, e->status, sizeof(int), cudaMemcpyDeviceToHost, s));
     DFT_CUDA_TRY(cudaStreamSynchronize(s));
-    if (jst != 0) return fail(DFTCUDA_ERR_EIGENSOLVER_FAILURE, "eig_solve: subspace Jacobi did not converge");
+    if (jst != 0) return fail(DFTCUDA_ERR_EIGENSOLVER_FAILURE, "eig_solve: subspace eigensolver failed (Jacobi not converged or barrier timeout)");
     max_res = 0.0;
     for (size_t b = 0; b < nbands; ++b) max_res = std::max(max_res, h_nr[b]);
     if (max_res < opts.tol) {
@@ -615,6 +672,7 @@ extern "C" int dftcuda_eig_solve(dftcuda_kctx* c, const double* diag, size_t nba
       ps_sub.stop();
       DFT_CUDA_TRY(cudaMemcpyAsync(e->V, e->ritz, sizeof(double2) * n * nbands, cudaMemcpyDeviceToDevice, s));
       m = nbands;
+      t_valid = 0;
       DFT_TRY(orthonormalize_all(c, (int)m, seed, s));
       DFT_TRY(kctx_apply_h_dev(c, e->V, e->W, m, s));
       applies += m;
@@ -633,6 +691,7 @@ extern "C" int dftcuda_eig_solve(dftcuda_kctx* c, const double* diag, size_t nba
   DFT_CUDA_TRY(cudaMemcpyAsync(vectors_out, e->ritz, sizeof(double2) * n * nbands,
                                is_device_pointer(vectors_out) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
   DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  DFT_TRY(kctx_check_error(c));
   if (info) {
     info->iterations = it;
     info->h_applies = applies;

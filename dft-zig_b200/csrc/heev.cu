@@ -1,0 +1,536 @@
+// Hermitian eigensolver for the Rayleigh-Ritz subspace problem: the zheev('V','U') calls of
+// lobpcg/common.zig:440-537 and linalg/linalg.zig:141-151, restricted to the lowest nev eigenpairs
+// (the Davidson loop reads only the first nbands, lobpcg/serial.zig:196-227).  FP64 throughout,
+// m <= 2048:
+//   1. Householder reduction to real symmetric tridiagonal form Q^H A Q = T, reflectors chosen as
+//      in LAPACK's zlarfg so the off-diagonal of T is real.  One cooperative launch; the matrix
+//      stays in L2 (m = 2048: 64 MB) and each column costs two grid barriers (bounded waits).
+//   2. The nev lowest eigenvalues of T by Sturm-count multisection: one warp per eigenvalue, its
+//      32 lanes evaluate the count at 32 interior points, so the bracket shrinks 33x per round.
+//   3. Eigenvectors of T by inverse iteration on a row-pivoted LU of T - lambda I (three sweeps
+//      from a hashed start vector).  Eigenvalues closer than 1e-5 ||T|| form a group whose vectors
+//      one thread computes in order, re-orthogonalising (modified Gram-Schmidt) after each solve.
+//   4. Back-transformation E = H_0 H_1 ... H_{m-2} Z with the stored reflectors, one warp per
+//      eigenvector, the vector held in shared memory.
+#include <cfloat>
+#include <cmath>
+
+#include "kctx.cuh"
+
+namespace dftcuda {
+
+namespace {
+
+constexpr int HT_THREADS = 512;              // tridiagonalisation block
+constexpr int HT_WARPS = HT_THREADS / 32;
+constexpr int BS_WARPS = 8;                  // bisection: eigenvalues per block
+constexpr int BT_WARPS = 4;                  // back-transformation: eigenvectors per block
+constexpr long kBarrierSpin = 1L << 24;      // polls (with 64 ns sleeps) before a barrier gives up
+constexpr double kGroupTol = 1e-5;           // eigenvalue grouping, relative to ||T||
+
+struct GridBarrier {
+  unsigned* count;
+  unsigned* gen;
+  int* err;
+  unsigned nblocks;
+};
+
+// All blocks of the (co-resident, cooperative) grid meet here.  Returns false for every thread of
+// a block when this or an earlier barrier gave up; the error flag is then set.
+__device__ bool grid_sync(const GridBarrier& b) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    volatile unsigned* vg = b.gen;
+    const unsigned g = *vg;
+    __threadfence();
+    const unsigned arrived = atomicAdd(b.count, 1u);
+    if (arrived == b.nblocks - 1) {
+      atomicExch(b.count, 0u);
+      __threadfence();
+      atomicAdd(b.gen, 1u);
+    } else {
+      long it = 0;
+      while (*vg == g) {
+        if (++it > kBarrierSpin) {
+          atomicExch(b.err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (*(volatile int*)b.err) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sum over the block (HT_THREADS threads), returned to every thread.
+__device__ double2 block_sum2(double2 v, double2* red) {
+  v.x = warp_sum(v.x);
+  v.y = warp_sum(v.y);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double2 t = make_double2(0.0, 0.0);
+  for (int i = 0; i < HT_WARPS; ++i) {
+    t.x += red[i].x;
+    t.y += red[i].y;
+  }
+  return t;
+}
+
+// Step 1.  A: m x m Hermitian, column-major, both triangles.  Column k of the result holds the
+// reflector v_k below the subdiagonal (v_k[0] = 1 implied at row k+1); d, e: T's diagonal and
+// (real) subdiagonal; tau[k]: H_k = I - tau_k v_k v_k^H with H_k^H A[k+1:, k] = e_k e_1.
+// Warp gw of the grid owns the columns r = gw (mod warps) of the trailing matrix.
+__global__ void __launch_bounds__(HT_THREADS) k_hetrd(double2* __restrict__ A, int m, double* __restrict__ dd,
+                                                      double* __restrict__ ee, double2* __restrict__ tau,
+                                                      double2* __restrict__ y, GridBarrier bar) {
+  extern __shared__ double2 hsm[];
+  double2* sv = hsm;      // v_k, m - k - 1 entries
+  double2* sw = hsm + m;  // w = tau A v + alpha v
+  __shared__ double2 red[HT_WARPS];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int gw = blockIdx.x * HT_WARPS + (tid >> 5);
+  const int W = gridDim.x * HT_WARPS;
+  for (int k = 0; k + 1 < m; ++k) {
+    const int n1 = m - k - 1;
+    const double2* col = A + (long)k * m + (k + 1);
+    // Phase A (every block): the reflector of column k.
+    double2 part = make_double2(0.0, 0.0);
+    for (int i = tid; i < n1; i += HT_THREADS) {
+      const double2 x = __ldcg(col + i);
+      sv[i] = x;
+      if (i > 0) part.x += x.x * x.x + x.y * x.y;
+    }
+    const double xnorm2 = block_sum2(part, red).x;
+    const double2 alpha = sv[0];
+    double2 t = make_double2(0.0, 0.0);
+    double beta = alpha.x;
+    if (!(xnorm2 == 0.0 && alpha.y == 0.0)) {
+      beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2), alpha.x);
+      t = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+    }
+    const bool active = !(t.x == 0.0 && t.y == 0.0);
+    // 1 / (alpha - beta)
+    const double2 den = make_double2(alpha.x - beta, alpha.y);
+    const double dn2 = den.x * den.x + den.y * den.y;
+    const double2 sc = active ? make_double2(den.x / dn2, -den.y / dn2) : make_double2(0.0, 0.0);
+    __syncthreads();
+    for (int i = tid; i < n1; i += HT_THREADS) sv[i] = i == 0 ? make_double2(1.0, 0.0) : cmul(sv[i], sc);
+    if (blockIdx.x == 0 && tid == 0) {
+      dd[k] = __ldcg(A + (long)k * m + k).x;
+      ee[k] = beta;
+      tau[k] = t;
+    }
+    __syncthreads();
+    // Phase B: y_r = tau (A22 v)_r = tau sum_c conj(A[c, r]) v_c, one warp per column r.
+    if (active) {
+      for (int r = gw; r < m; r += W) {
+        if (r <= k) continue;
+        const double2* ac = A + (long)r * m + (k + 1);
+        double sx = 0.0, sy = 0.0;
+        for (int i = lane; i < n1; i += 32) {
+          const double2 a = __ldcg(ac + i), v = sv[i];
+          sx += a.x * v.x + a.y * v.y;  // conj(a) v
+          sy += a.x * v.y - a.y * v.x;
+        }
+        sx = warp_sum(sx);
+        sy = warp_sum(sy);
+        if (lane == 0) y[r] = cmul(t, make_double2(sx, sy));
+      }
+    }
+    if (!grid_sync(bar)) return;
+    // Phase C: w = y + alpha v with alpha = -tau (y^H v) / 2; A22 -= v w^H + w v^H.
+    if (active) {
+      double2 p2 = make_double2(0.0, 0.0);
+      for (int i = tid; i < n1; i += HT_THREADS) {
+        const double2 yi = __ldcg(y + k + 1 + i), vi = sv[i];
+        sw[i] = yi;
+        p2.x += yi.x * vi.x + yi.y * vi.y;
+        p2.y += yi.x * vi.y - yi.y * vi.x;
+      }
+      const double2 s = block_sum2(p2, red);
+      const double2 al = cscale(cmul(t, s), -0.5);
+      for (int i = tid; i < n1; i += HT_THREADS) sw[i] = cadd(sw[i], cmul(al, sv[i]));
+      __syncthreads();
+      for (int r = gw; r < m; r += W) {
+        if (r <= k) continue;
+        const double2 wr = cconj(sw[r - k - 1]), vr = cconj(sv[r - k - 1]);
+        double2* ac = A + (long)r * m + (k + 1);
+        for (int i = lane; i < n1; i += 32) {
+          double2 a = __ldcg(ac + i);
+          a = csub(a, cadd(cmul(sv[i], wr), cmul(sw[i], vr)));
+          ac[i] = a;
+        }
+      }
+    }
+    if (blockIdx.x == 0) {
+      double2* cw = A + (long)k * m + (k + 1);
+      for (int i = tid; i < n1; i += HT_THREADS) cw[i] = i == 0 ? make_double2(beta, 0.0) : sv[i];
+    }
+    if (!grid_sync(bar)) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) dd[m - 1] = __ldcg(A + (long)(m - 1) * m + (m - 1)).x;
+}
+
+// Number of eigenvalues of T below x (Sturm sequence of the LDL^T pivots).
+__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int m, double x, double pivmin) {
+  double q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  int cnt = q < 0.0;
+  for (int i = 1; i < m; ++i) {
+    q = (d[i] - x) - e2[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    cnt += q < 0.0;
+  }
+  return cnt;
+}
+
+// Step 2.  w[j], j < nev: the j-th smallest eigenvalue of T.  Block 0 also writes ||T|| (the
+// Gershgorin radius bound) to *tnorm_out for step 3.
+__global__ void __launch_bounds__(BS_WARPS * 32) k_tridiag_bisect(const double* __restrict__ dd, const double* __restrict__ ee,
+                                                                  int m, int nev, double* __restrict__ w,
+                                                                  double* __restrict__ tnorm_out) {
+  extern __shared__ double bsm[];
+  double* d = bsm;
+  double* e2 = bsm + m;
+  __shared__ double red[3][BS_WARPS];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  double lo = DBL_MAX, hi = -DBL_MAX, emax = 0.0;
+  for (int i = tid; i < m; i += blockDim.x) {
+    const double di = dd[i];
+    const double el = i > 0 ? fabs(ee[i - 1]) : 0.0, er = i + 1 < m ? fabs(ee[i]) : 0.0;
+    d[i] = di;
+    if (i + 1 < m) e2[i] = ee[i] * ee[i];
+    lo = fmin(lo, di - el - er);
+    hi = fmax(hi, di + el + er);
+    emax = fmax(emax, er * er);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+  }
+  if (lane == 0) {
+    red[0][wid] = lo;
+    red[1][wid] = hi;
+    red[2][wid] = emax;
+  }
+  __syncthreads();
+  lo = red[0][0];
+  hi = red[1][0];
+  emax = red[2][0];
+  for (int i = 1; i < BS_WARPS; ++i) {
+    lo = fmin(lo, red[0][i]);
+    hi = fmax(hi, red[1][i]);
+    emax = fmax(emax, red[2][i]);
+  }
+  const double tnorm = fmax(fabs(lo), fabs(hi));
+  const double pivmin = DBL_MIN * fmax(1.0, emax);
+  if (blockIdx.x == 0 && tid == 0) *tnorm_out = tnorm;
+  const double fudge = 2.0 * DBL_EPSILON * tnorm + 4.0 * pivmin;
+  lo -= fudge;
+  hi += fudge;
+  const int j = blockIdx.x * BS_WARPS + wid;
+  if (j >= nev) return;
+  const double abstol = DBL_EPSILON * tnorm;
+  for (int it = 0; it < 64; ++it) {
+    const double width = hi - lo;
+    if (width <= fmax(abstol, 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi))) + pivmin) break;
+    const double x = lo + width * (double)(lane + 1) / 33.0;
+    const int c = sturm_count(d, e2, m, x, pivmin);
+    const unsigned ball = __ballot_sync(0xffffffffu, c > j);
+    if (ball) {
+      const int f = __ffs(ball) - 1;
+      const double nhi = __shfl_sync(0xffffffffu, x, f);
+      const double nlo = f > 0 ? __shfl_sync(0xffffffffu, x, f > 0 ? f - 1 : 0) : lo;
+      if (nhi >= hi && nlo <= lo) break;  // no progress: bracket at rounding level
+      lo = nlo;
+      hi = nhi;
+    } else {
+      const double nlo = __shfl_sync(0xffffffffu, x, 31);
+      if (nlo <= lo) break;
+      lo = nlo;
+    }
+  }
+  if (lane == 0) w[j] = 0.5 * (lo + hi);
+}
+
+__device__ __forceinline__ double hashed_unit(uint64_t a, uint64_t b) {
+  uint64_t z = a * 0x9E3779B97F4A7C15ULL + b + 0x632BE59BD9B4E019ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  z ^= z >> 31;
+  return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;  // [-1, 1)
+}
+
+// Step 3.  Z[:, j] (m x nev, column-major, real) = unit eigenvector of T for w[j].  Thread j works
+// when j starts a group (w[j] - w[j-1] > kGroupTol ||T||) and computes the whole group.  lu: per
+// thread 4 m doubles (U's diagonal and two superdiagonals, the multipliers) + m row-swap flags.
+__global__ void k_tridiag_invit(const double* __restrict__ dd, const double* __restrict__ ee, int m, int nev,
+                                const double* __restrict__ w, const double* __restrict__ tnorm_p,
+                                double* __restrict__ Z, double* __restrict__ lu) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nev) return;
+  const double tnorm = fmax(*tnorm_p, DBL_MIN);
+  const double gtol = kGroupTol * tnorm;
+  if (j > 0 && !(w[j] - w[j - 1] > gtol)) return;
+  int jend = j + 1;
+  while (jend < nev && !(w[jend] - w[jend - 1] > gtol)) ++jend;
+  double* u0 = lu + (size_t)j * 5 * m;
+  double* u1 = u0 + m;
+  double* u2 = u1 + m;
+  double* lm = u2 + m;
+  double* sw = lm + m;
+  const double tiny = DBL_EPSILON * tnorm;
+  for (int p = j; p < jend; ++p) {
+    const double lam = w[p];
+    // Row-pivoted elimination of T - lam I.  cur = (a, b): the running row at columns (i, i+1).
+    double a = dd[0] - lam, b = m > 1 ? ee[0] : 0.0;
+    for (int i = 0; i + 1 < m; ++i) {
+      const double sub = ee[i], dn = dd[i + 1] - lam, up = i + 2 < m ? ee[i + 1] : 0.0;
+      if (fabs(a) >= fabs(sub)) {
+        const double piv = fabs(a) < tiny ? (a < 0.0 ? -tiny : tiny) : a;
+        const double l = sub / piv;
+        u0[i] = piv; u1[i] = b; u2[i] = 0.0; lm[i] = l; sw[i] = 0.0;
+        a = dn - l * b;
+        b = up;
+      } else {
+        const double l = a / sub;
+        u0[i] = sub; u1[i] = dn; u2[i] = up; lm[i] = l; sw[i] = 1.0;
+        a = b - l * dn;
+        b = -l * up;
+      }
+    }
+    u0[m - 1] = fabs(a) < tiny ? (a < 0.0 ? -tiny : tiny) : a;
+    double* z = Z + (size_t)p * m;
+    for (int i = 0; i < m; ++i) z[i] = hashed_unit((uint64_t)p, (uint64_t)i);
+    for (int sweep = 0; sweep < 3; ++sweep) {
+      // forward: the same row operations on the right-hand side
+      double cb = z[0];
+      for (int i = 0; i + 1 < m; ++i) {
+        const double nb = z[i + 1];
+        if (sw[i] == 0.0) {
+          z[i] = cb;
+          cb = nb - lm[i] * cb;
+        } else {
+          z[i] = nb;
+          cb = cb - lm[i] * nb;
+        }
+      }
+      z[m - 1] = cb;
+      // back substitution with U (diagonal + two superdiagonals)
+      for (int i = m - 1; i >= 0; --i) {
+        double s = z[i];
+        if (i + 1 < m) s -= u1[i] * z[i + 1];
+        if (i + 2 < m) s -= u2[i] * z[i + 2];
+        z[i] = s / u0[i];
+      }
+      // modified Gram-Schmidt against the group's earlier vectors, then normalise
+      for (int q = j; q < p; ++q) {
+        const double* zq = Z + (size_t)q * m;
+        double dot = 0.0;
+        for (int i = 0; i < m; ++i) dot += zq[i] * z[i];
+        for (int i = 0; i < m; ++i) z[i] -= dot * zq[i];
+      }
+      double nrm = 0.0, big = 0.0;
+      int ib = 0;
+      for (int i = 0; i < m; ++i) {
+        nrm += z[i] * z[i];
+        if (fabs(z[i]) > big) { big = fabs(z[i]); ib = i; }
+      }
+      double sc = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
+      if (z[ib] < 0.0) sc = -sc;
+      for (int i = 0; i < m; ++i) z[i] *= sc;
+    }
+  }
+}
+
+// Step 4.  E[:, j] = H_0 H_1 ... H_{m-2} Z[:, j] (applied right to left), one warp per column.
+__global__ void __launch_bounds__(BT_WARPS * 32) k_hetrd_back(const double2* __restrict__ A, const double2* __restrict__ tau,
+                                                              int m, int nev, const double* __restrict__ Z,
+                                                              double2* __restrict__ E, long lde) {
+  extern __shared__ double2 esm[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int j = blockIdx.x * BT_WARPS + wid;
+  if (j >= nev) return;
+  double2* ev = esm + (size_t)wid * m;
+  const double* zj = Z + (size_t)j * m;
+  for (int i = lane; i < m; i += 32) ev[i] = make_double2(zj[i], 0.0);
+  __syncwarp();
+  for (int k = m - 2; k >= 0; --k) {
+    const double2 t = tau[k];
+    if (t.x == 0.0 && t.y == 0.0) continue;
+    const int n1 = m - k - 1;
+    const double2* vk = A + (long)k * m + (k + 1);
+    double sx = 0.0, sy = 0.0;
+    for (int i = lane; i < n1; i += 32) {
+      const double2 v = i == 0 ? make_double2(1.0, 0.0) : __ldg(vk + i);
+      const double2 x = ev[k + 1 + i];
+      sx += v.x * x.x + v.y * x.y;  // conj(v) x
+      sy += v.x * x.y - v.y * x.x;
+    }
+    sx = warp_sum(sx);
+    sy = warp_sum(sy);
+    const double2 ts = cmul(t, make_double2(sx, sy));
+    for (int i = lane; i < n1; i += 32) {
+      const double2 v = i == 0 ? make_double2(1.0, 0.0) : __ldg(vk + i);
+      ev[k + 1 + i] = csub(ev[k + 1 + i], cmul(ts, v));
+    }
+    __syncwarp();
+  }
+  for (int i = lane; i < m; i += 32) E[(size_t)j * lde + i] = ev[i];
+}
+
+__global__ void k_upper_to_full(const double2* __restrict__ src, long lds, double2* __restrict__ A, int m) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= (long)m * m) return;
+  const int r = (int)(idx % m), c = (int)(idx / m);
+  if (r < c) A[idx] = src[r + c * lds];
+  else if (r == c) A[idx] = make_double2(src[r + c * lds].x, 0.0);
+  else {
+    const double2 u = src[c + r * lds];
+    A[idx] = make_double2(u.x, -u.y);
+  }
+}
+
+}  // namespace
+
+size_t heev_work_bytes(int m, int nev) {
+  const size_t mm = (size_t)m;
+  return 256 * 8 + sizeof(double) * (3 * mm + 1) + sizeof(double2) * 2 * mm + sizeof(double) * mm * nev +
+         sizeof(double) * 5 * mm * nev;
+}
+
+void heev_bind(HeevWork& w, void* base, int m, int nev) {
+  char* b = (char*)base;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { char* p = b + off; off += (bytes + 255) / 256 * 256; return p; };
+  w.bar = (unsigned*)take(4 * sizeof(unsigned));
+  w.d = (double*)take(sizeof(double) * m);
+  w.e = (double*)take(sizeof(double) * m);
+  w.tnorm = (double*)take(sizeof(double));
+  w.tau = (double2*)take(sizeof(double2) * m);
+  w.y = (double2*)take(sizeof(double2) * m);
+  w.z = (double*)take(sizeof(double) * (size_t)m * nev);
+  w.lu = (double*)take(sizeof(double) * 5 * (size_t)m * nev);
+  w.m_cap = m;
+  w.nev_cap = nev;
+}
+
+int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde, const HeevWork& w, int* status,
+                cudaStream_t s) {
+  if (m < 1 || m > 2048 || nev < 1 || nev > m || m > (int)w.m_cap || nev > (int)w.nev_cap)
+    return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "heev: size outside the workspace");
+  static int attr_dev = -1;
+  static int n_sm = 0, per_sm = 0;
+  int dev = 0;
+  DFT_CUDA_TRY(cudaGetDevice(&dev));
+  const size_t smem_tr = sizeof(double2) * 2 * 2048;
+  if (attr_dev != dev) {
+    DFT_CUDA_TRY(cudaFuncSetAttribute(k_hetrd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tr));
+    DFT_CUDA_TRY(cudaFuncSetAttribute(k_hetrd_back, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(sizeof(double2) * BT_WARPS * 2048)));
+    DFT_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    DFT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hetrd, HT_THREADS, smem_tr));
+    attr_dev = dev;
+  }
+  if (per_sm < 1) return fail(DFTCUDA_ERR_UNSUPPORTED, "heev: tridiagonalisation kernel does not fit an SM");
+  DFT_CUDA_TRY(cudaMemsetAsync(w.bar, 0, 2 * sizeof(unsigned), s));
+  DFT_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), s));
+  if (m > 1) {
+    GridBarrier bar{w.bar, w.bar + 1, status, 0};
+    const int want = (m + HT_WARPS - 1) / HT_WARPS;
+    bar.nblocks = (unsigned)std::max(1, std::min(want, n_sm * std::min(per_sm, 1)));
+    double2* a_ = A;
+    int m_ = m;
+    double* d_ = w.d;
+    double* e_ = w.e;
+    double2* t_ = w.tau;
+    double2* y_ = w.y;
+    void* args[] = {&a_, &m_, &d_, &e_, &t_, &y_, &bar};
+    DFT_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_hetrd, dim3(bar.nblocks), dim3(HT_THREADS), args,
+                                             sizeof(double2) * 2 * m, s));
+    count_launch();
+  } else {
+    DFT_CUDA_TRY(cudaMemcpyAsync(w.d, A, sizeof(double), cudaMemcpyDeviceToDevice, s));
+    DFT_CUDA_TRY(cudaMemsetAsync(w.tau, 0, sizeof(double2), s));
+  }
+  k_tridiag_bisect<<<ceil_div(nev, BS_WARPS), BS_WARPS * 32, sizeof(double) * 2 * m, s>>>(w.d, w.e, m, nev, evals, w.tnorm);
+  count_launch();
+  k_tridiag_invit<<<ceil_div(nev, 64), 64, 0, s>>>(w.d, w.e, m, nev, evals, w.tnorm, w.z, w.lu);
+  count_launch();
+  k_hetrd_back<<<ceil_div(nev, BT_WARPS), BT_WARPS * 32, sizeof(double2) * BT_WARPS * m, s>>>(A, w.tau, m, nev, w.z, E, lde);
+  count_launch();
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}
+
+int hermitian_upper_to_full(const double2* src, long lds, double2* A, int m, cudaStream_t s) {
+  k_upper_to_full<<<ceil_div((size_t)m * m, 256), 256, 0, s>>>(src, lds, A, m);
+  count_launch();
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}
+
+}  // namespace dftcuda
+
+using namespace dftcuda;
+
+// linalg.hermitian_eigen_decomp (linalg/linalg.zig:141-151, zheev 'V','U'): the nev lowest
+// eigenpairs of the n x n Hermitian matrix a (column-major, upper triangle read).
+extern "C" int dftcuda_hermitian_eigen_decomp(size_t n, const double* a, size_t nev, double* values, double* vectors) {
+  if (n == 0 || nev == 0) return DFTCUDA_OK;
+  if (!a || !values || !vectors) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "hermitian_eigen_decomp: null argument");
+  if (n > 2048 || nev > n) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "hermitian_eigen_decomp: n > 2048 or nev > n");
+  const int m = (int)n, k = (int)nev;
+  cudaStream_t s = nullptr;
+  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct Guard {
+    cudaStream_t s;
+    void* p[4] = {nullptr, nullptr, nullptr, nullptr};
+    ~Guard() {
+      for (void* q : p)
+        if (q) cudaFree(q);
+      cudaStreamDestroy(s);
+    }
+  } g{s};
+  const size_t mat = sizeof(double2) * n * n;
+  DFT_CUDA_TRY(cudaMalloc(&g.p[0], mat));
+  DFT_CUDA_TRY(cudaMalloc(&g.p[1], mat + sizeof(double2) * n * nev + sizeof(double) * nev + 256));
+  DFT_CUDA_TRY(cudaMalloc(&g.p[2], heev_work_bytes(m, k)));
+  DFT_CUDA_TRY(cudaMalloc(&g.p[3], 256));
+  double2* src = (double2*)g.p[0];
+  double2* A = (double2*)g.p[1];
+  double2* E = A + n * n;
+  double* ev = (double*)(E + n * nev);
+  HeevWork w;
+  heev_bind(w, g.p[2], m, k);
+  int* status = (int*)g.p[3];
+  DFT_CUDA_TRY(cudaMemcpyAsync(src, a, mat, is_device_pointer(a) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  DFT_TRY(hermitian_upper_to_full(src, (long)n, A, m, s));
+  DFT_TRY(heev_lowest(A, m, k, ev, E, (long)n, w, status, s));
+  int h_status = 0;
+  DFT_CUDA_TRY(cudaMemcpyAsync(&h_status, status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DFT_CUDA_TRY(cudaMemcpyAsync(values, ev, sizeof(double) * nev,
+                               is_device_pointer(values) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+  DFT_CUDA_TRY(cudaMemcpyAsync(vectors, E, sizeof(double2) * n * nev,
+                               is_device_pointer(vectors) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+  DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h_status != 0) return fail(DFTCUDA_ERR_TIMEOUT, "hermitian_eigen_decomp: grid barrier timed out");
+  return DFTCUDA_OK;
+}

@@ -309,7 +309,7 @@ int kctx_ensure_coef(dftcuda_kctx* c, size_t cols) {
   }
   size_t need = std::max(zgemm_workspace_elems(c->nl.nproj, (int)cols, (int)c->npw),
                          zgemm_workspace_elems((int)cols, (int)c->npw, c->nl.nproj));
-  if (c->precision == DFTCUDA_PRECISION_TF32) {
+  if (precision_uses_tc(c->precision)) {
     need = std::max(need, cgemm_tf32_workspace_elems(c->nl.nproj, (int)cols, (int)c->npw));
     need = std::max(need, cgemm_tf32_workspace_elems((int)cols, (int)c->npw, c->nl.nproj));
     if (!c->d_err) {
@@ -336,7 +336,8 @@ int kctx_project(dftcuda_kctx* c, const double2* x, size_t ncols, cudaStream_t s
   g.B = x; g.ldb = (long)c->npw; g.b_kc = true; g.conj_b = false;
   g.O = c->d_coef; g.ldo_r = (long)ncols; g.ldo_c = 1;
   g.alpha = 1.0; g.beta = 0.0;
-  if (c->precision == DFTCUDA_PRECISION_TF32) return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err);
+  if (precision_uses_tc(c->precision))
+    return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err, c->precision == DFTCUDA_PRECISION_TF32X3);
   return zgemm(g, s, c->d_gemm_ws, c->gemm_ws_elems);
 }
 
@@ -359,7 +360,8 @@ static int nonlocal_block(dftcuda_kctx* c, const double2* x, double2* y, size_t 
   g.B = c->nl.P; g.ldb = (long)c->npw; g.b_kc = false; g.conj_b = true;
   g.O = y; g.ldo_r = (long)c->npw; g.ldo_c = 1;
   g.alpha = 1.0 / c->volume; g.beta = 1.0;
-  if (c->precision == DFTCUDA_PRECISION_TF32) return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err);
+  if (precision_uses_tc(c->precision))
+    return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err, c->precision == DFTCUDA_PRECISION_TF32X3);
   return zgemm(g, s, c->d_gemm_ws, c->gemm_ws_elems);
 }
 
@@ -503,7 +505,7 @@ extern "C" int dftcuda_kctx_create(dftcuda_kctx** out, int nx, int ny, int nz, d
   *out = nullptr;
   if (nx <= 0 || ny <= 0 || nz <= 0 || !(volume > 0.0) || n_pw == 0 || !hkl || !kinetic || !gcart)
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "kctx_create: bad arguments");
-  if (precision != DFTCUDA_PRECISION_FP64 && precision != DFTCUDA_PRECISION_FP32 && precision != DFTCUDA_PRECISION_TF32)
+  if (precision < DFTCUDA_PRECISION_FP64 || precision > DFTCUDA_PRECISION_TF32X3)
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "kctx_create: unknown precision");
   // Miller index range check, same rule as PwGridMap.init (pw_grid_map.zig:27-35).
   const int min_h = -(nx / 2), min_k = -(ny / 2), min_l = -(nz / 2);
@@ -901,7 +903,7 @@ extern "C" int dftcuda_accumulate_density_noalloc(dftcuda_kctx* c, const double*
   unsigned char* scratch = nullptr;
   DFT_TRY(noalloc_scratch(&scratch));
   const double2* x = reinterpret_cast<const double2*>(vectors);
-  if (c->precision == DFTCUDA_PRECISION_FP32)
+  if (c->precision != DFTCUDA_PRECISION_FP64)
     DFT_TRY(density_noalloc<float>(c, x, nbands, weights, rho, scratch, c->stream));
   else
     DFT_TRY(density_noalloc<double>(c, x, nbands, weights, rho, scratch, c->stream));

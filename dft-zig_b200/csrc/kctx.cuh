@@ -22,7 +22,9 @@ int zgemm(const GemmArgs& g, cudaStream_t s, double2* workspace, size_t workspac
 size_t zgemm_workspace_elems(int M, int N, int K);
 // The same contraction on the tensor cores (tc_gemm.cu): TF32 inputs, FP32 accumulation.  err_dev
 // receives 1 if a bounded wait gave up.
-int cgemm_tf32(const GemmArgs& g, cudaStream_t s, double2* workspace, size_t workspace_elems, int* err_dev);
+// split = true: 3xTF32 (hi + lo operand parts), FP32-class accuracy.
+int cgemm_tf32(const GemmArgs& g, cudaStream_t s, double2* workspace, size_t workspace_elems, int* err_dev, bool split);
+inline bool precision_uses_tc(int p) { return p == DFTCUDA_PRECISION_TF32 || p == DFTCUDA_PRECISION_TF32X3; }
 size_t cgemm_tf32_workspace_elems(int M, int N, int K);
 
 struct NonlocalDev {
@@ -128,6 +130,25 @@ int kctx_check_error(dftcuda_kctx* c);
 int kctx_density_dev(dftcuda_kctx* c, const double2* vecs, size_t nbands, const double* w_dev, double* rho_dev,
                      cudaStream_t s);
 void eig_destroy(KCtxImpl* e);
+
+// Hermitian eigensolver for the subspace problem (heev.cu): the nev lowest eigenpairs of an m x m
+// Hermitian matrix (both triangles, column-major, destroyed), m <= 2048.
+struct HeevWork {
+  unsigned* bar = nullptr;  // grid barrier: count, generation
+  double* d = nullptr;      // tridiagonal diagonal (m)
+  double* e = nullptr;      // subdiagonal (m - 1)
+  double* tnorm = nullptr;  // ||T|| bound
+  double2* tau = nullptr;   // reflector scalars (m)
+  double2* y = nullptr;     // tau A v (m)
+  double* z = nullptr;      // eigenvectors of T (m x nev)
+  double* lu = nullptr;     // inverse-iteration factors (5 m per eigenvalue)
+  size_t m_cap = 0, nev_cap = 0;
+};
+size_t heev_work_bytes(int m, int nev);
+void heev_bind(HeevWork& w, void* base, int m, int nev);
+int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde, const HeevWork& w, int* status,
+                cudaStream_t s);
+int hermitian_upper_to_full(const double2* src, long lds, double2* A, int m, cudaStream_t s);
 
 // Four-step register-FFT path (local4.cu).
 bool kctx_fast_path_ok(const dftcuda_kctx* c, int precision);

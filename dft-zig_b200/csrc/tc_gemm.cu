@@ -13,6 +13,11 @@
 // ring lets the next slice's conversion overlap the MMAs in flight.  The epilogue reads TMEM with
 // tcgen05.ld (each warp its 32 lanes = 32 rows) and writes FP64 results (or split-K partials).
 //
+// SPLIT = true is the 3xTF32 form: each operand element x is held as hi + lo with hi = tf32(x)
+// (round to nearest, cvt.rna.tf32.f32) and lo = tf32(x - hi), and every real product is taken as
+// hi*hi + hi*lo + lo*hi (the lo*lo term is below FP32 rounding).  Twelve MMAs per 8-deep K step
+// instead of four, two shared-memory planes per operand part; relative error ~1e-6 instead of ~1e-3.
+//
 // Every mbarrier wait is bounded: on timeout the CTA records an error flag, waits (bounded) for its
 // outstanding MMAs, frees its TMEM and returns; the host turns the flag into DFTCUDA_ERR_TIMEOUT.
 #include <algorithm>
@@ -27,7 +32,8 @@ constexpr int TC_STAGES = 2;
 constexpr int TC_A_BYTES = TC_M * TC_K * 4;  // one real plane of the A tile
 constexpr int TC_B_BYTES = TC_N * TC_K * 4;
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;  // Ar, Ai, Br, Bi
-constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 64;
+__host__ __device__ constexpr int tc_stage_bytes(bool split) { return split ? 2 * TC_STAGE_BYTES : TC_STAGE_BYTES; }
+__host__ __device__ constexpr int tc_smem(bool split) { return TC_STAGES * tc_stage_bytes(split) + 64; }
 constexpr uint32_t TC_TMEM_COLS = 128;  // Dr (64) + Di (64)
 constexpr long long TC_SPIN_LIMIT = 1LL << 26;
 
@@ -76,7 +82,13 @@ __device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
-template <bool AKC, bool BKC, bool CJA, bool CJB>
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t u;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(u) : "f"(x));
+  return __uint_as_float(u);
+}
+
+template <bool AKC, bool BKC, bool CJA, bool CJB, bool SPLIT>
 __global__ void __launch_bounds__(TC_THREADS) k_cgemm_tf32(int M, int N, int K, const double2* __restrict__ A, long lda,
                                                            const double2* __restrict__ B, long ldb,
                                                            double2* __restrict__ O, long ldo_r, long ldo_c,
@@ -84,7 +96,8 @@ __global__ void __launch_bounds__(TC_THREADS) k_cgemm_tf32(int M, int N, int K, 
                                                            double2* __restrict__ part, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char tsm[];
   unsigned char* stages = tsm;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm + TC_STAGES * TC_STAGE_BYTES);
+  constexpr int SB = tc_stage_bytes(SPLIT);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm + TC_STAGES * SB);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + TC_STAGES);
   __shared__ int s_abort;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -123,11 +136,16 @@ __global__ void __launch_bounds__(TC_THREADS) k_cgemm_tf32(int M, int N, int K, 
     }
     __syncthreads();
     if (s_abort) break;
-    unsigned char* st = stages + s * TC_STAGE_BYTES;
+    // stage layout: Ar, Ai, Br, Bi (hi parts), then for SPLIT Ar, Ai, Br, Bi lo parts
+    unsigned char* st = stages + s * SB;
     float* Ar = reinterpret_cast<float*>(st);
     float* Ai = reinterpret_cast<float*>(st + TC_A_BYTES);
     float* Br = reinterpret_cast<float*>(st + 2 * TC_A_BYTES);
     float* Bi = reinterpret_cast<float*>(st + 2 * TC_A_BYTES + TC_B_BYTES);
+    float* ArL = reinterpret_cast<float*>(st + TC_STAGE_BYTES);
+    float* AiL = reinterpret_cast<float*>(st + TC_STAGE_BYTES + TC_A_BYTES);
+    float* BrL = reinterpret_cast<float*>(st + TC_STAGE_BYTES + 2 * TC_A_BYTES);
+    float* BiL = reinterpret_cast<float*>(st + TC_STAGE_BYTES + 2 * TC_A_BYTES + TC_B_BYTES);
     const int k0 = kbeg + t * TC_K;
     // one 8 x 4 core matrix per warp instruction: lane = (row in core, k in core)
     const int rr = lane & 7, ee = lane >> 3;
@@ -138,8 +156,17 @@ __global__ void __launch_bounds__(TC_THREADS) k_cgemm_tf32(int M, int N, int K, 
       double2 v = make_double2(0.0, 0.0);
       if (gr < M && gk < kend) v = AKC ? __ldg(A + (long)gr * lda + gk) : __ldg(A + (long)gk * lda + gr);
       const uint32_t o = tc_off(r, k) >> 2;
-      Ar[o] = (float)v.x;
-      Ai[o] = CJA ? -(float)v.y : (float)v.y;
+      const double vi = CJA ? -v.y : v.y;
+      if (SPLIT) {
+        const float hr = tf32_rna((float)v.x), hi = tf32_rna((float)vi);
+        Ar[o] = hr;
+        Ai[o] = hi;
+        ArL[o] = tf32_rna((float)(v.x - (double)hr));
+        AiL[o] = tf32_rna((float)(vi - (double)hi));
+      } else {
+        Ar[o] = (float)v.x;
+        Ai[o] = (float)vi;
+      }
     }
     for (int cm = warp; cm < (TC_N / 8) * (TC_K / 4); cm += TC_THREADS / 32) {
       const int g = cm / (TC_K / 4), h = cm % (TC_K / 4);
@@ -148,24 +175,50 @@ __global__ void __launch_bounds__(TC_THREADS) k_cgemm_tf32(int M, int N, int K, 
       double2 v = make_double2(0.0, 0.0);
       if (gc < N && gk < kend) v = BKC ? __ldg(B + (long)gc * ldb + gk) : __ldg(B + (long)gk * ldb + gc);
       const uint32_t o = tc_off(c, k) >> 2;
-      Br[o] = (float)v.x;
-      Bi[o] = CJB ? -(float)v.y : (float)v.y;
+      const double vi = CJB ? -v.y : v.y;
+      if (SPLIT) {
+        const float hr = tf32_rna((float)v.x), hi = tf32_rna((float)vi);
+        Br[o] = hr;
+        Bi[o] = hi;
+        BrL[o] = tf32_rna((float)(v.x - (double)hr));
+        BiL[o] = tf32_rna((float)(vi - (double)hi));
+      } else {
+        Br[o] = (float)v.x;
+        Bi[o] = (float)vi;
+      }
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-      const uint32_t sa = smem_base + s * TC_STAGE_BYTES;
+      const uint32_t sa = smem_base + s * SB;
       const uint32_t sar = sa, sai = sa + TC_A_BYTES, sbr = sa + 2 * TC_A_BYTES, sbi = sbr + TC_B_BYTES;
+      const uint32_t lo = TC_STAGE_BYTES;  // offset of the lo planes
       const uint32_t id_pos = tc_idesc(false), id_neg = tc_idesc(true);
 #pragma unroll
       for (int kk = 0; kk < TC_K / 8; ++kk) {
         const uint32_t koff = kk * 256;  // two 128-byte core matrices per 8-deep step
         const bool acc = (t > 0) || (kk > 0);
-        tc_mma(d_re, tc_desc(sar + koff), tc_desc(sbr + koff), id_pos, acc);
-        tc_mma(d_re, tc_desc(sai + koff), tc_desc(sbi + koff), id_neg, true);
-        tc_mma(d_im, tc_desc(sar + koff), tc_desc(sbi + koff), id_pos, acc);
-        tc_mma(d_im, tc_desc(sai + koff), tc_desc(sbr + koff), id_pos, true);
+        if (SPLIT) {
+          // cross terms first (smaller), then hi*hi
+          tc_mma(d_re, tc_desc(sar + koff), tc_desc(sbr + lo + koff), id_pos, acc);
+          tc_mma(d_re, tc_desc(sar + lo + koff), tc_desc(sbr + koff), id_pos, true);
+          tc_mma(d_re, tc_desc(sai + koff), tc_desc(sbi + lo + koff), id_neg, true);
+          tc_mma(d_re, tc_desc(sai + lo + koff), tc_desc(sbi + koff), id_neg, true);
+          tc_mma(d_re, tc_desc(sar + koff), tc_desc(sbr + koff), id_pos, true);
+          tc_mma(d_re, tc_desc(sai + koff), tc_desc(sbi + koff), id_neg, true);
+          tc_mma(d_im, tc_desc(sar + koff), tc_desc(sbi + lo + koff), id_pos, acc);
+          tc_mma(d_im, tc_desc(sar + lo + koff), tc_desc(sbi + koff), id_pos, true);
+          tc_mma(d_im, tc_desc(sai + koff), tc_desc(sbr + lo + koff), id_pos, true);
+          tc_mma(d_im, tc_desc(sai + lo + koff), tc_desc(sbr + koff), id_pos, true);
+          tc_mma(d_im, tc_desc(sar + koff), tc_desc(sbi + koff), id_pos, true);
+          tc_mma(d_im, tc_desc(sai + koff), tc_desc(sbr + koff), id_pos, true);
+        } else {
+          tc_mma(d_re, tc_desc(sar + koff), tc_desc(sbr + koff), id_pos, acc);
+          tc_mma(d_re, tc_desc(sai + koff), tc_desc(sbi + koff), id_neg, true);
+          tc_mma(d_im, tc_desc(sar + koff), tc_desc(sbi + koff), id_pos, acc);
+          tc_mma(d_im, tc_desc(sai + koff), tc_desc(sbr + koff), id_pos, true);
+        }
       }
       tc_commit(mbar_base + 8 * s);
     }
@@ -265,19 +318,36 @@ size_t cgemm_tf32_workspace_elems(int M, int N, int K) {
   return s > 1 ? (size_t)s * M * N : 0;
 }
 
-template <bool AKC, bool BKC, bool CJA, bool CJB>
+template <bool AKC, bool BKC, bool CJA, bool CJB, bool SPLIT>
 static void tc_launch(const GemmArgs& g, dim3 grid, int kps, double2* part, int* err, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_cgemm_tf32<AKC, BKC, CJA, CJB>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-    attr = true;
+  static int attr_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    cudaFuncSetAttribute(k_cgemm_tf32<AKC, BKC, CJA, CJB, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(SPLIT));
+    attr_dev = dev;
   }
-  k_cgemm_tf32<AKC, BKC, CJA, CJB><<<grid, TC_THREADS, TC_SMEM, s>>>(g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r,
-                                                                    g.ldo_c, g.alpha, g.beta, kps, part, err);
+  k_cgemm_tf32<AKC, BKC, CJA, CJB, SPLIT><<<grid, TC_THREADS, tc_smem(SPLIT), s>>>(
+      g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r, g.ldo_c, g.alpha, g.beta, kps, part, err);
   count_launch();
 }
 
-int cgemm_tf32(const GemmArgs& g, cudaStream_t s, double2* ws, size_t ws_elems, int* err_dev) {
+template <bool SPLIT>
+static int tc_dispatch(const GemmArgs& g, dim3 grid, int kps, double2* part, int* err_dev, cudaStream_t s) {
+  const int key = (g.a_kc ? 8 : 0) | (g.b_kc ? 4 : 0) | (g.conj_a ? 2 : 0) | (g.conj_b ? 1 : 0);
+  switch (key) {
+    case 12: tc_launch<true, true, false, false, SPLIT>(g, grid, kps, part, err_dev, s); break;   // projection
+    case 1: tc_launch<false, false, false, true, SPLIT>(g, grid, kps, part, err_dev, s); break;   // back-projection
+    case 14: tc_launch<true, true, true, false, SPLIT>(g, grid, kps, part, err_dev, s); break;    // Gram V^H W
+    case 4: tc_launch<false, true, false, false, SPLIT>(g, grid, kps, part, err_dev, s); break;
+    case 8: tc_launch<true, false, false, false, SPLIT>(g, grid, kps, part, err_dev, s); break;   // V C
+    case 0: tc_launch<false, false, false, false, SPLIT>(g, grid, kps, part, err_dev, s); break;
+    default: return fail(DFTCUDA_ERR_UNSUPPORTED, "cgemm_tf32: operand layout not instantiated");
+  }
+  return DFTCUDA_OK;
+}
+
+int cgemm_tf32(const GemmArgs& g, cudaStream_t s, double2* ws, size_t ws_elems, int* err_dev, bool split) {
   if (g.M <= 0 || g.N <= 0) return DFTCUDA_OK;
   if (g.K <= 0) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "cgemm_tf32: K must be positive");
   int splits = tc_splits(g.M, g.N, g.K);
@@ -287,16 +357,7 @@ int cgemm_tf32(const GemmArgs& g, cudaStream_t s, double2* ws, size_t ws_elems, 
   splits = (g.K + kps - 1) / kps;
   dim3 grid(ceil_div(g.N, TC_N), ceil_div(g.M, TC_M), splits);
   double2* part = splits > 1 ? ws : nullptr;
-  const int key = (g.a_kc ? 8 : 0) | (g.b_kc ? 4 : 0) | (g.conj_a ? 2 : 0) | (g.conj_b ? 1 : 0);
-  switch (key) {
-    case 12: tc_launch<true, true, false, false>(g, grid, kps, part, err_dev, s); break;   // projection
-    case 1: tc_launch<false, false, false, true>(g, grid, kps, part, err_dev, s); break;   // back-projection
-    case 14: tc_launch<true, true, true, false>(g, grid, kps, part, err_dev, s); break;    // Gram V^H W
-    case 4: tc_launch<false, true, false, false>(g, grid, kps, part, err_dev, s); break;
-    case 8: tc_launch<true, false, false, false>(g, grid, kps, part, err_dev, s); break;
-    case 0: tc_launch<false, false, false, false>(g, grid, kps, part, err_dev, s); break;
-    default: return fail(DFTCUDA_ERR_UNSUPPORTED, "cgemm_tf32: operand layout not instantiated");
-  }
+  DFT_TRY(split ? tc_dispatch<true>(g, grid, kps, part, err_dev, s) : tc_dispatch<false>(g, grid, kps, part, err_dev, s));
   if (part) {
     const long tot = (long)g.M * g.N;
     k_cgemm_reduce<<<ceil_div(tot, 256), 256, 0, s>>>(g.M, g.N, splits, part, g.O, g.ldo_r, g.ldo_c, g.alpha, g.beta); count_launch();

@@ -38,14 +38,19 @@ extern "C" {
 #define DFTCUDA_ERR_TIMEOUT (-8)             /* a bounded device wait gave up (no reference counterpart) */
 
 /* Arithmetic of one k-point context's H|psi>:
- *  FP64  every pass in FP64;
- *  FP32  local-potential FFT passes in FP32, projector GEMMs in FP64;
- *  TF32  FFT passes in FP32 and the projector GEMMs on the tensor cores (tcgen05 kind::tf32, FP32
- *        accumulation in TMEM).
- * Wavefunctions are FP64 at the boundary in every mode; the eigensolver's subspace algebra is FP64. */
+ *  FP64    every pass in FP64;
+ *  FP32    local-potential FFT passes in FP32, projector GEMMs in FP64;
+ *  TF32    FFT passes in FP32 and the projector GEMMs on the tensor cores (tcgen05 kind::tf32, FP32
+ *          accumulation in TMEM); relative error ~1e-3;
+ *  TF32X3  as TF32 with every operand split into two TF32 parts (hi + lo, three MMAs per real
+ *          product): FP32-class accuracy (~1e-6) on the tensor cores.
+ * Wavefunctions are FP64 at the boundary in every mode.  In TF32 and TF32X3 contexts the
+ * eigensolver's Rayleigh-Ritz products (V^H W, V C, W C) use the same tensor-core GEMM (split form);
+ * orthonormalisation, the subspace eigensolver and residual norms stay FP64. */
 #define DFTCUDA_PRECISION_FP64 0
 #define DFTCUDA_PRECISION_FP32 1
 #define DFTCUDA_PRECISION_TF32 2
+#define DFTCUDA_PRECISION_TF32X3 3
 
 typedef struct dftcuda_kctx dftcuda_kctx;
 typedef struct dftcuda_fft_plan dftcuda_fft_plan;
@@ -131,6 +136,13 @@ typedef struct dftcuda_eig_info {
 int dftcuda_eig_solve(dftcuda_kctx* ctx, const double* diag, size_t nbands, const dftcuda_eig_opts* opts,
                       const double* init_vecs, size_t init_cols, double* values_out, double* vectors_out,
                       dftcuda_eig_info* info);
+
+/* Dense Hermitian eigensolver: linalg.hermitian_eigen_decomp (src/features/linalg/linalg.zig:141-151;
+ * zheev 'V','U' in hermitian_eigen_decomp_lapack) and lobpcg/common.zig:440-508, restricted to the
+ * nev lowest eigenpairs (nev = n gives the full decomposition).  a: n x n column-major complex, the
+ * upper triangle is read.  values[nev] ascending, vectors[n x nev]; host or device pointers.
+ * n <= 2048.  The Davidson loop above uses the same kernels for subspaces of 96 and more. */
+int dftcuda_hermitian_eigen_decomp(size_t n, const double* a, size_t nev, double* values, double* vectors);
 
 /* ------------------------------------------------------------------------------------------
  * Band density: rho(r) += sum_b weight_b |psi_b(r)|^2 / Omega
