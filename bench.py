@@ -36,6 +36,9 @@ if ROOT not in sys.path:
 CELL, SEED, ECUT, KMESH, NBANDS = "si64", 1, 30.0, (2, 2, 2), 160
 NCOLS = NBANDS + 4  # Davidson block (lobpcg/serial.zig:78-82)
 S = 16  # bytes per FP64 complex
+# Measured DRAM traffic of k_plane_inv4 + k_xline4 + k_plane_fwd4 per column (FP64, 75^3 box):
+# 315 MB for one 32-column application at Gamma (ncu dram__bytes_read.sum + dram__bytes_write.sum).
+LOCAL_DRAM_BYTES_PER_COLUMN = 315.0e6 / 32
 
 
 def bytes_per_column(npw: int, N: int, nb: int) -> float:
@@ -309,7 +312,11 @@ def run_ours(args):
             "unit": "GB/s",
             "frac": round(achieved / peak, 4) if achieved else None,
             "peak_source": peak_kind,
-            "traffic": None,
+            # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the three passes per column,
+            # from one ncu capture of the 32-column Gamma case, scaled to one 164-column block
+            "traffic": round(LOCAL_DRAM_BYTES_PER_COLUMN * NCOLS),
+            "algorithmic_bytes": round(bytes_per_column(int(npw_avg), N, NCOLS) * NCOLS),
+            "per": "one 164-column application of the local operator at one k-point",
         },
         "kernels": kern,
         "variants": variants,

@@ -53,7 +53,21 @@ ABI_SYMBOLS = (
     "dftcuda_kctx_get_profile",
     "dftcuda_accumulate_density_noalloc",
     "dftcuda_hermitian_eigen_decomp",
+    "dftcuda_eig_solve_batch",
+    "dftcuda_kctx_autotune",
+    "dftcuda_kctx_set_preconditioner",
+    "dftcuda_precond_mlp_loss_grad",
+    "dftcuda_precond_mlp_train",
+    "dftcuda_fno_forward",
+    "dftcuda_fno_loss_grad",
+    "dftcuda_fno_train",
 )
+
+PRECOND_REFERENCE = 0  # r / (|k+G|^2 - lambda), lobpcg/common.zig:214-226
+PRECOND_TPA = 1  # Teter-Payne-Allan
+PRECOND_MLP = 2  # learned per-plane-wave MLP
+PRECOND_MLP_PARAMS = 4481
+FNO_PARAMS = 2097473  # learned first SCF density (Fourier neural operator)
 
 PRECISION_FP64 = 0
 PRECISION_FP32 = 1
@@ -150,6 +164,11 @@ PROFILE_FIELDS = (
 )
 
 
+class _TuneReport(ct.Structure):
+    _fields_ = [("fft_path", ct.c_int), ("box_budget_mb", ct.c_double), ("proj_splits", ct.c_int), ("back_splits", ct.c_int),
+                ("default_ms", ct.c_double), ("tuned_ms", ct.c_double), ("candidates", ct.c_int)]
+
+
 class _Profile(ct.Structure):
     _fields_ = [(f, ct.c_uint64) for f in PROFILE_FIELDS]
 
@@ -189,6 +208,15 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.dftcuda_kctx_get_profile.argtypes = [vp, ct.POINTER(_Profile)]
     lib.dftcuda_accumulate_density_noalloc.argtypes = [vp, dp, sz, sz, dp, dp]
     lib.dftcuda_hermitian_eigen_decomp.argtypes = [sz, dp, sz, dp, dp]
+    pp = ct.POINTER(ct.c_void_p)
+    lib.dftcuda_kctx_autotune.argtypes = [vp, sz, ct.POINTER(_TuneReport)]
+    lib.dftcuda_kctx_set_preconditioner.argtypes = [vp, ip, vp, sz]
+    lib.dftcuda_precond_mlp_loss_grad.argtypes = [sz, sz, vp, vp, vp, vp, vp, vp, dp, vp]
+    lib.dftcuda_precond_mlp_train.argtypes = [sz, sz, vp, vp, vp, vp, vp, vp, sz, ct.c_float, dp]
+    lib.dftcuda_fno_forward.argtypes = [ip, ip, ip, vp, vp, vp]
+    lib.dftcuda_fno_loss_grad.argtypes = [sz, vp, vp, vp, vp, vp, dp, vp]
+    lib.dftcuda_fno_train.argtypes = [sz, vp, vp, vp, vp, vp, sz, ct.c_float, dp]
+    lib.dftcuda_eig_solve_batch.argtypes = [sz, pp, pp, sz, ct.POINTER(_EigOpts), pp, ct.POINTER(ct.c_size_t), pp, pp, ct.POINTER(_EigInfo)]
     _lib = lib
     return lib
 
@@ -377,6 +405,22 @@ class KpointContext:
         _check(self._lib.dftcuda_accumulate_density_noalloc(self._h, _ptr(vectors_dev), self.n, nb, _ptr(weights_dev), _ptr(rho_dev)))
         return rho_dev
 
+    def set_preconditioner(self, kind: int, params=None):
+        """Preconditioner of this context's Davidson correction step (PRECOND_*); the learned one
+        takes its PRECOND_MLP_PARAMS float32 weights."""
+        buf = None
+        n = 0
+        if params is not None:
+            buf = np.ascontiguousarray(params, dtype=np.float32)
+            n = buf.size
+        _check(self._lib.dftcuda_kctx_set_preconditioner(self._h, kind, _ptr(buf), n))
+
+    def autotune(self, ncols: int) -> dict:
+        """Time candidate H|psi> launch configurations on ncols columns and keep the fastest."""
+        r = _TuneReport()
+        _check(self._lib.dftcuda_kctx_autotune(self._h, ncols, ct.byref(r)))
+        return {f: getattr(r, f) for f, _ in r._fields_}
+
     def hermitian_eigen_decomp_iterative(self, diag, nbands, opts: Options = Options()) -> EigenDecomp:
         """iterative.zig:67-76 -> lobpcg_serial.solve with this context as the Operator."""
         diag = np.ascontiguousarray(diag, dtype=np.float64)
@@ -393,6 +437,126 @@ class KpointContext:
         info = _EigInfo()
         _check(self._lib.dftcuda_eig_solve(self._h, _ptr(diag), nbands, ct.byref(o), _ptr(init), icols, _ptr(vals), _ptr(vecs), ct.byref(info)))
         return EigenDecomp(vals, vecs, self.n, info.iterations, info.h_applies, bool(info.converged), info.max_residual)
+
+
+def hermitian_eigen_decomp_iterative_batch(ctxs, diags, nbands, opts: Options = Options(), init_vectors=None) -> list:
+    """The iterative solver for several k-point contexts at once (dftcuda_eig_solve_batch): the runs
+    advance in lockstep on their contexts' streams.  init_vectors: None or a list with an (icols, n_k)
+    array or None per context.  Returns one EigenDecomp per context."""
+    lib = load_library()
+    nk = len(ctxs)
+    if nk == 0:
+        return []
+    o = _EigOpts(opts.max_iter, opts.tol, opts.max_subspace, opts.block_size, 1 if opts.init_diagonal else 0)
+    keep = []
+    d_arr = (ct.c_void_p * nk)()
+    i_arr = (ct.c_void_p * nk)()
+    ic_arr = (ct.c_size_t * nk)()
+    v_arr = (ct.c_void_p * nk)()
+    x_arr = (ct.c_void_p * nk)()
+    out = []
+    for i, kc in enumerate(ctxs):
+        d = np.ascontiguousarray(diags[i], dtype=np.float64)
+        if d.size != kc.n:
+            raise InvalidMatrixSize("diag length != n")
+        keep.append(d)
+        d_arr[i] = d.ctypes.data
+        if init_vectors is not None and init_vectors[i] is not None:
+            iv = np.ascontiguousarray(init_vectors[i], dtype=np.complex128).reshape(-1, kc.n)
+            keep.append(iv)
+            i_arr[i] = iv.ctypes.data
+            ic_arr[i] = iv.shape[0]
+        vals = np.empty(nbands)
+        vecs = np.empty((nbands, kc.n), dtype=np.complex128)
+        out.append((vals, vecs))
+        v_arr[i] = vals.ctypes.data
+        x_arr[i] = vecs.ctypes.data
+    h_arr = (ct.c_void_p * nk)(*[kc.handle.value for kc in ctxs])
+    infos = (_EigInfo * nk)()
+    _check(lib.dftcuda_eig_solve_batch(nk, h_arr, d_arr, nbands, ct.byref(o), i_arr, ic_arr, v_arr, x_arr, infos))
+    return [EigenDecomp(v, x, kc.n, inf.iterations, inf.h_applies, bool(inf.converged), inf.max_residual)
+            for (v, x), kc, inf in zip(out, ctxs, infos)]
+
+
+def _mlp_arrays(off, feat, cc, w, dnorm):
+    off = np.ascontiguousarray(off, dtype=np.int32)
+    feat = np.ascontiguousarray(feat, dtype=np.float32)
+    cc = np.ascontiguousarray(np.stack([np.real(cc), np.imag(cc)], axis=1), dtype=np.float32)
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    dnorm = np.ascontiguousarray(dnorm, dtype=np.float32)
+    return off, feat, cc, w, dnorm
+
+
+def precond_mlp_loss_grad(params, off, feat, cc, w, dnorm):
+    """Loss and gradient of the learned preconditioner on the GPU (dftcuda_precond_mlp_loss_grad)."""
+    lib = load_library()
+    _require_device()
+    off, feat, cc, w, dnorm = _mlp_arrays(off, feat, cc, w, dnorm)
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    loss = ct.c_double(0.0)
+    grad = np.zeros(PRECOND_MLP_PARAMS, dtype=np.float32)
+    _check(lib.dftcuda_precond_mlp_loss_grad(len(off) - 1, feat.shape[0], _ptr(off), _ptr(feat), _ptr(cc), _ptr(w), _ptr(dnorm),
+                                             _ptr(p), ct.addressof(loss), _ptr(grad)))
+    return loss.value, grad
+
+
+def precond_mlp_train(params, off, feat, cc, w, dnorm, steps: int, lr: float = 1e-3):
+    """`steps` full-batch Adam steps on the GPU (dftcuda_precond_mlp_train); returns the trained
+    parameters and the loss before each step."""
+    lib = load_library()
+    _require_device()
+    off, feat, cc, w, dnorm = _mlp_arrays(off, feat, cc, w, dnorm)
+    p = np.array(params, dtype=np.float32)
+    hist = np.zeros(steps, dtype=np.float64)
+    _check(lib.dftcuda_precond_mlp_train(len(off) - 1, feat.shape[0], _ptr(off), _ptr(feat), _ptr(cc), _ptr(w), _ptr(dnorm),
+                                         _ptr(p), steps, lr, _ptr(hist)))
+    return p, hist
+
+
+def _fno_set(samples):
+    """samples: list of (dims (nx, ny, nz), u [2][N], target [N] or None)."""
+    dims = np.ascontiguousarray([d for dd, _, _ in samples for d in dd], dtype=np.int32)
+    sizes = [int(np.prod(dd)) for dd, _, _ in samples]
+    offs = np.ascontiguousarray(np.concatenate([[0], np.cumsum(sizes)]), dtype=np.uint64)
+    u = np.ascontiguousarray(np.concatenate([np.asarray(uu, np.float32).reshape(-1) for _, uu, _ in samples]), dtype=np.float32)
+    t = None
+    if all(tt is not None for _, _, tt in samples):
+        t = np.ascontiguousarray(np.concatenate([np.asarray(tt, np.float32).reshape(-1) for _, _, tt in samples]), dtype=np.float32)
+    return dims, offs, u, t
+
+
+def fno_forward(params, u, dims):
+    """The learned first-density operator on one cell: u [2][nx ny nz] -> [nx ny nz] (float32)."""
+    lib = load_library()
+    _require_device()
+    nx, ny, nz = dims
+    uu = np.ascontiguousarray(u, dtype=np.float32).reshape(-1)
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    out = np.empty(nx * ny * nz, dtype=np.float32)
+    _check(lib.dftcuda_fno_forward(nx, ny, nz, _ptr(uu), _ptr(p), _ptr(out)))
+    return out
+
+
+def fno_loss_grad(params, samples):
+    lib = load_library()
+    _require_device()
+    dims, offs, u, t = _fno_set(samples)
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    loss = ct.c_double(0.0)
+    grad = np.zeros(FNO_PARAMS, dtype=np.float32)
+    _check(lib.dftcuda_fno_loss_grad(len(samples), _ptr(dims), _ptr(offs), _ptr(u), _ptr(t), _ptr(p), ct.addressof(loss), _ptr(grad)))
+    return loss.value, grad
+
+
+def fno_train(params, samples, steps: int, lr: float = 1e-3):
+    """`steps` full-batch Adam steps on the GPU (dftcuda_fno_train); returns (params, loss history)."""
+    lib = load_library()
+    _require_device()
+    dims, offs, u, t = _fno_set(samples)
+    p = np.array(params, dtype=np.float32)
+    hist = np.zeros(steps, dtype=np.float64)
+    _check(lib.dftcuda_fno_train(len(samples), _ptr(dims), _ptr(offs), _ptr(u), _ptr(t), _ptr(p), steps, lr, _ptr(hist)))
+    return p, hist
 
 
 def hermitian_eigen_decomp(a, nev: Optional[int] = None) -> EigenDecomp:

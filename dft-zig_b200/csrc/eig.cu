@@ -14,9 +14,9 @@
 //  * new directions: r_b / (diag - lambda_b) clamped at |den| >= 1e-8 (common.zig:214-226), then
 //    modified Gram-Schmidt against V with a drop when the remaining norm is < 1e-8
 //    (common.zig:263-284, serial.zig:250-262).  The device does this for the whole block at once:
-//    project out V twice, then a Cholesky of the new block's Gram matrix taken column by column in
-//    the reference's order, dropping a column when its Cholesky pivot (= the MGS norm) is < 1e-8,
-//    and a second Cholesky pass for orthogonality (CholQR2).  This spans exactly the vectors MGS
+//    project out V, then a Cholesky of the new block's Gram matrix taken column by column in the
+//    reference's order, dropping a column when its Cholesky pivot (= the MGS norm) is < 1e-8, then
+//    project the kept vectors out of V once more and take a second Cholesky pass (CholQR2).  This spans exactly the vectors MGS
 //    keeps, in the same order; only rounding differs.
 #include <algorithm>
 #include <cmath>
@@ -274,87 +274,100 @@ __global__ void k_precondition(double2* __restrict__ Q, const double2* __restric
   Q[idx] = make_double2(v.x * inv, v.y * inv);
 }
 
-// Left-looking Cholesky of the k x k Gram matrix G (column-major) in column order, dropping column j
-// when its pivot sqrt(d) < drop (the MGS norm test).  Produces Z (k x kk, column-major, ld k) with
-// Q Z = the orthonormalised kept columns, kept[0..kk) and *kk_out.
-__global__ void __launch_bounds__(512) k_chol_drop(const double2* __restrict__ G, int k, double drop,
-                                                   double2* __restrict__ R, double2* __restrict__ Z,
-                                                   int* __restrict__ kept, int* __restrict__ kk_out) {
-  // R: k x k workspace, row j holds R[j][l] for kept j (row-major, ld k).
-  __shared__ int s_kept[1024];
-  __shared__ int s_nk;
+// Cholesky of the k x k Gram matrix G (column-major) in column order with the MGS drop rule: column
+// j is dropped when its pivot sqrt(d) < drop, where d, the Schur-complement diagonal after the kept
+// columns before j, is exactly the squared norm MGS leaves (common.zig:263-284).  Right-looking: each
+// kept column scales its row and updates the whole trailing upper triangle in parallel; dropped
+// columns update nothing.  A: k x k row-major workspace (its kept rows end up as R); kept[0..kk),
+// *kk_out.  One CTA; the working triangle stays in L2.
+__global__ void __launch_bounds__(1024) k_chol_right(const double2* __restrict__ G, int k, double drop,
+                                                     double2* __restrict__ A, int* __restrict__ kept, int* __restrict__ kk_out) {
   __shared__ double s_piv;
-  __shared__ double red[512];
+  __shared__ int s_nk;
   const int tid = threadIdx.x, nt = blockDim.x;
+  for (long idx = tid; idx < (long)k * k; idx += nt) {
+    const int j = (int)(idx / k), l = (int)(idx - (long)j * k);
+    if (l >= j) A[idx] = G[j + (long)l * k];
+  }
   if (tid == 0) s_nk = 0;
   __syncthreads();
   for (int j = 0; j < k; ++j) {
-    const int nk = s_nk;
-    // d = G[j][j] - sum_{i kept} |R[i][j]|^2
-    double part = 0.0;
-    for (int t = tid; t < nk; t += nt) {
-      const double2 r = R[(long)s_kept[t] * k + j];
-      part += r.x * r.x + r.y * r.y;
-    }
-    red[tid] = part;
-    __syncthreads();
-    for (int w = nt / 2; w > 0; w >>= 1) {
-      if (tid < w) red[tid] += red[tid + w];
-      __syncthreads();
-    }
     if (tid == 0) {
-      const double d = G[j + (long)j * k].x - red[0];
-      s_piv = (d > 0.0) ? sqrt(d) : 0.0;
+      const double d = A[(long)j * k + j].x;
+      s_piv = d > 0.0 ? sqrt(d) : 0.0;
     }
     __syncthreads();
     const double piv = s_piv;
-    if (piv < drop) {
+    if (!(piv >= drop) || piv == 0.0) {
       __syncthreads();
       continue;
     }
-    // R[j][l] = (G[j][l] - sum_{i kept} conj(R[i][j]) R[i][l]) / piv for l > j; R[j][j] = piv
-    for (int l = j + 1 + tid; l < k; l += nt) {
-      double2 s = G[j + (long)l * k];
-      for (int t = 0; t < nk; ++t) {
-        const int i = s_kept[t];
-        const double2 a = R[(long)i * k + j], b = R[(long)i * k + l];
-        s.x -= a.x * b.x + a.y * b.y;
-        s.y -= a.x * b.y - a.y * b.x;
-      }
-      R[(long)j * k + l] = make_double2(s.x / piv, s.y / piv);
-    }
+    const double inv = 1.0 / piv;
+    double2* rj = A + (long)j * k;
+    for (int l = j + 1 + tid; l < k; l += nt) rj[l] = make_double2(rj[l].x * inv, rj[l].y * inv);
     if (tid == 0) {
-      R[(long)j * k + j] = make_double2(piv, 0.0);
-      s_kept[nk] = j;
-      s_nk = nk + 1;
+      rj[j] = make_double2(piv, 0.0);
+      kept[s_nk] = j;
+      s_nk = s_nk + 1;
+    }
+    __syncthreads();
+    // A[l1][l2] -= conj(R[j][l1]) R[j][l2] for j < l1 <= l2 < k
+    const int n = k - j - 1;
+    for (long idx = tid; idx < (long)n * n; idx += nt) {
+      const int a1 = (int)(idx / n), a2 = (int)(idx - (long)a1 * n);
+      if (a1 > a2) continue;
+      const int l1 = j + 1 + a1, l2 = j + 1 + a2;
+      const double2 x = rj[l1], y = rj[l2];
+      double2* t = A + (long)l1 * k + l2;
+      double2 v = *t;
+      v.x -= x.x * y.x + x.y * y.y;
+      v.y -= x.x * y.y - x.y * y.x;
+      *t = v;
     }
     __syncthreads();
   }
-  const int kk = s_nk;
-  // Z[:, c] solves Rk z = e_c over the kept rows/cols (upper triangular back substitution);
-  // rows of dropped columns stay zero.
-  for (long i = tid; i < (long)k * kk; i += nt) Z[i] = make_double2(0.0, 0.0);
-  __syncthreads();
-  for (int c = tid; c < kk; c += nt) {
-    // unknowns z_t for kept index t = c down to 0
-    double2* zc = Z + (long)c * k;
-    for (int t = c; t >= 0; --t) {
-      const int i = s_kept[t];
-      double2 s = make_double2(t == c ? 1.0 : 0.0, 0.0);
-      for (int u = t + 1; u <= c; ++u) {
-        const int ju = s_kept[u];
-        const double2 r = R[(long)i * k + ju];
-        const double2 z = zc[ju];
-        s.x -= r.x * z.x - r.y * z.y;
-        s.y -= r.x * z.y + r.y * z.x;
-      }
-      const double d = R[(long)i * k + i].x;
-      zc[i] = make_double2(s.x / d, s.y / d);
-    }
-  }
-  for (int t = tid; t < kk; t += nt) kept[t] = s_kept[t];
-  if (tid == 0) *kk_out = kk;
+  if (tid == 0) *kk_out = s_nk;
 }
+
+// Z (k x k columns, ld k): column b < kk solves R_kept z = e_b on the kept rows (rows of dropped
+// columns zero), so Q Z has orthonormal columns; columns b >= kk are zeroed.  One warp per column,
+// the back substitution's dot products split over the lanes.
+__global__ void k_chol_inv(const double2* __restrict__ A, int k, const int* __restrict__ kept, const int* __restrict__ kk_p,
+                           double2* __restrict__ Z) {
+  const int lane = threadIdx.x & 31;
+  const int b = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+  if (b >= k) return;
+  const int kk = *kk_p;
+  double2* z = Z + (long)b * k;
+  for (int i = lane; i < k; i += 32) z[i] = make_double2(0.0, 0.0);
+  __syncwarp();
+  if (b >= kk) return;
+  const int kb = kept[b];
+  if (lane == 0) z[kb] = make_double2(1.0 / A[(long)kb * k + kb].x, 0.0);
+  __syncwarp();
+  for (int a = b - 1; a >= 0; --a) {
+    const int ka = kept[a];
+    const double2* ra = A + (long)ka * k;
+    double sx = 0.0, sy = 0.0;
+    for (int u = a + 1 + lane; u <= b; u += 32) {
+      const int ku = kept[u];
+      const double2 r = ra[ku], zz = z[ku];
+      sx += r.x * zz.x - r.y * zz.y;
+      sy += r.x * zz.y + r.y * zz.x;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sx += __shfl_xor_sync(0xffffffffu, sx, o);
+      sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    if (lane == 0) {
+      const double d = ra[ka].x;
+      z[ka] = make_double2(-sx / d, -sy / d);
+    }
+    __syncwarp();
+  }
+}
+
 
 // ------------------------------------------------------------------------------------------
 
@@ -363,7 +376,7 @@ struct KCtxImpl {
   double2 *V = nullptr, *W = nullptr, *ritz = nullptr, *res = nullptr, *Q = nullptr, *Q2 = nullptr;
   double2 *Tk = nullptr;  // persistent Rayleigh-Ritz matrix, leading dimension max_sub
   double2 *T = nullptr, *U = nullptr, *E = nullptr, *H = nullptr, *G = nullptr, *R = nullptr, *Z = nullptr;
-  double *evals = nullptr, *norms = nullptr, *diag = nullptr;
+  double *evals = nullptr, *norms = nullptr, *diag = nullptr, *ekin = nullptr;
   int *band = nullptr, *kept = nullptr, *status = nullptr;
   double2* ws = nullptr;
   size_t ws_elems = 0;
@@ -372,6 +385,10 @@ struct KCtxImpl {
   HeevWork hw;
   bool rr_tc = false;  // Rayleigh-Ritz products on the tensor cores (3xTF32), TF32/TF32X3 contexts
   int* err = nullptr;  // the context's tensor-core error flag
+  // pinned host mirrors of the per-iteration read-backs
+  void* pinned = nullptr;
+  double *h_ev = nullptr, *h_nr = nullptr;
+  int *h_st = nullptr, *h_kk = nullptr, *h_band = nullptr;
 };
 
 void eig_destroy(KCtxImpl* e) {
@@ -379,6 +396,7 @@ void eig_destroy(KCtxImpl* e) {
   if (e->all) cudaFree(e->all);
   if (e->ws) cudaFree(e->ws);
   if (e->heev_mem) cudaFree(e->heev_mem);
+  if (e->pinned) cudaFreeHost(e->pinned);
   delete e;
 }
 
@@ -399,6 +417,7 @@ static int eig_alloc(dftcuda_kctx* c, size_t n, size_t max_sub, size_t nb) {
   const size_t oH = take(sizeof(double2) * ms2), oG = take(sizeof(double2) * ms2), oR = take(sizeof(double2) * ms2);
   const size_t oZ = take(sizeof(double2) * ms2), oTk = take(sizeof(double2) * ms2);
   const size_t oev = take(sizeof(double) * max_sub), onr = take(sizeof(double) * nb), odg = take(sizeof(double) * n);
+  const size_t oek = take(sizeof(double) * kmax);
   const size_t obd = take(sizeof(int) * kmax), okp = take(sizeof(int) * kmax), ost = take(sizeof(int) * 4);
   if (cudaMalloc(&e->all, off) != cudaSuccess) {
     eig_destroy(e);
@@ -409,7 +428,7 @@ static int eig_alloc(dftcuda_kctx* c, size_t n, size_t max_sub, size_t nb) {
   e->V = (double2*)(b + oV); e->W = (double2*)(b + oW); e->ritz = (double2*)(b + oRi); e->res = (double2*)(b + oRe);
   e->Q = (double2*)(b + oQ); e->Q2 = (double2*)(b + oQ2); e->T = (double2*)(b + oT); e->U = (double2*)(b + oU);
   e->E = (double2*)(b + oE); e->H = (double2*)(b + oH); e->G = (double2*)(b + oG); e->R = (double2*)(b + oR);
-  e->Z = (double2*)(b + oZ); e->Tk = (double2*)(b + oTk); e->evals = (double*)(b + oev); e->norms = (double*)(b + onr); e->diag = (double*)(b + odg);
+  e->Z = (double2*)(b + oZ); e->Tk = (double2*)(b + oTk); e->evals = (double*)(b + oev); e->norms = (double*)(b + onr); e->diag = (double*)(b + odg); e->ekin = (double*)(b + oek);
   e->band = (int*)(b + obd); e->kept = (int*)(b + okp); e->status = (int*)(b + ost);
   size_t need = 0;
   const int ms = (int)max_sub;
@@ -427,6 +446,13 @@ static int eig_alloc(dftcuda_kctx* c, size_t n, size_t max_sub, size_t nb) {
   if (cudaMalloc(&e->heev_mem, heev_work_bytes(ms, (int)nb)) != cudaSuccess)
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "eig heev ws");
   heev_bind(e->hw, e->heev_mem, ms, (int)nb);
+  const size_t pin_bytes = sizeof(double) * 2 * nb + sizeof(int) * (8 + kmax);
+  if (cudaMallocHost(&e->pinned, pin_bytes) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "eig pinned host buffers");
+  e->h_ev = (double*)e->pinned;
+  e->h_nr = e->h_ev + nb;
+  e->h_st = (int*)(e->h_nr + nb);
+  e->h_kk = e->h_st + 4;
+  e->h_band = e->h_st + 8;
   return DFTCUDA_OK;
 }
 
@@ -461,32 +487,53 @@ static int combine(KCtxImpl* e, const double2* X, int mx, const double2* C, int 
 }
 
 // Orthonormalise the k vectors in Q against V[0:m] and among themselves (in order), writing the kept
-// vectors to dst.  Returns the number kept in *kk and their indices (into Q) in kept_host.
-static int block_orthonormalize(dftcuda_kctx* c, int m, double2* Q, int k, double2* dst, int* kk,
-                                std::vector<int>& kept_host, cudaStream_t s) {
-  KCtxImpl* e = c->eig;
+// vectors to dst.  Two phases around one host read of the kept count: phase A projects out V once
+// and takes the dropping Cholesky of the block's Gram matrix (kept count -> e->h_kk, pinned);
+// phase B (after the stream is synchronised) forms the kept vectors and their second CholQR pass.
+static int block_orth_a(KCtxImpl* e, int m, double2* Q, int k, cudaStream_t s) {
   if (k > 1024) return fail(DFTCUDA_ERR_UNSUPPORTED, "block_orthonormalize: more than 1024 new vectors");
-  for (int pass = 0; pass < 2 && m > 0; ++pass) {
+  // One classical projection pass here; phase B projects the kept vectors once more before their
+  // second Cholesky (classical Gram-Schmidt twice, with the drop test taken after the first pass:
+  // the first pass leaves components along V of order eps ||q||, far below the 1e-8 drop norm).
+  if (m > 0) {
     DFT_TRY(gram(e, e->V, m, Q, k, e->H, m, s));
     DFT_TRY(combine(e, e->V, m, e->H, m, k, Q, -1.0, 1.0, s));
   }
   DFT_TRY(gram(e, Q, k, Q, k, e->G, k, s));
-  k_chol_drop<<<1, 512, 0, s>>>(e->G, k, 1e-8, e->R, e->Z, e->kept, e->status + 1); count_launch();
-  int h_kk = 0;
-  DFT_CUDA_TRY(cudaMemcpyAsync(&h_kk, e->status + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  k_chol_right<<<1, 1024, 0, s>>>(e->G, k, 1e-8, e->R, e->kept, e->status + 1);
+  k_chol_inv<<<ceil_div(k, 8), 256, 0, s>>>(e->R, k, e->kept, e->status + 1, e->Z);
+  count_launch(2);
+  DFT_CUDA_TRY(cudaMemcpyAsync(e->h_kk, e->status + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  return DFTCUDA_OK;
+}
+
+static int block_orth_b(KCtxImpl* e, int m, double2* Q, int k, double2* dst, int kk, cudaStream_t s) {
+  if (kk <= 0) return DFTCUDA_OK;
+  DFT_TRY(combine(e, Q, k, e->Z, k, kk, e->Q2, 1.0, 0.0, s));
+  // second pass (CholQR2) without drops
+  if (m > 0) {
+    DFT_TRY(gram(e, e->V, m, e->Q2, kk, e->H, m, s));
+    DFT_TRY(combine(e, e->V, m, e->H, m, kk, e->Q2, -1.0, 1.0, s));
+  }
+  DFT_TRY(gram(e, e->Q2, kk, e->Q2, kk, e->G, kk, s));
+  k_chol_right<<<1, 1024, 0, s>>>(e->G, kk, 0.0, e->R, e->kept, e->status + 2);
+  k_chol_inv<<<ceil_div(kk, 8), 256, 0, s>>>(e->R, kk, e->kept, e->status + 2, e->Z);
+  count_launch(2);
+  DFT_TRY(combine(e, e->Q2, kk, e->Z, kk, kk, dst, 1.0, 0.0, s));
+  return DFTCUDA_OK;
+}
+
+// Both phases with the synchronisation in between; kept_host receives the kept indices (into Q).
+static int block_orthonormalize(dftcuda_kctx* c, int m, double2* Q, int k, double2* dst, int* kk,
+                                std::vector<int>& kept_host, cudaStream_t s) {
+  KCtxImpl* e = c->eig;
+  DFT_TRY(block_orth_a(e, m, Q, k, s));
   DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  const int h_kk = *e->h_kk;
   kept_host.assign(h_kk, 0);
   if (h_kk > 0) {
     DFT_CUDA_TRY(cudaMemcpyAsync(kept_host.data(), e->kept, sizeof(int) * h_kk, cudaMemcpyDeviceToHost, s));
-    DFT_TRY(combine(e, Q, k, e->Z, k, h_kk, e->Q2, 1.0, 0.0, s));
-    // second pass (CholQR2) without drops
-    if (m > 0) {
-      DFT_TRY(gram(e, e->V, m, e->Q2, h_kk, e->H, m, s));
-      DFT_TRY(combine(e, e->V, m, e->H, m, h_kk, e->Q2, -1.0, 1.0, s));
-    }
-    DFT_TRY(gram(e, e->Q2, h_kk, e->Q2, h_kk, e->G, h_kk, s));
-    k_chol_drop<<<1, 512, 0, s>>>(e->G, h_kk, 0.0, e->R, e->Z, e->kept, e->status + 2); count_launch();
-    DFT_TRY(combine(e, e->Q2, h_kk, e->Z, h_kk, h_kk, dst, 1.0, 0.0, s));
+    DFT_TRY(block_orth_b(e, m, Q, k, dst, h_kk, s));
     DFT_CUDA_TRY(cudaStreamSynchronize(s));
   }
   *kk = h_kk;
@@ -545,43 +592,68 @@ static int orthonormalize_all(dftcuda_kctx* c, int m, uint64_t& seed, cudaStream
 
 }  // namespace dftcuda
 
-using namespace dftcuda;
 
-extern "C" int dftcuda_eig_solve(dftcuda_kctx* c, const double* diag, size_t nbands, const dftcuda_eig_opts* opts_in,
-                                 const double* init_vecs, size_t init_cols, double* values_out, double* vectors_out,
-                                 dftcuda_eig_info* info) {
-  if (!c || !diag || (nbands && (!values_out || !vectors_out)))
-    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "eig_solve: null argument");
-  dftcuda_eig_opts opts{40, 1e-6, 0, 0, 0};
-  if (opts_in) opts = *opts_in;
+namespace dftcuda {
+
+// One k-point's Davidson run as a state machine, so that many k-points advance in lockstep on their
+// own streams with one host synchronisation per phase for all of them (the reference runs k-points
+// on worker threads, kpoint/workers.zig:133-180; here the GPU overlaps them instead).  The loop
+// body follows serial.zig:55-307:
+//   RR:      T = V^H W (new columns), small eigenproblem, Ritz vectors, residuals, norms  -> read-back
+//   DECIDE:  convergence test; candidates ||r_b|| >= tol in band order; precondition; phase A of the
+//            orthonormalisation of one chunk                                              -> read-back
+//   ORTH:    phase B; more chunks while room is left; then restart or H on the new columns.
+struct EigRun {
+  dftcuda_kctx* c = nullptr;
+  KCtxImpl* e = nullptr;
+  cudaStream_t s = nullptr;
+  size_t n = 0, nbands = 0, max_sub = 0, block = 0;
+  dftcuda_eig_opts opts{};
+  uint64_t seed = 0x6f3d3cbeULL;
+  size_t m = 0, it = 0, applies = 0, t_valid = 0;
+  bool done = false, converged = false, orth_pending = false;
+  double max_res = 0.0;
+  std::vector<int> cand;
+  size_t added = 0, next = 0, take = 0;
+  bool gram_full = false;
+  double* values_out = nullptr;
+  double* vectors_out = nullptr;
+  dftcuda_eig_info* info = nullptr;
+  int status = DFTCUDA_OK;
+};
+
+static int run_init(EigRun& r, const double* diag, const double* init_vecs, size_t init_cols) {
+  dftcuda_kctx* c = r.c;
   const size_t n = c->npw;
-  if (info) *info = dftcuda_eig_info{0, 0, 1, 0.0};
-  if (nbands == 0 || n == 0) return DFTCUDA_OK;
-  const size_t max_sub = opts.max_subspace == 0 ? std::min(n, 4 * nbands + 8)
-                                                : std::min(n, std::max(opts.max_subspace, nbands));
-  const size_t block = opts.block_size == 0 ? std::min(max_sub, nbands + 4)
-                                            : std::min(max_sub, std::max(opts.block_size, nbands));
-  if (nbands > max_sub) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "eig_solve: nbands exceeds the basis size");
-  if (max_sub > 2048) return fail(DFTCUDA_ERR_UNSUPPORTED, "eig_solve: max_subspace above 2048");
-  cudaStream_t s = c->stream;
-  DFT_TRY(eig_alloc(c, n, max_sub, nbands));
-  KCtxImpl* e = c->eig;
+  r.n = n;
+  if (r.info) *r.info = dftcuda_eig_info{0, 0, 1, 0.0};
+  if (r.nbands == 0 || n == 0) {
+    r.done = true;
+    r.converged = true;
+    return DFTCUDA_OK;
+  }
+  const dftcuda_eig_opts& opts = r.opts;
+  r.max_sub = opts.max_subspace == 0 ? std::min(n, 4 * r.nbands + 8) : std::min(n, std::max(opts.max_subspace, r.nbands));
+  r.block = opts.block_size == 0 ? std::min(r.max_sub, r.nbands + 4) : std::min(r.max_sub, std::max(opts.block_size, r.nbands));
+  if (r.nbands > r.max_sub) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "eig_solve: nbands exceeds the basis size");
+  if (r.max_sub > 2048) return fail(DFTCUDA_ERR_UNSUPPORTED, "eig_solve: max_subspace above 2048");
+  r.s = c->stream;
+  cudaStream_t s = r.s;
+  DFT_TRY(eig_alloc(c, n, r.max_sub, r.nbands));
+  KCtxImpl* e = r.e = c->eig;
   e->rr_tc = precision_uses_tc(c->precision);
   if (e->rr_tc && !c->d_err) {
     DFT_CUDA_TRY(cudaMalloc(&c->d_err, sizeof(int)));
-    DFT_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    DFT_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
   }
   e->err = c->d_err;
-  const long ln = (long)n;
-  // diagonal
-  if (is_device_pointer(diag))
-    DFT_CUDA_TRY(cudaMemcpyAsync(e->diag, diag, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-  else
-    DFT_CUDA_TRY(cudaMemcpyAsync(e->diag, diag, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-  uint64_t seed = 0x6f3d3cbeULL;
-  size_t m = block;
+  const char* gram_mode = std::getenv("DFTCUDA_GRAM");
+  r.gram_full = gram_mode && std::strcmp(gram_mode, "full") == 0;
+  DFT_CUDA_TRY(cudaMemcpyAsync(e->diag, diag, sizeof(double) * n,
+                               is_device_pointer(diag) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  const size_t m = r.block;
   size_t icols = 0;
-  if (init_vecs) icols = std::min(m, init_cols == 0 ? nbands : init_cols);
+  if (init_vecs) icols = std::min(m, init_cols == 0 ? r.nbands : init_cols);
   if (opts.init_diagonal) {
     std::vector<double> hd(n);
     DFT_CUDA_TRY(cudaMemcpyAsync(hd.data(), e->diag, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
@@ -595,108 +667,237 @@ extern "C" int dftcuda_eig_solve(dftcuda_kctx* c, const double* diag, size_t nba
       DFT_CUDA_TRY(cudaMemcpyAsync(e->V + col * n + order[col], &one, sizeof(double2), cudaMemcpyHostToDevice, s));
     DFT_CUDA_TRY(cudaStreamSynchronize(s));
   } else {
-    k_lcg_fill<<<ceil_div(n * m, 256), 256, 0, s>>>(e->V, (long)(n * m), seed); count_launch();
+    k_lcg_fill<<<ceil_div(n * m, 256), 256, 0, s>>>(e->V, (long)(n * m), r.seed); count_launch();
     uint64_t A, C;
     lcg_jump(2 * (uint64_t)(n * m), A, C);
-    seed = A * seed + C;
+    r.seed = A * r.seed + C;
   }
   if (icols) {
-    const bool dv = is_device_pointer(init_vecs);
     DFT_CUDA_TRY(cudaMemcpyAsync(e->V, init_vecs, sizeof(double2) * n * icols,
-                                 dv ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+                                 is_device_pointer(init_vecs) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
   }
-  DFT_TRY(orthonormalize_all(c, (int)m, seed, s));
+  DFT_TRY(orthonormalize_all(c, (int)m, r.seed, s));
   DFT_TRY(kctx_apply_h_dev(c, e->V, e->W, m, s));
-  size_t applies = m;
-  std::vector<double> h_ev(nbands), h_nr(nbands);
-  std::vector<int> cand;
-  size_t it = 0;
-  bool converged = false;
-  double max_res = 0.0;
-  // Columns of the Rayleigh-Ritz matrix still valid for the current V, W: only products with the
-  // columns added since the last iteration are formed (8 n m added flops instead of the full
-  // rebuild's 8 n m^2, serial.zig:170).  DFTCUDA_GRAM=full rebuilds every iteration.
-  const char* gram_mode = std::getenv("DFTCUDA_GRAM");
-  const bool gram_full = gram_mode && std::strcmp(gram_mode, "full") == 0;
-  size_t t_valid = 0;
-  const long ldt = (long)max_sub;
-  for (; it < opts.max_iter; ++it) {
-    const int mi = (int)m;
-    ProfScope ps_sub(c, P_SUBSPACE, s);
-    const int m_old = gram_full ? 0 : (int)t_valid;
-    DFT_TRY(gram(e, e->V, mi, e->W + (size_t)m_old * n, mi - m_old, e->Tk + (size_t)m_old * ldt, (int)ldt, s, true));
-    k_gram_finish<<<ceil_div((size_t)mi * mi, 256), 256, 0, s>>>(e->Tk, ldt, m_old, mi, e->T); count_launch();
-    k_gram_store<<<ceil_div((size_t)mi * mi, 256), 256, 0, s>>>(e->T, mi, e->Tk, ldt); count_launch();
-    t_valid = m;
-    DFT_TRY(small_eig(e, mi, (int)nbands, s));
-    DFT_TRY(combine(e, e->V, mi, e->E, mi, (int)nbands, e->ritz, 1.0, 0.0, s, true));
-    DFT_TRY(combine(e, e->W, mi, e->E, mi, (int)nbands, e->res, 1.0, 0.0, s, true));
-    k_residual<<<(unsigned)nbands, 256, 0, s>>>(e->res, e->ritz, e->evals, ln, e->norms); count_launch();
-    int jst = 0;
-    DFT_CUDA_TRY(cudaMemcpyAsync(h_ev.data(), e->evals, sizeof(double) * nbands, cudaMemcpyDeviceToHost, s));
-    DFT_CUDA_TRY(cudaMemcpyAsync(h_nr.data(), e->norms, sizeof(double) * nbands, cudaMemcpyDeviceToHost, s));
-    DFT_CUDA_TRY(cudaMemcpyAsync(&jst, e->status, sizeof(int), cudaMemcpyDeviceToHost, s));
-    DFT_CUDA_TRY(cudaStreamSynchronize(s));
-    if (jst != 0) return fail(DFTCUDA_ERR_EIGENSOLVER_FAILURE, "eig_solve: subspace eigensolver failed (Jacobi not converged or barrier timeout)");
-    max_res = 0.0;
-    for (size_t b = 0; b < nbands; ++b) max_res = std::max(max_res, h_nr[b]);
-    if (max_res < opts.tol) {
-      converged = true;
-      ++it;
-      break;
-    }
-    // Candidates in band order with ||r_b|| >= tol (serial.zig:242-264).
-    cand.clear();
-    for (size_t b = 0; b < nbands; ++b)
-      if (!(h_nr[b] < opts.tol)) cand.push_back((int)b);
-    size_t added = 0, next = 0;
-    while (m + added < max_sub && next < cand.size()) {
-      const size_t take = std::min(max_sub - (m + added), cand.size() - next);
-      DFT_CUDA_TRY(cudaMemcpyAsync(e->band, cand.data() + next, sizeof(int) * take, cudaMemcpyHostToDevice, s));
-      k_precondition<<<ceil_div(take * n, 256), 256, 0, s>>>(e->Q, e->res, e->diag, e->evals, e->band, (int)take, ln); count_launch();
-      // Orthonormalise against V[0:m+added]; the kept vectors land at V[m+added ...].
-      int kk = 0;
-      std::vector<int> kept;
-      DFT_TRY(block_orthonormalize(c, (int)(m + added), e->Q, (int)take, e->V + (m + added) * n, &kk, kept, s));
-      added += kk;
-      next += take;
-    }
-    if (added == 0) {
-      converged = true;
-      ++it;
-      break;
-    }
-    if (m + added >= max_sub) {
-      // Restart (serial.zig:285-293).  The reference also applies H to the vectors it is about to
-      // discard; that product is never read, so it is skipped here.
-      ps_sub.stop();
-      DFT_CUDA_TRY(cudaMemcpyAsync(e->V, e->ritz, sizeof(double2) * n * nbands, cudaMemcpyDeviceToDevice, s));
-      m = nbands;
-      t_valid = 0;
-      DFT_TRY(orthonormalize_all(c, (int)m, seed, s));
-      DFT_TRY(kctx_apply_h_dev(c, e->V, e->W, m, s));
-      applies += m;
-      continue;
-    }
-    ps_sub.stop();
-    DFT_TRY(kctx_apply_h_dev(c, e->V + m * n, e->W + m * n, added, s));
-    applies += added;
-    m += added;
+  r.applies = m;
+  r.m = m;
+  return DFTCUDA_OK;
+}
+
+// RR phase: everything up to the read-back of eigenvalues, residual norms and the solver status.
+static int run_rr(EigRun& r) {
+  KCtxImpl* e = r.e;
+  cudaStream_t s = r.s;
+  const size_t n = r.n;
+  const int mi = (int)r.m;
+  ProfScope ps_sub(r.c, P_SUBSPACE, s);
+  const int m_old = r.gram_full ? 0 : (int)r.t_valid;
+  const long ldt = (long)r.max_sub;
+  DFT_TRY(gram(e, e->V, mi, e->W + (size_t)m_old * n, mi - m_old, e->Tk + (size_t)m_old * ldt, (int)ldt, s, true));
+  k_gram_finish<<<ceil_div((size_t)mi * mi, 256), 256, 0, s>>>(e->Tk, ldt, m_old, mi, e->T); count_launch();
+  k_gram_store<<<ceil_div((size_t)mi * mi, 256), 256, 0, s>>>(e->T, mi, e->Tk, ldt); count_launch();
+  r.t_valid = r.m;
+  DFT_TRY(small_eig(e, mi, (int)r.nbands, s));
+  DFT_TRY(combine(e, e->V, mi, e->E, mi, (int)r.nbands, e->ritz, 1.0, 0.0, s, true));
+  DFT_TRY(combine(e, e->W, mi, e->E, mi, (int)r.nbands, e->res, 1.0, 0.0, s, true));
+  k_residual<<<(unsigned)r.nbands, 256, 0, s>>>(e->res, e->ritz, e->evals, (long)n, e->norms); count_launch();
+  DFT_CUDA_TRY(cudaMemcpyAsync(e->h_ev, e->evals, sizeof(double) * r.nbands, cudaMemcpyDeviceToHost, s));
+  DFT_CUDA_TRY(cudaMemcpyAsync(e->h_nr, e->norms, sizeof(double) * r.nbands, cudaMemcpyDeviceToHost, s));
+  DFT_CUDA_TRY(cudaMemcpyAsync(e->h_st, e->status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  return DFTCUDA_OK;
+}
+
+// Precondition the next chunk of candidates and launch phase A of its orthonormalisation.
+static int run_orth_a(EigRun& r) {
+  KCtxImpl* e = r.e;
+  cudaStream_t s = r.s;
+  r.take = std::min(r.max_sub - (r.m + r.added), r.cand.size() - r.next);
+  std::memcpy(e->h_band, r.cand.data() + r.next, sizeof(int) * r.take);
+  DFT_CUDA_TRY(cudaMemcpyAsync(e->band, e->h_band, sizeof(int) * r.take, cudaMemcpyHostToDevice, s));
+  ProfScope ps_sub(r.c, P_SUBSPACE, s);
+  DFT_TRY(precondition_launch(r.c, e->Q, e->res, e->diag, e->evals, e->norms, e->ritz, e->band, (int)r.take, (long)r.n,
+                              (double)r.it, e->ekin, s));
+  DFT_TRY(block_orth_a(e, (int)(r.m + r.added), e->Q, (int)r.take, s));
+  r.orth_pending = true;
+  return DFTCUDA_OK;
+}
+
+// After the RR read-back: convergence and candidate selection (serial.zig:228-264).
+static int run_decide(EigRun& r) {
+  KCtxImpl* e = r.e;
+  if (*e->h_st != 0)
+    return fail(DFTCUDA_ERR_EIGENSOLVER_FAILURE, "eig_solve: subspace eigensolver failed (Jacobi not converged or barrier timeout)");
+  r.max_res = 0.0;
+  for (size_t b = 0; b < r.nbands; ++b) r.max_res = std::max(r.max_res, e->h_nr[b]);
+  if (r.max_res < r.opts.tol) {
+    r.converged = true;
+    r.done = true;
+    ++r.it;
+    return DFTCUDA_OK;
   }
-  // values: last eigenvalues; vectors: last Ritz vectors (serial.zig:298-306)
-  if (is_device_pointer(values_out))
-    DFT_CUDA_TRY(cudaMemcpyAsync(values_out, e->evals, sizeof(double) * nbands, cudaMemcpyDeviceToDevice, s));
+  r.cand.clear();
+  for (size_t b = 0; b < r.nbands; ++b)
+    if (!(e->h_nr[b] < r.opts.tol)) r.cand.push_back((int)b);
+  r.added = 0;
+  r.next = 0;
+  if (r.m + r.added < r.max_sub && r.next < r.cand.size()) return run_orth_a(r);
+  return DFTCUDA_OK;
+}
+
+// After the phase-A read-back: finish the chunk; either another chunk, or the end of the iteration
+// (no vector added: converged; subspace full: restart; else H on the new columns).
+static int run_orth_b(EigRun& r) {
+  KCtxImpl* e = r.e;
+  cudaStream_t s = r.s;
+  r.orth_pending = false;
+  const int kk = *e->h_kk;
+  {
+    ProfScope ps_sub(r.c, P_SUBSPACE, s);
+    DFT_TRY(block_orth_b(e, (int)(r.m + r.added), e->Q, (int)r.take, e->V + (r.m + r.added) * r.n, kk, s));
+  }
+  r.added += (size_t)std::max(kk, 0);
+  r.next += r.take;
+  if (r.m + r.added < r.max_sub && r.next < r.cand.size()) return run_orth_a(r);
+  if (r.added == 0) {
+    r.converged = true;
+    r.done = true;
+    ++r.it;
+    return DFTCUDA_OK;
+  }
+  if (r.m + r.added >= r.max_sub) {
+    // Restart (serial.zig:285-293).  The reference also applies H to the vectors it is about to
+    // discard; that product is never read, so it is skipped here.
+    DFT_CUDA_TRY(cudaMemcpyAsync(e->V, e->ritz, sizeof(double2) * r.n * r.nbands, cudaMemcpyDeviceToDevice, s));
+    r.m = r.nbands;
+    r.t_valid = 0;
+    DFT_TRY(orthonormalize_all(r.c, (int)r.m, r.seed, s));
+    DFT_TRY(kctx_apply_h_dev(r.c, e->V, e->W, r.m, s));
+    r.applies += r.m;
+  } else {
+    DFT_TRY(kctx_apply_h_dev(r.c, e->V + r.m * r.n, e->W + r.m * r.n, r.added, s));
+    r.applies += r.added;
+    r.m += r.added;
+  }
+  ++r.it;
+  return DFTCUDA_OK;
+}
+
+// values: last eigenvalues; vectors: last Ritz vectors (serial.zig:298-306).
+static int run_finish(EigRun& r) {
+  if (r.nbands == 0 || r.n == 0) return DFTCUDA_OK;
+  KCtxImpl* e = r.e;
+  cudaStream_t s = r.s;
+  if (is_device_pointer(r.values_out))
+    DFT_CUDA_TRY(cudaMemcpyAsync(r.values_out, e->evals, sizeof(double) * r.nbands, cudaMemcpyDeviceToDevice, s));
   else
-    std::memcpy(values_out, h_ev.data(), sizeof(double) * nbands);
-  DFT_CUDA_TRY(cudaMemcpyAsync(vectors_out, e->ritz, sizeof(double2) * n * nbands,
-                               is_device_pointer(vectors_out) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    std::memcpy(r.values_out, e->h_ev, sizeof(double) * r.nbands);
+  DFT_CUDA_TRY(cudaMemcpyAsync(r.vectors_out, e->ritz, sizeof(double2) * r.n * r.nbands,
+                               is_device_pointer(r.vectors_out) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
   DFT_CUDA_TRY(cudaStreamSynchronize(s));
-  DFT_TRY(kctx_check_error(c));
-  if (info) {
-    info->iterations = it;
-    info->h_applies = applies;
-    info->converged = converged ? 1 : 0;
-    info->max_residual = max_res;
+  DFT_TRY(kctx_check_error(r.c));
+  if (r.info) {
+    r.info->iterations = r.it;
+    r.info->h_applies = r.applies;
+    r.info->converged = r.converged ? 1 : 0;
+    r.info->max_residual = r.max_res;
   }
   return DFTCUDA_OK;
+}
+
+static int sync_runs(std::vector<EigRun>& runs, bool only_pending) {
+  for (EigRun& r : runs) {
+    if (r.done || r.status != DFTCUDA_OK) continue;
+    if (only_pending && !r.orth_pending) continue;
+    const cudaError_t ce = cudaStreamSynchronize(r.s);
+    if (ce != cudaSuccess) r.status = fail(DFTCUDA_ERR_CUDA, std::string("eig_solve: ") + cudaGetErrorString(ce));
+  }
+  return DFTCUDA_OK;
+}
+
+// Lockstep driver: every active run does RR; one synchronisation; every run decides (and launches
+// phase A of a chunk); one synchronisation; phase B for those with a chunk (repeated while chunks
+// remain); loop.
+static int eig_solve_runs(std::vector<EigRun>& runs, const std::vector<const double*>& diags,
+                          const std::vector<const double*>& inits, const std::vector<size_t>& icols) {
+  for (size_t i = 0; i < runs.size(); ++i) {
+    runs[i].status = run_init(runs[i], diags[i], inits[i], icols[i]);
+    if (runs[i].status != DFTCUDA_OK) runs[i].done = true;
+  }
+  for (;;) {
+    bool any = false;
+    for (EigRun& r : runs) {
+      if (r.done || r.status != DFTCUDA_OK) continue;
+      if (r.it >= r.opts.max_iter) {
+        r.done = true;
+        continue;
+      }
+      r.status = run_rr(r);
+      any = true;
+    }
+    if (!any) break;
+    sync_runs(runs, false);
+    for (EigRun& r : runs) {
+      if (r.done || r.status != DFTCUDA_OK) continue;
+      r.status = run_decide(r);
+    }
+    for (;;) {
+      bool pend = false;
+      for (EigRun& r : runs) pend |= (!r.done && r.status == DFTCUDA_OK && r.orth_pending);
+      if (!pend) break;
+      sync_runs(runs, true);
+      for (EigRun& r : runs) {
+        if (r.done || r.status != DFTCUDA_OK || !r.orth_pending) continue;
+        r.status = run_orth_b(r);
+      }
+    }
+  }
+  int first = DFTCUDA_OK;
+  for (EigRun& r : runs) {
+    if (r.status == DFTCUDA_OK) r.status = run_finish(r);
+    if (first == DFTCUDA_OK && r.status != DFTCUDA_OK) first = r.status;
+  }
+  return first;
+}
+
+}  // namespace dftcuda
+
+using namespace dftcuda;
+
+extern "C" int dftcuda_eig_solve(dftcuda_kctx* c, const double* diag, size_t nbands, const dftcuda_eig_opts* opts_in,
+                                 const double* init_vecs, size_t init_cols, double* values_out, double* vectors_out,
+                                 dftcuda_eig_info* info) {
+  return dftcuda_eig_solve_batch(1, &c, &diag, nbands, opts_in, init_vecs ? &init_vecs : nullptr,
+                                 init_vecs ? &init_cols : nullptr, &values_out, &vectors_out, info);
+}
+
+extern "C" int dftcuda_eig_solve_batch(size_t nk, dftcuda_kctx* const* ctxs, const double* const* diags, size_t nbands,
+                                       const dftcuda_eig_opts* opts_in, const double* const* init_vecs,
+                                       const size_t* init_cols, double* const* values_out, double* const* vectors_out,
+                                       dftcuda_eig_info* infos) {
+  if (nk == 0) return DFTCUDA_OK;
+  if (!ctxs || !diags || (nbands && (!values_out || !vectors_out)))
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "eig_solve: null argument");
+  dftcuda_eig_opts opts{40, 1e-6, 0, 0, 0};
+  if (opts_in) opts = *opts_in;
+  std::vector<EigRun> runs(nk);
+  std::vector<const double*> dg(nk), iv(nk, nullptr);
+  std::vector<size_t> ic(nk, 0);
+  for (size_t i = 0; i < nk; ++i) {
+    if (!ctxs[i] || !diags[i] || (nbands && (!values_out[i] || !vectors_out[i])))
+      return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "eig_solve: null argument");
+    for (size_t j = 0; j < i; ++j)
+      if (ctxs[j] == ctxs[i]) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "eig_solve_batch: a context appears twice");
+    EigRun& r = runs[i];
+    r.c = ctxs[i];
+    r.nbands = nbands;
+    r.opts = opts;
+    r.values_out = values_out[i];
+    r.vectors_out = vectors_out[i];
+    r.info = infos ? infos + i : nullptr;
+    dg[i] = diags[i];
+    if (init_vecs) {
+      iv[i] = init_vecs[i];
+      ic[i] = init_cols ? init_cols[i] : 0;
+    }
+  }
+  return eig_solve_runs(runs, dg, iv, ic);
 }

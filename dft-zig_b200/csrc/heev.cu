@@ -27,6 +27,7 @@ constexpr int BS_WARPS = 8;                  // bisection: eigenvalues per block
 constexpr int BT_WARPS = 4;                  // back-transformation: eigenvectors per block
 constexpr long kBarrierSpin = 1L << 24;      // polls (with 64 ns sleeps) before a barrier gives up
 constexpr double kGroupTol = 1e-5;           // eigenvalue grouping, relative to ||T||
+constexpr int kHtMaxSplit = 8;               // warps per trailing column (row chunks)
 
 struct GridBarrier {
   unsigned* count;
@@ -94,7 +95,7 @@ __device__ double2 block_sum2(double2 v, double2* red) {
 // Step 1.  A: m x m Hermitian, column-major, both triangles.  Column k of the result holds the
 // reflector v_k below the subdiagonal (v_k[0] = 1 implied at row k+1); d, e: T's diagonal and
 // (real) subdiagonal; tau[k]: H_k = I - tau_k v_k v_k^H with H_k^H A[k+1:, k] = e_k e_1.
-// Warp gw of the grid owns the columns r = gw (mod warps) of the trailing matrix.
+// The grid's warps cover the (column, row chunk) pairs of the trailing matrix.
 __global__ void __launch_bounds__(HT_THREADS) k_hetrd(double2* __restrict__ A, int m, double* __restrict__ dd,
                                                       double* __restrict__ ee, double2* __restrict__ tau,
                                                       double2* __restrict__ y, GridBarrier bar) {
@@ -136,41 +137,52 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd(double2* __restrict__ A, i
       tau[k] = t;
     }
     __syncthreads();
-    // Phase B: y_r = tau (A22 v)_r = tau sum_c conj(A[c, r]) v_c, one warp per column r.
+    // Warps per column: S of them split the rows of each trailing column, so a step takes about
+    // n1 / (32 S) dependent loads per lane; every block derives the same S.
+    const int S = max(1, min(kHtMaxSplit, W / max(n1, 1)));
+    const int chunk = (n1 + S - 1) / S;
+    // Phase B: partial sums of (A22 v)_r = sum_c conj(A[c, r]) v_c over the rows of one chunk;
+    // ypart[s][r] for chunk s (tau is applied in phase C).
     if (active) {
-      for (int r = gw; r < m; r += W) {
-        if (r <= k) continue;
+      for (int g = gw; g < n1 * S; g += W) {
+        const int c = g / S, sidx = g - c * S;
+        const int r = k + 1 + c;
+        const int i0 = sidx * chunk, i1 = min(n1, i0 + chunk);
         const double2* ac = A + (long)r * m + (k + 1);
         double sx = 0.0, sy = 0.0;
-        for (int i = lane; i < n1; i += 32) {
+        for (int i = i0 + lane; i < i1; i += 32) {
           const double2 a = __ldcg(ac + i), v = sv[i];
           sx += a.x * v.x + a.y * v.y;  // conj(a) v
           sy += a.x * v.y - a.y * v.x;
         }
         sx = warp_sum(sx);
         sy = warp_sum(sy);
-        if (lane == 0) y[r] = cmul(t, make_double2(sx, sy));
+        if (lane == 0) y[(long)sidx * m + r] = make_double2(sx, sy);
       }
     }
     if (!grid_sync(bar)) return;
-    // Phase C: w = y + alpha v with alpha = -tau (y^H v) / 2; A22 -= v w^H + w v^H.
+    // Phase C: y = tau A22 v; w = y + alpha v with alpha = -tau (y^H v) / 2; A22 -= v w^H + w v^H.
     if (active) {
       double2 p2 = make_double2(0.0, 0.0);
       for (int i = tid; i < n1; i += HT_THREADS) {
-        const double2 yi = __ldcg(y + k + 1 + i), vi = sv[i];
+        double2 acc = make_double2(0.0, 0.0);
+        for (int q = 0; q < S; ++q) acc = cadd(acc, __ldcg(y + (long)q * m + k + 1 + i));
+        const double2 yi = cmul(t, acc), vi = sv[i];
         sw[i] = yi;
         p2.x += yi.x * vi.x + yi.y * vi.y;
         p2.y += yi.x * vi.y - yi.y * vi.x;
       }
-      const double2 s = block_sum2(p2, red);
-      const double2 al = cscale(cmul(t, s), -0.5);
+      const double2 sdot = block_sum2(p2, red);
+      const double2 al = cscale(cmul(t, sdot), -0.5);
       for (int i = tid; i < n1; i += HT_THREADS) sw[i] = cadd(sw[i], cmul(al, sv[i]));
       __syncthreads();
-      for (int r = gw; r < m; r += W) {
-        if (r <= k) continue;
-        const double2 wr = cconj(sw[r - k - 1]), vr = cconj(sv[r - k - 1]);
+      for (int g = gw; g < n1 * S; g += W) {
+        const int c = g / S, sidx = g - c * S;
+        const int r = k + 1 + c;
+        const int i0 = sidx * chunk, i1 = min(n1, i0 + chunk);
+        const double2 wr = cconj(sw[c]), vr = cconj(sv[c]);
         double2* ac = A + (long)r * m + (k + 1);
-        for (int i = lane; i < n1; i += 32) {
+        for (int i = i0 + lane; i < i1; i += 32) {
           double2 a = __ldcg(ac + i);
           a = csub(a, cadd(cmul(sv[i], wr), cmul(sw[i], vr)));
           ac[i] = a;
@@ -412,7 +424,7 @@ __global__ void k_upper_to_full(const double2* __restrict__ src, long lds, doubl
 
 size_t heev_work_bytes(int m, int nev) {
   const size_t mm = (size_t)m;
-  return 256 * 8 + sizeof(double) * (3 * mm + 1) + sizeof(double2) * 2 * mm + sizeof(double) * mm * nev +
+  return 256 * 8 + sizeof(double) * (3 * mm + 1) + sizeof(double2) * (1 + kHtMaxSplit) * mm + sizeof(double) * mm * nev +
          sizeof(double) * 5 * mm * nev;
 }
 
@@ -425,7 +437,7 @@ void heev_bind(HeevWork& w, void* base, int m, int nev) {
   w.e = (double*)take(sizeof(double) * m);
   w.tnorm = (double*)take(sizeof(double));
   w.tau = (double2*)take(sizeof(double2) * m);
-  w.y = (double2*)take(sizeof(double2) * m);
+  w.y = (double2*)take(sizeof(double2) * m * kHtMaxSplit);
   w.z = (double*)take(sizeof(double) * (size_t)m * nev);
   w.lu = (double*)take(sizeof(double) * 5 * (size_t)m * nev);
   w.m_cap = m;
@@ -454,7 +466,8 @@ int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde,
   DFT_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), s));
   if (m > 1) {
     GridBarrier bar{w.bar, w.bar + 1, status, 0};
-    const int want = (m + HT_WARPS - 1) / HT_WARPS;
+    // enough warps for kHtMaxSplit per column at the start, at most one block per SM
+    const int want = (m * kHtMaxSplit + HT_WARPS - 1) / HT_WARPS;
     bar.nblocks = (unsigned)std::max(1, std::min(want, n_sm * std::min(per_sm, 1)));
     double2* a_ = A;
     int m_ = m;

@@ -318,6 +318,9 @@ int kctx_ensure_coef(dftcuda_kctx* c, size_t cols) {
       DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
     }
   }
+  // forced split counts (autotuner) need their partial sums
+  need = std::max(need, (size_t)std::max(c->split_proj, 0) * c->nl.nproj * cols);
+  need = std::max(need, (size_t)std::min(std::max(c->split_back, 0), std::max(1, c->nl.nproj / 32)) * cols * c->npw);
   if (need > c->gemm_ws_elems) {
     if (c->d_gemm_ws) cudaFree(c->d_gemm_ws);
     c->d_gemm_ws = nullptr;
@@ -336,6 +339,7 @@ int kctx_project(dftcuda_kctx* c, const double2* x, size_t ncols, cudaStream_t s
   g.B = x; g.ldb = (long)c->npw; g.b_kc = true; g.conj_b = false;
   g.O = c->d_coef; g.ldo_r = (long)ncols; g.ldo_c = 1;
   g.alpha = 1.0; g.beta = 0.0;
+  g.splits = c->split_proj;
   if (precision_uses_tc(c->precision))
     return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err, c->precision == DFTCUDA_PRECISION_TF32X3);
   return zgemm(g, s, c->d_gemm_ws, c->gemm_ws_elems);
@@ -360,6 +364,7 @@ static int nonlocal_block(dftcuda_kctx* c, const double2* x, double2* y, size_t 
   g.B = c->nl.P; g.ldb = (long)c->npw; g.b_kc = false; g.conj_b = true;
   g.O = y; g.ldo_r = (long)c->npw; g.ldo_c = 1;
   g.alpha = 1.0 / c->volume; g.beta = 1.0;
+  g.splits = c->split_back;
   if (precision_uses_tc(c->precision))
     return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err, c->precision == DFTCUDA_PRECISION_TF32X3);
   return zgemm(g, s, c->d_gemm_ws, c->gemm_ws_elems);
@@ -379,12 +384,12 @@ int kctx_apply_h_dev(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols
     const double2* xc = x + c0 * c->npw;
     double2* yc = y + c0 * c->npw;
     if (c->precision != DFTCUDA_PRECISION_FP64) {
-      if (c->fast32)
+      if (c->fast32 && !c->fft_generic)
         DFT_TRY(local_block4<float>(c, xc, yc, nc, s));
       else
         DFT_TRY(local_block<float>(c, xc, yc, nc, s));
     } else {
-      if (c->fast64)
+      if (c->fast64 && !c->fft_generic)
         DFT_TRY(local_block4<double>(c, xc, yc, nc, s));
       else
         DFT_TRY(local_block<double>(c, xc, yc, nc, s));
@@ -426,12 +431,12 @@ int kctx_density_dev(dftcuda_kctx* c, const double2* vecs, size_t nbands, const 
   for (size_t c0 = 0; c0 < nbands; c0 += ch) {
     const size_t nc = std::min(ch, nbands - c0);
     if (c->precision != DFTCUDA_PRECISION_FP64) {
-      if (c->fast32)
+      if (c->fast32 && !c->fft_generic)
         DFT_TRY(density_block4<float>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
       else
         DFT_TRY(density_block<float>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
     } else {
-      if (c->fast64)
+      if (c->fast64 && !c->fft_generic)
         DFT_TRY(density_block4<double>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
       else
         DFT_TRY(density_block<double>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
@@ -490,7 +495,7 @@ extern "C" int dftcuda_kctx_destroy(dftcuda_kctx* c) {
   void* ptrs[] = {c->d_plane_off, c->d_pw_idx, c->d_pw_spos, c->d_slot_xpos, c->d_kinetic, c->d_gcart, c->d_vt,
                   c->d_vt32, c->d_box, c->d_coef, c->d_coef2, c->d_gemm_ws, c->d_x, c->d_y, c->d_rho, c->d_w,
                   c->d_pwmap, c->d_stick_off, c->d_stick_y, c->d_slot_of_x, c->d_tw4x64, c->d_tw4x32,
-                  c->d_tw4p64, c->d_tw4p32, c->d_err};
+                  c->d_tw4p64, c->d_tw4p32, c->d_err, c->d_mlp, c->d_vstage};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   c->fx.destroy(); c->fy.destroy(); c->fz.destroy();
@@ -601,15 +606,14 @@ extern "C" size_t dftcuda_kctx_npw(const dftcuda_kctx* c) { return c ? c->npw : 
 
 extern "C" int dftcuda_set_vloc(dftcuda_kctx* c, const double* v) {
   if (!c || !v) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_vloc: null argument");
-  double* dv = nullptr;
   const bool dev = is_device_pointer(v);
-  if (!dev) {
-    if (cudaMalloc(&dv, sizeof(double) * c->N) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_vloc staging");
-    DFT_CUDA_TRY(cudaMemcpyAsync(dv, v, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
-  }
-  k_transpose_vloc<<<ceil_div(c->N, 256), 256, 0, c->stream>>>(dev ? v : dv, c->d_vt, c->d_vt32, c->nx, c->ny, c->nz); count_launch();
+  // A staging buffer kept in the context: cudaFree would synchronise the whole device (every other
+  // k-point's stream) on each SCF iteration.
+  if (!dev && !c->d_vstage && cudaMalloc(&c->d_vstage, sizeof(double) * c->N) != cudaSuccess)
+    return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_vloc staging");
+  if (!dev) DFT_CUDA_TRY(cudaMemcpyAsync(c->d_vstage, v, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+  k_transpose_vloc<<<ceil_div(c->N, 256), 256, 0, c->stream>>>(dev ? v : c->d_vstage, c->d_vt, c->d_vt32, c->nx, c->ny, c->nz); count_launch();
   cudaError_t e = cudaStreamSynchronize(c->stream);
-  if (dv) cudaFree(dv);
   if (e != cudaSuccess) return fail(DFTCUDA_ERR_CUDA, std::string("set_vloc: ") + cudaGetErrorString(e));
   c->has_vloc = true;
   return DFTCUDA_OK;

@@ -17,6 +17,7 @@ struct GemmArgs {
   const double2* B; long ldb; bool b_kc; bool conj_b;
   double2* O; long ldo_r; long ldo_c;
   double alpha, beta;
+  int splits = 0;  // split-K count; 0 = the kernel's wave-filling heuristic
 };
 int zgemm(const GemmArgs& g, cudaStream_t s, double2* workspace, size_t workspace_elems);
 size_t zgemm_workspace_elems(int M, int N, int K);
@@ -79,6 +80,11 @@ struct dftcuda_kctx {
 
   // Four-step path tables (local4.cu): used when fast64 / fast32 is set for the precision.
   bool fast64 = false, fast32 = false;
+  bool fft_generic = false;  // autotuner choice: the generic shared-memory FFT passes even where the four-step path exists
+  int split_proj = 0, split_back = 0;  // autotuner choices for the projector GEMMs (0 = heuristic)
+  int precond_kind = 0;                // DFTCUDA_PRECOND_* of the Davidson correction step
+  float* d_mlp = nullptr;              // learned preconditioner weights (DFTCUDA_PRECOND_MLP_PARAMS)
+  double* d_vstage = nullptr;          // host V(r) staging (N doubles)
   int* d_pwmap = nullptr;      // [n_act][nz][ny] plane-wave index or -1
   int* d_stick_off = nullptr;  // [n_act+1]
   int* d_stick_y = nullptr;    // y of each stick, per slot, ascending
@@ -130,6 +136,12 @@ int kctx_check_error(dftcuda_kctx* c);
 int kctx_density_dev(dftcuda_kctx* c, const double2* vecs, size_t nbands, const double* w_dev, double* rho_dev,
                      cudaStream_t s);
 void eig_destroy(KCtxImpl* e);
+
+// Davidson correction step q_b = P(r_b) for the chosen preconditioner (learned.cu).  ekin_ws: take
+// doubles of scratch; t: the Davidson iteration index (an input of the learned preconditioner).
+int precondition_launch(dftcuda_kctx* c, double2* Q, const double2* res, const double* kin, const double* lam,
+                        const double* norms, const double2* ritz, const int* band, int take, long n, double t,
+                        double* ekin_ws, cudaStream_t s);
 
 // Hermitian eigensolver for the subspace problem (heev.cu): the nev lowest eigenpairs of an m x m
 // Hermitian matrix (both triangles, column-major, destroyed), m <= 2048.

@@ -1,0 +1,461 @@
+// Preconditioners for the Davidson correction step (the reference's is common.zig:214-226) and the
+// training kernels of the learned one.
+//
+//   kind 0  reference:  q_i = r_i / (|k+G_i|^2 - lambda_b), |den| clamped at 1e-8 (eig.cu)
+//   kind 1  Teter-Payne-Allan: q_i = K(x_i) r_i, x_i = |k+G_i|^2 / E_kin,b,
+//           K(x) = (27 + 18x + 12x^2 + 8x^3) / (27 + 18x + 12x^2 + 8x^3 + 16x^4)
+//           (Teter, Payne, Allan, Phys. Rev. B 40, 12255 (1989)); E_kin,b = <psi_b|T|psi_b>
+//   kind 2  learned: q_i = m_theta(u_i) r_i with a per-plane-wave MLP, FP32 weights,
+//           u_i = (log(x_i + 0.05), log(|r_i| / rms(r_b) + 1e-6), t / 20), t the iteration index,
+//           h1 = tanh(W1 u + b1), h2 = tanh(W2 h1 + b2), m = softplus(w3 . h2 + b3), 3 -> 64 -> 64 -> 1.
+//
+// Training (dftcuda_precond_mlp_loss_grad / _train): samples are bands b with plane-wave data
+// c_i = conj(r_i) delta_i, w_i = |r_i|^2 and D_b = ||delta_b||^2, where delta is the correction that
+// would have taken the Ritz vector to the converged eigenvector.  The loss is scale-free, as the
+// Davidson step is:  L = mean_b [1 - |A_b|^2 / (Q_b D_b)],  A_b = sum_i m_i c_i,  Q_b = sum_i m_i^2 w_i
+// (one minus the squared cosine between the preconditioned residual and the ideal correction).
+// One CTA per band for the forward sums; the backward pass recomputes the activations per tile of
+// 128 plane waves and accumulates the weight gradients as small tile GEMMs in registers.
+#include <cmath>
+#include <vector>
+
+#include "kctx.cuh"
+
+namespace dftcuda {
+
+constexpr int MLP_H = 64;
+constexpr int MLP_IN = 3;
+// parameter layout: W1[64][3], b1[64], W2[64][64] (row = output), b2[64], w3[64], b3
+constexpr int MLP_OFF_W1 = 0;
+constexpr int MLP_OFF_B1 = MLP_OFF_W1 + MLP_H * MLP_IN;
+constexpr int MLP_OFF_W2 = MLP_OFF_B1 + MLP_H;
+constexpr int MLP_OFF_B2 = MLP_OFF_W2 + MLP_H * MLP_H;
+constexpr int MLP_OFF_W3 = MLP_OFF_B2 + MLP_H;
+constexpr int MLP_OFF_B3 = MLP_OFF_W3 + MLP_H;
+constexpr int MLP_NPARAM = MLP_OFF_B3 + 1;  // 4481
+static_assert(MLP_NPARAM == DFTCUDA_PRECOND_MLP_PARAMS, "parameter count");
+
+__device__ __forceinline__ float softplusf(float z) { return z > 20.f ? z : log1pf(expf(z)); }
+__device__ __forceinline__ float sigmoidf(float z) { return 1.f / (1.f + expf(-z)); }
+
+// Forward for one input with the parameters in shared memory; returns z (before softplus) and
+// optionally the two hidden layers.
+__device__ __forceinline__ float mlp_forward(const float* __restrict__ p, const float u[3], float* h1, float* h2) {
+  float a1[MLP_H];
+#pragma unroll
+  for (int j = 0; j < MLP_H; ++j) {
+    const float* w = p + MLP_OFF_W1 + j * MLP_IN;
+    a1[j] = tanhf(fmaf(w[0], u[0], fmaf(w[1], u[1], fmaf(w[2], u[2], p[MLP_OFF_B1 + j]))));
+  }
+  float z = p[MLP_OFF_B3];
+#pragma unroll 4
+  for (int j = 0; j < MLP_H; ++j) {
+    const float* w = p + MLP_OFF_W2 + j * MLP_H;
+    float s = p[MLP_OFF_B2 + j];
+#pragma unroll
+    for (int i = 0; i < MLP_H; ++i) s = fmaf(w[i], a1[i], s);
+    const float t = tanhf(s);
+    if (h2) h2[j] = t;
+    z = fmaf(p[MLP_OFF_W3 + j], t, z);
+  }
+  if (h1) {
+#pragma unroll
+    for (int j = 0; j < MLP_H; ++j) h1[j] = a1[j];
+  }
+  return z;
+}
+
+__device__ __forceinline__ void mlp_features(double kin, double ekin, double rabs, double rms, double t, float u[3]) {
+  const double x = kin / fmax(ekin, 1e-6);
+  u[0] = (float)log(x + 0.05);
+  u[1] = (float)log(rabs / fmax(rms, 1e-300) + 1e-6);
+  u[2] = (float)fmin(t / 20.0, 2.0);
+}
+
+// E_kin,b = sum_i kin_i |psi_b,i|^2 for the bands in the list (one CTA per band).
+__global__ void k_band_kinetic(const double2* __restrict__ ritz, const double* __restrict__ kin, const int* __restrict__ band,
+                               long n, double* __restrict__ ekin) {
+  __shared__ double red[256];
+  const int b = band[blockIdx.x];
+  const double2* v = ritz + (long)b * n;
+  double s = 0.0;
+  for (long i = threadIdx.x; i < n; i += blockDim.x) s += kin[i] * (v[i].x * v[i].x + v[i].y * v[i].y);
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) ekin[blockIdx.x] = red[0];
+}
+
+__global__ void k_precondition_tpa(double2* __restrict__ Q, const double2* __restrict__ res, const double* __restrict__ kin,
+                                   const double* __restrict__ ekin, const int* __restrict__ band, int k, long n) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= (long)k * n) return;
+  const int j = (int)(idx / n);
+  const long i = idx - (long)j * n;
+  const double x = kin[i] / fmax(ekin[j], 1e-6);
+  const double num = 27.0 + x * (18.0 + x * (12.0 + 8.0 * x));
+  const double f = num / (num + 16.0 * x * x * x * x);
+  const double2 v = res[(long)band[j] * n + i];
+  Q[idx] = make_double2(v.x * f, v.y * f);
+}
+
+__global__ void __launch_bounds__(256) k_precondition_mlp(double2* __restrict__ Q, const double2* __restrict__ res,
+                                                          const double* __restrict__ kin, const double* __restrict__ ekin,
+                                                          const double* __restrict__ norms, const int* __restrict__ band,
+                                                          int k, long n, double t, const float* __restrict__ params) {
+  __shared__ float p[MLP_NPARAM];
+  for (int i = threadIdx.x; i < MLP_NPARAM; i += blockDim.x) p[i] = params[i];
+  __syncthreads();
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= (long)k * n) return;
+  const int j = (int)(idx / n);
+  const long i = idx - (long)j * n;
+  const int b = band[j];
+  const double2 v = res[(long)b * n + i];
+  float u[3];
+  mlp_features(kin[i], ekin[j], sqrt(v.x * v.x + v.y * v.y), norms[b] / sqrt((double)n), t, u);
+  const double m = (double)softplusf(mlp_forward(p, u, nullptr, nullptr));
+  Q[idx] = make_double2(v.x * m, v.y * m);
+}
+
+// The reference preconditioner (eig.cu).
+__global__ void k_precondition(double2* __restrict__ Q, const double2* __restrict__ res, const double* __restrict__ diag,
+                               const double* __restrict__ lam, const int* __restrict__ band, int k, long n);
+
+// ---- training -----------------------------------------------------------------------------------
+
+// Per band: A_b = sum m_i c_i (complex), Q_b = sum m_i^2 w_i.
+__global__ void __launch_bounds__(256) k_mlp_band_sums(const int* __restrict__ off, const float* __restrict__ feat,
+                                                       const float2* __restrict__ cc, const float* __restrict__ w,
+                                                       const float* __restrict__ params, double* __restrict__ sums) {
+  __shared__ float p[MLP_NPARAM];
+  __shared__ double red[3][256];
+  for (int i = threadIdx.x; i < MLP_NPARAM; i += blockDim.x) p[i] = params[i];
+  __syncthreads();
+  const int b = blockIdx.x;
+  double ar = 0.0, ai = 0.0, q = 0.0;
+  for (int i = off[b] + threadIdx.x; i < off[b + 1]; i += blockDim.x) {
+    const float u[3] = {feat[3 * i], feat[3 * i + 1], feat[3 * i + 2]};
+    const double m = (double)softplusf(mlp_forward(p, u, nullptr, nullptr));
+    ar += m * cc[i].x;
+    ai += m * cc[i].y;
+    q += m * m * w[i];
+  }
+  red[0][threadIdx.x] = ar;
+  red[1][threadIdx.x] = ai;
+  red[2][threadIdx.x] = q;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int r = 0; r < 3; ++r) red[r][threadIdx.x] += red[r][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    sums[3 * b] = red[0][0];
+    sums[3 * b + 1] = red[1][0];
+    sums[3 * b + 2] = red[2][0];
+  }
+}
+
+constexpr int BW_TILE = 128;  // plane waves per backward tile (= threads per CTA)
+
+// Gradient of L = (1/B) sum_b [1 - |A_b|^2 / (Q_b D_b)] with respect to the parameters, one CTA
+// per band.  Thread t owns the dW2 entries (row t / 2, columns 32 (t % 2) ... + 31) and the
+// first-layer / bias / w3 entries with index t (< 64).
+__global__ void __launch_bounds__(BW_TILE) k_mlp_backward(const int* __restrict__ off, const float* __restrict__ feat,
+                                                          const float2* __restrict__ cc, const float* __restrict__ w,
+                                                          const float* __restrict__ dnorm, const double* __restrict__ sums,
+                                                          const float* __restrict__ params, int nbands,
+                                                          float* __restrict__ grad) {
+  extern __shared__ float bsm[];
+  float* p = bsm;                       // MLP_NPARAM
+  float* H1 = p + MLP_NPARAM + 3;       // [BW_TILE][65] (padded)
+  float* DA2 = H1 + BW_TILE * 65;       // [BW_TILE][65]
+  float* DA1 = DA2 + BW_TILE * 65;      // [BW_TILE][65]
+  float* U = DA1 + BW_TILE * 65;        // [BW_TILE][3]
+  float* H2 = U + BW_TILE * 3;          // [BW_TILE][65]
+  float* DZ = H2 + BW_TILE * 65;        // [BW_TILE]
+  const int tid = threadIdx.x;
+  for (int i = tid; i < MLP_NPARAM; i += blockDim.x) p[i] = params[i];
+  __syncthreads();
+  const int b = blockIdx.x;
+  const double Ar = sums[3 * b], Ai = sums[3 * b + 1], Qb = fmax(sums[3 * b + 2], 1e-300), Db = fmax((double)dnorm[b], 1e-300);
+  const double A2 = Ar * Ar + Ai * Ai;
+  const double scale = 1.0 / (double)nbands;
+  // owned accumulators
+  const int row = tid >> 1, cbase = (tid & 1) * 32;
+  float gW2[32];
+#pragma unroll
+  for (int q = 0; q < 32; ++q) gW2[q] = 0.f;
+  float gW1[3] = {0.f, 0.f, 0.f}, gb1 = 0.f, gb2 = 0.f, gw3 = 0.f, gb3 = 0.f;
+  for (int t0 = off[b]; t0 < off[b + 1]; t0 += BW_TILE) {
+    const int i = t0 + tid;
+    const bool live = i < off[b + 1];
+    float* h1 = H1 + tid * 65;
+    float* h2 = H2 + tid * 65;
+    float* da2 = DA2 + tid * 65;
+    float u[3] = {0.f, 0.f, 0.f};
+    float dz = 0.f;
+    if (live) {
+      u[0] = feat[3 * i];
+      u[1] = feat[3 * i + 1];
+      u[2] = feat[3 * i + 2];
+      const float z = mlp_forward(p, u, h1, h2);
+      const double m = (double)softplusf(z);
+      // dL/dm_i = -(2 / (D Q)) [Re(conj(A) c_i) - (|A|^2 / Q) m_i w_i], times 1/B
+      const double re = Ar * cc[i].x + Ai * cc[i].y;
+      const double dm = -2.0 / (Db * Qb) * (re - A2 / Qb * m * w[i]) * scale;
+      dz = (float)(dm * (double)sigmoidf(z));
+    } else {
+      for (int j = 0; j < MLP_H; ++j) h1[j] = h2[j] = 0.f;
+    }
+    // da2 = dz w3 (1 - h2^2); da1 = (W2^T da2) (1 - h1^2)
+    for (int j = 0; j < MLP_H; ++j) da2[j] = dz * p[MLP_OFF_W3 + j] * (1.f - h2[j] * h2[j]);
+    for (int i2 = 0; i2 < MLP_H; ++i2) {
+      float sacc = 0.f;
+      for (int j = 0; j < MLP_H; ++j) sacc = fmaf(p[MLP_OFF_W2 + j * MLP_H + i2], da2[j], sacc);
+      DA1[tid * 65 + i2] = sacc * (1.f - h1[i2] * h1[i2]);
+    }
+    U[tid * 3] = u[0];
+    U[tid * 3 + 1] = u[1];
+    U[tid * 3 + 2] = u[2];
+    DZ[tid] = dz;
+    __syncthreads();
+    // dW2[row][c] += sum_t DA2[t][row] H1[t][c]
+    for (int t = 0; t < BW_TILE; ++t) {
+      const float a = DA2[t * 65 + row];
+#pragma unroll
+      for (int q = 0; q < 32; ++q) gW2[q] = fmaf(a, H1[t * 65 + cbase + q], gW2[q]);
+    }
+    if (tid < MLP_H) {
+      for (int t = 0; t < BW_TILE; ++t) {
+        const float a1 = DA1[t * 65 + tid];
+        gW1[0] = fmaf(a1, U[t * 3], gW1[0]);
+        gW1[1] = fmaf(a1, U[t * 3 + 1], gW1[1]);
+        gW1[2] = fmaf(a1, U[t * 3 + 2], gW1[2]);
+        gb1 += a1;
+        gb2 += DA2[t * 65 + tid];
+        gw3 = fmaf(DZ[t], H2[t * 65 + tid], gw3);
+      }
+    }
+    if (tid == 0)
+      for (int t = 0; t < BW_TILE; ++t) gb3 += DZ[t];
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 32; ++q) atomicAdd(&grad[MLP_OFF_W2 + row * MLP_H + cbase + q], gW2[q]);
+  if (tid < MLP_H) {
+    atomicAdd(&grad[MLP_OFF_W1 + tid * 3], gW1[0]);
+    atomicAdd(&grad[MLP_OFF_W1 + tid * 3 + 1], gW1[1]);
+    atomicAdd(&grad[MLP_OFF_W1 + tid * 3 + 2], gW1[2]);
+    atomicAdd(&grad[MLP_OFF_B1 + tid], gb1);
+    atomicAdd(&grad[MLP_OFF_B2 + tid], gb2);
+    atomicAdd(&grad[MLP_OFF_W3 + tid], gw3);
+  }
+  if (tid == 0) atomicAdd(&grad[MLP_OFF_B3], gb3);
+}
+
+__global__ void k_mlp_loss(const double* __restrict__ sums, const float* __restrict__ dnorm, int nbands, double* __restrict__ loss) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nbands; b += blockDim.x) {
+    const double Ar = sums[3 * b], Ai = sums[3 * b + 1], Q = fmax(sums[3 * b + 2], 1e-300), D = fmax((double)dnorm[b], 1e-300);
+    s += 1.0 - (Ar * Ar + Ai * Ai) / (Q * D);
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *loss = red[0] / nbands;
+}
+
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m1, float* __restrict__ m2,
+                       int np, float lr, float b1, float b2, float eps, int step) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const float gi = g[i];
+  const float a = b1 * m1[i] + (1.f - b1) * gi, v = b2 * m2[i] + (1.f - b2) * gi * gi;
+  m1[i] = a;
+  m2[i] = v;
+  const float ah = a / (1.f - powf(b1, (float)step)), vh = v / (1.f - powf(b2, (float)step));
+  p[i] -= lr * ah / (sqrtf(vh) + eps);
+}
+
+constexpr size_t kBackwardSmem = sizeof(float) * (MLP_NPARAM + 3 + 4 * BW_TILE * 65 + BW_TILE * 3 + BW_TILE);
+
+struct MlpData {
+  int nb = 0;
+  long np = 0;
+  int* off = nullptr;
+  float* feat = nullptr;
+  float2* cc = nullptr;
+  float* w = nullptr;
+  float* dn = nullptr;
+  double* sums = nullptr;
+  double* loss = nullptr;
+  float* params = nullptr;
+  float* grad = nullptr;
+  float* m1 = nullptr;
+  float* m2 = nullptr;
+  void* mem = nullptr;
+  ~MlpData() {
+    if (mem) cudaFree(mem);
+  }
+};
+
+static int mlp_upload(MlpData& d, size_t nbands, size_t npw, const int* off, const float* feat, const float* cc, const float* w,
+                      const float* dnorm, const float* params, cudaStream_t s) {
+  d.nb = (int)nbands;
+  d.np = (long)npw;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { const size_t r = o; o += (bytes + 255) / 256 * 256; return r; };
+  const size_t oo = take(sizeof(int) * (nbands + 1)), of = take(sizeof(float) * 3 * npw), oc = take(sizeof(float2) * npw),
+               ow = take(sizeof(float) * npw), od = take(sizeof(float) * nbands), os = take(sizeof(double) * 3 * nbands),
+               ol = take(sizeof(double)), op = take(sizeof(float) * MLP_NPARAM), og = take(sizeof(float) * MLP_NPARAM),
+               o1 = take(sizeof(float) * MLP_NPARAM), o2 = take(sizeof(float) * MLP_NPARAM);
+  if (cudaMalloc(&d.mem, o) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "precond_mlp: training data");
+  char* b = (char*)d.mem;
+  d.off = (int*)(b + oo); d.feat = (float*)(b + of); d.cc = (float2*)(b + oc); d.w = (float*)(b + ow);
+  d.dn = (float*)(b + od); d.sums = (double*)(b + os); d.loss = (double*)(b + ol); d.params = (float*)(b + op);
+  d.grad = (float*)(b + og); d.m1 = (float*)(b + o1); d.m2 = (float*)(b + o2);
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    return cudaMemcpyAsync(dst, src, bytes, is_device_pointer(src) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
+  };
+  DFT_CUDA_TRY(up(d.off, off, sizeof(int) * (nbands + 1)));
+  DFT_CUDA_TRY(up(d.feat, feat, sizeof(float) * 3 * npw));
+  DFT_CUDA_TRY(up(d.cc, cc, sizeof(float2) * npw));
+  DFT_CUDA_TRY(up(d.w, w, sizeof(float) * npw));
+  DFT_CUDA_TRY(up(d.dn, dnorm, sizeof(float) * nbands));
+  DFT_CUDA_TRY(up(d.params, params, sizeof(float) * MLP_NPARAM));
+  DFT_CUDA_TRY(cudaMemsetAsync(d.m1, 0, sizeof(float) * MLP_NPARAM, s));
+  DFT_CUDA_TRY(cudaMemsetAsync(d.m2, 0, sizeof(float) * MLP_NPARAM, s));
+  return DFTCUDA_OK;
+}
+
+static int mlp_loss_grad_dev(MlpData& d, cudaStream_t s) {
+  static int attr_dev = -1;
+  int dev = 0;
+  DFT_CUDA_TRY(cudaGetDevice(&dev));
+  if (attr_dev != dev) {
+    DFT_CUDA_TRY(cudaFuncSetAttribute(k_mlp_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBackwardSmem));
+    attr_dev = dev;
+  }
+  k_mlp_band_sums<<<d.nb, 256, 0, s>>>(d.off, d.feat, d.cc, d.w, d.params, d.sums); count_launch();
+  k_mlp_loss<<<1, 256, 0, s>>>(d.sums, d.dn, d.nb, d.loss); count_launch();
+  DFT_CUDA_TRY(cudaMemsetAsync(d.grad, 0, sizeof(float) * MLP_NPARAM, s));
+  k_mlp_backward<<<d.nb, BW_TILE, kBackwardSmem, s>>>(d.off, d.feat, d.cc, d.w, d.dn, d.sums, d.params, d.nb, d.grad); count_launch();
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}
+
+}  // namespace dftcuda
+
+using namespace dftcuda;
+
+extern "C" int dftcuda_kctx_set_preconditioner(dftcuda_kctx* c, int kind, const float* params, size_t nparams) {
+  if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_preconditioner: null context");
+  if (kind < DFTCUDA_PRECOND_REFERENCE || kind > DFTCUDA_PRECOND_MLP)
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_preconditioner: unknown kind");
+  if (kind == DFTCUDA_PRECOND_MLP) {
+    if (!params || nparams != (size_t)MLP_NPARAM)
+      return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_preconditioner: the MLP needs DFTCUDA_PRECOND_MLP_PARAMS weights");
+    if (!c->d_mlp && cudaMalloc(&c->d_mlp, sizeof(float) * MLP_NPARAM) != cudaSuccess)
+      return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_preconditioner: weights");
+    DFT_CUDA_TRY(cudaMemcpyAsync(c->d_mlp, params, sizeof(float) * MLP_NPARAM,
+                                 is_device_pointer(params) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
+    DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  c->precond_kind = kind;
+  return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_precond_mlp_loss_grad(size_t nbands, size_t npw, const int* band_off, const float* feat,
+                                             const float* cc, const float* w, const float* dnorm, const float* params,
+                                             double* loss, float* grad) {
+  if (nbands == 0 || npw == 0 || !band_off || !feat || !cc || !w || !dnorm || !params || !loss || !grad)
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "precond_mlp_loss_grad: empty or null argument");
+  cudaStream_t s = nullptr;
+  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  int st;
+  {
+    MlpData d;
+    st = mlp_upload(d, nbands, npw, band_off, feat, cc, w, dnorm, params, s);
+    if (st == DFTCUDA_OK) st = mlp_loss_grad_dev(d, s);
+    if (st == DFTCUDA_OK) {
+      cudaMemcpyAsync(loss, d.loss, sizeof(double), is_device_pointer(loss) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(grad, d.grad, sizeof(float) * MLP_NPARAM,
+                      is_device_pointer(grad) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);
+      const cudaError_t ce = cudaStreamSynchronize(s);
+      if (ce != cudaSuccess) st = fail(DFTCUDA_ERR_CUDA, cudaGetErrorString(ce));
+    }
+  }
+  cudaStreamDestroy(s);
+  return st;
+}
+
+extern "C" int dftcuda_precond_mlp_train(size_t nbands, size_t npw, const int* band_off, const float* feat, const float* cc,
+                                         const float* w, const float* dnorm, float* params, size_t steps, float lr,
+                                         double* loss_history) {
+  if (nbands == 0 || npw == 0 || !band_off || !feat || !cc || !w || !dnorm || !params)
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "precond_mlp_train: empty or null argument");
+  cudaStream_t s = nullptr;
+  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  int st;
+  {
+    MlpData d;
+    st = mlp_upload(d, nbands, npw, band_off, feat, cc, w, dnorm, params, s);
+    std::vector<double> hist(steps, 0.0);
+    double* dhist = nullptr;
+    if (st == DFTCUDA_OK && steps && cudaMalloc(&dhist, sizeof(double) * steps) != cudaSuccess)
+      st = fail(DFTCUDA_ERR_OUT_OF_MEMORY, "precond_mlp_train: history");
+    for (size_t it = 0; it < steps && st == DFTCUDA_OK; ++it) {
+      st = mlp_loss_grad_dev(d, s);
+      if (st != DFTCUDA_OK) break;
+      cudaMemcpyAsync(dhist + it, d.loss, sizeof(double), cudaMemcpyDeviceToDevice, s);
+      k_adam<<<ceil_div(MLP_NPARAM, 256), 256, 0, s>>>(d.params, d.grad, d.m1, d.m2, MLP_NPARAM, lr, 0.9f, 0.999f, 1e-8f,
+                                                      (int)it + 1);
+      count_launch();
+    }
+    if (st == DFTCUDA_OK) {
+      cudaMemcpyAsync(params, d.params, sizeof(float) * MLP_NPARAM,
+                      is_device_pointer(params) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);
+      if (steps) cudaMemcpyAsync(hist.data(), dhist, sizeof(double) * steps, cudaMemcpyDeviceToHost, s);
+      const cudaError_t ce = cudaStreamSynchronize(s);
+      if (ce != cudaSuccess) st = fail(DFTCUDA_ERR_CUDA, cudaGetErrorString(ce));
+      if (st == DFTCUDA_OK && loss_history)
+        for (size_t i = 0; i < steps; ++i) loss_history[i] = hist[i];
+    }
+    if (dhist) cudaFree(dhist);
+  }
+  cudaStreamDestroy(s);
+  return st;
+}
+
+namespace dftcuda {
+
+int precondition_launch(dftcuda_kctx* c, double2* Q, const double2* res, const double* kin, const double* lam,
+                        const double* norms, const double2* ritz, const int* band, int take, long n, double t,
+                        double* ekin_ws, cudaStream_t s) {
+  const unsigned grid = ceil_div((size_t)take * n, 256);
+  if (c->precond_kind == DFTCUDA_PRECOND_REFERENCE) {
+    k_precondition<<<grid, 256, 0, s>>>(Q, res, kin, lam, band, take, n);
+    count_launch();
+  } else {
+    k_band_kinetic<<<take, 256, 0, s>>>(ritz, kin, band, n, ekin_ws);
+    count_launch();
+    if (c->precond_kind == DFTCUDA_PRECOND_TPA)
+      k_precondition_tpa<<<grid, 256, 0, s>>>(Q, res, kin, ekin_ws, band, take, n);
+    else
+      k_precondition_mlp<<<grid, 256, 0, s>>>(Q, res, kin, ekin_ws, norms, band, take, n, t, c->d_mlp);
+    count_launch();
+  }
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}
+
+}  // namespace dftcuda

@@ -350,7 +350,7 @@ static int tc_dispatch(const GemmArgs& g, dim3 grid, int kps, double2* part, int
 int cgemm_tf32(const GemmArgs& g, cudaStream_t s, double2* ws, size_t ws_elems, int* err_dev, bool split) {
   if (g.M <= 0 || g.N <= 0) return DFTCUDA_OK;
   if (g.K <= 0) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "cgemm_tf32: K must be positive");
-  int splits = tc_splits(g.M, g.N, g.K);
+  int splits = g.splits > 0 ? std::min(g.splits, std::max(1, g.K / 32)) : tc_splits(g.M, g.N, g.K);
   if (splits > 1 && (size_t)splits * g.M * g.N > ws_elems) splits = 1;
   int kps = (g.K + splits - 1) / splits;
   kps = ((kps + TC_K - 1) / TC_K) * TC_K;

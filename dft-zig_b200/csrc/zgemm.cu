@@ -189,7 +189,7 @@ int zgemm(const GemmArgs& g, cudaStream_t s, double2* ws, size_t ws_elems) {
     // out = beta * out
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "zgemm: K must be positive");
   }
-  int splits = pick_splits(g.M, g.N, g.K);
+  int splits = g.splits > 0 ? std::min(g.splits, std::max(1, g.K / 32)) : pick_splits(g.M, g.N, g.K);
   if (splits > 1 && (size_t)splits * g.M * g.N > ws_elems) splits = 1;
   int kps = (g.K + splits - 1) / splits;
   kps = ((kps + BK - 1) / BK) * BK;

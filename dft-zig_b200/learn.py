@@ -1,0 +1,335 @@
+"""Learned components: data generation, GPU training and evaluation.
+
+Learned preconditioner (``precond``): a per-plane-wave MLP that replaces the diagonal of the
+Davidson correction step (the reference's r / (|k+G|^2 - lambda), lobpcg/common.zig:214-226; the
+Teter-Payne-Allan form is the other fixed alternative).  Training pairs come from plain runs of the
+device solver on seeded strained and displaced Si8 cells (``si8d``): the solver is deterministic
+(LCG start, serial.zig:75-95), so the run stopped after t iterations reproduces the Ritz vectors
+psi_b^t of the full run; the target is the correction delta_b = P(psi_b^inf) - psi_b^t that takes
+psi_b^t to its converged eigenspace (orthogonal to psi_b^t).  The network is trained on the GPU by
+the library's own CUDA forward/backward kernels (dftcuda_precond_mlp_train, Adam).
+
+Learned first density (``fno``): a Fourier neural operator (csrc/fno.cu) maps the superposition of
+atomic densities of a cell (build_atomic_density, scf/core_density.zig:128-183; two channels, Si-like
+and Ge-like) to the converged SCF density minus that superposition.  Targets come from plain SCF
+runs (flat start, the reference default, run_state.zig:98-115) on seeded SiGe8 cells; training runs
+on the GPU with the library's own FNO forward/backward kernels.  The learned start is
+rho0 = rho_atomic + mean * FNO(u), clipped positive and renormalised to N_e.
+
+Usage (the package directory is registered as ``dftzig_b200`` by dftzig_loader):
+    python -c "import dftzig_loader, importlib; dftzig_loader.load(); importlib.import_module('dftzig_b200.learn').main()" precond
+    python -c "...same..." fno
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import scf as scfm
+from . import system as sysm
+
+WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
+PRECOND_WEIGHTS = os.path.join(WEIGHTS_DIR, "precond_mlp.npz")
+FNO_WEIGHTS = os.path.join(WEIGHTS_DIR, "fno_density.npz")
+
+
+def _context(dz, inp, precision=0):
+    kc = dz.KpointContext(*inp.dims, inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart, precision)
+    kc.set_vloc(inp.local_r)
+    kc.set_projectors([dz.SpeciesProjectors(l, d, p) for (l, d, p) in inp.species_phi], inp.atom_species, inp.positions)
+    return kc
+
+
+def _features(kin, ekin, rabs, rms, t):
+    x = kin / max(ekin, 1e-6)
+    return np.stack([np.log(x + 0.05), np.log(rabs / max(rms, 1e-300) + 1e-6), np.full_like(x, min(t / 20.0, 2.0))], axis=1)
+
+
+def precond_samples(dz, cells, ecut: float, nbands: int, t_max: int = 8, kfrac=(0.0, 0.0, 0.0), cluster_tol: float = 1e-4):
+    """Residual -> correction samples from plain Davidson runs (one k-point per cell)."""
+    off = [0]
+    feats, ccs, ws, dns, kins, lams = [], [], [], [], [], []
+    for c in cells:
+        inp = sysm.kpoint_inputs(c, ecut, kfrac)
+        kc = _context(dz, inp)
+        kin = inp.basis.kinetic
+        nconv = nbands + 4
+        conv = kc.hermitian_eigen_decomp_iterative(kin, nconv, dz.Options(max_iter=400, tol=1e-10))
+        for t in range(1, t_max + 1):
+            r = kc.hermitian_eigen_decomp_iterative(kin, nbands, dz.Options(max_iter=t, tol=1e-14))
+            psi = r.vectors
+            hpsi = kc.apply_hamiltonian_batched(psi)
+            res = hpsi - r.values[:, None] * psi
+            for b in range(nbands):
+                rn = float(np.linalg.norm(res[b]))
+                if rn < 1e-7:
+                    continue
+                cl = np.nonzero(np.abs(conv.values - conv.values[b]) < cluster_tol)[0]
+                Y = conv.vectors[cl]
+                y = Y.T @ (Y.conj() @ psi[b])
+                ny = float(np.linalg.norm(y))
+                if ny < 0.5:
+                    continue
+                y /= ny
+                delta = y - psi[b] * np.vdot(psi[b], y)
+                dn = float(np.vdot(delta, delta).real)
+                if dn < 1e-20:
+                    continue
+                ekin = float(np.sum(kin * np.abs(psi[b]) ** 2))
+                feats.append(_features(kin, ekin, np.abs(res[b]), rn / np.sqrt(len(kin)), t - 1))
+                ccs.append(np.conj(res[b]) * delta)
+                ws.append(np.abs(res[b]) ** 2)
+                dns.append(dn)
+                kins.append(kin)
+                lams.append(float(r.values[b]))
+                off.append(off[-1] + len(kin))
+        kc.close()
+    return {
+        "off": np.array(off, dtype=np.int32),
+        "feat": np.concatenate(feats).astype(np.float32),
+        "cc": np.concatenate(ccs),
+        "w": np.concatenate(ws),
+        "dnorm": np.array(dns),
+        "kin": np.concatenate(kins),
+        "lam": np.array(lams),
+    }
+
+
+def fixed_loss(samples, kind: str) -> float:
+    """The training loss of a fixed preconditioner on the same samples (host arithmetic)."""
+    off = samples["off"]
+    nb = len(off) - 1
+    band = np.repeat(np.arange(nb), np.diff(off))
+    kin = samples["kin"]
+    if kind == "reference":
+        den = kin - samples["lam"][band]
+        den = np.where(np.abs(den) < 1e-8, np.where(den >= 0, 1e-8, -1e-8), den)
+        m = 1.0 / den
+    else:
+        x = np.exp(samples["feat"][:, 0].astype(np.float64)) - 0.05
+        num = 27.0 + x * (18.0 + x * (12.0 + 8.0 * x))
+        m = num / (num + 16.0 * x ** 4)
+    cc, w = samples["cc"], samples["w"]
+    A = np.bincount(band, weights=(m * cc).real, minlength=nb) + 1j * np.bincount(band, weights=(m * cc).imag, minlength=nb)
+    Q = np.bincount(band, weights=m * m * w, minlength=nb)
+    return float(np.mean(1.0 - np.abs(A) ** 2 / (Q * samples["dnorm"])))
+
+
+def init_params(seed: int = 0, scale: float = 0.3) -> np.ndarray:
+    """Random initial weights (layout of DFTCUDA_PRECOND_MLP_PARAMS: W1, b1, W2, b2, w3, b3)."""
+    H = 64
+    rng = np.random.default_rng(seed)
+    parts = [
+        rng.normal(0.0, scale, H * 3),
+        rng.normal(0.0, scale, H),
+        rng.normal(0.0, scale / np.sqrt(H), H * H),
+        rng.normal(0.0, scale, H),
+        rng.normal(0.0, scale / np.sqrt(H), H),
+        [0.5],
+    ]
+    return np.concatenate(parts).astype(np.float32)
+
+
+def train_precond(dz, samples, steps: int = 1500, lr: float = 2e-3, seed: int = 0):
+    p0 = init_params(seed)
+    p, hist = dz.precond_mlp_train(p0, samples["off"], samples["feat"], samples["cc"], samples["w"], samples["dnorm"], steps, lr)
+    return p, hist
+
+
+def eval_loss(dz, params, samples) -> float:
+    return dz.precond_mlp_loss_grad(params, samples["off"], samples["feat"], samples["cc"], samples["w"], samples["dnorm"])[0]
+
+
+def evaluate_precond(dz, cells, ecut: float, nbands: int, params, tol: float = 1e-6, kfrac=(0.0, 0.0, 0.0)) -> dict:
+    """Davidson iterations and H applications to reach tol from the random start, per preconditioner."""
+    out = {"reference": [], "tpa": [], "mlp": []}
+    for c in cells:
+        inp = sysm.kpoint_inputs(c, ecut, kfrac)
+        for kind, key in ((dz.PRECOND_REFERENCE, "reference"), (dz.PRECOND_TPA, "tpa"), (dz.PRECOND_MLP, "mlp")):
+            kc = _context(dz, inp)
+            kc.set_preconditioner(kind, params if kind == dz.PRECOND_MLP else None)
+            r = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, nbands, dz.Options(max_iter=300, tol=tol))
+            out[key].append({"iterations": r.iterations, "h_applies": r.h_applies, "converged": r.converged})
+            kc.close()
+    summ = {}
+    for key, rs in out.items():
+        summ[key] = {
+            "mean_iterations": float(np.mean([r["iterations"] for r in rs])),
+            "mean_h_applies": float(np.mean([r["h_applies"] for r in rs])),
+            "all_converged": all(r["converged"] for r in rs),
+        }
+    return summ
+
+
+def load_precond_weights(path: str = PRECOND_WEIGHTS) -> np.ndarray:
+    with np.load(path) as z:
+        return np.asarray(z["params"], dtype=np.float32)
+
+
+# ---- learned first density -------------------------------------------------------------------
+
+
+def fno_input(c, ecut: float):
+    """(dims, u [2][N] = atomic channels / mean density, rho_atomic [N], mean density)."""
+    dims = sysm.fft_box(ecut, c.recip)
+    ch = sysm.atomic_density_channels(c, dims)
+    mean = c.nelec / c.volume
+    return dims, ch / mean, ch.sum(axis=0), mean
+
+
+def fno_initial_density(dz, params, c, ecut: float) -> np.ndarray:
+    """rho0 = rho_atomic + mean * FNO(u), clipped at 1e-3 mean and renormalised to N_e."""
+    dims, u, rho_at, mean = fno_input(c, ecut)
+    d = dz.fno_forward(params, u, dims).astype(np.float64)
+    rho = np.maximum(rho_at + mean * d, 1e-3 * mean)
+    return rho * (c.nelec / (rho.mean() * c.volume))
+
+
+def _scf_params(ecut, kmesh, nbands, tol, init=None, smearing=None):
+    return scfm.ScfParams(ecut=ecut, kmesh=kmesh, nbands=nbands, convergence=tol, max_iter=80, smearing=smearing, initial_density=init)
+
+
+def fno_samples(dz, cells, ecut: float, nbands: int, kmesh=(2, 2, 2), tol: float = 1e-7):
+    """(dims, u, target) per cell; target = (rho_scf - rho_atomic) / mean from a plain SCF run."""
+    out = []
+    for c in cells:
+        dims, u, rho_at, mean = fno_input(c, ecut)
+        b = scfm.GpuBackend(dz, "fp64")
+        r = scfm.run_scf(c, _scf_params(ecut, kmesh, nbands, tol), b)
+        b.close()
+        out.append((dims, u, (r.rho - rho_at) / mean))
+    return out
+
+
+def fno_init_params(seed: int = 0, spec_scale: float = 0.5, scale: float = 0.3) -> np.ndarray:
+    """Random initial FNO weights (layout of DFTCUDA_FNO_PARAMS)."""
+    W, K, L = 8, 16 ** 3, 4
+    rng = np.random.default_rng(seed)
+    parts = [rng.normal(0.0, scale, W * 2), np.zeros(W)]
+    for _ in range(L):
+        parts.append(rng.normal(0.0, spec_scale / W, 2 * K * W * W))
+        parts.append(rng.normal(0.0, scale / np.sqrt(W), W * W))
+        parts.append(np.zeros(W))
+    parts.append(rng.normal(0.0, scale / np.sqrt(W), W))
+    parts.append([0.0])
+    return np.concatenate(parts).astype(np.float32)
+
+
+def evaluate_fno(dz, params, cells, ecut: float, nbands: int, kmesh=(2, 2, 2), tol: float = 1e-6) -> dict:
+    """SCF iterations from the flat start (the reference default), the atomic superposition and the
+    learned start; plus the initial density error against the converged density."""
+    rows = []
+    for c in cells:
+        dims, u, rho_at, mean = fno_input(c, ecut)
+        starts = {"flat": None, "atomic": rho_at * (c.nelec / (rho_at.mean() * c.volume)), "fno": fno_initial_density(dz, params, c, ecut)}
+        row = {}
+        conv_rho = None
+        for name, init in starts.items():
+            b = scfm.GpuBackend(dz, "fp64")
+            r = scfm.run_scf(c, _scf_params(ecut, kmesh, nbands, tol, init), b)
+            b.close()
+            row[name] = {"iterations": r.iterations, "converged": r.converged, "energy_per_atom": r.energy_per_atom, "wall_s": r.wall_s}
+            if name == "flat":
+                conv_rho = r.rho
+        for name, init in starts.items():
+            if init is not None:
+                row[name]["initial_rms_error"] = float(np.sqrt(np.mean((init - conv_rho) ** 2)) / mean)
+        rows.append(row)
+    summ = {}
+    for name in ("flat", "atomic", "fno"):
+        summ[name] = {
+            "mean_iterations": float(np.mean([r[name]["iterations"] for r in rows])),
+            "all_converged": all(r[name]["converged"] for r in rows),
+            "mean_wall_s": float(np.mean([r[name]["wall_s"] for r in rows])),
+        }
+        if name != "flat":
+            summ[name]["mean_initial_rms_error"] = float(np.mean([r[name]["initial_rms_error"] for r in rows]))
+    summ["max_energy_spread_per_atom"] = float(max(max(r[n]["energy_per_atom"] for n in r) - min(r[n]["energy_per_atom"] for n in r) for r in rows))
+    return summ
+
+
+def load_fno_weights(path: str = FNO_WEIGHTS) -> np.ndarray:
+    with np.load(path) as z:
+        return np.asarray(z["params"], dtype=np.float32)
+
+
+def main(argv=None):
+    import importlib
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("what", choices=("precond", "fno"))
+    ap.add_argument("--train-cells", type=int, default=48)
+    ap.add_argument("--eval-cells", type=int, default=8)
+    ap.add_argument("--ecut", type=float, default=12.0)
+    ap.add_argument("--nbands", type=int, default=16)
+    ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--out", default=PRECOND_WEIGHTS)
+    ap.add_argument("--fno-train-cells", type=int, default=64)
+    ap.add_argument("--fno-eval-cells", type=int, default=8)
+    ap.add_argument("--fno-steps", type=int, default=400)
+    ap.add_argument("--fno-lr", type=float, default=2e-3)
+    a = ap.parse_args(argv)
+    dz = importlib.import_module(__package__)
+    if a.what == "fno":
+        return main_fno(dz, a)
+    t0 = time.perf_counter()
+    train_cells = [sysm.crystal("si8d", 1000 + i) for i in range(a.train_cells)]
+    eval_cells = [sysm.crystal("si8d", 1200 + i) for i in range(a.eval_cells)]
+    tr = precond_samples(dz, train_cells, a.ecut, a.nbands)
+    ev = precond_samples(dz, eval_cells, a.ecut, a.nbands)
+    t1 = time.perf_counter()
+    p, hist = train_precond(dz, tr, a.steps, a.lr)
+    t2 = time.perf_counter()
+    report = {
+        "train_bands": int(len(tr["off"]) - 1),
+        "train_plane_waves": int(tr["feat"].shape[0]),
+        "data_seconds": round(t1 - t0, 2),
+        "train_seconds": round(t2 - t1, 2),
+        "loss_first": float(hist[0]),
+        "loss_last": float(hist[-1]),
+        "heldout_loss": eval_loss(dz, p, ev),
+        "heldout_loss_initial_weights": eval_loss(dz, init_params(0), ev),
+        "heldout_loss_reference_diagonal": fixed_loss(ev, "reference"),
+        "heldout_loss_tpa": fixed_loss(ev, "tpa"),
+        "heldout_davidson": evaluate_precond(dz, eval_cells, a.ecut, a.nbands, p),
+    }
+    os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
+    np.savez(a.out, params=p, loss_history=hist.astype(np.float32), report=json.dumps(report))
+    print(json.dumps(report), flush=True)
+
+
+def main_fno(dz, a):
+    """SiGe8 cells (20 Ry, 2x2x2 k, 20 bands): train on seeds 2000.., evaluate on seeds 2400.."""
+    ecut, nb = 20.0, 20
+    t0 = time.perf_counter()
+    train = fno_samples(dz, [sysm.crystal("sige8", 2000 + i) for i in range(a.fno_train_cells)], ecut, nb)
+    heldout_cells = [sysm.crystal("sige8", 2400 + i) for i in range(a.fno_eval_cells)]
+    heldout = fno_samples(dz, heldout_cells, ecut, nb)
+    t1 = time.perf_counter()
+    p0 = fno_init_params(0)
+    p, hist = dz.fno_train(p0, train, a.fno_steps, a.fno_lr)
+    t2 = time.perf_counter()
+    zero = np.zeros_like(p0)
+    report = {
+        "train_cells": len(train),
+        "data_seconds": round(t1 - t0, 2),
+        "train_seconds": round(t2 - t1, 2),
+        "loss_first": float(hist[0]),
+        "loss_last": float(hist[-1]),
+        "heldout_loss": dz.fno_loss_grad(p, heldout)[0],
+        "heldout_loss_atomic_start": dz.fno_loss_grad(zero, heldout)[0],
+        "heldout_scf": evaluate_fno(dz, p, heldout_cells, ecut, nb),
+    }
+    out = a.out if a.out != PRECOND_WEIGHTS else FNO_WEIGHTS
+    os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
+    np.savez(out, params=p, loss_history=hist.astype(np.float32), report=json.dumps(report))
+    print(json.dumps(report), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -209,18 +209,26 @@ def entropy_term(occ):
 class GpuBackend:
     """One libdftcuda k-point context per k-point (the GPU analogue of KpointApplyCache).
 
-    precision "fp64" runs every FFT pass in FP64.  "mixed" keeps a second, FP32 context per k-point
-    and uses it while the SCF density residual is above ``switch_drho``, then the FP64 one for the
-    rest (the subspace algebra, residual checks and occupations stay FP64 throughout)."""
+    precision "fp64" runs every pass in FP64.  "mixed" keeps a second context per k-point in
+    TF32X3 precision (FP32 FFT passes, split-TF32 tensor-core projector and Rayleigh-Ritz GEMMs) and
+    uses it while the SCF density residual is above ``switch_drho``, then the FP64 one for the rest.
+    It also switches when the residual stops falling (``stall`` iterations without a new minimum),
+    the sign that the reduced-precision operator's error floor has been reached.  Orthonormalisation,
+    the subspace eigensolver, residual checks, occupations and energies stay FP64 throughout."""
 
-    def __init__(self, dz, precision="fp64", switch_drho: float = 1e-5):
+    def __init__(self, dz, precision="fp64", switch_drho: float = 1e-5, stall: int = 3):
         self.dz = dz
         self.precision = precision
         self.switch_drho = switch_drho
+        self.stall = stall
         self.ctxs = []
         self.ctxs32 = []
         self.use32 = precision == "mixed"
         self.local_r = None
+        self.best = float("inf")
+        self.since_best = 0
+        self.switched_at = None
+        self.n_obs = 0
 
     def _make(self, inp, prec):
         kc = self.dz.KpointContext(*inp.dims, inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart, prec)
@@ -231,11 +239,17 @@ class GpuBackend:
         for inp in kinputs:
             self.ctxs.append(self._make(inp, 0))
             if self.precision == "mixed":
-                self.ctxs32.append(self._make(inp, 1))
+                self.ctxs32.append(self._make(inp, self.dz.PRECISION_TF32X3))
 
     def observe(self, drho: float):
-        if self.use32 and drho < self.switch_drho:
+        self.n_obs += 1
+        if drho < self.best:
+            self.best, self.since_best = drho, 0
+        else:
+            self.since_best += 1
+        if self.use32 and (drho < self.switch_drho or self.since_best >= self.stall):
             self.use32 = False
+            self.switched_at = self.n_obs
             if self.local_r is not None:
                 for kc in self.ctxs:
                     kc.set_vloc(self.local_r)
@@ -252,6 +266,11 @@ class GpuBackend:
         o = self.dz.Options(**opts, init_vectors=init)
         r = self._active()[k].hermitian_eigen_decomp_iterative(diag, nbands, o)
         return r.values, r.vectors
+
+    def eig_all(self, diags, nbands, opts: dict, inits):
+        """All k-points in one lockstep batch (dftcuda_eig_solve_batch)."""
+        rs = self.dz.hermitian_eigen_decomp_iterative_batch(self._active(), diags, nbands, self.dz.Options(**opts), inits)
+        return [(r.values, r.vectors) for r in rs]
 
     def density(self, k, vectors, weights, rho):
         self._active()[k].accumulate_band_density(vectors, weights, rho)
@@ -290,6 +309,7 @@ class ScfParams:
     smearing: Optional[float] = None  # Fermi-Dirac width (Ry); None = fixed occupations
     energy_tol_per_atom: Optional[float] = None  # stop once |E - E_target| < tol (time-to-SCF runs)
     energy_target: Optional[float] = None
+    initial_density: Optional[np.ndarray] = None  # rho(r) on the FFT grid; None = flat N_e / Omega
 
 
 @dataclass
@@ -350,7 +370,12 @@ def run_scf(c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False) -> Sc
         _, vxc = lda_pz(rho)
         return vh + to_g(vxc)
 
-    rho = np.full(N, nelec / vol)
+    if p.initial_density is None:
+        rho = np.full(N, nelec / vol)  # init_rho_from_user_or_flat (run_state.zig:98-115)
+    else:
+        rho = np.asarray(p.initial_density, dtype=np.float64).copy()
+        if rho.size != N:
+            raise ValueError("initial_density size does not match the FFT grid")
     v_hxc = hxc_g(rho)
     mixer = PulayMixer(p.pulay_history)
     vectors = [None] * len(kpts)
@@ -368,11 +393,18 @@ def run_scf(c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False) -> Sc
         warm = it <= p.warmup_steps
         opts = dict(max_iter=p.warmup_max_iter if warm else p.iterative_max_iter, tol=p.warmup_tol if warm else p.iterative_tol)
         values = []
-        for k, inp in enumerate(kin):
-            init = vectors[k] if (p.reuse_vectors and vectors[k] is not None) else None
-            ev, vec = backend.eig(k, inp.basis.kinetic, nbands, opts, init)
-            values.append(np.asarray(ev))
-            vectors[k] = vec
+        inits = [vectors[k] if (p.reuse_vectors and vectors[k] is not None) else None for k in range(len(kin))]
+        if hasattr(backend, "eig_all"):
+            # every k-point's solve at once (the k-point worker loop, kpoint/workers.zig:133-180)
+            res = backend.eig_all([inp.basis.kinetic for inp in kin], nbands, opts, inits)
+            for k, (ev, vec) in enumerate(res):
+                values.append(np.asarray(ev))
+                vectors[k] = vec
+        else:
+            for k, inp in enumerate(kin):
+                ev, vec = backend.eig(k, inp.basis.kinetic, nbands, opts, inits[k])
+                values.append(np.asarray(ev))
+                vectors[k] = vec
         # occupations
         if p.smearing:
             mu = fermi_level(nelec, p.smearing, kweights, values)

@@ -111,6 +111,15 @@ def crystal(name: str, seed: int = 1) -> Crystal:
         if sigma > 0:
             pos = pos + rng.normal(0.0, sigma * BOHR_PER_ANGSTROM, size=pos.shape)
         return Crystal(np.eye(3) * a * reps, [si], np.zeros(len(pos), int), pos)
+    if name == "si8d":
+        # training / evaluation cells of the learned preconditioner: the 8-atom cubic cell with a
+        # seeded symmetric strain in [-1%, 1%] and N(0, 0.05 A) displacements
+        rng = np.random.default_rng(seed)
+        e = rng.uniform(-0.01, 0.01, size=(3, 3))
+        e = 0.5 * (e + e.T)
+        cell = (np.eye(3) * 5.431 * BOHR_PER_ANGSTROM) @ (np.eye(3) + e)
+        pos = DIAMOND8 @ cell + rng.normal(0.0, 0.05 * BOHR_PER_ANGSTROM, size=(8, 3))
+        return Crystal(cell, [si], np.zeros(8, int), pos)
     if name == "al4":
         rng = np.random.default_rng(seed)
         e = rng.uniform(-0.01, 0.01, size=(3, 3))
@@ -127,6 +136,35 @@ def crystal(name: str, seed: int = 1) -> Crystal:
         occ = rng.uniform(0.0, 1.0, size=8) < x
         return Crystal(cell, [si, species("Ge")], occ.astype(int), DIAMOND8 @ cell)
     raise KeyError(name)
+
+
+# Width (bohr) of the Gaussian atomic valence density of the synthetic species (the UPF PP_RHOATOM
+# they lack): rho_atom(r) = Z / (pi^{3/2} a^3) exp(-r^2 / a^2), form factor Z exp(-G^2 a^2 / 4).
+ATOM_DENSITY_WIDTH = {"Si": 1.55, "Ge": 1.65, "Al": 1.75}
+
+
+def atomic_density_channels(c: "Crystal", dims) -> np.ndarray:
+    """Superposition of atomic valence densities on the FFT grid (x fastest), one channel per
+    species group: [0] all species except Ge, [1] Ge.  build_atomic_density (scf/core_density.zig:
+    128-183): rho(G) = (1/Omega) sum_atoms f(|G|) exp(-i G . R), inverse FFT to real space."""
+    nx, ny, nz = dims
+    f = [np.fft.fftfreq(n, 1.0 / n) for n in dims]
+    hz, hy, hx = np.meshgrid(f[2], f[1], f[0], indexing="ij")
+    hkl = np.stack([hx.ravel(), hy.ravel(), hz.ravel()], axis=1)
+    G = hkl @ c.recip
+    g2 = (G * G).sum(axis=1)
+    out = np.zeros((2, nx * ny * nz))
+    for ch in range(2):
+        rho_g = np.zeros(nx * ny * nz, dtype=np.complex128)
+        for a, s in enumerate(c.atom_species):
+            sp = c.species[s]
+            if (sp.name == "Ge") != (ch == 1):
+                continue
+            w = ATOM_DENSITY_WIDTH.get(sp.name, 1.6)
+            rho_g += sp.z_val * np.exp(-g2 * w * w / 4.0) * np.exp(-1j * (G @ c.positions[a]))
+        rho_g /= c.volume
+        out[ch] = np.fft.ifftn(rho_g.reshape(nz, ny, nx)).ravel().real * (nx * ny * nz)
+    return out
 
 
 def _smooth235(n):

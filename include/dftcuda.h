@@ -110,6 +110,20 @@ int dftcuda_apply_h_batch_async(dftcuda_kctx* ctx, const double* x_dev, double* 
 /* Re <psi_b|V_nl|psi_b> for nbands columns (kpoint/density.zig:145-165, 238-266). Host or device. */
 int dftcuda_nonlocal_energies(dftcuda_kctx* ctx, const double* psi, size_t n, size_t nbands, double* e_out);
 
+/* Autotuner: times candidate launch configurations of this context's H|psi> on ncols trial
+ * columns (FFT pass variant, column-chunk workspace budget, split-K of the two projector GEMMs)
+ * with CUDA events and keeps the fastest for all later calls.  report may be NULL. */
+typedef struct dftcuda_tune_report {
+  int fft_path;          /* 1 four-step register FFT passes, 0 generic shared-memory passes */
+  double box_budget_mb;  /* active-plane workspace budget per column chunk */
+  int proj_splits;       /* split-K of the projection GEMM (0 = built-in heuristic) */
+  int back_splits;       /* split-K of the back-projection GEMM (0 = built-in heuristic) */
+  double default_ms;     /* H|psi> on ncols columns with the built-in defaults */
+  double tuned_ms;       /* the same with the chosen configuration */
+  int candidates;        /* configurations timed */
+} dftcuda_tune_report;
+int dftcuda_kctx_autotune(dftcuda_kctx* ctx, size_t ncols, dftcuda_tune_report* report);
+
 /* ------------------------------------------------------------------------------------------
  * Eigensolver: lobpcg_serial.solve (src/features/linalg/lobpcg/serial.zig:55-307) with
  * Options (lobpcg/common.zig:44-52).  The whole Davidson loop runs on the device; H is the
@@ -136,6 +150,56 @@ typedef struct dftcuda_eig_info {
 int dftcuda_eig_solve(dftcuda_kctx* ctx, const double* diag, size_t nbands, const dftcuda_eig_opts* opts,
                       const double* init_vecs, size_t init_cols, double* values_out, double* vectors_out,
                       dftcuda_eig_info* info);
+
+/* The same solver for nk k-point contexts at once (the k-point loop of kpoint/workers.zig:133-180):
+ * the runs advance in lockstep, each on its own context's stream, with one host synchronisation per
+ * phase for all of them, so the GPU overlaps the k-points' kernels.  Per-k arrays of length nk:
+ * diags[k] (n_k), init_vecs (NULL, or per-k pointers that may be NULL) with init_cols, values_out[k]
+ * (nbands), vectors_out[k] (n_k x nbands); infos: NULL or nk entries.  Each context at most once. */
+int dftcuda_eig_solve_batch(size_t nk, dftcuda_kctx* const* ctxs, const double* const* diags, size_t nbands,
+                            const dftcuda_eig_opts* opts, const double* const* init_vecs, const size_t* init_cols,
+                            double* const* values_out, double* const* vectors_out, dftcuda_eig_info* infos);
+
+/* Preconditioner of the Davidson correction step for this context's solves:
+ *  REFERENCE  q_i = r_i / (diag_i - lambda_b), |den| >= 1e-8 (lobpcg/common.zig:214-226), the default;
+ *  TPA        Teter-Payne-Allan K(|k+G_i|^2 / E_kin,b) r_i;
+ *  MLP        a learned per-plane-wave multiplier m(|k+G|^2 / E_kin, |r_i| / rms(r), iteration) r_i:
+ *             a 3-64-64-1 tanh MLP with softplus output, FP32, params[DFTCUDA_PRECOND_MLP_PARAMS] in
+ *             the order W1[64][3], b1[64], W2[64][64], b2[64], w3[64], b3 (host or device).
+ * diag passed to dftcuda_eig_solve must be the kinetic energies |k+G|^2 for TPA and MLP. */
+#define DFTCUDA_PRECOND_REFERENCE 0
+#define DFTCUDA_PRECOND_TPA 1
+#define DFTCUDA_PRECOND_MLP 2
+#define DFTCUDA_PRECOND_MLP_PARAMS 4481
+int dftcuda_kctx_set_preconditioner(dftcuda_kctx* ctx, int kind, const float* params, size_t nparams);
+
+/* Training of the learned preconditioner on the GPU.  Samples are bands b = 0..nbands-1 whose
+ * plane waves occupy [band_off[b], band_off[b+1]) of npw rows: feat[3 npw] the MLP inputs above,
+ * cc[2 npw] = conj(r_i) delta_i (complex, interleaved), w[npw] = |r_i|^2, dnorm[nbands] = ||delta_b||^2,
+ * delta the correction from the Ritz vector to the converged eigenvector.  Loss (scale-free, as the
+ * Davidson step is) L = mean_b [1 - |sum m_i cc_i|^2 / (sum m_i^2 w_i * dnorm_b)].
+ * loss_grad: L and dL/dparams for the given params.  train: `steps` full-batch Adam steps (beta
+ * 0.9 / 0.999) with learning rate lr, params updated in place, loss_history[steps] (may be NULL). */
+int dftcuda_precond_mlp_loss_grad(size_t nbands, size_t npw, const int* band_off, const float* feat, const float* cc,
+                                  const float* w, const float* dnorm, const float* params, double* loss, float* grad);
+int dftcuda_precond_mlp_train(size_t nbands, size_t npw, const int* band_off, const float* feat, const float* cc,
+                              const float* w, const float* dnorm, float* params, size_t steps, float lr,
+                              double* loss_history);
+
+/* Learned first SCF density: a Fourier neural operator (4 Fourier layers, 16 modes per axis, 8
+ * channels, FP32) from the superposition-of-atoms density to (rho_scf - rho_atomic) / mean density,
+ * both on the cell's FFT grid (x fastest, every axis >= 16).  u: 2 channels [2][nx ny nz], the
+ * Si-like and Ge-like atomic superposition densities divided by the mean valence density.
+ * params[DFTCUDA_FNO_PARAMS]: P[8][2], p[8], then per layer R[4096][8][8] complex, W[8][8], b[8],
+ * then q[8], q0.  Samples of a training set: dims[3 s], grid-point offsets offs[s+1] (u for sample s
+ * at u + 2 offs[s], target at target + offs[s]).  Loss: mean over samples of the mean squared error.
+ * train: `steps` full-batch Adam steps, params updated in place.  Host or device pointers. */
+#define DFTCUDA_FNO_PARAMS 2097473
+int dftcuda_fno_forward(int nx, int ny, int nz, const float* u, const float* params, float* out);
+int dftcuda_fno_loss_grad(size_t nsamples, const int* dims, const size_t* offs, const float* u, const float* target,
+                          const float* params, double* loss, float* grad);
+int dftcuda_fno_train(size_t nsamples, const int* dims, const size_t* offs, const float* u, const float* target,
+                      float* params, size_t steps, float lr, double* loss_history);
 
 /* Dense Hermitian eigensolver: linalg.hermitian_eigen_decomp (src/features/linalg/linalg.zig:141-151;
  * zheev 'V','U' in hermitian_eigen_decomp_lapack) and lobpcg/common.zig:440-508, restricted to the

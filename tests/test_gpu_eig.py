@@ -106,3 +106,29 @@ def test_not_converged_returns_best_estimate(dz):
     assert not r.converged and r.iterations == 1
     assert np.all(np.isfinite(r.values))
     kc.close()
+
+
+def test_batch_matches_independent_solves(dz):
+    """dftcuda_eig_solve_batch on k-points with different n_pw (Si8, 751 / 762 / 765 / 740 plane
+    waves at 12 Ry) against one dftcuda_eig_solve per k-point: the same iteration counts and
+    eigenvalues (the runs share no data; only their order on the GPU differs)."""
+    ks = [(0.0, 0.0, 0.0), (0.125, 0.25, 0.0), (0.375, 0.125, 0.25), (0.5, 0.5, 0.25)]
+    kps = [kproblem("si8", 12.0, k) for k in ks]
+    assert len({kp.ctx.n for kp in kps}) > 1
+    opts = dict(max_iter=200, tol=1e-8)
+    nb = 16
+    single = []
+    for kp in kps:
+        kc = make_context(dz, kp)
+        single.append(kc.hermitian_eigen_decomp_iterative(kp.ctx.basis.kinetic, nb, dz.Options(**opts)))
+        kc.close()
+    ctxs = [make_context(dz, kp) for kp in kps]
+    batch = dz.hermitian_eigen_decomp_iterative_batch(ctxs, [kp.ctx.basis.kinetic for kp in kps], nb, dz.Options(**opts))
+    for kc in ctxs:
+        kc.close()
+    for a, b, kp in zip(single, batch, kps):
+        assert b.converged
+        assert a.iterations == b.iterations and a.h_applies == b.h_applies
+        assert np.abs(a.values - b.values).max() < 1e-12
+        dense = np.linalg.eigvalsh(kp.ctx.dense_hamiltonian())[:nb]
+        assert np.abs(b.values - dense).max() < 1e-7

@@ -151,3 +151,16 @@ def test_both_fft_paths_match_oracle(dz, monkeypatch, path, name, ecut, k, prec)
     ref = odens.accumulate_density(kp.grid, kp.ctx.map, x, w, 1.0 / kp.grid.volume)
     assert rel_err(rho, ref) < (1e-12 if prec == 0 else 5e-5)
     kc.close()
+
+
+def test_autotune_keeps_results(dz):
+    """The autotuner times launch configurations on the context's own data; whatever it picks, H|psi>
+    still matches the oracle at the FP64 bar."""
+    kp = kproblem("si8", 20.0, (0.25, 0.0, 0.0))
+    kc = make_context(dz, kp)
+    rep = kc.autotune(48)
+    assert rep["candidates"] >= 4 and rep["tuned_ms"] <= rep["default_ms"] + 1e-9
+    assert rep["fft_path"] in (0, 1) and rep["box_budget_mb"] > 0
+    x = random_block(kp.ctx.n, 48, 5)
+    assert rel_err(kc.apply_hamiltonian_batched(x), kp.ctx.apply_batch(x)) < 1e-11
+    kc.close()

@@ -1,0 +1,92 @@
+"""Learned preconditioner on the GPU: the CUDA forward/backward kernels against the CPU oracle
+(oracle/learned.py, itself checked against finite differences), training reduces the loss, and every
+preconditioner kind converges the Davidson solver to the same eigenvalues."""
+import numpy as np
+import pytest
+
+from oracle import learned
+from tests.helpers import kproblem, make_context
+
+pytestmark = pytest.mark.gpu
+
+
+def test_loss_and_gradient_match_oracle(dz):
+    off, feat, cc, w, dnorm = learned.random_problem(nbands=9, per_band=(100, 300), seed=5)
+    p = learned.init_params(seed=3)
+    # the GPU computes in FP32 from FP32 inputs: give the oracle the same rounded inputs
+    f32 = lambda a: np.asarray(a, np.float32).astype(np.float64)
+    cc32 = f32(cc.real) + 1j * f32(cc.imag)
+    L_ref, g_ref = learned.loss_grad(f32(p), off, f32(feat), cc32, f32(w), f32(dnorm))
+    L, g = dz.precond_mlp_loss_grad(p, off, feat, cc, w, dnorm)
+    assert abs(L - L_ref) < 1e-5
+    assert np.abs(g - g_ref).max() < 2e-4 * np.abs(g_ref).max()
+
+
+def test_training_reduces_loss(dz):
+    off, feat, cc, w, dnorm = learned.random_problem(nbands=24, per_band=(200, 400), seed=6)
+    p0 = learned.init_params(seed=4)
+    p, hist = dz.precond_mlp_train(p0, off, feat, cc, w, dnorm, steps=200, lr=3e-3)
+    assert hist[-1] < 0.8 * hist[0]
+    L_final, _ = dz.precond_mlp_loss_grad(p, off, feat, cc, w, dnorm)
+    assert L_final <= hist[-1] + 1e-6
+
+
+@pytest.mark.parametrize("kind", ["tpa", "mlp"])
+def test_preconditioners_reach_the_same_eigenvalues(dz, kind):
+    kp = kproblem("si8", 12.0, (0.25, 0.0, 0.0))
+    diag = kp.ctx.basis.kinetic
+    opts = dz.Options(max_iter=200, tol=1e-8)
+    kc = make_context(dz, kp)
+    ref = kc.hermitian_eigen_decomp_iterative(diag, 16, opts)
+    if kind == "tpa":
+        kc.set_preconditioner(dz.PRECOND_TPA)
+    else:
+        kc.set_preconditioner(dz.PRECOND_MLP, learned.init_params(seed=7).astype(np.float32))
+    alt = kc.hermitian_eigen_decomp_iterative(diag, 16, opts)
+    kc.close()
+    assert ref.converged and alt.converged
+    assert np.abs(ref.values - alt.values).max() < 1e-7
+
+
+def test_preconditioner_argument_errors(dz):
+    kp = kproblem("si2", 10.0)
+    kc = make_context(dz, kp)
+    with pytest.raises(dz.InvalidArgument):
+        kc.set_preconditioner(dz.PRECOND_MLP, np.zeros(10, np.float32))
+    with pytest.raises(dz.InvalidArgument):
+        kc.set_preconditioner(7)
+    kc.close()
+
+
+# ---- Fourier neural operator ----------------------------------------------------------------------
+
+
+def _fno_samples(seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for dims in ((16, 16, 18), (20, 16, 16)):
+        n = int(np.prod(dims))
+        u = rng.random((2, n))
+        out.append((dims, u, 0.1 * rng.normal(size=n)))
+    return out
+
+
+def test_fno_forward_and_gradient_match_autograd_oracle(dz):
+    samples = _fno_samples(1)
+    p = learned.fno_init_params(2)
+    f32 = lambda a: np.asarray(a, np.float32).astype(np.float64)
+    L_ref, g_ref = learned.fno_loss_grad(f32(p), [(d, f32(u), f32(t)) for d, u, t in samples])
+    L, g = dz.fno_loss_grad(p, samples)
+    assert abs(L - L_ref) < 1e-5 * max(1.0, L_ref)
+    assert np.abs(g - g_ref).max() < 1e-3 * np.abs(g_ref).max()
+    import torch
+    d0 = learned.fno_forward_torch(torch.tensor(f32(p)), f32(samples[0][1]), samples[0][0]).numpy()
+    out = dz.fno_forward(p, samples[0][1], samples[0][0])
+    assert np.abs(out - d0).max() < 1e-4 * max(1.0, np.abs(d0).max())
+
+
+def test_fno_training_reduces_loss(dz):
+    samples = _fno_samples(3)
+    p0 = learned.fno_init_params(4)
+    p, hist = dz.fno_train(p0, samples, steps=60, lr=2e-3)
+    assert hist[-1] < 0.7 * hist[0]
