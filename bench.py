@@ -53,7 +53,10 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile-case", action="store_true", help="small single-k case for ncu captures: Gamma, 32 columns, 2 applications")
-    ap.add_argument("--workload", choices=("hpsi", "scf"), default="hpsi", help="hpsi: H|psi> GB/s (default); scf: time-to-SCF")
+    ap.add_argument("--workload", choices=("hpsi", "scf", "scf64", "cells"), default="hpsi",
+                    help="hpsi: H|psi> GB/s (default); scf: time-to-SCF Si2; scf64: time-to-SCF Si64, mixed vs FP64; "
+                         "cells: many-cell SiGe8 SCF throughput, atomic vs learned start")
+    ap.add_argument("--cells", type=int, default=16, help="cells of the many-cell workload")
     ap.add_argument("--precision", choices=("fp64", "fp32", "tf32"), default="fp64", help="context precision of --profile-case")
     return ap.parse_args()
 
@@ -509,10 +512,112 @@ def run_scf_workload(args):
     print(json.dumps(line), flush=True)
 
 
+def run_scf64_workload(args):
+    """Time-to-SCF on Si64 (2x2x2 conventional, N(0, 0.02 A) displacements, seed 1), 30 Ry, 75^3,
+    2x2x2 MP (8 k), 160 bands, Fermi-Dirac 0.01 Ry, LDA-PZ, Pulay 8 / beta 0.3, the reference's
+    eigensolver defaults.  Target: a tight FP64 run (density RMS 1e-8).  Reported: wall seconds until
+    |E - E_target| < 1e-6 Ry/atom, plain FP64 and mixed (TF32X3 contexts until the density residual
+    is below 1e-5 or stalls, then FP64)."""
+    import importlib
+
+    import torch
+
+    import dftzig_loader
+
+    dz = dftzig_loader.load()
+    scf = importlib.import_module("dftzig_b200.scf")
+    system = importlib.import_module("dftzig_b200.system")
+    c = system.crystal("si64", 1)
+    base = dict(ecut=30.0, kmesh=(2, 2, 2), nbands=160, mixing_beta=0.3, pulay_history=8, max_iter=60, smearing=0.01)
+    b = scf.GpuBackend(dz, "fp64")
+    ref = scf.run_scf(c, scf.ScfParams(**base, convergence=1e-8), b)
+    b.close()
+    out = {}
+    for mode in ("fp64", "mixed"):
+        p = scf.ScfParams(**base, convergence=1e-12, energy_target=ref.energy, energy_tol_per_atom=1e-6)
+        torch.cuda.synchronize()
+        b = scf.GpuBackend(dz, mode)
+        r = scf.run_scf(c, p, b)
+        torch.cuda.synchronize()
+        b.close()
+        if not r.converged:
+            raise RuntimeError(f"time-to-SCF run ({mode}) did not reach the target")
+        out[mode] = (r.wall_s, r.iterations, r.energy_per_atom - ref.energy_per_atom, getattr(b, "switched_at", None))
+    line = {
+        "metric": "time-to-SCF (|dE| < 1e-6 Ry/atom vs tight FP64), Si64 30 Ry 2x2x2, mixed precision",
+        "value": round(out["mixed"][0], 3),
+        "unit": "s",
+        "higher_is_better": False,
+        "n_gpus": 1,
+        "steps": 1,
+        "dtype": "f64/f32/tf32x3",
+        "data": "synthetic (seeded displacements; synthetic GTH-form Si pseudopotential)",
+        "config": {"workload": "Si64 2x2x2 conventional, sigma 0.02 A (seed 1), 30 Ry, 75^3, 2x2x2 MP (8 k), 160 bands, FD 0.01 Ry",
+                   "target_energy_per_atom": ref.energy_per_atom, "target_iterations": ref.iterations},
+        "fp64": {"seconds": round(out["fp64"][0], 3), "scf_iterations": out["fp64"][1], "dE_per_atom": out["fp64"][2]},
+        "mixed": {"seconds": round(out["mixed"][0], 3), "scf_iterations": out["mixed"][1], "dE_per_atom": out["mixed"][2],
+                  "switched_to_fp64_at_iteration": out["mixed"][3]},
+        "speedup_mixed_vs_fp64": round(out["fp64"][0] / out["mixed"][0], 3),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_cells_workload(args):
+    """Many-cell SCF throughput on seeded SiGe8 cells (x ~ U(0,1), Vegard lattice 5.43-5.66 A,
+    +-2% strain; seeds 2400..), 20 Ry, 2x2x2 MP, 20 bands, FD 0.005 Ry: all cells' k-points go
+    through one lockstep eigensolver batch per SCF iteration.  Atomic-superposition start against
+    the learned (FNO) start; cells per second = cells / wall time to convergence (RMS drho 1e-6)."""
+    import importlib
+
+    import dftzig_loader
+
+    dz = dftzig_loader.load()
+    scf = importlib.import_module("dftzig_b200.scf")
+    system = importlib.import_module("dftzig_b200.system")
+    learn = importlib.import_module("dftzig_b200.learn")
+    cells = [system.crystal("sige8", 2400 + i) for i in range(args.cells)]
+    ecut = 20.0
+    p = scf.ScfParams(ecut=ecut, kmesh=(2, 2, 2), nbands=20, convergence=1e-6, max_iter=80, smearing=learn.FNO_SMEARING)
+    starts = {"atomic": [], "fno": []}
+    params = learn.load_fno_weights()
+    for c in cells:
+        dims, u, rho_at, mean = learn.fno_input(c, ecut)
+        starts["atomic"].append(rho_at * (c.nelec / (rho_at.mean() * c.volume)))
+        starts["fno"].append(learn.fno_initial_density(dz, params, c, ecut))
+    out = {}
+    for name in ("atomic", "fno"):
+        # the learned start skips the loose-tolerance warm-up iterations meant for poor densities
+        pn = p if name == "atomic" else scf.ScfParams(**{**p.__dict__, "warmup_steps": 0})
+        res, wall = scf.run_scf_many(dz, cells, pn, "fp64", starts[name])
+        out[name] = {"seconds": round(wall, 3), "cells_per_second": round(len(cells) / wall, 3),
+                     "mean_scf_iterations": float(np.mean([r.iterations for r in res])),
+                     "all_converged": all(r.converged for r in res)}
+    line = {
+        "metric": "many-cell SCF throughput (cells/s), SiGe8 20 Ry 2x2x2, learned FNO start",
+        "value": out["fno"]["cells_per_second"],
+        "unit": "cells/s",
+        "higher_is_better": True,
+        "n_gpus": 1,
+        "steps": 1,
+        "dtype": "f64 (FNO f32)",
+        "data": "synthetic seeded SiGe8 cells (synthetic GTH-form Si and Ge pseudopotentials)",
+        "config": {"workload": f"{len(cells)} SiGe8 cells, 20 Ry, 2x2x2 MP (8 k), 20 bands, FD 0.005 Ry, lockstep batch", "cells": len(cells)},
+        "atomic_start": out["atomic"],
+        "fno_start": out["fno"],
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "scf":
         run_scf_workload(args)
+        return
+    if args.workload == "scf64":
+        run_scf64_workload(args)
+        return
+    if args.workload == "cells":
+        run_cells_workload(args)
         return
     if args.profile_case:
         run_profile_case(args.precision)

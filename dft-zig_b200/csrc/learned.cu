@@ -7,7 +7,8 @@
 //           (Teter, Payne, Allan, Phys. Rev. B 40, 12255 (1989)); E_kin,b = <psi_b|T|psi_b>
 //   kind 2  learned: q_i = m_theta(u_i) r_i with a per-plane-wave MLP, FP32 weights,
 //           u_i = (log(x_i + 0.05), log(|r_i| / rms(r_b) + 1e-6), t / 20), t the iteration index,
-//           h1 = tanh(W1 u + b1), h2 = tanh(W2 h1 + b2), m = softplus(w3 . h2 + b3), 3 -> 64 -> 64 -> 1.
+//           h1 = tanh(W1 u + b1), h2 = tanh(W2 h1 + b2), z = w3 . h2 + b3 (3 -> 64 -> 64 -> 1),
+//           m = K(x_i) exp(clamp(z, -8, 8)): a learned refinement of Teter-Payne-Allan.
 //
 // Training (dftcuda_precond_mlp_loss_grad / _train): samples are bands b with plane-wave data
 // c_i = conj(r_i) delta_i, w_i = |r_i|^2 and D_b = ||delta_b||^2, where delta is the correction that
@@ -35,8 +36,16 @@ constexpr int MLP_OFF_B3 = MLP_OFF_W3 + MLP_H;
 constexpr int MLP_NPARAM = MLP_OFF_B3 + 1;  // 4481
 static_assert(MLP_NPARAM == DFTCUDA_PRECOND_MLP_PARAMS, "parameter count");
 
-__device__ __forceinline__ float softplusf(float z) { return z > 20.f ? z : log1pf(expf(z)); }
-__device__ __forceinline__ float sigmoidf(float z) { return 1.f / (1.f + expf(-z)); }
+// The learned multiplier refines Teter-Payne-Allan: m = K(x) exp(clamp(z)), x = exp(u0) - 0.05 the
+// kinetic ratio recovered from the first feature; with zero output weights the network is TPA.
+__device__ __forceinline__ double tpa_k(double x) {
+  const double num = 27.0 + x * (18.0 + x * (12.0 + 8.0 * x));
+  return num / (num + 16.0 * x * x * x * x);
+}
+__device__ __forceinline__ float zclamp(float z) { return fminf(fmaxf(z, -8.f), 8.f); }
+__device__ __forceinline__ double mlp_multiplier(float u0, float z) {
+  return tpa_k(fmax(exp((double)u0) - 0.05, 0.0)) * exp((double)zclamp(z));
+}
 
 // Forward for one input with the parameters in shared memory; returns z (before softplus) and
 // optionally the two hidden layers.
@@ -117,7 +126,7 @@ __global__ void __launch_bounds__(256) k_precondition_mlp(double2* __restrict__ 
   const double2 v = res[(long)b * n + i];
   float u[3];
   mlp_features(kin[i], ekin[j], sqrt(v.x * v.x + v.y * v.y), norms[b] / sqrt((double)n), t, u);
-  const double m = (double)softplusf(mlp_forward(p, u, nullptr, nullptr));
+  const double m = mlp_multiplier(u[0], mlp_forward(p, u, nullptr, nullptr));
   Q[idx] = make_double2(v.x * m, v.y * m);
 }
 
@@ -139,7 +148,7 @@ __global__ void __launch_bounds__(256) k_mlp_band_sums(const int* __restrict__ o
   double ar = 0.0, ai = 0.0, q = 0.0;
   for (int i = off[b] + threadIdx.x; i < off[b + 1]; i += blockDim.x) {
     const float u[3] = {feat[3 * i], feat[3 * i + 1], feat[3 * i + 2]};
-    const double m = (double)softplusf(mlp_forward(p, u, nullptr, nullptr));
+    const double m = mlp_multiplier(u[0], mlp_forward(p, u, nullptr, nullptr));
     ar += m * cc[i].x;
     ai += m * cc[i].y;
     q += m * m * w[i];
@@ -204,11 +213,12 @@ __global__ void __launch_bounds__(BW_TILE) k_mlp_backward(const int* __restrict_
       u[1] = feat[3 * i + 1];
       u[2] = feat[3 * i + 2];
       const float z = mlp_forward(p, u, h1, h2);
-      const double m = (double)softplusf(z);
-      // dL/dm_i = -(2 / (D Q)) [Re(conj(A) c_i) - (|A|^2 / Q) m_i w_i], times 1/B
+      const double m = mlp_multiplier(u[0], z);
+      // dL/dm_i = -(2 / (D Q)) [Re(conj(A) c_i) - (|A|^2 / Q) m_i w_i], times 1/B; dm/dz = m
+      // inside the clamp, 0 outside
       const double re = Ar * cc[i].x + Ai * cc[i].y;
       const double dm = -2.0 / (Db * Qb) * (re - A2 / Qb * m * w[i]) * scale;
-      dz = (float)(dm * (double)sigmoidf(z));
+      dz = (z > -8.f && z < 8.f) ? (float)(dm * m) : 0.f;
     } else {
       for (int j = 0; j < MLP_H; ++j) h1[j] = h2[j] = 0.f;
     }

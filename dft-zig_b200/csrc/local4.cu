@@ -13,6 +13,8 @@
 //                straight into the output column.
 //  k_xline_density4  inverse x transform and sum_b w_b |psi_b|^2 / Omega in registers.
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 #include <cmath>
 #include <mutex>
 #include <vector>
@@ -247,6 +249,194 @@ __global__ void __launch_bounds__(512) k_plane_fwd4(const cplx<T>* __restrict__ 
   }
 }
 
+// Single-buffer plane passes: every four-step phase works in place.  Step B of a transform writes
+// its N2 outputs for row (or column) k1 into the slots k1 N2 + k2 it read, i.e. frequency
+// k1 + N1 k2 sits at index perm(f) = (f mod N1) N2 + f / N1; later phases either work per row /
+// column (where the order does not matter) or un-permute when they read or write HBM.  One P-sized
+// shared buffer instead of two: two CTAs per SM at 75^2 in FP64, and planes up to 119^2 fit.
+constexpr int kPlaneThreads = 384;  // two CTAs per SM at <= 85 registers
+// Two CTAs per SM where two planes fit the 227 KB of shared memory; otherwise one, with the whole
+// register file for it.
+template <typename T, int NP> __host__ __device__ constexpr int plane_min_ctas() {
+  return sizeof(cplx<T>) * NP * NP <= 113 * 1024 ? 2 : 1;
+}
+
+template <int NP> __device__ __forceinline__ int dperm(int f) {
+  constexpr int N1 = Split<NP>::N1, N2 = Split<NP>::N2;
+  return (f % N1) * N2 + f / N1;
+}
+
+template <typename T, int NP>
+__global__ void __launch_bounds__(kPlaneThreads, plane_min_ctas<T, NP>()) k_plane_inv5(const double2* __restrict__ x, long npw, cplx<T>* __restrict__ W,
+                                                    int n_act, const int* __restrict__ pwmap,
+                                                    const int* __restrict__ stick_off, const int* __restrict__ stick_y,
+                                                    const cplx<T>* __restrict__ tw) {
+  using C = cplx<T>;
+  constexpr int N1 = Split<NP>::N1, N2 = Split<NP>::N2, P = NP * NP;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* S = reinterpret_cast<C*>(smraw);
+  int* sy = reinterpret_cast<int*>(S + P);
+  unsigned char* isst = reinterpret_cast<unsigned char*>(sy + NP);
+  const int slot = blockIdx.x;
+  const long b = blockIdx.y;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int s0 = stick_off[slot], ns = stick_off[slot + 1] - s0;
+  for (int i = tid; i < NP; i += nt) isst[i] = 0;
+  __syncthreads();
+  for (int i = tid; i < ns; i += nt) {
+    const int y = stick_y[s0 + i];
+    sy[i] = y;
+    isst[y] = 1;
+  }
+  __syncthreads();
+  const int* pm = pwmap + (long)slot * P;
+  const double2* xb = x + b * npw;
+  // z transform, step A: thread (t, stick), rows k1 N2 + t of column y
+  for (int w = tid; w < N2 * ns; w += nt) {
+    const int s = w % ns, t = w / ns, y = sy[s];
+    C v[N1];
+#pragma unroll
+    for (int j = 0; j < N1; ++j) {
+      const int idx = __ldg(pm + (j * N2 + t) * NP + y);
+      if (idx >= 0) {
+        const double2 c = __ldg(xb + idx);
+        v[j] = mk<C>(c.x, c.y);
+      } else {
+        v[j] = mk<C>(0.0, 0.0);
+      }
+    }
+    RegDft<T, N1>::run(v, (T)1);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1)
+      if (t) v[k1] = cmul(v[k1], tw_ld<T>(tw, (t * k1) % NP, (T)1));
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) S[(k1 * N2 + t) * NP + y] = v[k1];
+  }
+  __syncthreads();
+  // z transform, step B in place: z frequency k1 + N1 k2 lands in row k1 N2 + k2
+  for (int w = tid; w < N1 * ns; w += nt) {
+    const int s = w % ns, k1 = w / ns, y = sy[s];
+    C u[N2];
+#pragma unroll
+    for (int t = 0; t < N2; ++t) u[t] = S[(k1 * N2 + t) * NP + y];
+    RegDft<T, N2>::run(u, (T)1);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) S[(k1 * N2 + k2) * NP + y] = u[k2];
+  }
+  __syncthreads();
+  // y transform, step A in place on every row r (a permuted z); columns without plane waves are zero
+  for (int w = tid; w < N2 * NP; w += nt) {
+    const int t = w % N2, r = w / N2;
+    C v[N1];
+#pragma unroll
+    for (int j = 0; j < N1; ++j) {
+      const int y = j * N2 + t;
+      v[j] = isst[y] ? S[r * NP + y] : mk<C>(0.0, 0.0);
+    }
+    RegDft<T, N1>::run(v, (T)1);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1)
+      if (t) v[k1] = cmul(v[k1], tw_ld<T>(tw, (t * k1) % NP, (T)1));
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) S[r * NP + k1 * N2 + t] = v[k1];
+  }
+  __syncthreads();
+  // y transform, step B: thread (k1, row); the plane to HBM in natural (z, y) order
+  C* Wp = W + (b * n_act + slot) * (long)P;
+  for (int w = tid; w < N1 * NP; w += nt) {
+    const int k1 = w % N1, r = w / N1;
+    const int z = (r / N2) + N1 * (r % N2);
+    C u[N2];
+#pragma unroll
+    for (int t = 0; t < N2; ++t) u[t] = S[r * NP + k1 * N2 + t];
+    RegDft<T, N2>::run(u, (T)1);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) Wp[z * NP + k1 + N1 * k2] = u[k2];
+  }
+}
+
+template <typename T, int NP>
+__global__ void __launch_bounds__(kPlaneThreads, plane_min_ctas<T, NP>()) k_plane_fwd5(const cplx<T>* __restrict__ W, int n_act, const int* __restrict__ pwmap,
+                                                    const int* __restrict__ stick_off, const int* __restrict__ stick_y,
+                                                    const cplx<T>* __restrict__ tw, const double2* __restrict__ x,
+                                                    double2* __restrict__ y_out, long npw,
+                                                    const double* __restrict__ kinetic, double invN) {
+  using C = cplx<T>;
+  constexpr int N1 = Split<NP>::N1, N2 = Split<NP>::N2, P = NP * NP;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* S = reinterpret_cast<C*>(smraw);
+  int* sy = reinterpret_cast<int*>(S + P);
+  const int slot = blockIdx.x;
+  const long b = blockIdx.y;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int s0 = stick_off[slot], ns = stick_off[slot + 1] - s0;
+  const C* Wp = W + (b * n_act + slot) * (long)P;
+  for (int i = tid; i < P; i += nt) S[i] = Wp[i];
+  for (int i = tid; i < ns; i += nt) sy[i] = stick_y[s0 + i];
+  __syncthreads();
+  // y transform, step A in place: thread (t, z)
+  for (int w = tid; w < N2 * NP; w += nt) {
+    const int t = w % N2, z = w / N2;
+    C v[N1];
+#pragma unroll
+    for (int j = 0; j < N1; ++j) v[j] = S[z * NP + j * N2 + t];
+    RegDft<T, N1>::run(v, (T)-1);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1)
+      if (t) v[k1] = cmul(v[k1], tw_ld<T>(tw, (t * k1) % NP, (T)-1));
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) S[z * NP + k1 * N2 + t] = v[k1];
+  }
+  __syncthreads();
+  // y transform, step B in place: y frequency k1 + N1 k2 lands in column k1 N2 + k2
+  for (int w = tid; w < N1 * NP; w += nt) {
+    const int k1 = w % N1, z = w / N1;
+    C u[N2];
+#pragma unroll
+    for (int t = 0; t < N2; ++t) u[t] = S[z * NP + k1 * N2 + t];
+    RegDft<T, N2>::run(u, (T)-1);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) S[z * NP + k1 * N2 + k2] = u[k2];
+  }
+  __syncthreads();
+  // z transform, step A in place on the stick columns (stick y sits at column dperm(y))
+  for (int w = tid; w < N2 * ns; w += nt) {
+    const int s = w % ns, t = w / ns, col = dperm<NP>(sy[s]);
+    C v[N1];
+#pragma unroll
+    for (int j = 0; j < N1; ++j) v[j] = S[(j * N2 + t) * NP + col];
+    RegDft<T, N1>::run(v, (T)-1);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1)
+      if (t) v[k1] = cmul(v[k1], tw_ld<T>(tw, (t * k1) % NP, (T)-1));
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) S[(k1 * N2 + t) * NP + col] = v[k1];
+  }
+  __syncthreads();
+  // z transform, step B: thread (k1, stick); gather x 1/N plus kinetic into the output column
+  const int* pm = pwmap + (long)slot * P;
+  for (int w = tid; w < N1 * ns; w += nt) {
+    const int s = w % ns, k1 = w / ns, y = sy[s], col = dperm<NP>(y);
+    C u[N2];
+#pragma unroll
+    for (int t = 0; t < N2; ++t) u[t] = S[(k1 * N2 + t) * NP + col];
+    RegDft<T, N2>::run(u, (T)-1);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+      const int z = k1 + N1 * k2;
+      const int g = __ldg(pm + z * NP + y);
+      if (g >= 0) {
+        const double2 xv = __ldg(x + b * npw + g);
+        const double kin = __ldg(kinetic + g);
+        double2 o;
+        o.x = kin * xv.x + (double)u[k2].x * invN;
+        o.y = kin * xv.y + (double)u[k2].y * invN;
+        y_out[b * npw + g] = o;
+      }
+    }
+  }
+}
+
 template <typename T, int NX>
 __global__ void __launch_bounds__(256) k_xline4(cplx<T>* __restrict__ W, int n_act, const int* __restrict__ slot_of_x,
                                                 const T* __restrict__ Vt, int P, int ncols, int cols_per_cta,
@@ -311,6 +501,96 @@ __global__ void __launch_bounds__(256) k_xline4(cplx<T>* __restrict__ W, int n_a
   }
 }
 
+// Geometry of the warp-synchronous x-line pass: a line's x transform is done by N2 lanes of one
+// warp (LW lines per warp).  Exchange-buffer stride S >= NX with S = N2 (mod 8), so the step-A writes
+// of the N2 lanes of consecutive lines fall in distinct 16-byte bank groups.
+template <int NX> struct XLineGeom {
+  static constexpr int N1 = Split<NX>::N1, N2 = Split<NX>::N2;
+  static constexpr int LW = 32 / N2;
+  static constexpr int Q = (N1 + N2 - 1) / N2;
+  static constexpr int S = NX + ((N2 - NX) % 8 + 8) % 8;
+};
+constexpr int kXlWarps = 3;
+
+// x-line pass with every lane busy in every phase: lane t of a line
+//   1. inverse step A for index t: DFT_N1 over the inputs x = m N2 + t (the active slots),
+//   2. for its rows k1 = t, t + N2, ... < N1: inverse step B (DFT_N2), x V(r) at x = k1 + N1 k2,
+//      forward step A (DFT_N2, lengths swapped) and its twiddles,
+//   3. forward step B for frequency index t: DFT_N1, outputs x = t + N2 m back to the active slots.
+// The exchanges go through two per-warp shared buffers with __syncwarp only (no block barriers);
+// the input and output slot sets of a lane coincide ({t + N2 m}).  V(r) and the slot table are read
+// through L1 (reused by the CTA's columns) instead of being held in registers.
+template <typename T, int NX>
+__global__ void __launch_bounds__(kXlWarps * 32, 5) k_xline5(cplx<T>* __restrict__ W, int n_act, const int* __restrict__ slot_of_x,
+                                                             const T* __restrict__ Vt, int P, int ncols, int cols_per_cta,
+                                                             const cplx<T>* __restrict__ tw) {
+  using C = cplx<T>;
+  using G = XLineGeom<NX>;
+  constexpr int N1 = G::N1, N2 = G::N2, LW = G::LW, Q = G::Q, S = G::S;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int L = lane / N2, t = lane - L * N2;
+  const bool lane_ok = L < LW;
+  C* B1 = reinterpret_cast<C*>(smraw) + ((size_t)warp * LW + (lane_ok ? L : 0)) * S;
+  C* B2 = B1 + (size_t)kXlWarps * LW * S;
+  const int j = (blockIdx.x * kXlWarps + warp) * LW + L;
+  const bool lv = lane_ok && j < P;
+  const int c0 = blockIdx.y * cols_per_cta;
+  const int c1 = min(ncols, c0 + cols_per_cta);
+  const int* slt = slot_of_x + t;  // slot of x = t + N2 m at slt[N2 m]
+  for (int c = c0; c < c1; ++c) {
+    C* Wc = W + (long)c * n_act * P + j;
+    {  // 1. inverse step A
+      C v[N1];
+#pragma unroll
+      for (int m = 0; m < N1; ++m) {
+        const int sm = lv ? __ldg(slt + N2 * m) : -1;
+        v[m] = sm >= 0 ? Wc[(long)sm * P] : mk<C>(0.0, 0.0);
+      }
+      RegDft<T, N1>::run(v, (T)1);
+#pragma unroll
+      for (int k1 = 1; k1 < N1; ++k1)
+        if (t) v[k1] = cmul(v[k1], tw_ld<T>(tw, (t * k1) % NX, (T)1));
+      if (lane_ok) {
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) B1[k1 * N2 + t] = v[k1];
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {  // 2. inverse step B, x V(r), forward step A
+      const int k1 = t + N2 * q;
+      if (lane_ok && k1 < N1) {
+        C u[N2];
+#pragma unroll
+        for (int tt = 0; tt < N2; ++tt) u[tt] = B1[k1 * N2 + tt];
+        RegDft<T, N2>::run(u, (T)1);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) u[k2] = cscale(u[k2], lv ? __ldg(Vt + (long)(k1 + N1 * k2) * P + j) : (T)0);
+        RegDft<T, N2>::run(u, (T)-1);
+#pragma unroll
+        for (int k1f = 1; k1f < N2; ++k1f)
+          if (k1) u[k1f] = cmul(u[k1f], tw_ld<T>(tw, (k1 * k1f) % NX, (T)-1));
+#pragma unroll
+        for (int k1f = 0; k1f < N2; ++k1f) B2[k1f * N1 + k1] = u[k1f];
+      }
+    }
+    __syncwarp();
+    {  // 3. forward step B for frequency index t
+      C v[N1];
+#pragma unroll
+      for (int tf = 0; tf < N1; ++tf) v[tf] = lane_ok ? B2[t * N1 + tf] : mk<C>(0.0, 0.0);
+      RegDft<T, N1>::run(v, (T)-1);
+#pragma unroll
+      for (int m = 0; m < N1; ++m) {
+        const int sm = lv ? __ldg(slt + N2 * m) : -1;
+        if (sm >= 0) Wc[(long)sm * P] = v[m];
+      }
+    }
+    __syncwarp();
+  }
+}
+
 template <typename T, int NX>
 __global__ void __launch_bounds__(256) k_xline_density4(const cplx<T>* __restrict__ W, int n_act,
                                                         const int* __restrict__ slot_of_x, int P, int ncols,
@@ -365,22 +645,49 @@ __global__ void __launch_bounds__(256) k_xline_density4(const cplx<T>* __restric
 
 static constexpr size_t kSmem4 = 227 * 1024;
 
+// Shared memory of a plane pass: `buffers` planes of N^2 complex plus the stick list and flags.
+static size_t plane_smem_bytes(size_t cs, int N, int buffers) {
+  return buffers * cs * (size_t)N * N + sizeof(int) * N + N + 16;
+}
 template <typename T, int N>
-static size_t plane_smem() {
-  return 2 * sizeof(cplx<T>) * (size_t)N * N + sizeof(int) * N + N + 16;
+static size_t plane_smem(int buffers) {
+  return plane_smem_bytes(sizeof(cplx<T>), N, buffers);
+}
+
+// DFTCUDA_FFT4=legacy selects the earlier two-buffer plane passes and the block-barrier x-line
+// pass (for A/B measurements); the default single-buffer and warp-synchronous kernels fit planes up
+// to 119^2 in FP64.
+static bool fft4_legacy() {
+  static const bool v = [] {
+    const char* e = std::getenv("DFTCUDA_FFT4");
+    return e && std::string(e) == "legacy";
+  }();
+  return v;
 }
 
 bool kctx_fast_path_ok(const dftcuda_kctx* c, int precision) {
   if (!four_step_supported(c->nx) || !four_step_supported(c->ny) || c->ny != c->nz) return false;
   const size_t cs = precision == DFTCUDA_PRECISION_FP32 ? sizeof(float2) : sizeof(double2);
-  const size_t smem = 2 * cs * (size_t)c->P + sizeof(int) * c->ny + c->ny + 16;
-  return smem <= kSmem4;
+  return plane_smem_bytes(cs, c->ny, fft4_legacy() ? 2 : 1) <= kSmem4;
 }
 
 template <typename T, int NP>
 static int launch_plane_inv4(dftcuda_kctx* c, const double2* x, cplx<T>* W, size_t ncols, cudaStream_t s) {
+  const cplx<T>* tw5 = std::is_same<T, double>::value ? (const cplx<T>*)c->d_tw4p64 : (const cplx<T>*)c->d_tw4p32;
+  if (!fft4_legacy()) {
+    static bool attr5 = false;
+    if (!attr5) {
+      cudaFuncSetAttribute(k_plane_inv5<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem4);
+      attr5 = true;
+    }
+    dim3 g(c->n_act, (unsigned)ncols);
+    k_plane_inv5<T, NP><<<g, kPlaneThreads, plane_smem<T, NP>(1), s>>>(x, (long)c->npw, W, c->n_act, c->d_pwmap, c->d_stick_off,
+                                                              c->d_stick_y, tw5);
+    count_launch();
+    return DFTCUDA_OK;
+  }
   static bool attr = false;
-  const size_t smem = plane_smem<T, NP>();
+  const size_t smem = plane_smem<T, NP>(2);
   if (!attr) {
     cudaFuncSetAttribute(k_plane_inv4<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem4);
     attr = true;
@@ -394,8 +701,21 @@ static int launch_plane_inv4(dftcuda_kctx* c, const double2* x, cplx<T>* W, size
 template <typename T, int NP>
 static int launch_plane_fwd4(dftcuda_kctx* c, const cplx<T>* W, const double2* x, double2* y, size_t ncols,
                              cudaStream_t s) {
+  if (!fft4_legacy()) {
+    static bool attr5 = false;
+    if (!attr5) {
+      cudaFuncSetAttribute(k_plane_fwd5<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem4);
+      attr5 = true;
+    }
+    const cplx<T>* tw5 = std::is_same<T, double>::value ? (const cplx<T>*)c->d_tw4p64 : (const cplx<T>*)c->d_tw4p32;
+    dim3 g(c->n_act, (unsigned)ncols);
+    k_plane_fwd5<T, NP><<<g, kPlaneThreads, plane_smem<T, NP>(1), s>>>(W, c->n_act, c->d_pwmap, c->d_stick_off, c->d_stick_y, tw5, x, y,
+                                                              (long)c->npw, c->d_kinetic, 1.0 / (double)c->N);
+    count_launch();
+    return DFTCUDA_OK;
+  }
   static bool attr = false;
-  const size_t smem = plane_smem<T, NP>();
+  const size_t smem = plane_smem<T, NP>(2);
   if (!attr) {
     cudaFuncSetAttribute(k_plane_fwd4<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem4);
     attr = true;
@@ -410,6 +730,22 @@ static int launch_plane_fwd4(dftcuda_kctx* c, const cplx<T>* W, const double2* x
 template <typename T, int NX>
 static int launch_xline4(dftcuda_kctx* c, cplx<T>* W, size_t ncols, cudaStream_t s) {
   constexpr int N1 = Split<NX>::N1;
+  const T* vt = std::is_same<T, double>::value ? (const T*)c->d_vt : (const T*)c->d_vt32;
+  const cplx<T>* tw = std::is_same<T, double>::value ? (const cplx<T>*)c->d_tw4x64 : (const cplx<T>*)c->d_tw4x32;
+  if (!fft4_legacy()) {
+    using G = XLineGeom<NX>;
+    const size_t smem5 = 2 * sizeof(cplx<T>) * (size_t)kXlWarps * G::LW * G::S;
+    static bool attr5 = false;
+    if (!attr5) {
+      cudaFuncSetAttribute(k_xline5<T, NX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem4);
+      attr5 = true;
+    }
+    const int cpc = 4;
+    dim3 g(ceil_div(c->P, kXlWarps * G::LW), ceil_div(ncols, cpc));
+    k_xline5<T, NX><<<g, kXlWarps * 32, smem5, s>>>(W, c->n_act, c->d_slot_of_x, vt, c->P, (int)ncols, cpc, tw);
+    count_launch();
+    return DFTCUDA_OK;
+  }
   const int J = N1 > 8 ? 16 : 32;
   static bool attr = false;
   if (!attr) {
@@ -420,8 +756,6 @@ static int launch_xline4(dftcuda_kctx* c, cplx<T>* W, size_t ncols, cudaStream_t
   const int cpc = 4;
   dim3 g(ceil_div(c->P, J), ceil_div(ncols, cpc));
   dim3 b(J, N1);
-  const T* vt = std::is_same<T, double>::value ? (const T*)c->d_vt : (const T*)c->d_vt32;
-  const cplx<T>* tw = std::is_same<T, double>::value ? (const cplx<T>*)c->d_tw4x64 : (const cplx<T>*)c->d_tw4x32;
   k_xline4<T, NX><<<g, b, smem, s>>>(W, c->n_act, c->d_slot_of_x, vt, c->P, (int)ncols, cpc, tw); count_launch();
   return DFTCUDA_OK;
 }

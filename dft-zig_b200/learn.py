@@ -1,12 +1,12 @@
 """Learned components: data generation, GPU training and evaluation.
 
-Learned preconditioner (``precond``): a per-plane-wave MLP that replaces the diagonal of the
-Davidson correction step (the reference's r / (|k+G|^2 - lambda), lobpcg/common.zig:214-226; the
-Teter-Payne-Allan form is the other fixed alternative).  Training pairs come from plain runs of the
-device solver on seeded strained and displaced Si8 cells (``si8d``): the solver is deterministic
-(LCG start, serial.zig:75-95), so the run stopped after t iterations reproduces the Ritz vectors
-psi_b^t of the full run; the target is the correction delta_b = P(psi_b^inf) - psi_b^t that takes
-psi_b^t to its converged eigenspace (orthogonal to psi_b^t).  The network is trained on the GPU by
+Learned preconditioner (``precond``): a per-plane-wave MLP that refines the Teter-Payne-Allan
+diagonal of the Davidson correction step (m = K_TPA(x) exp(z_theta); the reference's own form is
+r / (|k+G|^2 - lambda), lobpcg/common.zig:214-226).  Training pairs come from TPA-preconditioned
+runs of the device solver on seeded strained and displaced Si8 cells (``si8d``): the solver is
+deterministic (LCG start, serial.zig:75-95), so the run stopped after t iterations reproduces the
+Ritz vectors psi_b^t of the full run; the target is the correction from psi_b^t to its converged
+eigenspace.  The network is trained on the GPU by
 the library's own CUDA forward/backward kernels (dftcuda_precond_mlp_train, Adam).
 
 Learned first density (``fno``): a Fourier neural operator (csrc/fno.cu) maps the superposition of
@@ -49,16 +49,20 @@ def _features(kin, ekin, rabs, rms, t):
     return np.stack([np.log(x + 0.05), np.log(rabs / max(rms, 1e-300) + 1e-6), np.full_like(x, min(t / 20.0, 2.0))], axis=1)
 
 
-def precond_samples(dz, cells, ecut: float, nbands: int, t_max: int = 8, kfrac=(0.0, 0.0, 0.0), cluster_tol: float = 1e-4):
-    """Residual -> correction samples from plain Davidson runs (one k-point per cell)."""
+def precond_samples(dz, cells, ecut: float, nbands: int, t_max: int = 20, kfrac=(0.0, 0.0, 0.0), cluster_tol: float = 1e-4,
+                    min_overlap: float = 0.5):
+    """Residual -> correction samples along Davidson trajectories preconditioned by TPA (the form
+    the network refines).  Target of band b at iteration t: delta_b = y - psi_b <psi_b|y>, y the
+    normalised projection of psi_b^t on the converged eigenspace of its group of (near-)degenerate
+    bands (gaps < cluster_tol Ry), kept when that projection has norm >= min_overlap."""
     off = [0]
     feats, ccs, ws, dns, kins, lams = [], [], [], [], [], []
     for c in cells:
         inp = sysm.kpoint_inputs(c, ecut, kfrac)
         kc = _context(dz, inp)
+        kc.set_preconditioner(dz.PRECOND_TPA)
         kin = inp.basis.kinetic
-        nconv = nbands + 4
-        conv = kc.hermitian_eigen_decomp_iterative(kin, nconv, dz.Options(max_iter=400, tol=1e-10))
+        conv = kc.hermitian_eigen_decomp_iterative(kin, nbands + 4, dz.Options(max_iter=400, tol=1e-10))
         for t in range(1, t_max + 1):
             r = kc.hermitian_eigen_decomp_iterative(kin, nbands, dz.Options(max_iter=t, tol=1e-14))
             psi = r.vectors
@@ -72,12 +76,12 @@ def precond_samples(dz, cells, ecut: float, nbands: int, t_max: int = 8, kfrac=(
                 Y = conv.vectors[cl]
                 y = Y.T @ (Y.conj() @ psi[b])
                 ny = float(np.linalg.norm(y))
-                if ny < 0.5:
+                if ny < min_overlap:
                     continue
                 y /= ny
                 delta = y - psi[b] * np.vdot(psi[b], y)
                 dn = float(np.vdot(delta, delta).real)
-                if dn < 1e-20:
+                if dn < 1e-24:
                     continue
                 ekin = float(np.sum(kin * np.abs(psi[b]) ** 2))
                 feats.append(_features(kin, ekin, np.abs(res[b]), rn / np.sqrt(len(kin)), t - 1))
@@ -88,6 +92,8 @@ def precond_samples(dz, cells, ecut: float, nbands: int, t_max: int = 8, kfrac=(
                 lams.append(float(r.values[b]))
                 off.append(off[-1] + len(kin))
         kc.close()
+    if len(off) == 1:
+        raise RuntimeError("precond_samples: no band passed the overlap test")
     return {
         "off": np.array(off, dtype=np.int32),
         "feat": np.concatenate(feats).astype(np.float32),
@@ -120,7 +126,8 @@ def fixed_loss(samples, kind: str) -> float:
 
 
 def init_params(seed: int = 0, scale: float = 0.3) -> np.ndarray:
-    """Random initial weights (layout of DFTCUDA_PRECOND_MLP_PARAMS: W1, b1, W2, b2, w3, b3)."""
+    """Initial weights (layout of DFTCUDA_PRECOND_MLP_PARAMS: W1, b1, W2, b2, w3, b3): random hidden
+    layers and a zero output layer, so the untrained preconditioner is exactly Teter-Payne-Allan."""
     H = 64
     rng = np.random.default_rng(seed)
     parts = [
@@ -128,8 +135,8 @@ def init_params(seed: int = 0, scale: float = 0.3) -> np.ndarray:
         rng.normal(0.0, scale, H),
         rng.normal(0.0, scale / np.sqrt(H), H * H),
         rng.normal(0.0, scale, H),
-        rng.normal(0.0, scale / np.sqrt(H), H),
-        [0.5],
+        np.zeros(H),
+        [0.0],
     ]
     return np.concatenate(parts).astype(np.float32)
 
@@ -189,8 +196,12 @@ def fno_initial_density(dz, params, c, ecut: float) -> np.ndarray:
     return rho * (c.nelec / (rho.mean() * c.volume))
 
 
-def _scf_params(ecut, kmesh, nbands, tol, init=None, smearing=None):
-    return scfm.ScfParams(ecut=ecut, kmesh=kmesh, nbands=nbands, convergence=tol, max_iter=80, smearing=smearing, initial_density=init)
+def _scf_params(ecut, kmesh, nbands, tol, init=None, smearing=None, warmup_steps=2):
+    return scfm.ScfParams(ecut=ecut, kmesh=kmesh, nbands=nbands, convergence=tol, max_iter=80, smearing=smearing, initial_density=init,
+                          warmup_steps=warmup_steps)
+
+
+FNO_SMEARING = 0.005  # Ry, Fermi-Dirac: random SiGe occupancies can close the gap of fixed occupations
 
 
 def fno_samples(dz, cells, ecut: float, nbands: int, kmesh=(2, 2, 2), tol: float = 1e-7):
@@ -199,7 +210,7 @@ def fno_samples(dz, cells, ecut: float, nbands: int, kmesh=(2, 2, 2), tol: float
     for c in cells:
         dims, u, rho_at, mean = fno_input(c, ecut)
         b = scfm.GpuBackend(dz, "fp64")
-        r = scfm.run_scf(c, _scf_params(ecut, kmesh, nbands, tol), b)
+        r = scfm.run_scf(c, _scf_params(ecut, kmesh, nbands, tol, smearing=FNO_SMEARING), b)
         b.close()
         out.append((dims, u, (r.rho - rho_at) / mean))
     return out
@@ -225,12 +236,16 @@ def evaluate_fno(dz, params, cells, ecut: float, nbands: int, kmesh=(2, 2, 2), t
     rows = []
     for c in cells:
         dims, u, rho_at, mean = fno_input(c, ecut)
-        starts = {"flat": None, "atomic": rho_at * (c.nelec / (rho_at.mean() * c.volume)), "fno": fno_initial_density(dz, params, c, ecut)}
+        rho_fno = fno_initial_density(dz, params, c, ecut)
+        starts = {"flat": None, "atomic": rho_at * (c.nelec / (rho_at.mean() * c.volume)), "fno": rho_fno, "fno_no_warmup": rho_fno}
         row = {}
         conv_rho = None
         for name, init in starts.items():
             b = scfm.GpuBackend(dz, "fp64")
-            r = scfm.run_scf(c, _scf_params(ecut, kmesh, nbands, tol, init), b)
+            # the reference's loose-tolerance warm-up iterations (density.zig:128-183) exist for poor
+            # starting densities; the learned start is also run without them
+            wu = 0 if name == "fno_no_warmup" else 2
+            r = scfm.run_scf(c, _scf_params(ecut, kmesh, nbands, tol, init, smearing=FNO_SMEARING, warmup_steps=wu), b)
             b.close()
             row[name] = {"iterations": r.iterations, "converged": r.converged, "energy_per_atom": r.energy_per_atom, "wall_s": r.wall_s}
             if name == "flat":
@@ -240,7 +255,7 @@ def evaluate_fno(dz, params, cells, ecut: float, nbands: int, kmesh=(2, 2, 2), t
                 row[name]["initial_rms_error"] = float(np.sqrt(np.mean((init - conv_rho) ** 2)) / mean)
         rows.append(row)
     summ = {}
-    for name in ("flat", "atomic", "fno"):
+    for name in ("flat", "atomic", "fno", "fno_no_warmup"):
         summ[name] = {
             "mean_iterations": float(np.mean([r[name]["iterations"] for r in rows])),
             "all_converged": all(r[name]["converged"] for r in rows),
@@ -273,6 +288,7 @@ def main(argv=None):
     ap.add_argument("--fno-eval-cells", type=int, default=8)
     ap.add_argument("--fno-steps", type=int, default=400)
     ap.add_argument("--fno-lr", type=float, default=2e-3)
+    ap.add_argument("--eval-only", action="store_true", help="fno: evaluate the shipped weights, no training")
     a = ap.parse_args(argv)
     dz = importlib.import_module(__package__)
     if a.what == "fno":
@@ -293,7 +309,7 @@ def main(argv=None):
         "loss_first": float(hist[0]),
         "loss_last": float(hist[-1]),
         "heldout_loss": eval_loss(dz, p, ev),
-        "heldout_loss_initial_weights": eval_loss(dz, init_params(0), ev),
+        "heldout_loss_initial_weights_tpa": eval_loss(dz, init_params(0), ev),
         "heldout_loss_reference_diagonal": fixed_loss(ev, "reference"),
         "heldout_loss_tpa": fixed_loss(ev, "tpa"),
         "heldout_davidson": evaluate_precond(dz, eval_cells, a.ecut, a.nbands, p),
@@ -306,6 +322,11 @@ def main(argv=None):
 def main_fno(dz, a):
     """SiGe8 cells (20 Ry, 2x2x2 k, 20 bands): train on seeds 2000.., evaluate on seeds 2400.."""
     ecut, nb = 20.0, 20
+    if a.eval_only:
+        p = load_fno_weights()
+        cells = [sysm.crystal("sige8", 2400 + i) for i in range(a.fno_eval_cells)]
+        print(json.dumps({"heldout_scf": evaluate_fno(dz, p, cells, ecut, nb)}), flush=True)
+        return
     t0 = time.perf_counter()
     train = fno_samples(dz, [sysm.crystal("sige8", 2000 + i) for i in range(a.fno_train_cells)], ecut, nb)
     heldout_cells = [sysm.crystal("sige8", 2400 + i) for i in range(a.fno_eval_cells)]

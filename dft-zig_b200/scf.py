@@ -340,121 +340,192 @@ def ionic_potential_g(c: sysm.Crystal, dims, ecut: float) -> np.ndarray:
     return np.fft.fftn(vr.reshape(dims[2], dims[1], dims[0])).ravel() / n
 
 
-def run_scf(c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False) -> ScfResult:
-    t0 = time.perf_counter()
-    dims = sysm.fft_box(p.ecut, c.recip)
-    N = dims[0] * dims[1] * dims[2]
-    vol = c.volume
-    kpts = sysm.monkhorst_pack(p.kmesh)
-    tables = [[sysm.radial_table(sp, i, p.ecut) for i in range(len(sp.betas))] for sp in c.species]
-    vloc_r = sysm.local_potential(c, dims, p.ecut)
-    kin = [sysm.kpoint_inputs(c, p.ecut, k, dims=dims, local_r=vloc_r, tables=tables) for k, _ in kpts]
-    kweights = [w for _, w in kpts]
-    backend.setup(kin)
-    g2 = g_vectors(dims, c.recip)
-    gmask = g2 > 1e-12
-    nelec = c.nelec
-    nocc = int(math.ceil(nelec / 2.0 - 1e-12))
-    nbands = max(p.nbands, nocc)
+class ScfState:
+    """One cell's SCF loop (scf.zig:148-188 control flow) split around its eigensolves, so several
+    cells can share one batched eigensolver call per iteration (run_scf_many)."""
 
-    def to_g(fr):
-        return np.fft.fftn(fr.reshape(dims[2], dims[1], dims[0])).ravel() / N
-
-    def to_r(fg):
-        return np.fft.ifftn(fg.reshape(dims[2], dims[1], dims[0])).ravel().real * N
-
-    def hxc_g(rho):
-        rg = to_g(rho)
-        vh = np.zeros_like(rg)
-        vh[gmask] = 8.0 * math.pi * rg[gmask] / g2[gmask]
-        _, vxc = lda_pz(rho)
-        return vh + to_g(vxc)
-
-    if p.initial_density is None:
-        rho = np.full(N, nelec / vol)  # init_rho_from_user_or_flat (run_state.zig:98-115)
-    else:
-        rho = np.asarray(p.initial_density, dtype=np.float64).copy()
-        if rho.size != N:
-            raise ValueError("initial_density size does not match the FFT grid")
-    v_hxc = hxc_g(rho)
-    mixer = PulayMixer(p.pulay_history)
-    vectors = [None] * len(kpts)
-    e_ion = ewald_energy(c.cell, np.array([c.species[s].z_val for s in c.atom_species]), c.positions)
-    psp_core = sum(gth_alpha(c.species[s]) for s in c.atom_species) * nelec / vol
-    history = []
-    energy = float("nan")
-    terms = {}
-    converged = False
-    values = []
-    it = 0
-    for it in range(1, p.max_iter + 1):
-        local_r = vloc_r + to_r(v_hxc)
-        backend.set_vloc(local_r)
-        warm = it <= p.warmup_steps
-        opts = dict(max_iter=p.warmup_max_iter if warm else p.iterative_max_iter, tol=p.warmup_tol if warm else p.iterative_tol)
-        values = []
-        inits = [vectors[k] if (p.reuse_vectors and vectors[k] is not None) else None for k in range(len(kin))]
-        if hasattr(backend, "eig_all"):
-            # every k-point's solve at once (the k-point worker loop, kpoint/workers.zig:133-180)
-            res = backend.eig_all([inp.basis.kinetic for inp in kin], nbands, opts, inits)
-            for k, (ev, vec) in enumerate(res):
-                values.append(np.asarray(ev))
-                vectors[k] = vec
+    def __init__(self, c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False):
+        self.t0 = time.perf_counter()
+        self.c, self.p, self.backend, self.verbose = c, p, backend, verbose
+        dims = self.dims = sysm.fft_box(p.ecut, c.recip)
+        N = self.N = dims[0] * dims[1] * dims[2]
+        self.vol = c.volume
+        kpts = sysm.monkhorst_pack(p.kmesh)
+        tables = [[sysm.radial_table(sp, i, p.ecut) for i in range(len(sp.betas))] for sp in c.species]
+        self.vloc_r = sysm.local_potential(c, dims, p.ecut)
+        self.kin = [sysm.kpoint_inputs(c, p.ecut, k, dims=dims, local_r=self.vloc_r, tables=tables) for k, _ in kpts]
+        self.kweights = [w for _, w in kpts]
+        backend.setup(self.kin)
+        self.g2 = g_vectors(dims, c.recip)
+        self.gmask = self.g2 > 1e-12
+        self.nelec = c.nelec
+        self.nocc = int(math.ceil(self.nelec / 2.0 - 1e-12))
+        self.nbands = max(p.nbands, self.nocc)
+        if p.initial_density is None:
+            self.rho = np.full(N, self.nelec / self.vol)  # init_rho_from_user_or_flat (run_state.zig:98-115)
         else:
-            for k, inp in enumerate(kin):
-                ev, vec = backend.eig(k, inp.basis.kinetic, nbands, opts, inits[k])
-                values.append(np.asarray(ev))
-                vectors[k] = vec
-        # occupations
+            self.rho = np.asarray(p.initial_density, dtype=np.float64).copy()
+            if self.rho.size != N:
+                raise ValueError("initial_density size does not match the FFT grid")
+        self.v_hxc = self.hxc_g(self.rho)
+        self.mixer = PulayMixer(p.pulay_history)
+        self.vectors = [None] * len(kpts)
+        self.e_ion = ewald_energy(c.cell, np.array([c.species[s].z_val for s in c.atom_species]), c.positions)
+        self.psp_core = sum(gth_alpha(c.species[s]) for s in c.atom_species) * self.nelec / self.vol
+        self.history = []
+        self.energy = float("nan")
+        self.terms = {}
+        self.converged = False
+        self.done = False
+        self.values = []
+        self.it = 0
+
+    def to_g(self, fr):
+        d = self.dims
+        return np.fft.fftn(fr.reshape(d[2], d[1], d[0])).ravel() / self.N
+
+    def to_r(self, fg):
+        d = self.dims
+        return np.fft.ifftn(fg.reshape(d[2], d[1], d[0])).ravel().real * self.N
+
+    def hxc_g(self, rho):
+        rg = self.to_g(rho)
+        vh = np.zeros_like(rg)
+        vh[self.gmask] = 8.0 * math.pi * rg[self.gmask] / self.g2[self.gmask]
+        _, vxc = lda_pz(rho)
+        return vh + self.to_g(vxc)
+
+    def begin(self):
+        """Start the next iteration: set V(r); returns the eigensolver options and warm starts."""
+        p = self.p
+        self.it += 1
+        local_r = self.vloc_r + self.to_r(self.v_hxc)
+        self.backend.set_vloc(local_r)
+        warm = self.it <= p.warmup_steps
+        opts = dict(max_iter=p.warmup_max_iter if warm else p.iterative_max_iter, tol=p.warmup_tol if warm else p.iterative_tol)
+        inits = [self.vectors[k] if (p.reuse_vectors and self.vectors[k] is not None) else None for k in range(len(self.kin))]
+        return opts, inits
+
+    def finish(self, results):
+        """Occupations, density, energy, convergence test and mixing from the eigenpairs of begin()."""
+        p, c, N, vol = self.p, self.c, self.N, self.vol
+        self.values = []
+        for k, (ev, vec) in enumerate(results):
+            self.values.append(np.asarray(ev))
+            self.vectors[k] = vec
+        values, nbands, nelec = self.values, self.nbands, self.nelec
         if p.smearing:
-            mu = fermi_level(nelec, p.smearing, kweights, values)
+            mu = fermi_level(nelec, p.smearing, self.kweights, values)
             occs = [fd_occ(v, mu, p.smearing) for v in values]
         else:
             occ = np.zeros(nbands)
-            occ[: nocc - 1] = 1.0
-            occ[nocc - 1] = nelec / 2.0 - (nocc - 1)
+            occ[: self.nocc - 1] = 1.0
+            occ[self.nocc - 1] = nelec / 2.0 - (self.nocc - 1)
             occs = [occ for _ in values]
         rho_out = np.zeros(N)
         e_band = 0.0
         e_ent = 0.0
-        for k in range(len(kin)):
-            wts = kweights[k] * occs[k] * 2.0
+        for k in range(len(self.kin)):
+            wts = self.kweights[k] * occs[k] * 2.0
             e_band += float(np.dot(wts, values[k]))
             if p.smearing:
-                e_ent += kweights[k] * 2.0 * p.smearing * float(entropy_term(occs[k]).sum())
-            backend.density(k, vectors[k], wts, rho_out)
-        diff = math.sqrt(float(np.mean((rho_out - rho) ** 2)))
-        if hasattr(backend, "observe"):
-            backend.observe(diff)
+                e_ent += self.kweights[k] * 2.0 * p.smearing * float(entropy_term(occs[k]).sum())
+            self.backend.density(k, self.vectors[k], wts, rho_out)
+        diff = math.sqrt(float(np.mean((rho_out - self.rho) ** 2)))
+        if hasattr(self.backend, "observe"):
+            self.backend.observe(diff)
         # energy of rho_out with eigenvalues from V_in (energy.zig:372-396)
-        rg = to_g(rho_out)
-        e_h = 0.5 * vol * float(np.sum(8.0 * math.pi * np.abs(rg[gmask]) ** 2 / g2[gmask]))
-        fxc, vxc_out = lda_pz(rho_out)
+        rg = self.to_g(rho_out)
+        gm = self.gmask
+        e_h = 0.5 * vol * float(np.sum(8.0 * math.pi * np.abs(rg[gm]) ** 2 / self.g2[gm]))
+        fxc, _ = lda_pz(rho_out)
         dv = vol / N
         e_xc = float(fxc.sum()) * dv
-        v_in_r = to_r(v_hxc)
+        v_in_r = self.to_r(self.v_hxc)
         int_vin_rho = float(np.dot(v_in_r, rho_out)) * dv
-        energy = e_band - int_vin_rho + e_h + e_xc + e_ion + psp_core - e_ent
-        terms = dict(band=e_band, hartree=e_h, xc=e_xc, vin_rho=int_vin_rho, ion_ion=e_ion, psp_core=psp_core, entropy=e_ent)
-        history.append((it, energy, diff, time.perf_counter() - t0))
-        if verbose:
-            print(f"scf {it:3d}  E={energy:.10f} Ry  drho={diff:.3e}", flush=True)
+        self.energy = e_band - int_vin_rho + e_h + e_xc + self.e_ion + self.psp_core - e_ent
+        self.terms = dict(band=e_band, hartree=e_h, xc=e_xc, vin_rho=int_vin_rho, ion_ion=self.e_ion, psp_core=self.psp_core, entropy=e_ent)
+        self.history.append((self.it, self.energy, diff, time.perf_counter() - self.t0))
+        if self.verbose:
+            print(f"scf {self.it:3d}  E={self.energy:.10f} Ry  drho={diff:.3e}", flush=True)
         if p.energy_target is not None and p.energy_tol_per_atom is not None:
-            if abs(energy - p.energy_target) / len(c.atom_species) < p.energy_tol_per_atom:
-                converged = True
-                rho = rho_out
-                break
+            if abs(self.energy - p.energy_target) / len(c.atom_species) < p.energy_tol_per_atom:
+                self.converged = self.done = True
+                self.rho = rho_out
+                return True
         if diff < p.convergence:
-            converged = True
-            rho = rho_out
-            break
-        v_out = hxc_g(rho_out)
-        resid = v_out - v_hxc
-        if it >= p.pulay_start:
-            flat = mixer.mix(np.concatenate([v_hxc.real, v_hxc.imag]), np.concatenate([resid.real, resid.imag]), p.mixing_beta)
-            v_hxc = flat[:N] + 1j * flat[N:]
+            self.converged = self.done = True
+            self.rho = rho_out
+            return True
+        resid = self.hxc_g(rho_out) - self.v_hxc
+        if self.it >= p.pulay_start:
+            flat = self.mixer.mix(np.concatenate([self.v_hxc.real, self.v_hxc.imag]), np.concatenate([resid.real, resid.imag]), p.mixing_beta)
+            self.v_hxc = flat[:N] + 1j * flat[N:]
         else:
-            v_hxc = v_hxc + p.mixing_beta * resid
-        rho = rho_out
-    natom = len(c.atom_species)
-    return ScfResult(converged, it, energy, energy / natom, values, terms, rho, history, time.perf_counter() - t0)
+            self.v_hxc = self.v_hxc + p.mixing_beta * resid
+        self.rho = rho_out
+        if self.it >= p.max_iter:
+            self.done = True
+        return self.done
+
+    def result(self) -> ScfResult:
+        natom = len(self.c.atom_species)
+        return ScfResult(self.converged, self.it, self.energy, self.energy / natom, self.values, self.terms, self.rho, self.history,
+                         time.perf_counter() - self.t0)
+
+
+def run_scf(c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False) -> ScfResult:
+    st = ScfState(c, p, backend, verbose)
+    while not st.done:
+        opts, inits = st.begin()
+        diags = [inp.basis.kinetic for inp in st.kin]
+        if hasattr(backend, "eig_all"):
+            # every k-point's solve at once (the k-point worker loop, kpoint/workers.zig:133-180)
+            res = backend.eig_all(diags, st.nbands, opts, inits)
+        else:
+            res = [backend.eig(k, diags[k], st.nbands, opts, inits[k]) for k in range(len(st.kin))]
+        st.finish(res)
+    return st.result()
+
+
+def run_scf_many(dz, cells, p: ScfParams, precision: str = "fp64", initial_densities=None):
+    """Independent SCF runs of many cells advanced together: each iteration, the eigensolves of
+    every (cell, k-point) pair still running go through one lockstep batch
+    (dftcuda_eig_solve_batch) on their contexts' streams.  All cells need the same band count."""
+    t0 = time.perf_counter()
+    states = []
+    for i, c in enumerate(cells):
+        pi = p if initial_densities is None else ScfParams(**{**p.__dict__, "initial_density": initial_densities[i]})
+        states.append(ScfState(c, pi, GpuBackend(dz, precision)))
+    if len({st.nbands for st in states}) != 1:
+        raise ValueError("run_scf_many: the cells need the same number of bands")
+    nb = states[0].nbands
+    while True:
+        active = [st for st in states if not st.done]
+        if not active:
+            break
+        groups = {}
+        begun = []
+        for st in active:
+            opts, inits = st.begin()
+            begun.append((st, inits))
+            groups.setdefault((opts["max_iter"], opts["tol"]), []).append((st, inits))
+        out = {}
+        for (mi, tol), members in groups.items():
+            ctxs, diags, inits = [], [], []
+            for st, iv in members:
+                ctxs += st.backend._active()
+                diags += [inp.basis.kinetic for inp in st.kin]
+                inits += iv
+            rs = dz.hermitian_eigen_decomp_iterative_batch(ctxs, diags, nb, dz.Options(max_iter=mi, tol=tol), inits)
+            o = 0
+            for st, _ in members:
+                nk = len(st.kin)
+                out[id(st)] = [(r.values, r.vectors) for r in rs[o:o + nk]]
+                o += nk
+        for st, _ in begun:
+            st.finish(out[id(st)])
+    results = [st.result() for st in states]
+    for st in states:
+        st.backend.close()
+    return results, time.perf_counter() - t0

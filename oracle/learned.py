@@ -9,7 +9,8 @@ can be checked against it (and it against finite differences):
         K(x) = (27 + 18x + 12x^2 + 8x^3) / (27 + 18x + 12x^2 + 8x^3 + 16x^4)
         (Teter, Payne, Allan, Phys. Rev. B 40, 12255 (1989))
   MLP   q_i = m(u_i) r_i,  u = (log(x + 0.05), log(|r_i| / rms(r) + 1e-6), min(t / 20, 2)),
-        h1 = tanh(W1 u + b1), h2 = tanh(W2 h1 + b2), m = softplus(w3 . h2 + b3)   (3 -> 64 -> 64 -> 1)
+        h1 = tanh(W1 u + b1), h2 = tanh(W2 h1 + b2), z = w3 . h2 + b3   (3 -> 64 -> 64 -> 1),
+        m = K(x) exp(clamp(z, -8, 8)) with x = exp(u0) - 0.05 (a refinement of TPA)
   loss  L = mean_b [1 - |A_b|^2 / (Q_b D_b)],  A_b = sum_i m_i c_i,  Q_b = sum_i m_i^2 w_i,
         c_i = conj(r_i) delta_i, w_i = |r_i|^2, D_b = ||delta_b||^2.
 
@@ -61,8 +62,13 @@ def forward(p, u):
     return z, h1, h2
 
 
+def _mult(u0, z):
+    x = np.maximum(np.exp(u0) - 0.05, 0.0)
+    return tpa(x) * np.exp(np.clip(z, -8.0, 8.0))
+
+
 def multiplier(p, u):
-    return softplus(forward(p, u)[0])
+    return _mult(u[:, 0], forward(p, u)[0])
 
 
 def loss_grad(p, off, feat, cc, w, dnorm):
@@ -70,8 +76,8 @@ def loss_grad(p, off, feat, cc, w, dnorm):
     off = np.asarray(off)
     nb = len(off) - 1
     z, h1, h2 = forward(p, feat)
-    m = softplus(z)
-    sig = 1.0 / (1.0 + np.exp(-z))
+    m = _mult(feat[:, 0], z)
+    sig = np.where((z > -8.0) & (z < 8.0), m, 0.0)  # dm/dz
     W1, b1, W2, b2, w3, b3 = unpack(p)
     band = np.repeat(np.arange(nb), np.diff(off))
     A = np.bincount(band, weights=m * cc.real, minlength=nb) + 1j * np.bincount(band, weights=m * cc.imag, minlength=nb)

@@ -38,3 +38,22 @@ def test_al4_smeared_scf_gpu_matches_oracle(dz):
     r_ref = scf.run_scf(c, p, OracleBackend())
     assert r_gpu.converged and r_ref.converged
     assert abs(r_gpu.energy_per_atom - r_ref.energy_per_atom) < 1e-8
+
+
+def test_many_cell_scf_matches_single_runs(dz):
+    """run_scf_many (every cell's k-points in one lockstep eigensolver batch per SCF iteration) gives
+    the same converged energies as one run_scf per cell."""
+    import importlib
+
+    scf = importlib.import_module("dftzig_b200.scf")
+    system = importlib.import_module("dftzig_b200.system")
+    cells = [system.crystal("sige8", 2900 + i) for i in range(3)]
+    p = scf.ScfParams(ecut=10.0, kmesh=(1, 1, 1), nbands=20, convergence=1e-8, iterative_tol=1e-9,
+                      iterative_max_iter=100, warmup_steps=0, smearing=0.01, max_iter=60)
+    many, _ = scf.run_scf_many(dz, cells, p)
+    for c, r in zip(cells, many):
+        b = scf.GpuBackend(dz)
+        one = scf.run_scf(c, p, b)
+        b.close()
+        assert r.converged and one.converged
+        assert abs(r.energy_per_atom - one.energy_per_atom) < 1e-8
