@@ -53,9 +53,11 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile-case", action="store_true", help="small single-k case for ncu captures: Gamma, 32 columns, 2 applications")
-    ap.add_argument("--workload", choices=("hpsi", "scf", "scf64", "cells"), default="hpsi",
+    ap.add_argument("--workload", choices=("hpsi", "scf", "scf64", "cells", "eig"), default="hpsi",
                     help="hpsi: H|psi> GB/s (default); scf: time-to-SCF Si2; scf64: time-to-SCF Si64, mixed vs FP64; "
-                         "cells: many-cell SiGe8 SCF throughput, atomic vs learned start")
+                         "cells: many-cell SiGe8 SCF throughput, atomic vs learned start; "
+                         "eig: one Si64 Gamma Davidson solve (profiling case)")
+    ap.add_argument("--eig-iters", type=int, default=6, help="Davidson iterations of --workload eig")
     ap.add_argument("--cells", type=int, default=16, help="cells of the many-cell workload")
     ap.add_argument("--precision", choices=("fp64", "fp32", "tf32"), default="fp64", help="context precision of --profile-case")
     return ap.parse_args()
@@ -590,6 +592,7 @@ def run_cells_workload(args):
         pn = p if name == "atomic" else scf.ScfParams(**{**p.__dict__, "warmup_steps": 0})
         res, wall = scf.run_scf_many(dz, cells, pn, "fp64", starts[name])
         out[name] = {"seconds": round(wall, 3), "cells_per_second": round(len(cells) / wall, 3),
+                     "phases_s": getattr(scf.run_scf_many, "last_phases", None),
                      "mean_scf_iterations": float(np.mean([r.iterations for r in res])),
                      "all_converged": all(r.converged for r in res)}
     line = {
@@ -608,8 +611,40 @@ def run_cells_workload(args):
     print(json.dumps(line), flush=True)
 
 
+def run_eig_workload(args):
+    """One Davidson solve at Gamma of the Si64 cell (30 Ry, 160 bands) from the random start,
+    --eig-iters iterations, FP64: the case the eigensolver's launch lists are taken on."""
+    import importlib
+
+    import torch
+
+    import dftzig_loader
+
+    dz = dftzig_loader.load()
+    system = importlib.import_module("dftzig_b200.system")
+    c = system.crystal(CELL, SEED)
+    inp = system.kpoint_inputs(c, ECUT, (0.0, 0.0, 0.0))
+    kc = dz.KpointContext(*inp.dims, inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart)
+    kc.set_vloc(inp.local_r)
+    kc.set_projectors([dz.SpeciesProjectors(l, d, p) for (l, d, p) in inp.species_phi], inp.atom_species, inp.positions)
+    kc.set_profiling(True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, NBANDS, dz.Options(max_iter=args.eig_iters, tol=1e-9))
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    pr = kc.profile()
+    kc.close()
+    print(json.dumps({"metric": "Davidson solve wall time, Si64 Gamma 30 Ry 160 bands", "value": round(wall * 1e3, 2), "unit": "ms",
+                      "iterations": r.iterations, "h_applies": r.h_applies, "apply_h_ms": round(pr["apply_h_ns"] / 1e6, 2),
+                      "subspace_ms": round(pr["subspace_ns"] / 1e6, 2)}), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "eig":
+        run_eig_workload(args)
+        return
     if args.workload == "scf":
         run_scf_workload(args)
         return

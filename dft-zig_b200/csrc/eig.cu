@@ -439,6 +439,9 @@ static int eig_alloc(dftcuda_kctx* c, size_t n, size_t max_sub, size_t nb) {
   need = std::max(need, zgemm_workspace_elems((int)kmax, (int)kmax, (int)n));
   need = std::max(need, cgemm_tf32_workspace_elems(ms, ms, (int)n));
   need = std::max(need, cgemm_tf32_workspace_elems((int)nb, (int)n, ms));
+  need = std::max(need, cgemm_tf32_workspace_elems(ms, (int)kmax, (int)n));
+  need = std::max(need, cgemm_tf32_workspace_elems((int)kmax, (int)n, ms));
+  need = std::max(need, cgemm_tf32_workspace_elems((int)kmax, (int)kmax, (int)n));
   if (need) {
     if (cudaMalloc(&e->ws, need * sizeof(double2)) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "eig gemm ws");
     e->ws_elems = need;
@@ -458,8 +461,12 @@ static int eig_alloc(dftcuda_kctx* c, size_t n, size_t max_sub, size_t nb) {
 
 // Gram products on blocks stored as rows of length n ("vector blocks", column-major [n x cols]).
 // out[i + j*ldo] = sum_g conj(X[i][g]) Y[j][g]
-static int gemm_dispatch(KCtxImpl* e, const GemmArgs& g, bool rr, cudaStream_t s) {
-  if (rr && e->rr_tc) return cgemm_tf32(g, s, e->ws, e->ws_elems, e->err, true);
+// In TF32 / TF32X3 contexts every subspace product (Rayleigh-Ritz V^H W, V C, W C and the
+// orthonormalisation's projections and block overlaps) runs on the tensor cores in the split-TF32
+// form (FP32-class accuracy); the Cholesky factorisations, the subspace eigensolver and the residual
+// norms stay FP64.  FP64 and FP32 contexts use the FP64 GEMM throughout.
+static int gemm_dispatch(KCtxImpl* e, const GemmArgs& g, bool /*rr*/, cudaStream_t s) {
+  if (e->rr_tc) return cgemm_tf32(g, s, e->ws, e->ws_elems, e->err, true);
   return zgemm(g, s, e->ws, e->ws_elems);
 }
 

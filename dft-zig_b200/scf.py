@@ -493,10 +493,12 @@ def run_scf_many(dz, cells, p: ScfParams, precision: str = "fp64", initial_densi
     every (cell, k-point) pair still running go through one lockstep batch
     (dftcuda_eig_solve_batch) on their contexts' streams.  All cells need the same band count."""
     t0 = time.perf_counter()
+    phases = {"setup": 0.0, "begin": 0.0, "eig": 0.0, "finish": 0.0}
     states = []
     for i, c in enumerate(cells):
         pi = p if initial_densities is None else ScfParams(**{**p.__dict__, "initial_density": initial_densities[i]})
         states.append(ScfState(c, pi, GpuBackend(dz, precision)))
+    phases["setup"] = time.perf_counter() - t0
     if len({st.nbands for st in states}) != 1:
         raise ValueError("run_scf_many: the cells need the same number of bands")
     nb = states[0].nbands
@@ -506,10 +508,13 @@ def run_scf_many(dz, cells, p: ScfParams, precision: str = "fp64", initial_densi
             break
         groups = {}
         begun = []
+        tb = time.perf_counter()
         for st in active:
             opts, inits = st.begin()
             begun.append((st, inits))
             groups.setdefault((opts["max_iter"], opts["tol"]), []).append((st, inits))
+        te = time.perf_counter()
+        phases["begin"] += te - tb
         out = {}
         for (mi, tol), members in groups.items():
             ctxs, diags, inits = [], [], []
@@ -523,9 +528,13 @@ def run_scf_many(dz, cells, p: ScfParams, precision: str = "fp64", initial_densi
                 nk = len(st.kin)
                 out[id(st)] = [(r.values, r.vectors) for r in rs[o:o + nk]]
                 o += nk
+        tf = time.perf_counter()
+        phases["eig"] += tf - te
         for st, _ in begun:
             st.finish(out[id(st)])
+        phases["finish"] += time.perf_counter() - tf
     results = [st.result() for st in states]
     for st in states:
         st.backend.close()
+    run_scf_many.last_phases = {k: round(v, 3) for k, v in phases.items()}
     return results, time.perf_counter() - t0

@@ -44,9 +44,10 @@ extern "C" {
  *          accumulation in TMEM); relative error ~1e-3;
  *  TF32X3  as TF32 with every operand split into two TF32 parts (hi + lo, three MMAs per real
  *          product): FP32-class accuracy (~1e-6) on the tensor cores.
- * Wavefunctions are FP64 at the boundary in every mode.  In TF32 and TF32X3 contexts the
- * eigensolver's Rayleigh-Ritz products (V^H W, V C, W C) use the same tensor-core GEMM (split form);
- * orthonormalisation, the subspace eigensolver and residual norms stay FP64. */
+ * Wavefunctions are FP64 at the boundary in every mode.  In TF32 and TF32X3 contexts every
+ * eigensolver subspace product (V^H W, V C, W C, the orthonormalisation's projections and block
+ * overlaps) uses the same tensor-core GEMM (split form); the Cholesky factorisations, the subspace
+ * eigensolver and the residual norms stay FP64. */
 #define DFTCUDA_PRECISION_FP64 0
 #define DFTCUDA_PRECISION_FP32 1
 #define DFTCUDA_PRECISION_TF32 2

@@ -90,3 +90,52 @@ def test_fno_training_reduces_loss(dz):
     p0 = learned.fno_init_params(4)
     p, hist = dz.fno_train(p0, samples, steps=60, lr=2e-3)
     assert hist[-1] < 0.7 * hist[0]
+
+
+# ---- the shipped trained weights on held-out cells ------------------------------------------------
+
+
+def test_trained_preconditioner_gain(dz):
+    """The committed MLP preconditioner on a held-out strained/displaced Si8 cell: converges to the
+    reference eigenvalues in far fewer H applications than the reference diagonal and within 10% of
+    Teter-Payne-Allan (the form it refines)."""
+    import importlib
+
+    learn = importlib.import_module("dftzig_b200.learn")
+    system = importlib.import_module("dftzig_b200.system")
+    params = learn.load_precond_weights()
+    c = system.crystal("si8d", 1290)
+    inp = system.kpoint_inputs(c, 12.0, (0.0, 0.0, 0.0))
+    out = {}
+    for kind in (dz.PRECOND_REFERENCE, dz.PRECOND_TPA, dz.PRECOND_MLP):
+        kc = learn._context(dz, inp)
+        kc.set_preconditioner(kind, params if kind == dz.PRECOND_MLP else None)
+        out[kind] = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, 16, dz.Options(max_iter=400, tol=1e-6))
+        kc.close()
+    ref, tpa, mlp = out[dz.PRECOND_REFERENCE], out[dz.PRECOND_TPA], out[dz.PRECOND_MLP]
+    assert ref.converged and tpa.converged and mlp.converged
+    assert np.abs(mlp.values - ref.values).max() < 1e-7
+    assert mlp.h_applies < 0.5 * ref.h_applies
+    assert mlp.h_applies <= 1.1 * tpa.h_applies
+
+
+def test_trained_fno_start_beats_atomic_superposition(dz):
+    """The committed FNO on a held-out SiGe8 cell: its first density is far closer to the converged
+    SCF density than the atomic superposition it starts from."""
+    import importlib
+
+    learn = importlib.import_module("dftzig_b200.learn")
+    scf = importlib.import_module("dftzig_b200.scf")
+    system = importlib.import_module("dftzig_b200.system")
+    c = system.crystal("sige8", 2490)
+    ecut = 20.0
+    dims, u, rho_at, mean = learn.fno_input(c, ecut)
+    rho_fno = learn.fno_initial_density(dz, learn.load_fno_weights(), c, ecut)
+    b = scf.GpuBackend(dz)
+    r = scf.run_scf(c, scf.ScfParams(ecut=ecut, kmesh=(2, 2, 2), nbands=20, convergence=1e-7, smearing=learn.FNO_SMEARING, max_iter=80), b)
+    b.close()
+    assert r.converged
+    rho_atomic = rho_at * (c.nelec / (rho_at.mean() * c.volume))
+    err_fno = np.sqrt(np.mean((rho_fno - r.rho) ** 2))
+    err_at = np.sqrt(np.mean((rho_atomic - r.rho) ** 2))
+    assert err_fno < 0.2 * err_at
