@@ -53,13 +53,16 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile-case", action="store_true", help="small single-k case for ncu captures: Gamma, 32 columns, 2 applications")
-    ap.add_argument("--workload", choices=("hpsi", "scf", "scf64", "cells", "eig"), default="hpsi",
+    ap.add_argument("--workload", choices=("hpsi", "scf", "scf64", "scf216", "cells", "eig"), default="hpsi",
                     help="hpsi: H|psi> GB/s (default); scf: time-to-SCF Si2; scf64: time-to-SCF Si64, mixed vs FP64; "
+                         "scf216: time-to-SCF Si216 (Gamma, 448 bands), FP64 vs learned+mixed; "
                          "cells: many-cell SiGe8 SCF throughput, atomic vs learned start; "
                          "eig: one Si64 Gamma Davidson solve (profiling case)")
     ap.add_argument("--eig-iters", type=int, default=6, help="Davidson iterations of --workload eig")
+    ap.add_argument("--eig-cell", choices=("si64", "si216"), default="si64", help="cell of --workload eig")
     ap.add_argument("--cells", type=int, default=16, help="cells of the many-cell workload")
-    ap.add_argument("--precision", choices=("fp64", "fp32", "tf32"), default="fp64", help="context precision of --profile-case")
+    ap.add_argument("--precision", choices=("fp64", "fp32", "tf32"), default="fp64",
+                    help="context precision of --profile-case (tf32 = TF32 GEMMs) and --workload eig (tf32 = TF32X3)")
     return ap.parse_args()
 
 
@@ -514,12 +517,65 @@ def run_scf_workload(args):
     print(json.dumps(line), flush=True)
 
 
+def run_scf216_workload(args):
+    """Time-to-SCF on Si216 (3x3x3 conventional, N(0, 0.05 A) displacements, seed 3), 25 Ry, Gamma
+    only, 448 bands, LDA-PZ, fixed occupations, Pulay 8 / beta 0.3, the reference's eigensolver
+    defaults (max_subspace 4 nb + 8 = 1800).  Target: a tight FP64 run (density RMS 1e-8).  Reported:
+    wall seconds until |E - E_target| < 1e-6 Ry/atom, plain FP64 (reference preconditioner) against
+    learned+mixed (TF32X3 contexts until the density residual is below 1e-4, then FP64; the trained
+    TPA-refining MLP preconditioner throughout)."""
+    import importlib
+
+    import torch
+
+    import dftzig_loader
+
+    dz = dftzig_loader.load()
+    scf = importlib.import_module("dftzig_b200.scf")
+    system = importlib.import_module("dftzig_b200.system")
+    learn = importlib.import_module("dftzig_b200.learn")
+    c = system.crystal("si216", 3)
+    base = dict(ecut=25.0, kmesh=(1, 1, 1), nbands=448, mixing_beta=0.3, pulay_history=8, max_iter=60)
+    b = scf.GpuBackend(dz, "fp64")
+    ref = scf.run_scf(c, scf.ScfParams(**base, convergence=1e-8), b)
+    b.close()
+    mlp = (dz.PRECOND_MLP, learn.load_precond_weights())
+    out = {}
+    for mode, prec, pc in (("fp64", "fp64", None), ("learned_mixed", "mixed", mlp)):
+        p = scf.ScfParams(**base, convergence=1e-12, energy_target=ref.energy, energy_tol_per_atom=1e-6)
+        torch.cuda.synchronize()
+        b = scf.GpuBackend(dz, prec, precond=pc)
+        r = scf.run_scf(c, p, b)
+        torch.cuda.synchronize()
+        b.close()
+        if not r.converged:
+            raise RuntimeError(f"time-to-SCF run ({mode}) did not reach the target")
+        out[mode] = {"seconds": round(r.wall_s, 3), "scf_iterations": r.iterations, "dE_per_atom": r.energy_per_atom - ref.energy_per_atom,
+                     "switched_to_fp64_at_iteration": getattr(b, "switched_at", None)}
+    line = {
+        "metric": "time-to-SCF (|dE| < 1e-6 Ry/atom vs tight FP64), Si216 25 Ry Gamma, learned+mixed vs plain FP64",
+        "value": out["learned_mixed"]["seconds"],
+        "unit": "s",
+        "higher_is_better": False,
+        "n_gpus": 1,
+        "steps": 1,
+        "dtype": "f64/f32/tf32x3",
+        "data": "synthetic (seeded displacements; synthetic GTH-form Si pseudopotential)",
+        "config": {"workload": "Si216 3x3x3 conventional, sigma 0.05 A (seed 3), 25 Ry, Gamma, 448 bands, fixed occupations",
+                   "target_energy_per_atom": ref.energy_per_atom, "target_iterations": ref.iterations, "target_seconds": round(ref.wall_s, 3)},
+        "fp64": out["fp64"],
+        "learned_mixed": out["learned_mixed"],
+        "speedup_vs_fp64": round(out["fp64"]["seconds"] / out["learned_mixed"]["seconds"], 3),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_scf64_workload(args):
     """Time-to-SCF on Si64 (2x2x2 conventional, N(0, 0.02 A) displacements, seed 1), 30 Ry, 75^3,
     2x2x2 MP (8 k), 160 bands, Fermi-Dirac 0.01 Ry, LDA-PZ, Pulay 8 / beta 0.3, the reference's
     eigensolver defaults.  Target: a tight FP64 run (density RMS 1e-8).  Reported: wall seconds until
     |E - E_target| < 1e-6 Ry/atom, plain FP64 and mixed (TF32X3 contexts until the density residual
-    is below 1e-5 or stalls, then FP64)."""
+    is below 1e-4 or stalls, then FP64)."""
     import importlib
 
     import torch
@@ -612,8 +668,9 @@ def run_cells_workload(args):
 
 
 def run_eig_workload(args):
-    """One Davidson solve at Gamma of the Si64 cell (30 Ry, 160 bands) from the random start,
-    --eig-iters iterations, FP64: the case the eigensolver's launch lists are taken on."""
+    """One Davidson solve at Gamma from the random start, --eig-iters iterations: the Si64 cell (30 Ry,
+    160 bands) or the Si216 cell (25 Ry, 448 bands, subspace up to 1800); --precision selects the
+    context precision.  The case the eigensolver's launch lists are taken on."""
     import importlib
 
     import torch
@@ -622,20 +679,22 @@ def run_eig_workload(args):
 
     dz = dftzig_loader.load()
     system = importlib.import_module("dftzig_b200.system")
-    c = system.crystal(CELL, SEED)
-    inp = system.kpoint_inputs(c, ECUT, (0.0, 0.0, 0.0))
-    kc = dz.KpointContext(*inp.dims, inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart)
+    cell, seed, ecut, nb = (CELL, SEED, ECUT, NBANDS) if args.eig_cell == "si64" else ("si216", 3, 25.0, 448)
+    c = system.crystal(cell, seed)
+    inp = system.kpoint_inputs(c, ecut, (0.0, 0.0, 0.0))
+    prec = {"fp64": dz.PRECISION_FP64, "fp32": dz.PRECISION_FP32, "tf32": dz.PRECISION_TF32X3}[args.precision]
+    kc = dz.KpointContext(*inp.dims, inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart, prec)
     kc.set_vloc(inp.local_r)
     kc.set_projectors([dz.SpeciesProjectors(l, d, p) for (l, d, p) in inp.species_phi], inp.atom_species, inp.positions)
     kc.set_profiling(True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    r = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, NBANDS, dz.Options(max_iter=args.eig_iters, tol=1e-9))
+    r = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, nb, dz.Options(max_iter=args.eig_iters, tol=1e-9))
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     pr = kc.profile()
     kc.close()
-    print(json.dumps({"metric": "Davidson solve wall time, Si64 Gamma 30 Ry 160 bands", "value": round(wall * 1e3, 2), "unit": "ms",
+    print(json.dumps({"metric": f"Davidson solve wall time, {cell} Gamma {ecut:g} Ry {nb} bands ({args.precision})", "value": round(wall * 1e3, 2), "unit": "ms",
                       "iterations": r.iterations, "h_applies": r.h_applies, "apply_h_ms": round(pr["apply_h_ns"] / 1e6, 2),
                       "subspace_ms": round(pr["subspace_ns"] / 1e6, 2)}), flush=True)
 
@@ -650,6 +709,9 @@ def main():
         return
     if args.workload == "scf64":
         run_scf64_workload(args)
+        return
+    if args.workload == "scf216":
+        run_scf216_workload(args)
         return
     if args.workload == "cells":
         run_cells_workload(args)

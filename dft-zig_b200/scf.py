@@ -211,14 +211,15 @@ class GpuBackend:
 
     precision "fp64" runs every pass in FP64.  "mixed" keeps a second context per k-point in
     TF32X3 precision (FP32 FFT passes, split-TF32 tensor-core projector and Rayleigh-Ritz GEMMs) and
-    uses it while the SCF density residual is above ``switch_drho``, then the FP64 one for the rest.
+    uses it while the SCF density residual is above ``switch_drho`` (1e-4), then the FP64 one for the rest.
     It also switches when the residual stops falling (``stall`` iterations without a new minimum),
     the sign that the reduced-precision operator's error floor has been reached.  Orthonormalisation,
     the subspace eigensolver, residual checks, occupations and energies stay FP64 throughout."""
 
-    def __init__(self, dz, precision="fp64", switch_drho: float = 1e-5, stall: int = 3):
+    def __init__(self, dz, precision="fp64", switch_drho: float = 1e-4, stall: int = 3, precond=None):
         self.dz = dz
         self.precision = precision
+        self.precond = precond  # None (reference form) or (kind, params) for every context
         self.switch_drho = switch_drho
         self.stall = stall
         self.ctxs = []
@@ -233,6 +234,8 @@ class GpuBackend:
     def _make(self, inp, prec):
         kc = self.dz.KpointContext(*inp.dims, inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart, prec)
         kc.set_projectors([self.dz.SpeciesProjectors(l, d, p) for (l, d, p) in inp.species_phi], inp.atom_species, inp.positions)
+        if self.precond is not None:
+            kc.set_preconditioner(*self.precond)
         return kc
 
     def setup(self, kinputs):
