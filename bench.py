@@ -48,7 +48,7 @@ def bytes_per_column(npw: int, N: int, nb: int) -> float:
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -313,7 +313,7 @@ def run_ours(args):
         "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d, "timer": "host wall clock around synchronous C-ABI calls", "matches_device_result": ok},
         "gpu_launches": launches,
         "roofline": {
-            "kernel": "local H|psi>: k_plane_inv + k_xline + k_plane_fwd",
+            "kernel": "local H|psi>: k_plane_inv5 + k_xline5 + k_plane_fwd5 (one 164-column block)",
             "bound": "hbm",
             "achieved": round(achieved, 1) if achieved else None,
             "peak": peak,

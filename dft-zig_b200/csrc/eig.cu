@@ -329,6 +329,66 @@ __global__ void __launch_bounds__(1024) k_chol_right(const double2* __restrict__
   if (tid == 0) *kk_out = s_nk;
 }
 
+// Blocked form of the same factorisation for larger blocks: one CTA factors the rows of a panel of
+// kChPanel columns (pivots, drops, row scaling and the updates among the panel's own rows, over all
+// columns); the panel's rank-kChPanel update of the trailing triangle is an FP64 GEMM.  Dropped rows
+// are zeroed so they add nothing to the GEMM.  Launch j0 = 0 first: it copies G and resets *kk.
+constexpr int kChPanel = 32;
+__global__ void __launch_bounds__(1024) k_chol_panel(const double2* __restrict__ G, int k, double drop,
+                                                     double2* __restrict__ A, int* __restrict__ kept, int* __restrict__ kk,
+                                                     int j0, int j1) {
+  __shared__ double s_piv;
+  __shared__ int s_nk;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (j0 == 0) {
+    for (long idx = tid; idx < (long)k * k; idx += nt) {
+      const int j = (int)(idx / k), l = (int)(idx - (long)j * k);
+      if (l >= j) A[idx] = G[j + (long)l * k];
+    }
+    if (tid == 0) *kk = 0;
+    __syncthreads();
+  }
+  if (tid == 0) s_nk = *kk;
+  __syncthreads();
+  for (int j = j0; j < j1; ++j) {
+    if (tid == 0) {
+      const double d = A[(long)j * k + j].x;
+      s_piv = d > 0.0 ? sqrt(d) : 0.0;
+    }
+    __syncthreads();
+    const double piv = s_piv;
+    double2* rj = A + (long)j * k;
+    if (!(piv >= drop) || piv == 0.0) {
+      for (int l = j + tid; l < k; l += nt) rj[l] = make_double2(0.0, 0.0);
+      __syncthreads();
+      continue;
+    }
+    const double inv = 1.0 / piv;
+    for (int l = j + 1 + tid; l < k; l += nt) rj[l] = make_double2(rj[l].x * inv, rj[l].y * inv);
+    if (tid == 0) {
+      rj[j] = make_double2(piv, 0.0);
+      kept[s_nk] = j;
+      s_nk = s_nk + 1;
+    }
+    __syncthreads();
+    // rows j' of the panel after j: A[j'][l] -= conj(R[j][j']) R[j][l] for l >= j'
+    const int nr = j1 - j - 1, nc = k - j - 1;
+    for (long idx = tid; idx < (long)nr * nc; idx += nt) {
+      const int a = (int)(idx / nc), b = (int)(idx - (long)a * nc);
+      const int jr = j + 1 + a, l = j + 1 + b;
+      if (l < jr) continue;
+      const double2 x = rj[jr], y = rj[l];
+      double2* t = A + (long)jr * k + l;
+      double2 v = *t;
+      v.x -= x.x * y.x + x.y * y.y;
+      v.y -= x.x * y.y - x.y * y.x;
+      *t = v;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) *kk = s_nk;
+}
+
 // Z (k x k columns, ld k): column b < kk solves R_kept z = e_b on the kept rows (rows of dropped
 // columns zero), so Q Z has orthonormal columns; columns b >= kk are zeroed.  One warp per column,
 // the back substitution's dot products split over the lanes.
@@ -493,6 +553,36 @@ static int combine(KCtxImpl* e, const double2* X, int mx, const double2* C, int 
   return gemm_dispatch(e, g, rr, s);
 }
 
+// Cholesky with the drop rule of the k x k Gram matrix G into e->R / e->kept, kept count at kk_dev,
+// then Z = the inverse on the kept rows.  One CTA below 97 columns, the panel form above.
+static int chol_drop(KCtxImpl* e, const double2* G, int k, double drop, int* kk_dev, cudaStream_t s) {
+  if (k <= 96) {
+    k_chol_right<<<1, 1024, 0, s>>>(G, k, drop, e->R, e->kept, kk_dev);
+    count_launch();
+  } else {
+    for (int j0 = 0; j0 < k; j0 += kChPanel) {
+      const int j1 = std::min(k, j0 + kChPanel);
+      k_chol_panel<<<1, 1024, 0, s>>>(G, k, drop, e->R, e->kept, kk_dev, j0, j1);
+      count_launch();
+      if (j1 < k) {
+        // A[l1][l2] -= sum_{j in panel} conj(R[j][l1]) R[j][l2], l1, l2 >= j1 (the lower triangle
+        // of A is scratch)
+        GemmArgs g{};
+        g.M = k - j1; g.N = k - j1; g.K = j1 - j0;
+        g.A = e->R + (size_t)j0 * k + j1; g.lda = k; g.a_kc = false; g.conj_a = true;
+        g.B = e->R + (size_t)j0 * k + j1; g.ldb = k; g.b_kc = false; g.conj_b = false;
+        g.O = e->R + (size_t)j1 * k + j1; g.ldo_r = k; g.ldo_c = 1;
+        g.alpha = -1.0; g.beta = 1.0;
+        DFT_TRY(zgemm(g, s, e->ws, e->ws_elems));
+      }
+    }
+  }
+  k_chol_inv<<<ceil_div(k, 8), 256, 0, s>>>(e->R, k, e->kept, kk_dev, e->Z);
+  count_launch();
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}
+
 // Orthonormalise the k vectors in Q against V[0:m] and among themselves (in order), writing the kept
 // vectors to dst.  Two phases around one host read of the kept count: phase A projects out V once
 // and takes the dropping Cholesky of the block's Gram matrix (kept count -> e->h_kk, pinned);
@@ -507,9 +597,7 @@ static int block_orth_a(KCtxImpl* e, int m, double2* Q, int k, cudaStream_t s) {
     DFT_TRY(combine(e, e->V, m, e->H, m, k, Q, -1.0, 1.0, s));
   }
   DFT_TRY(gram(e, Q, k, Q, k, e->G, k, s));
-  k_chol_right<<<1, 1024, 0, s>>>(e->G, k, 1e-8, e->R, e->kept, e->status + 1);
-  k_chol_inv<<<ceil_div(k, 8), 256, 0, s>>>(e->R, k, e->kept, e->status + 1, e->Z);
-  count_launch(2);
+  DFT_TRY(chol_drop(e, e->G, k, 1e-8, e->status + 1, s));
   DFT_CUDA_TRY(cudaMemcpyAsync(e->h_kk, e->status + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
   return DFTCUDA_OK;
 }
@@ -523,9 +611,7 @@ static int block_orth_b(KCtxImpl* e, int m, double2* Q, int k, double2* dst, int
     DFT_TRY(combine(e, e->V, m, e->H, m, kk, e->Q2, -1.0, 1.0, s));
   }
   DFT_TRY(gram(e, e->Q2, kk, e->Q2, kk, e->G, kk, s));
-  k_chol_right<<<1, 1024, 0, s>>>(e->G, kk, 0.0, e->R, e->kept, e->status + 2);
-  k_chol_inv<<<ceil_div(kk, 8), 256, 0, s>>>(e->R, kk, e->kept, e->status + 2, e->Z);
-  count_launch(2);
+  DFT_TRY(chol_drop(e, e->G, kk, 0.0, e->status + 2, s));
   DFT_TRY(combine(e, e->Q2, kk, e->Z, kk, kk, dst, 1.0, 0.0, s));
   return DFTCUDA_OK;
 }
