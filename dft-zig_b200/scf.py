@@ -32,6 +32,7 @@ from typing import Optional
 
 import numpy as np
 
+from . import kpar
 from . import system as sysm
 
 
@@ -347,16 +348,22 @@ class ScfState:
     """One cell's SCF loop (scf.zig:148-188 control flow) split around its eigensolves, so several
     cells can share one batched eigensolver call per iteration (run_scf_many)."""
 
-    def __init__(self, c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False):
+    def __init__(self, c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False, comm=None):
         self.t0 = time.perf_counter()
         self.c, self.p, self.backend, self.verbose = c, p, backend, verbose
+        self.comm = comm if comm is not None else kpar.SerialComm()
         dims = self.dims = sysm.fft_box(p.ecut, c.recip)
         N = self.N = dims[0] * dims[1] * dims[2]
         self.vol = c.volume
         kpts = sysm.monkhorst_pack(p.kmesh)
+        self.nk = len(kpts)
+        # k-points dealt to the ranks by basis size; this rank builds inputs and contexts for its own
+        costs = [sysm.basis(c.recip, p.ecut, k).hkl.shape[0] for k, _ in kpts] if self.comm.size > 1 else None
+        self.owner = kpar.deal_kpoints(self.nk, self.comm.size, costs)
+        self.kglobal = [k for k in range(self.nk) if self.owner[k] == self.comm.rank]
         tables = [[sysm.radial_table(sp, i, p.ecut) for i in range(len(sp.betas))] for sp in c.species]
         self.vloc_r = sysm.local_potential(c, dims, p.ecut)
-        self.kin = [sysm.kpoint_inputs(c, p.ecut, k, dims=dims, local_r=self.vloc_r, tables=tables) for k, _ in kpts]
+        self.kin = [sysm.kpoint_inputs(c, p.ecut, kpts[k][0], dims=dims, local_r=self.vloc_r, tables=tables) for k in self.kglobal]
         self.kweights = [w for _, w in kpts]
         backend.setup(self.kin)
         self.g2 = g_vectors(dims, c.recip)
@@ -372,7 +379,7 @@ class ScfState:
                 raise ValueError("initial_density size does not match the FFT grid")
         self.v_hxc = self.hxc_g(self.rho)
         self.mixer = PulayMixer(p.pulay_history)
-        self.vectors = [None] * len(kpts)
+        self.vectors = [None] * len(self.kin)  # this rank's k-points, in kglobal order
         self.e_ion = ewald_energy(c.cell, np.array([c.species[s].z_val for s in c.atom_species]), c.positions)
         self.psp_core = sum(gth_alpha(c.species[s]) for s in c.atom_species) * self.nelec / self.vol
         self.history = []
@@ -410,13 +417,18 @@ class ScfState:
         return opts, inits
 
     def finish(self, results):
-        """Occupations, density, energy, convergence test and mixing from the eigenpairs of begin()."""
+        """Occupations, density, energy, convergence test and mixing from the eigenpairs of begin()
+        (``results`` for this rank's k-points).  With several ranks the eigenvalue table and the
+        density are sum-reduced over them; everything after that is replicated."""
         p, c, N, vol = self.p, self.c, self.N, self.vol
-        self.values = []
-        for k, (ev, vec) in enumerate(results):
-            self.values.append(np.asarray(ev))
-            self.vectors[k] = vec
-        values, nbands, nelec = self.values, self.nbands, self.nelec
+        nbands, nelec = self.nbands, self.nelec
+        table = np.zeros((self.nk, nbands))
+        for i, (ev, vec) in enumerate(results):
+            table[self.kglobal[i]] = np.asarray(ev)[:nbands]
+            self.vectors[i] = vec
+        if self.comm.size > 1:
+            table = self.comm.sum(table)
+        self.values = values = [table[k] for k in range(self.nk)]
         if p.smearing:
             mu = fermi_level(nelec, p.smearing, self.kweights, values)
             occs = [fd_occ(v, mu, p.smearing) for v in values]
@@ -428,12 +440,15 @@ class ScfState:
         rho_out = np.zeros(N)
         e_band = 0.0
         e_ent = 0.0
-        for k in range(len(self.kin)):
+        for k in range(self.nk):
             wts = self.kweights[k] * occs[k] * 2.0
             e_band += float(np.dot(wts, values[k]))
             if p.smearing:
                 e_ent += self.kweights[k] * 2.0 * p.smearing * float(entropy_term(occs[k]).sum())
-            self.backend.density(k, self.vectors[k], wts, rho_out)
+        for i, k in enumerate(self.kglobal):
+            self.backend.density(i, self.vectors[i], self.kweights[k] * occs[k] * 2.0, rho_out)
+        if self.comm.size > 1:
+            rho_out = self.comm.sum(rho_out)
         diff = math.sqrt(float(np.mean((rho_out - self.rho) ** 2)))
         if hasattr(self.backend, "observe"):
             self.backend.observe(diff)
@@ -449,7 +464,7 @@ class ScfState:
         self.energy = e_band - int_vin_rho + e_h + e_xc + self.e_ion + self.psp_core - e_ent
         self.terms = dict(band=e_band, hartree=e_h, xc=e_xc, vin_rho=int_vin_rho, ion_ion=self.e_ion, psp_core=self.psp_core, entropy=e_ent)
         self.history.append((self.it, self.energy, diff, time.perf_counter() - self.t0))
-        if self.verbose:
+        if self.verbose and self.comm.rank == 0:
             print(f"scf {self.it:3d}  E={self.energy:.10f} Ry  drho={diff:.3e}", flush=True)
         if p.energy_target is not None and p.energy_tol_per_atom is not None:
             if abs(self.energy - p.energy_target) / len(c.atom_species) < p.energy_tol_per_atom:
@@ -477,8 +492,10 @@ class ScfState:
                          time.perf_counter() - self.t0)
 
 
-def run_scf(c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False) -> ScfResult:
-    st = ScfState(c, p, backend, verbose)
+def run_scf(c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False, comm=None) -> ScfResult:
+    """The SCF loop.  ``comm`` (a kpar.KpointComm) deals the k-points over the ranks of a process
+    group; every rank returns the same result."""
+    st = ScfState(c, p, backend, verbose, comm)
     while not st.done:
         opts, inits = st.begin()
         diags = [inp.basis.kinetic for inp in st.kin]
