@@ -10,8 +10,10 @@
 //   3. Eigenvectors of T by inverse iteration on a row-pivoted LU of T - lambda I (three sweeps
 //      from a hashed start vector).  Eigenvalues closer than 1e-5 ||T|| form a group whose vectors
 //      one thread computes in order, re-orthogonalising (modified Gram-Schmidt) after each solve.
-//   4. Back-transformation E = H_0 H_1 ... H_{m-2} Z with the stored reflectors, one warp per
-//      eigenvector, the vector held in shared memory.
+//   4. Back-transformation E = H_0 H_1 ... H_{m-2} Z with the stored reflectors.  Small problems:
+//      one warp per eigenvector, the vector held in shared memory.  From m = 192 and nev = 32 on:
+//      blocks of 64 reflectors in compact WY form (I - V T V^H, as LAPACK's zlarft/zlarfb), each
+//      block applied to all eigenvectors at once by three complex GEMMs.
 #include <cfloat>
 #include <cmath>
 
@@ -408,6 +410,121 @@ __global__ void __launch_bounds__(BT_WARPS * 32) k_hetrd_back(const double2* __r
   for (int i = lane; i < m; i += 32) E[(size_t)j * lde + i] = ev[i];
 }
 
+// ---- blocked back-transformation (compact WY) ----------------------------------------------------
+// The reflectors k0 .. k0+nb-1 multiply to H_k0 ... H_{k0+nb-1} = I - V T V^H with T upper
+// triangular, T[j][j] = tau_j and T[0:j, j] = -tau_j T[0:j, 0:j] (V[:, 0:j]^H v_j).  Then
+// E <- E - V (T (V^H E)) is three GEMMs; the blocks are applied from the last to the first.
+constexpr int kWyB = 64;
+
+// Vb (m x nb, column-major): v_{k0+j} with its implicit unit at row k0+j+1 and zeros above.
+__global__ void k_wy_v(const double2* __restrict__ A, int m, int k0, int nb, double2* __restrict__ Vb) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= (long)m * nb) return;
+  const int j = (int)(idx / m), row = (int)(idx - (long)j * m);
+  const int k = k0 + j;
+  double2 v = make_double2(0.0, 0.0);
+  if (row == k + 1) v = make_double2(1.0, 0.0);
+  else if (row > k + 1) v = A[row + (long)k * m];
+  Vb[idx] = v;
+}
+
+// T (ld kWyB) from G = V^H V (ld kWyB) and tau[k0 ...]: one CTA of 4 x kWyB threads, G and T in
+// shared memory.  Column j needs the triangular product T[0:j, 0:j] G[0:j, j]; its row i is summed
+// by the four consecutive lanes of row group i (terms l = i + q, i + q + 4, ...) and two shuffles.
+constexpr int kWyTThreads = 4 * kWyB;
+constexpr size_t kWyTSmem = sizeof(double2) * 2 * kWyB * (kWyB + 1);
+__global__ void __launch_bounds__(kWyTThreads) k_wy_t(const double2* __restrict__ G, const double2* __restrict__ tau, int k0,
+                                                      int nb, double2* __restrict__ T) {
+  extern __shared__ __align__(16) unsigned char wsm[];
+  double2(*gs)[kWyB + 1] = reinterpret_cast<double2(*)[kWyB + 1]>(wsm);  // gs[col][row]
+  double2(*ts)[kWyB + 1] = gs + kWyB;                                   // ts[col][row]
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < kWyB * kWyB; idx += kWyTThreads) {
+    const int r = idx % kWyB, c = idx / kWyB;
+    gs[c][r] = (r < nb && c < nb) ? G[r + c * kWyB] : make_double2(0.0, 0.0);
+    ts[c][r] = make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  const int i = tid >> 2, q = tid & 3;
+  for (int j = 0; j < nb; ++j) {
+    double2 sum = make_double2(0.0, 0.0);
+    if (i < j)
+      for (int l = i + q; l < j; l += 4) sum = cadd(sum, cmul(ts[l][i], gs[j][l]));
+    sum.x += __shfl_xor_sync(0xffffffffu, sum.x, 1);
+    sum.y += __shfl_xor_sync(0xffffffffu, sum.y, 1);
+    sum.x += __shfl_xor_sync(0xffffffffu, sum.x, 2);
+    sum.y += __shfl_xor_sync(0xffffffffu, sum.y, 2);
+    if (q == 0) {
+      const double2 tj = tau[k0 + j];
+      if (i < j) ts[j][i] = cscale(cmul(tj, sum), -1.0);
+      else if (i == j) ts[j][i] = tj;
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < kWyB * kWyB; idx += kWyTThreads) {
+    const int r = idx % kWyB, c = idx / kWyB;
+    T[r + c * kWyB] = ts[c][r];
+  }
+}
+
+__global__ void k_real_to_complex(const double* __restrict__ Z, int m, int nev, double2* __restrict__ E, long lde) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= (long)m * nev) return;
+  const int j = (int)(idx / m), row = (int)(idx - (long)j * m);
+  E[row + j * lde] = make_double2(Z[idx], 0.0);
+}
+
+int heev_back_blocked(const double2* A, const double2* tau, int m, int nev, const double* Z, double2* E, long lde,
+                      const HeevWork& w, cudaStream_t s) {
+  double2* Vb = w.wy;
+  double2* G = Vb + (size_t)m * kWyB;
+  double2* T = G + kWyB * kWyB;
+  double2* W = T + kWyB * kWyB;
+  double2* W2 = W + (size_t)kWyB * nev;
+  double2* ws = W2 + (size_t)kWyB * nev;
+  k_real_to_complex<<<ceil_div((size_t)m * nev, 256), 256, 0, s>>>(Z, m, nev, E, lde);
+  count_launch();
+  const int nref = m - 1;
+  const int nblk = (nref + kWyB - 1) / kWyB;
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int k0 = b * kWyB, nb = std::min(kWyB, nref - k0);
+    const int rows = m - k0 - 1;  // rows k0+1 .. m-1 hold the block's reflectors
+    k_wy_v<<<ceil_div((size_t)m * nb, 256), 256, 0, s>>>(A, m, k0, nb, Vb);
+    count_launch();
+    GemmArgs g{};
+    // G = V^H V
+    g.M = nb; g.N = nb; g.K = rows;
+    g.A = Vb + k0 + 1; g.lda = m; g.a_kc = true; g.conj_a = true;
+    g.B = Vb + k0 + 1; g.ldb = m; g.b_kc = true; g.conj_b = false;
+    g.O = G; g.ldo_r = 1; g.ldo_c = kWyB; g.alpha = 1.0; g.beta = 0.0;
+    DFT_TRY(zgemm(g, s, ws, w.wy_ws_elems));
+    k_wy_t<<<1, kWyTThreads, kWyTSmem, s>>>(G, tau, k0, nb, T);
+    count_launch();
+    // W = V^H E
+    g = GemmArgs{};
+    g.M = nb; g.N = nev; g.K = rows;
+    g.A = Vb + k0 + 1; g.lda = m; g.a_kc = true; g.conj_a = true;
+    g.B = E + k0 + 1; g.ldb = lde; g.b_kc = true; g.conj_b = false;
+    g.O = W; g.ldo_r = 1; g.ldo_c = kWyB; g.alpha = 1.0; g.beta = 0.0;
+    DFT_TRY(zgemm(g, s, ws, w.wy_ws_elems));
+    // W2 = T W
+    g = GemmArgs{};
+    g.M = nb; g.N = nev; g.K = nb;
+    g.A = T; g.lda = kWyB; g.a_kc = false; g.conj_a = false;
+    g.B = W; g.ldb = kWyB; g.b_kc = true; g.conj_b = false;
+    g.O = W2; g.ldo_r = 1; g.ldo_c = kWyB; g.alpha = 1.0; g.beta = 0.0;
+    DFT_TRY(zgemm(g, s, ws, w.wy_ws_elems));
+    // E[k0+1:, :] -= V W2
+    g = GemmArgs{};
+    g.M = rows; g.N = nev; g.K = nb;
+    g.A = Vb + k0 + 1; g.lda = m; g.a_kc = false; g.conj_a = false;
+    g.B = W2; g.ldb = kWyB; g.b_kc = true; g.conj_b = false;
+    g.O = E + k0 + 1; g.ldo_r = 1; g.ldo_c = lde; g.alpha = -1.0; g.beta = 1.0;
+    DFT_TRY(zgemm(g, s, ws, w.wy_ws_elems));
+  }
+  return DFTCUDA_OK;
+}
+
 __global__ void k_upper_to_full(const double2* __restrict__ src, long lds, double2* __restrict__ A, int m) {
   const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (idx >= (long)m * m) return;
@@ -422,10 +539,16 @@ __global__ void k_upper_to_full(const double2* __restrict__ src, long lds, doubl
 
 }  // namespace
 
+// Split-K space of the blocked back-transformation's GEMMs: up to 32 partial kWyB x nev products.
+static size_t wy_ws_elems(int nev) { return (size_t)32 * kWyB * std::max(nev, kWyB); }
+static size_t wy_elems(int m, int nev) {
+  return (size_t)m * kWyB + 2 * kWyB * kWyB + 2 * (size_t)kWyB * nev + wy_ws_elems(nev);
+}
+
 size_t heev_work_bytes(int m, int nev) {
   const size_t mm = (size_t)m;
-  return 256 * 8 + sizeof(double) * (3 * mm + 1) + sizeof(double2) * (1 + kHtMaxSplit) * mm + sizeof(double) * mm * nev +
-         sizeof(double) * 5 * mm * nev;
+  return 256 * 9 + sizeof(double) * (3 * mm + 1) + sizeof(double2) * (1 + kHtMaxSplit) * mm + sizeof(double) * mm * nev +
+         sizeof(double) * 5 * mm * nev + sizeof(double2) * wy_elems(m, nev);
 }
 
 void heev_bind(HeevWork& w, void* base, int m, int nev) {
@@ -440,6 +563,8 @@ void heev_bind(HeevWork& w, void* base, int m, int nev) {
   w.y = (double2*)take(sizeof(double2) * m * kHtMaxSplit);
   w.z = (double*)take(sizeof(double) * (size_t)m * nev);
   w.lu = (double*)take(sizeof(double) * 5 * (size_t)m * nev);
+  w.wy_ws_elems = wy_ws_elems(nev);
+  w.wy = (double2*)take(sizeof(double2) * wy_elems(m, nev));
   w.m_cap = m;
   w.nev_cap = nev;
 }
@@ -457,6 +582,7 @@ int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde,
     DFT_CUDA_TRY(cudaFuncSetAttribute(k_hetrd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tr));
     DFT_CUDA_TRY(cudaFuncSetAttribute(k_hetrd_back, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(sizeof(double2) * BT_WARPS * 2048)));
+    DFT_CUDA_TRY(cudaFuncSetAttribute(k_wy_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWyTSmem));
     DFT_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
     DFT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hetrd, HT_THREADS, smem_tr));
     attr_dev = dev;
@@ -487,8 +613,12 @@ int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde,
   count_launch();
   k_tridiag_invit<<<ceil_div(nev, 64), 64, 0, s>>>(w.d, w.e, m, nev, evals, w.tnorm, w.z, w.lu);
   count_launch();
-  k_hetrd_back<<<ceil_div(nev, BT_WARPS), BT_WARPS * 32, sizeof(double2) * BT_WARPS * m, s>>>(A, w.tau, m, nev, w.z, E, lde);
-  count_launch();
+  if (m >= 192 && nev >= 32) {
+    DFT_TRY(heev_back_blocked(A, w.tau, m, nev, w.z, E, lde, w, s));
+  } else {
+    k_hetrd_back<<<ceil_div(nev, BT_WARPS), BT_WARPS * 32, sizeof(double2) * BT_WARPS * m, s>>>(A, w.tau, m, nev, w.z, E, lde);
+    count_launch();
+  }
   DFT_CUDA_TRY(cudaGetLastError());
   return DFTCUDA_OK;
 }

@@ -152,7 +152,7 @@ static int pick_splits(int M, int N, int K) {
   const long tiles = (long)ceil_div(M, BM) * ceil_div(N, BN);
   const long wave = 2 * 148;
   if (tiles >= wave || K < 4 * BK * 8) return 1;
-  const long maxs = std::max<long>(1, K / (BK * 64));  // at least 64 K slices per split
+  const long maxs = std::max<long>(1, K / (BK * 8));  // at least 8 K slices per split
   long best = 1;
   double best_eff = 0.0;
   for (long sp = 1; sp <= std::min<long>(maxs, 64); ++sp) {
@@ -190,7 +190,7 @@ int zgemm(const GemmArgs& g, cudaStream_t s, double2* ws, size_t ws_elems) {
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "zgemm: K must be positive");
   }
   int splits = g.splits > 0 ? std::min(g.splits, std::max(1, g.K / 32)) : pick_splits(g.M, g.N, g.K);
-  if (splits > 1 && (size_t)splits * g.M * g.N > ws_elems) splits = 1;
+  if (splits > 1) splits = (int)std::max<size_t>(1, std::min<size_t>(splits, ws_elems / ((size_t)g.M * g.N)));  // what fits the workspace
   int kps = (g.K + splits - 1) / splits;
   kps = ((kps + BK - 1) / BK) * BK;
   splits = (g.K + kps - 1) / kps;
