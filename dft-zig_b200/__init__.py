@@ -61,6 +61,13 @@ ABI_SYMBOLS = (
     "dftcuda_fno_forward",
     "dftcuda_fno_loss_grad",
     "dftcuda_fno_train",
+    "dftcuda_complex_gemm",
+    "dftcuda_pctx_create",
+    "dftcuda_pctx_destroy",
+    "dftcuda_hxc_potential",
+    "dftcuda_potential_real",
+    "dftcuda_pulay_mix",
+    "dftcuda_pulay_reset",
 )
 
 PRECOND_REFERENCE = 0  # r / (|k+G|^2 - lambda), lobpcg/common.zig:214-226
@@ -173,6 +180,10 @@ class _Profile(ct.Structure):
     _fields_ = [(f, ct.c_uint64) for f in PROFILE_FIELDS]
 
 
+class _HxcTerms(ct.Structure):
+    _fields_ = [("e_hartree", ct.c_double), ("e_xc", ct.c_double), ("int_vin_rho", ct.c_double)]
+
+
 _lib = None
 
 
@@ -217,6 +228,14 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.dftcuda_fno_loss_grad.argtypes = [sz, vp, vp, vp, vp, vp, dp, vp]
     lib.dftcuda_fno_train.argtypes = [sz, vp, vp, vp, vp, vp, sz, ct.c_float, dp]
     lib.dftcuda_eig_solve_batch.argtypes = [sz, pp, pp, sz, ct.POINTER(_EigOpts), pp, ct.POINTER(ct.c_size_t), pp, pp, ct.POINTER(_EigInfo)]
+    lib.dftcuda_pctx_create.argtypes = [ct.POINTER(vp), ip, ip, ip, ct.c_double, vp, ip]
+    lib.dftcuda_pctx_destroy.argtypes = [vp]
+    lib.dftcuda_hxc_potential.argtypes = [vp, dp, dp, dp, ct.POINTER(_HxcTerms)]
+    lib.dftcuda_potential_real.argtypes = [vp, dp, dp, dp]
+    lib.dftcuda_pulay_mix.argtypes = [vp, dp, dp, sz, ct.c_double]
+    lib.dftcuda_pulay_reset.argtypes = [vp]
+    lb = ct.c_long
+    lib.dftcuda_complex_gemm.argtypes = [ip, sz, sz, sz, vp, lb, ip, ip, vp, lb, ip, ip, vp, lb, lb, ct.c_double, ct.c_double]
     _lib = lib
     return lib
 
@@ -557,6 +576,134 @@ def fno_train(params, samples, steps: int, lr: float = 1e-3):
     hist = np.zeros(steps, dtype=np.float64)
     _check(lib.dftcuda_fno_train(len(samples), _ptr(dims), _ptr(offs), _ptr(u), _ptr(t), _ptr(p), steps, lr, _ptr(hist)))
     return p, hist
+
+
+class PotentialContext:
+    """SCF potential build and Pulay mixing on the device (dftcuda_pctx_*): the FFT box `dims`
+    (nx, ny, nz; x fastest), the cell volume, the reciprocal vectors (rows b1, b2, b3) and the Pulay
+    history length.  Arrays may be numpy (host) or CUDA torch tensors; results come back in the
+    kind given (numpy in -> numpy out)."""
+
+    def __init__(self, dims, volume: float, recip, history: int = 8):
+        lib = load_library()
+        _require_device()
+        self.dims = tuple(int(d) for d in dims)
+        self.N = self.dims[0] * self.dims[1] * self.dims[2]
+        r = np.ascontiguousarray(np.asarray(recip, dtype=np.float64).reshape(3, 3))
+        h = ct.c_void_p()
+        _check(lib.dftcuda_pctx_create(ct.byref(h), *self.dims, float(volume), r.ctypes.data, int(history)))
+        self._h = h
+
+    def _out_like(self, ref, shape, dtype):
+        if _is_torch_cuda(ref):
+            import torch
+
+            return torch.empty(shape, dtype={np.complex128: torch.complex128, np.float64: torch.float64}[dtype], device=ref.device)
+        return np.empty(shape, dtype=dtype)
+
+    def hxc(self, rho, v_in=None, out=None):
+        """(V_H + V_xc)(G) of rho(r) and the energy terms {e_hartree, e_xc, int_vin_rho}."""
+        rho = _as_array(rho, np.float64, self.N)
+        v_in = None if v_in is None else _as_array(v_in, np.complex128, self.N)
+        if out is None:
+            out = self._out_like(rho, (self.N,), np.complex128)
+        t = _HxcTerms()
+        _check(load_library().dftcuda_hxc_potential(self._h, _ptr(rho), _ptr(v_in) if v_in is not None else None, _ptr(out), ct.byref(t)))
+        return out, {"e_hartree": t.e_hartree, "e_xc": t.e_xc, "int_vin_rho": t.int_vin_rho}
+
+    def real(self, v_g, vloc=None, out=None):
+        """V(r) = vloc(r) + FFT^-1 v(G) (the local potential for set_vloc)."""
+        v_g = _as_array(v_g, np.complex128, self.N)
+        vloc = None if vloc is None else _as_array(vloc, np.float64, self.N)
+        if out is None:
+            out = self._out_like(v_g, (self.N,), np.float64)
+        _check(load_library().dftcuda_potential_real(self._h, _ptr(v_g), _ptr(vloc) if vloc is not None else None, _ptr(out)))
+        return out
+
+    def pulay_mix(self, x, residual, beta: float):
+        """Pulay step in place on x (float64, any length; complex arrays as their interleaved view)."""
+        n = _nbytes(x) // 8
+        if _nbytes(residual) != _nbytes(x):
+            raise InvalidMatrixSize("pulay_mix: x and residual differ in size")
+        _check(load_library().dftcuda_pulay_mix(self._h, _ptr(x), _ptr(residual), n, float(beta)))
+        return x
+
+    def reset(self):
+        _check(load_library().dftcuda_pulay_reset(self._h))
+
+    def close(self):
+        if self._h:
+            load_library().dftcuda_pctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _is_torch_cuda(a) -> bool:
+    return type(a).__module__.startswith("torch") and getattr(a, "is_cuda", False)
+
+
+def _as_array(a, dtype, n):
+    """A contiguous array of n elements of dtype: CUDA tensors are checked, numpy data converted."""
+    if _is_torch_cuda(a):
+        import torch
+
+        want = {np.complex128: torch.complex128, np.float64: torch.float64}[dtype]
+        if a.dtype != want or a.numel() != n or not a.is_contiguous():
+            raise InvalidMatrixSize(f"expected a contiguous CUDA tensor of {n} {want}")
+        return a
+    a = np.ascontiguousarray(a, dtype=dtype)
+    if a.size != n:
+        raise InvalidMatrixSize(f"expected {n} elements, got {a.size}")
+    return a
+
+
+def _nbytes(a) -> int:
+    if _is_torch_cuda(a):
+        return a.numel() * a.element_size()
+    return np.asarray(a).nbytes
+
+
+def complex_gemm(a, b, out=None, *, conj_a: bool = False, conj_b: bool = False, precision: int = 0, alpha: float = 1.0,
+                 beta: float = 0.0):
+    """out[r, c] = alpha * sum_k opA(a)[r, k] opB(b)[c, k] + beta * out[r, c] on the GPU
+    (dftcuda_complex_gemm): a (M, K) and b (N, K) CUDA complex128 tensors, each with a unit stride
+    along one of its two dimensions; opX conjugates when conj_x.  precision 0 runs the FP64 kernel,
+    PRECISION_TF32 / PRECISION_TF32X3 the tensor-core kernels.  Returns out (allocated (M, N) when
+    None)."""
+    import torch
+
+    lib = load_library()
+    _require_device()
+
+    def layout(t, name):
+        if t.dtype != torch.complex128 or not t.is_cuda or t.dim() != 2:
+            raise InvalidArgument(f"complex_gemm: {name} must be a 2-D CUDA complex128 tensor")
+        sr, sk = t.stride()
+        if sk == 1:
+            return 1, max(sr, 1)
+        if sr == 1:
+            return 0, max(sk, 1)
+        raise InvalidArgument(f"complex_gemm: {name} needs a unit stride along one dimension")
+
+    M, K = a.shape
+    N, K2 = b.shape
+    if K2 != K:
+        raise InvalidMatrixSize("complex_gemm: a and b disagree on K")
+    if out is None:
+        out = torch.zeros((M, N), dtype=torch.complex128, device=a.device)
+    if tuple(out.shape) != (M, N) or out.dtype != torch.complex128:
+        raise InvalidMatrixSize("complex_gemm: out must be (M, N) complex128")
+    a_kc, lda = layout(a, "a")
+    b_kc, ldb = layout(b, "b")
+    torch.cuda.synchronize(a.device)
+    _check(lib.dftcuda_complex_gemm(int(precision), M, N, K, a.data_ptr(), lda, a_kc, int(conj_a), b.data_ptr(), ldb, b_kc,
+                                    int(conj_b), out.data_ptr(), out.stride(0), out.stride(1), float(alpha), float(beta)))
+    return out
 
 
 def hermitian_eigen_decomp(a, nev: Optional[int] = None) -> EigenDecomp:

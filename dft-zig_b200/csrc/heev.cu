@@ -4,7 +4,8 @@
 // m <= 2048:
 //   1. Householder reduction to real symmetric tridiagonal form Q^H A Q = T, reflectors chosen as
 //      in LAPACK's zlarfg so the off-diagonal of T is real.  One cooperative launch; the matrix
-//      stays in L2 (m = 2048: 64 MB) and each column costs two grid barriers (bounded waits).
+//      stays in L2 (m = 2048: 64 MB) and each column costs one grid barrier (bounded waits): the
+//      rank-2 update of step k and the matrix-vector product of step k+1 share one sweep.
 //   2. The nev lowest eigenvalues of T by Sturm-count multisection: one warp per eigenvalue, its
 //      32 lanes evaluate the count at 32 interior points, so the bracket shrinks 33x per round.
 //   3. Eigenvectors of T by inverse iteration on a row-pivoted LU of T - lambda I (three sweeps
@@ -16,6 +17,8 @@
 //      block applied to all eigenvectors at once by three complex GEMMs.
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
+#include <string>
 
 #include "kctx.cuh"
 
@@ -198,6 +201,174 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd(double2* __restrict__ A, i
     if (!grid_sync(bar)) return;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) dd[m - 1] = __ldcg(A + (long)(m - 1) * m + (m - 1)).x;
+}
+
+// Householder reflector of x[0 .. n) in shared memory (zlarfg: x[0] = alpha), by every thread of the
+// block: x becomes v (v[0] = 1), returns tau and beta with H^H x = beta e_1, H = I - tau v v^H.
+__device__ void block_reflector(double2* x, int n, double2* red, double2& t, double& beta) {
+  const int tid = threadIdx.x;
+  double2 part = make_double2(0.0, 0.0);
+  for (int i = tid + 1; i < n; i += HT_THREADS) part.x += x[i].x * x[i].x + x[i].y * x[i].y;
+  const double xnorm2 = block_sum2(part, red).x;
+  const double2 alpha = x[0];
+  t = make_double2(0.0, 0.0);
+  beta = alpha.x;
+  if (!(xnorm2 == 0.0 && alpha.y == 0.0)) {
+    beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2), alpha.x);
+    t = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+  }
+  const bool active = !(t.x == 0.0 && t.y == 0.0);
+  const double2 den = make_double2(alpha.x - beta, alpha.y);  // v = x / (alpha - beta)
+  const double dn2 = den.x * den.x + den.y * den.y;
+  const double2 sc = active ? make_double2(den.x / dn2, -den.y / dn2) : make_double2(0.0, 0.0);
+  __syncthreads();
+  for (int i = tid; i < n; i += HT_THREADS) x[i] = i == 0 ? make_double2(1.0, 0.0) : cmul(x[i], sc);
+  __syncthreads();
+}
+
+// Step 1 with one grid barrier per column.  The update of step k and the matrix-vector product of
+// step k+1 share one sweep over the trailing matrix: every block first applies step k's rank-2
+// update to column k+1 alone (redundantly, from the unmodified global copy) and forms reflector
+// k+1 from it, so the warps that then update a (column, row chunk) pair of the trailing matrix
+// can take its partial product with v_{k+1} while the updated entries are in registers.  Column
+// k+1 itself is never updated in global memory: its reflector is written there instead.  The
+// trailing matrix is read once and written once per column (the two-barrier form reads it twice).
+// The partial products alternate between two halves of y by step parity: a block still summing
+// step k's partials while another already writes step k+1's never shares a buffer with it.
+__global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, int m, double* __restrict__ dd,
+                                                       double* __restrict__ ee, double2* __restrict__ tau,
+                                                       double2* __restrict__ y, GridBarrier bar) {
+  extern __shared__ double2 hsm[];
+  double2* sv = hsm;          // v_k (n1 entries)
+  double2* sw = hsm + m;      // w_k
+  double2* sn = hsm + 2 * m;  // v_{k+1}
+  __shared__ double2 red[HT_WARPS];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int gw = blockIdx.x * HT_WARPS + (tid >> 5);
+  const int W = gridDim.x * HT_WARPS;
+  // prologue: reflector 0 and the partial products of step 0
+  double2 t;
+  double beta;
+  {
+    const int n1 = m - 1;
+    for (int i = tid; i < n1; i += HT_THREADS) sv[i] = __ldcg(A + 1 + i);
+    __syncthreads();
+    block_reflector(sv, n1, red, t, beta);
+    if (blockIdx.x == 0 && tid == 0) {
+      dd[0] = __ldcg(A).x;
+      ee[0] = beta;
+      tau[0] = t;
+    }
+  }
+  int S_prev;
+  {
+    const int n1 = m - 1;
+    const int S = max(1, min(kHtMaxSplit, W / max(n1, 1)));
+    const int chunk = (n1 + S - 1) / S;
+    for (int g = gw; g < n1 * S; g += W) {
+      const int c = g / S, sidx = g - c * S;
+      const int r = 1 + c;
+      const int i0 = sidx * chunk, i1 = min(n1, i0 + chunk);
+      const double2* ac = A + (long)r * m + 1;
+      double sx = 0.0, sy = 0.0;
+      for (int i = i0 + lane; i < i1; i += 32) {
+        const double2 a = __ldcg(ac + i), v = sv[i];
+        sx += a.x * v.x + a.y * v.y;  // conj(a) v
+        sy += a.x * v.y - a.y * v.x;
+      }
+      sx = warp_sum(sx);
+      sy = warp_sum(sy);
+      if (lane == 0) y[(long)sidx * m + r] = make_double2(sx, sy);
+    }
+    S_prev = S;
+  }
+  if (!grid_sync(bar)) return;
+  for (int k = 0; k + 1 < m; ++k) {
+    const int n1 = m - k - 1;
+    const double2* yk = y + (size_t)(k & 1) * kHtMaxSplit * m;      // step k's partials
+    double2* yn = y + (size_t)((k + 1) & 1) * kHtMaxSplit * m;      // step k+1's
+    // (1) y = tau A22 v from the partial products; w = y + alpha v, alpha = -tau (y^H v) / 2
+    {
+      double2 p2 = make_double2(0.0, 0.0);
+      for (int i = tid; i < n1; i += HT_THREADS) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int q = 0; q < S_prev; ++q) acc = cadd(acc, __ldcg(yk + (long)q * m + k + 1 + i));
+        const double2 yi = cmul(t, acc), vi = sv[i];
+        sw[i] = yi;
+        p2.x += yi.x * vi.x + yi.y * vi.y;
+        p2.y += yi.x * vi.y - yi.y * vi.x;
+      }
+      const double2 sdot = block_sum2(p2, red);
+      const double2 al = cscale(cmul(t, sdot), -0.5);
+      for (int i = tid; i < n1; i += HT_THREADS) sw[i] = cadd(sw[i], cmul(al, sv[i]));
+      if (blockIdx.x == 0) {
+        // column k now holds its reflector (no block reads column k any more)
+        double2* cw = A + (long)k * m + (k + 1);
+        for (int i = tid; i < n1; i += HT_THREADS) cw[i] = i == 0 ? make_double2(beta, 0.0) : sv[i];
+      }
+      __syncthreads();
+    }
+    // (2) column k+1 after step k's update (rows k+1 .. m-1), its diagonal, and reflector k+1
+    const bool next = k + 2 < m;  // a reflector k+1 exists
+    double2 tn = make_double2(0.0, 0.0);
+    double betan = 0.0;
+    {
+      const double2* col = A + (long)(k + 1) * m + (k + 1);
+      const double2 w0c = cconj(sw[0]);  // v_0 = 1
+      for (int i = tid; i < n1; i += HT_THREADS) {
+        const double2 x = csub(__ldcg(col + i), cadd(cmul(sv[i], w0c), sw[i]));
+        if (i == 0) {
+          if (blockIdx.x == 0) dd[k + 1] = x.x;
+        } else {
+          sn[i - 1] = x;
+        }
+      }
+      __syncthreads();
+      if (next) {
+        block_reflector(sn, n1 - 1, red, tn, betan);
+        if (blockIdx.x == 0 && tid == 0) {
+          ee[k + 1] = betan;
+          tau[k + 1] = tn;
+        }
+      }
+    }
+    if (!next) break;
+    // (3) rank-2 update of columns k+2 .. m-1 (all rows k+1 .. m-1) and, on the updated entries,
+    // the partial products of step k+1 (rows k+2 ..)
+    {
+      const int nc = n1 - 1;
+      const int S = max(1, min(kHtMaxSplit, W / max(nc, 1)));
+      const int chunk = (n1 + S - 1) / S;
+      for (int g = gw; g < nc * S; g += W) {
+        const int c = 1 + g / S, sidx = g - (c - 1) * S;
+        const int r = k + 1 + c;
+        const int i0 = sidx * chunk, i1 = min(n1, i0 + chunk);
+        const double2 wr = cconj(sw[c]), vr = cconj(sv[c]);
+        double2* ac = A + (long)r * m + (k + 1);
+        double sx = 0.0, sy = 0.0;
+        for (int i = i0 + lane; i < i1; i += 32) {
+          double2 a = __ldcg(ac + i);
+          a = csub(a, cadd(cmul(sv[i], wr), cmul(sw[i], vr)));
+          ac[i] = a;
+          if (i > 0) {
+            const double2 v = sn[i - 1];
+            sx += a.x * v.x + a.y * v.y;  // conj(a) v
+            sy += a.x * v.y - a.y * v.x;
+          }
+        }
+        sx = warp_sum(sx);
+        sy = warp_sum(sy);
+        if (lane == 0) yn[(long)sidx * m + r] = make_double2(sx, sy);
+      }
+      S_prev = S;
+    }
+    if (!grid_sync(bar)) return;
+    double2* tmp = sv;
+    sv = sn;
+    sn = tmp;
+    t = tn;
+    beta = betan;
+  }
 }
 
 // Number of eigenvalues of T below x (Sturm sequence of the LDL^T pivots).
@@ -547,7 +718,7 @@ static size_t wy_elems(int m, int nev) {
 
 size_t heev_work_bytes(int m, int nev) {
   const size_t mm = (size_t)m;
-  return 256 * 9 + sizeof(double) * (3 * mm + 1) + sizeof(double2) * (1 + kHtMaxSplit) * mm + sizeof(double) * mm * nev +
+  return 256 * 9 + sizeof(double) * (3 * mm + 1) + sizeof(double2) * (1 + 2 * kHtMaxSplit) * mm + sizeof(double) * mm * nev +
          sizeof(double) * 5 * mm * nev + sizeof(double2) * wy_elems(m, nev);
 }
 
@@ -560,7 +731,7 @@ void heev_bind(HeevWork& w, void* base, int m, int nev) {
   w.e = (double*)take(sizeof(double) * m);
   w.tnorm = (double*)take(sizeof(double));
   w.tau = (double2*)take(sizeof(double2) * m);
-  w.y = (double2*)take(sizeof(double2) * m * kHtMaxSplit);
+  w.y = (double2*)take(sizeof(double2) * m * 2 * kHtMaxSplit);  // two halves for the one-barrier form
   w.z = (double*)take(sizeof(double) * (size_t)m * nev);
   w.lu = (double*)take(sizeof(double) * 5 * (size_t)m * nev);
   w.wy_ws_elems = wy_ws_elems(nev);
@@ -577,14 +748,21 @@ int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde,
   static int n_sm = 0, per_sm = 0;
   int dev = 0;
   DFT_CUDA_TRY(cudaGetDevice(&dev));
-  const size_t smem_tr = sizeof(double2) * 2 * 2048;
+  // DFTCUDA_HETRD=2barrier selects the two-barrier tridiagonalisation (A/B measurements)
+  static const bool two_barrier = [] {
+    const char* e = std::getenv("DFTCUDA_HETRD");
+    return e && std::string(e) == "2barrier";
+  }();
+  const void* hetrd_fn = two_barrier ? (const void*)k_hetrd : (const void*)k_hetrd1;
+  const int hetrd_bufs = two_barrier ? 2 : 3;  // shared-memory vectors of m entries
+  const size_t smem_tr = sizeof(double2) * hetrd_bufs * 2048;
   if (attr_dev != dev) {
-    DFT_CUDA_TRY(cudaFuncSetAttribute(k_hetrd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tr));
+    DFT_CUDA_TRY(cudaFuncSetAttribute(hetrd_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tr));
     DFT_CUDA_TRY(cudaFuncSetAttribute(k_hetrd_back, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(sizeof(double2) * BT_WARPS * 2048)));
     DFT_CUDA_TRY(cudaFuncSetAttribute(k_wy_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWyTSmem));
     DFT_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-    DFT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hetrd, HT_THREADS, smem_tr));
+    DFT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_fn, HT_THREADS, smem_tr));
     attr_dev = dev;
   }
   if (per_sm < 1) return fail(DFTCUDA_ERR_UNSUPPORTED, "heev: tridiagonalisation kernel does not fit an SM");
@@ -602,8 +780,8 @@ int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde,
     double2* t_ = w.tau;
     double2* y_ = w.y;
     void* args[] = {&a_, &m_, &d_, &e_, &t_, &y_, &bar};
-    DFT_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_hetrd, dim3(bar.nblocks), dim3(HT_THREADS), args,
-                                             sizeof(double2) * 2 * m, s));
+    DFT_CUDA_TRY(cudaLaunchCooperativeKernel(hetrd_fn, dim3(bar.nblocks), dim3(HT_THREADS), args,
+                                             sizeof(double2) * hetrd_bufs * m, s));
     count_launch();
   } else {
     DFT_CUDA_TRY(cudaMemcpyAsync(w.d, A, sizeof(double), cudaMemcpyDeviceToDevice, s));

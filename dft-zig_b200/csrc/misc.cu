@@ -128,3 +128,49 @@ extern "C" int dftcuda_kctx_get_profile(dftcuda_kctx* c, dftcuda_profile* out) {
   *out = r;
   return DFTCUDA_OK;
 }
+
+// The library's complex GEMM for tests and benchmarks (zgemm.cu / tc_gemm.cu behind one call).
+extern "C" int dftcuda_complex_gemm(int precision, size_t M, size_t N, size_t K, const double* a, long lda, int a_kc,
+                                    int conj_a, const double* b, long ldb, int b_kc, int conj_b, double* out, long ldo_r,
+                                    long ldo_c, double alpha, double beta) {
+  using namespace dftcuda;
+  if (M == 0 || N == 0) return DFTCUDA_OK;
+  if (K == 0 || !a || !b || !out) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "complex_gemm: K == 0 or null pointer");
+  if (M > INT32_MAX || N > INT32_MAX || K > INT32_MAX)
+    return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "complex_gemm: dimension above 2^31 - 1");
+  if (precision != DFTCUDA_PRECISION_FP64 && !precision_uses_tc(precision))
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "complex_gemm: precision must be FP64, TF32 or TF32X3");
+  GemmArgs g{};
+  g.M = (int)M; g.N = (int)N; g.K = (int)K;
+  g.A = reinterpret_cast<const double2*>(a); g.lda = lda; g.a_kc = a_kc != 0; g.conj_a = conj_a != 0;
+  g.B = reinterpret_cast<const double2*>(b); g.ldb = ldb; g.b_kc = b_kc != 0; g.conj_b = conj_b != 0;
+  g.O = reinterpret_cast<double2*>(out); g.ldo_r = ldo_r; g.ldo_c = ldo_c;
+  g.alpha = alpha; g.beta = beta;
+  const bool tc = precision_uses_tc(precision);
+  const size_t ws_elems = tc ? cgemm_tf32_workspace_elems(g.M, g.N, g.K) : zgemm_workspace_elems(g.M, g.N, g.K);
+  cudaStream_t s = nullptr;
+  double2* ws = nullptr;
+  int* err = nullptr;
+  int rc = DFTCUDA_OK;
+  auto cleanup = [&] {
+    if (s) cudaStreamDestroy(s);
+    if (ws) cudaFree(ws);
+    if (err) cudaFree(err);
+  };
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+      (ws_elems && cudaMalloc(&ws, sizeof(double2) * ws_elems) != cudaSuccess) || cudaMalloc(&err, sizeof(int)) != cudaSuccess ||
+      cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) {
+    cleanup();
+    return fail(DFTCUDA_ERR_CUDA, "complex_gemm: stream or workspace allocation failed");
+  }
+  rc = tc ? cgemm_tf32(g, s, ws, ws_elems, err, precision == DFTCUDA_PRECISION_TF32X3) : zgemm(g, s, ws, ws_elems);
+  int herr = 0;
+  if (rc == DFTCUDA_OK) {
+    const cudaError_t e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    const cudaError_t e2 = cudaStreamSynchronize(s);
+    if (e != cudaSuccess || e2 != cudaSuccess) rc = fail(DFTCUDA_ERR_CUDA, std::string("complex_gemm: ") + cudaGetErrorString(e2));
+    else if (herr) rc = fail(DFTCUDA_ERR_TIMEOUT, "complex_gemm: a tensor-core pipeline wait timed out");
+  }
+  cleanup();
+  return rc;
+}

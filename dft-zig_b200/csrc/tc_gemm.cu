@@ -540,6 +540,374 @@ __global__ void __launch_bounds__(T2_THREADS) k_cgemm_tc2(int M, int N, int K, c
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TC_TMEM_COLS));
 }
 
+// ---- k_cgemm_tc3: warp-specialised 128 x 256 tiles ---------------------------------------------
+// For products whose both output dimensions reach 128 (Rayleigh-Ritz Gram matrices, subspace
+// rotations): a 256-column tile gives every converted operand element four times the MMA work of
+// the 64-column tiles above.  Warps 0-7 are converters: each thread owns three of the slot's 768
+// core-matrix rows (A: 16 row groups x 2 k groups x 8 rows, B: 32 x 2 x 8), loads their FP64
+// elements one K step ahead into registers, waits for the slot to be free, writes the TF32 planes
+// (hi and lo parts for 3xTF32) into the ring as 16-byte vectors and arrives on the slot's "full"
+// mbarrier.  Lane 0 of warp 8 waits for full slots and
+// issues one 8-deep K step per slot (12 MMAs for 3xTF32, 4 otherwise) of 128 x 256 x 8, committing
+// each slot back to its "empty" mbarrier.  TMEM holds the two 256-column FP32 accumulators (all 512
+// columns; the shared-memory footprint keeps one CTA per SM).  Waits are bounded; a timeout sets the
+// error flag and every role winds down (no asynchronous copies are used, so only the MMAs in flight
+// are waited for before the TMEM is freed).
+constexpr int T3_N = 256;
+constexpr int T3_K = 8;
+constexpr int T3_CONV_WARPS = 8;
+constexpr int T3_THREADS = 32 * (T3_CONV_WARPS + 1);
+constexpr int T3_APL = TC_M * T3_K * 4;  // one TF32 plane of the A slot (4 KB)
+constexpr int T3_BPL = T3_N * T3_K * 4;  // one TF32 plane of the B slot (8 KB)
+constexpr int T3_SLOT = 2 * T3_APL + 2 * T3_BPL;  // Ar, Ai, Br, Bi
+constexpr int T3_ACM = (TC_M / 8) * (T3_K / 4);   // 32 core matrices of A per slot
+constexpr int T3_BCM = (T3_N / 8) * (T3_K / 4);   // 64 of B
+constexpr uint32_t T3_TMEM_COLS = 512;
+__host__ __device__ constexpr int t3_slot(bool split) { return split ? 2 * T3_SLOT : T3_SLOT; }
+__host__ __device__ constexpr int t3_stages(bool split) { return split ? 4 : 8; }
+__host__ __device__ constexpr int t3_smem(bool split) { return t3_stages(split) * t3_slot(split) + 256; }  // + barriers, TMEM slot
+
+// Byte offset of (row, k) in a slot plane: core matrices of 8 rows x 4 k (128 B), the two k groups
+// of a row group adjacent (LBO 128 B), row groups 256 B apart (SBO).
+__device__ __forceinline__ uint32_t t3_off(int row, int k) {
+  return (uint32_t)((row >> 3) * 256 + (k >> 2) * 128 + (row & 7) * 16 + (k & 3) * 4);
+}
+__device__ __forceinline__ uint64_t t3_desc(uint32_t smem_addr) {
+  const uint64_t lbo = 128 >> 4, sbo = 256 >> 4;
+  return (uint64_t)((smem_addr >> 4) & 0x3FFF) | (lbo << 16) | (sbo << 32) | (1ULL << 46);
+}
+__device__ __forceinline__ uint32_t t3_idesc(bool neg_a) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(T3_N >> 3) << 17) |
+         ((uint32_t)(TC_M >> 4) << 24);
+}
+
+// One core-matrix row (4 consecutive k of one row) of an operand: hi parts (and lo parts for 3xTF32)
+// of its real and imaginary planes, stored as 16-byte vectors.  The split is taken in FP32: x is
+// rounded to FP32, hi = tf32(x) (round to nearest), lo = tf32(x - hi).
+template <bool CJ, bool SPLIT>
+__device__ __forceinline__ void t3_store_row(unsigned char* plane0, int plane_bytes, int slot_lo, uint32_t off,
+                                             const double2* v) {
+  float hr[4], hi[4], lr[4], li[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float fr = (float)v[j].x, fi = CJ ? -(float)v[j].y : (float)v[j].y;
+    if (SPLIT) {
+      hr[j] = tf32_rna(fr);
+      hi[j] = tf32_rna(fi);
+      lr[j] = tf32_rna(fr - hr[j]);
+      li[j] = tf32_rna(fi - hi[j]);
+    } else {
+      hr[j] = fr;
+      hi[j] = fi;
+    }
+  }
+  *reinterpret_cast<float4*>(plane0 + off) = make_float4(hr[0], hr[1], hr[2], hr[3]);
+  *reinterpret_cast<float4*>(plane0 + plane_bytes + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+  if (SPLIT) {
+    *reinterpret_cast<float4*>(plane0 + slot_lo + off) = make_float4(lr[0], lr[1], lr[2], lr[3]);
+    *reinterpret_cast<float4*>(plane0 + slot_lo + plane_bytes + off) = make_float4(li[0], li[1], li[2], li[3]);
+  }
+}
+
+__device__ __forceinline__ void t3_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(mbar) : "memory");
+}
+
+// The tensor cores' FP32 accumulation is not round-to-nearest: its error grows with the number of
+// accumulation steps (measured on 3xTF32 products: ~1e-5 relative after 1000 terms, ~1e-4 after
+// 120000).  So the FP32 accumulators only ever hold T3_CHUNK K steps (2048 terms): at each chunk
+// end the converter warps drain TMEM into FP64 sums kept in the destination (the output tile, or the
+// split's partial block), and the MMA warp starts the next chunk afresh once the drain is done.
+constexpr int T3_CHUNK = 256;  // default chunk, in K steps of 8
+
+// Drain of the TMEM accumulators into the FP64 destination by one converter warp (TMEM lanes
+// 32 (warp % 4) .. = rows, columns 128 (warp / 4) .. + 127).  first: this split's first chunk (the
+// destination starts as beta * out, or as the partial block).
+__device__ __forceinline__ void t3_drain(uint32_t d_re, uint32_t d_im, int warp, int lane, bool have, bool first, int M,
+                                         int N, int r0, int c0, double2* __restrict__ O, long ldo_r, long ldo_c,
+                                         double alpha, double beta, double2* __restrict__ part, int z) {
+  const int quarter = warp & 3, half = warp >> 2;
+  const int r = r0 + quarter * 32 + lane;
+  const uint32_t lane_addr = ((uint32_t)(quarter * 32) << 16);
+#pragma unroll 1
+  for (int ch = 0; ch < 16; ++ch) {
+    const int cbase = half * 128 + ch * 8;
+    if (c0 + cbase >= N) break;
+    uint32_t vr[8], vi[8];
+    if (have) {
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                   : "=r"(vr[0]), "=r"(vr[1]), "=r"(vr[2]), "=r"(vr[3]), "=r"(vr[4]), "=r"(vr[5]), "=r"(vr[6]), "=r"(vr[7])
+                   : "r"(d_re + lane_addr + cbase));
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                   : "=r"(vi[0]), "=r"(vi[1]), "=r"(vi[2]), "=r"(vi[3]), "=r"(vi[4]), "=r"(vi[5]), "=r"(vi[6]), "=r"(vi[7])
+                   : "r"(d_im + lane_addr + cbase));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) vr[j] = vi[j] = 0u;
+    }
+    if (r < M) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int c = c0 + cbase + j;
+        if (c >= N) continue;
+        const double re = (double)__uint_as_float(vr[j]), im = (double)__uint_as_float(vi[j]);
+        if (part) {
+          double2* o = part + ((long)z * N + c) * M + r;  // column-major partials
+          double2 v = make_double2(re, im);
+          if (!first) {
+            const double2 old = *o;
+            v.x += old.x;
+            v.y += old.y;
+          }
+          *o = v;
+        } else {
+          double2* o = O + (long)r * ldo_r + (long)c * ldo_c;
+          double2 v = make_double2(alpha * re, alpha * im);
+          const double2 old = (first && beta == 0.0) ? make_double2(0.0, 0.0) : *o;
+          const double b = first ? beta : 1.0;
+          v.x += b * old.x;
+          v.y += b * old.y;
+          *o = v;
+        }
+      }
+    }
+  }
+}
+
+template <bool AKC, bool BKC, bool CJA, bool CJB, bool SPLIT>
+__global__ void __launch_bounds__(T3_THREADS, 1) k_cgemm_tc3(int M, int N, int K, const double2* __restrict__ A, long lda,
+                                                             const double2* __restrict__ B, long ldb,
+                                                             double2* __restrict__ O, long ldo_r, long ldo_c,
+                                                             double alpha, double beta, int kps,
+                                                             double2* __restrict__ part, int* __restrict__ err,
+                                                             int chunk) {
+  extern __shared__ __align__(1024) unsigned char tsm3[];
+  constexpr int NS = t3_stages(SPLIT);
+  constexpr int SL = t3_slot(SPLIT);
+  // barriers: full[NS] (converters -> MMA), empty[NS] (MMA -> converters), chunk_done (MMA ->
+  // converters: a chunk's MMAs are complete), drained (converters -> MMA: TMEM read out), fin (all
+  // MMAs complete)
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm3 + NS * SL);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2 * NS + 3);
+  __shared__ volatile int s_abort;
+  __shared__ int s_issued;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int r0 = blockIdx.y * TC_M, c0 = blockIdx.x * T3_N;
+  const int kbeg = blockIdx.z * kps;
+  const int kend = min(K, kbeg + kps);
+  const int ntiles = kend > kbeg ? (kend - kbeg + T3_K - 1) / T3_K : 0;
+  const int nchunks = (ntiles + chunk - 1) / chunk;
+  const uint32_t ring = (uint32_t)__cvta_generic_to_shared(tsm3);
+  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(mbar);
+  const uint32_t mb_chunk = mb + 16 * NS, mb_drained = mb_chunk + 8, mb_fin = mb_chunk + 16;
+  if (tid == 0) {
+    s_abort = 0;
+    for (int q = 0; q < NS; ++q) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mb + 8 * q), "r"(T3_CONV_WARPS));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb + 8 * (NS + q)));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb_chunk));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mb_drained), "r"(T3_CONV_WARPS));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb_fin));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+  }
+  if (warp == T3_CONV_WARPS) {
+    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(tmem_slot);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(slot), "r"(T3_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t d_re = tmem, d_im = tmem + T3_N;
+  if (warp < T3_CONV_WARPS) {
+    // ---- converters (and, at chunk ends, the drain) ----
+    // Thread t owns three core-matrix rows per slot: unit t of A and units t, t + 256 of B, a unit
+    // being (row group, k group, row in group) with the row fastest, so 8 consecutive lanes fill one
+    // 128-byte core matrix (conflict-free 16-byte stores) and read consecutive rows (coalesced
+    // when rows are contiguous) or one 64-byte run each (K-contiguous storage).
+    const double2* up[3];
+    long ustep[3];
+    bool uok[3];
+    uint32_t uoff[3];
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+      const int unit = tid + u * T3_CONV_WARPS * 32;
+      const int cm = unit >> 3, r8 = unit & 7;
+      const bool isA = cm < T3_ACM;
+      const int cc = isA ? cm : cm - T3_ACM;
+      const int rg = cc >> 1, kg = cc & 1;
+      const int row = (isA ? r0 : c0) + rg * 8 + r8;
+      const bool kc = isA ? AKC : BKC;
+      const long ld = isA ? lda : ldb;
+      uok[u] = row < (isA ? M : N);
+      const double2* X = isA ? A : B;
+      up[u] = kc ? X + (long)(uok[u] ? row : 0) * ld + kbeg + kg * 4 : X + (long)(kbeg + kg * 4) * ld + (uok[u] ? row : 0);
+      ustep[u] = kc ? 1 : ld;  // between consecutive k
+      uoff[u] = (uint32_t)(rg * 256 + kg * 128 + r8 * 16);
+    }
+    double2 cur[12], nxt[12];
+    // loads of K step t (pointers advance by 8 k per step; the k bound only matters on the last)
+    auto load_step = [&](int t, double2* v) {
+      const int kk0 = kbeg + t * T3_K;
+      const bool full = kk0 + T3_K <= kend;
+#pragma unroll
+      for (int u = 0; u < 3; ++u) {
+        const int kgu = (int)((uoff[u] >> 7) & 1);
+        const double2* p = up[u] + (long)t * T3_K * ustep[u];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const bool ok = uok[u] && (full || kk0 + kgu * 4 + j < kend);
+          v[u * 4 + j] = ok ? __ldg(p + (long)j * ustep[u]) : make_double2(0.0, 0.0);
+        }
+      }
+    };
+    int drained = 0;  // chunks drained so far
+    // wait for chunk `drained` to finish, drain it, release the accumulators; false on abort
+    auto drain_next = [&]() -> bool {
+      int ok = 1;
+      if (lane == 0) ok = tc_wait(mb_chunk, (uint32_t)(drained & 1)) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        if (lane == 0) atomicExch(err, 1);
+        s_abort = 1;
+        return false;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      t3_drain(d_re, d_im, warp, lane, true, drained == 0, M, N, r0, c0, O, ldo_r, ldo_c, alpha, beta, part, blockIdx.z);
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+      __syncwarp();
+      if (lane == 0) t3_arrive(mb_drained);
+      ++drained;
+      return true;
+    };
+    if (ntiles > 0) load_step(0, cur);
+    for (int t = 0; t < ntiles; ++t) {
+      const int q = t % NS;
+      // the slot's previous stage t - NS opens a new chunk: its MMAs wait for the previous chunk's
+      // drain, so drain it before waiting for the slot (before the next loads, to keep registers low)
+      if (t >= NS && (t - NS) % chunk == 0 && (t - NS) / chunk > drained) {
+        if (!__shfl_sync(0xffffffffu, s_abort, 0)) drain_next();
+      }
+      if (t + 1 < ntiles) load_step(t + 1, nxt);
+      if (t >= NS) {
+        int ok = 1;
+        if (lane == 0) ok = tc_wait(mb + 8 * (NS + q), (uint32_t)((t / NS - 1) & 1)) ? 1 : 0;
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) {
+          if (lane == 0) atomicExch(err, 1);
+          s_abort = 1;
+        }
+      }
+      if (__shfl_sync(0xffffffffu, s_abort, 0)) break;  // one read per warp: the warp leaves together
+      unsigned char* slot = tsm3 + q * SL;
+      t3_store_row<CJA, SPLIT>(slot, T3_APL, T3_SLOT, uoff[0], cur);
+      t3_store_row<CJB, SPLIT>(slot + 2 * T3_APL, T3_BPL, T3_SLOT, uoff[1], cur + 4);
+      t3_store_row<CJB, SPLIT>(slot + 2 * T3_APL, T3_BPL, T3_SLOT, uoff[2], cur + 8);
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0) t3_arrive(mb + 8 * q);
+#pragma unroll
+      for (int i = 0; i < 12; ++i) cur[i] = nxt[i];
+    }
+    // the chunks not drained inside the loop, the last one included
+    while (drained < nchunks && !__shfl_sync(0xffffffffu, s_abort, 0)) {
+      if (!drain_next()) break;
+    }
+  } else if (lane == 0) {
+    // ---- MMA issuer ----
+    const uint32_t id_pos = t3_idesc(false), id_neg = t3_idesc(true);
+    int issued = 0;
+    for (int t = 0; t < ntiles; ++t) {
+      const int q = t % NS;
+      const int tc = t % chunk;
+      if (tc == 0 && t > 0) {
+        // the accumulators are reused once the previous chunk is drained
+        if (!tc_wait(mb_drained, (uint32_t)((t / chunk - 1) & 1))) {
+          atomicExch(err, 1);
+          s_abort = 1;
+        }
+      }
+      if (!s_abort && !tc_wait(mb + 8 * q, (uint32_t)((t / NS) & 1))) {
+        atomicExch(err, 1);
+        s_abort = 1;
+      }
+      if (s_abort) break;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      const uint32_t sar = ring + q * SL, sai = sar + T3_APL, sbr = sar + 2 * T3_APL, sbi = sbr + T3_BPL;
+      const uint32_t lo = T3_SLOT;
+      const bool acc = tc > 0;
+      if (SPLIT) {
+        tc_mma(d_re, t3_desc(sar), t3_desc(sbr + lo), id_pos, acc);
+        tc_mma(d_re, t3_desc(sar + lo), t3_desc(sbr), id_pos, true);
+        tc_mma(d_re, t3_desc(sai), t3_desc(sbi + lo), id_neg, true);
+        tc_mma(d_re, t3_desc(sai + lo), t3_desc(sbi), id_neg, true);
+        tc_mma(d_re, t3_desc(sar), t3_desc(sbr), id_pos, true);
+        tc_mma(d_re, t3_desc(sai), t3_desc(sbi), id_neg, true);
+        tc_mma(d_im, t3_desc(sar), t3_desc(sbi + lo), id_pos, acc);
+        tc_mma(d_im, t3_desc(sar + lo), t3_desc(sbi), id_pos, true);
+        tc_mma(d_im, t3_desc(sai), t3_desc(sbr + lo), id_pos, true);
+        tc_mma(d_im, t3_desc(sai + lo), t3_desc(sbr), id_pos, true);
+        tc_mma(d_im, t3_desc(sar), t3_desc(sbi), id_pos, true);
+        tc_mma(d_im, t3_desc(sai), t3_desc(sbr), id_pos, true);
+      } else {
+        tc_mma(d_re, t3_desc(sar), t3_desc(sbr), id_pos, acc);
+        tc_mma(d_re, t3_desc(sai), t3_desc(sbi), id_neg, true);
+        tc_mma(d_im, t3_desc(sar), t3_desc(sbi), id_pos, acc);
+        tc_mma(d_im, t3_desc(sai), t3_desc(sbr), id_pos, true);
+      }
+      tc_commit(mb + 8 * (NS + q));
+      ++issued;
+      // chunk end: the chunk barrier tracks every MMA issued so far
+      if (tc == chunk - 1 || t == ntiles - 1) tc_commit(mb_chunk);
+    }
+    // no MMA may be in flight when the TMEM is freed, also after an abort: one more commit, on a
+    // barrier of its own, tracks them all (bounded wait)
+    if (issued > 0) {
+      tc_commit(mb_fin);
+      if (!tc_wait(mb_fin, 0u)) {
+        atomicExch(err, 1);
+        s_abort = 1;
+      }
+    }
+    s_issued = issued;
+  }
+  __syncwarp();  // the MMA warp's lanes reconverge before the block barrier
+  __syncthreads();
+  bool ok = !s_abort;
+  if (ok && ntiles == 0 && warp < T3_CONV_WARPS) {
+    // an empty K range: the destination still receives its (zero) contribution
+    t3_drain(d_re, d_im, warp, lane, false, true, M, N, r0, c0, O, ldo_r, ldo_c, alpha, beta, part, blockIdx.z);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == T3_CONV_WARPS) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(T3_TMEM_COLS));
+}
+
+// Sum of the column-major split-K partials of k_cgemm_tc3 into the output.
+__global__ void k_cgemm_reduce_cm(int M, int N, int splits, const double2* __restrict__ part, double2* __restrict__ O,
+                                  long ldo_r, long ldo_c, double alpha, double beta) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)M * N) return;
+  const int c = (int)(i / M), r = (int)(i - (long)c * M);
+  double2 s = make_double2(0.0, 0.0);
+  for (int z = 0; z < splits; ++z) {
+    const double2 v = part[(long)z * M * N + i];
+    s.x += v.x;
+    s.y += v.y;
+  }
+  double2* o = O + (long)r * ldo_r + (long)c * ldo_c;
+  double2 v = make_double2(alpha * s.x, alpha * s.y);
+  if (beta != 0.0) {
+    const double2 old = *o;
+    v.x += beta * old.x;
+    v.y += beta * old.y;
+  }
+  *o = v;
+}
+
 __global__ void k_cgemm_reduce(int M, int N, int splits, const double2* __restrict__ part, double2* __restrict__ O,
                                long ldo_r, long ldo_c, double alpha, double beta) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -569,10 +937,92 @@ static int tc_splits(int M, int N, int K) {
   return (int)std::max<long>(1, std::min<long>(maxs, (wave + tiles - 1) / tiles));
 }
 
+// Split-K of the 128 x 256 kernel (one CTA per SM): the fewest splits whose CTAs fill at least 85 %
+// of their waves on 148 SMs and three quarters of one wave, else the best wave fill; at least 512 K
+// per split.
+static int t3_splits(int M, int N, int K) {
+  const long tiles = (long)ceil_div(M, TC_M) * ceil_div(N, T3_N);
+  const long wave = 148;
+  if (tiles >= wave || K < 1024) return 1;
+  const long maxs = std::max<long>(1, std::min<long>(K / 512, 64));
+  long best = 1;
+  double best_eff = 0.0;
+  for (long sp = 1; sp <= maxs; ++sp) {
+    const long ctas = tiles * sp;
+    const double eff = (double)ctas / (double)(((ctas + wave - 1) / wave) * wave);
+    if (eff >= 0.85 && ctas * 4 >= wave * 3) return (int)sp;
+    const double score = eff * std::min(1.0, (double)ctas / wave);
+    if (score > best_eff + 1e-9) {
+      best_eff = score;
+      best = sp;
+    }
+  }
+  return (int)best;
+}
+
+// DFTCUDA_TC=v1 / v2 select the earlier 128 x 64 kernels for every shape (A/B measurements).
+static int tc_variant() {
+  static const int v = [] {
+    const char* e = std::getenv("DFTCUDA_TC");
+    if (e && std::string(e) == "v1") return 1;
+    if (e && std::string(e) == "v2") return 2;
+    return 3;
+  }();
+  return v;
+}
+
+// Accumulation chunk of the wide kernel in K steps (DFTCUDA_TC_CHUNK overrides, for measurements).
+static int t3_chunk() {
+  static const int c = [] {
+    const char* e = std::getenv("DFTCUDA_TC_CHUNK");
+    const int v = e ? std::atoi(e) : 0;
+    return v >= 1 ? v : T3_CHUNK;
+  }();
+  return c;
+}
+
+struct TcPlan {
+  GemmArgs g;      // the problem as run (possibly transposed)
+  bool wide;       // k_cgemm_tc3 (128 x 256 tiles) rather than the 128 x 64 kernels
+  int splits;      // heuristic split-K count before the workspace clamp
+};
+
+// out(r, c) = sum_k A(r, k) B(c, k) is also out^T(c, r) = sum_k B(c, k) A(r, k).  With both output
+// dimensions at 128 or more the wide kernel runs, oriented so consecutive tile rows are consecutive
+// output addresses (coalesced FP64 stores).  Otherwise, with fewer rows than one 128-row MMA tile
+// and more columns, the transpose runs so the wide dimension fills the MMA's M (the
+// back-projection: rows = bands, columns = plane waves).
+static TcPlan tc_plan(const GemmArgs& g0) {
+  auto transposed = [](const GemmArgs& a) {
+    GemmArgs g = a;
+    g.M = a.N; g.N = a.M;
+    g.A = a.B; g.lda = a.ldb; g.a_kc = a.b_kc; g.conj_a = a.conj_b;
+    g.B = a.A; g.ldb = a.lda; g.b_kc = a.a_kc; g.conj_b = a.conj_a;
+    g.ldo_r = a.ldo_c; g.ldo_c = a.ldo_r;
+    return g;
+  };
+  TcPlan p{g0, false, 1};
+  if (tc_variant() == 3 && g0.M >= TC_M && g0.N >= TC_M) {
+    p.wide = true;
+    if (g0.ldo_c == 1 && g0.ldo_r != 1) p.g = transposed(g0);
+    p.splits = t3_splits(p.g.M, p.g.N, p.g.K);
+    return p;
+  }
+  if (g0.M < TC_M && g0.N > g0.M) p.g = transposed(g0);
+  p.splits = tc_splits(p.g.M, p.g.N, p.g.K);
+  return p;
+}
+
 size_t cgemm_tf32_workspace_elems(int M, int N, int K) {
-  if (M < TC_M && N > M) std::swap(M, N);  // the transposed problem cgemm_tf32 runs
-  const int s = tc_splits(M, N, K);
-  return s > 1 ? (size_t)s * M * N : 0;
+  GemmArgs g{};
+  g.M = M; g.N = N; g.K = K; g.ldo_r = 1; g.ldo_c = M;
+  size_t need = 0;
+  for (int o = 0; o < 2; ++o) {  // either output orientation
+    if (o == 1) { g.ldo_r = N; g.ldo_c = 1; }
+    const TcPlan p = tc_plan(g);
+    if (p.splits > 1) need = std::max(need, (size_t)p.splits * M * N);
+  }
+  return need;
 }
 
 template <bool AKC, bool BKC, bool CJA, bool CJB, bool SPLIT>
@@ -603,33 +1053,39 @@ static void tc2_launch(const GemmArgs& g, dim3 grid, int kps, double2* part, int
   count_launch();
 }
 
-// DFTCUDA_TC=v1 selects the first (synchronous-load) kernel for A/B measurements.
-static bool tc_v1() {
-  static const bool v = [] {
-    const char* e = std::getenv("DFTCUDA_TC");
-    return e && std::string(e) == "v1";
-  }();
-  return v;
+template <bool AKC, bool BKC, bool CJA, bool CJB, bool SPLIT>
+static void tc3_launch(const GemmArgs& g, dim3 grid, int kps, double2* part, int* err, cudaStream_t s) {
+  static int attr_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    cudaFuncSetAttribute(k_cgemm_tc3<AKC, BKC, CJA, CJB, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, t3_smem(SPLIT));
+    attr_dev = dev;
+  }
+  k_cgemm_tc3<AKC, BKC, CJA, CJB, SPLIT><<<grid, T3_THREADS, t3_smem(SPLIT), s>>>(
+      g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r, g.ldo_c, g.alpha, g.beta, kps, part, err, t3_chunk());
+  count_launch();
 }
 
 template <bool AKC, bool BKC, bool CJA, bool CJB, bool SPLIT>
-static void tc_any(const GemmArgs& g, dim3 grid, int kps, double2* part, int* err, cudaStream_t s) {
-  if (tc_v1()) tc_launch<AKC, BKC, CJA, CJB, SPLIT>(g, grid, kps, part, err, s);
+static void tc_any(const GemmArgs& g, bool wide, dim3 grid, int kps, double2* part, int* err, cudaStream_t s) {
+  if (wide) tc3_launch<AKC, BKC, CJA, CJB, SPLIT>(g, grid, kps, part, err, s);
+  else if (tc_variant() == 1) tc_launch<AKC, BKC, CJA, CJB, SPLIT>(g, grid, kps, part, err, s);
   else tc2_launch<AKC, BKC, CJA, CJB, SPLIT>(g, grid, kps, part, err, s);
 }
 
 template <bool SPLIT>
-static int tc_dispatch(const GemmArgs& g, dim3 grid, int kps, double2* part, int* err_dev, cudaStream_t s) {
+static int tc_dispatch(const GemmArgs& g, bool wide, dim3 grid, int kps, double2* part, int* err_dev, cudaStream_t s) {
   const int key = (g.a_kc ? 8 : 0) | (g.b_kc ? 4 : 0) | (g.conj_a ? 2 : 0) | (g.conj_b ? 1 : 0);
   switch (key) {
-    case 12: tc_any<true, true, false, false, SPLIT>(g, grid, kps, part, err_dev, s); break;   // projection
-    case 1: tc_any<false, false, false, true, SPLIT>(g, grid, kps, part, err_dev, s); break;   // back-projection
-    case 14: tc_any<true, true, true, false, SPLIT>(g, grid, kps, part, err_dev, s); break;    // Gram V^H W
-    case 4: tc_any<false, true, false, false, SPLIT>(g, grid, kps, part, err_dev, s); break;
-    case 8: tc_any<true, false, false, false, SPLIT>(g, grid, kps, part, err_dev, s); break;   // V C
-    case 0: tc_any<false, false, false, false, SPLIT>(g, grid, kps, part, err_dev, s); break;
-    case 2: tc_any<false, false, true, false, SPLIT>(g, grid, kps, part, err_dev, s); break;    // back-projection, transposed
-    case 13: tc_any<true, true, false, true, SPLIT>(g, grid, kps, part, err_dev, s); break;    // Gram, transposed
+    case 12: tc_any<true, true, false, false, SPLIT>(g, wide, grid, kps, part, err_dev, s); break;   // projection
+    case 1: tc_any<false, false, false, true, SPLIT>(g, wide, grid, kps, part, err_dev, s); break;   // back-projection
+    case 14: tc_any<true, true, true, false, SPLIT>(g, wide, grid, kps, part, err_dev, s); break;    // Gram V^H W
+    case 4: tc_any<false, true, false, false, SPLIT>(g, wide, grid, kps, part, err_dev, s); break;   // V C, transposed
+    case 8: tc_any<true, false, false, false, SPLIT>(g, wide, grid, kps, part, err_dev, s); break;   // V C
+    case 0: tc_any<false, false, false, false, SPLIT>(g, wide, grid, kps, part, err_dev, s); break;
+    case 2: tc_any<false, false, true, false, SPLIT>(g, wide, grid, kps, part, err_dev, s); break;    // back-projection, transposed
+    case 13: tc_any<true, true, false, true, SPLIT>(g, wide, grid, kps, part, err_dev, s); break;    // Gram, transposed
     default: return fail(DFTCUDA_ERR_UNSUPPORTED, "cgemm_tf32: operand layout not instantiated");
   }
   return DFTCUDA_OK;
@@ -637,28 +1093,26 @@ static int tc_dispatch(const GemmArgs& g, dim3 grid, int kps, double2* part, int
 
 int cgemm_tf32(const GemmArgs& g0, cudaStream_t s, double2* ws, size_t ws_elems, int* err_dev, bool split) {
   if (g0.M <= 0 || g0.N <= 0) return DFTCUDA_OK;
-  // out(r, c) = sum_k A(r, k) B(c, k) is also out^T(c, r) = sum_k B(c, k) A(r, k): with fewer rows
-  // than one 128-row MMA tile and more columns, compute the transpose so the wide dimension fills
-  // the MMA's M (the back-projection: rows = bands, columns = plane waves).
-  GemmArgs g = g0;
-  if (g0.M < TC_M && g0.N > g0.M) {
-    g.M = g0.N; g.N = g0.M;
-    g.A = g0.B; g.lda = g0.ldb; g.a_kc = g0.b_kc; g.conj_a = g0.conj_b;
-    g.B = g0.A; g.ldb = g0.lda; g.b_kc = g0.a_kc; g.conj_b = g0.conj_a;
-    g.ldo_r = g0.ldo_c; g.ldo_c = g0.ldo_r;
-  }
-  if (g.K <= 0) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "cgemm_tf32: K must be positive");
-  int splits = g.splits > 0 ? std::min(g.splits, std::max(1, g.K / 32)) : tc_splits(g.M, g.N, g.K);
-  if (splits > 1 && (size_t)splits * g.M * g.N > ws_elems) splits = 1;
+  if (g0.K <= 0) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "cgemm_tf32: K must be positive");
+  const TcPlan p = tc_plan(g0);
+  const GemmArgs& g = p.g;
+  int splits = g.splits > 0 ? std::min(g.splits, std::max(1, g.K / 32)) : p.splits;
+  if (splits > 1) splits = (int)std::max<size_t>(1, std::min<size_t>(splits, ws_elems / ((size_t)g.M * g.N)));  // what fits the workspace
   int kps = (g.K + splits - 1) / splits;
-  kps = ((kps + TC_K - 1) / TC_K) * TC_K;  // a multiple of both kernels' K slice
+  kps = ((kps + TC_K - 1) / TC_K) * TC_K;  // a multiple of every kernel's K slice
   splits = (g.K + kps - 1) / kps;
-  dim3 grid(ceil_div(g.N, TC_N), ceil_div(g.M, TC_M), splits);
+  const dim3 grid(ceil_div(g.N, p.wide ? T3_N : TC_N), ceil_div(g.M, TC_M), splits);
   double2* part = splits > 1 ? ws : nullptr;
-  DFT_TRY(split ? tc_dispatch<true>(g, grid, kps, part, err_dev, s) : tc_dispatch<false>(g, grid, kps, part, err_dev, s));
+  DFT_TRY(split ? tc_dispatch<true>(g, p.wide, grid, kps, part, err_dev, s)
+                : tc_dispatch<false>(g, p.wide, grid, kps, part, err_dev, s));
   if (part) {
     const long tot = (long)g.M * g.N;
-    k_cgemm_reduce<<<ceil_div(tot, 256), 256, 0, s>>>(g.M, g.N, splits, part, g.O, g.ldo_r, g.ldo_c, g.alpha, g.beta); count_launch();
+    if (p.wide) {
+      k_cgemm_reduce_cm<<<ceil_div(tot, 256), 256, 0, s>>>(g.M, g.N, splits, part, g.O, g.ldo_r, g.ldo_c, g.alpha, g.beta);
+    } else {
+      k_cgemm_reduce<<<ceil_div(tot, 256), 256, 0, s>>>(g.M, g.N, splits, part, g.O, g.ldo_r, g.ldo_c, g.alpha, g.beta);
+    }
+    count_launch();
   }
   DFT_CUDA_TRY(cudaGetLastError());
   return DFTCUDA_OK;

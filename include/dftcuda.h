@@ -273,6 +273,61 @@ int dftcuda_fft_plan_create(dftcuda_fft_plan** out, int nx, int ny, int nz);
 int dftcuda_fft_plan_destroy(dftcuda_fft_plan* plan);
 int dftcuda_fft3d(dftcuda_fft_plan* plan, double* data, int direction);
 
+/* ------------------------------------------------------------------------------------------
+ * SCF potential build and mixing on the device (the per-iteration host work around the path).
+ *
+ * A potential context holds the FFT box (nx, ny, nz; x fastest), the cell volume and |G|^2 of every
+ * box point (G = h b1 + k b2 + l b3, recip = the rows b1, b2, b3 in bohr^-1, h, k, l in FFT order
+ * 0, 1, ..., -1), and the Pulay history.  G-space fields are N complex numbers normalised as
+ * f(G) = (1/N) sum_r f(r) e^{-iGr}.  Every pointer may be host or device memory; the calls return
+ * when their results are written.
+ *
+ * dftcuda_hxc_potential: from the density rho(r) (N doubles, electrons/bohr^3), the Hartree + XC
+ * potential in G space (build_potential_grid, scf/potential.zig:144-203: V_H(G) = 8 pi rho(G)/G^2
+ * for G^2 > 1e-12, else 0, plus V_xc(G) of LDA-PZ, xc/xc.zig:195-211, 344-384) into v_out_g (N
+ * complex, interleaved), and the energy terms of that density (scf/energy.zig:372-396):
+ * e_hartree = (vol/2) sum_G 8 pi |rho(G)|^2 / G^2, e_xc = (vol/N) sum_r f_xc(rho(r)), and, when
+ * v_in_g is not NULL, int_vin_rho = (vol/N) sum_r v_in(r) rho(r) for the real-space field of v_in_g.
+ *
+ * dftcuda_potential_real: out_r = vloc_r + v(r) with v(r) = sum_G v_g(G) e^{iGr} (real part);
+ * vloc_r may be NULL.  The local potential handed to dftcuda_set_vloc.
+ *
+ * dftcuda_pulay_mix: Pulay / DIIS step of PulayMixer.mix_with_residual (scf/mixing.zig:182-248) on
+ * n doubles: x (in: current input, out: mixed) and residual; the context keeps the last `history`
+ * (x, residual) pairs on the device; with fewer than two it returns x + beta * residual, else
+ * sum_i c_i (x_i + beta r_i) with c from the bordered system B_ij = <r_i|r_j>, sum c = 1.
+ * dftcuda_pulay_reset clears the history.  These have no reference counterpart as device calls.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct dftcuda_pctx dftcuda_pctx;
+typedef struct dftcuda_hxc_terms {
+  double e_hartree;
+  double e_xc;
+  double int_vin_rho;
+} dftcuda_hxc_terms;
+int dftcuda_pctx_create(dftcuda_pctx** out, int nx, int ny, int nz, double volume, const double* recip,
+                        int pulay_history);
+int dftcuda_pctx_destroy(dftcuda_pctx* ctx);
+int dftcuda_hxc_potential(dftcuda_pctx* ctx, const double* rho_r, const double* v_in_g, double* v_out_g,
+                          dftcuda_hxc_terms* terms);
+int dftcuda_potential_real(dftcuda_pctx* ctx, const double* v_g, const double* vloc_r, double* out_r);
+int dftcuda_pulay_mix(dftcuda_pctx* ctx, double* x, const double* residual, size_t n, double beta);
+int dftcuda_pulay_reset(dftcuda_pctx* ctx);
+
+/* ------------------------------------------------------------------------------------------
+ * The library's complex GEMM (no counterpart in the reference; the contraction its projector and
+ * Rayleigh-Ritz code paths run), exposed for tests and benchmarks:
+ *   out(r, c) = alpha * sum_k opA(A(r, k)) * opB(B(c, k)) + beta * out(r, c),   r < M, c < N, k < K
+ * A(r, k) is A[r*lda + k] when a_kc != 0 (K contiguous), else A[k*lda + r]; the same for B; opX
+ * conjugates when conj_x != 0.  out(r, c) is out[r*ldo_r + c*ldo_c].  All pointers are device
+ * pointers to interleaved complex128.  precision: DFTCUDA_PRECISION_FP64 (FP64 FMA kernel),
+ * DFTCUDA_PRECISION_TF32 or DFTCUDA_PRECISION_TF32X3 (tcgen05 tensor-core kernels); FP32 is not
+ * accepted.  The call allocates its split-K workspace, runs on a private stream and returns after
+ * the product is complete.
+ * ------------------------------------------------------------------------------------------ */
+int dftcuda_complex_gemm(int precision, size_t M, size_t N, size_t K, const double* a, long lda, int a_kc, int conj_a,
+                         const double* b, long ldb, int b_kc, int conj_b, double* out, long ldo_r, long ldo_c, double alpha,
+                         double beta);
+
 #ifdef __cplusplus
 }
 #endif
