@@ -3,7 +3,7 @@
 #include <cmath>
 #include <vector>
 
-#include "fft_core.cuh"
+#include "kctx.cuh"
 
 namespace dftcuda {
 
@@ -199,15 +199,15 @@ struct dftcuda_fft_plan {
 };
 
 static int run_axis(dftcuda_fft_plan* pl, double2* d, const Fft1d& p, int es, int ninner, int nouter, long os, int dir,
-                    double scale) {
+                    double scale, cudaStream_t stream) {
   const int lines = ninner >= 16 ? 16 : ninner;
   dim3 block(16, lines);
   dim3 grid(ceil_div(ninner, lines), nouter);
   const size_t smem = (size_t)p.n * lines * sizeof(double2);
   if (dir > 0)
-    k_fft_axis<true><<<grid, block, smem, pl->stream>>>(d, p, es, ninner, nouter, os, +1.0, scale);
+    k_fft_axis<true><<<grid, block, smem, stream>>>(d, p, es, ninner, nouter, os, +1.0, scale);
   else
-    k_fft_axis<false><<<grid, block, smem, pl->stream>>>(d, p, es, ninner, nouter, os, -1.0, scale);
+    k_fft_axis<false><<<grid, block, smem, stream>>>(d, p, es, ninner, nouter, os, -1.0, scale);
   count_launch();
   DFT_CUDA_TRY(cudaGetLastError());
   return DFTCUDA_OK;
@@ -241,6 +241,17 @@ extern "C" int dftcuda_fft_plan_destroy(dftcuda_fft_plan* pl) {
   return DFTCUDA_OK;
 }
 
+// The three axis passes on device data, queued on stream s (no synchronisation): z, then y (each
+// over x-contiguous lines), then x; the inverse carries the 1/N.
+int dftcuda::fft3d_on_stream(dftcuda_fft_plan* pl, double2* d, int direction, cudaStream_t s) {
+  const long nx = pl->nx, ny = pl->ny, nz = pl->nz, N = nx * ny * nz;
+  const double inv = direction > 0 ? 1.0 / (double)N : 1.0;
+  DFT_TRY(run_axis(pl, d, pl->pz.dev, (int)(nx * ny), (int)nx, (int)ny, nx, direction, 1.0, s));
+  DFT_TRY(run_axis(pl, d, pl->py.dev, (int)nx, (int)nx, (int)nz, nx * ny, direction, 1.0, s));
+  DFT_TRY(run_axis(pl, d, pl->px.dev, 1, 1, (int)(ny * nz), nx, direction, inv, s));
+  return DFTCUDA_OK;
+}
+
 extern "C" int dftcuda_fft3d(dftcuda_fft_plan* pl, double* data, int direction) {
   if (!pl || !data || (direction != 1 && direction != -1)) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "fft3d: bad arguments");
   const long nx = pl->nx, ny = pl->ny, nz = pl->nz, N = nx * ny * nz;
@@ -251,17 +262,7 @@ extern "C" int dftcuda_fft3d(dftcuda_fft_plan* pl, double* data, int direction) 
     d = pl->staging;
     DFT_CUDA_TRY(cudaMemcpyAsync(d, data, N * sizeof(double2), cudaMemcpyHostToDevice, pl->stream));
   }
-  const double inv = direction > 0 ? 1.0 / (double)N : 1.0;
-  // x pencils: element stride 1; lines = y (inner, stride nx ... ) -> treat each (y,z) line with es=1:
-  // use ninner = 1 consecutive? Instead transform x as pencils with es=1, inner over y*z lines of stride nx.
-  // Axis z: es = nx*ny, inner = x (nx consecutive), outer = y (stride nx).
-  DFT_TRY(run_axis(pl, d, pl->pz.dev, (int)(nx * ny), (int)nx, (int)ny, nx, direction, 1.0));
-  // Axis y: es = nx, inner = x, outer = z (stride nx*ny).
-  DFT_TRY(run_axis(pl, d, pl->py.dev, (int)nx, (int)nx, (int)nz, nx * ny, direction, 1.0));
-  // Axis x: es = 1 would make lines strided; transform x via a tile whose "inner" lines are
-  // consecutive (y,z) rows: view as es=1 pencils with inner stride nx -> handled by k_fft_axis with
-  // es = 1 and one line per CTA row block.  Simplest correct mapping: inner = 1 line, outer = ny*nz.
-  DFT_TRY(run_axis(pl, d, pl->px.dev, 1, 1, (int)(ny * nz), nx, direction, inv));
+  DFT_TRY(dftcuda::fft3d_on_stream(pl, d, direction, pl->stream));
   if (!dev) DFT_CUDA_TRY(cudaMemcpyAsync(data, d, N * sizeof(double2), cudaMemcpyDeviceToHost, pl->stream));
   DFT_CUDA_TRY(cudaStreamSynchronize(pl->stream));
   return DFTCUDA_OK;

@@ -158,6 +158,8 @@ struct HeevWork {
   size_t wy_ws_elems = 0;   // the split-K part of wy (complex elements)
   size_t m_cap = 0, nev_cap = 0;
 };
+// 3D FFT of device data on stream s (fft_plan.cu): direction -1 forward unnormalised, +1 inverse / N.
+int fft3d_on_stream(dftcuda_fft_plan* pl, double2* d, int direction, cudaStream_t s);
 size_t heev_work_bytes(int m, int nev);
 void heev_bind(HeevWork& w, void* base, int m, int nev);
 int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde, const HeevWork& w, int* status,

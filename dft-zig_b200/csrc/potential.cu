@@ -1,0 +1,453 @@
+// SCF potential build and Pulay mixing on the device: the per-iteration work around the eigensolver
+// and density path (scf/scf.zig:148-188), kept next to the data so the density, the potential and
+// the mixing history never leave HBM between iterations.
+//
+//   dftcuda_hxc_potential   build_potential_grid (scf/potential.zig:144-203): FFT of rho, Hartree
+//                           8 pi rho(G)/G^2 (hartree_potential_at_g, potential.zig:34-44), LDA-PZ
+//                           f and V_xc (xc/xc.zig:195-211, 344-384) and the FFT of V_xc; energy
+//                           terms of scf/energy.zig:372-396 from the same passes
+//   dftcuda_potential_real  V(r) = V_loc(r) + FFT^-1 V(G) (build_local_potential_real,
+//                           potential.zig:320-334)
+//   dftcuda_pulay_mix       PulayMixer.mix_with_residual (scf/mixing.zig:182-248) with the bordered
+//                           system solved as solve_pulay_system (mixing.zig:341-405)
+//
+// Bounds: every kernel here streams N-point fields once or twice (HBM bound); the FFTs are the
+// library's axis passes.  Sums are taken as fixed per-block partials added on the host in block
+// order, so results do not depend on scheduling.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "kctx.cuh"
+
+namespace dftcuda {
+namespace {
+
+constexpr int kPotThreads = 256;
+constexpr int kPotBlocks = 592;  // 4 per SM on 148 SMs; per-block partial sums
+constexpr double kPi = 3.14159265358979323846;
+
+__global__ void k_pot_g2(int nx, int ny, int nz, double b00, double b01, double b02, double b10, double b11, double b12,
+                         double b20, double b21, double b22, double* __restrict__ g2) {
+  const long N = (long)nx * ny * nz;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long)nx * ny));
+    const double h = x < (nx + 1) / 2 ? x : x - nx;
+    const double k = y < (ny + 1) / 2 ? y : y - ny;
+    const double l = z < (nz + 1) / 2 ? z : z - nz;
+    const double gx = h * b00 + k * b10 + l * b20;
+    const double gy = h * b01 + k * b11 + l * b21;
+    const double gz = h * b02 + k * b12 + l * b22;
+    g2[i] = gx * gx + gy * gy + gz * gz;
+  }
+}
+
+// LDA-PZ in Ry: f (energy per volume) and v = df/dn; zero for n <= 1e-12 (xc.zig:195-211, 344-384).
+__device__ __forceinline__ void lda_pz(double n, double& f, double& v) {
+  if (n <= 1e-12) {
+    f = 0.0;
+    v = 0.0;
+    return;
+  }
+  const double n13 = pow(n, 1.0 / 3.0);
+  const double c_x = -0.75 * pow(3.0 / kPi, 1.0 / 3.0);
+  const double ex = n * c_x * n13;
+  const double rs = pow(3.0 / (4.0 * kPi * n), 1.0 / 3.0);
+  double eps_c, v_c;
+  if (rs < 1.0) {
+    const double a = 0.0311, b = -0.048, c = 0.0020, d = -0.0116;
+    const double lr = log(rs);
+    eps_c = a * lr + b + c * rs * lr + d * rs;
+    const double de = a / rs + c * lr + c + d;
+    v_c = eps_c - (rs / 3.0) * de;
+  } else {
+    const double g = -0.1423, b1 = 1.0529, b2 = 0.3334;
+    const double sr = sqrt(rs);
+    const double den = 1.0 + b1 * sr + b2 * rs;
+    eps_c = g / den;
+    const double de = -g * (0.5 * b1 / sr + b2) / (den * den);
+    v_c = eps_c - (rs / 3.0) * de;
+  }
+  f = 2.0 * (ex + n * eps_c);
+  v = 2.0 * (4.0 / 3.0 * c_x * n13 + v_c);
+}
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < kPotThreads / 32; ++i) t += red[i];
+  return t;
+}
+
+// a = rho (complex), b = V_xc (complex); part[block] = sum of f_xc over the block's points.
+__global__ void __launch_bounds__(kPotThreads) k_pot_xc(const double* __restrict__ rho, long N, double2* __restrict__ a,
+                                                        double2* __restrict__ b, double* __restrict__ part) {
+  __shared__ double red[kPotThreads / 32];
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const double n = rho[i];
+    double f, v;
+    lda_pz(n, f, v);
+    a[i] = make_double2(n, 0.0);
+    b[i] = make_double2(v, 0.0);
+    s += f;
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// a = N rho(G), b = N V_xc(G) (unnormalised forward FFTs).  out = V_H + V_xc (normalised);
+// part[0][block] = sum 8 pi |rho(G)|^2 / G^2, part[1][block] = sum Re(v_in(G) conj(rho(G))).
+__global__ void __launch_bounds__(kPotThreads) k_pot_hartree(const double2* __restrict__ a, const double2* __restrict__ b,
+                                                             const double* __restrict__ g2, long N,
+                                                             const double2* __restrict__ v_in, double2* __restrict__ out,
+                                                             double* __restrict__ part) {
+  __shared__ double red[kPotThreads / 32];
+  const double inv = 1.0 / (double)N;
+  double eh = 0.0, ei = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const double2 rg = make_double2(a[i].x * inv, a[i].y * inv);
+    const double q = g2[i];
+    double2 v = make_double2(b[i].x * inv, b[i].y * inv);
+    if (q > 1e-12) {
+      const double k = 8.0 * kPi / q;
+      v.x += k * rg.x;
+      v.y += k * rg.y;
+      eh += k * (rg.x * rg.x + rg.y * rg.y);
+    }
+    out[i] = v;
+    if (v_in) {
+      const double2 w = v_in[i];
+      ei += w.x * rg.x + w.y * rg.y;
+    }
+  }
+  eh = block_sum(eh, red);
+  ei = block_sum(ei, red);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = eh;
+    part[kPotBlocks + blockIdx.x] = ei;
+  }
+}
+
+// out_r = vloc + Re(v) * N (v holds FFT^-1 / N of the G-space field).
+__global__ void k_pot_real(const double2* __restrict__ v, const double* __restrict__ vloc, long N, double* __restrict__ out) {
+  const double scale = (double)N;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+    out[i] = (vloc ? vloc[i] : 0.0) + v[i].x * scale;
+}
+
+// part[j][block] = <r_new, hist_r[j]> over the block's share, j < m.
+__global__ void __launch_bounds__(kPotThreads) k_pulay_dots(const double* __restrict__ rn, const double* __restrict__ hist,
+                                                            const int* __restrict__ slots, int m, long n,
+                                                            double* __restrict__ part) {
+  __shared__ double red[kPotThreads / 32];
+  for (int j = 0; j < m; ++j) {
+    const double* h = hist + (long)slots[j] * n;
+    double s = 0.0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) s += rn[i] * h[i];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) part[(long)j * kPotBlocks + blockIdx.x] = s;
+  }
+}
+
+// x = sum_j c_j (x_j + beta r_j) over the history slots.
+__global__ void k_pulay_combine(const double* __restrict__ hx, const double* __restrict__ hr, const int* __restrict__ slots,
+                                const double* __restrict__ c, int m, long n, double beta, double* __restrict__ x) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int j = 0; j < m; ++j) {
+      const long o = (long)slots[j] * n + i;
+      s += c[j] * (hx[o] + beta * hr[o]);
+    }
+    x[i] = s;
+  }
+}
+
+__global__ void k_axpy_into(const double* __restrict__ x, const double* __restrict__ r, long n, double beta,
+                            double* __restrict__ out) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) out[i] = x[i] + beta * r[i];
+}
+
+// solve_pulay_system (mixing.zig:341-405): Gaussian elimination with partial pivoting on the
+// bordered (m+1) x (m+1) system; a pivot below 1e-12 gives equal weights.  The overlap block is
+// first divided by its largest diagonal entry: the weights are unchanged, and the pivot test acts
+// relative to the residual size (with the reference's absolute test the mixing falls back to equal
+// weights, and stalls, once residual overlaps drop below 1e-12).
+std::vector<double> solve_pulay(std::vector<double> A, std::vector<double> b, int size) {
+  {
+    const int m = size - 1;
+    double d = 0.0;
+    for (int i = 0; i < m; ++i) d = std::max(d, A[i * size + i]);
+    if (d > 0.0)
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) A[i * size + j] /= d;
+  }
+  for (int col = 0; col < size; ++col) {
+    int max_row = col;
+    double max_val = std::fabs(A[col * size + col]);
+    for (int row = col + 1; row < size; ++row) {
+      const double v = std::fabs(A[row * size + col]);
+      if (v > max_val) {
+        max_val = v;
+        max_row = row;
+      }
+    }
+    if (max_row != col) {
+      for (int j = 0; j < size; ++j) std::swap(A[col * size + j], A[max_row * size + j]);
+      std::swap(b[col], b[max_row]);
+    }
+    const double pivot = A[col * size + col];
+    if (std::fabs(pivot) < 1e-12) {
+      std::vector<double> r(size, 1.0 / (double)(size - 1));
+      r[size - 1] = 0.0;
+      return r;
+    }
+    for (int row = col + 1; row < size; ++row) {
+      const double factor = A[row * size + col] / pivot;
+      for (int j = col; j < size; ++j) A[row * size + j] -= factor * A[col * size + j];
+      b[row] -= factor * b[col];
+    }
+  }
+  std::vector<double> r(size);
+  for (int i = size - 1; i >= 0; --i) {
+    double s = b[i];
+    for (int j = i + 1; j < size; ++j) s -= A[i * size + j] * r[j];
+    r[i] = s / A[i * size + i];
+  }
+  return r;
+}
+
+}  // namespace
+}  // namespace dftcuda
+
+using namespace dftcuda;
+
+struct dftcuda_pctx {
+  int nx = 0, ny = 0, nz = 0;
+  long N = 0;
+  double volume = 0.0;
+  int history = 0;
+  dftcuda_fft_plan* plan = nullptr;
+  cudaStream_t stream = nullptr;
+  double* g2 = nullptr;       // N
+  double2* a = nullptr;       // N complex scratch
+  double2* b = nullptr;       // N complex scratch
+  double* rho = nullptr;      // N staging for host densities
+  double2* vin = nullptr;     // N complex staging for host inputs
+  double2* vout = nullptr;    // N complex staging for host outputs
+  double* part = nullptr;     // kPotBlocks x max(2, history) partial sums
+  double* h_part = nullptr;   // pinned host copy
+  // Pulay history: `history` slots of n doubles each for inputs and residuals, plus staging
+  long pn = 0;                // vector length the history holds (0 until the first mix)
+  double* hx = nullptr;
+  double* hr = nullptr;
+  double* px = nullptr;       // n staging (x in / out)
+  double* pr = nullptr;       // n staging (residual)
+  int* d_slots = nullptr;
+  double* d_coef = nullptr;
+  std::vector<int> order;     // slots oldest first
+  std::vector<double> B;      // history x history residual overlaps, by slot
+};
+
+static int pctx_fail_free(dftcuda_pctx* c, int status) {
+  dftcuda_pctx_destroy(c);
+  return status;
+}
+
+extern "C" int dftcuda_pctx_create(dftcuda_pctx** out, int nx, int ny, int nz, double volume, const double* recip,
+                                   int pulay_history) {
+  if (!out || nx <= 0 || ny <= 0 || nz <= 0 || !(volume > 0.0) || !recip || pulay_history < 0 || pulay_history > 64)
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "pctx_create: bad arguments (history must be 0..64)");
+  *out = nullptr;
+  auto* c = new dftcuda_pctx();
+  c->nx = nx; c->ny = ny; c->nz = nz;
+  c->N = (long)nx * ny * nz;
+  c->volume = volume;
+  c->history = pulay_history;
+  int st = dftcuda_fft_plan_create(&c->plan, nx, ny, nz);
+  if (st != DFTCUDA_OK) return pctx_fail_free(c, st);
+  const long N = c->N;
+  const int nparts = std::max(2, pulay_history);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&c->g2, sizeof(double) * N) != cudaSuccess || cudaMalloc(&c->a, sizeof(double2) * N) != cudaSuccess ||
+      cudaMalloc(&c->b, sizeof(double2) * N) != cudaSuccess || cudaMalloc(&c->rho, sizeof(double) * N) != cudaSuccess ||
+      cudaMalloc(&c->vin, sizeof(double2) * N) != cudaSuccess || cudaMalloc(&c->vout, sizeof(double2) * N) != cudaSuccess ||
+      cudaMalloc(&c->part, sizeof(double) * kPotBlocks * nparts) != cudaSuccess ||
+      cudaMallocHost(&c->h_part, sizeof(double) * kPotBlocks * nparts) != cudaSuccess ||
+      cudaMalloc(&c->d_slots, sizeof(int) * 64) != cudaSuccess || cudaMalloc(&c->d_coef, sizeof(double) * 65) != cudaSuccess)
+    return pctx_fail_free(c, fail(DFTCUDA_ERR_CUDA, "pctx_create: device allocation failed"));
+  const double* r = recip;
+  k_pot_g2<<<kPotBlocks, kPotThreads, 0, c->stream>>>(nx, ny, nz, r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8], c->g2);
+  count_launch();
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return pctx_fail_free(c, fail(DFTCUDA_ERR_CUDA, "pctx_create: G^2"));
+  *out = c;
+  return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_pctx_destroy(dftcuda_pctx* c) {
+  if (!c) return DFTCUDA_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (void* p : {(void*)c->g2, (void*)c->a, (void*)c->b, (void*)c->rho, (void*)c->vin, (void*)c->vout, (void*)c->part, (void*)c->hx,
+                  (void*)c->hr, (void*)c->px, (void*)c->pr, (void*)c->d_slots, (void*)c->d_coef})
+    if (p) cudaFree(p);
+  if (c->h_part) cudaFreeHost(c->h_part);
+  if (c->plan) dftcuda_fft_plan_destroy(c->plan);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return DFTCUDA_OK;
+}
+
+// A device view of n bytes of `src` (host or device): device pointers pass through, host data is
+// copied into `staging`.
+static const void* device_view(const void* src, void* staging, size_t bytes, cudaStream_t s, int* st) {
+  if (is_device_pointer(src)) return src;
+  if (cudaMemcpyAsync(staging, src, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    *st = fail(DFTCUDA_ERR_CUDA, "potential: host-to-device copy failed");
+  return staging;
+}
+
+static int copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  DFT_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, is_device_pointer(dst) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+  return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_hxc_potential(dftcuda_pctx* c, const double* rho_r, const double* v_in_g, double* v_out_g,
+                                     dftcuda_hxc_terms* terms) {
+  if (!c || !rho_r || !v_out_g) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "hxc_potential: null argument");
+  const long N = c->N;
+  cudaStream_t s = c->stream;
+  int st = DFTCUDA_OK;
+  const double* rho = (const double*)device_view(rho_r, c->rho, sizeof(double) * N, s, &st);
+  const double2* vin = v_in_g ? (const double2*)device_view(v_in_g, c->vin, sizeof(double2) * N, s, &st) : nullptr;
+  if (st != DFTCUDA_OK) return st;
+  k_pot_xc<<<kPotBlocks, kPotThreads, 0, s>>>(rho, N, c->a, c->b, c->part);
+  count_launch();
+  DFT_CUDA_TRY(cudaMemcpyAsync(c->h_part, c->part, sizeof(double) * kPotBlocks, cudaMemcpyDeviceToHost, s));
+  DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  double exc = 0.0;
+  for (int i = 0; i < kPotBlocks; ++i) exc += c->h_part[i];
+  DFT_TRY(fft3d_on_stream(c->plan, c->a, -1, s));
+  DFT_TRY(fft3d_on_stream(c->plan, c->b, -1, s));
+  double2* out = is_device_pointer(v_out_g) ? (double2*)v_out_g : c->vout;
+  k_pot_hartree<<<kPotBlocks, kPotThreads, 0, s>>>(c->a, c->b, c->g2, N, vin, out, c->part);
+  count_launch();
+  if (out != (double2*)v_out_g) DFT_TRY(copy_out(v_out_g, out, sizeof(double2) * N, s));
+  DFT_CUDA_TRY(cudaMemcpyAsync(c->h_part, c->part, sizeof(double) * 2 * kPotBlocks, cudaMemcpyDeviceToHost, s));
+  DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  double eh = 0.0, ei = 0.0;
+  for (int i = 0; i < kPotBlocks; ++i) {
+    eh += c->h_part[i];
+    ei += c->h_part[kPotBlocks + i];
+  }
+  if (terms) {
+    terms->e_hartree = 0.5 * c->volume * eh;
+    terms->e_xc = exc * c->volume / (double)N;
+    terms->int_vin_rho = v_in_g ? c->volume * ei : 0.0;
+  }
+  return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_potential_real(dftcuda_pctx* c, const double* v_g, const double* vloc_r, double* out_r) {
+  if (!c || !v_g || !out_r) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "potential_real: null argument");
+  const long N = c->N;
+  cudaStream_t s = c->stream;
+  DFT_CUDA_TRY(cudaMemcpyAsync(c->a, v_g, sizeof(double2) * N,
+                               is_device_pointer(v_g) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  int st = DFTCUDA_OK;
+  const double* vloc = vloc_r ? (const double*)device_view(vloc_r, c->rho, sizeof(double) * N, s, &st) : nullptr;
+  if (st != DFTCUDA_OK) return st;
+  DFT_TRY(fft3d_on_stream(c->plan, c->a, +1, s));
+  double* out = is_device_pointer(out_r) ? out_r : reinterpret_cast<double*>(c->b);
+  k_pot_real<<<kPotBlocks, kPotThreads, 0, s>>>(c->a, vloc, N, out);
+  count_launch();
+  if (out != out_r) DFT_TRY(copy_out(out_r, out, sizeof(double) * N, s));
+  DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_pulay_reset(dftcuda_pctx* c) {
+  if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "pulay_reset: null context");
+  c->order.clear();
+  return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_pulay_mix(dftcuda_pctx* c, double* x, const double* residual, size_t n, double beta) {
+  if (!c || !x || !residual || n == 0) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "pulay_mix: bad arguments");
+  if (c->history < 1) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "pulay_mix: the context was created without history");
+  cudaStream_t s = c->stream;
+  const int H = c->history;
+  if (c->pn != (long)n) {
+    // (re)size the history for this vector length
+    for (double** p : {&c->hx, &c->hr, &c->px, &c->pr})
+      if (*p) {
+        cudaFree(*p);
+        *p = nullptr;
+      }
+    if (cudaMalloc(&c->hx, sizeof(double) * n * H) != cudaSuccess || cudaMalloc(&c->hr, sizeof(double) * n * H) != cudaSuccess ||
+        cudaMalloc(&c->px, sizeof(double) * n) != cudaSuccess || cudaMalloc(&c->pr, sizeof(double) * n) != cudaSuccess) {
+      c->pn = 0;
+      return fail(DFTCUDA_ERR_CUDA, "pulay_mix: history allocation failed");
+    }
+    c->pn = (long)n;
+    c->order.clear();
+    c->B.assign((size_t)H * H, 0.0);
+  }
+  // the new pair goes into the oldest slot once the history is full (mix_with_residual appends,
+  // then drops the oldest beyond `history`)
+  int slot;
+  if ((int)c->order.size() < H) {
+    std::vector<bool> used(H, false);
+    for (int o : c->order) used[o] = true;
+    slot = 0;
+    while (used[slot]) ++slot;
+  } else {
+    slot = c->order.front();
+    c->order.erase(c->order.begin());
+  }
+  c->order.push_back(slot);
+  DFT_CUDA_TRY(cudaMemcpyAsync(c->hx + (long)slot * n, x, sizeof(double) * n,
+                               is_device_pointer(x) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  DFT_CUDA_TRY(cudaMemcpyAsync(c->hr + (long)slot * n, residual, sizeof(double) * n,
+                               is_device_pointer(residual) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  double* xo = is_device_pointer(x) ? x : c->px;
+  const int m = (int)c->order.size();
+  if (m < 2) {
+    k_axpy_into<<<kPotBlocks, kPotThreads, 0, s>>>(c->hx + (long)slot * n, c->hr + (long)slot * n, (long)n, beta, xo);
+    count_launch();
+  } else {
+    // overlaps of the new residual with every residual held (itself included)
+    DFT_CUDA_TRY(cudaMemcpyAsync(c->d_slots, c->order.data(), sizeof(int) * m, cudaMemcpyHostToDevice, s));
+    k_pulay_dots<<<kPotBlocks, kPotThreads, 0, s>>>(c->hr + (long)slot * n, c->hr, c->d_slots, m, (long)n, c->part);
+    count_launch();
+    DFT_CUDA_TRY(cudaMemcpyAsync(c->h_part, c->part, sizeof(double) * kPotBlocks * m, cudaMemcpyDeviceToHost, s));
+    DFT_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int j = 0; j < m; ++j) {
+      double d = 0.0;
+      for (int i = 0; i < kPotBlocks; ++i) d += c->h_part[(long)j * kPotBlocks + i];
+      c->B[(size_t)slot * H + c->order[j]] = d;
+      c->B[(size_t)c->order[j] * H + slot] = d;
+    }
+    const int sz = m + 1;
+    std::vector<double> A((size_t)sz * sz, 0.0), rhs(sz, 0.0);
+    for (int i = 0; i < m; ++i) {
+      for (int j = 0; j < m; ++j) A[(size_t)i * sz + j] = c->B[(size_t)c->order[i] * H + c->order[j]];
+      A[(size_t)i * sz + m] = -1.0;
+      A[(size_t)m * sz + i] = -1.0;
+    }
+    rhs[m] = -1.0;
+    const std::vector<double> coef = solve_pulay(A, rhs, sz);
+    DFT_CUDA_TRY(cudaMemcpyAsync(c->d_coef, coef.data(), sizeof(double) * m, cudaMemcpyHostToDevice, s));
+    k_pulay_combine<<<kPotBlocks, kPotThreads, 0, s>>>(c->hx, c->hr, c->d_slots, c->d_coef, m, (long)n, beta, xo);
+    count_launch();
+  }
+  if (xo != x) DFT_CUDA_TRY(cudaMemcpyAsync(x, xo, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}

@@ -120,9 +120,41 @@ def gth_alpha(sp: sysm.SpeciesData) -> float:
 # ---------------------------------------------------------------------------------------------
 
 
+def _solve_pulay_system(B, rhs):
+    """mixing.zig:341-405: Gaussian elimination with partial pivoting of the bordered system, the
+    overlap block first divided by its largest diagonal entry (the weights do not change).  Returns
+    None for a pivot below 1e-12 (the reference averages the history then; the mixer drops its
+    oldest pair and solves again instead, which keeps DIIS working once more pairs are held than
+    the residuals have independent directions)."""
+    A = np.array(B, dtype=np.float64)
+    m = A.shape[0] - 1
+    d = float(np.max(np.diag(A)[:m]))
+    if d > 0.0:
+        A[:m, :m] /= d
+    b = np.array(rhs, dtype=np.float64)
+    size = b.size
+    for col in range(size):
+        max_row = col + int(np.argmax(np.abs(A[col:, col])))
+        if max_row != col:
+            A[[col, max_row]] = A[[max_row, col]]
+            b[[col, max_row]] = b[[max_row, col]]
+        pivot = A[col, col]
+        if abs(pivot) < 1e-12:
+            return None
+        for row in range(col + 1, size):
+            f = A[row, col] / pivot
+            A[row, col:] -= f * A[col, col:]
+            b[row] -= f * b[col]
+    r = np.zeros(size)
+    for i in range(size - 1, -1, -1):
+        r[i] = (b[i] - np.dot(A[i, i + 1:], r[i + 1:])) / A[i, i]
+    return r
+
+
 class PulayMixer:
     """mixing.zig:182-248 (mix_with_residual): history of inputs and residuals, DIIS coefficients
-    from B_ij = <R_i|R_j> with the constraint sum c = 1, new = sum c_i (x_i + beta R_i)."""
+    from B_ij = <R_i|R_j> with the constraint sum c = 1, new = sum c_i (x_i + beta R_i); a singular
+    system drops the oldest pairs (see _solve_pulay_system)."""
 
     def __init__(self, history: int):
         self.history = history
@@ -136,23 +168,27 @@ class PulayMixer:
             self.xs.pop(0)
             self.rs.pop(0)
         m = len(self.xs)
-        if m < 2:
+        first = 0  # oldest pair used
+        c = None
+        while m - first >= 2:
+            k = m - first
+            B = np.zeros((k + 1, k + 1))
+            for i in range(k):
+                for j in range(k):
+                    B[i, j] = float(np.dot(self.rs[first + i], self.rs[first + j]))
+            B[:k, k] = -1.0
+            B[k, :k] = -1.0
+            rhs = np.zeros(k + 1)
+            rhs[k] = -1.0
+            c = _solve_pulay_system(B, rhs)
+            if c is not None:
+                break
+            first += 1
+        if c is None:
             return x + beta * residual
-        B = np.zeros((m + 1, m + 1))
-        for i in range(m):
-            for j in range(m):
-                B[i, j] = float(np.dot(self.rs[i], self.rs[j]))
-        B[:m, m] = -1.0
-        B[m, :m] = -1.0
-        rhs = np.zeros(m + 1)
-        rhs[m] = -1.0
-        try:
-            c = np.linalg.solve(B, rhs)
-        except np.linalg.LinAlgError:
-            c = np.linalg.lstsq(B, rhs, rcond=None)[0]
         out = np.zeros_like(x)
-        for i in range(m):
-            out += c[i] * (self.xs[i] + beta * self.rs[i])
+        for i in range(m - first):
+            out += c[i] * (self.xs[first + i] + beta * self.rs[first + i])
         return out
 
 

@@ -1,0 +1,173 @@
+"""Test infrastructure: the CPU restatement of the SCF potential build and Pulay mixing that the
+device module (dft-zig_b200/csrc/potential.cu) is checked against.  Only tests, the smoke check and
+the benchmark's CPU-baseline leg use it.
+
+Fields live on the FFT box with x fastest; G-space fields are f(G) = (1/N) sum_r f(r) e^{-iGr}
+(numpy fftn of the (z, y, x) array divided by N)."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+def lda_pz(n):
+    """xc/xc.zig:195-211 (lda_pz), 344-384 (PZ correlation energy and potential): f per volume and
+    v = df/dn in Ry; both zero for n <= 1e-12."""
+    n = np.asarray(n, dtype=np.float64)
+    f = np.zeros_like(n)
+    v = np.zeros_like(n)
+    m = n > 1e-12
+    nn = n[m]
+    n13 = np.power(nn, 1.0 / 3.0)
+    c_x = -0.75 * math.pow(3.0 / math.pi, 1.0 / 3.0)
+    rs = np.power(3.0 / (4.0 * math.pi * nn), 1.0 / 3.0)
+    eps_c = np.empty_like(nn)
+    v_c = np.empty_like(nn)
+    lo = rs < 1.0
+    a, b, c, d = 0.0311, -0.048, 0.0020, -0.0116
+    r = rs[lo]
+    lr = np.log(r)
+    e = a * lr + b + c * r * lr + d * r
+    eps_c[lo] = e
+    v_c[lo] = e - (r / 3.0) * (a / r + c * lr + c + d)
+    g, b1, b2 = -0.1423, 1.0529, 0.3334
+    r = rs[~lo]
+    sr = np.sqrt(r)
+    den = 1.0 + b1 * sr + b2 * r
+    e = g / den
+    eps_c[~lo] = e
+    v_c[~lo] = e - (r / 3.0) * (-g * (0.5 * b1 / sr + b2) / (den * den))
+    f[m] = 2.0 * (nn * c_x * n13 + nn * eps_c)
+    v[m] = 2.0 * (4.0 / 3.0 * c_x * n13 + v_c)
+    return f, v
+
+
+def g2_table(dims, recip):
+    """|G|^2 of every box point, G = h b1 + k b2 + l b3 with h, k, l in FFT order (gvec_iter)."""
+    f = [np.fft.fftfreq(n, 1.0 / n) for n in dims]
+    hz, hy, hx = np.meshgrid(f[2], f[1], f[0], indexing="ij")
+    G = np.stack([hx.ravel(), hy.ravel(), hz.ravel()], axis=1) @ np.asarray(recip, dtype=np.float64)
+    return (G * G).sum(axis=1)
+
+
+def to_g(fr, dims):
+    n = dims[0] * dims[1] * dims[2]
+    return np.fft.fftn(np.asarray(fr).reshape(dims[2], dims[1], dims[0])).ravel() / n
+
+
+def to_r(fg, dims):
+    n = dims[0] * dims[1] * dims[2]
+    return np.fft.ifftn(np.asarray(fg).reshape(dims[2], dims[1], dims[0])).ravel().real * n
+
+
+def hxc_potential(rho, dims, recip, volume, v_in_g=None):
+    """build_potential_grid (scf/potential.zig:144-203) without core charge, cutoff Coulomb or an
+    ecutrho filter: V(G) = 8 pi rho(G)/G^2 [G^2 > 1e-12] + V_xc(G) (hartree_potential_at_g,
+    potential.zig:34-44).  Energy terms as scf/energy.zig:372-396: E_H = (vol/2) sum 8 pi |rho(G)|^2/G^2,
+    E_xc = (vol/N) sum f_xc, and int v_in rho = (vol/N) sum_r v_in(r) rho(r).
+    Returns (v_out_g, e_hartree, e_xc, int_vin_rho)."""
+    rho = np.asarray(rho, dtype=np.float64)
+    n = rho.size
+    g2 = g2_table(dims, recip)
+    rg = to_g(rho, dims)
+    f, vxc = lda_pz(rho)
+    m = g2 > 1e-12
+    vh = np.zeros_like(rg)
+    vh[m] = 8.0 * math.pi * rg[m] / g2[m]
+    v_out = vh + to_g(vxc, dims)
+    e_h = 0.5 * volume * float(np.sum(8.0 * math.pi * np.abs(rg[m]) ** 2 / g2[m]))
+    e_xc = float(f.sum()) * volume / n
+    ivr = 0.0
+    if v_in_g is not None:
+        ivr = float(np.dot(to_r(v_in_g, dims), rho)) * volume / n
+    return v_out, e_h, e_xc, ivr
+
+
+def potential_real(v_g, vloc_r, dims):
+    """build_local_potential_real (scf/potential.zig:320-334): V(r) = V_loc(r) + FFT^-1 V(G)."""
+    out = to_r(v_g, dims)
+    return out if vloc_r is None else out + np.asarray(vloc_r, dtype=np.float64)
+
+
+def solve_pulay_system(B, rhs, scaled: bool = False, singular=None):
+    """scf/mixing.zig:341-405: Gaussian elimination with partial pivoting; a pivot below 1e-12
+    returns equal weights (and 0 for the multiplier).  scaled: the overlap block is first divided by
+    its largest diagonal entry (the device module's form), which leaves the weights unchanged and
+    makes the pivot test relative to the residual size."""
+    A = np.array(B, dtype=np.float64)
+    if scaled:
+        m = A.shape[0] - 1
+        d = float(np.max(np.diag(A)[:m]))
+        if d > 0.0:
+            A[:m, :m] /= d
+    b = np.array(rhs, dtype=np.float64)
+    size = b.size
+    for col in range(size):
+        max_row = col + int(np.argmax(np.abs(A[col:, col])))
+        if np.abs(A[max_row, col]) <= np.abs(A[col, col]):
+            max_row = col
+        if max_row != col:
+            A[[col, max_row]] = A[[max_row, col]]
+            b[[col, max_row]] = b[[max_row, col]]
+        pivot = A[col, col]
+        if abs(pivot) < 1e-12:
+            if singular is not None:
+                return singular
+            r = np.full(size, 1.0 / (size - 1))
+            r[-1] = 0.0
+            return r
+        for row in range(col + 1, size):
+            factor = A[row, col] / pivot
+            A[row, col:] -= factor * A[col, col:]
+            b[row] -= factor * b[col]
+    r = np.zeros(size)
+    for i in range(size - 1, -1, -1):
+        r[i] = (b[i] - np.dot(A[i, i + 1:], r[i + 1:])) / A[i, i]
+    return r
+
+
+class Pulay:
+    """PulayMixer.mix_with_residual (scf/mixing.zig:182-248): append (x, r), drop the oldest beyond
+    `history`; fewer than two pairs -> x + beta r; else sum c_i (x_i + beta r_i) with the bordered
+    system B_ij = <r_i|r_j>, sum c_i = 1.
+
+    device_form: the library's variant -- the overlap block scaled by its largest diagonal entry
+    and, where the reference would average the history on a pivot below 1e-12, the oldest pair
+    dropped and the system solved again (down to plain linear mixing)."""
+
+    def __init__(self, history: int, scaled: bool = False, device_form: bool = False):
+        self.history = history
+        self.scaled = scaled or device_form
+        self.device_form = device_form
+        self.xs, self.rs = [], []
+
+    def mix(self, x, r, beta):
+        self.xs.append(np.array(x, dtype=np.float64))
+        self.rs.append(np.array(r, dtype=np.float64))
+        while len(self.xs) > self.history:
+            self.xs.pop(0)
+            self.rs.pop(0)
+        m = len(self.xs)
+        first = 0
+        c = None
+        while m - first >= 2:
+            k = m - first
+            B = np.zeros((k + 1, k + 1))
+            for i in range(k):
+                for j in range(k):
+                    B[i, j] = float(np.dot(self.rs[first + i], self.rs[first + j]))
+                B[i, k] = B[k, i] = -1.0
+            rhs = np.zeros(k + 1)
+            rhs[k] = -1.0
+            c = solve_pulay_system(B, rhs, self.scaled, singular=False if self.device_form else None)
+            if c is not False:
+                break
+            c = None
+            first += 1
+        if c is None:
+            return self.xs[-1] + beta * self.rs[-1]
+        out = np.zeros_like(self.xs[0])
+        for i in range(m - first):
+            out += c[i] * (self.xs[first + i] + beta * self.rs[first + i])
+        return out

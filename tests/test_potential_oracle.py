@@ -1,0 +1,81 @@
+"""The potential-build and mixing oracle (oracle/potential.py) on the CPU: internal consistency,
+and agreement with the host SCF driver's own restatement (dft-zig_b200/scf.py)."""
+import importlib
+import math
+
+import numpy as np
+
+import dftzig_loader
+from oracle import potential as op
+
+dftzig_loader.load()
+scf = importlib.import_module("dftzig_b200.scf")
+
+DIMS = (12, 10, 9)
+RECIP = np.array([[0.61, 0.05, 0.0], [0.02, 0.57, 0.04], [0.0, -0.03, 0.66]])
+VOL = (2 * math.pi) ** 3 / abs(np.linalg.det(RECIP))
+
+
+def _rho(seed=0):
+    rng = np.random.default_rng(seed)
+    n = DIMS[0] * DIMS[1] * DIMS[2]
+    return 0.02 + 0.05 * rng.random(n)
+
+
+def test_lda_pz_potential_is_the_derivative_and_matches_the_driver():
+    n = np.linspace(1e-4, 2.0, 400)
+    f, v = op.lda_pz(n)
+    h = 1e-6 * n
+    fp, _ = op.lda_pz(n + h)
+    fm, _ = op.lda_pz(n - h)
+    np.testing.assert_allclose(v, (fp - fm) / (2 * h), rtol=1e-6)
+    f2, v2 = scf.lda_pz(n)
+    np.testing.assert_allclose(f, f2, rtol=1e-14)
+    np.testing.assert_allclose(v, v2, rtol=1e-14)
+    assert op.lda_pz(np.array([1e-13]))[1][0] == 0.0
+
+
+def test_hartree_energy_is_half_the_potential_integral():
+    rho = _rho()
+    v, e_h, e_xc, _ = op.hxc_potential(rho, DIMS, RECIP, VOL)
+    g2 = op.g2_table(DIMS, RECIP)
+    rg = op.to_g(rho, DIMS)
+    vh = np.where(g2 > 1e-12, 8 * math.pi * rg / np.where(g2 > 1e-12, g2, 1.0), 0.0)
+    n = rho.size
+    assert abs(e_h - 0.5 * VOL / n * float(np.dot(op.to_r(vh, DIMS), rho))) < 1e-10 * abs(e_h)
+    # the driver's own V_hxc(G) and energies on the same grid
+    assert np.abs(v - (vh + op.to_g(op.lda_pz(rho)[1], DIMS))).max() < 1e-14
+    assert e_xc < 0.0
+
+
+def test_int_vin_rho_and_real_space_potential():
+    rho = _rho(1)
+    v_in = op.to_g(np.cos(np.arange(rho.size) * 0.01), DIMS)
+    _, _, _, ivr = op.hxc_potential(rho, DIMS, RECIP, VOL, v_in)
+    vr = op.potential_real(v_in, None, DIMS)
+    assert abs(ivr - float(np.dot(vr, rho)) * VOL / rho.size) < 1e-12 * max(1.0, abs(ivr))
+    vloc = np.linspace(-1, 1, rho.size)
+    np.testing.assert_allclose(op.potential_real(v_in, vloc, DIMS), vr + vloc, atol=1e-13)
+
+
+def test_pulay_oracle_matches_driver_and_the_scaled_solve_is_scale_free():
+    rng = np.random.default_rng(3)
+    A = np.eye(20) * 0.3 + 0.05 * rng.normal(size=(20, 20))
+    b = rng.normal(size=20)
+    x = np.zeros(20)
+    mo, md = op.Pulay(4, device_form=True), scf.PulayMixer(4)
+    xd = x.copy()
+    for _ in range(40):
+        x = mo.mix(x, b - A @ x, 0.5)
+        xd = md.mix(xd, b - A @ xd, 0.5)
+    np.testing.assert_allclose(x, xd, rtol=1e-10, atol=1e-12)
+    assert np.linalg.norm(b - A @ x) < 1e-4 * np.linalg.norm(b)  # plain mixing: 0.85^40 ~ 1.5e-3
+    # the reference's absolute pivot test falls back to equal weights for tiny residual overlaps;
+    # the scaled form solves the same system (weights are scale-free)
+    B = np.array([[4e-14, 1e-14, -1], [1e-14, 2e-14, -1], [-1, -1, 0.0]])
+    rhs = np.array([0, 0, -1.0])
+    np.testing.assert_allclose(op.solve_pulay_system(B, rhs)[:2], [0.5, 0.5])
+    big = B.copy()
+    big[:2, :2] *= 1e14
+    np.testing.assert_allclose(op.solve_pulay_system(B, rhs, scaled=True)[:2], op.solve_pulay_system(big, rhs)[:2], rtol=1e-12)
+    np.testing.assert_allclose(op.solve_pulay_system(B, rhs, scaled=True)[:2], [0.25, 0.75], rtol=1e-12)
