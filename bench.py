@@ -523,7 +523,8 @@ def run_scf216_workload(args):
     defaults (max_subspace 4 nb + 8 = 1800).  Target: a tight FP64 run (density RMS 1e-8).  Reported:
     wall seconds until |E - E_target| < 1e-6 Ry/atom, plain FP64 (reference preconditioner) against
     learned+mixed (TF32X3 contexts until the density residual is below 1e-4, then FP64; the trained
-    TPA-refining MLP preconditioner throughout)."""
+    TPA-refining MLP preconditioner throughout).  Both runs use the resident driver (eigenvectors,
+    density, Hartree-XC potential and Pulay history on the device)."""
     import importlib
 
     import torch
@@ -536,7 +537,7 @@ def run_scf216_workload(args):
     learn = importlib.import_module("dftzig_b200.learn")
     c = system.crystal("si216", 3)
     base = dict(ecut=25.0, kmesh=(1, 1, 1), nbands=448, mixing_beta=0.3, pulay_history=8, max_iter=60)
-    b = scf.GpuBackend(dz, "fp64")
+    b = scf.GpuBackend(dz, "fp64", resident=True)
     ref = scf.run_scf(c, scf.ScfParams(**base, convergence=1e-8), b)
     b.close()
     mlp = (dz.PRECOND_MLP, learn.load_precond_weights())
@@ -544,7 +545,8 @@ def run_scf216_workload(args):
     for mode, prec, pc in (("fp64", "fp64", None), ("learned_mixed", "mixed", mlp)):
         p = scf.ScfParams(**base, convergence=1e-12, energy_target=ref.energy, energy_tol_per_atom=1e-6)
         torch.cuda.synchronize()
-        b = scf.GpuBackend(dz, prec, precond=pc)
+        # resident: eigenvectors, density, potential and Pulay history stay on the device
+        b = scf.GpuBackend(dz, prec, precond=pc, resident=True)
         r = scf.run_scf(c, p, b)
         torch.cuda.synchronize()
         b.close()

@@ -458,10 +458,13 @@ class KpointContext:
         return EigenDecomp(vals, vecs, self.n, info.iterations, info.h_applies, bool(info.converged), info.max_residual)
 
 
-def hermitian_eigen_decomp_iterative_batch(ctxs, diags, nbands, opts: Options = Options(), init_vectors=None) -> list:
+def hermitian_eigen_decomp_iterative_batch(ctxs, diags, nbands, opts: Options = Options(), init_vectors=None,
+                                           device: bool = False) -> list:
     """The iterative solver for several k-point contexts at once (dftcuda_eig_solve_batch): the runs
     advance in lockstep on their contexts' streams.  init_vectors: None or a list with an (icols, n_k)
-    array or None per context.  Returns one EigenDecomp per context."""
+    array (numpy, or a CUDA complex128 tensor read in place) or None per context.  device=True
+    returns the eigenvectors as CUDA tensors (nothing crosses to the host but the eigenvalues).
+    Returns one EigenDecomp per context."""
     lib = load_library()
     nk = len(ctxs)
     if nk == 0:
@@ -481,15 +484,29 @@ def hermitian_eigen_decomp_iterative_batch(ctxs, diags, nbands, opts: Options = 
         keep.append(d)
         d_arr[i] = d.ctypes.data
         if init_vectors is not None and init_vectors[i] is not None:
-            iv = np.ascontiguousarray(init_vectors[i], dtype=np.complex128).reshape(-1, kc.n)
+            iv = init_vectors[i]
+            if _is_torch_cuda(iv):
+                import torch
+
+                if iv.dtype != torch.complex128 or not iv.is_contiguous() or iv.numel() % kc.n:
+                    raise InvalidMatrixSize("init_vectors: contiguous complex128 tensors of whole columns")
+                i_arr[i] = iv.data_ptr()
+                ic_arr[i] = iv.numel() // kc.n
+            else:
+                iv = np.ascontiguousarray(iv, dtype=np.complex128).reshape(-1, kc.n)
+                i_arr[i] = iv.ctypes.data
+                ic_arr[i] = iv.shape[0]
             keep.append(iv)
-            i_arr[i] = iv.ctypes.data
-            ic_arr[i] = iv.shape[0]
         vals = np.empty(nbands)
-        vecs = np.empty((nbands, kc.n), dtype=np.complex128)
+        if device:
+            import torch
+
+            vecs = torch.empty((nbands, kc.n), dtype=torch.complex128, device="cuda")
+        else:
+            vecs = np.empty((nbands, kc.n), dtype=np.complex128)
         out.append((vals, vecs))
         v_arr[i] = vals.ctypes.data
-        x_arr[i] = vecs.ctypes.data
+        x_arr[i] = _ptr(vecs)
     h_arr = (ct.c_void_p * nk)(*[kc.handle.value for kc in ctxs])
     infos = (_EigInfo * nk)()
     _check(lib.dftcuda_eig_solve_batch(nk, h_arr, d_arr, nbands, ct.byref(o), i_arr, ic_arr, v_arr, x_arr, infos))

@@ -175,10 +175,11 @@ __global__ void k_axpy_into(const double* __restrict__ x, const double* __restri
 }
 
 // solve_pulay_system (mixing.zig:341-405): Gaussian elimination with partial pivoting on the
-// bordered (m+1) x (m+1) system; a pivot below 1e-12 gives equal weights.  The overlap block is
-// first divided by its largest diagonal entry: the weights are unchanged, and the pivot test acts
-// relative to the residual size (with the reference's absolute test the mixing falls back to equal
-// weights, and stalls, once residual overlaps drop below 1e-12).
+// bordered (m+1) x (m+1) system.  Two departures, both in the host driver too: the overlap block is
+// first divided by its largest diagonal entry (the weights are unchanged; the pivot test becomes
+// relative to the residual size), and a pivot below 1e-12 returns no solution, upon which the
+// caller drops its oldest pair and solves again, where the reference averages the whole history
+// (which stalls the mixing once more pairs are held than the residuals have directions).
 std::vector<double> solve_pulay(std::vector<double> A, std::vector<double> b, int size) {
   {
     const int m = size - 1;
@@ -203,11 +204,7 @@ std::vector<double> solve_pulay(std::vector<double> A, std::vector<double> b, in
       std::swap(b[col], b[max_row]);
     }
     const double pivot = A[col * size + col];
-    if (std::fabs(pivot) < 1e-12) {
-      std::vector<double> r(size, 1.0 / (double)(size - 1));
-      r[size - 1] = 0.0;
-      return r;
-    }
+    if (std::fabs(pivot) < 1e-12) return {};  // singular: the caller drops its oldest pair
     for (int row = col + 1; row < size; ++row) {
       const double factor = A[row * size + col] / pivot;
       for (int j = col; j < size; ++j) A[row * size + j] -= factor * A[col * size + j];
@@ -417,33 +414,42 @@ extern "C" int dftcuda_pulay_mix(dftcuda_pctx* c, double* x, const double* resid
                                is_device_pointer(residual) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
   double* xo = is_device_pointer(x) ? x : c->px;
   const int m = (int)c->order.size();
-  if (m < 2) {
+  // overlaps of the new residual with every residual held, itself included (every call, so the
+  // overlap table is complete when the history first reaches two pairs)
+  DFT_CUDA_TRY(cudaMemcpyAsync(c->d_slots, c->order.data(), sizeof(int) * m, cudaMemcpyHostToDevice, s));
+  k_pulay_dots<<<kPotBlocks, kPotThreads, 0, s>>>(c->hr + (long)slot * n, c->hr, c->d_slots, m, (long)n, c->part);
+  count_launch();
+  DFT_CUDA_TRY(cudaMemcpyAsync(c->h_part, c->part, sizeof(double) * kPotBlocks * m, cudaMemcpyDeviceToHost, s));
+  DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int j = 0; j < m; ++j) {
+    double d = 0.0;
+    for (int i = 0; i < kPotBlocks; ++i) d += c->h_part[(long)j * kPotBlocks + i];
+    c->B[(size_t)slot * H + c->order[j]] = d;
+    c->B[(size_t)c->order[j] * H + slot] = d;
+  }
+  // DIIS weights over the newest k pairs, k from m down to 2 while the system is singular
+  std::vector<double> coef;
+  int first = 0;
+  for (; m - first >= 2; ++first) {
+    const int k = m - first, sz = k + 1;
+    std::vector<double> A((size_t)sz * sz, 0.0), rhs(sz, 0.0);
+    for (int i = 0; i < k; ++i) {
+      for (int j = 0; j < k; ++j) A[(size_t)i * sz + j] = c->B[(size_t)c->order[first + i] * H + c->order[first + j]];
+      A[(size_t)i * sz + k] = -1.0;
+      A[(size_t)k * sz + i] = -1.0;
+    }
+    rhs[k] = -1.0;
+    coef = solve_pulay(A, rhs, sz);
+    if (!coef.empty()) break;
+  }
+  if (coef.empty()) {
     k_axpy_into<<<kPotBlocks, kPotThreads, 0, s>>>(c->hx + (long)slot * n, c->hr + (long)slot * n, (long)n, beta, xo);
     count_launch();
   } else {
-    // overlaps of the new residual with every residual held (itself included)
-    DFT_CUDA_TRY(cudaMemcpyAsync(c->d_slots, c->order.data(), sizeof(int) * m, cudaMemcpyHostToDevice, s));
-    k_pulay_dots<<<kPotBlocks, kPotThreads, 0, s>>>(c->hr + (long)slot * n, c->hr, c->d_slots, m, (long)n, c->part);
-    count_launch();
-    DFT_CUDA_TRY(cudaMemcpyAsync(c->h_part, c->part, sizeof(double) * kPotBlocks * m, cudaMemcpyDeviceToHost, s));
-    DFT_CUDA_TRY(cudaStreamSynchronize(s));
-    for (int j = 0; j < m; ++j) {
-      double d = 0.0;
-      for (int i = 0; i < kPotBlocks; ++i) d += c->h_part[(long)j * kPotBlocks + i];
-      c->B[(size_t)slot * H + c->order[j]] = d;
-      c->B[(size_t)c->order[j] * H + slot] = d;
-    }
-    const int sz = m + 1;
-    std::vector<double> A((size_t)sz * sz, 0.0), rhs(sz, 0.0);
-    for (int i = 0; i < m; ++i) {
-      for (int j = 0; j < m; ++j) A[(size_t)i * sz + j] = c->B[(size_t)c->order[i] * H + c->order[j]];
-      A[(size_t)i * sz + m] = -1.0;
-      A[(size_t)m * sz + i] = -1.0;
-    }
-    rhs[m] = -1.0;
-    const std::vector<double> coef = solve_pulay(A, rhs, sz);
-    DFT_CUDA_TRY(cudaMemcpyAsync(c->d_coef, coef.data(), sizeof(double) * m, cudaMemcpyHostToDevice, s));
-    k_pulay_combine<<<kPotBlocks, kPotThreads, 0, s>>>(c->hx, c->hr, c->d_slots, c->d_coef, m, (long)n, beta, xo);
+    const int k = m - first;
+    DFT_CUDA_TRY(cudaMemcpyAsync(c->d_slots, c->order.data() + first, sizeof(int) * k, cudaMemcpyHostToDevice, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(c->d_coef, coef.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
+    k_pulay_combine<<<kPotBlocks, kPotThreads, 0, s>>>(c->hx, c->hr, c->d_slots, c->d_coef, k, (long)n, beta, xo);
     count_launch();
   }
   if (xo != x) DFT_CUDA_TRY(cudaMemcpyAsync(x, xo, sizeof(double) * n, cudaMemcpyDeviceToHost, s));

@@ -55,10 +55,19 @@ class KpointComm:
             device = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
         self.device = torch.device(device)
 
-    def sum(self, a: np.ndarray) -> np.ndarray:
-        """Element-wise sum over the ranks (all-reduce), returned to every rank."""
+    def sum(self, a):
+        """Element-wise sum over the ranks (all-reduce), returned to every rank: numpy arrays come
+        back as numpy, tensors as tensors on their own device (reduced in place on the group's
+        device when they are already there: NCCL on GPU ranks)."""
+        torch = self._torch
+        if isinstance(a, torch.Tensor):
+            t = a.to(self.device, dtype=torch.float64).contiguous()
+            if t.data_ptr() == a.data_ptr():
+                t = t.clone()
+            self._dist.all_reduce(t, op=self._dist.ReduceOp.SUM, group=self.group)
+            return t.to(a.device)
         a = np.ascontiguousarray(a, dtype=np.float64)
-        t = self._torch.from_numpy(a.copy()).to(self.device)
+        t = torch.from_numpy(a.copy()).to(self.device)
         self._dist.all_reduce(t, op=self._dist.ReduceOp.SUM, group=self.group)
         return t.cpu().numpy().reshape(a.shape)
 
@@ -72,7 +81,9 @@ class SerialComm:
     rank = 0
     size = 1
 
-    def sum(self, a: np.ndarray) -> np.ndarray:
+    def sum(self, a):
+        if hasattr(a, "clone"):
+            return a.clone()
         return np.array(a, dtype=np.float64, copy=True)
 
     def barrier(self):

@@ -253,9 +253,13 @@ class GpuBackend:
     the sign that the reduced-precision operator's error floor has been reached.  Orthonormalisation,
     the subspace eigensolver, residual checks, occupations and energies stay FP64 throughout."""
 
-    def __init__(self, dz, precision="fp64", switch_drho: float = 1e-4, stall: int = 3, precond=None):
+    def __init__(self, dz, precision="fp64", switch_drho: float = 1e-4, stall: int = 3, precond=None,
+                 resident: bool = False):
         self.dz = dz
         self.precision = precision
+        # resident: eigenvectors stay on the device between iterations, and the SCF state (density,
+        # Hartree-XC potential, Pulay history) lives there too (ScfState uses the device potential)
+        self.resident = resident
         self.precond = precond  # None (reference form) or (kind, params) for every context
         self.switch_drho = switch_drho
         self.stall = stall
@@ -309,7 +313,8 @@ class GpuBackend:
 
     def eig_all(self, diags, nbands, opts: dict, inits):
         """All k-points in one lockstep batch (dftcuda_eig_solve_batch)."""
-        rs = self.dz.hermitian_eigen_decomp_iterative_batch(self._active(), diags, nbands, self.dz.Options(**opts), inits)
+        rs = self.dz.hermitian_eigen_decomp_iterative_batch(self._active(), diags, nbands, self.dz.Options(**opts), inits,
+                                                            device=self.resident)
         return [(r.values, r.vectors) for r in rs]
 
     def density(self, k, vectors, weights, rho):
@@ -413,7 +418,17 @@ class ScfState:
             self.rho = np.asarray(p.initial_density, dtype=np.float64).copy()
             if self.rho.size != N:
                 raise ValueError("initial_density size does not match the FFT grid")
-        self.v_hxc = self.hxc_g(self.rho)
+        # resident backends: density, potential and mixing history on the device (csrc/potential.cu)
+        self.dev = bool(getattr(backend, "resident", False))
+        if self.dev:
+            import torch
+
+            self.pot = backend.dz.PotentialContext(dims, self.vol, c.recip, history=max(1, p.pulay_history))
+            self.rho = torch.from_numpy(self.rho).cuda()
+            self.vloc_d = torch.from_numpy(np.ascontiguousarray(self.vloc_r)).cuda()
+            self.v_hxc, _ = self.pot.hxc(self.rho)
+        else:
+            self.v_hxc = self.hxc_g(self.rho)
         self.mixer = PulayMixer(p.pulay_history)
         self.vectors = [None] * len(self.kin)  # this rank's k-points, in kglobal order
         self.e_ion = ewald_energy(c.cell, np.array([c.species[s].z_val for s in c.atom_species]), c.positions)
@@ -445,7 +460,7 @@ class ScfState:
         """Start the next iteration: set V(r); returns the eigensolver options and warm starts."""
         p = self.p
         self.it += 1
-        local_r = self.vloc_r + self.to_r(self.v_hxc)
+        local_r = self.pot.real(self.v_hxc, self.vloc_d) if self.dev else self.vloc_r + self.to_r(self.v_hxc)
         self.backend.set_vloc(local_r)
         warm = self.it <= p.warmup_steps
         opts = dict(max_iter=p.warmup_max_iter if warm else p.iterative_max_iter, tol=p.warmup_tol if warm else p.iterative_tol)
@@ -473,7 +488,12 @@ class ScfState:
             occ[: self.nocc - 1] = 1.0
             occ[self.nocc - 1] = nelec / 2.0 - (self.nocc - 1)
             occs = [occ for _ in values]
-        rho_out = np.zeros(N)
+        if self.dev:
+            import torch
+
+            rho_out = torch.zeros(N, dtype=torch.float64, device="cuda")
+        else:
+            rho_out = np.zeros(N)
         e_band = 0.0
         e_ent = 0.0
         for k in range(self.nk):
@@ -485,18 +505,25 @@ class ScfState:
             self.backend.density(i, self.vectors[i], self.kweights[k] * occs[k] * 2.0, rho_out)
         if self.comm.size > 1:
             rho_out = self.comm.sum(rho_out)
-        diff = math.sqrt(float(np.mean((rho_out - self.rho) ** 2)))
+        if self.dev:
+            diff = math.sqrt(float(((rho_out - self.rho) ** 2).mean()))
+        else:
+            diff = math.sqrt(float(np.mean((rho_out - self.rho) ** 2)))
         if hasattr(self.backend, "observe"):
             self.backend.observe(diff)
         # energy of rho_out with eigenvalues from V_in (energy.zig:372-396)
-        rg = self.to_g(rho_out)
-        gm = self.gmask
-        e_h = 0.5 * vol * float(np.sum(8.0 * math.pi * np.abs(rg[gm]) ** 2 / self.g2[gm]))
-        fxc, _ = lda_pz(rho_out)
-        dv = vol / N
-        e_xc = float(fxc.sum()) * dv
-        v_in_r = self.to_r(self.v_hxc)
-        int_vin_rho = float(np.dot(v_in_r, rho_out)) * dv
+        if self.dev:
+            v_out_d, terms = self.pot.hxc(rho_out, v_in=self.v_hxc)
+            e_h, e_xc, int_vin_rho = terms["e_hartree"], terms["e_xc"], terms["int_vin_rho"]
+        else:
+            rg = self.to_g(rho_out)
+            gm = self.gmask
+            e_h = 0.5 * vol * float(np.sum(8.0 * math.pi * np.abs(rg[gm]) ** 2 / self.g2[gm]))
+            fxc, _ = lda_pz(rho_out)
+            dv = vol / N
+            e_xc = float(fxc.sum()) * dv
+            v_in_r = self.to_r(self.v_hxc)
+            int_vin_rho = float(np.dot(v_in_r, rho_out)) * dv
         self.energy = e_band - int_vin_rho + e_h + e_xc + self.e_ion + self.psp_core - e_ent
         self.terms = dict(band=e_band, hartree=e_h, xc=e_xc, vin_rho=int_vin_rho, ion_ion=self.e_ion, psp_core=self.psp_core, entropy=e_ent)
         self.history.append((self.it, self.energy, diff, time.perf_counter() - self.t0))
@@ -511,12 +538,23 @@ class ScfState:
             self.converged = self.done = True
             self.rho = rho_out
             return True
-        resid = self.hxc_g(rho_out) - self.v_hxc
-        if self.it >= p.pulay_start:
-            flat = self.mixer.mix(np.concatenate([self.v_hxc.real, self.v_hxc.imag]), np.concatenate([resid.real, resid.imag]), p.mixing_beta)
-            self.v_hxc = flat[:N] + 1j * flat[N:]
+        if self.dev:
+            import torch
+
+            resid = v_out_d - self.v_hxc
+            if self.it >= p.pulay_start:
+                x = torch.view_as_real(self.v_hxc).reshape(-1).clone()
+                self.pot.pulay_mix(x, torch.view_as_real(resid).reshape(-1).contiguous(), p.mixing_beta)
+                self.v_hxc = torch.view_as_complex(x.view(-1, 2))
+            else:
+                self.v_hxc = self.v_hxc + p.mixing_beta * resid
         else:
-            self.v_hxc = self.v_hxc + p.mixing_beta * resid
+            resid = self.hxc_g(rho_out) - self.v_hxc
+            if self.it >= p.pulay_start:
+                flat = self.mixer.mix(np.concatenate([self.v_hxc.real, self.v_hxc.imag]), np.concatenate([resid.real, resid.imag]), p.mixing_beta)
+                self.v_hxc = flat[:N] + 1j * flat[N:]
+            else:
+                self.v_hxc = self.v_hxc + p.mixing_beta * resid
         self.rho = rho_out
         if self.it >= p.max_iter:
             self.done = True
@@ -524,14 +562,26 @@ class ScfState:
 
     def result(self) -> ScfResult:
         natom = len(self.c.atom_species)
-        return ScfResult(self.converged, self.it, self.energy, self.energy / natom, self.values, self.terms, self.rho, self.history,
+        rho = self.rho.cpu().numpy() if self.dev else self.rho
+        return ScfResult(self.converged, self.it, self.energy, self.energy / natom, self.values, self.terms, rho, self.history,
                          time.perf_counter() - self.t0)
+
+    def close(self):
+        if self.dev:
+            self.pot.close()
 
 
 def run_scf(c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False, comm=None) -> ScfResult:
     """The SCF loop.  ``comm`` (a kpar.KpointComm) deals the k-points over the ranks of a process
     group; every rank returns the same result."""
     st = ScfState(c, p, backend, verbose, comm)
+    try:
+        return _run(st, backend)
+    finally:
+        st.close()
+
+
+def _run(st, backend) -> ScfResult:
     while not st.done:
         opts, inits = st.begin()
         diags = [inp.basis.kinetic for inp in st.kin]
@@ -591,6 +641,7 @@ def run_scf_many(dz, cells, p: ScfParams, precision: str = "fp64", initial_densi
         phases["finish"] += time.perf_counter() - tf
     results = [st.result() for st in states]
     for st in states:
+        st.close()
         st.backend.close()
     run_scf_many.last_phases = {k: round(v, 3) for k, v in phases.items()}
     return results, time.perf_counter() - t0

@@ -65,10 +65,13 @@ def test_potential_real_matches_oracle(dz):
 @pytest.mark.parametrize("on_device", [False, True], ids=["host", "device"])
 def test_pulay_mix_matches_oracle(dz, on_device):
     """Eight steps with a history of four on a linear fixed point x = b + (1 - A) x in 2000 dims,
-    then a reset: the device history, overlaps and DIIS weights follow the oracle's device form."""
+    then a reset: the device history, overlaps and DIIS weights follow the oracle's device form.
+    The operator's spectrum is wide (0.3 .. 1.2): with a narrow one the residuals are nearly
+    collinear and the DIIS weights amplify summation-order rounding to 1e-9 (the oracle against
+    itself with its dot products summed in another order)."""
     rng = np.random.default_rng(5)
     n = 2000
-    A = 0.3 + 0.05 * rng.random(n)  # a diagonal operator: residual b - A x
+    A = 0.3 + 0.9 * rng.random(n)  # a diagonal operator: residual b - A x
     b = rng.normal(size=n)
     pc = dz.PotentialContext((4, 4, 4), 1.0, np.eye(3), history=4)
     try:
@@ -89,7 +92,7 @@ def test_pulay_mix_matches_oracle(dz, on_device):
                 pc.pulay_mix(x, r, 0.5)
             got = x.cpu().numpy() if on_device else x
             assert np.abs(got - x_ref).max() < 1e-10 * max(1.0, np.abs(x_ref).max()), it
-        assert np.linalg.norm(b - A * x_ref) < 0.05 * np.linalg.norm(b)
+        assert np.linalg.norm(b - A * x_ref) < 0.1 * np.linalg.norm(b)
     finally:
         pc.close()
 
