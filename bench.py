@@ -553,7 +553,10 @@ def run_scf216_workload(args):
         if not r.converged:
             raise RuntimeError(f"time-to-SCF run ({mode}) did not reach the target")
         out[mode] = {"seconds": round(r.wall_s, 3), "scf_iterations": r.iterations, "dE_per_atom": r.energy_per_atom - ref.energy_per_atom,
-                     "switched_to_fp64_at_iteration": getattr(b, "switched_at", None)}
+                     "switched_to_fp64_at_iteration": getattr(b, "switched_at", None),
+                     # per SCF iteration: seconds since start, density residual, solver precision,
+                     # Davidson iterations, H applications
+                     "trace": [[round(h[3], 2), float(f"{h[2]:.2e}"), sv[0], sv[1], sv[2]] for h, sv in zip(r.history, b.solves)]}
     line = {
         "metric": "time-to-SCF (|dE| < 1e-6 Ry/atom vs tight FP64), Si216 25 Ry Gamma, learned+mixed vs plain FP64",
         "value": out["learned_mixed"]["seconds"],

@@ -68,6 +68,7 @@ ABI_SYMBOLS = (
     "dftcuda_potential_real",
     "dftcuda_pulay_mix",
     "dftcuda_pulay_reset",
+    "dftcuda_ionic_potential",
 )
 
 PRECOND_REFERENCE = 0  # r / (|k+G|^2 - lambda), lobpcg/common.zig:214-226
@@ -234,6 +235,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.dftcuda_potential_real.argtypes = [vp, dp, dp, dp]
     lib.dftcuda_pulay_mix.argtypes = [vp, dp, dp, sz, ct.c_double]
     lib.dftcuda_pulay_reset.argtypes = [vp]
+    lib.dftcuda_ionic_potential.argtypes = [vp, ip, vp, ip, vp, vp, ct.c_double, dp, dp]
     lb = ct.c_long
     lib.dftcuda_complex_gemm.argtypes = [ip, sz, sz, sz, vp, lb, ip, ip, vp, lb, ip, ip, vp, lb, lb, ct.c_double, ct.c_double]
     _lib = lib
@@ -647,6 +649,24 @@ class PotentialContext:
 
     def reset(self):
         _check(load_library().dftcuda_pulay_reset(self._h))
+
+    def ionic(self, gth, atom_species, positions, g2max: float = 0.0, device: bool = False):
+        """V_loc(r) of GTH-local pseudopotentials: gth (nspecies, 6) = Z, r_loc, C1..C4; atoms by
+        species index and Cartesian bohr positions.  Returns (V(G), V_loc(r)), numpy or CUDA tensors."""
+        g = np.ascontiguousarray(np.asarray(gth, dtype=np.float64).reshape(-1, 6))
+        sp = np.ascontiguousarray(atom_species, dtype=np.int32)
+        pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1, 3))
+        if device:
+            import torch
+
+            vg = torch.empty(self.N, dtype=torch.complex128, device="cuda")
+            vr = torch.empty(self.N, dtype=torch.float64, device="cuda")
+        else:
+            vg = np.empty(self.N, dtype=np.complex128)
+            vr = np.empty(self.N, dtype=np.float64)
+        _check(load_library().dftcuda_ionic_potential(self._h, g.shape[0], g.ctypes.data, sp.size, sp.ctypes.data, pos.ctypes.data,
+                                                      float(g2max), _ptr(vg), _ptr(vr)))
+        return vg, vr
 
     def close(self):
         if self._h:

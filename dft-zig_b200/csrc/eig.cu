@@ -19,6 +19,8 @@
 //    project the kept vectors out of V once more and take a second Cholesky pass (CholQR2).  This spans exactly the vectors MGS
 //    keeps, in the same order; only rounding differs.
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -906,17 +908,36 @@ static int sync_runs(std::vector<EigRun>& runs, bool only_pending) {
   return DFTCUDA_OK;
 }
 
+// Host-side phase timers of the lockstep driver, printed to stderr after each solve when
+// DFTCUDA_EIG_TIMERS is set: host time spent issuing each phase and blocked in the syncs.
+struct EigTimers {
+  double t[6] = {0, 0, 0, 0, 0, 0};  // init, rr issue, sync after rr, decide issue, orth syncs, orth_b issue
+  long syncs = 0;
+};
+static bool eig_timers_on() {
+  static const bool on = std::getenv("DFTCUDA_EIG_TIMERS") != nullptr;
+  return on;
+}
+static double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 // Lockstep driver: every active run does RR; one synchronisation; every run decides (and launches
 // phase A of a chunk); one synchronisation; phase B for those with a chunk (repeated while chunks
 // remain); loop.
 static int eig_solve_runs(std::vector<EigRun>& runs, const std::vector<const double*>& diags,
                           const std::vector<const double*>& inits, const std::vector<size_t>& icols) {
+  EigTimers tm;
+  double t0 = now_s();
   for (size_t i = 0; i < runs.size(); ++i) {
     runs[i].status = run_init(runs[i], diags[i], inits[i], icols[i]);
     if (runs[i].status != DFTCUDA_OK) runs[i].done = true;
   }
+  double t1 = now_s();
+  tm.t[0] += t1 - t0;
   for (;;) {
     bool any = false;
+    t0 = now_s();
     for (EigRun& r : runs) {
       if (r.done || r.status != DFTCUDA_OK) continue;
       if (r.it >= r.opts.max_iter) {
@@ -926,23 +947,40 @@ static int eig_solve_runs(std::vector<EigRun>& runs, const std::vector<const dou
       r.status = run_rr(r);
       any = true;
     }
+    t1 = now_s();
+    tm.t[1] += t1 - t0;
     if (!any) break;
     sync_runs(runs, false);
+    ++tm.syncs;
+    t0 = now_s();
+    tm.t[2] += t0 - t1;
     for (EigRun& r : runs) {
       if (r.done || r.status != DFTCUDA_OK) continue;
       r.status = run_decide(r);
     }
+    t1 = now_s();
+    tm.t[3] += t1 - t0;
     for (;;) {
       bool pend = false;
       for (EigRun& r : runs) pend |= (!r.done && r.status == DFTCUDA_OK && r.orth_pending);
       if (!pend) break;
+      t0 = now_s();
       sync_runs(runs, true);
+      ++tm.syncs;
+      t1 = now_s();
+      tm.t[4] += t1 - t0;
       for (EigRun& r : runs) {
         if (r.done || r.status != DFTCUDA_OK || !r.orth_pending) continue;
         r.status = run_orth_b(r);
       }
+      tm.t[5] += now_s() - t1;
     }
   }
+  if (eig_timers_on())
+    std::fprintf(stderr,
+                 "eig timers: init %.1f ms, rr issue %.1f, rr sync %.1f, decide issue %.1f, orth syncs %.1f, orth_b issue "
+                 "%.1f (%ld syncs)\n",
+                 1e3 * tm.t[0], 1e3 * tm.t[1], 1e3 * tm.t[2], 1e3 * tm.t[3], 1e3 * tm.t[4], 1e3 * tm.t[5], tm.syncs);
   int first = DFTCUDA_OK;
   for (EigRun& r : runs) {
     if (r.status == DFTCUDA_OK) r.status = run_finish(r);

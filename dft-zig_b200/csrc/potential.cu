@@ -8,6 +8,8 @@
 //                           terms of scf/energy.zig:372-396 from the same passes
 //   dftcuda_potential_real  V(r) = V_loc(r) + FFT^-1 V(G) (build_local_potential_real,
 //                           potential.zig:320-334)
+//   dftcuda_ionic_potential V_ion(G) and V_loc(r) (build_ionic_potential_grid, potential.zig:279-318)
+//                           with the analytic GTH local form factor
 //   dftcuda_pulay_mix       PulayMixer.mix_with_residual (scf/mixing.zig:182-248) with the bordered
 //                           system solved as solve_pulay_system (mixing.zig:341-405)
 //
@@ -135,6 +137,78 @@ __global__ void __launch_bounds__(kPotThreads) k_pot_hartree(const double2* __re
   }
 }
 
+// Ionic local potential in G space (build_ionic_potential_grid, scf/potential.zig:279-318):
+// V(G) = (2 / Omega) sum_atoms ff_s(|G|) e^{-i G . tau} for 1e-12 < G^2 <= g2max, else 0, with the
+// analytic local form factor of Goedecker-Teter-Hutter pseudopotentials (Hartree, hence the 2 for Ry):
+//   ff(G) = -4 pi Z / G^2 e^{-x} + sqrt(8 pi^3) r^3 e^{-x} [C1 + C2 (3 - y) + C3 (15 - 10 y + y^2)
+//           + C4 (105 - 105 y + 21 y^2 - y^3)],  y = G^2 r^2, x = y / 2.
+// One thread per G point; atom positions and species parameters in shared memory.
+constexpr int kIonMaxSpecies = 8;
+constexpr int kIonAtomTile = 512;
+__global__ void __launch_bounds__(kPotThreads) k_pot_ionic(const double* __restrict__ g2, int nx, int ny, int nz, double b00,
+                                                           double b01, double b02, double b10, double b11, double b12,
+                                                           double b20, double b21, double b22, int nspecies,
+                                                           const double* __restrict__ gth, int natoms,
+                                                           const int* __restrict__ species, const double* __restrict__ pos,
+                                                           double g2max, double inv_volume, double2* __restrict__ out) {
+  __shared__ double sx[kIonAtomTile], sy[kIonAtomTile], sz[kIonAtomTile];
+  __shared__ int ss[kIonAtomTile];
+  const long N = (long)nx * ny * nz;
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double gx = 0.0, gy = 0.0, gz = 0.0, q = 0.0;
+  if (i < N) {
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long)nx * ny));
+    const double h = x < (nx + 1) / 2 ? x : x - nx;
+    const double k = y < (ny + 1) / 2 ? y : y - ny;
+    const double l = z < (nz + 1) / 2 ? z : z - nz;
+    gx = h * b00 + k * b10 + l * b20;
+    gy = h * b01 + k * b11 + l * b21;
+    gz = h * b02 + k * b12 + l * b22;
+    q = g2[i];
+  }
+  double sre[kIonMaxSpecies], sim[kIonMaxSpecies];
+#pragma unroll
+  for (int s = 0; s < kIonMaxSpecies; ++s) sre[s] = sim[s] = 0.0;
+  for (int a0 = 0; a0 < natoms; a0 += kIonAtomTile) {
+    const int na = min(kIonAtomTile, natoms - a0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < na; t += blockDim.x) {
+      sx[t] = pos[3 * (a0 + t)];
+      sy[t] = pos[3 * (a0 + t) + 1];
+      sz[t] = pos[3 * (a0 + t) + 2];
+      ss[t] = species[a0 + t];
+    }
+    __syncthreads();
+    for (int t = 0; t < na; ++t) {
+      double sn, cs;
+      sincos(gx * sx[t] + gy * sy[t] + gz * sz[t], &sn, &cs);
+      const int sp = ss[t];
+#pragma unroll
+      for (int s = 0; s < kIonMaxSpecies; ++s)
+        if (s == sp) {
+          sre[s] += cs;
+          sim[s] -= sn;  // e^{-i G . tau}
+        }
+    }
+  }
+  if (i >= N) return;
+  double2 v = make_double2(0.0, 0.0);
+  if (q > 1e-12 && q <= g2max) {
+    for (int s = 0; s < nspecies; ++s) {
+      const double Z = gth[6 * s], r = gth[6 * s + 1];
+      const double c1 = gth[6 * s + 2], c2 = gth[6 * s + 3], c3 = gth[6 * s + 4], c4 = gth[6 * s + 5];
+      const double yy = q * r * r, e = exp(-0.5 * yy);
+      const double poly = c1 + c2 * (3.0 - yy) + c3 * (15.0 - 10.0 * yy + yy * yy) +
+                          c4 * (105.0 - 105.0 * yy + 21.0 * yy * yy - yy * yy * yy);
+      const double ff = -4.0 * kPi * Z / q * e + sqrt(8.0 * kPi * kPi * kPi) * r * r * r * e * poly;
+      const double w = 2.0 * ff * inv_volume;
+      v.x += w * sre[s];
+      v.y += w * sim[s];
+    }
+  }
+  out[i] = v;
+}
+
 // out_r = vloc + Re(v) * N (v holds FFT^-1 / N of the G-space field).
 __global__ void k_pot_real(const double2* __restrict__ v, const double* __restrict__ vloc, long N, double* __restrict__ out) {
   const double scale = (double)N;
@@ -229,6 +303,7 @@ struct dftcuda_pctx {
   int nx = 0, ny = 0, nz = 0;
   long N = 0;
   double volume = 0.0;
+  double recip[9] = {};
   int history = 0;
   dftcuda_fft_plan* plan = nullptr;
   cudaStream_t stream = nullptr;
@@ -266,6 +341,7 @@ extern "C" int dftcuda_pctx_create(dftcuda_pctx** out, int nx, int ny, int nz, d
   c->nx = nx; c->ny = ny; c->nz = nz;
   c->N = (long)nx * ny * nz;
   c->volume = volume;
+  for (int i = 0; i < 9; ++i) c->recip[i] = recip[i];
   c->history = pulay_history;
   int st = dftcuda_fft_plan_create(&c->plan, nx, ny, nz);
   if (st != DFTCUDA_OK) return pctx_fail_free(c, st);
@@ -366,6 +442,57 @@ extern "C" int dftcuda_potential_real(dftcuda_pctx* c, const double* v_g, const 
   if (out != out_r) DFT_TRY(copy_out(out_r, out, sizeof(double) * N, s));
   DFT_CUDA_TRY(cudaStreamSynchronize(s));
   return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_ionic_potential(dftcuda_pctx* c, int nspecies, const double* gth, int natoms, const int* atom_species,
+                                       const double* positions, double g2max, double* v_out_g, double* vloc_r) {
+  if (!c || nspecies < 1 || nspecies > kIonMaxSpecies || !gth || natoms < 0 || (natoms > 0 && (!atom_species || !positions)))
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "ionic_potential: bad arguments (1..8 species)");
+  for (int a = 0; a < natoms; ++a)
+    if (atom_species[a] < 0 || atom_species[a] >= nspecies)
+      return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "ionic_potential: atom species index out of range");
+  const long N = c->N;
+  cudaStream_t s = c->stream;
+  double* d_gth = nullptr;
+  double* d_pos = nullptr;
+  int* d_sp = nullptr;
+  auto cleanup = [&] {
+    if (d_gth) cudaFree(d_gth);
+    if (d_pos) cudaFree(d_pos);
+    if (d_sp) cudaFree(d_sp);
+  };
+  if (cudaMalloc(&d_gth, sizeof(double) * 6 * nspecies) != cudaSuccess ||
+      cudaMalloc(&d_pos, sizeof(double) * 3 * std::max(natoms, 1)) != cudaSuccess ||
+      cudaMalloc(&d_sp, sizeof(int) * std::max(natoms, 1)) != cudaSuccess) {
+    cleanup();
+    return fail(DFTCUDA_ERR_CUDA, "ionic_potential: allocation failed");
+  }
+  int st = DFTCUDA_OK;
+  if (cudaMemcpyAsync(d_gth, gth, sizeof(double) * 6 * nspecies, cudaMemcpyDefault, s) != cudaSuccess ||
+      (natoms > 0 && (cudaMemcpyAsync(d_pos, positions, sizeof(double) * 3 * natoms, cudaMemcpyDefault, s) != cudaSuccess ||
+                      cudaMemcpyAsync(d_sp, atom_species, sizeof(int) * natoms, cudaMemcpyDefault, s) != cudaSuccess)))
+    st = fail(DFTCUDA_ERR_CUDA, "ionic_potential: copy failed");
+  if (st == DFTCUDA_OK) {
+    const double* r = c->recip;
+    k_pot_ionic<<<(unsigned)ceil_div(N, kPotThreads), kPotThreads, 0, s>>>(
+        c->g2, c->nx, c->ny, c->nz, r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8], nspecies, d_gth, natoms, d_sp, d_pos,
+        g2max > 0.0 ? g2max : 1e300, 1.0 / c->volume, c->b);
+    count_launch();
+    if (v_out_g && copy_out(v_out_g, c->b, sizeof(double2) * N, s) != DFTCUDA_OK) st = DFTCUDA_ERR_CUDA;
+  }
+  if (st == DFTCUDA_OK && vloc_r) {
+    DFT_CUDA_TRY(cudaMemcpyAsync(c->a, c->b, sizeof(double2) * N, cudaMemcpyDeviceToDevice, s));
+    st = fft3d_on_stream(c->plan, c->a, +1, s);
+    if (st == DFTCUDA_OK) {
+      double* out = is_device_pointer(vloc_r) ? vloc_r : reinterpret_cast<double*>(c->b);
+      k_pot_real<<<kPotBlocks, kPotThreads, 0, s>>>(c->a, nullptr, N, out);
+      count_launch();
+      if (out != vloc_r) st = copy_out(vloc_r, out, sizeof(double) * N, s);
+    }
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess && st == DFTCUDA_OK) st = fail(DFTCUDA_ERR_CUDA, "ionic_potential: kernel failed");
+  cleanup();
+  return st;
 }
 
 extern "C" int dftcuda_pulay_reset(dftcuda_pctx* c) {

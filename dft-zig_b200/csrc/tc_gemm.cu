@@ -544,10 +544,10 @@ __global__ void __launch_bounds__(T2_THREADS) k_cgemm_tc2(int M, int N, int K, c
 // For products whose both output dimensions reach 128 (Rayleigh-Ritz Gram matrices, subspace
 // rotations): a 256-column tile gives every converted operand element four times the MMA work of
 // the 64-column tiles above.  Warps 0-7 are converters: each thread owns three of the slot's 768
-// core-matrix rows (A: 16 row groups x 2 k groups x 8 rows, B: 32 x 2 x 8), loads their FP64
-// elements one K step ahead into registers, waits for the slot to be free, writes the TF32 planes
-// (hi and lo parts for 3xTF32) into the ring as 16-byte vectors and arrives on the slot's "full"
-// mbarrier.  Lane 0 of warp 8 waits for full slots and
+// core-matrix rows (A: 16 row groups x 2 k groups x 8 rows, B: 32 x 2 x 8), copies their FP64
+// elements with cp.async two K steps ahead into its own part of a shared-memory staging ring, waits
+// for the TF32 slot to be free, writes the TF32 planes (hi and lo parts for 3xTF32) into the ring
+// as 16-byte vectors and arrives on the slot's "full" mbarrier.  Lane 0 of warp 8 waits for full slots and
 // issues one 8-deep K step per slot (12 MMAs for 3xTF32, 4 otherwise) of 128 x 256 x 8, committing
 // each slot back to its "empty" mbarrier.  TMEM holds the two 256-column FP32 accumulators (all 512
 // columns; the shared-memory footprint keeps one CTA per SM).  Waits are bounded; a timeout sets the
@@ -564,8 +564,15 @@ constexpr int T3_ACM = (TC_M / 8) * (T3_K / 4);   // 32 core matrices of A per s
 constexpr int T3_BCM = (T3_N / 8) * (T3_K / 4);   // 64 of B
 constexpr uint32_t T3_TMEM_COLS = 512;
 __host__ __device__ constexpr int t3_slot(bool split) { return split ? 2 * T3_SLOT : T3_SLOT; }
-__host__ __device__ constexpr int t3_stages(bool split) { return split ? 4 : 8; }
-__host__ __device__ constexpr int t3_smem(bool split) { return t3_stages(split) * t3_slot(split) + 256; }  // + barriers, TMEM slot
+__host__ __device__ constexpr int t3_stages(bool split) { return split ? 2 : 4; }
+// FP64 staging: each converter thread's 12 elements of a K step, element-major (element e of
+// thread t at e * 4 KB + t * 16 B, so consecutive lanes touch consecutive 16 bytes), T3_D steps
+// deep: the cp.async copies of step t + T3_D are in flight while step t converts.
+constexpr int T3_D = 2;
+constexpr int T3_STG = 12 * T3_CONV_WARPS * 32 * 16;  // 48 KB
+__host__ __device__ constexpr int t3_smem(bool split) {
+  return t3_stages(split) * t3_slot(split) + T3_D * T3_STG + 256;  // + barriers, TMEM slot
+}
 
 // Byte offset of (row, k) in a slot plane: core matrices of 8 rows x 4 k (128 B), the two k groups
 // of a row group adjacent (LBO 128 B), row groups 256 B apart (SBO).
@@ -688,7 +695,7 @@ __global__ void __launch_bounds__(T3_THREADS, 1) k_cgemm_tc3(int M, int N, int K
   // barriers: full[NS] (converters -> MMA), empty[NS] (MMA -> converters), chunk_done (MMA ->
   // converters: a chunk's MMAs are complete), drained (converters -> MMA: TMEM read out), fin (all
   // MMAs complete)
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm3 + NS * SL);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm3 + NS * SL + T3_D * T3_STG);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2 * NS + 3);
   __shared__ volatile int s_abort;
   __shared__ int s_issued;
@@ -748,21 +755,29 @@ __global__ void __launch_bounds__(T3_THREADS, 1) k_cgemm_tc3(int M, int N, int K
       ustep[u] = kc ? 1 : ld;  // between consecutive k
       uoff[u] = (uint32_t)(rg * 256 + kg * 128 + r8 * 16);
     }
-    double2 cur[12], nxt[12];
-    // loads of K step t (pointers advance by 8 k per step; the k bound only matters on the last)
-    auto load_step = [&](int t, double2* v) {
-      const int kk0 = kbeg + t * T3_K;
-      const bool full = kk0 + T3_K <= kend;
+    double2 cur[12];
+    const uint32_t stg = (uint32_t)__cvta_generic_to_shared(tsm3 + NS * SL) + (uint32_t)tid * 16;
+    const double2* stg_own = reinterpret_cast<const double2*>(tsm3 + NS * SL) + tid;
+    // cp.async copies of K step t into staging slot t % T3_D (zero-filled outside the matrix;
+    // pointers advance by 8 k per step, the k bound only matters on the last step); one commit group
+    auto issue_step = [&](int t) {
+      if (t < ntiles) {
+        const int kk0 = kbeg + t * T3_K;
+        const bool full = kk0 + T3_K <= kend;
+        const uint32_t sb = stg + (uint32_t)((t % T3_D) * T3_STG);
 #pragma unroll
-      for (int u = 0; u < 3; ++u) {
-        const int kgu = (int)((uoff[u] >> 7) & 1);
-        const double2* p = up[u] + (long)t * T3_K * ustep[u];
+        for (int u = 0; u < 3; ++u) {
+          const int kgu = (int)((uoff[u] >> 7) & 1);
+          const double2* p = up[u] + (long)t * T3_K * ustep[u];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const bool ok = uok[u] && (full || kk0 + kgu * 4 + j < kend);
-          v[u * 4 + j] = ok ? __ldg(p + (long)j * ustep[u]) : make_double2(0.0, 0.0);
+          for (int j = 0; j < 4; ++j) {
+            const bool ok = uok[u] && (full || kk0 + kgu * 4 + j < kend);
+            // a predicated-off copy reads nothing (zero fill); its source is the operand's base
+            t2_cp16(sb + (uint32_t)((u * 4 + j) * 4096), ok ? (const void*)(p + (long)j * ustep[u]) : (const void*)(u == 0 ? A : B), ok);
+          }
         }
       }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
     int drained = 0;  // chunks drained so far
     // wait for chunk `drained` to finish, drain it, release the accumulators; false on abort
@@ -783,7 +798,8 @@ __global__ void __launch_bounds__(T3_THREADS, 1) k_cgemm_tc3(int M, int N, int K
       ++drained;
       return true;
     };
-    if (ntiles > 0) load_step(0, cur);
+#pragma unroll
+    for (int d = 0; d < T3_D; ++d) issue_step(d);
     for (int t = 0; t < ntiles; ++t) {
       const int q = t % NS;
       // the slot's previous stage t - NS opens a new chunk: its MMAs wait for the previous chunk's
@@ -791,7 +807,12 @@ __global__ void __launch_bounds__(T3_THREADS, 1) k_cgemm_tc3(int M, int N, int K
       if (t >= NS && (t - NS) % chunk == 0 && (t - NS) / chunk > drained) {
         if (!__shfl_sync(0xffffffffu, s_abort, 0)) drain_next();
       }
-      if (t + 1 < ntiles) load_step(t + 1, nxt);
+      // this thread's copies of step t have landed (the T3_D - 1 younger groups may be pending);
+      // the thread reads only what it copied itself, so no block barrier is needed
+      asm volatile("cp.async.wait_group %0;\n" ::"n"(T3_D - 1) : "memory");
+#pragma unroll
+      for (int e = 0; e < 12; ++e) cur[e] = stg_own[(t % T3_D) * (T3_STG / 16) + e * 256];
+      issue_step(t + T3_D);
       if (t >= NS) {
         int ok = 1;
         if (lane == 0) ok = tc_wait(mb + 8 * (NS + q), (uint32_t)((t / NS - 1) & 1)) ? 1 : 0;
@@ -809,9 +830,9 @@ __global__ void __launch_bounds__(T3_THREADS, 1) k_cgemm_tc3(int M, int N, int K
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       __syncwarp();
       if (lane == 0) t3_arrive(mb + 8 * q);
-#pragma unroll
-      for (int i = 0; i < 12; ++i) cur[i] = nxt[i];
     }
+    // every copy this thread issued has landed before the CTA goes on (also after an abort)
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     // the chunks not drained inside the loop, the last one included
     while (drained < nchunks && !__shfl_sync(0xffffffffu, s_abort, 0)) {
       if (!drain_next()) break;

@@ -75,13 +75,17 @@ def lda_pz(n: np.ndarray):
     return f, v
 
 
-def ewald_energy(cell: np.ndarray, charges: np.ndarray, pos: np.ndarray, tol: float = 1e-14) -> float:
-    """Ion-ion energy (Ry) by the Ewald split: real-space erfc sum + reciprocal sum - self - background."""
+def ewald_energy(cell: np.ndarray, charges: np.ndarray, pos: np.ndarray, tol: float = 1e-14, eta: Optional[float] = None) -> float:
+    """Ion-ion energy (Ry) by the Ewald split: real-space erfc sum + reciprocal sum - self - background.
+    The split parameter eta (bohr^-1) does not change the result; by default it follows the atom
+    density, 0.85 sqrt(pi) (N / V^2)^(1/6), which balances the real-space image sum against the
+    reciprocal one for large cells (Si216: 0.3 s instead of seconds)."""
     from scipy.special import erfc
 
     vol = abs(np.linalg.det(cell))
     recip = 2.0 * math.pi * np.linalg.inv(cell).T
-    eta = math.sqrt(math.pi) / vol ** (1.0 / 3.0)
+    if eta is None:
+        eta = 0.85 * math.sqrt(math.pi) * (len(charges) / vol**2) ** (1.0 / 6.0)
     # real-space cutoff where erfc(eta r) < tol, reciprocal cutoff where exp(-G^2/4eta^2) < tol
     rcut = math.sqrt(-math.log(tol)) / eta + 1e-9
     gcut = 2.0 * eta * math.sqrt(-math.log(tol))
@@ -89,11 +93,14 @@ def ewald_energy(cell: np.ndarray, charges: np.ndarray, pos: np.ndarray, tol: fl
     e_real = 0.0
     rng = [np.arange(-n, n + 1) for n in na]
     L = np.stack(np.meshgrid(*rng, indexing="ij"), axis=-1).reshape(-1, 3) @ cell
+    dmax = float(np.linalg.norm(pos[:, None, :] - pos[None, :, :], axis=2).max())
+    L = L[np.linalg.norm(L, axis=1) < rcut + dmax + 1e-9]  # |d + L| < rcut needs |L| < rcut + |d|
     for i in range(len(charges)):
         d = pos[i][None, :] - pos  # [j, 3]
         r = np.linalg.norm(d[:, None, :] + L[None, :, :], axis=2)  # [j, L]
         mask = (r > 1e-10) & (r < rcut)
-        e_real += 0.5 * charges[i] * np.sum((charges[:, None] * erfc(eta * r) / np.where(mask, r, 1.0)) * mask)
+        rr = r[mask]
+        e_real += 0.5 * charges[i] * float(np.sum(np.broadcast_to(charges[:, None], r.shape)[mask] * erfc(eta * rr) / rr))
     ng = [int(math.ceil(gcut / np.linalg.norm(recip[i]))) + 1 for i in range(3)]
     rng = [np.arange(-n, n + 1) for n in ng]
     G = np.stack(np.meshgrid(*rng, indexing="ij"), axis=-1).reshape(-1, 3) @ recip
@@ -271,6 +278,7 @@ class GpuBackend:
         self.since_best = 0
         self.switched_at = None
         self.n_obs = 0
+        self.solves = []  # (precision, Davidson iterations, H applications) per eig_all call
 
     def _make(self, inp, prec):
         kc = self.dz.KpointContext(*inp.dims, inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart, prec)
@@ -315,6 +323,7 @@ class GpuBackend:
         """All k-points in one lockstep batch (dftcuda_eig_solve_batch)."""
         rs = self.dz.hermitian_eigen_decomp_iterative_batch(self._active(), diags, nbands, self.dz.Options(**opts), inits,
                                                             device=self.resident)
+        self.solves.append(("tf32x3" if self.use32 else "fp64", max(r.iterations for r in rs), sum(r.h_applies for r in rs)))
         return [(r.values, r.vectors) for r in rs]
 
     def density(self, k, vectors, weights, rho):
@@ -402,13 +411,32 @@ class ScfState:
         costs = [sysm.basis(c.recip, p.ecut, k).hkl.shape[0] for k, _ in kpts] if self.comm.size > 1 else None
         self.owner = kpar.deal_kpoints(self.nk, self.comm.size, costs)
         self.kglobal = [k for k in range(self.nk) if self.owner[k] == self.comm.rank]
+        tm = self.setup_times = {}
+        t = time.perf_counter()
         tables = [[sysm.radial_table(sp, i, p.ecut) for i in range(len(sp.betas))] for sp in c.species]
-        self.vloc_r = sysm.local_potential(c, dims, p.ecut)
+        tm["radial_tables"], t = time.perf_counter() - t, time.perf_counter()
+        # resident backends: density, potential and mixing history on the device (csrc/potential.cu),
+        # the ionic local potential built there too
+        self.dev = bool(getattr(backend, "resident", False))
+        if self.dev:
+            import torch
+
+            self.pot = backend.dz.PotentialContext(dims, self.vol, c.recip, history=max(1, p.pulay_history))
+            gth = [[sp.params["z"], sp.params["rloc"], sp.params.get("c1", 0.0), sp.params.get("c2", 0.0),
+                    sp.params.get("c3", 0.0), sp.params.get("c4", 0.0)] for sp in c.species]
+            _, self.vloc_d = self.pot.ionic(gth, c.atom_species, c.positions, 4.0 * p.ecut, device=True)
+            self.vloc_r = self.vloc_d.cpu().numpy()
+        else:
+            self.vloc_r = sysm.local_potential(c, dims, p.ecut)
+        tm["local_potential"], t = time.perf_counter() - t, time.perf_counter()
         self.kin = [sysm.kpoint_inputs(c, p.ecut, kpts[k][0], dims=dims, local_r=self.vloc_r, tables=tables) for k in self.kglobal]
         self.kweights = [w for _, w in kpts]
+        tm["kpoint_inputs"], t = time.perf_counter() - t, time.perf_counter()
         backend.setup(self.kin)
-        self.g2 = g_vectors(dims, c.recip)
-        self.gmask = self.g2 > 1e-12
+        tm["contexts"], t = time.perf_counter() - t, time.perf_counter()
+        if not self.dev:  # the host potential path's G-vector table
+            self.g2 = g_vectors(dims, c.recip)
+            self.gmask = self.g2 > 1e-12
         self.nelec = c.nelec
         self.nocc = int(math.ceil(self.nelec / 2.0 - 1e-12))
         self.nbands = max(p.nbands, self.nocc)
@@ -418,20 +446,18 @@ class ScfState:
             self.rho = np.asarray(p.initial_density, dtype=np.float64).copy()
             if self.rho.size != N:
                 raise ValueError("initial_density size does not match the FFT grid")
-        # resident backends: density, potential and mixing history on the device (csrc/potential.cu)
-        self.dev = bool(getattr(backend, "resident", False))
         if self.dev:
             import torch
 
-            self.pot = backend.dz.PotentialContext(dims, self.vol, c.recip, history=max(1, p.pulay_history))
             self.rho = torch.from_numpy(self.rho).cuda()
-            self.vloc_d = torch.from_numpy(np.ascontiguousarray(self.vloc_r)).cuda()
             self.v_hxc, _ = self.pot.hxc(self.rho)
         else:
             self.v_hxc = self.hxc_g(self.rho)
         self.mixer = PulayMixer(p.pulay_history)
         self.vectors = [None] * len(self.kin)  # this rank's k-points, in kglobal order
+        t = time.perf_counter()
         self.e_ion = ewald_energy(c.cell, np.array([c.species[s].z_val for s in c.atom_species]), c.positions)
+        tm["ewald"] = time.perf_counter() - t
         self.psp_core = sum(gth_alpha(c.species[s]) for s in c.atom_species) * self.nelec / self.vol
         self.history = []
         self.energy = float("nan")

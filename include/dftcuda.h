@@ -311,6 +311,14 @@ int dftcuda_hxc_potential(dftcuda_pctx* ctx, const double* rho_r, const double* 
                           dftcuda_hxc_terms* terms);
 int dftcuda_potential_real(dftcuda_pctx* ctx, const double* v_g, const double* vloc_r, double* out_r);
 int dftcuda_pulay_mix(dftcuda_pctx* ctx, double* x, const double* residual, size_t n, double beta);
+/* build_ionic_potential_grid (scf/potential.zig:279-318) for pseudopotentials with the analytic
+ * Goedecker-Teter-Hutter local part: V(G) = (2/vol) sum_atoms ff_s(|G|) e^{-iG.tau} for
+ * 1e-12 < G^2 <= g2max (g2max <= 0: no cut), ff the GTH local form factor (Hartree) of species s with
+ * gth[6 s .. 6 s + 5] = Z_ion, r_loc, C1, C2, C3, C4.  atom_species[natoms] in 0..nspecies-1 (at most
+ * 8 species), positions[natoms*3] Cartesian bohr.  Writes V(G) to v_out_g (N complex) and/or
+ * V_loc(r) = sum_G V(G) e^{iGr} to vloc_r (N doubles); either may be NULL. */
+int dftcuda_ionic_potential(dftcuda_pctx* ctx, int nspecies, const double* gth, int natoms, const int* atom_species,
+                            const double* positions, double g2max, double* v_out_g, double* vloc_r);
 int dftcuda_pulay_reset(dftcuda_pctx* ctx);
 
 /* ------------------------------------------------------------------------------------------

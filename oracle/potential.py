@@ -171,3 +171,31 @@ class Pulay:
         for i in range(m - first):
             out += c[i] * (self.xs[first + i] + beta * self.rs[first + i])
         return out
+
+
+def ionic_potential(gth, atom_species, positions, dims, recip, volume, g2max=0.0):
+    """build_ionic_potential_grid (scf/potential.zig:279-318) with the analytic Goedecker-Teter-Hutter
+    local form factor (Hartree, x2 for Ry): V(G) = (2/vol) sum_a ff_s(|G|) e^{-iG.tau_a} for
+    1e-12 < G^2 <= g2max (no cut for g2max <= 0).  gth[s] = (Z, r_loc, C1, C2, C3, C4).
+    Returns (V(G), V_loc(r))."""
+    gth = np.asarray(gth, dtype=np.float64).reshape(-1, 6)
+    f = [np.fft.fftfreq(n, 1.0 / n) for n in dims]
+    hz, hy, hx = np.meshgrid(f[2], f[1], f[0], indexing="ij")
+    gv = np.stack([hx.ravel(), hy.ravel(), hz.ravel()], axis=1) @ np.asarray(recip, dtype=np.float64)
+    g2 = (gv * gv).sum(axis=1)
+    keep = g2 > 1e-12
+    if g2max > 0.0:
+        keep &= g2 <= g2max
+    safe = np.where(keep, g2, 1.0)
+    vg = np.zeros(g2.size, complex)
+    pos = np.asarray(positions, dtype=np.float64).reshape(-1, 3)
+    for s, (Z, r, c1, c2, c3, c4) in enumerate(gth):
+        y = safe * r * r
+        e = np.exp(-0.5 * y)
+        poly = c1 + c2 * (3 - y) + c3 * (15 - 10 * y + y * y) + c4 * (105 - 105 * y + 21 * y * y - y ** 3)
+        ff = -4 * math.pi * Z / safe * e + math.sqrt(8 * math.pi ** 3) * r ** 3 * e * poly
+        sf = np.zeros(g2.size, complex)
+        for a in np.where(np.asarray(atom_species) == s)[0]:
+            sf += np.exp(-1j * (gv @ pos[a]))
+        vg += np.where(keep, sf * 2.0 * ff / volume, 0.0)
+    return vg, to_r(vg, dims)

@@ -104,3 +104,27 @@ def test_pulay_mix_rejects_missing_history(dz):
             pc.pulay_mix(np.zeros(8), np.zeros(8), 0.5)
     finally:
         pc.close()
+
+
+def test_ionic_potential_matches_oracle(dz):
+    """Two species with all four GTH coefficients, 37 atoms in a triclinic cell, an odd box, with and
+    without the |G|^2 cut; V(G) and V_loc(r) to host and device buffers."""
+    dims = (27, 24, 25)
+    rng = np.random.default_rng(11)
+    cell = np.linalg.inv(RECIP).T * 2 * math.pi
+    pos = rng.random((37, 3)) @ cell
+    sp = rng.integers(0, 2, 37).astype(np.int32)
+    gth = [[4.0, 0.44, -7.3, 1.1, -0.2, 0.03], [3.0, 0.5, -6.0, 0.0, 0.4, 0.0]]
+    pc = dz.PotentialContext(dims, VOL, RECIP, history=1)
+    try:
+        for g2max in (0.0, 30.0):
+            ref_g, ref_r = op.ionic_potential(gth, sp, pos, dims, RECIP, VOL, g2max)
+            vg, vr = pc.ionic(gth, sp, pos, g2max)
+            assert np.abs(vg - ref_g).max() < 1e-12 * np.abs(ref_g).max()
+            assert np.abs(vr - ref_r).max() < 1e-11 * np.abs(ref_r).max()
+            vgd, vrd = pc.ionic(gth, sp, pos, g2max, device=True)
+            assert vrd.is_cuda and np.abs(vrd.cpu().numpy() - ref_r).max() < 1e-11 * np.abs(ref_r).max()
+        with pytest.raises(dz.DftCudaError):
+            pc.ionic(gth, np.array([0, 2], dtype=np.int32), pos[:2])
+    finally:
+        pc.close()

@@ -79,3 +79,16 @@ def test_pulay_oracle_matches_driver_and_the_scaled_solve_is_scale_free():
     big[:2, :2] *= 1e14
     np.testing.assert_allclose(op.solve_pulay_system(B, rhs, scaled=True)[:2], op.solve_pulay_system(big, rhs)[:2], rtol=1e-12)
     np.testing.assert_allclose(op.solve_pulay_system(B, rhs, scaled=True)[:2], [0.25, 0.75], rtol=1e-12)
+
+
+def test_ionic_potential_oracle_matches_the_input_builder():
+    """The oracle's GTH ionic potential equals the host input builder's V_loc(r) for the synthetic
+    species (C3 = C4 = 0), with the builder's |G|^2 <= 4 ecut cut."""
+    system = importlib.import_module("dftzig_b200.system")
+    c = system.crystal("si8")
+    ecut = 10.0
+    dims = system.fft_box(ecut, c.recip)
+    gth = [[sp.params["z"], sp.params["rloc"], sp.params["c1"], sp.params["c2"], 0.0, 0.0] for sp in c.species]
+    _, vr = op.ionic_potential(gth, c.atom_species, c.positions, dims, c.recip, c.volume, 4 * ecut)
+    ref = system.local_potential(c, dims, ecut)
+    assert np.abs(vr - ref).max() < 1e-11 * np.abs(ref).max()

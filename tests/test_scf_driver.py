@@ -42,6 +42,15 @@ def test_ewald_independent_of_split():
     assert abs(e1 - e2) < 1e-9 * abs(e1)
 
 
+def test_ewald_split_parameter_does_not_change_the_energy():
+    """The Ewald energy for three split parameters (the default grows with the atom density)."""
+    c = system.crystal("si64")
+    z = np.array([4.0] * len(c.atom_species))
+    e0 = scf.ewald_energy(c.cell, z, c.positions)
+    for eta in (0.12, 0.3):
+        assert abs(scf.ewald_energy(c.cell, z, c.positions, eta=eta) - e0) < 1e-10 * abs(e0)
+
+
 def test_pulay_mixer_solves_linear_fixed_point():
     rng = np.random.default_rng(0)
     A = rng.normal(size=(6, 6)) * 0.1
