@@ -271,6 +271,7 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
       const int i0 = sidx * chunk, i1 = min(n1, i0 + chunk);
       const double2* ac = A + (long)r * m + 1;
       double sx = 0.0, sy = 0.0;
+#pragma unroll 4
       for (int i = i0 + lane; i < i1; i += 32) {
         const double2 a = __ldcg(ac + i), v = sv[i];
         sx += a.x * v.x + a.y * v.y;  // conj(a) v
@@ -292,6 +293,7 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
       double2 p2 = make_double2(0.0, 0.0);
       for (int i = tid; i < n1; i += HT_THREADS) {
         double2 acc = make_double2(0.0, 0.0);
+#pragma unroll 8
         for (int q = 0; q < S_prev; ++q) acc = cadd(acc, __ldcg(yk + (long)q * m + k + 1 + i));
         const double2 yi = cmul(t, acc), vi = sv[i];
         sw[i] = yi;
@@ -346,6 +348,7 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
         const double2 wr = cconj(sw[c]), vr = cconj(sv[c]);
         double2* ac = A + (long)r * m + (k + 1);
         double sx = 0.0, sy = 0.0;
+#pragma unroll 4
         for (int i = i0 + lane; i < i1; i += 32) {
           double2 a = __ldcg(ac + i);
           a = csub(a, cadd(cmul(sv[i], wr), cmul(sw[i], vr)));
@@ -771,8 +774,13 @@ int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde,
   if (m > 1) {
     GridBarrier bar{w.bar, w.bar + 1, status, 0};
     // enough warps for kHtMaxSplit per column at the start, at most one block per SM
+    // (DFTCUDA_HETRD_BPS=2 allows two where they fit, for measurements)
+    static const int bps = [] {
+      const char* e = std::getenv("DFTCUDA_HETRD_BPS");
+      return e && std::atoi(e) == 2 ? 2 : 1;
+    }();
     const int want = (m * kHtMaxSplit + HT_WARPS - 1) / HT_WARPS;
-    bar.nblocks = (unsigned)std::max(1, std::min(want, n_sm * std::min(per_sm, 1)));
+    bar.nblocks = (unsigned)std::max(1, std::min(want, n_sm * std::min(per_sm, bps)));
     double2* a_ = A;
     int m_ = m;
     double* d_ = w.d;
