@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--eig-iters", type=int, default=6, help="Davidson iterations of --workload eig")
     ap.add_argument("--eig-cell", choices=("si64", "si216"), default="si64", help="cell of --workload eig")
     ap.add_argument("--cells", type=int, default=16, help="cells of the many-cell workload")
+    ap.add_argument("--switch-drho", type=float, default=1.5e-5,
+                    help="density residual at which the Si216 learned+mixed run switches to FP64 (its TF32X3 "
+                         "residuals track the FP64 run's to 1e-5; the stall rule still switches earlier on a floor)")
     ap.add_argument("--precision", choices=("fp64", "fp32", "tf32"), default="fp64",
                     help="context precision of --profile-case (tf32 = TF32 GEMMs) and --workload eig (tf32 = TF32X3)")
     return ap.parse_args()
@@ -546,7 +549,7 @@ def run_scf216_workload(args):
         p = scf.ScfParams(**base, convergence=1e-12, energy_target=ref.energy, energy_tol_per_atom=1e-6)
         torch.cuda.synchronize()
         # resident: eigenvectors, density, potential and Pulay history stay on the device
-        b = scf.GpuBackend(dz, prec, precond=pc, resident=True)
+        b = scf.GpuBackend(dz, prec, precond=pc, resident=True, switch_drho=args.switch_drho)
         r = scf.run_scf(c, p, b)
         torch.cuda.synchronize()
         b.close()
@@ -567,6 +570,7 @@ def run_scf216_workload(args):
         "dtype": "f64/f32/tf32x3",
         "data": "synthetic (seeded displacements; synthetic GTH-form Si pseudopotential)",
         "config": {"workload": "Si216 3x3x3 conventional, sigma 0.05 A (seed 3), 25 Ry, Gamma, 448 bands, fixed occupations",
+                   "switch_drho": args.switch_drho,
                    "target_energy_per_atom": ref.energy_per_atom, "target_iterations": ref.iterations, "target_seconds": round(ref.wall_s, 3)},
         "fp64": out["fp64"],
         "learned_mixed": out["learned_mixed"],
