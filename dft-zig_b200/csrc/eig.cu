@@ -393,41 +393,52 @@ __global__ void __launch_bounds__(1024) k_chol_panel(const double2* __restrict__
 
 // Z (k x k columns, ld k): column b < kk solves R_kept z = e_b on the kept rows (rows of dropped
 // columns zero), so Q Z has orthonormal columns; columns b >= kk are zeroed.  One warp per column,
-// the back substitution's dot products split over the lanes.
-__global__ void k_chol_inv(const double2* __restrict__ A, int k, const int* __restrict__ kept, const int* __restrict__ kk_p,
-                           double2* __restrict__ Z) {
-  const int lane = threadIdx.x & 31;
-  const int b = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
-  if (b >= k) return;
+// the back substitution's dot products split over the lanes; the column being solved and the kept
+// index table live in shared memory, so each of the (up to k - 1) dependent steps waits only on
+// shared-memory and L1 latency.
+constexpr int kCiWarps = 4;
+__global__ void __launch_bounds__(kCiWarps * 32) k_chol_inv(const double2* __restrict__ A, int k, const int* __restrict__ kept,
+                                                            const int* __restrict__ kk_p, double2* __restrict__ Z) {
+  extern __shared__ __align__(16) unsigned char cism[];
+  double2* zs = reinterpret_cast<double2*>(cism);                // [kCiWarps][k]
+  int* skept = reinterpret_cast<int*>(zs + (size_t)kCiWarps * k);  // [k]
   const int kk = *kk_p;
-  double2* z = Z + (long)b * k;
+  for (int i = threadIdx.x; i < kk; i += blockDim.x) skept[i] = kept[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int b = blockIdx.x * kCiWarps + w;
+  if (b >= k) return;
+  double2* z = zs + (size_t)w * k;
   for (int i = lane; i < k; i += 32) z[i] = make_double2(0.0, 0.0);
   __syncwarp();
-  if (b >= kk) return;
-  const int kb = kept[b];
-  if (lane == 0) z[kb] = make_double2(1.0 / A[(long)kb * k + kb].x, 0.0);
-  __syncwarp();
-  for (int a = b - 1; a >= 0; --a) {
-    const int ka = kept[a];
-    const double2* ra = A + (long)ka * k;
-    double sx = 0.0, sy = 0.0;
-    for (int u = a + 1 + lane; u <= b; u += 32) {
-      const int ku = kept[u];
-      const double2 r = ra[ku], zz = z[ku];
-      sx += r.x * zz.x - r.y * zz.y;
-      sy += r.x * zz.y + r.y * zz.x;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      sx += __shfl_xor_sync(0xffffffffu, sx, o);
-      sy += __shfl_xor_sync(0xffffffffu, sy, o);
-    }
-    if (lane == 0) {
-      const double d = ra[ka].x;
-      z[ka] = make_double2(-sx / d, -sy / d);
-    }
+  if (b < kk) {
+    const int kb = skept[b];
+    if (lane == 0) z[kb] = make_double2(1.0 / A[(long)kb * k + kb].x, 0.0);
     __syncwarp();
+    for (int a = b - 1; a >= 0; --a) {
+      const int ka = skept[a];
+      const double2* ra = A + (long)ka * k;
+      double sx = 0.0, sy = 0.0;
+      for (int u = a + 1 + lane; u <= b; u += 32) {
+        const int ku = skept[u];
+        const double2 r = __ldg(ra + ku), zz = z[ku];
+        sx += r.x * zz.x - r.y * zz.y;
+        sy += r.x * zz.y + r.y * zz.x;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+      }
+      if (lane == 0) {
+        const double d = ra[ka].x;
+        z[ka] = make_double2(-sx / d, -sy / d);
+      }
+      __syncwarp();
+    }
   }
+  double2* zo = Z + (long)b * k;
+  for (int i = lane; i < k; i += 32) zo[i] = z[i];
 }
 
 
@@ -579,7 +590,16 @@ static int chol_drop(KCtxImpl* e, const double2* G, int k, double drop, int* kk_
       }
     }
   }
-  k_chol_inv<<<ceil_div(k, 8), 256, 0, s>>>(e->R, k, e->kept, kk_dev, e->Z);
+  const size_t ci_smem = sizeof(double2) * kCiWarps * (size_t)k + sizeof(int) * (size_t)k;
+  static int ci_attr_dev = -1;
+  int dev = 0;
+  DFT_CUDA_TRY(cudaGetDevice(&dev));
+  if (ci_attr_dev != dev) {  // k <= 1024: at most 68 KB
+    DFT_CUDA_TRY(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(sizeof(double2) * kCiWarps * 1024 + sizeof(int) * 1024)));
+    ci_attr_dev = dev;
+  }
+  k_chol_inv<<<ceil_div(k, kCiWarps), kCiWarps * 32, ci_smem, s>>>(e->R, k, e->kept, kk_dev, e->Z);
   count_launch();
   DFT_CUDA_TRY(cudaGetLastError());
   return DFTCUDA_OK;

@@ -623,16 +623,17 @@ def _run(st, backend) -> ScfResult:
     return st.result()
 
 
-def run_scf_many(dz, cells, p: ScfParams, precision: str = "fp64", initial_densities=None):
+def run_scf_many(dz, cells, p: ScfParams, precision: str = "fp64", initial_densities=None, resident: bool = False):
     """Independent SCF runs of many cells advanced together: each iteration, the eigensolves of
     every (cell, k-point) pair still running go through one lockstep batch
-    (dftcuda_eig_solve_batch) on their contexts' streams.  All cells need the same band count."""
+    (dftcuda_eig_solve_batch) on their contexts' streams.  All cells need the same band count.
+    resident: every cell's eigenvectors, density, potential and mixing stay on the device."""
     t0 = time.perf_counter()
     phases = {"setup": 0.0, "begin": 0.0, "eig": 0.0, "finish": 0.0}
     states = []
     for i, c in enumerate(cells):
         pi = p if initial_densities is None else ScfParams(**{**p.__dict__, "initial_density": initial_densities[i]})
-        states.append(ScfState(c, pi, GpuBackend(dz, precision)))
+        states.append(ScfState(c, pi, GpuBackend(dz, precision, resident=resident)))
     phases["setup"] = time.perf_counter() - t0
     if len({st.nbands for st in states}) != 1:
         raise ValueError("run_scf_many: the cells need the same number of bands")
@@ -657,7 +658,8 @@ def run_scf_many(dz, cells, p: ScfParams, precision: str = "fp64", initial_densi
                 ctxs += st.backend._active()
                 diags += [inp.basis.kinetic for inp in st.kin]
                 inits += iv
-            rs = dz.hermitian_eigen_decomp_iterative_batch(ctxs, diags, nb, dz.Options(max_iter=mi, tol=tol), inits)
+            rs = dz.hermitian_eigen_decomp_iterative_batch(ctxs, diags, nb, dz.Options(max_iter=mi, tol=tol), inits,
+                                                            device=resident)
             o = 0
             for st, _ in members:
                 nk = len(st.kin)
@@ -672,5 +674,10 @@ def run_scf_many(dz, cells, p: ScfParams, precision: str = "fp64", initial_densi
     for st in states:
         st.close()
         st.backend.close()
+    setup = {}
+    for st in states:
+        for k, v in st.setup_times.items():
+            setup[k] = setup.get(k, 0.0) + v
+    phases.update({f"setup_{k}": v for k, v in setup.items()})
     run_scf_many.last_phases = {k: round(v, 3) for k, v in phases.items()}
     return results, time.perf_counter() - t0

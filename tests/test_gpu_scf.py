@@ -51,12 +51,14 @@ def test_many_cell_scf_matches_single_runs(dz):
     p = scf.ScfParams(ecut=10.0, kmesh=(1, 1, 1), nbands=20, convergence=1e-8, iterative_tol=1e-9,
                       iterative_max_iter=100, warmup_steps=0, smearing=0.01, max_iter=60)
     many, _ = scf.run_scf_many(dz, cells, p)
-    for c, r in zip(cells, many):
+    many_dev, _ = scf.run_scf_many(dz, cells, p, resident=True)
+    for c, r, rd in zip(cells, many, many_dev):
         b = scf.GpuBackend(dz)
         one = scf.run_scf(c, p, b)
         b.close()
-        assert r.converged and one.converged
+        assert r.converged and one.converged and rd.converged
         assert abs(r.energy_per_atom - one.energy_per_atom) < 1e-8
+        assert abs(rd.energy_per_atom - one.energy_per_atom) < 1e-8
 
 
 @pytest.mark.parametrize("cell,kw", [
