@@ -401,7 +401,7 @@ class ScfState:
     """One cell's SCF loop (scf.zig:148-188 control flow) split around its eigensolves, so several
     cells can share one batched eigensolver call per iteration (run_scf_many)."""
 
-    def __init__(self, c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False, comm=None):
+    def __init__(self, c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False, comm=None, table_cache=None):
         self.t0 = time.perf_counter()
         self.c, self.p, self.backend, self.verbose = c, p, backend, verbose
         self.comm = comm if comm is not None else kpar.SerialComm()
@@ -416,7 +416,15 @@ class ScfState:
         self.kglobal = [k for k in range(self.nk) if self.owner[k] == self.comm.rank]
         tm = self.setup_times = {}
         t = time.perf_counter()
-        tables = [[sysm.radial_table(sp, i, p.ecut) for i in range(len(sp.betas))] for sp in c.species]
+        # radial projector tables per species (nonlocal_context.zig builds them once per species);
+        # run_scf_many shares them across its cells through table_cache
+        tc = table_cache if table_cache is not None else {}
+        tables = []
+        for sp in c.species:
+            key = (sp.name, p.ecut)
+            if key not in tc:
+                tc[key] = [sysm.radial_table(sp, i, p.ecut) for i in range(len(sp.betas))]
+            tables.append(tc[key])
         tm["radial_tables"], t = time.perf_counter() - t, time.perf_counter()
         # resident backends: density, potential and mixing history on the device (csrc/potential.cu),
         # the ionic local potential built there too
@@ -631,9 +639,10 @@ def run_scf_many(dz, cells, p: ScfParams, precision: str = "fp64", initial_densi
     t0 = time.perf_counter()
     phases = {"setup": 0.0, "begin": 0.0, "eig": 0.0, "finish": 0.0}
     states = []
+    tables = {}  # radial tables shared by the cells' species
     for i, c in enumerate(cells):
         pi = p if initial_densities is None else ScfParams(**{**p.__dict__, "initial_density": initial_densities[i]})
-        states.append(ScfState(c, pi, GpuBackend(dz, precision, resident=resident)))
+        states.append(ScfState(c, pi, GpuBackend(dz, precision, resident=resident), table_cache=tables))
     phases["setup"] = time.perf_counter() - t0
     if len({st.nbands for st in states}) != 1:
         raise ValueError("run_scf_many: the cells need the same number of bands")

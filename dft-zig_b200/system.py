@@ -210,18 +210,13 @@ def basis(recip: np.ndarray, ecut: float, k_frac) -> PwBasis:
 
 
 def _sph_jl(l: int, x: np.ndarray) -> np.ndarray:
-    out = np.empty_like(x)
     small = np.abs(x) < 1e-6
-    xs, xb = x[small], x[~small]
+    xs = np.where(small, 1.0, x)  # keeps the closed form finite where the series is used
     if l == 0:
-        out[small] = 1.0 - xs**2 / 6.0 + xs**4 / 120.0
-        out[~small] = np.sin(xb) / xb
-    elif l == 1:
-        out[small] = xs / 3.0 - xs**3 / 30.0
-        out[~small] = np.sin(xb) / (xb * xb) - np.cos(xb) / xb
-    else:
-        raise NotImplementedError("synthetic species carry l <= 1 projectors")
-    return out
+        return np.where(small, 1.0 - x**2 / 6.0 + x**4 / 120.0, np.sin(xs) / xs)
+    if l == 1:
+        return np.where(small, x / 3.0 - x**3 / 30.0, np.sin(xs) / (xs * xs) - np.cos(xs) / xs)
+    raise NotImplementedError("synthetic species carry l <= 1 projectors")
 
 
 def radial_table(sp: SpeciesData, b: int, ecut: float, npts: int = 2048) -> tuple:
