@@ -545,7 +545,7 @@ __global__ void __launch_bounds__(T2_THREADS) k_cgemm_tc2(int M, int N, int K, c
 // rotations): a 256-column tile gives every converted operand element four times the MMA work of
 // the 64-column tiles above.  Warps 0-7 are converters: each thread owns three of the slot's 768
 // core-matrix rows (A: 16 row groups x 2 k groups x 8 rows, B: 32 x 2 x 8), copies their FP64
-// elements with cp.async two K steps ahead into its own part of a shared-memory staging ring, waits
+// elements with cp.async one K step ahead into its own part of a shared-memory staging area, waits
 // for the TF32 slot to be free, writes the TF32 planes (hi and lo parts for 3xTF32) into the ring
 // as 16-byte vectors and arrives on the slot's "full" mbarrier.  Lane 0 of warp 8 waits for full slots and
 // issues one 8-deep K step per slot (12 MMAs for 3xTF32, 4 otherwise) of 128 x 256 x 8, committing
@@ -564,11 +564,13 @@ constexpr int T3_ACM = (TC_M / 8) * (T3_K / 4);   // 32 core matrices of A per s
 constexpr int T3_BCM = (T3_N / 8) * (T3_K / 4);   // 64 of B
 constexpr uint32_t T3_TMEM_COLS = 512;
 __host__ __device__ constexpr int t3_slot(bool split) { return split ? 2 * T3_SLOT : T3_SLOT; }
-__host__ __device__ constexpr int t3_stages(bool split) { return split ? 2 : 4; }
+__host__ __device__ constexpr int t3_stages(bool split) { return split ? 3 : 6; }
 // FP64 staging: each converter thread's 12 elements of a K step, element-major (element e of
 // thread t at e * 4 KB + t * 16 B, so consecutive lanes touch consecutive 16 bytes), T3_D steps
-// deep: the cp.async copies of step t + T3_D are in flight while step t converts.
-constexpr int T3_D = 2;
+// deep: the cp.async copies of step t + T3_D are in flight while step t converts.  One step of
+// lead covers the load latency (a K step takes ~2 us); the shared memory goes to a 3-slot TF32 ring
+// instead (measured: 5 % faster than 2 staging and 2 ring slots).
+constexpr int T3_D = 1;
 constexpr int T3_STG = 12 * T3_CONV_WARPS * 32 * 16;  // 48 KB
 __host__ __device__ constexpr int t3_smem(bool split) {
   return t3_stages(split) * t3_slot(split) + T3_D * T3_STG + 256;  // + barriers, TMEM slot
