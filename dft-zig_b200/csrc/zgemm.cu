@@ -1,10 +1,13 @@
 // FP64 complex GEMM over strided operands, used for the Kleinman-Bylander projections
 // (apply.zig:1143-1183, 1278-1336) and the Rayleigh-Ritz contractions V^H W and V C
 // (lobpcg/common.zig:113-143, 231-259).  B200 has no FP64 tcgen05 kind, so the FP64 path runs on
-// the FP64 FMA pipe: 64x64 output tiles per 256-thread CTA, 4x4 complex outputs per thread,
-// K staged through shared memory in slices of 16, and split-K with a deterministic second-pass
-// reduction when the output has too few tiles to fill the 148 SMs.
+// the FP64 tensor cores through mma.sync m8n8k4 .f64 (k_zgemm_dmma, the default) or on the FP64
+// FMA pipe (k_zgemm, DFTCUDA_ZGEMM=fma): 64x64 output tiles per 256-thread CTA, K staged through
+// shared memory in slices of 16 with cp.async double buffering, and split-K with a deterministic
+// second-pass reduction when the output has too few tiles to fill the 148 SMs.
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 
 #include "kctx.cuh"
 
@@ -21,8 +24,8 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
 // One BK-deep slice of A and B into shared memory with cp.async (4 x 16 B per thread each).
-template <bool AKC, bool BKC>
-__device__ __forceinline__ void zgemm_fetch(double2 (*As)[BM + 1], double2 (*Bs)[BN + 1], int M, int N, int kend, int r0,
+template <bool AKC, bool BKC, int PAD = 1>
+__device__ __forceinline__ void zgemm_fetch(double2 (*As)[BM + PAD], double2 (*Bs)[BN + PAD], int M, int N, int kend, int r0,
                                             int c0, int k0, const double2* __restrict__ A, long lda,
                                             const double2* __restrict__ B, long ldb, int tid) {
 #pragma unroll
@@ -126,6 +129,101 @@ __global__ void __launch_bounds__(256, 2) k_zgemm(int M, int N, int K, const dou
 
 static const size_t kZgemmSmem = 2 * sizeof(double2) * BK * (BM + 1) + 2 * sizeof(double2) * BK * (BN + 1);
 
+// The same contraction on the FP64 tensor cores (mma.sync m8n8k4 .f64; tcgen05 has no f64 kind):
+// one warp instruction is 256 FMAs instead of 32, which relieves the issue pressure of the FMA
+// kernel above.  Fragments of mma.m8n8k4.row.col.f64, lane = 4 g + t:
+//   A (8 x 4): A[g][t];  B (4 x 8): B[t][g];  C (8 x 8): C[g][2t], C[g][2t + 1].
+// The 8 warps tile the 64 x 64 output as 4 x 2 blocks of 16 x 32 (2 x 4 tiles of 8 x 8); a complex
+// product is four real MMAs (the negated imaginary A fragment gives -Ai Bi).  Shared memory holds
+// the slices as [k][row] complex with a row stride of 66: the 8 lanes of a 16-byte load phase
+// (g in {0,1}, t in 0..3) then fall on 8 distinct 16-byte bank groups.
+constexpr int kZmPad = 2;
+static const size_t kZgemmDmmaSmem = 2 * sizeof(double2) * BK * (BM + kZmPad) + 2 * sizeof(double2) * BK * (BN + kZmPad);
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+template <bool AKC, bool BKC, bool CJA, bool CJB>
+__global__ void __launch_bounds__(256, 2) k_zgemm_dmma(int M, int N, int K, const double2* __restrict__ A, long lda,
+                                                       const double2* __restrict__ B, long ldb, double2* __restrict__ O,
+                                                       long ldo_r, long ldo_c, double alpha, double beta, int kps,
+                                                       double2* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char zsm[];
+  double2(*As)[BK][BM + kZmPad] = reinterpret_cast<double2(*)[BK][BM + kZmPad]>(zsm);
+  double2(*Bs)[BK][BN + kZmPad] = reinterpret_cast<double2(*)[BK][BN + kZmPad]>(zsm + 2 * sizeof(double2) * BK * (BM + kZmPad));
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wr = warp >> 1, wc = warp & 1;  // warp block: rows 16 wr .., columns 32 wc ..
+  const int r0 = blockIdx.y * BM, c0 = blockIdx.x * BN;
+  const int kbeg = blockIdx.z * kps;
+  const int kend = min(K, kbeg + kps);
+  const double sa = CJA ? -1.0 : 1.0, sb = CJB ? -1.0 : 1.0;
+  double cre[2][4][2], cim[2][4][2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) cre[i][j][0] = cre[i][j][1] = cim[i][j][0] = cim[i][j][1] = 0.0;
+  if (kbeg < kend) zgemm_fetch<AKC, BKC, kZmPad>(As[0], Bs[0], M, N, kend, r0, c0, kbeg, A, lda, B, ldb, tid);
+  int buf = 0;
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
+    cp_async_wait_all();
+    __syncthreads();
+    if (k0 + BK < kend) zgemm_fetch<AKC, BKC, kZmPad>(As[buf ^ 1], Bs[buf ^ 1], M, N, kend, r0, c0, k0 + BK, A, lda, B, ldb, tid);
+#pragma unroll
+    for (int k4 = 0; k4 < BK; k4 += 4) {
+      double ar[2], ai[2], nai[2], br[4], bi[4];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const double2 v = As[buf][k4 + t][wr * 16 + i * 8 + g];
+        ar[i] = v.x;
+        ai[i] = sa * v.y;
+        nai[i] = -ai[i];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double2 v = Bs[buf][k4 + t][wc * 32 + j * 8 + g];
+        br[j] = v.x;
+        bi[j] = sb * v.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          dmma(cre[i][j][0], cre[i][j][1], ar[i], br[j]);
+          dmma(cre[i][j][0], cre[i][j][1], nai[i], bi[j]);
+          dmma(cim[i][j][0], cim[i][j][1], ar[i], bi[j]);
+          dmma(cim[i][j][0], cim[i][j][1], ai[i], br[j]);
+        }
+    }
+    buf ^= 1;
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = r0 + wr * 16 + i * 8 + g, c = c0 + wc * 32 + j * 8 + 2 * t + h;
+        if (r >= M || c >= N) continue;
+        const double2 acc = make_double2(cre[i][j][h], cim[i][j][h]);
+        if (part) {
+          part[((long)blockIdx.z * M + r) * N + c] = acc;
+        } else {
+          double2* o = O + (long)r * ldo_r + (long)c * ldo_c;
+          double2 v = make_double2(alpha * acc.x, alpha * acc.y);
+          if (beta != 0.0) {
+            const double2 old = *o;
+            v.x += beta * old.x;
+            v.y += beta * old.y;
+          }
+          *o = v;
+        }
+      }
+}
+
 __global__ void k_zgemm_reduce(int M, int N, int splits, const double2* __restrict__ part, double2* __restrict__ O,
                                long ldo_r, long ldo_c, double alpha, double beta) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -172,8 +270,30 @@ size_t zgemm_workspace_elems(int M, int N, int K) {
   return s > 1 ? (size_t)s * M * N : 0;
 }
 
+// DFTCUDA_ZGEMM=fma selects the FMA-pipe kernel (A/B measurements); the FP64 tensor-core kernel is the default.
+static bool zgemm_fma() {
+  static const bool v = [] {
+    const char* e = std::getenv("DFTCUDA_ZGEMM");
+    return e && std::string(e) == "fma";
+  }();
+  return v;
+}
+
 template <bool AKC, bool BKC, bool CJA, bool CJB>
 static void launch(const GemmArgs& g, dim3 grid, int kps, double2* part, cudaStream_t s) {
+  if (!zgemm_fma()) {
+    static int dattr = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dattr != dev) {
+      cudaFuncSetAttribute(k_zgemm_dmma<AKC, BKC, CJA, CJB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kZgemmDmmaSmem);
+      dattr = dev;
+    }
+    k_zgemm_dmma<AKC, BKC, CJA, CJB><<<grid, 256, kZgemmDmmaSmem, s>>>(g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r,
+                                                                      g.ldo_c, g.alpha, g.beta, kps, part);
+    count_launch();
+    return;
+  }
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_zgemm<AKC, BKC, CJA, CJB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kZgemmSmem);
