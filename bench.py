@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--eig-iters", type=int, default=6, help="Davidson iterations of --workload eig")
     ap.add_argument("--eig-cell", choices=("si64", "si216"), default="si64", help="cell of --workload eig")
     ap.add_argument("--cells", type=int, default=16, help="cells of the many-cell workload")
+    ap.add_argument("--xc", choices=("lda", "pbe"), default="pbe", help="functional of the Si64 time-to-SCF workload")
     ap.add_argument("--switch-drho", type=float, default=1.5e-5,
                     help="density residual at which the Si216 learned+mixed run switches to FP64 (its TF32X3 "
                          "residuals track the FP64 run's to 1e-5; the stall rule still switches earlier on a floor)")
@@ -581,10 +582,10 @@ def run_scf216_workload(args):
 
 def run_scf64_workload(args):
     """Time-to-SCF on Si64 (2x2x2 conventional, N(0, 0.02 A) displacements, seed 1), 30 Ry, 75^3,
-    2x2x2 MP (8 k), 160 bands, Fermi-Dirac 0.01 Ry, LDA-PZ, Pulay 8 / beta 0.3, the reference's
-    eigensolver defaults.  Target: a tight FP64 run (density RMS 1e-8).  Reported: wall seconds until
-    |E - E_target| < 1e-6 Ry/atom, plain FP64 and mixed (TF32X3 contexts until the density residual
-    is below 1e-4 or stalls, then FP64)."""
+    2x2x2 MP (8 k), 160 bands, Fermi-Dirac 0.01 Ry, PBE (--xc lda for LDA-PZ), Pulay 8 / beta 0.3,
+    the reference's eigensolver defaults, the resident driver.  Target: a tight FP64 run (density
+    RMS 1e-8).  Reported: wall seconds until |E - E_target| < 1e-6 Ry/atom, plain FP64 and mixed
+    (TF32X3 contexts until the density residual is below 1e-4 or stalls, then FP64)."""
     import importlib
 
     import torch
@@ -595,15 +596,15 @@ def run_scf64_workload(args):
     scf = importlib.import_module("dftzig_b200.scf")
     system = importlib.import_module("dftzig_b200.system")
     c = system.crystal("si64", 1)
-    base = dict(ecut=30.0, kmesh=(2, 2, 2), nbands=160, mixing_beta=0.3, pulay_history=8, max_iter=60, smearing=0.01)
-    b = scf.GpuBackend(dz, "fp64")
+    base = dict(ecut=30.0, kmesh=(2, 2, 2), nbands=160, mixing_beta=0.3, pulay_history=8, max_iter=60, smearing=0.01, xc=args.xc)
+    b = scf.GpuBackend(dz, "fp64", resident=True)
     ref = scf.run_scf(c, scf.ScfParams(**base, convergence=1e-8), b)
     b.close()
     out = {}
     for mode in ("fp64", "mixed"):
         p = scf.ScfParams(**base, convergence=1e-12, energy_target=ref.energy, energy_tol_per_atom=1e-6)
         torch.cuda.synchronize()
-        b = scf.GpuBackend(dz, mode)
+        b = scf.GpuBackend(dz, mode, resident=True)
         r = scf.run_scf(c, p, b)
         torch.cuda.synchronize()
         b.close()
@@ -619,7 +620,7 @@ def run_scf64_workload(args):
         "steps": 1,
         "dtype": "f64/f32/tf32x3",
         "data": "synthetic (seeded displacements; synthetic GTH-form Si pseudopotential)",
-        "config": {"workload": "Si64 2x2x2 conventional, sigma 0.02 A (seed 1), 30 Ry, 75^3, 2x2x2 MP (8 k), 160 bands, FD 0.01 Ry",
+        "config": {"workload": f"Si64 2x2x2 conventional, sigma 0.02 A (seed 1), 30 Ry, 75^3, 2x2x2 MP (8 k), 160 bands, FD 0.01 Ry, {args.xc.upper()}",
                    "target_energy_per_atom": ref.energy_per_atom, "target_iterations": ref.iterations},
         "fp64": {"seconds": round(out["fp64"][0], 3), "scf_iterations": out["fp64"][1], "dE_per_atom": out["fp64"][2]},
         "mixed": {"seconds": round(out["mixed"][0], 3), "scf_iterations": out["mixed"][1], "dE_per_atom": out["mixed"][2],

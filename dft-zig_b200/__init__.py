@@ -69,6 +69,7 @@ ABI_SYMBOLS = (
     "dftcuda_pulay_mix",
     "dftcuda_pulay_reset",
     "dftcuda_ionic_potential",
+    "dftcuda_pctx_set_functional",
 )
 
 PRECOND_REFERENCE = 0  # r / (|k+G|^2 - lambda), lobpcg/common.zig:214-226
@@ -236,6 +237,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.dftcuda_pulay_mix.argtypes = [vp, dp, dp, sz, ct.c_double]
     lib.dftcuda_pulay_reset.argtypes = [vp]
     lib.dftcuda_ionic_potential.argtypes = [vp, ip, vp, ip, vp, vp, ct.c_double, dp, dp]
+    lib.dftcuda_pctx_set_functional.argtypes = [vp, ip]
     lb = ct.c_long
     lib.dftcuda_complex_gemm.argtypes = [ip, sz, sz, sz, vp, lb, ip, ip, vp, lb, ip, ip, vp, lb, lb, ct.c_double, ct.c_double]
     _lib = lib
@@ -603,7 +605,9 @@ class PotentialContext:
     history length.  Arrays may be numpy (host) or CUDA torch tensors; results come back in the
     kind given (numpy in -> numpy out)."""
 
-    def __init__(self, dims, volume: float, recip, history: int = 8):
+    FUNCTIONALS = {"lda": 0, "pbe": 1}
+
+    def __init__(self, dims, volume: float, recip, history: int = 8, functional: str = "lda"):
         lib = load_library()
         _require_device()
         self.dims = tuple(int(d) for d in dims)
@@ -612,6 +616,9 @@ class PotentialContext:
         h = ct.c_void_p()
         _check(lib.dftcuda_pctx_create(ct.byref(h), *self.dims, float(volume), r.ctypes.data, int(history)))
         self._h = h
+        if functional not in self.FUNCTIONALS:
+            raise InvalidArgument(f"functional must be one of {sorted(self.FUNCTIONALS)}")
+        _check(lib.dftcuda_pctx_set_functional(self._h, self.FUNCTIONALS[functional]))
 
     def _out_like(self, ref, shape, dtype):
         if _is_torch_cuda(ref):

@@ -4,8 +4,9 @@
 //
 //   dftcuda_hxc_potential   build_potential_grid (scf/potential.zig:144-203): FFT of rho, Hartree
 //                           8 pi rho(G)/G^2 (hartree_potential_at_g, potential.zig:34-44), LDA-PZ
-//                           f and V_xc (xc/xc.zig:195-211, 344-384) and the FFT of V_xc; energy
-//                           terms of scf/energy.zig:372-396 from the same passes
+//                           (xc/xc.zig:195-211, 344-384) or PBE (xc.zig:213-342 with the gradient
+//                           assembly of scf/xc_fields.zig:108-142, 306-375) f and V_xc and the FFT
+//                           of V_xc; energy terms of scf/energy.zig:372-396 from the same passes
 //   dftcuda_potential_real  V(r) = V_loc(r) + FFT^-1 V(G) (build_local_potential_real,
 //                           potential.zig:320-334)
 //   dftcuda_ionic_potential V_ion(G) and V_loc(r) (build_ionic_potential_grid, potential.zig:279-318)
@@ -209,6 +210,135 @@ __global__ void __launch_bounds__(kPotThreads) k_pot_ionic(const double* __restr
   out[i] = v;
 }
 
+// ---- PBE (generalised-gradient) exchange-correlation -------------------------------------------
+// Point functional of xc/xc.zig:213-342 (pbe, pbe_exchange, pbe_correlation, pw92_correlation), in
+// Ry: f per volume, df/dn and df/dg2 with g2 = |grad n|^2; all zero for n <= 1e-12.
+__device__ void pbe_point(double n, double g2, double& f, double& vn, double& vg) {
+  if (n <= 1e-12) {
+    f = vn = vg = 0.0;
+    return;
+  }
+  // exchange
+  const double mu = 0.2195149727645171, kappa = 0.804;
+  const double c_x = -0.75 * pow(3.0 / kPi, 1.0 / 3.0);
+  const double n13 = pow(n, 1.0 / 3.0);
+  const double ex0 = n * c_x * n13;
+  const double kf = pow(3.0 * kPi * kPi * n, 1.0 / 3.0);
+  const double den_x = 4.0 * kf * kf * n * n;
+  const double s2 = (g2 > 0.0 && den_x > 0.0) ? g2 / den_x : 0.0;
+  const double t = 1.0 + mu * s2 / kappa;
+  const double fx = 1.0 + kappa - kappa / t;
+  const double dfs = mu / (t * t);
+  const double ex_dn = 4.0 / 3.0 * c_x * n13 * fx + ex0 * dfs * (-8.0 / 3.0 * s2 / n);
+  const double ex_dg = ex0 * dfs * (den_x > 0.0 ? 1.0 / den_x : 0.0);
+  // correlation: PW92 local part and the PBE gradient term H
+  const double beta = 0.06672455060314922, gamma = 0.031090690869654895;
+  const double rs = pow(3.0 / (4.0 * kPi * n), 1.0 / 3.0);
+  double eps_c = 0.0, deps_drs = 0.0;
+  if (rs > 1e-12) {
+    const double a = 0.031091, a1 = 0.21370, b1 = 7.5957, b2 = 3.5876, b3 = 1.6382, b4 = 0.49294;
+    const double sq = sqrt(rs);
+    const double ff = b1 * sq + b2 * rs + b3 * rs * sq + b4 * rs * rs;
+    const double gg = 1.0 + 1.0 / (2.0 * a * ff);
+    const double lg = log(gg);
+    eps_c = -2.0 * a * (1.0 + a1 * rs) * lg;
+    const double dfr = 0.5 * b1 / sq + b2 + 1.5 * b3 * sq + 2.0 * b4 * rs;
+    const double dlg = -(1.0 / (2.0 * a * ff * ff * gg)) * dfr;
+    deps_drs = -2.0 * a * (a1 * lg + (1.0 + a1 * rs) * dlg);
+  }
+  const double v_c = eps_c - (rs / 3.0) * deps_drs;
+  const double deps_dn = deps_drs * (-rs / (3.0 * n));
+  const double ks2 = 4.0 * kf / kPi;
+  const double den_c = 4.0 * ks2 * n * n;
+  const double t2 = (g2 > 0.0 && den_c > 0.0) ? g2 / den_c : 0.0;
+  const double bg = beta / gamma;
+  const double x = bg * t2;
+  const double u = exp(-eps_c / gamma);
+  const double um = u - 1.0;
+  const bool big = fabs(um) > 1e-12;
+  const double A = big ? bg / um : 0.0;
+  const double y = A * t2;
+  const double d2 = 1.0 + y + y * y;
+  const double q = (1.0 + y) / d2;
+  const double arg = 1.0 + x * q;
+  const double H = arg > 0.0 ? gamma * log(arg) : 0.0;
+  const double d2s = d2 * d2;
+  const double dq_dt2 = -A * y * (2.0 + y) / d2s;
+  const double darg = bg * q + x * dq_dt2;
+  const double dH_dt2 = arg > 0.0 ? gamma * darg / arg : 0.0;
+  const double dH_dA = arg > 0.0 ? -gamma * x * t2 * y * (2.0 + y) / (arg * d2s) : 0.0;
+  const double dA_dn = big ? bg * u / (gamma * um * um) * deps_dn : 0.0;
+  const double dH_dn = dH_dt2 * (-7.0 / 3.0 * t2 / n) + dH_dA * dA_dn;
+  const double dH_dg = dH_dt2 * (den_c > 0.0 ? 1.0 / den_c : 0.0);
+  f = 2.0 * (ex0 * fx + n * (eps_c + H));
+  vn = 2.0 * (ex_dn + v_c + H + n * dH_dn);
+  vg = 2.0 * (ex_dg + n * dH_dg);
+}
+
+struct Recip9 {
+  double b[9];  // rows b1, b2, b3
+};
+
+// Cartesian component d of the G vector of box point i (FFT order, x fastest).
+__device__ __forceinline__ double pot_gcomp(long i, int nx, int ny, int nz, const Recip9& r, int d) {
+  const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long)nx * ny));
+  const double h = x < (nx + 1) / 2 ? x : x - nx;
+  const double k = y < (ny + 1) / 2 ? y : y - ny;
+  const double l = z < (nz + 1) / 2 ? z : z - nz;
+  return h * r.b[d] + k * r.b[3 + d] + l * r.b[6 + d];
+}
+
+__global__ void k_pot_to_complex(const double* __restrict__ x, long N, double2* __restrict__ out) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+    out[i] = make_double2(x[i], 0.0);
+}
+
+// out (=, or += when accumulate) i G_d in (gradient_from_real / divergence_from_real in G space).
+__global__ void k_pot_igd(const double2* __restrict__ in, int nx, int ny, int nz, Recip9 r, int d, bool accumulate,
+                          double2* __restrict__ out) {
+  const long N = (long)nx * ny * nz;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const double g = pot_gcomp(i, nx, ny, nz, r, d);
+    const double2 v = in[i];
+    double2 o = make_double2(-g * v.y, g * v.x);
+    if (accumulate) {
+      o.x += out[i].x;
+      o.y += out[i].y;
+    }
+    out[i] = o;
+  }
+}
+
+__global__ void k_pot_real_part(const double2* __restrict__ in, long N, double* __restrict__ out) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) out[i] = in[i].x;
+}
+
+// fill_gga_xc_fields (scf/xc_fields.zig:86-106): vr = df/dn, grad_d <- df/dg2 grad_d, part = sum f.
+__global__ void __launch_bounds__(kPotThreads) k_pot_pbe(const double* __restrict__ rho, long N, double* __restrict__ gx,
+                                                         double* __restrict__ gy, double* __restrict__ gz,
+                                                         double* __restrict__ vr, double* __restrict__ part) {
+  __shared__ double red[kPotThreads / 32];
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const double x = gx[i], y = gy[i], z = gz[i];
+    double f, vn, vg;
+    pbe_point(rho[i], x * x + y * y + z * z, f, vn, vg);
+    vr[i] = vn;
+    gx[i] = vg * x;
+    gy[i] = vg * y;
+    gz[i] = vg * z;
+    s += f;
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// out = (vr - 2 Re(div)) as a complex field (compute_gga_xc_fields, xc_fields.zig:137-139).
+__global__ void k_pot_gga_vxc(const double* __restrict__ vr, const double2* __restrict__ div, long N, double2* __restrict__ out) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+    out[i] = make_double2(vr[i] - 2.0 * div[i].x, 0.0);
+}
+
 // out_r = vloc + Re(v) * N (v holds FFT^-1 / N of the G-space field).
 __global__ void k_pot_real(const double2* __restrict__ v, const double* __restrict__ vloc, long N, double* __restrict__ out) {
   const double scale = (double)N;
@@ -313,6 +443,10 @@ struct dftcuda_pctx {
   double* rho = nullptr;      // N staging for host densities
   double2* vin = nullptr;     // N complex staging for host inputs
   double2* vout = nullptr;    // N complex staging for host outputs
+  int functional = DFTCUDA_XC_LDA_PZ;
+  double2* w = nullptr;       // GGA: N complex (the divergence in G space)
+  double* gr = nullptr;       // GGA: 3 N real (grad n, then df/dg2 grad n)
+  double* vr = nullptr;       // GGA: N real (df/dn, then V_xc)
   double* part = nullptr;     // kPotBlocks x max(2, history) partial sums
   double* h_part = nullptr;   // pinned host copy
   // Pulay history: `history` slots of n doubles each for inputs and residuals, plus staging
@@ -366,6 +500,8 @@ extern "C" int dftcuda_pctx_create(dftcuda_pctx** out, int nx, int ny, int nz, d
 extern "C" int dftcuda_pctx_destroy(dftcuda_pctx* c) {
   if (!c) return DFTCUDA_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (void* p : {(void*)c->w, (void*)c->gr, (void*)c->vr})
+    if (p) cudaFree(p);
   for (void* p : {(void*)c->g2, (void*)c->a, (void*)c->b, (void*)c->rho, (void*)c->vin, (void*)c->vout, (void*)c->part, (void*)c->hx,
                   (void*)c->hr, (void*)c->px, (void*)c->pr, (void*)c->d_slots, (void*)c->d_coef})
     if (p) cudaFree(p);
@@ -390,6 +526,62 @@ static int copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   return DFTCUDA_OK;
 }
 
+extern "C" int dftcuda_pctx_set_functional(dftcuda_pctx* c, int functional) {
+  if (!c || (functional != DFTCUDA_XC_LDA_PZ && functional != DFTCUDA_XC_PBE))
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "pctx_set_functional: LDA-PZ (0) or PBE (1)");
+  if (functional == DFTCUDA_XC_PBE && !c->w) {
+    const long N = c->N;
+    if (cudaMalloc(&c->w, sizeof(double2) * N) != cudaSuccess || cudaMalloc(&c->gr, sizeof(double) * 3 * N) != cudaSuccess ||
+        cudaMalloc(&c->vr, sizeof(double) * N) != cudaSuccess) {
+      for (void** p : {(void**)&c->w, (void**)&c->gr, (void**)&c->vr})
+        if (*p) {
+          cudaFree(*p);
+          *p = nullptr;
+        }
+      return fail(DFTCUDA_ERR_CUDA, "pctx_set_functional: GGA buffers");
+    }
+  }
+  c->functional = functional;
+  return DFTCUDA_OK;
+}
+
+// compute_gga_xc_fields (scf/xc_fields.zig:108-142) on the device: grad n from three inverse FFTs of
+// i G rho(G); the point functional; the divergence of df/dg2 grad n from three forward FFTs and one
+// inverse; V_xc = df/dn - 2 div back to G space in b (N V_xc(G), unnormalised).  On entry a holds
+// N rho(G); returns the sum of f over the grid.
+static int gga_vxc(dftcuda_pctx* c, const double* rho, double* exc_sum) {
+  const long N = c->N;
+  cudaStream_t s = c->stream;
+  Recip9 r;
+  for (int i = 0; i < 9; ++i) r.b[i] = c->recip[i];
+  for (int d = 0; d < 3; ++d) {
+    k_pot_igd<<<kPotBlocks, kPotThreads, 0, s>>>(c->a, c->nx, c->ny, c->nz, r, d, false, c->b);
+    count_launch();
+    DFT_TRY(fft3d_on_stream(c->plan, c->b, +1, s));
+    k_pot_real_part<<<kPotBlocks, kPotThreads, 0, s>>>(c->b, N, c->gr + (long)d * N);
+    count_launch();
+  }
+  k_pot_pbe<<<kPotBlocks, kPotThreads, 0, s>>>(rho, N, c->gr, c->gr + N, c->gr + 2 * N, c->vr, c->part);
+  count_launch();
+  DFT_CUDA_TRY(cudaMemcpyAsync(c->h_part, c->part, sizeof(double) * kPotBlocks, cudaMemcpyDeviceToHost, s));
+  for (int d = 0; d < 3; ++d) {
+    k_pot_to_complex<<<kPotBlocks, kPotThreads, 0, s>>>(c->gr + (long)d * N, N, c->b);
+    count_launch();
+    DFT_TRY(fft3d_on_stream(c->plan, c->b, -1, s));
+    k_pot_igd<<<kPotBlocks, kPotThreads, 0, s>>>(c->b, c->nx, c->ny, c->nz, r, d, d > 0, c->w);
+    count_launch();
+  }
+  DFT_TRY(fft3d_on_stream(c->plan, c->w, +1, s));  // div(r) = (1/N) sum_G i G . B(G) e^{iGr}
+  k_pot_gga_vxc<<<kPotBlocks, kPotThreads, 0, s>>>(c->vr, c->w, N, c->b);
+  count_launch();
+  DFT_TRY(fft3d_on_stream(c->plan, c->b, -1, s));
+  DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  double e = 0.0;
+  for (int i = 0; i < kPotBlocks; ++i) e += c->h_part[i];
+  *exc_sum = e;
+  return DFTCUDA_OK;
+}
+
 extern "C" int dftcuda_hxc_potential(dftcuda_pctx* c, const double* rho_r, const double* v_in_g, double* v_out_g,
                                      dftcuda_hxc_terms* terms) {
   if (!c || !rho_r || !v_out_g) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "hxc_potential: null argument");
@@ -399,14 +591,21 @@ extern "C" int dftcuda_hxc_potential(dftcuda_pctx* c, const double* rho_r, const
   const double* rho = (const double*)device_view(rho_r, c->rho, sizeof(double) * N, s, &st);
   const double2* vin = v_in_g ? (const double2*)device_view(v_in_g, c->vin, sizeof(double2) * N, s, &st) : nullptr;
   if (st != DFTCUDA_OK) return st;
-  k_pot_xc<<<kPotBlocks, kPotThreads, 0, s>>>(rho, N, c->a, c->b, c->part);
-  count_launch();
-  DFT_CUDA_TRY(cudaMemcpyAsync(c->h_part, c->part, sizeof(double) * kPotBlocks, cudaMemcpyDeviceToHost, s));
-  DFT_CUDA_TRY(cudaStreamSynchronize(s));
   double exc = 0.0;
-  for (int i = 0; i < kPotBlocks; ++i) exc += c->h_part[i];
-  DFT_TRY(fft3d_on_stream(c->plan, c->a, -1, s));
-  DFT_TRY(fft3d_on_stream(c->plan, c->b, -1, s));
+  if (c->functional == DFTCUDA_XC_PBE) {
+    k_pot_to_complex<<<kPotBlocks, kPotThreads, 0, s>>>(rho, N, c->a);
+    count_launch();
+    DFT_TRY(fft3d_on_stream(c->plan, c->a, -1, s));
+    DFT_TRY(gga_vxc(c, rho, &exc));
+  } else {
+    k_pot_xc<<<kPotBlocks, kPotThreads, 0, s>>>(rho, N, c->a, c->b, c->part);
+    count_launch();
+    DFT_CUDA_TRY(cudaMemcpyAsync(c->h_part, c->part, sizeof(double) * kPotBlocks, cudaMemcpyDeviceToHost, s));
+    DFT_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int i = 0; i < kPotBlocks; ++i) exc += c->h_part[i];
+    DFT_TRY(fft3d_on_stream(c->plan, c->a, -1, s));
+    DFT_TRY(fft3d_on_stream(c->plan, c->b, -1, s));
+  }
   double2* out = is_device_pointer(v_out_g) ? (double2*)v_out_g : c->vout;
   k_pot_hartree<<<kPotBlocks, kPotThreads, 0, s>>>(c->a, c->b, c->g2, N, vin, out, c->part);
   count_launch();

@@ -364,6 +364,7 @@ class ScfParams:
     warmup_tol: float = 1e-3
     reuse_vectors: bool = True
     smearing: Optional[float] = None  # Fermi-Dirac width (Ry); None = fixed occupations
+    xc: str = "lda"  # "lda" (LDA-PZ) or "pbe" (the resident driver's device potential)
     energy_tol_per_atom: Optional[float] = None  # stop once |E - E_target| < tol (time-to-SCF runs)
     energy_target: Optional[float] = None
     initial_density: Optional[np.ndarray] = None  # rho(r) on the FFT grid; None = flat N_e / Omega
@@ -432,12 +433,14 @@ class ScfState:
         if self.dev:
             import torch
 
-            self.pot = backend.dz.PotentialContext(dims, self.vol, c.recip, history=max(1, p.pulay_history))
+            self.pot = backend.dz.PotentialContext(dims, self.vol, c.recip, history=max(1, p.pulay_history), functional=p.xc)
             gth = [[sp.params["z"], sp.params["rloc"], sp.params.get("c1", 0.0), sp.params.get("c2", 0.0),
                     sp.params.get("c3", 0.0), sp.params.get("c4", 0.0)] for sp in c.species]
             _, self.vloc_d = self.pot.ionic(gth, c.atom_species, c.positions, 4.0 * p.ecut, device=True)
             self.vloc_r = self.vloc_d.cpu().numpy()
         else:
+            if p.xc != "lda":
+                raise ValueError("ScfParams.xc = 'pbe' needs the resident driver (GpuBackend(resident=True))")
             self.vloc_r = sysm.local_potential(c, dims, p.ecut)
         tm["local_potential"], t = time.perf_counter() - t, time.perf_counter()
         self.kin = [sysm.kpoint_inputs(c, p.ecut, kpts[k][0], dims=dims, local_r=self.vloc_r, tables=tables) for k in self.kglobal]

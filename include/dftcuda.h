@@ -307,6 +307,12 @@ typedef struct dftcuda_hxc_terms {
 int dftcuda_pctx_create(dftcuda_pctx** out, int nx, int ny, int nz, double volume, const double* recip,
                         int pulay_history);
 int dftcuda_pctx_destroy(dftcuda_pctx* ctx);
+/* Exchange-correlation functional of dftcuda_hxc_potential (xc.Functional, xc/xc.zig:5-8):
+ * DFTCUDA_XC_LDA_PZ (the default) or DFTCUDA_XC_PBE (gradient from FFTs, compute_gga_xc_fields,
+ * scf/xc_fields.zig:108-142). */
+#define DFTCUDA_XC_LDA_PZ 0
+#define DFTCUDA_XC_PBE 1
+int dftcuda_pctx_set_functional(dftcuda_pctx* ctx, int functional);
 int dftcuda_hxc_potential(dftcuda_pctx* ctx, const double* rho_r, const double* v_in_g, double* v_out_g,
                           dftcuda_hxc_terms* terms);
 int dftcuda_potential_real(dftcuda_pctx* ctx, const double* v_g, const double* vloc_r, double* out_r);

@@ -43,6 +43,103 @@ def lda_pz(n):
     return f, v
 
 
+def pw92_correlation(rs):
+    """xc/xc.zig:320-342: Perdew-Wang 92 unpolarised correlation (Hartree): eps, d eps / d rs and
+    v_c = eps - rs/3 d eps / d rs."""
+    rs = np.asarray(rs, dtype=np.float64)
+    a, a1, b1, b2, b3, b4 = 0.031091, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294
+    sq = np.sqrt(rs)
+    f = b1 * sq + b2 * rs + b3 * rs * sq + b4 * rs * rs
+    g = 1.0 + 1.0 / (2.0 * a * f)
+    lg = np.log(g)
+    eps = -2.0 * a * (1.0 + a1 * rs) * lg
+    dfr = 0.5 * b1 / sq + b2 + 1.5 * b3 * sq + 2.0 * b4 * rs
+    dlg = -(1.0 / (2.0 * a * f * f * g)) * dfr
+    deps = -2.0 * a * (a1 * lg + (1.0 + a1 * rs) * dlg)
+    return eps, deps, eps - (rs / 3.0) * deps
+
+
+def pbe(n, g2):
+    """xc/xc.zig:213-318 (pbe, pbe_exchange, pbe_correlation): f per volume, df/dn and df/d|grad n|^2,
+    in Ry; all zero for n <= 1e-12."""
+    n = np.asarray(n, dtype=np.float64)
+    g2 = np.asarray(g2, dtype=np.float64)
+    f = np.zeros_like(n)
+    vn = np.zeros_like(n)
+    vg = np.zeros_like(n)
+    m = n > 1e-12
+    nn, gg = n[m], g2[m]
+    pi = math.pi
+    # exchange
+    mu, kappa = 0.2195149727645171, 0.804
+    c_x = -0.75 * math.pow(3.0 / pi, 1.0 / 3.0)
+    n13 = np.power(nn, 1.0 / 3.0)
+    ex0 = nn * c_x * n13
+    kf = np.power(3.0 * pi * pi * nn, 1.0 / 3.0)
+    den_x = 4.0 * kf * kf * nn * nn
+    s2 = np.where((gg > 0.0) & (den_x > 0.0), gg / np.where(den_x > 0.0, den_x, 1.0), 0.0)
+    t = 1.0 + mu * s2 / kappa
+    fx = 1.0 + kappa - kappa / t
+    dfs = mu / (t * t)
+    ex_dn = 4.0 / 3.0 * c_x * n13 * fx + ex0 * dfs * (-8.0 / 3.0 * s2 / nn)
+    ex_dg = ex0 * dfs * np.where(den_x > 0.0, 1.0 / np.where(den_x > 0.0, den_x, 1.0), 0.0)
+    # correlation
+    beta, gamma = 0.06672455060314922, 0.031090690869654895
+    rs = np.power(3.0 / (4.0 * pi * nn), 1.0 / 3.0)
+    eps_c, deps_drs, v_c = pw92_correlation(rs)
+    deps_dn = deps_drs * (-rs / (3.0 * nn))
+    ks2 = 4.0 * kf / pi
+    den_c = 4.0 * ks2 * nn * nn
+    t2 = np.where((gg > 0.0) & (den_c > 0.0), gg / np.where(den_c > 0.0, den_c, 1.0), 0.0)
+    bg = beta / gamma
+    x = bg * t2
+    u = np.exp(-eps_c / gamma)
+    um = u - 1.0
+    big = np.abs(um) > 1e-12
+    A = np.where(big, bg / np.where(big, um, 1.0), 0.0)
+    y = A * t2
+    d2 = 1.0 + y + y * y
+    q = (1.0 + y) / d2
+    arg = 1.0 + x * q
+    pos = arg > 0.0
+    H = gamma * np.where(pos, np.log(np.where(pos, arg, 1.0)), 0.0)
+    d2s = d2 * d2
+    dq_dt2 = -A * y * (2.0 + y) / d2s
+    darg = bg * q + x * dq_dt2
+    safe_arg = np.where(pos, arg, 1.0)
+    dH_dt2 = np.where(pos, gamma * darg / safe_arg, 0.0)
+    dH_dA = np.where(pos, -gamma * x * t2 * y * (2.0 + y) / (safe_arg * d2s), 0.0)
+    dA_dn = np.where(big, bg * u / (gamma * np.where(big, um, 1.0) ** 2) * deps_dn, 0.0)
+    dH_dn = dH_dt2 * (-7.0 / 3.0 * t2 / nn) + dH_dA * dA_dn
+    dH_dg = dH_dt2 * np.where(den_c > 0.0, 1.0 / np.where(den_c > 0.0, den_c, 1.0), 0.0)
+    f[m] = 2.0 * (ex0 * fx + nn * (eps_c + H))
+    vn[m] = 2.0 * (ex_dn + v_c + H + nn * dH_dn)
+    vg[m] = 2.0 * (ex_dg + nn * dH_dg)
+    return f, vn, vg
+
+
+def g_vectors_cart(dims, recip):
+    """Cartesian G of every box point in FFT order (N x 3)."""
+    f = [np.fft.fftfreq(n, 1.0 / n) for n in dims]
+    hz, hy, hx = np.meshgrid(f[2], f[1], f[0], indexing="ij")
+    return np.stack([hx.ravel(), hy.ravel(), hz.ravel()], axis=1) @ np.asarray(recip, dtype=np.float64)
+
+
+def gga_xc_fields(rho, dims, recip, xc=pbe):
+    """compute_gga_xc_fields (scf/xc_fields.zig:108-142): grad n by FFT (gradient_from_real,
+    xc_fields.zig:306-339), the point functional, V_xc = df/dn - 2 div(df/dg2 grad n) with the
+    divergence by FFT (divergence_from_real, xc_fields.zig:341-375).  Returns (f, V_xc) on the grid."""
+    rho = np.asarray(rho, dtype=np.float64)
+    G = g_vectors_cart(dims, recip)
+    rg = to_g(rho, dims)
+    grad = [np.fft.ifftn((1j * G[:, d] * rg).reshape(dims[2], dims[1], dims[0])).ravel().real * rho.size for d in range(3)]
+    g2 = grad[0] ** 2 + grad[1] ** 2 + grad[2] ** 2
+    f, vn, vg = xc(rho, g2)
+    div_g = sum(1j * G[:, d] * to_g(vg * grad[d], dims) for d in range(3))
+    div = to_r(div_g, dims)
+    return f, vn - 2.0 * div
+
+
 def g2_table(dims, recip):
     """|G|^2 of every box point, G = h b1 + k b2 + l b3 with h, k, l in FFT order (gvec_iter)."""
     f = [np.fft.fftfreq(n, 1.0 / n) for n in dims]
@@ -61,17 +158,17 @@ def to_r(fg, dims):
     return np.fft.ifftn(np.asarray(fg).reshape(dims[2], dims[1], dims[0])).ravel().real * n
 
 
-def hxc_potential(rho, dims, recip, volume, v_in_g=None):
+def hxc_potential(rho, dims, recip, volume, v_in_g=None, functional="lda"):
     """build_potential_grid (scf/potential.zig:144-203) without core charge, cutoff Coulomb or an
     ecutrho filter: V(G) = 8 pi rho(G)/G^2 [G^2 > 1e-12] + V_xc(G) (hartree_potential_at_g,
-    potential.zig:34-44).  Energy terms as scf/energy.zig:372-396: E_H = (vol/2) sum 8 pi |rho(G)|^2/G^2,
+    potential.zig:34-44), V_xc of LDA-PZ or PBE (compute_xc_fields, xc_fields.zig:377-389).  Energy terms as scf/energy.zig:372-396: E_H = (vol/2) sum 8 pi |rho(G)|^2/G^2,
     E_xc = (vol/N) sum f_xc, and int v_in rho = (vol/N) sum_r v_in(r) rho(r).
     Returns (v_out_g, e_hartree, e_xc, int_vin_rho)."""
     rho = np.asarray(rho, dtype=np.float64)
     n = rho.size
     g2 = g2_table(dims, recip)
     rg = to_g(rho, dims)
-    f, vxc = lda_pz(rho)
+    f, vxc = lda_pz(rho) if functional == "lda" else gga_xc_fields(rho, dims, recip)
     m = g2 > 1e-12
     vh = np.zeros_like(rg)
     vh[m] = 8.0 * math.pi * rg[m] / g2[m]

@@ -128,3 +128,26 @@ def test_ionic_potential_matches_oracle(dz):
             pc.ionic(gth, np.array([0, 2], dtype=np.int32), pos[:2])
     finally:
         pc.close()
+
+
+@pytest.mark.parametrize("dims", [(12, 10, 9), (24, 24, 24)])
+def test_pbe_potential_matches_oracle(dz, dims):
+    """PBE through the device: gradient by three inverse FFTs, the point functional, the divergence by
+    FFTs; V_hxc(G) and the energy terms against the oracle's assembly."""
+    pc = dz.PotentialContext(dims, VOL, RECIP, history=1, functional="pbe")
+    try:
+        rng = np.random.default_rng(3)
+        N = dims[0] * dims[1] * dims[2]
+        g2 = op.g2_table(dims, RECIP)
+        rho = 0.03 + 0.01 * op.to_r(np.where(g2 < 2.0, op.to_g(rng.normal(size=N), dims), 0.0), dims)
+        v_in = op.to_g(np.cos(np.arange(N) * 0.01), dims)
+        ref, e_h, e_xc, ivr = op.hxc_potential(rho, dims, RECIP, VOL, v_in, functional="pbe")
+        v, t = pc.hxc(rho, v_in)
+        assert np.abs(v - ref).max() < 1e-11 * np.abs(ref).max()
+        assert abs(t["e_xc"] - e_xc) < 1e-11 * abs(e_xc)
+        assert abs(t["e_hartree"] - e_h) < 1e-11 * abs(e_h)
+        # the gradient term matters: PBE and LDA potentials differ
+        lda, *_ = op.hxc_potential(rho, dims, RECIP, VOL)
+        assert np.abs(ref - lda).max() > 1e-4 * np.abs(ref).max()
+    finally:
+        pc.close()

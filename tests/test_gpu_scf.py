@@ -85,3 +85,25 @@ def test_resident_scf_matches_host_driver(dz, cell, kw):
     assert np.abs(r_dev.rho - r_host.rho).max() < 1e-9 * np.abs(r_host.rho).max()
     for a, b in zip(r_dev.eigenvalues, r_host.eigenvalues):
         assert np.abs(np.asarray(a) - np.asarray(b)).max() < 1e-9
+
+
+def test_pbe_scf_converges_and_differs_from_lda(dz):
+    """Si2 with the PBE functional (device potential, resident driver) converges; its energy is
+    within the usual PBE-LDA spread and its final potential matches the oracle's PBE build."""
+    scf = importlib.import_module("dftzig_b200.scf")
+    system = importlib.import_module("dftzig_b200.system")
+    from oracle import potential as op
+    c = system.crystal("si2")
+    out = {}
+    for xc in ("lda", "pbe"):
+        p = scf.ScfParams(ecut=20.0, kmesh=(2, 2, 2), nbands=8, convergence=1e-8, iterative_max_iter=200, iterative_tol=1e-10,
+                          warmup_steps=0, max_iter=40, xc=xc)
+        b = scf.GpuBackend(dz, resident=True)
+        out[xc] = scf.run_scf(c, p, b)
+        b.close()
+        assert out[xc].converged, xc
+    d = out["pbe"].energy_per_atom - out["lda"].energy_per_atom
+    assert 1e-3 < abs(d) < 0.5, d
+    dims = system.fft_box(20.0, c.recip)
+    _, _, e_xc, _ = op.hxc_potential(out["pbe"].rho, dims, c.recip, c.volume, functional="pbe")
+    assert abs(out["pbe"].terms["xc"] - e_xc) < 1e-9 * abs(e_xc)

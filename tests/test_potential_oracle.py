@@ -92,3 +92,35 @@ def test_ionic_potential_oracle_matches_the_input_builder():
     _, vr = op.ionic_potential(gth, c.atom_species, c.positions, dims, c.recip, c.volume, 4 * ecut)
     ref = system.local_potential(c, dims, ecut)
     assert np.abs(vr - ref).max() < 1e-11 * np.abs(ref).max()
+
+
+def test_pbe_derivatives_match_finite_differences():
+    rng = np.random.default_rng(4)
+    n = 10 ** rng.uniform(-3, 0.3, 300)
+    # reduced gradients s^2 = |grad n|^2 / (4 kF^2 n^2) from 1e-2 to 10, where df/dg2 is resolvable
+    kf = (3 * math.pi ** 2 * n) ** (1.0 / 3.0)
+    g2 = 10 ** rng.uniform(-2, 1, 300) * 4 * kf ** 2 * n ** 2
+    f, vn, vg = op.pbe(n, g2)
+    hn, hg = 1e-6 * n, 1e-4 * g2
+    np.testing.assert_allclose(vn, (op.pbe(n + hn, g2)[0] - op.pbe(n - hn, g2)[0]) / (2 * hn), rtol=2e-6, atol=1e-10)
+    np.testing.assert_allclose(vg, (op.pbe(n, g2 + hg)[0] - op.pbe(n, g2 - hg)[0]) / (2 * hg), rtol=1e-6, atol=0)
+    # no gradient: PBE exchange is the LDA exchange; the correlation is PW92 rather than PZ
+    f0, v0, _ = op.pbe(n, np.zeros_like(n))
+    assert np.all(np.abs(f0 - op.lda_pz(n)[0]) < 0.05 * np.abs(f0))
+
+
+def test_gga_potential_is_the_functional_derivative():
+    """E_xc[n + e dn] - E_xc[n - e dn] = 2 e (vol/N) sum V_xc dn for the PBE assembly (gradient and
+    divergence by FFT): the sign and the factor 2 of the divergence term."""
+    rng = np.random.default_rng(6)
+    N = DIMS[0] * DIMS[1] * DIMS[2]
+    x = rng.normal(size=N)
+    rho = 0.03 + 0.01 * op.to_r(np.where(op.g2_table(DIMS, RECIP) < 2.0, op.to_g(x, DIMS), 0.0), DIMS)
+    dn = op.to_r(np.where(op.g2_table(DIMS, RECIP) < 1.5, op.to_g(rng.normal(size=N), DIMS), 0.0), DIMS)
+    f, v = op.gga_xc_fields(rho, DIMS, RECIP)
+    eps = 1e-5
+    ep = op.gga_xc_fields(rho + eps * dn, DIMS, RECIP)[0].sum()
+    em = op.gga_xc_fields(rho - eps * dn, DIMS, RECIP)[0].sum()
+    lhs = (ep - em) / (2 * eps)
+    rhs = float(np.dot(v, dn))
+    assert abs(lhs - rhs) < 1e-6 * abs(rhs)
