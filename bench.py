@@ -585,7 +585,8 @@ def run_scf64_workload(args):
     2x2x2 MP (8 k), 160 bands, Fermi-Dirac 0.01 Ry, PBE (--xc lda for LDA-PZ), Pulay 8 / beta 0.3,
     the reference's eigensolver defaults, the resident driver.  Target: a tight FP64 run (density
     RMS 1e-8).  Reported: wall seconds until |E - E_target| < 1e-6 Ry/atom, plain FP64 and mixed
-    (TF32X3 contexts until the density residual is below 1e-4 or stalls, then FP64)."""
+    (TF32X3 contexts until the density residual is below 1e-4 or stalls, then FP64), with each run's
+    largest force and eigenvalue error against the tight FP64 run."""
     import importlib
 
     import torch
@@ -598,19 +599,24 @@ def run_scf64_workload(args):
     c = system.crystal("si64", 1)
     base = dict(ecut=30.0, kmesh=(2, 2, 2), nbands=160, mixing_beta=0.3, pulay_history=8, max_iter=60, smearing=0.01, xc=args.xc)
     b = scf.GpuBackend(dz, "fp64", resident=True)
-    ref = scf.run_scf(c, scf.ScfParams(**base, convergence=1e-8), b)
+    ref = scf.run_scf(c, scf.ScfParams(**base, convergence=1e-8), b, forces=True)
     b.close()
     out = {}
+    errs = {}
     for mode in ("fp64", "mixed"):
         p = scf.ScfParams(**base, convergence=1e-12, energy_target=ref.energy, energy_tol_per_atom=1e-6)
         torch.cuda.synchronize()
         b = scf.GpuBackend(dz, mode, resident=True)
-        r = scf.run_scf(c, p, b)
+        r = scf.run_scf(c, p, b, forces=True)  # forces after the timed loop (not in wall_s)
         torch.cuda.synchronize()
         b.close()
         if not r.converged:
             raise RuntimeError(f"time-to-SCF run ({mode}) did not reach the target")
         out[mode] = (r.wall_s, r.iterations, r.energy_per_atom - ref.energy_per_atom, getattr(b, "switched_at", None))
+        nb = min(len(ref.eigenvalues[0]), len(r.eigenvalues[0]))
+        errs[mode] = {"force_error_max_ry_per_bohr": float(np.abs(r.forces - ref.forces).max()),
+                      "eigenvalue_error_max_ry": float(max(np.abs(np.asarray(a)[:nb] - np.asarray(e)[:nb]).max()
+                                                           for a, e in zip(r.eigenvalues, ref.eigenvalues)))}
     line = {
         "metric": "time-to-SCF (|dE| < 1e-6 Ry/atom vs tight FP64), Si64 30 Ry 2x2x2, mixed precision",
         "value": round(out["mixed"][0], 3),
@@ -622,9 +628,10 @@ def run_scf64_workload(args):
         "data": "synthetic (seeded displacements; synthetic GTH-form Si pseudopotential)",
         "config": {"workload": f"Si64 2x2x2 conventional, sigma 0.02 A (seed 1), 30 Ry, 75^3, 2x2x2 MP (8 k), 160 bands, FD 0.01 Ry, {args.xc.upper()}",
                    "target_energy_per_atom": ref.energy_per_atom, "target_iterations": ref.iterations},
-        "fp64": {"seconds": round(out["fp64"][0], 3), "scf_iterations": out["fp64"][1], "dE_per_atom": out["fp64"][2]},
+        "fp64": {"seconds": round(out["fp64"][0], 3), "scf_iterations": out["fp64"][1], "dE_per_atom": out["fp64"][2], **errs["fp64"]},
         "mixed": {"seconds": round(out["mixed"][0], 3), "scf_iterations": out["mixed"][1], "dE_per_atom": out["mixed"][2],
-                  "switched_to_fp64_at_iteration": out["mixed"][3]},
+                  "switched_to_fp64_at_iteration": out["mixed"][3], **errs["mixed"]},
+        "reference_max_force_ry_per_bohr": float(np.abs(ref.forces).max()),
         "speedup_mixed_vs_fp64": round(out["fp64"][0] / out["mixed"][0], 3),
     }
     print(json.dumps(line), flush=True)

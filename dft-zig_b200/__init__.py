@@ -70,6 +70,8 @@ ABI_SYMBOLS = (
     "dftcuda_pulay_reset",
     "dftcuda_ionic_potential",
     "dftcuda_pctx_set_functional",
+    "dftcuda_local_forces",
+    "dftcuda_nonlocal_forces",
 )
 
 PRECOND_REFERENCE = 0  # r / (|k+G|^2 - lambda), lobpcg/common.zig:214-226
@@ -238,6 +240,8 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.dftcuda_pulay_reset.argtypes = [vp]
     lib.dftcuda_ionic_potential.argtypes = [vp, ip, vp, ip, vp, vp, ct.c_double, dp, dp]
     lib.dftcuda_pctx_set_functional.argtypes = [vp, ip]
+    lib.dftcuda_local_forces.argtypes = [vp, ip, vp, ip, vp, vp, ct.c_double, dp, dp]
+    lib.dftcuda_nonlocal_forces.argtypes = [vp, dp, sz, sz, dp, dp]
     lb = ct.c_long
     lib.dftcuda_complex_gemm.argtypes = [ip, sz, sz, sz, vp, lb, ip, ip, vp, lb, ip, ip, vp, lb, lb, ct.c_double, ct.c_double]
     _lib = lib
@@ -419,6 +423,16 @@ class KpointContext:
             vectors = np.ascontiguousarray(vectors, dtype=np.complex128).reshape(-1, self.n)
         _check(self._lib.dftcuda_accumulate_density(self._h, _ptr(vectors), self.n, w.size, _ptr(w), _ptr(rho)))
         return rho
+
+    def nonlocal_forces(self, vectors, weights, natoms: int) -> np.ndarray:
+        """Nonlocal Hellmann-Feynman forces (natoms, 3) in Ry/bohr of the bands `vectors` (nbands, n)
+        with weights k weight x occupation x spin, for the atoms given to set_projectors."""
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        if isinstance(vectors, np.ndarray):
+            vectors = np.ascontiguousarray(vectors, dtype=np.complex128).reshape(-1, self.n)
+        out = np.zeros((natoms, 3))
+        _check(self._lib.dftcuda_nonlocal_forces(self._h, _ptr(vectors), self.n, w.size, w.ctypes.data, out.ctypes.data))
+        return out
 
     def accumulate_band_density_noalloc(self, vectors_dev, weights_dev, rho_dev, nbands=None):
         """Same result as accumulate_band_density for device tensors, without any device allocation
@@ -656,6 +670,17 @@ class PotentialContext:
 
     def reset(self):
         _check(load_library().dftcuda_pulay_reset(self._h))
+
+    def local_forces(self, gth, atom_species, positions, rho, g2max: float = 0.0) -> np.ndarray:
+        """Local-pseudopotential forces (natoms, 3) in Ry/bohr from the density rho (numpy or CUDA)."""
+        g = np.ascontiguousarray(np.asarray(gth, dtype=np.float64).reshape(-1, 6))
+        sp = np.ascontiguousarray(atom_species, dtype=np.int32)
+        pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1, 3))
+        rho = _as_array(rho, np.float64, self.N)
+        out = np.empty((sp.size, 3))
+        _check(load_library().dftcuda_local_forces(self._h, g.shape[0], g.ctypes.data, sp.size, sp.ctypes.data, pos.ctypes.data,
+                                                   float(g2max), _ptr(rho), out.ctypes.data))
+        return out
 
     def ionic(self, gth, atom_species, positions, g2max: float = 0.0, device: bool = False):
         """V_loc(r) of GTH-local pseudopotentials: gth (nspecies, 6) = Z, r_loc, C1..C4; atoms by

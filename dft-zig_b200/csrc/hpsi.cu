@@ -624,6 +624,9 @@ extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const d
   if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_projectors: null context");
   cudaStreamSynchronize(c->stream);
   free_nonlocal(c);
+  c->natoms = 0;
+  c->atom_row.clear();
+  c->atom_mt.clear();
   if (n_species == 0 || n_atoms == 0) return DFTCUDA_OK;
   if (!species || !atom_species || !atom_pos) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_projectors: null array");
   // Projector order follows apply.zig:1454-1482: species in order, then that species' atoms in order.
@@ -655,6 +658,9 @@ extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const d
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_projectors: projector matrix");
   }
   double* dphi = nullptr;
+  c->natoms = (int)n_atoms;
+  c->atom_row.assign(n_atoms, 0);
+  c->atom_mt.assign(n_atoms, 0);
   int p = 0;
   for (size_t s = 0; s < n_species; ++s) {
     const dftcuda_species& sp = species[s];
@@ -678,6 +684,8 @@ extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const d
     cudaMemcpyAsync(dphi, sp.phi, sizeof(double) * (size_t)mt * c->npw, cudaMemcpyHostToDevice, c->stream);
     for (size_t a = 0; a < n_atoms; ++a) {
       if ((size_t)atom_species[a] != s) continue;
+      c->atom_row[a] = p;
+      c->atom_mt[a] = mt;
       k_build_projectors<<<ceil_div(c->npw, 256), 256, 0, c->stream>>>(nl.P + (size_t)p * c->npw, dphi, mt, (long)c->npw,
                                                                       c->d_gcart, atom_pos[3 * a], atom_pos[3 * a + 1],
                                                                       atom_pos[3 * a + 2]); count_launch();
@@ -773,6 +781,111 @@ extern "C" int dftcuda_nonlocal_energies(dftcuda_kctx* c, const double* psi, siz
   if (!de) DFT_CUDA_TRY(cudaMemcpyAsync(e_out, ed, sizeof(double) * nbands, cudaMemcpyDeviceToHost, c->stream));
   DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return DFTCUDA_OK;
+}
+
+// y[c][g] = (k + G)_d x[c][g]: the band times one Cartesian component of k + G.
+__global__ void k_scale_kpg(const double2* __restrict__ x, const double* __restrict__ gcart, int d, long npw, long ncols,
+                            double2* __restrict__ y) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < npw * ncols; i += (long)gridDim.x * blockDim.x) {
+    const double q = gcart[3 * (i % npw) + d];
+    y[i] = make_double2(q * x[i].x, q * x[i].y);
+  }
+}
+
+// F[3 a + d] += scale sum_{p of atom a} sum_c w[c] Im(conj(Dp[p][c]) t[p][c]), one block per atom
+// (rows row0[a] .. row0[a] + mt[a] - 1).
+__global__ void k_nl_force(const double2* __restrict__ t, const double2* __restrict__ dp, const double* __restrict__ w,
+                           const int* __restrict__ row0, const int* __restrict__ mt, int ncols, int d, double scale,
+                           double* __restrict__ F) {
+  const int a = blockIdx.x;
+  const int p0 = row0[a], p1 = row0[a] + mt[a];
+  double sum = 0.0;
+  for (long i = threadIdx.x; i < (long)(p1 - p0) * ncols; i += blockDim.x) {
+    const long idx = (long)p0 * ncols + i;
+    const int c = (int)(idx % ncols);
+    const double2 x = dp[idx], y = t[idx];
+    sum += w[c] * (x.x * y.y - x.y * y.x);
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = sum;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) F[3 * a + d] += scale * red[0];
+}
+
+// Nonlocal Hellmann-Feynman forces of the context's atoms (accumulate_atom_force_at_kpoint,
+// forces/nonlocal_force.zig:283-341): with p = P psi (projector rows e^{+i(k+G).tau} phi), Dp = D p
+// and t_d = P ((k+G)_d psi), F[a][d] = (2 / Omega) sum_b w_b Im sum_{j of atom a} conj(Dp_jb) t_jbd.
+// Three more projection GEMMs than the nonlocal energy, in the context's precision.
+extern "C" int dftcuda_nonlocal_forces(dftcuda_kctx* c, const double* vectors, size_t n, size_t nbands, const double* weights,
+                                       double* forces) {
+  if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_forces: null context");
+  if (n != c->npw) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "nonlocal_forces: n != n_pw");
+  if (!forces || (nbands && (!vectors || !weights))) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_forces: null buffer");
+  const int nproj = c->nl.nproj;
+  const int natoms = c->natoms;
+  std::vector<double> hf(3 * (size_t)natoms, 0.0);
+  if (nproj == 0 || nbands == 0 || natoms == 0) {
+    if (natoms > 0) {
+      if (is_device_pointer(forces)) DFT_CUDA_TRY(cudaMemset(forces, 0, sizeof(double) * 3 * natoms));
+      else std::memcpy(forces, hf.data(), sizeof(double) * 3 * natoms);
+    }
+    return DFTCUDA_OK;
+  }
+  cudaStream_t s = c->stream;
+  const size_t nch = std::min<size_t>(nbands, 256);
+  DFT_TRY(kctx_stage(c, nch));
+  DFT_TRY(kctx_ensure_coef(c, nch));
+  int* d_row = nullptr;
+  double* d_w = nullptr;
+  double* d_F = nullptr;
+  auto cleanup = [&] {
+    if (d_row) cudaFree(d_row);
+    if (d_w) cudaFree(d_w);
+    if (d_F) cudaFree(d_F);
+  };
+  if (cudaMalloc(&d_row, sizeof(int) * 2 * (size_t)natoms) != cudaSuccess || cudaMalloc(&d_w, sizeof(double) * nbands) != cudaSuccess ||
+      cudaMalloc(&d_F, sizeof(double) * 3 * (size_t)natoms) != cudaSuccess) {
+    cleanup();
+    return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "nonlocal_forces: buffers");
+  }
+  int st = DFTCUDA_OK;
+  auto run = [&]() -> int {
+    DFT_CUDA_TRY(cudaMemcpyAsync(d_row, c->atom_row.data(), sizeof(int) * natoms, cudaMemcpyHostToDevice, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(d_row + natoms, c->atom_mt.data(), sizeof(int) * natoms, cudaMemcpyHostToDevice, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(d_w, weights, sizeof(double) * nbands, cudaMemcpyDefault, s));
+    DFT_CUDA_TRY(cudaMemsetAsync(d_F, 0, sizeof(double) * 3 * natoms, s));
+    const bool dv = is_device_pointer(vectors);
+    for (size_t c0 = 0; c0 < nbands; c0 += nch) {
+      const size_t nc = std::min(nch, nbands - c0);
+      const double2* x = (const double2*)vectors + c0 * n;
+      if (!dv) {
+        DFT_CUDA_TRY(cudaMemcpyAsync(c->d_x, x, sizeof(double2) * n * nc, cudaMemcpyHostToDevice, s));
+        x = c->d_x;
+      }
+      DFT_TRY(kctx_project(c, x, nc, s));
+      const long tot = (long)nproj * nc;
+      k_apply_dij<<<ceil_div(tot, 256), 256, 0, s>>>(c->d_coef, c->d_coef2, c->nl.D, c->nl.proj_off, c->nl.proj_mt, c->nl.maxm,
+                                                   nproj, (int)nc); count_launch();
+      for (int d = 0; d < 3; ++d) {
+        k_scale_kpg<<<ceil_div((long)n * nc, 256), 256, 0, s>>>(x, c->d_gcart, d, (long)n, (long)nc, c->d_y); count_launch();
+        DFT_TRY(kctx_project(c, c->d_y, nc, s));
+        k_nl_force<<<natoms, 256, 0, s>>>(c->d_coef, c->d_coef2, d_w + c0, d_row, d_row + natoms, (int)nc, d, 2.0 / c->volume, d_F);
+        count_launch();
+      }
+    }
+    DFT_CUDA_TRY(cudaMemcpyAsync(hf.data(), d_F, sizeof(double) * 3 * natoms, cudaMemcpyDeviceToHost, s));
+    DFT_CUDA_TRY(cudaStreamSynchronize(s));
+    if (is_device_pointer(forces)) DFT_CUDA_TRY(cudaMemcpy(forces, hf.data(), sizeof(double) * 3 * natoms, cudaMemcpyHostToDevice));
+    else std::memcpy(forces, hf.data(), sizeof(double) * 3 * natoms);
+    return DFTCUDA_OK;
+  };
+  st = run();
+  cleanup();
+  return st;
 }
 
 extern "C" int dftcuda_accumulate_density(dftcuda_kctx* c, const double* vectors, size_t n, size_t nbands,

@@ -104,6 +104,8 @@ struct dftcuda_kctx {
   size_t box_cols = 0;
 
   dftcuda::NonlocalDev nl;
+  int natoms = 0;                   // atoms given to set_projectors
+  std::vector<int> atom_row, atom_mt;  // per atom (set_projectors order): first projector row, row count
   double2* d_coef = nullptr;   // [nproj][cols] projector coefficients
   double2* d_coef2 = nullptr;
   size_t coef_cols = 0;

@@ -339,6 +339,53 @@ __global__ void k_pot_gga_vxc(const double* __restrict__ vr, const double2* __re
     out[i] = make_double2(vr[i] - 2.0 * div[i].x, 0.0);
 }
 
+// Local pseudopotential forces (local_pseudo_forces, forces/local_force.zig:21-80):
+// F_a = sum_G 2 ff_s(|G|) G Im(e^{iG.tau_a} rho(G)) over 1e-12 < G^2 <= g2max, rho(G) = a / N.
+// Grid (chunks, atoms): each block sums its chunk of G for one atom; part[(a * chunks + chunk) * 3 + d].
+constexpr int kLfChunks = 64;
+__global__ void __launch_bounds__(kPotThreads) k_pot_local_force(const double2* __restrict__ a, const double* __restrict__ g2,
+                                                                 int nx, int ny, int nz, Recip9 r,
+                                                                 const double* __restrict__ gth, const int* __restrict__ species,
+                                                                 const double* __restrict__ pos, double g2max,
+                                                                 double* __restrict__ part) {
+  __shared__ double red[kPotThreads / 32];
+  const long N = (long)nx * ny * nz;
+  const int atom = blockIdx.y, chunk = blockIdx.x;
+  const long per = (N + kLfChunks - 1) / kLfChunks;
+  const long i0 = chunk * per, i1 = min(N, i0 + per);
+  const int sp = species[atom];
+  const double Z = gth[6 * sp], rl = gth[6 * sp + 1];
+  const double c1 = gth[6 * sp + 2], c2 = gth[6 * sp + 3], c3 = gth[6 * sp + 4], c4 = gth[6 * sp + 5];
+  const double tx = pos[3 * atom], ty = pos[3 * atom + 1], tz = pos[3 * atom + 2];
+  const double inv = 1.0 / (double)N;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+    const double q = g2[i];
+    if (!(q > 1e-12 && q <= g2max)) continue;
+    const double gx = pot_gcomp(i, nx, ny, nz, r, 0), gy = pot_gcomp(i, nx, ny, nz, r, 1), gz = pot_gcomp(i, nx, ny, nz, r, 2);
+    const double yy = q * rl * rl, e = exp(-0.5 * yy);
+    const double poly = c1 + c2 * (3.0 - yy) + c3 * (15.0 - 10.0 * yy + yy * yy) +
+                        c4 * (105.0 - 105.0 * yy + 21.0 * yy * yy - yy * yy * yy);
+    const double ff = -4.0 * kPi * Z / q * e + sqrt(8.0 * kPi * kPi * kPi) * rl * rl * rl * e * poly;
+    double sn, cs;
+    sincos(gx * tx + gy * ty + gz * tz, &sn, &cs);
+    const double2 rg = make_double2(a[i].x * inv, a[i].y * inv);
+    const double w = 2.0 * ff * (cs * rg.y + sn * rg.x);  // Im(e^{iG.tau} rho(G))
+    fx += w * gx;
+    fy += w * gy;
+    fz += w * gz;
+  }
+  fx = block_sum(fx, red);
+  fy = block_sum(fy, red);
+  fz = block_sum(fz, red);
+  if (threadIdx.x == 0) {
+    double* o = part + ((long)atom * kLfChunks + chunk) * 3;
+    o[0] = fx;
+    o[1] = fy;
+    o[2] = fz;
+  }
+}
+
 // out_r = vloc + Re(v) * N (v holds FFT^-1 / N of the G-space field).
 __global__ void k_pot_real(const double2* __restrict__ v, const double* __restrict__ vloc, long N, double* __restrict__ out) {
   const double scale = (double)N;
@@ -690,6 +737,60 @@ extern "C" int dftcuda_ionic_potential(dftcuda_pctx* c, int nspecies, const doub
     }
   }
   if (cudaStreamSynchronize(s) != cudaSuccess && st == DFTCUDA_OK) st = fail(DFTCUDA_ERR_CUDA, "ionic_potential: kernel failed");
+  cleanup();
+  return st;
+}
+
+extern "C" int dftcuda_local_forces(dftcuda_pctx* c, int nspecies, const double* gth, int natoms, const int* atom_species,
+                                    const double* positions, double g2max, const double* rho_r, double* forces) {
+  if (!c || nspecies < 1 || !gth || natoms < 1 || !atom_species || !positions || !rho_r || !forces)
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "local_forces: bad arguments");
+  for (int a = 0; a < natoms; ++a)
+    if (atom_species[a] < 0 || atom_species[a] >= nspecies)
+      return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "local_forces: atom species index out of range");
+  const long N = c->N;
+  cudaStream_t s = c->stream;
+  int st = DFTCUDA_OK;
+  const double* rho = (const double*)device_view(rho_r, c->rho, sizeof(double) * N, s, &st);
+  if (st != DFTCUDA_OK) return st;
+  double* d_gth = nullptr;
+  double* d_pos = nullptr;
+  int* d_sp = nullptr;
+  double* d_part = nullptr;
+  auto cleanup = [&] {
+    for (void* p : {(void*)d_gth, (void*)d_pos, (void*)d_sp, (void*)d_part})
+      if (p) cudaFree(p);
+  };
+  const size_t npart = (size_t)natoms * kLfChunks * 3;
+  if (cudaMalloc(&d_gth, sizeof(double) * 6 * nspecies) != cudaSuccess || cudaMalloc(&d_pos, sizeof(double) * 3 * natoms) != cudaSuccess ||
+      cudaMalloc(&d_sp, sizeof(int) * natoms) != cudaSuccess || cudaMalloc(&d_part, sizeof(double) * npart) != cudaSuccess) {
+    cleanup();
+    return fail(DFTCUDA_ERR_CUDA, "local_forces: allocation failed");
+  }
+  std::vector<double> hp(npart);
+  auto run = [&]() -> int {
+    DFT_CUDA_TRY(cudaMemcpyAsync(d_gth, gth, sizeof(double) * 6 * nspecies, cudaMemcpyDefault, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(d_pos, positions, sizeof(double) * 3 * natoms, cudaMemcpyDefault, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(d_sp, atom_species, sizeof(int) * natoms, cudaMemcpyDefault, s));
+    k_pot_to_complex<<<kPotBlocks, kPotThreads, 0, s>>>(rho, N, c->a);
+    count_launch();
+    DFT_TRY(fft3d_on_stream(c->plan, c->a, -1, s));
+    Recip9 r;
+    for (int i = 0; i < 9; ++i) r.b[i] = c->recip[i];
+    k_pot_local_force<<<dim3(kLfChunks, natoms), kPotThreads, 0, s>>>(c->a, c->g2, c->nx, c->ny, c->nz, r, d_gth, d_sp, d_pos,
+                                                                       g2max > 0.0 ? g2max : 1e300, d_part);
+    count_launch();
+    DFT_CUDA_TRY(cudaMemcpyAsync(hp.data(), d_part, sizeof(double) * npart, cudaMemcpyDeviceToHost, s));
+    DFT_CUDA_TRY(cudaStreamSynchronize(s));
+    std::vector<double> f(3 * (size_t)natoms, 0.0);
+    for (int a = 0; a < natoms; ++a)
+      for (int ch = 0; ch < kLfChunks; ++ch)
+        for (int d = 0; d < 3; ++d) f[3 * a + d] += hp[((size_t)a * kLfChunks + ch) * 3 + d];
+    if (is_device_pointer(forces)) DFT_CUDA_TRY(cudaMemcpy(forces, f.data(), sizeof(double) * f.size(), cudaMemcpyHostToDevice));
+    else std::memcpy(forces, f.data(), sizeof(double) * f.size());
+    return DFTCUDA_OK;
+  };
+  st = run();
   cleanup();
   return st;
 }

@@ -114,6 +114,46 @@ def ewald_energy(cell: np.ndarray, charges: np.ndarray, pos: np.ndarray, tol: fl
     return 2.0 * float(e_real + e_rec + e_self + e_bg)
 
 
+def ewald_forces(cell: np.ndarray, charges: np.ndarray, pos: np.ndarray, tol: float = 1e-14, eta: Optional[float] = None) -> np.ndarray:
+    """Ion-ion forces (Ry/bohr; compute_ion_ion_forces, forces/forces.zig:59-104): minus the
+    gradient of ewald_energy, real-space erfc sum and reciprocal sum with the same split."""
+    from scipy.special import erfc
+
+    pos = np.asarray(pos, dtype=np.float64)
+    charges = np.asarray(charges, dtype=np.float64)
+    vol = abs(np.linalg.det(cell))
+    recip = 2.0 * math.pi * np.linalg.inv(cell).T
+    if eta is None:
+        eta = 0.85 * math.sqrt(math.pi) * (len(charges) / vol**2) ** (1.0 / 6.0)
+    rcut = math.sqrt(-math.log(tol)) / eta + 1e-9
+    gcut = 2.0 * eta * math.sqrt(-math.log(tol))
+    na = [int(math.ceil(rcut * np.linalg.norm(recip[i]) / (2.0 * math.pi))) + 1 for i in range(3)]
+    rng = [np.arange(-n, n + 1) for n in na]
+    L = np.stack(np.meshgrid(*rng, indexing="ij"), axis=-1).reshape(-1, 3) @ cell
+    dmax = float(np.linalg.norm(pos[:, None, :] - pos[None, :, :], axis=2).max())
+    L = L[np.linalg.norm(L, axis=1) < rcut + dmax + 1e-9]
+    f = np.zeros_like(pos)
+    c2 = 2.0 * eta / math.sqrt(math.pi)
+    for i in range(len(charges)):
+        d = pos[i][None, None, :] - pos[:, None, :] + L[None, :, :]  # [j, L, 3]
+        r = np.linalg.norm(d, axis=2)
+        m = (r > 1e-10) & (r < rcut)
+        rr = np.where(m, r, 1.0)
+        radial = np.where(m, (erfc(eta * rr) / rr + c2 * np.exp(-(eta * rr) ** 2)) / (rr * rr), 0.0)
+        f[i] += charges[i] * np.einsum("jl,jlx->x", charges[:, None] * radial, d)
+    ng = [int(math.ceil(gcut / np.linalg.norm(recip[i]))) + 1 for i in range(3)]
+    rng = [np.arange(-n, n + 1) for n in ng]
+    G = np.stack(np.meshgrid(*rng, indexing="ij"), axis=-1).reshape(-1, 3) @ recip
+    g2 = (G * G).sum(axis=1)
+    sel = (g2 > 1e-12) & (g2 < gcut * gcut)
+    G, g2 = G[sel], g2[sel]
+    ph = np.exp(1j * (G @ pos.T))  # [G, atom]
+    S = ph @ charges
+    k = np.exp(-g2 / (4.0 * eta * eta)) / g2
+    f += (4.0 * math.pi / vol) * charges[:, None] * (np.imag(ph * np.conj(S)[:, None]) * k[:, None]).T @ G
+    return 2.0 * f
+
+
 def gth_alpha(sp: sysm.SpeciesData) -> float:
     """G -> 0 limit of Omega (V_loc(G) + 8 pi Z / G^2) for the GTH form (Ry): the epsatm of
     energy.zig:350-365 for the synthetic species."""
@@ -335,6 +375,9 @@ class GpuBackend:
     def nonlocal_energies(self, k, vectors):
         return self._active()[k].nonlocal_energies(vectors)
 
+    def nonlocal_forces(self, k, vectors, weights, natoms):
+        return self._active()[k].nonlocal_forces(vectors, weights, natoms)
+
     def close(self):
         for kc in self.ctxs + self.ctxs32:
             kc.close()
@@ -381,6 +424,7 @@ class ScfResult:
     rho: np.ndarray
     history: list = field(default_factory=list)
     wall_s: float = 0.0
+    forces: Optional[np.ndarray] = None  # (natoms, 3) Ry/bohr when run_scf(..., forces=True)
 
 
 def g_vectors(dims, recip):
@@ -528,6 +572,7 @@ class ScfState:
             occ[: self.nocc - 1] = 1.0
             occ[self.nocc - 1] = nelec / 2.0 - (self.nocc - 1)
             occs = [occ for _ in values]
+        self.occs = occs
         if self.dev:
             import torch
 
@@ -606,17 +651,43 @@ class ScfState:
         return ScfResult(self.converged, self.it, self.energy, self.energy / natom, self.values, self.terms, rho, self.history,
                          time.perf_counter() - self.t0)
 
+    def forces(self) -> np.ndarray:
+        """Hellmann-Feynman forces (natoms, 3, Ry/bohr) of the last iteration's density and bands
+        (compute_forces, forces/forces.zig:785-851, without NLCC, PAW or dispersion terms): local
+        pseudopotential (device), nonlocal (device, summed over this rank's k-points and over the
+        ranks) and ion-ion (host Ewald)."""
+        if not self.dev:
+            raise ValueError("forces need the resident driver (GpuBackend(resident=True))")
+        c, p = self.c, self.p
+        gth = [[sp.params["z"], sp.params["rloc"], sp.params.get("c1", 0.0), sp.params.get("c2", 0.0),
+                sp.params.get("c3", 0.0), sp.params.get("c4", 0.0)] for sp in c.species]
+        natoms = len(c.atom_species)
+        f_loc = self.pot.local_forces(gth, c.atom_species, c.positions, self.rho, 4.0 * p.ecut)
+        f_nl = np.zeros((natoms, 3))
+        for i, k in enumerate(self.kglobal):
+            w = self.kweights[k] * np.asarray(self.occs[k]) * 2.0
+            f_nl += self.backend.nonlocal_forces(i, self.vectors[i], w, natoms)
+        if self.comm.size > 1:
+            f_nl = self.comm.sum(f_nl)
+        f_ion = ewald_forces(c.cell, np.array([c.species[s].z_val for s in c.atom_species]), c.positions)
+        self.force_terms = {"local": f_loc, "nonlocal": f_nl, "ion_ion": f_ion}
+        return f_loc + f_nl + f_ion
+
     def close(self):
         if self.dev:
             self.pot.close()
 
 
-def run_scf(c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False, comm=None) -> ScfResult:
+def run_scf(c: sysm.Crystal, p: ScfParams, backend, verbose: bool = False, comm=None, forces: bool = False) -> ScfResult:
     """The SCF loop.  ``comm`` (a kpar.KpointComm) deals the k-points over the ranks of a process
-    group; every rank returns the same result."""
+    group; every rank returns the same result.  forces: also the Hellmann-Feynman forces of the
+    final state (resident driver)."""
     st = ScfState(c, p, backend, verbose, comm)
     try:
-        return _run(st, backend)
+        r = _run(st, backend)
+        if forces:
+            r.forces = st.forces()
+        return r
     finally:
         st.close()
 

@@ -111,6 +111,14 @@ int dftcuda_apply_h_batch_async(dftcuda_kctx* ctx, const double* x_dev, double* 
 /* Re <psi_b|V_nl|psi_b> for nbands columns (kpoint/density.zig:145-165, 238-266). Host or device. */
 int dftcuda_nonlocal_energies(dftcuda_kctx* ctx, const double* psi, size_t n, size_t nbands, double* e_out);
 
+/* Nonlocal Hellmann-Feynman forces on the context's atoms (accumulate_atom_force_at_kpoint,
+ * forces/nonlocal_force.zig:283-341): F[a][d] = (2/Omega) sum_b w_b Im sum_{j of atom a}
+ * conj((D p)_jb) <beta_j|(k+G)_d psi_b>, p = <beta|psi>.  vectors: (nbands, n) complex128,
+ * weights: nbands doubles (k weight x occupation x spin), forces: natoms x 3 doubles (Ry/bohr), the
+ * atoms in the order given to dftcuda_set_projectors.  Sum the k-points' results for the total. */
+int dftcuda_nonlocal_forces(dftcuda_kctx* ctx, const double* vectors, size_t n, size_t nbands, const double* weights,
+                            double* forces);
+
 /* Autotuner: times candidate launch configurations of this context's H|psi> on ncols trial
  * columns (FFT pass variant, column-chunk workspace budget, split-K of the two projector GEMMs)
  * with CUDA events and keeps the fastest for all later calls.  report may be NULL. */
@@ -325,6 +333,12 @@ int dftcuda_pulay_mix(dftcuda_pctx* ctx, double* x, const double* residual, size
  * V_loc(r) = sum_G V(G) e^{iGr} to vloc_r (N doubles); either may be NULL. */
 int dftcuda_ionic_potential(dftcuda_pctx* ctx, int nspecies, const double* gth, int natoms, const int* atom_species,
                             const double* positions, double g2max, double* v_out_g, double* vloc_r);
+/* local_pseudo_forces (forces/local_force.zig:21-80): the local-pseudopotential Hellmann-Feynman
+ * force on every atom, F_a = sum_G 2 ff_s(|G|) G Im(e^{iG.tau_a} rho(G)) for 1e-12 < G^2 <= g2max
+ * (same species parameters as dftcuda_ionic_potential), from the density rho_r (N doubles).
+ * forces: natoms x 3 doubles, Ry/bohr. */
+int dftcuda_local_forces(dftcuda_pctx* ctx, int nspecies, const double* gth, int natoms, const int* atom_species,
+                         const double* positions, double g2max, const double* rho_r, double* forces);
 int dftcuda_pulay_reset(dftcuda_pctx* ctx);
 
 /* ------------------------------------------------------------------------------------------
