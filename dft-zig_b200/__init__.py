@@ -72,6 +72,7 @@ ABI_SYMBOLS = (
     "dftcuda_pctx_set_functional",
     "dftcuda_local_forces",
     "dftcuda_nonlocal_forces",
+    "dftcuda_radial_table",
 )
 
 PRECOND_REFERENCE = 0  # r / (|k+G|^2 - lambda), lobpcg/common.zig:214-226
@@ -242,6 +243,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.dftcuda_pctx_set_functional.argtypes = [vp, ip]
     lib.dftcuda_local_forces.argtypes = [vp, ip, vp, ip, vp, vp, ct.c_double, dp, dp]
     lib.dftcuda_nonlocal_forces.argtypes = [vp, dp, sz, sz, dp, dp]
+    lib.dftcuda_radial_table.argtypes = [ip, sz, dp, dp, dp, sz, ct.c_double, dp]
     lb = ct.c_long
     lib.dftcuda_complex_gemm.argtypes = [ip, sz, sz, sz, vp, lb, ip, ip, vp, lb, ip, ip, vp, lb, lb, ct.c_double, ct.c_double]
     _lib = lib
@@ -735,6 +737,19 @@ def _nbytes(a) -> int:
     if _is_torch_cuda(a):
         return a.numel() * a.element_size()
     return np.asarray(a).nbytes
+
+
+def radial_table(l: int, r, rbeta, rab, gmax: float, npts: int = 2048):
+    """Radial projector table of one beta on the device (dftcuda_radial_table): values on
+    q_i = i gmax / (npts - 1).  Returns (values, gmax, dq) like system.radial_table."""
+    lib = load_library()
+    _require_device()
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    rbeta = np.ascontiguousarray(rbeta, dtype=np.float64)
+    rab = np.ascontiguousarray(rab, dtype=np.float64)
+    out = np.empty(int(npts))
+    _check(lib.dftcuda_radial_table(int(l), r.size, r.ctypes.data, rbeta.ctypes.data, rab.ctypes.data, out.size, float(gmax), out.ctypes.data))
+    return out, float(gmax), float(gmax) / (npts - 1)
 
 
 def complex_gemm(a, b, out=None, *, conj_a: bool = False, conj_b: bool = False, precision: int = 0, alpha: float = 1.0,

@@ -18,6 +18,7 @@
 // library's axis passes.  Sums are taken as fixed per-block partials added on the host in block
 // order, so results do not depend on scheduling.
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <vector>
 
@@ -384,6 +385,65 @@ __global__ void __launch_bounds__(kPotThreads) k_pot_local_force(const double2* 
     o[1] = fy;
     o[2] = fz;
   }
+}
+
+// ---- radial projector tables (RadialTableSet, pseudopotential/nonlocal.zig:8-21, 59-71, 250-338) ----
+// Spherical Bessel j_l(x): the series below 1e-6, closed forms for l <= 1, downward (Miller)
+// recursion normalised by j_0 above (up to 256 terms, else the upward recurrence).
+__device__ double sph_bessel(int l, double x) {
+  if (fabs(x) < 1e-6) {
+    const double x2 = x * x;
+    if (l == 0) return 1.0 - x2 / 6.0 + x2 * x2 / 120.0;
+    if (l == 1) return x / 3.0 - x * x2 / 30.0;
+    if (l == 2) return x2 / 15.0 - x2 * x2 / 210.0;
+    if (l == 3) return x * x2 / 105.0;
+    return 0.0;
+  }
+  if (l == 0) return sin(x) / x;
+  if (l == 1) return sin(x) / (x * x) - cos(x) / x;
+  const int nm = l + 1;
+  const int nlim = x < 1.0 ? nm + (int)(15.0 * x) + 1 : nm + (int)(1.36 * x) + 15;
+  if (nlim > 256) {
+    if (l > x + 50.0) return 0.0;
+    double jlm1 = sin(x) / x, jl = sin(x) / (x * x) - cos(x) / x;
+    for (int n = 1; n < l; ++n) {
+      const double jlp1 = (2.0 * n + 1.0) / x * jl - jlm1;
+      jlm1 = jl;
+      jl = jlp1;
+      if (!isfinite(jl)) return 0.0;
+    }
+    return jl;
+  }
+  const double xi = 1.0 / x;
+  double up = 0.0, cur = 1.0e-18, want = 0.0;  // sb[n+1], sb[n]; nlim > l, so sb[l] is set below
+  for (int n = nlim; n > 0; --n) {
+    const double down = (2.0 * n + 1.0) * xi * cur - up;  // sb[n-1]
+    up = cur;
+    cur = down;
+    if (n - 1 == nm - 1) want = cur;
+  }
+  return want * ((sin(x) / x) / cur);
+}
+
+// out[i] = sum_j r_j (r beta)_j j_l(q_i r_j) rab_j w_j, q_i = i * gmax / (nq - 1), w the composite
+// trapezoid weights of radial_integration.zig:7-13.  One block per q point.
+__global__ void __launch_bounds__(kPotThreads) k_radial_table(int l, int nr, const double* __restrict__ r,
+                                                              const double* __restrict__ rbeta, const double* __restrict__ rab,
+                                                              double dq, double* __restrict__ out) {
+  __shared__ double red[kPotThreads / 32];
+  const double q = dq * blockIdx.x;
+  const double cw[5] = {23.75 / 72.0, 95.10 / 72.0, 55.20 / 72.0, 79.30 / 72.0, 70.65 / 72.0};
+  double s = 0.0;
+  for (int j = threadIdx.x; j < nr; j += blockDim.x) {
+    double w = 1.0;
+    if (nr >= 10) {
+      if (j < 5) w = cw[j];
+      else if (j >= nr - 5) w = cw[nr - 1 - j];
+    }
+    s += r[j] * rbeta[j] * sph_bessel(l, q * r[j]) * rab[j] * w;
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) out[blockIdx.x] = s;
 }
 
 // out_r = vloc + Re(v) * N (v holds FFT^-1 / N of the G-space field).
@@ -792,6 +852,32 @@ extern "C" int dftcuda_local_forces(dftcuda_pctx* c, int nspecies, const double*
   };
   st = run();
   cleanup();
+  return st;
+}
+
+extern "C" int dftcuda_radial_table(int l, size_t nr, const double* r, const double* rbeta, const double* rab, size_t nq,
+                                    double gmax, double* out) {
+  if (l < 0 || nr == 0 || nq < 2 || !r || !rbeta || !rab || !out || !(gmax > 0.0) || nr > (size_t)INT32_MAX || nq > 65535)
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "radial_table: bad arguments (nq 2..65535)");
+  double* d = nullptr;
+  const size_t bytes = sizeof(double) * (3 * nr + nq);
+  if (cudaMalloc(&d, bytes) != cudaSuccess) return fail(DFTCUDA_ERR_CUDA, "radial_table: allocation failed");
+  cudaStream_t s = nullptr;
+  int st = DFTCUDA_OK;
+  auto run = [&]() -> int {
+    DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    DFT_CUDA_TRY(cudaMemcpyAsync(d, r, sizeof(double) * nr, cudaMemcpyDefault, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(d + nr, rbeta, sizeof(double) * nr, cudaMemcpyDefault, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(d + 2 * nr, rab, sizeof(double) * nr, cudaMemcpyDefault, s));
+    k_radial_table<<<(unsigned)nq, kPotThreads, 0, s>>>(l, (int)nr, d, d + nr, d + 2 * nr, gmax / (double)(nq - 1), d + 3 * nr);
+    count_launch();
+    DFT_CUDA_TRY(cudaMemcpyAsync(out, d + 3 * nr, sizeof(double) * nq, cudaMemcpyDefault, s));
+    DFT_CUDA_TRY(cudaStreamSynchronize(s));
+    return DFTCUDA_OK;
+  };
+  st = run();
+  if (s) cudaStreamDestroy(s);
+  cudaFree(d);
   return st;
 }
 

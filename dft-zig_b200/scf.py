@@ -465,10 +465,15 @@ class ScfState:
         # run_scf_many shares them across its cells through table_cache
         tc = table_cache if table_cache is not None else {}
         tables = []
+        resident = bool(getattr(backend, "resident", False))
         for sp in c.species:
             key = (sp.name, p.ecut)
             if key not in tc:
-                tc[key] = [sysm.radial_table(sp, i, p.ecut) for i in range(len(sp.betas))]
+                if resident:  # one kernel launch per beta (dftcuda_radial_table)
+                    gmax = 1.5 * math.sqrt(2.0 * p.ecut)
+                    tc[key] = [backend.dz.radial_table(l, sp.r, beta, sp.rab, gmax) for (l, beta) in sp.betas]
+                else:
+                    tc[key] = [sysm.radial_table(sp, i, p.ecut) for i in range(len(sp.betas))]
             tables.append(tc[key])
         tm["radial_tables"], t = time.perf_counter() - t, time.perf_counter()
         # resident backends: density, potential and mixing history on the device (csrc/potential.cu),

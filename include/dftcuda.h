@@ -341,6 +341,14 @@ int dftcuda_local_forces(dftcuda_pctx* ctx, int nspecies, const double* gth, int
                          const double* positions, double g2max, const double* rho_r, double* forces);
 int dftcuda_pulay_reset(dftcuda_pctx* ctx);
 
+/* Radial projector table of one beta (RadialTableSet.init, pseudopotential/nonlocal.zig:250-338,
+ * entries radial_projector, nonlocal.zig:8-21): out[i] = sum_j r_j rbeta_j j_l(q_i r_j) rab_j w_j on
+ * q_i = i gmax / (nq - 1), w the composite-trapezoid weights of radial_integration.zig:7-13 and j_l
+ * as nonlocal.zig:59-71.  r, rbeta (r times beta), rab: the radial mesh (nr points); out: nq doubles.
+ * Any pointer may be host or device memory. */
+int dftcuda_radial_table(int l, size_t nr, const double* r, const double* rbeta, const double* rab, size_t nq, double gmax,
+                         double* out);
+
 /* ------------------------------------------------------------------------------------------
  * The library's complex GEMM (no counterpart in the reference; the contraction its projector and
  * Rayleigh-Ritz code paths run), exposed for tests and benchmarks:
