@@ -53,11 +53,16 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile-case", action="store_true", help="small single-k case for ncu captures: Gamma, 32 columns, 2 applications")
-    ap.add_argument("--workload", choices=("hpsi", "scf", "scf64", "scf216", "cells", "eig"), default="hpsi",
+    ap.add_argument("--workload", choices=("hpsi", "scf", "scf64", "scf216", "cells", "eig", "heev"), default="hpsi",
                     help="hpsi: H|psi> GB/s (default); scf: time-to-SCF Si2; scf64: time-to-SCF Si64, mixed vs FP64; "
                          "scf216: time-to-SCF Si216 (Gamma, 448 bands), FP64 vs learned+mixed; "
                          "cells: many-cell SiGe8 SCF throughput, atomic vs learned start; "
-                         "eig: one Si64 Gamma Davidson solve (profiling case)")
+                         "eig: one Si64 Gamma Davidson solve (profiling case); "
+                         "heev: the subspace eigensolver on a seeded Hermitian matrix (--heev-m, lowest m/3 pairs)")
+    ap.add_argument("--heev-m", type=int, default=1344, help="matrix size of --workload heev")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="scf216: instead of time-to-SCF, run N SCF steps of each arm and print its kernel-time "
+                         "table (CUPTI activity records through torch.profiler)")
     ap.add_argument("--eig-iters", type=int, default=6, help="Davidson iterations of --workload eig")
     ap.add_argument("--eig-cell", choices=("si64", "si216"), default="si64", help="cell of --workload eig")
     ap.add_argument("--cells", type=int, default=16, help="cells of the many-cell workload")
@@ -717,8 +722,83 @@ def run_eig_workload(args):
                       "subspace_ms": round(pr["subspace_ns"] / 1e6, 2)}), flush=True)
 
 
+def run_heev_workload(args):
+    """The subspace eigensolver (dftcuda_hermitian_eigen_decomp: tridiagonalisation, bisection,
+    inverse iteration, WY back-transformation) on a seeded random Hermitian m x m matrix, lowest m/3
+    pairs: device time of two calls after one warm-up, and the eigenvalue error against LAPACK."""
+    import torch
+
+    import dftzig_loader
+
+    dz = dftzig_loader.load()
+    lib = dz.load_library()
+    m = args.heev_m
+    nev = max(1, m // 3)
+    rng = np.random.default_rng(m)
+    x = rng.normal(size=(m, m)) + 1j * rng.normal(size=(m, m))
+    a = 0.05 * (x + x.conj().T) / 2
+    at = torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+    vals = torch.empty(nev, dtype=torch.float64, device="cuda")
+    vecs = torch.empty((nev, m), dtype=torch.complex128, device="cuda")
+    ms = []
+    for rep in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = lib.dftcuda_hermitian_eigen_decomp(m, at.data_ptr(), nev, vals.data_ptr(), vecs.data_ptr())
+        torch.cuda.synchronize()
+        if st != 0:
+            raise RuntimeError(f"hermitian_eigen_decomp failed ({st})")
+        ms.append(1e3 * (time.perf_counter() - t0))
+    err = float(np.abs(vals.cpu().numpy() - np.linalg.eigvalsh(a)[:nev]).max())
+    print(json.dumps({"metric": f"subspace eigensolver wall time, m = {m}, lowest {nev} pairs", "value": round(min(ms[1:]), 2),
+                      "unit": "ms", "eigenvalue_error_max": err}), flush=True)
+
+
+def run_scf216_kernel_table(args):
+    """The first --profile-steps SCF steps of both Si216 arms under torch.profiler (CUPTI activity
+    records): per arm, the GPU time of each kernel summed over the steps, and the wall time."""
+    import importlib
+
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    import dftzig_loader
+
+    dz = dftzig_loader.load()
+    scf = importlib.import_module("dftzig_b200.scf")
+    system = importlib.import_module("dftzig_b200.system")
+    learn = importlib.import_module("dftzig_b200.learn")
+    c = system.crystal("si216", 3)
+    base = dict(ecut=25.0, kmesh=(1, 1, 1), nbands=448, mixing_beta=0.3, pulay_history=8, max_iter=args.profile_steps)
+    mlp = (dz.PRECOND_MLP, learn.load_precond_weights())
+    out = {}
+    for mode, prec, pc in (("fp64", "fp64", None), ("learned_mixed", "mixed", mlp)):
+        b = scf.GpuBackend(dz, prec, precond=pc, resident=True, switch_drho=args.switch_drho)
+        t0 = time.perf_counter()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            scf.run_scf(c, scf.ScfParams(**base, convergence=1e-12), b)
+            torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        b.close()
+        rows = []
+        for e in prof.key_averages():
+            t = getattr(e, "device_time_total", 0) or getattr(e, "cuda_time_total", 0)
+            if t > 0:
+                rows.append((round(t / 1e3, 1), e.count, e.key.replace("(anonymous namespace)::", "").split("(")[0][:80]))
+        rows.sort(reverse=True)
+        out[mode] = {"wall_s": round(wall, 2), "gpu_kernel_ms": round(sum(r[0] for r in rows), 1), "davidson": b.solves,
+                     "top": [{"ms": r[0], "launches": r[1], "kernel": r[2]} for r in rows[:20]]}
+    print(json.dumps({"metric": f"Si216 kernel-time table, first {args.profile_steps} SCF steps", **out}), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "heev":
+        run_heev_workload(args)
+        return
+    if args.workload == "scf216" and args.profile_steps > 0:
+        run_scf216_kernel_table(args)
+        return
     if args.workload == "eig":
         run_eig_workload(args)
         return

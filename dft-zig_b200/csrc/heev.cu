@@ -33,42 +33,46 @@ constexpr int BT_WARPS = 4;                  // back-transformation: eigenvector
 constexpr long kBarrierSpin = 1L << 24;      // polls (with 64 ns sleeps) before a barrier gives up
 constexpr double kGroupTol = 1e-5;           // eigenvalue grouping, relative to ||T||
 constexpr int kHtMaxSplit = 8;               // warps per trailing column (row chunks)
+constexpr int kHtColRegs = 4;                // column entries per thread (m <= 4 HT_THREADS)
+static_assert(kHtColRegs * HT_THREADS >= 2048, "k_hetrd1 holds a column of up to 2047 entries in registers");
+constexpr int kIvChunk = 8;                  // inverse iteration: entries loaded ahead per sweep step
 
 struct GridBarrier {
-  unsigned* count;
-  unsigned* gen;
+  unsigned* count;  // arrivals since the launch (zeroed by the host)
   int* err;
   unsigned nblocks;
 };
 
-// All blocks of the (co-resident, cooperative) grid meet here.  Returns false for every thread of
-// a block when this or an earlier barrier gave up; the error flag is then set.
-__device__ bool grid_sync(const GridBarrier& b) {
+// All blocks of the (co-resident, cooperative) grid meet here.  The arrival counter only grows
+// (reset by the host before the launch): the t-th barrier is passed once it reaches t * nblocks, so
+// arriving is one atomic and waiting one acquire-load poll.  Returns false for every thread of a
+// block whose wait gave up (the error flag is then set); a block that gives up returns, and the
+// others give up at their next barrier, which it never reaches.
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ bool grid_sync(const GridBarrier& b, unsigned& epoch) {
   __shared__ int s_ok;
   __syncthreads();
+  ++epoch;
   if (threadIdx.x == 0) {
     int ok = 1;
-    volatile unsigned* vg = b.gen;
-    const unsigned g = *vg;
+    const unsigned target = epoch * b.nblocks;
     __threadfence();
-    const unsigned arrived = atomicAdd(b.count, 1u);
-    if (arrived == b.nblocks - 1) {
-      atomicExch(b.count, 0u);
-      __threadfence();
-      atomicAdd(b.gen, 1u);
-    } else {
-      long it = 0;
-      while (*vg == g) {
-        if (++it > kBarrierSpin) {
-          atomicExch(b.err, 1);
-          ok = 0;
-          break;
-        }
-        __nanosleep(64);
+    atomicAdd(b.count, 1u);
+    long it = 0;
+    while (ld_acquire_gpu(b.count) < target) {
+      if (++it > kBarrierSpin) {
+        atomicExch(b.err, 1);
+        ok = 0;
+        break;
       }
+      __nanosleep(32);
     }
     __threadfence();
-    if (*(volatile int*)b.err) ok = 0;
     s_ok = ok;
   }
   __syncthreads();
@@ -111,6 +115,7 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd(double2* __restrict__ A, i
   const int tid = threadIdx.x, lane = tid & 31;
   const int gw = blockIdx.x * HT_WARPS + (tid >> 5);
   const int W = gridDim.x * HT_WARPS;
+  unsigned epoch = 0;
   for (int k = 0; k + 1 < m; ++k) {
     const int n1 = m - k - 1;
     const double2* col = A + (long)k * m + (k + 1);
@@ -165,7 +170,7 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd(double2* __restrict__ A, i
         if (lane == 0) y[(long)sidx * m + r] = make_double2(sx, sy);
       }
     }
-    if (!grid_sync(bar)) return;
+    if (!grid_sync(bar, epoch)) return;
     // Phase C: y = tau A22 v; w = y + alpha v with alpha = -tau (y^H v) / 2; A22 -= v w^H + w v^H.
     if (active) {
       double2 p2 = make_double2(0.0, 0.0);
@@ -198,7 +203,7 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd(double2* __restrict__ A, i
       double2* cw = A + (long)k * m + (k + 1);
       for (int i = tid; i < n1; i += HT_THREADS) cw[i] = i == 0 ? make_double2(beta, 0.0) : sv[i];
     }
-    if (!grid_sync(bar)) return;
+    if (!grid_sync(bar, epoch)) return;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) dd[m - 1] = __ldcg(A + (long)(m - 1) * m + (m - 1)).x;
 }
@@ -246,6 +251,7 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
   const int tid = threadIdx.x, lane = tid & 31;
   const int gw = blockIdx.x * HT_WARPS + (tid >> 5);
   const int W = gridDim.x * HT_WARPS;
+  unsigned epoch = 0;
   // prologue: reflector 0 and the partial products of step 0
   double2 t;
   double beta;
@@ -283,11 +289,21 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
     }
     S_prev = S;
   }
-  if (!grid_sync(bar)) return;
+  if (!grid_sync(bar, epoch)) return;
   for (int k = 0; k + 1 < m; ++k) {
     const int n1 = m - k - 1;
     const double2* yk = y + (size_t)(k & 1) * kHtMaxSplit * m;      // step k's partials
     double2* yn = y + (size_t)((k + 1) & 1) * kHtMaxSplit * m;      // step k+1's
+    // column k+1 as the previous sweep left it (rows k+1 ..), loaded with step k's partials
+    double2 colr[kHtColRegs];
+    {
+      const double2* col = A + (long)(k + 1) * m + (k + 1);
+#pragma unroll
+      for (int q = 0; q < kHtColRegs; ++q) {
+        const int i = tid + q * HT_THREADS;
+        colr[q] = i < n1 ? __ldcg(col + i) : make_double2(0.0, 0.0);
+      }
+    }
     // (1) y = tau A22 v from the partial products; w = y + alpha v, alpha = -tau (y^H v) / 2
     {
       double2 p2 = make_double2(0.0, 0.0);
@@ -315,10 +331,12 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
     double2 tn = make_double2(0.0, 0.0);
     double betan = 0.0;
     {
-      const double2* col = A + (long)(k + 1) * m + (k + 1);
       const double2 w0c = cconj(sw[0]);  // v_0 = 1
-      for (int i = tid; i < n1; i += HT_THREADS) {
-        const double2 x = csub(__ldcg(col + i), cadd(cmul(sv[i], w0c), sw[i]));
+#pragma unroll
+      for (int q = 0; q < kHtColRegs; ++q) {
+        const int i = tid + q * HT_THREADS;
+        if (i >= n1) break;
+        const double2 x = csub(colr[q], cadd(cmul(sv[i], w0c), sw[i]));
         if (i == 0) {
           if (blockIdx.x == 0) dd[k + 1] = x.x;
         } else {
@@ -348,7 +366,7 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
         const double2 wr = cconj(sw[c]), vr = cconj(sv[c]);
         double2* ac = A + (long)r * m + (k + 1);
         double sx = 0.0, sy = 0.0;
-#pragma unroll 4
+#pragma unroll 8
         for (int i = i0 + lane; i < i1; i += 32) {
           double2 a = __ldcg(ac + i);
           a = csub(a, cadd(cmul(sv[i], wr), cmul(sw[i], vr)));
@@ -365,7 +383,7 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
       }
       S_prev = S;
     }
-    if (!grid_sync(bar)) return;
+    if (!grid_sync(bar, epoch)) return;
     double2* tmp = sv;
     sv = sn;
     sn = tmp;
@@ -467,8 +485,11 @@ __device__ __forceinline__ double hashed_unit(uint64_t a, uint64_t b) {
 }
 
 // Step 3.  Z[:, j] (m x nev, column-major, real) = unit eigenvector of T for w[j].  Thread j works
-// when j starts a group (w[j] - w[j-1] > kGroupTol ||T||) and computes the whole group.  lu: per
-// thread 4 m doubles (U's diagonal and two superdiagonals, the multipliers) + m row-swap flags.
+// when j starts a group (w[j] - w[j-1] > kGroupTol ||T||) and computes the whole group.  lu holds
+// six arrays of m entries per thread (U's diagonal and two superdiagonals, the multipliers, the
+// row-swap flags, the working vector), interleaved across threads, entry (q, i) of thread j at
+// lu[(q m + i) nev + j], so a warp's accesses at one i are one coalesced transaction.  The sweeps
+// load kIvChunk entries ahead of the recurrence that consumes them.
 __global__ void k_tridiag_invit(const double* __restrict__ dd, const double* __restrict__ ee, int m, int nev,
                                 const double* __restrict__ w, const double* __restrict__ tnorm_p,
                                 double* __restrict__ Z, double* __restrict__ lu) {
@@ -479,11 +500,13 @@ __global__ void k_tridiag_invit(const double* __restrict__ dd, const double* __r
   if (j > 0 && !(w[j] - w[j - 1] > gtol)) return;
   int jend = j + 1;
   while (jend < nev && !(w[jend] - w[jend - 1] > gtol)) ++jend;
-  double* u0 = lu + (size_t)j * 5 * m;
-  double* u1 = u0 + m;
-  double* u2 = u1 + m;
-  double* lm = u2 + m;
-  double* sw = lm + m;
+  const size_t st = (size_t)nev;
+  double* const u0 = lu + j;
+  double* const u1 = u0 + (size_t)m * st;
+  double* const u2 = u1 + (size_t)m * st;
+  double* const lm = u2 + (size_t)m * st;
+  double* const sw = lm + (size_t)m * st;
+  double* const zz = sw + (size_t)m * st;
   const double tiny = DBL_EPSILON * tnorm;
   for (int p = j; p < jend; ++p) {
     const double lam = w[p];
@@ -491,60 +514,112 @@ __global__ void k_tridiag_invit(const double* __restrict__ dd, const double* __r
     double a = dd[0] - lam, b = m > 1 ? ee[0] : 0.0;
     for (int i = 0; i + 1 < m; ++i) {
       const double sub = ee[i], dn = dd[i + 1] - lam, up = i + 2 < m ? ee[i + 1] : 0.0;
+      const size_t o = (size_t)i * st;
       if (fabs(a) >= fabs(sub)) {
         const double piv = fabs(a) < tiny ? (a < 0.0 ? -tiny : tiny) : a;
         const double l = sub / piv;
-        u0[i] = piv; u1[i] = b; u2[i] = 0.0; lm[i] = l; sw[i] = 0.0;
+        u0[o] = piv; u1[o] = b; u2[o] = 0.0; lm[o] = l; sw[o] = 0.0;
         a = dn - l * b;
         b = up;
       } else {
         const double l = a / sub;
-        u0[i] = sub; u1[i] = dn; u2[i] = up; lm[i] = l; sw[i] = 1.0;
+        u0[o] = sub; u1[o] = dn; u2[o] = up; lm[o] = l; sw[o] = 1.0;
         a = b - l * dn;
         b = -l * up;
       }
     }
-    u0[m - 1] = fabs(a) < tiny ? (a < 0.0 ? -tiny : tiny) : a;
-    double* z = Z + (size_t)p * m;
-    for (int i = 0; i < m; ++i) z[i] = hashed_unit((uint64_t)p, (uint64_t)i);
+    u0[(size_t)(m - 1) * st] = fabs(a) < tiny ? (a < 0.0 ? -tiny : tiny) : a;
+    u1[(size_t)(m - 1) * st] = 0.0;  // the back substitution reads row m-1's superdiagonals
+    u2[(size_t)(m - 1) * st] = 0.0;
+    // zz holds the vector up to the factor scl (the previous sweep's normalisation, applied as the
+    // next sweep reads it); the first sweep starts from a hashed vector
+    double scl = 1.0;
     for (int sweep = 0; sweep < 3; ++sweep) {
-      // forward: the same row operations on the right-hand side
-      double cb = z[0];
-      for (int i = 0; i + 1 < m; ++i) {
-        const double nb = z[i + 1];
-        if (sw[i] == 0.0) {
-          z[i] = cb;
-          cb = nb - lm[i] * cb;
-        } else {
-          z[i] = nb;
-          cb = cb - lm[i] * nb;
+      auto rhs = [&](int i) { return sweep == 0 ? hashed_unit((uint64_t)p, (uint64_t)i) : zz[(size_t)i * st] * scl; };
+      // forward: the same row operations on the right-hand side (entry i+1 is read before
+      // entry i is written, so a chunk's loads may all precede its stores)
+      double cb = rhs(0);
+      for (int i0 = 0; i0 + 1 < m; i0 += kIvChunk) {
+        const int n = min(kIvChunk, m - 1 - i0);
+        double zn[kIvChunk], lv[kIvChunk], sv[kIvChunk];
+#pragma unroll
+        for (int c = 0; c < kIvChunk; ++c) {
+          if (c < n) {
+            const size_t o = (size_t)(i0 + c) * st;
+            zn[c] = rhs(i0 + c + 1);
+            lv[c] = lm[o];
+            sv[c] = sw[o];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < kIvChunk; ++c) {
+          if (c < n) {
+            const size_t o = (size_t)(i0 + c) * st;
+            if (sv[c] == 0.0) {
+              zz[o] = cb;
+              cb = zn[c] - lv[c] * cb;
+            } else {
+              zz[o] = zn[c];
+              cb = cb - lv[c] * zn[c];
+            }
+          }
         }
       }
-      z[m - 1] = cb;
-      // back substitution with U (diagonal + two superdiagonals)
-      for (int i = m - 1; i >= 0; --i) {
-        double s = z[i];
-        if (i + 1 < m) s -= u1[i] * z[i + 1];
-        if (i + 2 < m) s -= u2[i] * z[i + 2];
-        z[i] = s / u0[i];
+      zz[(size_t)(m - 1) * st] = cb;
+      // back substitution with U (diagonal + two superdiagonals), z[i+1], z[i+2] carried; the
+      // squared norm and the entry of largest magnitude (first in index order) on the way
+      double zp1 = 0.0, zp2 = 0.0, nrm = 0.0, big = -1.0, bigv = 0.0;
+      for (int i1 = m; i1 > 0; i1 -= kIvChunk) {
+        const int n = min(kIvChunk, i1);
+        double zr[kIvChunk], d0[kIvChunk], d1[kIvChunk], d2[kIvChunk];
+#pragma unroll
+        for (int c = 0; c < kIvChunk; ++c) {
+          if (c < n) {
+            const size_t o = (size_t)(i1 - 1 - c) * st;
+            zr[c] = zz[o];
+            d0[c] = u0[o];
+            d1[c] = u1[o];
+            d2[c] = u2[o];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < kIvChunk; ++c) {
+          if (c < n) {
+            const double x = (zr[c] - d1[c] * zp1 - d2[c] * zp2) / d0[c];
+            zz[(size_t)(i1 - 1 - c) * st] = x;
+            nrm += x * x;
+            if (fabs(x) >= big) { big = fabs(x); bigv = x; }
+            zp2 = zp1;
+            zp1 = x;
+          }
+        }
       }
-      // modified Gram-Schmidt against the group's earlier vectors, then normalise
-      for (int q = j; q < p; ++q) {
-        const double* zq = Z + (size_t)q * m;
-        double dot = 0.0;
-        for (int i = 0; i < m; ++i) dot += zq[i] * z[i];
-        for (int i = 0; i < m; ++i) z[i] -= dot * zq[i];
+      if (p > j) {
+        // modified Gram-Schmidt against the group's earlier vectors, then the norm again
+        for (int q = j; q < p; ++q) {
+          const double* zq = Z + (size_t)q * m;
+          double dot = 0.0;
+#pragma unroll 8
+          for (int i = 0; i < m; ++i) dot += zq[i] * zz[(size_t)i * st];
+#pragma unroll 8
+          for (int i = 0; i < m; ++i) zz[(size_t)i * st] -= dot * zq[i];
+        }
+        nrm = 0.0;
+        big = -1.0;
+        bigv = 0.0;
+#pragma unroll 8
+        for (int i = 0; i < m; ++i) {
+          const double zi = zz[(size_t)i * st];
+          nrm += zi * zi;
+          if (fabs(zi) > big) { big = fabs(zi); bigv = zi; }
+        }
       }
-      double nrm = 0.0, big = 0.0;
-      int ib = 0;
-      for (int i = 0; i < m; ++i) {
-        nrm += z[i] * z[i];
-        if (fabs(z[i]) > big) { big = fabs(z[i]); ib = i; }
-      }
-      double sc = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
-      if (z[ib] < 0.0) sc = -sc;
-      for (int i = 0; i < m; ++i) z[i] *= sc;
+      scl = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
+      if (bigv < 0.0) scl = -scl;
     }
+    double* z = Z + (size_t)p * m;
+#pragma unroll 8
+    for (int i = 0; i < m; ++i) z[i] = zz[(size_t)i * st] * scl;
   }
 }
 
@@ -722,7 +797,7 @@ static size_t wy_elems(int m, int nev) {
 size_t heev_work_bytes(int m, int nev) {
   const size_t mm = (size_t)m;
   return 256 * 9 + sizeof(double) * (3 * mm + 1) + sizeof(double2) * (1 + 2 * kHtMaxSplit) * mm + sizeof(double) * mm * nev +
-         sizeof(double) * 5 * mm * nev + sizeof(double2) * wy_elems(m, nev);
+         sizeof(double) * 6 * mm * nev + sizeof(double2) * wy_elems(m, nev);
 }
 
 void heev_bind(HeevWork& w, void* base, int m, int nev) {
@@ -736,7 +811,7 @@ void heev_bind(HeevWork& w, void* base, int m, int nev) {
   w.tau = (double2*)take(sizeof(double2) * m);
   w.y = (double2*)take(sizeof(double2) * m * 2 * kHtMaxSplit);  // two halves for the one-barrier form
   w.z = (double*)take(sizeof(double) * (size_t)m * nev);
-  w.lu = (double*)take(sizeof(double) * 5 * (size_t)m * nev);
+  w.lu = (double*)take(sizeof(double) * 6 * (size_t)m * nev);
   w.wy_ws_elems = wy_ws_elems(nev);
   w.wy = (double2*)take(sizeof(double2) * wy_elems(m, nev));
   w.m_cap = m;
@@ -772,7 +847,7 @@ int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde,
   DFT_CUDA_TRY(cudaMemsetAsync(w.bar, 0, 2 * sizeof(unsigned), s));
   DFT_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), s));
   if (m > 1) {
-    GridBarrier bar{w.bar, w.bar + 1, status, 0};
+    GridBarrier bar{w.bar, status, 0};
     // enough warps for kHtMaxSplit per column at the start, at most one block per SM
     // (DFTCUDA_HETRD_BPS=2 allows two where they fit, for measurements)
     static const int bps = [] {

@@ -17,7 +17,9 @@
 // (one minus the squared cosine between the preconditioned residual and the ideal correction).
 // One CTA per band for the forward sums; the backward pass recomputes the activations per tile of
 // 128 plane waves and accumulates the weight gradients as small tile GEMMs in registers.
+#include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <vector>
 
 #include "kctx.cuh"
@@ -111,23 +113,127 @@ __global__ void k_precondition_tpa(double2* __restrict__ Q, const double2* __res
   Q[idx] = make_double2(v.x * f, v.y * f);
 }
 
-__global__ void __launch_bounds__(256) k_precondition_mlp(double2* __restrict__ Q, const double2* __restrict__ res,
-                                                          const double* __restrict__ kin, const double* __restrict__ ekin,
-                                                          const double* __restrict__ norms, const int* __restrict__ band,
-                                                          int k, long n, double t, const float* __restrict__ params) {
-  __shared__ float p[MLP_NPARAM];
-  for (int i = threadIdx.x; i < MLP_NPARAM; i += blockDim.x) p[i] = params[i];
-  __syncthreads();
-  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (idx >= (long)k * n) return;
-  const int j = (int)(idx / n);
-  const long i = idx - (long)j * n;
-  const int b = band[j];
-  const double2 v = res[(long)b * n + i];
-  float u[3];
-  mlp_features(kin[i], ekin[j], sqrt(v.x * v.x + v.y * v.y), norms[b] / sqrt((double)n), t, u);
-  const double m = mlp_multiplier(u[0], mlp_forward(p, u, nullptr, nullptr));
-  Q[idx] = make_double2(v.x * m, v.y * m);
+// Inference (the Davidson preconditioner) over tiles of MLP_TE plane-wave entries.  The first layer
+// per entry, then the 64 x 64 second layer on the tensor cores (mma.sync m16n8k8, TF32 operands,
+// FP32 accumulation; each warp takes 16 entries x 64 hidden units), its tanh and the output layer on
+// the accumulator fragments, and a shuffle sum over the four lanes that share an entry.  TF32
+// operands and the hardware tanh (tanh.approx.f32) move the learned multiplier by ~1e-3 relative
+// from the FP32 network of mlp_forward (the training kernels); a preconditioner only steers the
+// Davidson corrections, so the eigenpairs it converges to are unchanged.
+constexpr int MLP_TE = 128;             // entries per tile
+constexpr int MLP_IT = 256;             // threads: 8 warps x 16 entries
+constexpr int MLP_AS = MLP_TE + 8;      // activation row stride (conflict-free fragment loads)
+constexpr int MLP_WS = MLP_H + 8;       // transposed-weight row stride
+struct MlpInferSmem {
+  uint32_t a[MLP_H][MLP_AS];    // first-layer activations (TF32 bits), hidden unit major
+  uint32_t w2t[MLP_H][MLP_WS];  // W2 transposed (TF32 bits): w2t[i][j] = W2[j][i]
+  float w1[MLP_H * MLP_IN], b1[MLP_H], b2[MLP_H], w3[MLP_H];
+  float u0[MLP_TE];
+  double m[MLP_TE];
+};
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float tanh_hw(float x) {
+  float r;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+__global__ void __launch_bounds__(MLP_IT) k_precondition_mlp(double2* __restrict__ Q, const double2* __restrict__ res,
+                                                             const double* __restrict__ kin, const double* __restrict__ ekin,
+                                                             const double* __restrict__ norms, const int* __restrict__ band,
+                                                             int k, long n, double t, const float* __restrict__ params) {
+  extern __shared__ __align__(16) unsigned char mlp_smraw[];
+  MlpInferSmem& S = *reinterpret_cast<MlpInferSmem*>(mlp_smraw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int q = tid; q < MLP_H * MLP_H; q += MLP_IT) {
+    const int j = q / MLP_H, i = q - j * MLP_H;
+    S.w2t[i][j] = to_tf32(params[MLP_OFF_W2 + q]);
+  }
+  for (int q = tid; q < MLP_H * MLP_IN; q += MLP_IT) S.w1[q] = params[MLP_OFF_W1 + q];
+  for (int q = tid; q < MLP_H; q += MLP_IT) {
+    S.b1[q] = params[MLP_OFF_B1 + q];
+    S.b2[q] = params[MLP_OFF_B2 + q];
+    S.w3[q] = params[MLP_OFF_W3 + q];
+  }
+  const float b3 = params[MLP_OFF_B3];
+  const long total = (long)k * n;
+  const int e1 = tid % MLP_TE, half = tid / MLP_TE;  // first layer: entry, half of the hidden units
+  const int g = lane >> 2, tq = lane & 3;            // mma fragment coordinates
+  const int e0 = warp * 16;                          // this warp's entries in the tile
+  for (long base = (long)blockIdx.x * MLP_TE; base < total; base += (long)gridDim.x * MLP_TE) {
+    __syncthreads();  // the previous tile's shared data is consumed
+    {
+      const long idx = base + e1;
+      float u[3] = {0.f, 0.f, 0.f};
+      if (idx < total) {
+        const int j = (int)(idx / n);
+        const long i = idx - (long)j * n;
+        const int b = band[j];
+        const double2 v = res[(long)b * n + i];
+        mlp_features(kin[i], ekin[j], sqrt(v.x * v.x + v.y * v.y), norms[b] / sqrt((double)n), t, u);
+      }
+      if (half == 0) S.u0[e1] = u[0];
+#pragma unroll 4
+      for (int h = half * (MLP_H / 2); h < (half + 1) * (MLP_H / 2); ++h) {
+        const float* w = S.w1 + h * MLP_IN;
+        S.a[h][e1] = to_tf32(tanh_hw(fmaf(w[0], u[0], fmaf(w[1], u[1], fmaf(w[2], u[2], S.b1[h])))));
+      }
+    }
+    __syncthreads();
+    // A fragments of the warp's 16 entries for the eight k steps
+    uint32_t af[8][4];
+#pragma unroll
+    for (int ks = 0; ks < 8; ++ks) {
+      af[ks][0] = S.a[8 * ks + tq][e0 + g];
+      af[ks][1] = S.a[8 * ks + tq][e0 + g + 8];
+      af[ks][2] = S.a[8 * ks + tq + 4][e0 + g];
+      af[ks][3] = S.a[8 * ks + tq + 4][e0 + g + 8];
+    }
+    float zlo = 0.f, zhi = 0.f;  // output-layer partial sums of entries e0 + g and e0 + g + 8
+#pragma unroll 2
+    for (int nt = 0; nt < 8; ++nt) {
+      float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int ks = 0; ks < 8; ++ks) {
+        const uint32_t b0 = S.w2t[8 * ks + tq][8 * nt + g], b1 = S.w2t[8 * ks + tq + 4][8 * nt + g];
+        asm volatile(
+            "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+            "{%0, %1, %2, %3};"
+            : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+            : "r"(af[ks][0]), "r"(af[ks][1]), "r"(af[ks][2]), "r"(af[ks][3]), "r"(b0), "r"(b1));
+      }
+      const int j0 = 8 * nt + 2 * tq;
+      zlo = fmaf(S.w3[j0], tanh_hw(c[0] + S.b2[j0]), zlo);
+      zlo = fmaf(S.w3[j0 + 1], tanh_hw(c[1] + S.b2[j0 + 1]), zlo);
+      zhi = fmaf(S.w3[j0], tanh_hw(c[2] + S.b2[j0]), zhi);
+      zhi = fmaf(S.w3[j0 + 1], tanh_hw(c[3] + S.b2[j0 + 1]), zhi);
+    }
+    zlo += __shfl_xor_sync(0xffffffffu, zlo, 1);
+    zlo += __shfl_xor_sync(0xffffffffu, zlo, 2);
+    zhi += __shfl_xor_sync(0xffffffffu, zhi, 1);
+    zhi += __shfl_xor_sync(0xffffffffu, zhi, 2);
+    if (tq == 0) {
+      S.m[e0 + g] = mlp_multiplier(S.u0[e0 + g], zlo + b3);
+      S.m[e0 + g + 8] = mlp_multiplier(S.u0[e0 + g + 8], zhi + b3);
+    }
+    __syncthreads();
+    // scale the residual entries (two threads per entry: real and imaginary parts)
+    {
+      const int e = tid >> 1, part = tid & 1;
+      const long idx = base + e;
+      if (idx < total) {
+        const int j = (int)(idx / n);
+        const long i = idx - (long)j * n;
+        const double* src = reinterpret_cast<const double*>(res + (long)band[j] * n + i);
+        reinterpret_cast<double*>(Q + idx)[part] = src[part] * S.m[e];
+      }
+    }
+  }
 }
 
 // The reference preconditioner (eig.cu).
@@ -460,8 +566,21 @@ int precondition_launch(dftcuda_kctx* c, double2* Q, const double2* res, const d
     count_launch();
     if (c->precond_kind == DFTCUDA_PRECOND_TPA)
       k_precondition_tpa<<<grid, 256, 0, s>>>(Q, res, kin, ekin_ws, band, take, n);
-    else
-      k_precondition_mlp<<<grid, 256, 0, s>>>(Q, res, kin, ekin_ws, norms, band, take, n, t, c->d_mlp);
+    else {
+      // tiles of MLP_TE entries, up to eight blocks per SM (about three resident)
+      int dev = 0, nsm = 148;
+      DFT_CUDA_TRY(cudaGetDevice(&dev));
+      DFT_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+      static int attr_dev = -1;
+      if (attr_dev != dev) {
+        DFT_CUDA_TRY(cudaFuncSetAttribute(k_precondition_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)sizeof(MlpInferSmem)));
+        attr_dev = dev;
+      }
+      const size_t tiles = ((size_t)take * n + MLP_TE - 1) / MLP_TE;
+      const unsigned g = (unsigned)std::min<size_t>(tiles, (size_t)nsm * 8);
+      k_precondition_mlp<<<g, MLP_IT, sizeof(MlpInferSmem), s>>>(Q, res, kin, ekin_ws, norms, band, take, n, t, c->d_mlp);
+    }
     count_launch();
   }
   DFT_CUDA_TRY(cudaGetLastError());
