@@ -677,42 +677,89 @@ __global__ void k_wy_v(const double2* __restrict__ A, int m, int k0, int nb, dou
   Vb[idx] = v;
 }
 
-// T (ld kWyB) from G = V^H V (ld kWyB) and tau[k0 ...]: one CTA of 4 x kWyB threads, G and T in
-// shared memory.  Column j needs the triangular product T[0:j, 0:j] G[0:j, j]; its row i is summed
-// by the four consecutive lanes of row group i (terms l = i + q, i + q + 4, ...) and two shuffles.
+// Every block's triangular factor at once (the factors depend on the reflectors only): CTA b
+// forms G = V_b^H V_b for reflectors k0 = b kWyB .. k0 + nb - 1 straight from the factored matrix
+// (v_k = 1 at row k+1, A[row, k] below, 0 above), 4 x 4 outputs per thread (rows tr + 16 q,
+// columns tc + 16 q) over row chunks staged in shared memory, then T_b (ld kWyB, at T + b kWyB^2) by the zlarft recurrence: column j needs
+// T[0:j, 0:j] G[0:j, j]; its row i is summed by the four consecutive lanes of row group i and two
+// shuffles.
 constexpr int kWyTThreads = 4 * kWyB;
-constexpr size_t kWyTSmem = sizeof(double2) * 2 * kWyB * (kWyB + 1);
-__global__ void __launch_bounds__(kWyTThreads) k_wy_t(const double2* __restrict__ G, const double2* __restrict__ tau, int k0,
-                                                      int nb, double2* __restrict__ T) {
+constexpr int kWyRows = 32;  // reflector rows per staged chunk
+struct WyTSmem {
+  double2 gs[kWyB][kWyB + 1];  // gs[col][row]
+  double2 ts[kWyB][kWyB + 1];  // ts[col][row]
+  double2 vc[kWyRows][kWyB + 1];  // a chunk of V_b's rows
+};
+constexpr size_t kWyTSmem = sizeof(WyTSmem);
+__global__ void __launch_bounds__(kWyTThreads) k_wy_t_all(const double2* __restrict__ A, int m, const double2* __restrict__ tau,
+                                                          int nref, double2* __restrict__ T) {
   extern __shared__ __align__(16) unsigned char wsm[];
-  double2(*gs)[kWyB + 1] = reinterpret_cast<double2(*)[kWyB + 1]>(wsm);  // gs[col][row]
-  double2(*ts)[kWyB + 1] = gs + kWyB;                                   // ts[col][row]
+  WyTSmem& S = *reinterpret_cast<WyTSmem*>(wsm);
   const int tid = threadIdx.x;
-  for (int idx = tid; idx < kWyB * kWyB; idx += kWyTThreads) {
-    const int r = idx % kWyB, c = idx / kWyB;
-    gs[c][r] = (r < nb && c < nb) ? G[r + c * kWyB] : make_double2(0.0, 0.0);
-    ts[c][r] = make_double2(0.0, 0.0);
+  const int k0 = blockIdx.x * kWyB, nb = min(kWyB, nref - k0);
+  const int tr = tid >> 4, tc = tid & 15;  // G tile: rows tr + 16 q, columns tc + 16 q
+  double2 acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[r][c] = make_double2(0.0, 0.0);
+  for (int row0 = k0 + 1; row0 < m; row0 += kWyRows) {
+    __syncthreads();
+    for (int idx = tid; idx < kWyRows * kWyB; idx += kWyTThreads) {  // along each reflector's rows
+      const int j = idx / kWyRows, rr = idx - j * kWyRows, row = row0 + rr, k = k0 + j;
+      double2 v = make_double2(0.0, 0.0);
+      if (j < nb && row < m) {
+        if (row == k + 1) v = make_double2(1.0, 0.0);
+        else if (row > k + 1) v = A[row + (long)k * m];
+      }
+      S.vc[rr][j] = v;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int rr = 0; rr < kWyRows; ++rr) {
+      double2 vr[4], vcol[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        vr[q] = S.vc[rr][tr + 16 * q];
+        vcol[q] = S.vc[rr][tc + 16 * q];
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {  // acc += conj(vr) vcol
+          acc[r][c].x += vr[r].x * vcol[c].x + vr[r].y * vcol[c].y;
+          acc[r][c].y += vr[r].x * vcol[c].y - vr[r].y * vcol[c].x;
+        }
+    }
   }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      S.gs[tc + 16 * c][tr + 16 * r] = acc[r][c];
+      S.ts[tc + 16 * c][tr + 16 * r] = make_double2(0.0, 0.0);
+    }
   __syncthreads();
   const int i = tid >> 2, q = tid & 3;
   for (int j = 0; j < nb; ++j) {
     double2 sum = make_double2(0.0, 0.0);
     if (i < j)
-      for (int l = i + q; l < j; l += 4) sum = cadd(sum, cmul(ts[l][i], gs[j][l]));
+      for (int l = i + q; l < j; l += 4) sum = cadd(sum, cmul(S.ts[l][i], S.gs[j][l]));
     sum.x += __shfl_xor_sync(0xffffffffu, sum.x, 1);
     sum.y += __shfl_xor_sync(0xffffffffu, sum.y, 1);
     sum.x += __shfl_xor_sync(0xffffffffu, sum.x, 2);
     sum.y += __shfl_xor_sync(0xffffffffu, sum.y, 2);
     if (q == 0) {
       const double2 tj = tau[k0 + j];
-      if (i < j) ts[j][i] = cscale(cmul(tj, sum), -1.0);
-      else if (i == j) ts[j][i] = tj;
+      if (i < j) S.ts[j][i] = cscale(cmul(tj, sum), -1.0);
+      else if (i == j) S.ts[j][i] = tj;
     }
     __syncthreads();
   }
+  double2* Tb = T + (size_t)blockIdx.x * kWyB * kWyB;
   for (int idx = tid; idx < kWyB * kWyB; idx += kWyTThreads) {
     const int r = idx % kWyB, c = idx / kWyB;
-    T[r + c * kWyB] = ts[c][r];
+    Tb[r + c * kWyB] = S.ts[c][r];
   }
 }
 
@@ -725,41 +772,33 @@ __global__ void k_real_to_complex(const double* __restrict__ Z, int m, int nev, 
 
 int heev_back_blocked(const double2* A, const double2* tau, int m, int nev, const double* Z, double2* E, long lde,
                       const HeevWork& w, cudaStream_t s) {
+  const int nref = m - 1;
+  const int nblk = (nref + kWyB - 1) / kWyB;
   double2* Vb = w.wy;
-  double2* G = Vb + (size_t)m * kWyB;
-  double2* T = G + kWyB * kWyB;
-  double2* W = T + kWyB * kWyB;
+  double2* T = Vb + (size_t)m * kWyB;  // nblk triangular factors
+  double2* W = T + (size_t)nblk * kWyB * kWyB;
   double2* W2 = W + (size_t)kWyB * nev;
   double2* ws = W2 + (size_t)kWyB * nev;
   k_real_to_complex<<<ceil_div((size_t)m * nev, 256), 256, 0, s>>>(Z, m, nev, E, lde);
   count_launch();
-  const int nref = m - 1;
-  const int nblk = (nref + kWyB - 1) / kWyB;
+  k_wy_t_all<<<nblk, kWyTThreads, kWyTSmem, s>>>(A, m, tau, nref, T);
+  count_launch();
   for (int b = nblk - 1; b >= 0; --b) {
     const int k0 = b * kWyB, nb = std::min(kWyB, nref - k0);
     const int rows = m - k0 - 1;  // rows k0+1 .. m-1 hold the block's reflectors
     k_wy_v<<<ceil_div((size_t)m * nb, 256), 256, 0, s>>>(A, m, k0, nb, Vb);
     count_launch();
-    GemmArgs g{};
-    // G = V^H V
-    g.M = nb; g.N = nb; g.K = rows;
-    g.A = Vb + k0 + 1; g.lda = m; g.a_kc = true; g.conj_a = true;
-    g.B = Vb + k0 + 1; g.ldb = m; g.b_kc = true; g.conj_b = false;
-    g.O = G; g.ldo_r = 1; g.ldo_c = kWyB; g.alpha = 1.0; g.beta = 0.0;
-    DFT_TRY(zgemm(g, s, ws, w.wy_ws_elems));
-    k_wy_t<<<1, kWyTThreads, kWyTSmem, s>>>(G, tau, k0, nb, T);
-    count_launch();
     // W = V^H E
-    g = GemmArgs{};
+    GemmArgs g{};
     g.M = nb; g.N = nev; g.K = rows;
     g.A = Vb + k0 + 1; g.lda = m; g.a_kc = true; g.conj_a = true;
     g.B = E + k0 + 1; g.ldb = lde; g.b_kc = true; g.conj_b = false;
     g.O = W; g.ldo_r = 1; g.ldo_c = kWyB; g.alpha = 1.0; g.beta = 0.0;
     DFT_TRY(zgemm(g, s, ws, w.wy_ws_elems));
-    // W2 = T W
+    // W2 = T_b W
     g = GemmArgs{};
     g.M = nb; g.N = nev; g.K = nb;
-    g.A = T; g.lda = kWyB; g.a_kc = false; g.conj_a = false;
+    g.A = T + (size_t)b * kWyB * kWyB; g.lda = kWyB; g.a_kc = false; g.conj_a = false;
     g.B = W; g.ldb = kWyB; g.b_kc = true; g.conj_b = false;
     g.O = W2; g.ldo_r = 1; g.ldo_c = kWyB; g.alpha = 1.0; g.beta = 0.0;
     DFT_TRY(zgemm(g, s, ws, w.wy_ws_elems));
@@ -791,7 +830,8 @@ __global__ void k_upper_to_full(const double2* __restrict__ src, long lds, doubl
 // Split-K space of the blocked back-transformation's GEMMs: up to 32 partial kWyB x nev products.
 static size_t wy_ws_elems(int nev) { return (size_t)32 * kWyB * std::max(nev, kWyB); }
 static size_t wy_elems(int m, int nev) {
-  return (size_t)m * kWyB + 2 * kWyB * kWyB + 2 * (size_t)kWyB * nev + wy_ws_elems(nev);
+  const size_t nblk = (size_t)(std::max(m - 1, 1) + kWyB - 1) / kWyB;
+  return (size_t)m * kWyB + nblk * kWyB * kWyB + 2 * (size_t)kWyB * nev + wy_ws_elems(nev);
 }
 
 size_t heev_work_bytes(int m, int nev) {
@@ -838,7 +878,7 @@ int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde,
     DFT_CUDA_TRY(cudaFuncSetAttribute(hetrd_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tr));
     DFT_CUDA_TRY(cudaFuncSetAttribute(k_hetrd_back, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(sizeof(double2) * BT_WARPS * 2048)));
-    DFT_CUDA_TRY(cudaFuncSetAttribute(k_wy_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWyTSmem));
+    DFT_CUDA_TRY(cudaFuncSetAttribute(k_wy_t_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWyTSmem));
     DFT_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
     DFT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_fn, HT_THREADS, smem_tr));
     attr_dev = dev;
