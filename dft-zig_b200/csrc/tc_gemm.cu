@@ -551,8 +551,9 @@ __global__ void __launch_bounds__(T2_THREADS) k_cgemm_tc2(int M, int N, int K, c
 // issues one 8-deep K step per slot (12 MMAs for 3xTF32, 4 otherwise) of 128 x 256 x 8, committing
 // each slot back to its "empty" mbarrier.  TMEM holds the two 256-column FP32 accumulators (all 512
 // columns; the shared-memory footprint keeps one CTA per SM).  Waits are bounded; a timeout sets the
-// error flag and every role winds down (no asynchronous copies are used, so only the MMAs in flight
-// are waited for before the TMEM is freed).
+// error flag and every role winds down: each converter thread waits for its own staging copies
+// (cp.async.wait_all) before it leaves, and one final commit is waited for so that no MMA is in
+// flight when the TMEM is freed.
 constexpr int T3_N = 256;
 constexpr int T3_K = 8;
 constexpr int T3_CONV_WARPS = 8;
