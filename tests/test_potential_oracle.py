@@ -109,6 +109,17 @@ def test_pbe_derivatives_match_finite_differences():
     assert np.all(np.abs(f0 - op.lda_pz(n)[0]) < 0.05 * np.abs(f0))
 
 
+def test_pbe_matches_the_reference_libxc_point():
+    """The reference's own PBE known-answer tests (xc/xc.zig:1048-1108): libxc values at n = 0.1,
+    sigma = |grad n|^2 = 0.01 (Hartree).  The oracle returns the exchange + correlation total in Ry;
+    the reference checks the totals of e_xc and v_sigma to 1e-4 and the correlation v_rho to 1e-3."""
+    f, vn, vg = op.pbe(np.array([0.1]), np.array([0.01]))
+    exc_ha, vrho_ha, vsigma_ha = f[0] / 0.1 / 2.0, vn[0] / 2.0, vg[0] / 2.0
+    assert abs(exc_ha - (-0.3516400536 + -0.0452782280)) <= 1e-4 * 0.3969182816
+    assert abs(vsigma_ha - (-0.0854846156 + 0.0697928401)) <= 1e-4 * 0.0156917755
+    assert abs(vrho_ha - (-0.4460575074 + -0.0688510243)) <= 1e-3 * 0.0688510243
+
+
 def test_gga_potential_is_the_functional_derivative():
     """E_xc[n + e dn] - E_xc[n - e dn] = 2 e (vol/N) sum V_xc dn for the PBE assembly (gradient and
     divergence by FFT): the sign and the factor 2 of the divergence term."""

@@ -33,6 +33,30 @@ def test_ewald_graphene_golden():
     assert abs(e_ha - 50.1056) / 50.1056 < 0.01
 
 
+def test_ewald_cscl_madelung_and_forces():
+    """The cell of the reference's Ewald force tests (ewald/ewald.zig:608-700): charges +1 / -1 at the
+    corner and the body centre of a 5 bohr cube.  Its energy is the CsCl Madelung energy
+    -alpha / d Ha per cell (alpha = 1.762675, d = a sqrt(3) / 2); the forces, taken off the symmetric
+    site, are minus the finite-difference energy gradient (h = 1e-5) and sum to zero."""
+    a = 5.0
+    cell = np.eye(3) * a
+    z = np.array([1.0, -1.0])
+    pos = np.array([[0.0, 0.0, 0.0], [a / 2, a / 2, a / 2]])
+    e_ha = scf.ewald_energy(cell, z, pos) / 2.0
+    assert abs(e_ha - (-1.76267477307099 / (a * math.sqrt(3.0) / 2.0))) < 1e-10
+    pos = pos + np.array([[0.0, 0.0, 0.0], [0.31, -0.12, 0.05]])
+    f = scf.ewald_forces(cell, z, pos)
+    h = 1e-5
+    for atom in range(2):
+        for d in range(3):
+            pp, pm = pos.copy(), pos.copy()
+            pp[atom, d] += h
+            pm[atom, d] -= h
+            fd = -(scf.ewald_energy(cell, z, pp) - scf.ewald_energy(cell, z, pm)) / (2 * h)
+            assert abs(f[atom, d] - fd) < 1e-6 * max(1.0, abs(fd))
+    assert np.abs(f.sum(axis=0)).max() < 1e-10
+
+
 def test_ewald_independent_of_split():
     c = system.crystal("si8")
     z = np.array([4.0] * 8)
