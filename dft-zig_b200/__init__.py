@@ -73,6 +73,7 @@ ABI_SYMBOLS = (
     "dftcuda_local_forces",
     "dftcuda_nonlocal_forces",
     "dftcuda_radial_table",
+    "dftcuda_symmetrize_density",
 )
 
 PRECOND_REFERENCE = 0  # r / (|k+G|^2 - lambda), lobpcg/common.zig:214-226
@@ -244,6 +245,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.dftcuda_local_forces.argtypes = [vp, ip, vp, ip, vp, vp, ct.c_double, dp, dp]
     lib.dftcuda_nonlocal_forces.argtypes = [vp, dp, sz, sz, dp, dp]
     lib.dftcuda_radial_table.argtypes = [ip, sz, dp, dp, dp, sz, ct.c_double, dp]
+    lib.dftcuda_symmetrize_density.argtypes = [vp, ip, vp, vp, vp]
     lb = ct.c_long
     lib.dftcuda_complex_gemm.argtypes = [ip, sz, sz, sz, vp, lb, ip, ip, vp, lb, ip, ip, vp, lb, lb, ct.c_double, ct.c_double]
     _lib = lib
@@ -661,6 +663,16 @@ class PotentialContext:
             out = self._out_like(v_g, (self.N,), np.float64)
         _check(load_library().dftcuda_potential_real(self._h, _ptr(v_g), _ptr(vloc) if vloc is not None else None, _ptr(out)))
         return out
+
+    def symmetrize(self, rho, ops):
+        """Density symmetrisation in place (dftcuda_symmetrize_density): ops is a list of
+        (rot, k_rot, trans) or of (k_rot, trans), k_rot acting on Miller indices, trans fractional."""
+        rho = _as_array(rho, np.float64, self.N)
+        kr = np.ascontiguousarray([np.asarray(o[-2], dtype=np.int32).reshape(9) for o in ops], dtype=np.int32).reshape(-1)
+        tr = np.ascontiguousarray([np.asarray(o[-1], dtype=np.float64).reshape(3) for o in ops], dtype=np.float64).reshape(-1)
+        _check(load_library().dftcuda_symmetrize_density(self._h, len(ops), kr.ctypes.data if kr.size else None,
+                                                         tr.ctypes.data if tr.size else None, _ptr(rho)))
+        return rho
 
     def pulay_mix(self, x, residual, beta: float):
         """Pulay step in place on x (float64, any length; complex arrays as their interleaved view)."""

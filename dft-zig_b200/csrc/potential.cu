@@ -446,6 +446,51 @@ __global__ void __launch_bounds__(kPotThreads) k_radial_table(int l, int nr, con
   if (threadIdx.x == 0) out[blockIdx.x] = s;
 }
 
+// ---- density symmetrisation (symmetrize_density, scf/density_symmetry.zig:27-94) ----
+// out(G) = (1/nops) sum_op in(k_rot G) e^{-2 pi i frac(G . t)}, G the signed Miller indices of the
+// box (index i <-> i if i <= (n-1)/2, else i - n), the rotated G wrapped into the box, the phase
+// only where frac(G . t) is more than 1e-12 from an integer.  One thread per output G; the
+// operations are staged in shared memory (k_rot as 9 ints row-major, t fractional).
+constexpr int kSymMaxOps = 192;  // a cubic conventional cell: 48 rotations x 4 centring translations
+__device__ __forceinline__ int sym_freq(int i, int n) { return i <= (n - 1) / 2 ? i : i - n; }
+__device__ __forceinline__ int sym_wrap(int g, int n) {
+  const int r = g % n;
+  return r < 0 ? r + n : r;
+}
+__global__ void __launch_bounds__(kPotThreads) k_sym_density(const double2* __restrict__ in, int nx, int ny, int nz, int nops,
+                                                             const int* __restrict__ k_rot, const double* __restrict__ trans,
+                                                             double2* __restrict__ out) {
+  __shared__ int skr[kSymMaxOps * 9];
+  __shared__ double st[kSymMaxOps * 3];
+  for (int q = threadIdx.x; q < nops * 9; q += blockDim.x) skr[q] = k_rot[q];
+  for (int q = threadIdx.x; q < nops * 3; q += blockDim.x) st[q] = trans[q];
+  __syncthreads();
+  const long N = (long)nx * ny * nz;
+  const double inv = 1.0 / (double)nops;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < N; idx += (long)gridDim.x * blockDim.x) {
+    const int x = (int)(idx % nx), y = (int)((idx / nx) % ny), z = (int)(idx / ((long)nx * ny));
+    const int h = sym_freq(x, nx), k = sym_freq(y, ny), l = sym_freq(z, nz);
+    double2 sum = make_double2(0.0, 0.0);
+    for (int o = 0; o < nops; ++o) {
+      const int* m = skr + 9 * o;
+      const int ix = sym_wrap(m[0] * h + m[1] * k + m[2] * l, nx);
+      const int iy = sym_wrap(m[3] * h + m[4] * k + m[5] * l, ny);
+      const int iz = sym_wrap(m[6] * h + m[7] * k + m[8] * l, nz);
+      double2 term = in[ix + (long)nx * (iy + (long)ny * iz)];
+      const double dot = (double)h * st[3 * o] + (double)k * st[3 * o + 1] + (double)l * st[3 * o + 2];
+      const double fr = dot - floor(dot);
+      if (fr > 1e-12 && fr < 1.0 - 1e-12) {
+        double sn, cs;
+        sincospi(-2.0 * fr, &sn, &cs);
+        term = make_double2(term.x * cs - term.y * sn, term.x * sn + term.y * cs);
+      }
+      sum.x += term.x;
+      sum.y += term.y;
+    }
+    out[idx] = make_double2(sum.x * inv, sum.y * inv);
+  }
+}
+
 // out_r = vloc + Re(v) * N (v holds FFT^-1 / N of the G-space field).
 __global__ void k_pot_real(const double2* __restrict__ v, const double* __restrict__ vloc, long N, double* __restrict__ out) {
   const double scale = (double)N;
@@ -564,6 +609,8 @@ struct dftcuda_pctx {
   double* pr = nullptr;       // n staging (residual)
   int* d_slots = nullptr;
   double* d_coef = nullptr;
+  int* sym_kr = nullptr;      // symmetry operations (kSymMaxOps x 9 ints, x 3 doubles), on first use
+  double* sym_t = nullptr;
   std::vector<int> order;     // slots oldest first
   std::vector<double> B;      // history x history residual overlaps, by slot
 };
@@ -610,7 +657,8 @@ extern "C" int dftcuda_pctx_destroy(dftcuda_pctx* c) {
   for (void* p : {(void*)c->w, (void*)c->gr, (void*)c->vr})
     if (p) cudaFree(p);
   for (void* p : {(void*)c->g2, (void*)c->a, (void*)c->b, (void*)c->rho, (void*)c->vin, (void*)c->vout, (void*)c->part, (void*)c->hx,
-                  (void*)c->hr, (void*)c->px, (void*)c->pr, (void*)c->d_slots, (void*)c->d_coef})
+                  (void*)c->hr, (void*)c->px, (void*)c->pr, (void*)c->d_slots, (void*)c->d_coef, (void*)c->sym_kr,
+                  (void*)c->sym_t})
     if (p) cudaFree(p);
   if (c->h_part) cudaFreeHost(c->h_part);
   if (c->plan) dftcuda_fft_plan_destroy(c->plan);
@@ -746,6 +794,38 @@ extern "C" int dftcuda_potential_real(dftcuda_pctx* c, const double* v_g, const 
   k_pot_real<<<kPotBlocks, kPotThreads, 0, s>>>(c->a, vloc, N, out);
   count_launch();
   if (out != out_r) DFT_TRY(copy_out(out_r, out, sizeof(double) * N, s));
+  DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_symmetrize_density(dftcuda_pctx* c, int nops, const int* k_rot, const double* trans, double* rho_r) {
+  if (!c || !rho_r || nops < 0 || nops > kSymMaxOps || (nops > 1 && (!k_rot || !trans)))
+    return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "symmetrize_density: bad arguments (0..192 operations)");
+  if (nops <= 1) return DFTCUDA_OK;  // the identity alone leaves the density as it is
+  for (int q = 0; q < 3 * nops; ++q)
+    if (!std::isfinite(trans[q])) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "symmetrize_density: non-finite translation");
+  const long N = c->N;
+  cudaStream_t s = c->stream;
+  if (!c->sym_kr) {
+    if (cudaMalloc(&c->sym_kr, sizeof(int) * 9 * kSymMaxOps) != cudaSuccess ||
+        cudaMalloc(&c->sym_t, sizeof(double) * 3 * kSymMaxOps) != cudaSuccess)
+      return fail(DFTCUDA_ERR_CUDA, "symmetrize_density: allocation failed");
+  }
+  DFT_CUDA_TRY(cudaMemcpyAsync(c->sym_kr, k_rot, sizeof(int) * 9 * nops, cudaMemcpyDefault, s));
+  DFT_CUDA_TRY(cudaMemcpyAsync(c->sym_t, trans, sizeof(double) * 3 * nops, cudaMemcpyDefault, s));
+  int st = DFTCUDA_OK;
+  const double* rho = (const double*)device_view(rho_r, c->rho, sizeof(double) * N, s, &st);
+  if (st != DFTCUDA_OK) return st;
+  k_pot_to_complex<<<kPotBlocks, kPotThreads, 0, s>>>(rho, N, c->a);
+  count_launch();
+  DFT_TRY(fft3d_on_stream(c->plan, c->a, -1, s));
+  k_sym_density<<<kPotBlocks, kPotThreads, 0, s>>>(c->a, c->nx, c->ny, c->nz, nops, c->sym_kr, c->sym_t, c->b);
+  count_launch();
+  DFT_TRY(fft3d_on_stream(c->plan, c->b, +1, s));
+  double* out = is_device_pointer(rho_r) ? rho_r : c->rho;
+  k_pot_real_part<<<kPotBlocks, kPotThreads, 0, s>>>(c->b, N, out);
+  count_launch();
+  if (out != rho_r) DFT_TRY(copy_out(rho_r, out, sizeof(double) * N, s));
   DFT_CUDA_TRY(cudaStreamSynchronize(s));
   return DFTCUDA_OK;
 }

@@ -341,6 +341,14 @@ int dftcuda_local_forces(dftcuda_pctx* ctx, int nspecies, const double* gth, int
                          const double* positions, double g2max, const double* rho_r, double* forces);
 int dftcuda_pulay_reset(dftcuda_pctx* ctx);
 
+/* Density symmetrisation (symmetrize_density, scf/density_symmetry.zig:27-94), in place on rho_r
+ * (N doubles, x fastest, host or device): rho(G) <- (1/nops) sum_op rho(k_rot G) e^{-2 pi i frac(G.t)}
+ * over the box's signed Miller indices G, rotated indices wrapped into the box.  k_rot: 9 ints per
+ * operation, row-major (SymOp.k_rot = (rot^-1)^T, symmetry/symmetry.zig:229-233); trans: 3 doubles
+ * per operation, fractional (SymOp.trans).  Host pointers or device.  nops <= 1 leaves rho as it is;
+ * at most 192 operations. */
+int dftcuda_symmetrize_density(dftcuda_pctx* ctx, int nops, const int* k_rot, const double* trans, double* rho_r);
+
 /* Radial projector table of one beta (RadialTableSet.init, pseudopotential/nonlocal.zig:250-338,
  * entries radial_projector, nonlocal.zig:8-21): out[i] = sum_j r_j rbeta_j j_l(q_i r_j) rab_j w_j on
  * q_i = i gmax / (nq - 1), w the composite-trapezoid weights of radial_integration.zig:7-13 and j_l
