@@ -76,6 +76,24 @@ def test_ctrap_weights():
     assert abs(s - spec["exact"]) < spec["tol"]
 
 
+def test_radial_projector_large_g():
+    """src/tests.zig:1108-1145: beta = r exp(-r^2) (stored as r beta) on r = 0, 0.1, .. 9.9 with
+    rab = 0.1; the projector at g = 10 is smaller than at g = 1.  For l = 0 the integral is also
+    known in closed form, sum r (r beta) j0(g r) dr ~ int r^2 e^{-r^2} j0(g r) dr = sqrt(pi)/4
+    e^{-g^2/4}, which the corrected trapezoid rule on this mesh meets to 1e-5 up to g = 4 (8e-7 at
+    g = 0.1, 7e-6 at g = 4, where g dr = 0.4 starts to under-resolve the oscillation of j0)."""
+    r = 0.1 * np.arange(100)
+    rab = np.full(100, 0.1)
+    beta = r * np.exp(-r * r)
+    for l in (0, 1):
+        small = pseudo.radial_projector(beta, r, rab, l, 1.0)
+        large = pseudo.radial_projector(beta, r, rab, l, 10.0)
+        assert abs(large) < abs(small)
+    for g in (0.1, 1.0, 2.0, 4.0):
+        exact = np.sqrt(np.pi) / 4.0 * np.exp(-g * g / 4.0)
+        assert abs(pseudo.radial_projector(beta, r, rab, 0, g) - exact) < 1e-5
+
+
 def test_lcg_stream():
     doc = _json("lcg.json")
     r = lobpcg.Lcg(doc["seed"])
