@@ -273,6 +273,49 @@ def projectors(sp: SpeciesData, kpg: np.ndarray, tables) -> np.ndarray:
     return np.array(rows)
 
 
+def _interp_deriv(table, g):
+    """dR/dq from the table as RadialTable.eval_deriv (pseudopotential/nonlocal.zig:294-299): a central
+    difference of the interpolant with the table step, one-sided below the first step."""
+    _, _, dq = table
+    fwd = (_interp(table, np.full_like(g, dq)) - _interp(table, np.zeros_like(g))) / dq
+    cen = (_interp(table, g + dq) - _interp(table, g - dq)) / (2.0 * dq)
+    return np.where(g < dq, fwd, cen)
+
+
+def _dylm(l, m, v):
+    """Gradient of Y_lm(v / |v|) with respect to v (stress/stress.zig:79-107): zero for l = 0 and at
+    |v| < 1e-15; for l = 1, c (e_j - n n_j) / |v| with Y_1m = c n_j."""
+    out = np.zeros_like(v)
+    if l == 0:
+        return out
+    r = np.sqrt((v * v).sum(axis=1))
+    ok = r >= 1e-15
+    inv = np.where(ok, 1.0 / np.where(ok, r, 1.0), 0.0)
+    u = v * inv[:, None]
+    j = {-1: 1, 0: 2, 1: 0}[m]
+    c = math.sqrt(3.0 / (4 * math.pi))
+    out = -c * u * u[:, j:j + 1]
+    out[:, j] += c
+    return out * inv[:, None]
+
+
+def projector_derivatives(sp: SpeciesData, kpg: np.ndarray, tables) -> np.ndarray:
+    """dphi[m_total, 3, n_pw] = d phi_bm / d q_a = 4 pi (R_b'(|q|) q_a / |q| Y_lm + R_b dY_lm/dq_a) for
+    one species, zero where |q| < 1e-12: the derivative projectors of the nonlocal stress
+    (project_p_and_dp, stress/nonlocal_stress.zig:108-165)."""
+    g = np.sqrt((kpg * kpg).sum(axis=1))
+    live = g >= 1e-12
+    nhat = kpg * np.where(live, 1.0 / np.where(live, g, 1.0), 0.0)[:, None]
+    rows = []
+    for b, (l, _) in enumerate(sp.betas):
+        rad, drad = _interp(tables[b], g), _interp_deriv(tables[b], g)
+        for mi in range(2 * l + 1):
+            y = _ylm(l, mi - l, kpg)
+            d = 4.0 * math.pi * (drad[:, None] * nhat * y[:, None] + rad[:, None] * _dylm(l, mi - l, kpg))
+            rows.append((d * live[:, None]).T)
+    return np.array(rows)
+
+
 def local_potential(c: Crystal, dims, ecut: float) -> np.ndarray:
     """V(r) (Ry) on the x-fastest box from the analytic GTH local form factors, |G|^2 <= 4 ecut, V(0) = 0."""
     nx, ny, nz = dims

@@ -148,6 +148,13 @@ class RadialTable:
         out[g <= 0.0] = self.values[0]
         return out
 
+    def eval_deriv(self, g: np.ndarray) -> np.ndarray:
+        """nonlocal.zig:294-299: central difference of eval with the table step; one-sided below dg."""
+        g = np.asarray(g, dtype=np.float64)
+        fwd = (self.eval(np.full_like(g, self.dg)) - self.eval(np.zeros_like(g))) / self.dg
+        cen = (self.eval(g + self.dg) - self.eval(g - self.dg)) / (2.0 * self.dg)
+        return np.where(g < self.dg, fwd, cen)
+
 
 def real_ylm(l: int, m: int, x, y, z) -> np.ndarray:
     """nonlocal.zig:152-241 (vectorised over points)."""

@@ -69,6 +69,29 @@ def _dp(l_list, dij, p):
     return dp
 
 
+def projector_derivatives(l_list, rad, drad, kpg):
+    """phi_bm(q) = 4 pi R_b(|q|) Y_lm(q) (m_total, n) and dphi_bm/dq_a = 4 pi (R_b' n_a Y_lm +
+    R_b dY_lm/dq_a) (m_total, 3, n), zero where |q| < 1e-12 (project_p_and_dp,
+    nonlocal_stress.zig:108-165); rad(b, q), drad(b, q) give R_b and R_b'."""
+    kpg = np.asarray(kpg, dtype=np.float64)
+    qm = np.sqrt((kpg * kpg).sum(axis=1))
+    live = qm >= 1e-12
+    inv = np.where(live, 1.0 / np.where(live, qm, 1.0), 0.0)
+    nhat = kpg * inv[:, None]
+    offs, mt = _offsets(l_list)
+    phi = np.zeros((mt, len(kpg)))
+    dphi = np.zeros((mt, 3, len(kpg)))
+    for b, l in enumerate(l_list):
+        r, dr = rad(b, qm), drad(b, qm)
+        for mi in range(2 * l + 1):
+            m = mi - l
+            y = real_ylm(l, m, kpg[:, 0], kpg[:, 1], kpg[:, 2])
+            dy = d_ylm_dq(l, m, kpg)
+            phi[offs[b] + mi] = 4.0 * math.pi * r * y
+            dphi[offs[b] + mi] = 4.0 * math.pi * (dr[None, :] * nhat.T * y[None, :] + r[None, :] * dy.T) * live[None, :]
+    return phi, dphi
+
+
 def nonlocal_stress(kpg, gcart, species, atom_species, positions, vectors, weights, volume):
     """sigma_ab (a <= b) = -(2 f_n / Omega^2) sum_G sum_bm dphi_bm/dq_a q_b Re[conj(Dp_bm) S(G) c(G)]
     - delta_ab f_n E_nl,n / Omega over bands n and atoms, with p_bm = sum_G phi_bm(G) S(G) c(G),
@@ -78,26 +101,12 @@ def nonlocal_stress(kpg, gcart, species, atom_species, positions, vectors, weigh
     k weight x spin factor per band (bands with f_n <= 0 are skipped)."""
     kpg = np.asarray(kpg, dtype=np.float64)
     gcart = np.asarray(gcart, dtype=np.float64)
-    qm = np.sqrt((kpg * kpg).sum(axis=1))
-    live = qm >= 1e-12
-    inv = np.where(live, 1.0 / np.where(live, qm, 1.0), 0.0)
-    nhat = kpg * inv[:, None]
     sigma = np.zeros((3, 3))
     vecs = np.asarray(vectors)
     for s, tau in zip(atom_species, np.asarray(positions, dtype=np.float64)):
         l_list, dij, rad, drad = species[s]
         dij = np.asarray(dij, dtype=np.float64)
-        offs, mt = _offsets(l_list)
-        phi = np.zeros((mt, len(kpg)))
-        dphi = np.zeros((mt, 3, len(kpg)))
-        for b, l in enumerate(l_list):
-            r, dr = rad(b, qm), drad(b, qm)
-            for mi in range(2 * l + 1):
-                m = mi - l
-                y = real_ylm(l, m, kpg[:, 0], kpg[:, 1], kpg[:, 2])
-                dy = d_ylm_dq(l, m, kpg)
-                phi[offs[b] + mi] = 4.0 * math.pi * r * y
-                dphi[offs[b] + mi] = 4.0 * math.pi * (dr[None, :] * nhat.T * y[None, :] + r[None, :] * dy.T) * live[None, :]
+        phi, dphi = projector_derivatives(l_list, rad, drad, kpg)
         phase = np.exp(1j * (gcart @ tau))
         for f, c in zip(weights, vecs):
             if f <= 0.0:

@@ -29,6 +29,26 @@ def test_inputs_match_oracle(name, ecut, k):
         assert np.abs(phi - ns.phi).max() < 1e-12 * np.abs(ns.phi).max()
 
 
+@pytest.mark.parametrize("name,k", [("si2", (0.25, 0.125, 0.0)), ("sige8", (0.0, 0.0, 0.0))])
+def test_projector_derivatives_match_oracle(name, k):
+    """The host derivative projectors of the nonlocal stress equal the oracle's (oracle/stress.py,
+    with the oracle's radial tables and RadialTable.eval_deriv), Gamma's q = 0 entry included."""
+    from oracle import pseudo
+    from oracle import stress as ost
+
+    ecut = 20.0
+    c = system.crystal(name, 1)
+    kpg = system.basis(c.recip, ecut, k).kpg
+    oc = cases.make_cell(name, 1)
+    for sp, osp in zip(c.species, oc.species):
+        host = system.projector_derivatives(sp, kpg, [system.radial_table(sp, i, ecut) for i in range(len(sp.betas))])
+        tabs = pseudo.radial_tables(osp, ecut)
+        _, ref = ost.projector_derivatives([l for l, _ in osp.betas], lambda b, q: tabs[b].eval(q),
+                                           lambda b, q: tabs[b].eval_deriv(q), kpg)
+        assert host.shape == ref.shape
+        assert np.abs(host - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
 def test_monkhorst_pack_weights():
     k = system.monkhorst_pack((2, 2, 2))
     assert len(k) == 8 and abs(sum(w for _, w in k) - 1.0) < 1e-15
