@@ -110,6 +110,28 @@ def test_two_rank_kpoint_scf_matches_one_process():
     _check_two_ranks("oracle", OracleBackend, CASES, 1e-10, 1e-9, 1e-10)
 
 
+def test_rank_without_kpoints_follows_the_run():
+    """Gamma only on two ranks: rank 1 owns no k-point, builds no context and solves nothing, yet
+    takes part in every reduction and ends with the same state as rank 0 and the one-process run."""
+    import torch.multiprocessing as mp
+
+    from tests.helpers import OracleBackend
+
+    cases = {"gamma": dict(CASES["fixed"], kmesh=(1, 1, 1))}
+    s = scf.run_scf(system.crystal("si2"), scf.ScfParams(**cases["gamma"]), OracleBackend())
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_rank_main, args=(2, _free_port(), d, "oracle", cases), nprocs=2, join=True, start_method="spawn")
+        r0 = np.load(os.path.join(d, "gamma_0.npz"))
+        r1 = np.load(os.path.join(d, "gamma_1.npz"))
+    assert int(r0["nlocal"]) == 1 and int(r1["nlocal"]) == 0
+    assert float(r0["energy"]) == float(r1["energy"])
+    np.testing.assert_array_equal(r0["rho"], r1["rho"])
+    np.testing.assert_array_equal(r0["values"], r1["values"])
+    assert int(r0["iterations"]) == s.iterations
+    assert abs(float(r0["energy"]) - s.energy) < 1e-12
+    np.testing.assert_allclose(r0["values"], np.array(s.eigenvalues), atol=1e-12)
+
+
 @pytest.mark.gpu
 def test_two_rank_kpoint_scf_on_gpu_matches_one_process(dz):
     """The same split with libdftcuda contexts: two processes share the one GPU, each holding the
