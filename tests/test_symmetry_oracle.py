@@ -82,6 +82,38 @@ def test_symmetric_density_is_unchanged():
     assert np.abs(sym - rho).max() < 1e-10 * np.abs(rho).max()
 
 
+def _si_conventional(swap):
+    """The cells of the reference's space-group tests (src/tests.zig:46-135): diamond Si, a = 5.431,
+    eight atoms; `swap` exchanges the first two lattice vectors (a left-handed basis)."""
+    a = 5.431
+    h, q, t = a / 2, a / 4, 3 * a / 4
+    cell = np.array([[0.0, a, 0.0], [a, 0.0, 0.0], [0.0, 0.0, a]]) if swap else np.eye(3) * a
+    pos = np.array([[0, 0, 0], [0, h, h], [h, 0, h], [h, h, 0], [q, q, q], [q, t, t], [t, q, t], [t, t, q]], dtype=np.float64)
+    return cell, pos @ np.linalg.inv(cell)
+
+
+def test_reference_space_group_cells():
+    """Fd-3m (No. 227, the reference's expected group) in the conventional cell: 48 rotations x 4
+    face-centring translations, in both bases; symmetrising atom-centred Gaussians in the swapped
+    basis returns them unchanged."""
+    for swap in (False, True):
+        cell, frac = _si_conventional(swap)
+        ops = sy.symmetry_ops(cell, frac, [0] * 8)
+        assert len(ops) == 192
+        assert sum(1 for rot, _, t in ops if np.array_equal(rot, np.eye(3, dtype=np.int64))) == 4  # pure translations
+    cell, frac = _si_conventional(True)
+    ops = sy.symmetry_ops(cell, frac, [0] * 8)
+    dims = (20, 20, 20)
+    n = dims[0] * dims[1] * dims[2]
+    grid = np.stack(np.meshgrid(*[np.arange(d) / d for d in dims], indexing="ij"), axis=-1).transpose(2, 1, 0, 3).reshape(n, 3)
+    rho = np.zeros(n)
+    for f in frac:
+        d = grid - f
+        d -= np.rint(d)
+        rho += np.exp(-((d @ cell) ** 2).sum(axis=1) / 0.6)
+    assert np.abs(sy.symmetrize_density(rho, dims, ops) - rho).max() < 1e-10 * rho.max()
+
+
 def test_identity_only_is_a_copy():
     dims = (6, 5, 4)
     rho = np.random.default_rng(3).random(6 * 5 * 4)
