@@ -94,6 +94,57 @@ def test_radial_projector_large_g():
         assert abs(pseudo.radial_projector(beta, r, rab, 0, g) - exact) < 1e-5
 
 
+GRAPHENE_A, GRAPHENE_C = 4.6487262675, 37.7945225  # bohr (2.46 and 20 Angstrom)
+
+
+def _graphene(c=GRAPHENE_C):
+    a = GRAPHENE_A
+    return np.array([[a, 0.0, 0.0], [a * 0.5, a * np.sqrt(3.0) / 2.0, 0.0], [0.0, 0.0, c]])
+
+
+def test_basis_kinetic_and_smallest_g():
+    """src/tests.zig:437-518: graphene at Gamma; |k+G|^2 of G = 0 is 0 (10 Ry, 10 Angstrom cell), and
+    the smallest non-zero |G| of the 20 Angstrom cell at 30 Ry is 2 pi / c to 1 %."""
+    b = generate_basis(reciprocal(_graphene(18.8972613)), 10.0, np.zeros(3))
+    zero = np.all(b.hkl == 0, axis=1)
+    assert zero.sum() == 1 and abs(float(b.kinetic[zero][0])) < 1e-10
+    b = generate_basis(reciprocal(_graphene()), 30.0, np.zeros(3))
+    g = np.sqrt(b.kinetic[b.kinetic > 1e-20])
+    assert abs(g.min() - 2.0 * np.pi / GRAPHENE_C) <= 0.01 * 2.0 * np.pi / GRAPHENE_C
+
+
+def test_graphene_phase_factor():
+    """src/tests.zig:1148-1216: with the oracle's reciprocal vectors, G = b1 - b2 has zero phase
+    across the C-C bond and K = (1/3, 2/3, 0) has K . d = 2 pi / 3, |1 + e^{-i K . d}| = 1."""
+    cell = _graphene()
+    recip = reciprocal(cell)
+    bond = np.array([1.0 / 3.0, 1.0 / 3.0, 0.0]) @ cell
+    assert 2.5 < np.linalg.norm(bond) < 2.9
+    assert abs(float((recip[0] - recip[1]) @ bond)) < 1e-10
+    k = np.array([1.0 / 3.0, 2.0 / 3.0, 0.0]) @ recip
+    kd = float(k @ bond)
+    assert abs(kd - 2.0 * np.pi / 3.0) < 1e-8
+    assert abs(abs(1.0 + np.exp(-1j * kd)) - 1.0) < 1e-8
+
+
+def test_angular_factor_from_the_real_harmonics():
+    """src/tests.zig:1218-1245 (angular_factor = 4 pi (2l+1) P_l(cos g): 4 pi for l = 0 and 12 pi for
+    l = 1 at cos g = 1): the projectors' harmonics give it through the addition theorem,
+    sum_m (4 pi Y_lm(a)) (4 pi Y_lm(b)) = 4 pi (2l+1) P_l(a . b)."""
+    from numpy.polynomial import legendre
+
+    rng = np.random.default_rng(2)
+    a = rng.normal(size=(40, 3))
+    b = rng.normal(size=(40, 3))
+    cos = (a * b).sum(1) / np.linalg.norm(a, axis=1) / np.linalg.norm(b, axis=1)
+    for l in range(5):
+        s = sum(pseudo.real_ylm(l, m, *a.T) * pseudo.real_ylm(l, m, *b.T) for m in range(-l, l + 1)) * (4.0 * np.pi) ** 2
+        pl = legendre.legval(cos, [0.0] * l + [1.0])
+        np.testing.assert_allclose(s, 4.0 * np.pi * (2 * l + 1) * pl, atol=1e-12)
+        same = sum(pseudo.real_ylm(l, m, *a[:1].T) ** 2 for m in range(-l, l + 1)) * (4.0 * np.pi) ** 2
+        assert abs(float(same[0]) - 4.0 * np.pi * (2 * l + 1)) < 1e-10  # 4 pi, 12 pi, ... at cos g = 1
+
+
 def test_lcg_stream():
     doc = _json("lcg.json")
     r = lobpcg.Lcg(doc["seed"])
