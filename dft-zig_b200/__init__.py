@@ -35,6 +35,10 @@ ABI_SYMBOLS = (
     "dftcuda_status_string",
     "dftcuda_last_error_message",
     "dftcuda_device_count",
+    "dftcuda_debug_set_wait_limits",
+    "dftcuda_fermi_occupations",
+    "dftcuda_ionic_potential_radial",
+    "dftcuda_local_forces_radial",
     "dftcuda_kctx_create",
     "dftcuda_kctx_destroy",
     "dftcuda_kctx_npw",
@@ -248,6 +252,10 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.dftcuda_symmetrize_density.argtypes = [vp, ip, vp, vp, vp]
     lb = ct.c_long
     lib.dftcuda_complex_gemm.argtypes = [ip, sz, sz, sz, vp, lb, ip, ip, vp, lb, ip, ip, vp, lb, lb, ct.c_double, ct.c_double]
+    lib.dftcuda_debug_set_wait_limits.argtypes = [lb, ip]
+    lib.dftcuda_fermi_occupations.argtypes = [sz, sz, dp, dp, ct.c_double, ct.c_double, ct.c_double, dp, dp, dp]
+    lib.dftcuda_ionic_potential_radial.argtypes = [vp, ip, vp, vp, vp, vp, vp, ip, vp, vp, ct.c_double, dp, dp]
+    lib.dftcuda_local_forces_radial.argtypes = [vp, ip, vp, vp, vp, vp, vp, ip, vp, vp, ct.c_double, dp, dp]
     _lib = lib
     return lib
 
@@ -714,6 +722,38 @@ class PotentialContext:
                                                       float(g2max), _ptr(vg), _ptr(vr)))
         return vg, vr
 
+    def ionic_radial(self, meshes, atom_species, positions, g2max: float = 0.0, device: bool = False):
+        """V_loc from each species' radial mesh with the reference's short-range form factor
+        (dftcuda_ionic_potential_radial): meshes [(r, rab, vloc_Ry, z_valence)] per species.
+        Returns (V(G), V_loc(r)), numpy or CUDA tensors."""
+        off, r, rab, vl, z = _radial_meshes(meshes)
+        sp = np.ascontiguousarray(atom_species, dtype=np.int32)
+        pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1, 3))
+        if device:
+            import torch
+
+            vg = torch.empty(self.N, dtype=torch.complex128, device="cuda")
+            vr = torch.empty(self.N, dtype=torch.float64, device="cuda")
+        else:
+            vg = np.empty(self.N, dtype=np.complex128)
+            vr = np.empty(self.N, dtype=np.float64)
+        _check(load_library().dftcuda_ionic_potential_radial(self._h, len(meshes), off.ctypes.data, r.ctypes.data, rab.ctypes.data,
+                                                             vl.ctypes.data, z.ctypes.data, sp.size, sp.ctypes.data, pos.ctypes.data,
+                                                             float(g2max), _ptr(vg), _ptr(vr)))
+        return vg, vr
+
+    def local_forces_radial(self, meshes, atom_species, positions, rho, g2max: float = 0.0) -> np.ndarray:
+        """Local-pseudopotential forces (natoms, 3) in Ry/bohr from each species' radial mesh."""
+        off, r, rab, vl, z = _radial_meshes(meshes)
+        sp = np.ascontiguousarray(atom_species, dtype=np.int32)
+        pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).reshape(-1, 3))
+        rho = _as_array(rho, np.float64, self.N)
+        out = np.empty((sp.size, 3))
+        _check(load_library().dftcuda_local_forces_radial(self._h, len(meshes), off.ctypes.data, r.ctypes.data, rab.ctypes.data,
+                                                          vl.ctypes.data, z.ctypes.data, sp.size, sp.ctypes.data, pos.ctypes.data,
+                                                          float(g2max), _ptr(rho), out.ctypes.data))
+        return out
+
     def close(self):
         if self._h:
             load_library().dftcuda_pctx_destroy(self._h)
@@ -724,6 +764,44 @@ class PotentialContext:
             self.close()
         except Exception:
             pass
+
+
+def fermi_occupations(values, kweights, nelec: float, sigma: float, spin: float = 2.0):
+    """Fermi level, Fermi-Dirac occupations and energy sums of an eigenvalue table on the device
+    (dftcuda_fermi_occupations; find_fermi_level_spin, fermi_level.zig:61-124).  values (nk, nbands),
+    kweights (nk,).  Returns (mu, occ (nk, nbands), band_sum, entropy_sum) with band_sum =
+    sum spin w_k f e and entropy_sum = sum spin w_k S(f)."""
+    lib = load_library()
+    _require_device()
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    if v.ndim != 2:
+        raise InvalidMatrixSize("values must be (nk, nbands)")
+    w = np.ascontiguousarray(kweights, dtype=np.float64)
+    if w.size != v.shape[0]:
+        raise InvalidMatrixSize("one weight per k-point")
+    mu = ct.c_double(0.0)
+    occ = np.zeros_like(v)
+    sums = np.zeros(2)
+    _check(lib.dftcuda_fermi_occupations(v.shape[0], v.shape[1], v.ctypes.data, w.ctypes.data, float(nelec), float(sigma),
+                                         float(spin), ct.addressof(mu), occ.ctypes.data, sums.ctypes.data))
+    return mu.value, occ, float(sums[0]), float(sums[1])
+
+
+def _radial_meshes(meshes):
+    """Packs [(r, rab, vloc, z)] per species into (offsets, r, rab, vloc, z) for the *_radial calls."""
+    off = np.zeros(len(meshes) + 1, dtype=np.uint64)
+    for i, (r, _, _, _) in enumerate(meshes):
+        off[i + 1] = off[i] + len(r)
+    cat = [np.ascontiguousarray(np.concatenate([np.asarray(m[j], dtype=np.float64) for m in meshes])) for j in range(3)]
+    z = np.ascontiguousarray([float(m[3]) for m in meshes], dtype=np.float64)
+    return off, cat[0], cat[1], cat[2], z
+
+
+def debug_set_wait_limits(polls: int = 0, unreachable: bool = False):
+    """Failure injection for the bounded device waits (dftcuda_debug_set_wait_limits): polls > 0 sets
+    the subspace eigensolver's grid-barrier poll budget, unreachable makes every barrier wait run it
+    out (the call then raises Timeout).  debug_set_wait_limits() restores the defaults."""
+    _check(load_library().dftcuda_debug_set_wait_limits(int(polls), 1 if unreachable else 0))
 
 
 def _is_torch_cuda(a) -> bool:

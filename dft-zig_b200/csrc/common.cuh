@@ -74,4 +74,31 @@ void count_launch(int n = 1);
 // True when p is device (or managed) memory, false for host memory (pageable or pinned).
 bool is_device_pointer(const void* p);
 
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) once per (device, kernel, size), under a lock: the
+// attribute belongs to the device, so a process that drives several GPUs sets it on each of them.
+int ensure_max_dynamic_smem(const void* kernel, int bytes);
+
+// Failure injection for the bounded device waits (dftcuda_debug_set_wait_limits): polls > 0 replaces
+// the grid barrier's poll budget; unreachable raises every barrier target by one arrival no block makes.
+struct WaitLimits {
+  long polls;
+  bool unreachable;
+};
+WaitLimits wait_limits();
+// Value a timed-out grid barrier writes to its status flag (the Jacobi solver writes 1 for "not
+// converged"), so callers can tell a timeout from a numerical failure.
+constexpr int kBarrierTimeoutFlag = 2;
+
+// Makes `dev` the current device for the guard's lifetime (no-op when it already is, or dev < 0)
+// and restores the caller's device afterwards.  status is DFTCUDA_OK unless the switch failed.
+struct DeviceGuard {
+  int prev = -1;
+  bool switched = false;
+  int status = DFTCUDA_OK;
+  explicit DeviceGuard(int dev);
+  ~DeviceGuard();
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 }  // namespace dftcuda

@@ -665,11 +665,7 @@ static int small_eig(KCtxImpl* e, int m, int nev, cudaStream_t s) {
   if (tri) return heev_lowest(e->T, m, nev, e->evals, e->E, m, e->hw, e->status, s);
   const int m2 = m + (m & 1);
   const size_t smem = (sizeof(int2) + 2 * sizeof(double) + sizeof(double2)) * (size_t)(m2 / 2);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    attr = true;
-  }
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_jacobi, 160 * 1024));
   k_jacobi<<<1, 1024, smem, s>>>(e->T, e->U, e->evals, e->E, m, 60, 1e-14, e->status); count_launch();
   DFT_CUDA_TRY(cudaGetLastError());
   return DFTCUDA_OK;
@@ -839,8 +835,10 @@ static int run_orth_a(EigRun& r) {
 // After the RR read-back: convergence and candidate selection (serial.zig:228-264).
 static int run_decide(EigRun& r) {
   KCtxImpl* e = r.e;
+  if (*e->h_st == kBarrierTimeoutFlag)
+    return fail(DFTCUDA_ERR_TIMEOUT, "eig_solve: a grid barrier of the subspace eigensolver timed out");
   if (*e->h_st != 0)
-    return fail(DFTCUDA_ERR_EIGENSOLVER_FAILURE, "eig_solve: subspace eigensolver failed (Jacobi not converged or barrier timeout)");
+    return fail(DFTCUDA_ERR_EIGENSOLVER_FAILURE, "eig_solve: subspace eigensolver failed (Jacobi not converged)");
   r.max_res = 0.0;
   for (size_t b = 0; b < r.nbands; ++b) r.max_res = std::max(r.max_res, e->h_nr[b]);
   if (r.max_res < r.opts.tol) {

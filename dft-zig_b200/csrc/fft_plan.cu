@@ -71,8 +71,8 @@ int Fft1dPlan::create(int n) {
   const size_t b64 = tw.size() * sizeof(double2), b32 = tw.size() * sizeof(float2), bp = n * sizeof(int);
   DFT_CUDA_TRY(cudaMalloc(&d_buf, b64 + b32 + bp + 64));
   char* base = (char*)d_buf;
-  // A pageable-host cudaMemcpy may return before its DMA lands, and kernels on non-blocking streams
-  // do not wait for the legacy stream; synchronise the device before the tables are used.
+  // A pageable-host cudaMemcpy may return before its DMA lands; synchronise the device before the
+  // tables are used.
   DFT_CUDA_TRY(cudaMemcpy(base, tw.data(), b64, cudaMemcpyHostToDevice));
   DFT_CUDA_TRY(cudaMemcpy(base + b64, tw32.data(), b32, cudaMemcpyHostToDevice));
   DFT_CUDA_TRY(cudaMemcpy(base + b64 + b32, pinv.data(), bp, cudaMemcpyHostToDevice));
@@ -224,7 +224,7 @@ extern "C" int dftcuda_fft_plan_create(dftcuda_fft_plan** out, int nx, int ny, i
     delete pl;
     return s;
   }
-  if (cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&pl->stream, cudaStreamDefault) != cudaSuccess) {
     delete pl;
     return fail(DFTCUDA_ERR_CUDA, "fft_plan_create: stream");
   }

@@ -430,7 +430,7 @@ using namespace dftcuda;
 extern "C" int dftcuda_fno_forward(int nx, int ny, int nz, const float* u, const float* params, float* out) {
   if (!u || !params || !out) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "fno_forward: null argument");
   cudaStream_t s = nullptr;
-  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamDefault));
   int st;
   {
     const long N = (long)nx * ny * nz;
@@ -457,7 +457,7 @@ extern "C" int dftcuda_fno_loss_grad(size_t nsamples, const int* dims, const siz
   if (!nsamples || !dims || !offs || !u || !target || !params || !loss || !grad)
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "fno_loss_grad: null argument");
   cudaStream_t s = nullptr;
-  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamDefault));
   int st;
   {
     FnoSet d;
@@ -481,7 +481,7 @@ extern "C" int dftcuda_fno_train(size_t nsamples, const int* dims, const size_t*
   if (!nsamples || !dims || !offs || !u || !target || !params)
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "fno_train: null argument");
   cudaStream_t s = nullptr;
-  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamDefault));
   int st;
   {
     FnoSet d;

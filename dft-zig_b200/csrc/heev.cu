@@ -30,7 +30,7 @@ constexpr int HT_THREADS = 512;              // tridiagonalisation block
 constexpr int HT_WARPS = HT_THREADS / 32;
 constexpr int BS_WARPS = 8;                  // bisection: eigenvalues per block
 constexpr int BT_WARPS = 4;                  // back-transformation: eigenvectors per block
-constexpr long kBarrierSpin = 1L << 24;      // polls (with 64 ns sleeps) before a barrier gives up
+constexpr long kBarrierSpin = 1L << 24;      // polls (with 32 ns sleeps) before a barrier gives up
 constexpr double kGroupTol = 1e-5;           // eigenvalue grouping, relative to ||T||
 constexpr int kHtMaxSplit = 8;               // warps per trailing column (row chunks)
 constexpr int kHtColRegs = 4;                // column entries per thread (m <= 4 HT_THREADS)
@@ -41,6 +41,8 @@ struct GridBarrier {
   unsigned* count;  // arrivals since the launch (zeroed by the host)
   int* err;
   unsigned nblocks;
+  long spin = kBarrierSpin;  // polls before a wait gives up
+  unsigned extra = 0;        // arrivals added to every target (failure injection: 1 = never reached)
 };
 
 // All blocks of the (co-resident, cooperative) grid meet here.  The arrival counter only grows
@@ -60,13 +62,13 @@ __device__ bool grid_sync(const GridBarrier& b, unsigned& epoch) {
   ++epoch;
   if (threadIdx.x == 0) {
     int ok = 1;
-    const unsigned target = epoch * b.nblocks;
+    const unsigned target = epoch * b.nblocks + b.extra;
     __threadfence();
     atomicAdd(b.count, 1u);
     long it = 0;
     while (ld_acquire_gpu(b.count) < target) {
-      if (++it > kBarrierSpin) {
-        atomicExch(b.err, 1);
+      if (++it > b.spin) {
+        atomicExch(b.err, kBarrierTimeoutFlag);
         ok = 0;
         break;
       }
@@ -888,6 +890,9 @@ int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde,
   DFT_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), s));
   if (m > 1) {
     GridBarrier bar{w.bar, status, 0};
+    const WaitLimits wl = wait_limits();
+    if (wl.polls > 0) bar.spin = wl.polls;
+    bar.extra = wl.unreachable ? 1u : 0u;
     // enough warps for kHtMaxSplit per column at the start, at most one block per SM
     // (DFTCUDA_HETRD_BPS=2 allows two where they fit, for measurements)
     static const int bps = [] {
@@ -943,7 +948,7 @@ extern "C" int dftcuda_hermitian_eigen_decomp(size_t n, const double* a, size_t 
   if (n > 2048 || nev > n) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "hermitian_eigen_decomp: n > 2048 or nev > n");
   const int m = (int)n, k = (int)nev;
   cudaStream_t s = nullptr;
-  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamDefault));
   struct Guard {
     cudaStream_t s;
     void* p[4] = {nullptr, nullptr, nullptr, nullptr};

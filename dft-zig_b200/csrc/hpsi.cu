@@ -211,10 +211,14 @@ __global__ void k_nl_energy(const double2* __restrict__ coef, const double2* __r
 }
 
 __global__ void k_transpose_vloc(const double* __restrict__ v, double* __restrict__ vt, float* __restrict__ vt32, int nx,
-                                 int ny, int nz) {
+                                 int ny, int nz, double* __restrict__ vn, float* __restrict__ vn32) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long N = (long)nx * ny * nz;
   if (i >= N) return;
+  if (vn) {  // natural order for the stick-layout passes
+    vn[i] = v[i];
+    vn32[i] = (float)v[i];
+  }
   // i = x + nx*(y + ny*z)  ->  vt[x][z][y]
   const int xx = (int)(i % nx);
   const long r = i / nx;
@@ -230,14 +234,12 @@ __global__ void k_transpose_vloc(const double* __restrict__ v, double* __restric
 static const size_t kSmemMax = 227 * 1024;
 
 template <typename T>
-static void set_smem_attrs() {
-  static bool done = false;
-  if (done) return;
-  cudaFuncSetAttribute(k_plane_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax);
-  cudaFuncSetAttribute(k_plane_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax);
-  cudaFuncSetAttribute(k_xline<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax);
-  cudaFuncSetAttribute(k_xline_density<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax);
-  done = true;
+static int set_smem_attrs() {
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_plane_inv<T>, (int)kSmemMax));
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_plane_fwd<T>, (int)kSmemMax));
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_xline<T>, (int)kSmemMax));
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_xline_density<T>, (int)kSmemMax));
+  return DFTCUDA_OK;
 }
 
 static int line_tile(int nx) { return nx > 64 ? 16 : 32; }
@@ -247,26 +249,39 @@ static size_t box_bytes_per_col(const dftcuda_kctx* c) {
   return sizeof(cplx<T>) * (size_t)c->n_act * c->P;
 }
 
-static size_t chunk_cols(const dftcuda_kctx* c, size_t ncols) {
-  const size_t per = (c->precision != DFTCUDA_PRECISION_FP64 ? sizeof(float2) : sizeof(double2)) * (size_t)c->n_act * c->P;
-  size_t ch = (size_t)std::max(1.0, c->w_budget_bytes / (double)per);
+// The local passes of this context's precision use the stick layout (local_sticks.cu).
+static bool use_sticks(const dftcuda_kctx* c) {
+  if (c->fft_generic) return false;
+  return c->precision == DFTCUDA_PRECISION_FP64 ? c->sticks64 : c->sticks32;
+}
+
+// Workspace bytes per column of the local passes (apply = H|psi>, else the density passes, which
+// keep the plane layout).
+static size_t box_col_bytes(const dftcuda_kctx* c, bool apply) {
+  const size_t cs = c->precision != DFTCUDA_PRECISION_FP64 ? sizeof(float2) : sizeof(double2);
+  if (apply && use_sticks(c)) return sticks_bytes_per_col(c, cs);
+  return cs * (size_t)c->n_act * c->P;
+}
+
+static size_t chunk_cols(const dftcuda_kctx* c, size_t ncols, bool apply) {
+  size_t ch = (size_t)std::max(1.0, c->w_budget_bytes / (double)box_col_bytes(c, apply));
   return std::min(ch, std::max<size_t>(ncols, 1));
 }
 
-static int ensure_box(dftcuda_kctx* c, size_t cols) {
-  if (cols <= c->box_cols) return DFTCUDA_OK;
+static int ensure_box(dftcuda_kctx* c, size_t cols, bool apply) {
+  const size_t bytes = box_col_bytes(c, apply) * cols;
+  if (bytes <= c->box_bytes) return DFTCUDA_OK;
   if (c->d_box) cudaFree(c->d_box);
   c->d_box = nullptr;
-  c->box_cols = 0;
-  const size_t bytes = sizeof(double2) * (size_t)c->n_act * c->P * cols;
+  c->box_bytes = 0;
   if (cudaMalloc(&c->d_box, bytes) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "box workspace");
-  c->box_cols = cols;
+  c->box_bytes = bytes;
   return DFTCUDA_OK;
 }
 
 template <typename T>
 static int local_block(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols, cudaStream_t s) {
-  set_smem_attrs<T>();
+  DFT_TRY(set_smem_attrs<T>());
   cplx<T>* W = reinterpret_cast<cplx<T>*>(c->d_box);
   const size_t smem_plane = sizeof(cplx<T>) * (size_t)c->P;
   if (smem_plane > kSmemMax) return fail(DFTCUDA_ERR_UNSUPPORTED, "y-z plane does not fit shared memory");
@@ -377,13 +392,19 @@ int kctx_apply_h_dev(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols
     c->prof.calls += 1;
     c->prof.columns += ncols;
   }
-  const size_t ch = chunk_cols(c, ncols);
-  DFT_TRY(ensure_box(c, ch));
+  const size_t ch = chunk_cols(c, ncols, true);
+  DFT_TRY(ensure_box(c, ch, true));
+  const bool sticks = use_sticks(c);
   for (size_t c0 = 0; c0 < ncols; c0 += ch) {
     const size_t nc = std::min(ch, ncols - c0);
     const double2* xc = x + c0 * c->npw;
     double2* yc = y + c0 * c->npw;
-    if (c->precision != DFTCUDA_PRECISION_FP64) {
+    if (sticks) {
+      if (c->precision != DFTCUDA_PRECISION_FP64)
+        DFT_TRY(local_block_sticks<float>(c, xc, yc, nc, s));
+      else
+        DFT_TRY(local_block_sticks<double>(c, xc, yc, nc, s));
+    } else if (c->precision != DFTCUDA_PRECISION_FP64) {
       if (c->fast32 && !c->fft_generic)
         DFT_TRY(local_block4<float>(c, xc, yc, nc, s));
       else
@@ -408,7 +429,7 @@ int kctx_apply_h_dev(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols
 
 template <typename T>
 static int density_block(dftcuda_kctx* c, const double2* x, size_t ncols, const double* w, double* rho, cudaStream_t s) {
-  set_smem_attrs<T>();
+  DFT_TRY(set_smem_attrs<T>());
   ProfScope ps(c, P_DENSITY, s);
   cplx<T>* W = reinterpret_cast<cplx<T>*>(c->d_box);
   const size_t smem_plane = sizeof(cplx<T>) * (size_t)c->P;
@@ -426,8 +447,8 @@ static int density_block(dftcuda_kctx* c, const double2* x, size_t ncols, const 
 int kctx_density_dev(dftcuda_kctx* c, const double2* vecs, size_t nbands, const double* w_dev, double* rho_dev,
                      cudaStream_t s) {
   if (nbands == 0) return DFTCUDA_OK;
-  const size_t ch = chunk_cols(c, nbands);
-  DFT_TRY(ensure_box(c, ch));
+  const size_t ch = chunk_cols(c, nbands, false);
+  DFT_TRY(ensure_box(c, ch, false));
   for (size_t c0 = 0; c0 < nbands; c0 += ch) {
     const size_t nc = std::min(ch, nbands - c0);
     if (c->precision != DFTCUDA_PRECISION_FP64) {
@@ -495,10 +516,12 @@ extern "C" int dftcuda_kctx_destroy(dftcuda_kctx* c) {
   void* ptrs[] = {c->d_plane_off, c->d_pw_idx, c->d_pw_spos, c->d_slot_xpos, c->d_kinetic, c->d_gcart, c->d_vt,
                   c->d_vt32, c->d_box, c->d_coef, c->d_coef2, c->d_gemm_ws, c->d_x, c->d_y, c->d_rho, c->d_w,
                   c->d_pwmap, c->d_stick_off, c->d_stick_y, c->d_slot_of_x, c->d_tw4x64, c->d_tw4x32,
-                  c->d_tw4p64, c->d_tw4p32, c->d_err, c->d_mlp, c->d_vstage};
+                  c->d_tw4p64, c->d_tw4p32, c->d_err, c->d_mlp, c->d_vstage, c->d_st_sy, c->d_st_map, c->d_st_sox,
+                  c->d_twz64, c->d_twz32, c->d_twx64, c->d_twx32, c->d_vn, c->d_vn32};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   c->fx.destroy(); c->fy.destroy(); c->fz.destroy();
+  if (c->ev_order) cudaEventDestroy(c->ev_order);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return DFTCUDA_OK;
@@ -535,7 +558,11 @@ extern "C" int dftcuda_kctx_create(dftcuda_kctx** out, int nx, int ny, int nz, d
     dftcuda_kctx_destroy(c);
     return fail(DFTCUDA_ERR_UNSUPPORTED, "kctx_create: ny*nz plane exceeds shared memory for FP64");
   }
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  // A blocking stream: its work is ordered after what the caller queued on the legacy default stream
+  // (torch's default stream, plain cudaMemcpy), so device inputs written there are complete when the
+  // context's kernels read them; contexts' streams still run concurrently with one another.
+  if (cudaGetDevice(&c->device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_order, cudaEventDisableTiming) != cudaSuccess) {
     dftcuda_kctx_destroy(c);
     return fail(DFTCUDA_ERR_CUDA, "kctx_create: stream");
   }
@@ -576,9 +603,8 @@ extern "C" int dftcuda_kctx_create(dftcuda_kctx** out, int nx, int ny, int nz, d
     dftcuda_kctx_destroy(c);
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "kctx_create: device tables");
   }
-  // Uploads are ordered on the context's own stream: kernels on that (non-blocking) stream do not
-  // wait for the legacy default stream, where a plain cudaMemcpy from pageable memory may still be
-  // in flight when it returns.
+  // Uploads are ordered on the context's own stream (a plain cudaMemcpy from pageable memory may
+  // return before its DMA lands).
   cudaStream_t st = c->stream;
   cudaMemcpyAsync(c->d_plane_off, cnt.data(), sizeof(int) * (c->n_act + 1), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(c->d_pw_idx, pw_idx.data(), sizeof(int) * n_pw, cudaMemcpyHostToDevice, st);
@@ -593,7 +619,8 @@ extern "C" int dftcuda_kctx_create(dftcuda_kctx** out, int nx, int ny, int nz, d
   // The four-step register-FFT passes, unless DFTCUDA_FFT_PATH=generic asks for the stage-by-stage ones.
   const char* path = std::getenv("DFTCUDA_FFT_PATH");
   if (!(path && std::string(path) == "generic")) {
-    if ((s = kctx_setup_fast_path(c, slot_of_x, xpos, hkl)) != DFTCUDA_OK) {
+    if ((s = kctx_setup_fast_path(c, slot_of_x, xpos, hkl)) != DFTCUDA_OK ||
+        (s = kctx_setup_sticks(c, slot_of_x, xpos, hkl)) != DFTCUDA_OK) {
       dftcuda_kctx_destroy(c);
       return s;
     }
@@ -612,7 +639,8 @@ extern "C" int dftcuda_set_vloc(dftcuda_kctx* c, const double* v) {
   if (!dev && !c->d_vstage && cudaMalloc(&c->d_vstage, sizeof(double) * c->N) != cudaSuccess)
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_vloc staging");
   if (!dev) DFT_CUDA_TRY(cudaMemcpyAsync(c->d_vstage, v, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
-  k_transpose_vloc<<<ceil_div(c->N, 256), 256, 0, c->stream>>>(dev ? v : c->d_vstage, c->d_vt, c->d_vt32, c->nx, c->ny, c->nz); count_launch();
+  k_transpose_vloc<<<ceil_div(c->N, 256), 256, 0, c->stream>>>(dev ? v : c->d_vstage, c->d_vt, c->d_vt32, c->nx, c->ny, c->nz,
+                                                                c->d_vn, c->d_vn32); count_launch();
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return fail(DFTCUDA_ERR_CUDA, std::string("set_vloc: ") + cudaGetErrorString(e));
   c->has_vloc = true;
@@ -980,7 +1008,7 @@ __global__ void k_nonneg_weights(const double* __restrict__ w, double* __restric
 template <typename T>
 static int density_noalloc(dftcuda_kctx* c, const double2* x, size_t nbands, const double* w, double* rho,
                            unsigned char* scratch, cudaStream_t s) {
-  set_smem_attrs<T>();
+  DFT_TRY(set_smem_attrs<T>());
   double* ws = reinterpret_cast<double*>(scratch);
   cplx<T>* W = reinterpret_cast<cplx<T>*>(scratch + kNoAllocWeightBytes);
   const size_t per_col = sizeof(cplx<T>) * (size_t)c->n_act * c->P;
@@ -988,8 +1016,11 @@ static int density_noalloc(dftcuda_kctx* c, const double2* x, size_t nbands, con
   if (cols == 0)
     return fail(DFTCUDA_ERR_UNSUPPORTED, "accumulate_density_noalloc: one column's planes (" + std::to_string(per_col) +
                                              " bytes) exceed the fixed scratch of " + std::to_string(kNoAllocScratchBytes) + " bytes");
-  k_nonneg_weights<<<ceil_div(nbands, 256), 256, 0, s>>>(w, ws, (int)nbands); count_launch();
   const size_t smem_plane = sizeof(cplx<T>) * (size_t)c->P;
+  if (smem_plane > kSmemMax)
+    return fail(DFTCUDA_ERR_UNSUPPORTED, "accumulate_density_noalloc: a y-z plane (" + std::to_string(smem_plane) +
+                                             " bytes) does not fit shared memory");
+  k_nonneg_weights<<<ceil_div(nbands, 256), 256, 0, s>>>(w, ws, (int)nbands); count_launch();
   const int J = line_tile(c->nx);
   const size_t smem_x = (sizeof(cplx<T>) + sizeof(double)) * (size_t)c->nx * J;
   for (size_t c0 = 0; c0 < nbands; c0 += cols) {
@@ -1017,8 +1048,14 @@ extern "C" int dftcuda_accumulate_density_noalloc(dftcuda_kctx* c, const double*
   if (!vectors || !weights || !rho) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "accumulate_density_noalloc: null buffer");
   if (!is_device_pointer(vectors) || !is_device_pointer(weights) || !is_device_pointer(rho))
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "accumulate_density_noalloc: vectors, weights and rho must be device pointers");
+  // Run on the context's device (the scratch address is per device), and after the work the caller
+  // queued on the legacy default stream (where torch and plain CUDA code write these inputs).
+  DeviceGuard dg(c->device);
+  DFT_TRY(dg.status);
   unsigned char* scratch = nullptr;
   DFT_TRY(noalloc_scratch(&scratch));
+  DFT_CUDA_TRY(cudaEventRecord(c->ev_order, cudaStreamLegacy));
+  DFT_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_order, 0));
   const double2* x = reinterpret_cast<const double2*>(vectors);
   if (c->precision != DFTCUDA_PRECISION_FP64)
     DFT_TRY(density_noalloc<float>(c, x, nbands, weights, rho, scratch, c->stream));

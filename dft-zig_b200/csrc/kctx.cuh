@@ -66,6 +66,8 @@ struct dftcuda_kctx {
   size_t npw;
   int precision;
   cudaStream_t stream = nullptr;
+  int device = -1;                  // the CUDA device current when the context was created
+  cudaEvent_t ev_order = nullptr;   // orders the context's stream after the caller's legacy-stream work
   dftcuda::Fft1dPlan fx, fy, fz;
 
   // G-sphere grouped by active x-plane ("slot").
@@ -94,6 +96,19 @@ struct dftcuda_kctx {
   void* d_tw4p64 = nullptr;
   void* d_tw4p32 = nullptr;
 
+  // Stick-layout passes (local_sticks.cu), used when sticks64 / sticks32 is set for the precision.
+  bool sticks64 = false, sticks32 = false;
+  int n_st = 0;                // sticks: (x, y) pairs holding plane waves, in slot order
+  int* d_st_sy = nullptr;      // [n_st] slot << 16 | y
+  int* d_st_map = nullptr;     // [n_st][nz] plane-wave index of (stick, z) or -1
+  int* d_st_sox = nullptr;     // [nx] slot of each x frequency or -1
+  void* d_twz64 = nullptr;     // twiddles of the z length
+  void* d_twz32 = nullptr;
+  void* d_twx64 = nullptr;     // twiddles of the x (= y) length
+  void* d_twx32 = nullptr;
+  double* d_vn = nullptr;      // V(r) in natural box order (x fastest), FP64 and FP32
+  float* d_vn32 = nullptr;
+
   // Local potential transposed to [x][z][y]; FP32 copy for the FP32 passes.
   double* d_vt = nullptr;
   float* d_vt32 = nullptr;
@@ -101,7 +116,7 @@ struct dftcuda_kctx {
 
   // Box workspace for a chunk of columns: [chunk][n_act][P] complex.
   void* d_box = nullptr;
-  size_t box_cols = 0;
+  size_t box_bytes = 0;
 
   dftcuda::NonlocalDev nl;
   int natoms = 0;                   // atoms given to set_projectors
@@ -173,6 +188,11 @@ bool kctx_fast_path_ok(const dftcuda_kctx* c, int precision);
 int kctx_setup_fast_path(dftcuda_kctx* c, const std::vector<int>& slot_of_x, const std::vector<int>& xpos,
                          const int32_t* hkl);
 template <typename T> int local_block4(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols, cudaStream_t s);
+// Stick-layout passes (local_sticks.cu).
+bool kctx_sticks_ok(const dftcuda_kctx* c, int precision);
+int kctx_setup_sticks(dftcuda_kctx* c, const std::vector<int>& slot_of_x, const std::vector<int>& xpos, const int32_t* hkl);
+size_t sticks_bytes_per_col(const dftcuda_kctx* c, size_t cs);
+template <typename T> int local_block_sticks(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols, cudaStream_t s);
 template <typename T>
 int density_block4(dftcuda_kctx* c, const double2* x, size_t ncols, const double* w, double* rho, cudaStream_t s);
 

@@ -496,7 +496,7 @@ extern "C" int dftcuda_precond_mlp_loss_grad(size_t nbands, size_t npw, const in
   if (nbands == 0 || npw == 0 || !band_off || !feat || !cc || !w || !dnorm || !params || !loss || !grad)
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "precond_mlp_loss_grad: empty or null argument");
   cudaStream_t s = nullptr;
-  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamDefault));
   int st;
   {
     MlpData d;
@@ -520,7 +520,7 @@ extern "C" int dftcuda_precond_mlp_train(size_t nbands, size_t npw, const int* b
   if (nbands == 0 || npw == 0 || !band_off || !feat || !cc || !w || !dnorm || !params)
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "precond_mlp_train: empty or null argument");
   cudaStream_t s = nullptr;
-  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamDefault));
   int st;
   {
     MlpData d;

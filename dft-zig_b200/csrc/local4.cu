@@ -675,23 +675,15 @@ template <typename T, int NP>
 static int launch_plane_inv4(dftcuda_kctx* c, const double2* x, cplx<T>* W, size_t ncols, cudaStream_t s) {
   const cplx<T>* tw5 = std::is_same<T, double>::value ? (const cplx<T>*)c->d_tw4p64 : (const cplx<T>*)c->d_tw4p32;
   if (!fft4_legacy()) {
-    static bool attr5 = false;
-    if (!attr5) {
-      cudaFuncSetAttribute(k_plane_inv5<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem4);
-      attr5 = true;
-    }
+    DFT_TRY(ensure_max_dynamic_smem((const void*)k_plane_inv5<T, NP>, (int)kSmem4));
     dim3 g(c->n_act, (unsigned)ncols);
     k_plane_inv5<T, NP><<<g, kPlaneThreads, plane_smem<T, NP>(1), s>>>(x, (long)c->npw, W, c->n_act, c->d_pwmap, c->d_stick_off,
                                                               c->d_stick_y, tw5);
     count_launch();
     return DFTCUDA_OK;
   }
-  static bool attr = false;
   const size_t smem = plane_smem<T, NP>(2);
-  if (!attr) {
-    cudaFuncSetAttribute(k_plane_inv4<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem4);
-    attr = true;
-  }
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_plane_inv4<T, NP>, (int)kSmem4));
   const cplx<T>* tw = std::is_same<T, double>::value ? (const cplx<T>*)c->d_tw4p64 : (const cplx<T>*)c->d_tw4p32;
   dim3 g(c->n_act, (unsigned)ncols);
   k_plane_inv4<T, NP><<<g, 512, smem, s>>>(x, (long)c->npw, W, c->n_act, c->d_pwmap, c->d_stick_off, c->d_stick_y, tw); count_launch();
@@ -702,11 +694,7 @@ template <typename T, int NP>
 static int launch_plane_fwd4(dftcuda_kctx* c, const cplx<T>* W, const double2* x, double2* y, size_t ncols,
                              cudaStream_t s) {
   if (!fft4_legacy()) {
-    static bool attr5 = false;
-    if (!attr5) {
-      cudaFuncSetAttribute(k_plane_fwd5<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem4);
-      attr5 = true;
-    }
+    DFT_TRY(ensure_max_dynamic_smem((const void*)k_plane_fwd5<T, NP>, (int)kSmem4));
     const cplx<T>* tw5 = std::is_same<T, double>::value ? (const cplx<T>*)c->d_tw4p64 : (const cplx<T>*)c->d_tw4p32;
     dim3 g(c->n_act, (unsigned)ncols);
     k_plane_fwd5<T, NP><<<g, kPlaneThreads, plane_smem<T, NP>(1), s>>>(W, c->n_act, c->d_pwmap, c->d_stick_off, c->d_stick_y, tw5, x, y,
@@ -714,12 +702,8 @@ static int launch_plane_fwd4(dftcuda_kctx* c, const cplx<T>* W, const double2* x
     count_launch();
     return DFTCUDA_OK;
   }
-  static bool attr = false;
   const size_t smem = plane_smem<T, NP>(2);
-  if (!attr) {
-    cudaFuncSetAttribute(k_plane_fwd4<T, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem4);
-    attr = true;
-  }
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_plane_fwd4<T, NP>, (int)kSmem4));
   const cplx<T>* tw = std::is_same<T, double>::value ? (const cplx<T>*)c->d_tw4p64 : (const cplx<T>*)c->d_tw4p32;
   dim3 g(c->n_act, (unsigned)ncols);
   k_plane_fwd4<T, NP><<<g, 512, smem, s>>>(W, c->n_act, c->d_pwmap, c->d_stick_off, c->d_stick_y, tw, x, y, (long)c->npw,
@@ -735,11 +719,7 @@ static int launch_xline4(dftcuda_kctx* c, cplx<T>* W, size_t ncols, cudaStream_t
   if (!fft4_legacy()) {
     using G = XLineGeom<NX>;
     const size_t smem5 = 2 * sizeof(cplx<T>) * (size_t)kXlWarps * G::LW * G::S;
-    static bool attr5 = false;
-    if (!attr5) {
-      cudaFuncSetAttribute(k_xline5<T, NX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem4);
-      attr5 = true;
-    }
+    DFT_TRY(ensure_max_dynamic_smem((const void*)k_xline5<T, NX>, (int)kSmem4));
     const int cpc = 4;
     dim3 g(ceil_div(c->P, kXlWarps * G::LW), ceil_div(ncols, cpc));
     k_xline5<T, NX><<<g, kXlWarps * 32, smem5, s>>>(W, c->n_act, c->d_slot_of_x, vt, c->P, (int)ncols, cpc, tw);
@@ -747,11 +727,7 @@ static int launch_xline4(dftcuda_kctx* c, cplx<T>* W, size_t ncols, cudaStream_t
     return DFTCUDA_OK;
   }
   const int J = N1 > 8 ? 16 : 32;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_xline4<T, NX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem4);
-    attr = true;
-  }
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_xline4<T, NX>, (int)kSmem4));
   const size_t smem = 2 * sizeof(cplx<T>) * (size_t)NX * J;
   const int cpc = 4;
   dim3 g(ceil_div(c->P, J), ceil_div(ncols, cpc));
@@ -765,11 +741,7 @@ static int launch_xline_density4(dftcuda_kctx* c, const cplx<T>* W, size_t ncols
                                  cudaStream_t s) {
   constexpr int N1 = Split<NX>::N1;
   const int J = N1 > 8 ? 16 : 32;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_xline_density4<T, NX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem4);
-    attr = true;
-  }
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_xline_density4<T, NX>, (int)kSmem4));
   const size_t smem = sizeof(cplx<T>) * (size_t)NX * J;
   dim3 g(ceil_div(c->P, J));
   dim3 b(J, N1);

@@ -1,6 +1,9 @@
 // Status strings, per-thread last-error message, pointer classification.
 #include <atomic>
+#include <mutex>
+#include <set>
 #include <string>
+#include <tuple>
 
 #include "kctx.cuh"
 
@@ -62,7 +65,47 @@ bool is_device_pointer(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+int ensure_max_dynamic_smem(const void* kernel, int bytes) {
+  static std::mutex mu;
+  static std::set<std::tuple<int, const void*, int>> done;
+  int dev = 0;
+  DFT_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_tuple(dev, kernel, bytes);
+  if (done.count(key)) return DFTCUDA_OK;
+  const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess)
+    return fail(DFTCUDA_ERR_CUDA, std::string("cudaFuncSetAttribute(MaxDynamicSharedMemorySize): ") + cudaGetErrorString(e));
+  done.insert(key);
+  return DFTCUDA_OK;
+}
+
+static std::atomic<long> g_wait_polls{0};
+static std::atomic<bool> g_wait_unreachable{false};
+WaitLimits wait_limits() { return WaitLimits{g_wait_polls.load(), g_wait_unreachable.load()}; }
+
+DeviceGuard::DeviceGuard(int dev) {
+  if (cudaGetDevice(&prev) != cudaSuccess) {
+    cudaGetLastError();
+    prev = -1;
+  }
+  if (dev >= 0 && dev != prev) {
+    status = cudaSetDevice(dev) == cudaSuccess ? DFTCUDA_OK : fail(DFTCUDA_ERR_CUDA, "cudaSetDevice to the context's device");
+    switched = status == DFTCUDA_OK;
+  }
+}
+DeviceGuard::~DeviceGuard() {
+  if (switched && prev >= 0) cudaSetDevice(prev);
+}
+
 }  // namespace dftcuda
+
+extern "C" int dftcuda_debug_set_wait_limits(long polls, int unreachable) {
+  if (polls < 0) return dftcuda::fail(DFTCUDA_ERR_INVALID_ARGUMENT, "debug_set_wait_limits: polls < 0");
+  dftcuda::g_wait_polls.store(polls);
+  dftcuda::g_wait_unreachable.store(unreachable != 0);
+  return DFTCUDA_OK;
+}
 
 extern "C" const char* dftcuda_status_string(int status) {
   switch (status) {
@@ -157,7 +200,7 @@ extern "C" int dftcuda_complex_gemm(int precision, size_t M, size_t N, size_t K,
     if (ws) cudaFree(ws);
     if (err) cudaFree(err);
   };
-  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+  if (cudaStreamCreateWithFlags(&s, cudaStreamDefault) != cudaSuccess ||
       (ws_elems && cudaMalloc(&ws, sizeof(double2) * ws_elems) != cudaSuccess) || cudaMalloc(&err, sizeof(int)) != cudaSuccess ||
       cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) {
     cleanup();

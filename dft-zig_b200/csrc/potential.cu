@@ -147,10 +147,69 @@ __global__ void __launch_bounds__(kPotThreads) k_pot_hartree(const double2* __re
 // One thread per G point; atom positions and species parameters in shared memory.
 constexpr int kIonMaxSpecies = 8;
 constexpr int kIonAtomTile = 512;
+
+// Local form factor of a species in Ry, either the analytic GTH form above (gth != nullptr, 6
+// parameters per species) or values precomputed per box point (vq[s * N + i], from the species'
+// radial mesh by k_pot_vq_radial).  keep() is the G-vector selection of each: GTH
+// 1e-12 < G^2 <= g2max; radial |G| >= 1e-10 and G^2 < g2max (build_ionic_potential_grid,
+// potential.zig:291-306, and ionic_local_potential_with_table, hamiltonian.zig).
+struct LocalFF {
+  const double* gth = nullptr;
+  const double* vq = nullptr;
+  long N = 0;
+  __device__ bool keep(double g2, double g2max) const {
+    return vq ? (sqrt(g2) >= 1e-10 && g2 < g2max) : (g2 > 1e-12 && g2 <= g2max);
+  }
+  __device__ double ry(int s, double g2, long i) const {
+    if (vq) return vq[(long)s * N + i];
+    const double Z = gth[6 * s], r = gth[6 * s + 1];
+    const double c1 = gth[6 * s + 2], c2 = gth[6 * s + 3], c3 = gth[6 * s + 4], c4 = gth[6 * s + 5];
+    const double yy = g2 * r * r, e = exp(-0.5 * yy);
+    const double poly = c1 + c2 * (3.0 - yy) + c3 * (15.0 - 10.0 * yy + yy * yy) +
+                        c4 * (105.0 - 105.0 * yy + 21.0 * yy * yy - yy * yy * yy);
+    return 2.0 * (-4.0 * kPi * Z / g2 * e + sqrt(8.0 * kPi * kPi * kPi) * r * r * r * e * poly);
+  }
+};
+
+// local_vq_short_range (form_factor.zig:223-262, the default local_potential mode of
+// config/defaults.zig:28) at every box point, per species:
+//   vq[s][i] = 4 pi sum_j r_j^2 [V_loc(r_j) + 2 Z / r_j] sinc(|G_i| r_j) rab_j w_j - 8 pi Z / |G_i|^2  (Ry)
+// summed in mesh order like the reference's loop, the 2Z/r term skipped at r < 1e-10 and the
+// Coulomb term at |G| < 1e-10; w the composite-trapezoid weights of radial_integration.zig:7-13.
+// Species s uses mesh points [off[s], off[s+1]); every thread of a warp reads the same mesh entry.
+__global__ void __launch_bounds__(kPotThreads) k_pot_vq_radial(const double* __restrict__ g2, long N, int nspecies,
+                                                               const int* __restrict__ off, const double* __restrict__ r,
+                                                               const double* __restrict__ rab, const double* __restrict__ vloc,
+                                                               const double* __restrict__ zval, double* __restrict__ vq) {
+  const double cw[5] = {23.75 / 72.0, 95.10 / 72.0, 55.20 / 72.0, 79.30 / 72.0, 70.65 / 72.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x) {
+    const double q = sqrt(g2[i]);
+    for (int s = 0; s < nspecies; ++s) {
+      const int j0 = off[s], n = off[s + 1] - j0;
+      const double z = zval[s];
+      double sum = 0.0;
+      for (int jj = 0; jj < n; ++jj) {
+        double w = 1.0;
+        if (n >= 10) {
+          if (jj < 5) w = cw[jj];
+          else if (jj >= n - 5) w = cw[n - 1 - jj];
+        }
+        const double rj = __ldg(r + j0 + jj);
+        const double vc = rj < 1e-10 ? 0.0 : 2.0 * z / rj;
+        const double x = q * rj;
+        const double sinc = fabs(x) < 1e-12 ? 1.0 : sin(x) / x;
+        sum += rj * rj * (__ldg(vloc + j0 + jj) + vc) * sinc * __ldg(rab + j0 + jj) * w;
+      }
+      double v = 4.0 * kPi * sum;
+      if (q >= 1e-10) v -= 8.0 * kPi * z / (q * q);
+      vq[(long)s * N + i] = v;
+    }
+  }
+}
 __global__ void __launch_bounds__(kPotThreads) k_pot_ionic(const double* __restrict__ g2, int nx, int ny, int nz, double b00,
                                                            double b01, double b02, double b10, double b11, double b12,
                                                            double b20, double b21, double b22, int nspecies,
-                                                           const double* __restrict__ gth, int natoms,
+                                                           LocalFF ff, int natoms,
                                                            const int* __restrict__ species, const double* __restrict__ pos,
                                                            double g2max, double inv_volume, double2* __restrict__ out) {
   __shared__ double sx[kIonAtomTile], sy[kIonAtomTile], sz[kIonAtomTile];
@@ -195,15 +254,9 @@ __global__ void __launch_bounds__(kPotThreads) k_pot_ionic(const double* __restr
   }
   if (i >= N) return;
   double2 v = make_double2(0.0, 0.0);
-  if (q > 1e-12 && q <= g2max) {
+  if (ff.keep(q, g2max)) {
     for (int s = 0; s < nspecies; ++s) {
-      const double Z = gth[6 * s], r = gth[6 * s + 1];
-      const double c1 = gth[6 * s + 2], c2 = gth[6 * s + 3], c3 = gth[6 * s + 4], c4 = gth[6 * s + 5];
-      const double yy = q * r * r, e = exp(-0.5 * yy);
-      const double poly = c1 + c2 * (3.0 - yy) + c3 * (15.0 - 10.0 * yy + yy * yy) +
-                          c4 * (105.0 - 105.0 * yy + 21.0 * yy * yy - yy * yy * yy);
-      const double ff = -4.0 * kPi * Z / q * e + sqrt(8.0 * kPi * kPi * kPi) * r * r * r * e * poly;
-      const double w = 2.0 * ff * inv_volume;
+      const double w = ff.ry(s, q, i) * inv_volume;
       v.x += w * sre[s];
       v.y += w * sim[s];
     }
@@ -346,7 +399,7 @@ __global__ void k_pot_gga_vxc(const double* __restrict__ vr, const double2* __re
 constexpr int kLfChunks = 64;
 __global__ void __launch_bounds__(kPotThreads) k_pot_local_force(const double2* __restrict__ a, const double* __restrict__ g2,
                                                                  int nx, int ny, int nz, Recip9 r,
-                                                                 const double* __restrict__ gth, const int* __restrict__ species,
+                                                                 LocalFF ff, const int* __restrict__ species,
                                                                  const double* __restrict__ pos, double g2max,
                                                                  double* __restrict__ part) {
   __shared__ double red[kPotThreads / 32];
@@ -355,23 +408,17 @@ __global__ void __launch_bounds__(kPotThreads) k_pot_local_force(const double2* 
   const long per = (N + kLfChunks - 1) / kLfChunks;
   const long i0 = chunk * per, i1 = min(N, i0 + per);
   const int sp = species[atom];
-  const double Z = gth[6 * sp], rl = gth[6 * sp + 1];
-  const double c1 = gth[6 * sp + 2], c2 = gth[6 * sp + 3], c3 = gth[6 * sp + 4], c4 = gth[6 * sp + 5];
   const double tx = pos[3 * atom], ty = pos[3 * atom + 1], tz = pos[3 * atom + 2];
   const double inv = 1.0 / (double)N;
   double fx = 0.0, fy = 0.0, fz = 0.0;
   for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
     const double q = g2[i];
-    if (!(q > 1e-12 && q <= g2max)) continue;
+    if (!ff.keep(q, g2max)) continue;
     const double gx = pot_gcomp(i, nx, ny, nz, r, 0), gy = pot_gcomp(i, nx, ny, nz, r, 1), gz = pot_gcomp(i, nx, ny, nz, r, 2);
-    const double yy = q * rl * rl, e = exp(-0.5 * yy);
-    const double poly = c1 + c2 * (3.0 - yy) + c3 * (15.0 - 10.0 * yy + yy * yy) +
-                        c4 * (105.0 - 105.0 * yy + 21.0 * yy * yy - yy * yy * yy);
-    const double ff = -4.0 * kPi * Z / q * e + sqrt(8.0 * kPi * kPi * kPi) * rl * rl * rl * e * poly;
     double sn, cs;
     sincos(gx * tx + gy * ty + gz * tz, &sn, &cs);
     const double2 rg = make_double2(a[i].x * inv, a[i].y * inv);
-    const double w = 2.0 * ff * (cs * rg.y + sn * rg.x);  // Im(e^{iG.tau} rho(G))
+    const double w = ff.ry(sp, q, i) * (cs * rg.y + sn * rg.x);  // Im(e^{iG.tau} rho(G))
     fx += w * gx;
     fy += w * gy;
     fz += w * gz;
@@ -635,7 +682,7 @@ extern "C" int dftcuda_pctx_create(dftcuda_pctx** out, int nx, int ny, int nz, d
   if (st != DFTCUDA_OK) return pctx_fail_free(c, st);
   const long N = c->N;
   const int nparts = std::max(2, pulay_history);
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault) != cudaSuccess ||
       cudaMalloc(&c->g2, sizeof(double) * N) != cudaSuccess || cudaMalloc(&c->a, sizeof(double2) * N) != cudaSuccess ||
       cudaMalloc(&c->b, sizeof(double2) * N) != cudaSuccess || cudaMalloc(&c->rho, sizeof(double) * N) != cudaSuccess ||
       cudaMalloc(&c->vin, sizeof(double2) * N) != cudaSuccess || cudaMalloc(&c->vout, sizeof(double2) * N) != cudaSuccess ||
@@ -830,38 +877,89 @@ extern "C" int dftcuda_symmetrize_density(dftcuda_pctx* c, int nops, const int* 
   return DFTCUDA_OK;
 }
 
-extern "C" int dftcuda_ionic_potential(dftcuda_pctx* c, int nspecies, const double* gth, int natoms, const int* atom_species,
-                                       const double* positions, double g2max, double* v_out_g, double* vloc_r) {
-  if (!c || nspecies < 1 || nspecies > kIonMaxSpecies || !gth || natoms < 0 || (natoms > 0 && (!atom_species || !positions)))
+// The species form factors of the ionic-potential and local-force calls: the 6 GTH parameters per
+// species (gth), or each species' radial mesh (mesh_off[nspecies + 1] into r, rab, vloc; z[nspecies]),
+// whose form factor k_pot_vq_radial evaluates at every box point.
+struct FFArgs {
+  const double* gth = nullptr;
+  const size_t* mesh_off = nullptr;
+  const double *r = nullptr, *rab = nullptr, *vloc = nullptr, *z = nullptr;
+};
+
+// Device copies of the form-factor inputs and, for radial meshes, the per-point form factors.
+struct FFDevice {
+  double* buf = nullptr;
+  int* off = nullptr;
+  LocalFF ff;
+  ~FFDevice() {
+    if (buf) cudaFree(buf);
+    if (off) cudaFree(off);
+  }
+  int init(const FFArgs& a, int nspecies, const double* g2, long N, cudaStream_t s) {
+    if (a.gth) {
+      if (cudaMalloc(&buf, sizeof(double) * 6 * nspecies) != cudaSuccess) return fail(DFTCUDA_ERR_CUDA, "form factors: allocation failed");
+      DFT_CUDA_TRY(cudaMemcpyAsync(buf, a.gth, sizeof(double) * 6 * nspecies, cudaMemcpyDefault, s));
+      ff.gth = buf;
+      return DFTCUDA_OK;
+    }
+    std::vector<int> ho(nspecies + 1);
+    for (int i = 0; i <= nspecies; ++i) {
+      if (a.mesh_off[i] > (size_t)INT32_MAX || (i > 0 && a.mesh_off[i] < a.mesh_off[i - 1]))
+        return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "radial form factors: mesh offsets must ascend");
+      ho[i] = (int)a.mesh_off[i];
+    }
+    const size_t nr = (size_t)ho[nspecies] - ho[0];
+    if (ho[0] != 0 || nr == 0) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "radial form factors: empty mesh");
+    if (cudaMalloc(&buf, sizeof(double) * (3 * nr + nspecies + (size_t)nspecies * N)) != cudaSuccess ||
+        cudaMalloc(&off, sizeof(int) * (nspecies + 1)) != cudaSuccess)
+      return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "radial form factors: allocation failed");
+    double *dr = buf, *drab = buf + nr, *dv = buf + 2 * nr, *dz = buf + 3 * nr, *vq = dz + nspecies;
+    DFT_CUDA_TRY(cudaMemcpyAsync(dr, a.r, sizeof(double) * nr, cudaMemcpyDefault, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(drab, a.rab, sizeof(double) * nr, cudaMemcpyDefault, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(dv, a.vloc, sizeof(double) * nr, cudaMemcpyDefault, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(dz, a.z, sizeof(double) * nspecies, cudaMemcpyDefault, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(off, ho.data(), sizeof(int) * (nspecies + 1), cudaMemcpyHostToDevice, s));
+    k_pot_vq_radial<<<(unsigned)std::min<long>(ceil_div(N, kPotThreads), 65535), kPotThreads, 0, s>>>(g2, N, nspecies, off, dr, drab, dv,
+                                                                                                      dz, vq);
+    count_launch();
+    DFT_CUDA_TRY(cudaGetLastError());
+    DFT_CUDA_TRY(cudaStreamSynchronize(s));  // ho goes out of scope
+    ff.vq = vq;
+    ff.N = N;
+    return DFTCUDA_OK;
+  }
+};
+
+static int ionic_impl(dftcuda_pctx* c, int nspecies, const FFArgs& ffa, int natoms, const int* atom_species, const double* positions,
+                      double g2max, double* v_out_g, double* vloc_r) {
+  if (!c || nspecies < 1 || nspecies > kIonMaxSpecies || natoms < 0 || (natoms > 0 && (!atom_species || !positions)))
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "ionic_potential: bad arguments (1..8 species)");
   for (int a = 0; a < natoms; ++a)
     if (atom_species[a] < 0 || atom_species[a] >= nspecies)
       return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "ionic_potential: atom species index out of range");
   const long N = c->N;
   cudaStream_t s = c->stream;
-  double* d_gth = nullptr;
   double* d_pos = nullptr;
   int* d_sp = nullptr;
   auto cleanup = [&] {
-    if (d_gth) cudaFree(d_gth);
     if (d_pos) cudaFree(d_pos);
     if (d_sp) cudaFree(d_sp);
   };
-  if (cudaMalloc(&d_gth, sizeof(double) * 6 * nspecies) != cudaSuccess ||
-      cudaMalloc(&d_pos, sizeof(double) * 3 * std::max(natoms, 1)) != cudaSuccess ||
+  FFDevice ffd;
+  DFT_TRY(ffd.init(ffa, nspecies, c->g2, N, s));
+  if (cudaMalloc(&d_pos, sizeof(double) * 3 * std::max(natoms, 1)) != cudaSuccess ||
       cudaMalloc(&d_sp, sizeof(int) * std::max(natoms, 1)) != cudaSuccess) {
     cleanup();
     return fail(DFTCUDA_ERR_CUDA, "ionic_potential: allocation failed");
   }
   int st = DFTCUDA_OK;
-  if (cudaMemcpyAsync(d_gth, gth, sizeof(double) * 6 * nspecies, cudaMemcpyDefault, s) != cudaSuccess ||
-      (natoms > 0 && (cudaMemcpyAsync(d_pos, positions, sizeof(double) * 3 * natoms, cudaMemcpyDefault, s) != cudaSuccess ||
+  if ((natoms > 0 && (cudaMemcpyAsync(d_pos, positions, sizeof(double) * 3 * natoms, cudaMemcpyDefault, s) != cudaSuccess ||
                       cudaMemcpyAsync(d_sp, atom_species, sizeof(int) * natoms, cudaMemcpyDefault, s) != cudaSuccess)))
     st = fail(DFTCUDA_ERR_CUDA, "ionic_potential: copy failed");
   if (st == DFTCUDA_OK) {
     const double* r = c->recip;
     k_pot_ionic<<<(unsigned)ceil_div(N, kPotThreads), kPotThreads, 0, s>>>(
-        c->g2, c->nx, c->ny, c->nz, r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8], nspecies, d_gth, natoms, d_sp, d_pos,
+        c->g2, c->nx, c->ny, c->nz, r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8], nspecies, ffd.ff, natoms, d_sp, d_pos,
         g2max > 0.0 ? g2max : 1e300, 1.0 / c->volume, c->b);
     count_launch();
     if (v_out_g && copy_out(v_out_g, c->b, sizeof(double2) * N, s) != DFTCUDA_OK) st = DFTCUDA_ERR_CUDA;
@@ -881,9 +979,9 @@ extern "C" int dftcuda_ionic_potential(dftcuda_pctx* c, int nspecies, const doub
   return st;
 }
 
-extern "C" int dftcuda_local_forces(dftcuda_pctx* c, int nspecies, const double* gth, int natoms, const int* atom_species,
-                                    const double* positions, double g2max, const double* rho_r, double* forces) {
-  if (!c || nspecies < 1 || !gth || natoms < 1 || !atom_species || !positions || !rho_r || !forces)
+static int local_forces_impl(dftcuda_pctx* c, int nspecies, const FFArgs& ffa, int natoms, const int* atom_species,
+                             const double* positions, double g2max, const double* rho_r, double* forces) {
+  if (!c || nspecies < 1 || natoms < 1 || !atom_species || !positions || !rho_r || !forces)
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "local_forces: bad arguments");
   for (int a = 0; a < natoms; ++a)
     if (atom_species[a] < 0 || atom_species[a] >= nspecies)
@@ -893,23 +991,23 @@ extern "C" int dftcuda_local_forces(dftcuda_pctx* c, int nspecies, const double*
   int st = DFTCUDA_OK;
   const double* rho = (const double*)device_view(rho_r, c->rho, sizeof(double) * N, s, &st);
   if (st != DFTCUDA_OK) return st;
-  double* d_gth = nullptr;
   double* d_pos = nullptr;
   int* d_sp = nullptr;
   double* d_part = nullptr;
   auto cleanup = [&] {
-    for (void* p : {(void*)d_gth, (void*)d_pos, (void*)d_sp, (void*)d_part})
+    for (void* p : {(void*)d_pos, (void*)d_sp, (void*)d_part})
       if (p) cudaFree(p);
   };
   const size_t npart = (size_t)natoms * kLfChunks * 3;
-  if (cudaMalloc(&d_gth, sizeof(double) * 6 * nspecies) != cudaSuccess || cudaMalloc(&d_pos, sizeof(double) * 3 * natoms) != cudaSuccess ||
+  FFDevice ffd;
+  DFT_TRY(ffd.init(ffa, nspecies, c->g2, N, s));
+  if (cudaMalloc(&d_pos, sizeof(double) * 3 * natoms) != cudaSuccess ||
       cudaMalloc(&d_sp, sizeof(int) * natoms) != cudaSuccess || cudaMalloc(&d_part, sizeof(double) * npart) != cudaSuccess) {
     cleanup();
     return fail(DFTCUDA_ERR_CUDA, "local_forces: allocation failed");
   }
   std::vector<double> hp(npart);
   auto run = [&]() -> int {
-    DFT_CUDA_TRY(cudaMemcpyAsync(d_gth, gth, sizeof(double) * 6 * nspecies, cudaMemcpyDefault, s));
     DFT_CUDA_TRY(cudaMemcpyAsync(d_pos, positions, sizeof(double) * 3 * natoms, cudaMemcpyDefault, s));
     DFT_CUDA_TRY(cudaMemcpyAsync(d_sp, atom_species, sizeof(int) * natoms, cudaMemcpyDefault, s));
     k_pot_to_complex<<<kPotBlocks, kPotThreads, 0, s>>>(rho, N, c->a);
@@ -917,7 +1015,7 @@ extern "C" int dftcuda_local_forces(dftcuda_pctx* c, int nspecies, const double*
     DFT_TRY(fft3d_on_stream(c->plan, c->a, -1, s));
     Recip9 r;
     for (int i = 0; i < 9; ++i) r.b[i] = c->recip[i];
-    k_pot_local_force<<<dim3(kLfChunks, natoms), kPotThreads, 0, s>>>(c->a, c->g2, c->nx, c->ny, c->nz, r, d_gth, d_sp, d_pos,
+    k_pot_local_force<<<dim3(kLfChunks, natoms), kPotThreads, 0, s>>>(c->a, c->g2, c->nx, c->ny, c->nz, r, ffd.ff, d_sp, d_pos,
                                                                        g2max > 0.0 ? g2max : 1e300, d_part);
     count_launch();
     DFT_CUDA_TRY(cudaMemcpyAsync(hp.data(), d_part, sizeof(double) * npart, cudaMemcpyDeviceToHost, s));
@@ -935,6 +1033,50 @@ extern "C" int dftcuda_local_forces(dftcuda_pctx* c, int nspecies, const double*
   return st;
 }
 
+extern "C" int dftcuda_ionic_potential(dftcuda_pctx* c, int nspecies, const double* gth, int natoms, const int* atom_species,
+                                       const double* positions, double g2max, double* v_out_g, double* vloc_r) {
+  if (!gth) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "ionic_potential: null parameters");
+  FFArgs f;
+  f.gth = gth;
+  return ionic_impl(c, nspecies, f, natoms, atom_species, positions, g2max, v_out_g, vloc_r);
+}
+
+extern "C" int dftcuda_ionic_potential_radial(dftcuda_pctx* c, int nspecies, const size_t* mesh_off, const double* r,
+                                              const double* rab, const double* vloc, const double* z_valence, int natoms,
+                                              const int* atom_species, const double* positions, double g2max, double* v_out_g,
+                                              double* vloc_r) {
+  if (!mesh_off || !r || !rab || !vloc || !z_valence) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "ionic_potential_radial: null mesh");
+  FFArgs f;
+  f.mesh_off = mesh_off;
+  f.r = r;
+  f.rab = rab;
+  f.vloc = vloc;
+  f.z = z_valence;
+  return ionic_impl(c, nspecies, f, natoms, atom_species, positions, g2max, v_out_g, vloc_r);
+}
+
+extern "C" int dftcuda_local_forces(dftcuda_pctx* c, int nspecies, const double* gth, int natoms, const int* atom_species,
+                                    const double* positions, double g2max, const double* rho_r, double* forces) {
+  if (!gth) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "local_forces: null parameters");
+  FFArgs f;
+  f.gth = gth;
+  return local_forces_impl(c, nspecies, f, natoms, atom_species, positions, g2max, rho_r, forces);
+}
+
+extern "C" int dftcuda_local_forces_radial(dftcuda_pctx* c, int nspecies, const size_t* mesh_off, const double* r,
+                                           const double* rab, const double* vloc, const double* z_valence, int natoms,
+                                           const int* atom_species, const double* positions, double g2max, const double* rho_r,
+                                           double* forces) {
+  if (!mesh_off || !r || !rab || !vloc || !z_valence) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "local_forces_radial: null mesh");
+  FFArgs f;
+  f.mesh_off = mesh_off;
+  f.r = r;
+  f.rab = rab;
+  f.vloc = vloc;
+  f.z = z_valence;
+  return local_forces_impl(c, nspecies, f, natoms, atom_species, positions, g2max, rho_r, forces);
+}
+
 extern "C" int dftcuda_radial_table(int l, size_t nr, const double* r, const double* rbeta, const double* rab, size_t nq,
                                     double gmax, double* out) {
   if (l < 0 || nr == 0 || nq < 2 || !r || !rbeta || !rab || !out || !(gmax > 0.0) || nr > (size_t)INT32_MAX || nq > 65535)
@@ -945,7 +1087,7 @@ extern "C" int dftcuda_radial_table(int l, size_t nr, const double* r, const dou
   cudaStream_t s = nullptr;
   int st = DFTCUDA_OK;
   auto run = [&]() -> int {
-    DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamDefault));
     DFT_CUDA_TRY(cudaMemcpyAsync(d, r, sizeof(double) * nr, cudaMemcpyDefault, s));
     DFT_CUDA_TRY(cudaMemcpyAsync(d + nr, rbeta, sizeof(double) * nr, cudaMemcpyDefault, s));
     DFT_CUDA_TRY(cudaMemcpyAsync(d + 2 * nr, rab, sizeof(double) * nr, cudaMemcpyDefault, s));

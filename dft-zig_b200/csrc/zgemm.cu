@@ -282,23 +282,13 @@ static bool zgemm_fma() {
 template <bool AKC, bool BKC, bool CJA, bool CJB>
 static void launch(const GemmArgs& g, dim3 grid, int kps, double2* part, cudaStream_t s) {
   if (!zgemm_fma()) {
-    static int dattr = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dattr != dev) {
-      cudaFuncSetAttribute(k_zgemm_dmma<AKC, BKC, CJA, CJB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kZgemmDmmaSmem);
-      dattr = dev;
-    }
+    ensure_max_dynamic_smem((const void*)k_zgemm_dmma<AKC, BKC, CJA, CJB>, (int)kZgemmDmmaSmem);
     k_zgemm_dmma<AKC, BKC, CJA, CJB><<<grid, 256, kZgemmDmmaSmem, s>>>(g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r,
                                                                       g.ldo_c, g.alpha, g.beta, kps, part);
     count_launch();
     return;
   }
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_zgemm<AKC, BKC, CJA, CJB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kZgemmSmem);
-    attr = true;
-  }
+  ensure_max_dynamic_smem((const void*)k_zgemm<AKC, BKC, CJA, CJB>, (int)kZgemmSmem);
   k_zgemm<AKC, BKC, CJA, CJB><<<grid, 256, kZgemmSmem, s>>>(g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r, g.ldo_c, g.alpha,
                                                    g.beta, kps, part); count_launch();
 }

@@ -154,14 +154,6 @@ def ewald_forces(cell: np.ndarray, charges: np.ndarray, pos: np.ndarray, tol: fl
     return 2.0 * f
 
 
-def gth_alpha(sp: sysm.SpeciesData) -> float:
-    """G -> 0 limit of Omega (V_loc(G) + 8 pi Z / G^2) for the GTH form (Ry): the epsatm of
-    energy.zig:350-365 for the synthetic species."""
-    p = sp.params
-    rl = p["rloc"]
-    return 2.0 * (2.0 * math.pi * p["z"] * rl * rl + math.sqrt(8.0 * math.pi**3) * rl**3 * (p["c1"] + 3.0 * p["c2"]))
-
-
 # ---------------------------------------------------------------------------------------------
 # Mixing
 # ---------------------------------------------------------------------------------------------
@@ -411,6 +403,7 @@ class ScfParams:
     energy_tol_per_atom: Optional[float] = None  # stop once |E - E_target| < tol (time-to-SCF runs)
     energy_target: Optional[float] = None
     initial_density: Optional[np.ndarray] = None  # rho(r) on the FFT grid; None = flat N_e / Omega
+    kpoints: Optional[list] = None  # explicit [(k_frac, weight)] in place of the kmesh (weights sum to 1)
 
 
 @dataclass
@@ -453,7 +446,7 @@ class ScfState:
         dims = self.dims = sysm.fft_box(p.ecut, c.recip)
         N = self.N = dims[0] * dims[1] * dims[2]
         self.vol = c.volume
-        kpts = sysm.monkhorst_pack(p.kmesh)
+        kpts = [(np.asarray(k, float), float(w)) for k, w in p.kpoints] if p.kpoints is not None else sysm.monkhorst_pack(p.kmesh)
         self.nk = len(kpts)
         # k-points dealt to the ranks by basis size; this rank builds inputs and contexts for its own
         costs = [sysm.basis(c.recip, p.ecut, k).hkl.shape[0] for k, _ in kpts] if self.comm.size > 1 else None
@@ -483,9 +476,8 @@ class ScfState:
             import torch
 
             self.pot = backend.dz.PotentialContext(dims, self.vol, c.recip, history=max(1, p.pulay_history), functional=p.xc)
-            gth = [[sp.params["z"], sp.params["rloc"], sp.params.get("c1", 0.0), sp.params.get("c2", 0.0),
-                    sp.params.get("c3", 0.0), sp.params.get("c4", 0.0)] for sp in c.species]
-            _, self.vloc_d = self.pot.ionic(gth, c.atom_species, c.positions, 4.0 * p.ecut, device=True)
+            _, self.vloc_d = self.pot.ionic_radial([sp.mesh for sp in c.species], c.atom_species, c.positions, 4.0 * p.ecut,
+                                                   device=True)
             self.vloc_r = self.vloc_d.cpu().numpy()
         else:
             if p.xc != "lda":
@@ -521,7 +513,9 @@ class ScfState:
         t = time.perf_counter()
         self.e_ion = ewald_energy(c.cell, np.array([c.species[s].z_val for s in c.atom_species]), c.positions)
         tm["ewald"] = time.perf_counter() - t
-        self.psp_core = sum(gth_alpha(c.species[s]) for s in c.atom_species) * self.nelec / self.vol
+        # psp_core = sum of epsatm over the atoms x N_e / Omega (energy.zig:350-365)
+        eps = [sysm.epsatm(sp) for sp in c.species]
+        self.psp_core = sum(eps[s] for s in c.atom_species) * self.nelec / self.vol
         self.history = []
         self.energy = float("nan")
         self.terms = {}
@@ -569,7 +563,13 @@ class ScfState:
         if self.comm.size > 1:
             table = self.comm.sum(table)
         self.values = values = [table[k] for k in range(self.nk)]
-        if p.smearing:
+        dev_occ = None
+        if p.smearing and self.dev:
+            # Fermi level, occupations and the band / entropy sums in FP64 on the device
+            mu, occ_tab, eb, es = self.backend.dz.fermi_occupations(table, self.kweights, nelec, p.smearing)
+            occs = [occ_tab[k] for k in range(self.nk)]
+            dev_occ = (eb, es)
+        elif p.smearing:
             mu = fermi_level(nelec, p.smearing, self.kweights, values)
             occs = [fd_occ(v, mu, p.smearing) for v in values]
         else:
@@ -586,11 +586,14 @@ class ScfState:
             rho_out = np.zeros(N)
         e_band = 0.0
         e_ent = 0.0
-        for k in range(self.nk):
-            wts = self.kweights[k] * occs[k] * 2.0
-            e_band += float(np.dot(wts, values[k]))
-            if p.smearing:
-                e_ent += self.kweights[k] * 2.0 * p.smearing * float(entropy_term(occs[k]).sum())
+        if dev_occ is not None:
+            e_band, e_ent = dev_occ[0], p.smearing * dev_occ[1]
+        else:
+            for k in range(self.nk):
+                wts = self.kweights[k] * occs[k] * 2.0
+                e_band += float(np.dot(wts, values[k]))
+                if p.smearing:
+                    e_ent += self.kweights[k] * 2.0 * p.smearing * float(entropy_term(occs[k]).sum())
         for i, k in enumerate(self.kglobal):
             self.backend.density(i, self.vectors[i], self.kweights[k] * occs[k] * 2.0, rho_out)
         if self.comm.size > 1:
@@ -664,10 +667,8 @@ class ScfState:
         if not self.dev:
             raise ValueError("forces need the resident driver (GpuBackend(resident=True))")
         c, p = self.c, self.p
-        gth = [[sp.params["z"], sp.params["rloc"], sp.params.get("c1", 0.0), sp.params.get("c2", 0.0),
-                sp.params.get("c3", 0.0), sp.params.get("c4", 0.0)] for sp in c.species]
         natoms = len(c.atom_species)
-        f_loc = self.pot.local_forces(gth, c.atom_species, c.positions, self.rho, 4.0 * p.ecut)
+        f_loc = self.pot.local_forces_radial([sp.mesh for sp in c.species], c.atom_species, c.positions, self.rho, 4.0 * p.ecut)
         f_nl = np.zeros((natoms, 3))
         for i, k in enumerate(self.kglobal):
             w = self.kweights[k] * np.asarray(self.occs[k]) * 2.0

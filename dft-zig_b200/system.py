@@ -44,6 +44,12 @@ class SpeciesData:
     betas: list  # (l, r*beta(r))
     dij: np.ndarray  # Ry
     params: dict = field(default_factory=dict)
+    vloc: np.ndarray = None  # local potential on the mesh (Ry), the UPF's PP_LOCAL
+
+    @property
+    def mesh(self):
+        """(r, rab, vloc, z_valence): the inputs of the radial local form factor."""
+        return (self.r, self.rab, self.vloc, self.z_val)
 
 
 def log_mesh(zmesh=14.0, xmin=-7.0, dx=0.0125, rmax=10.0):
@@ -70,7 +76,12 @@ def species(name: str) -> SpeciesData:
         k = h.shape[0]
         dij[o : o + k, o : o + k] = 2.0 * h
         o += k
-    return SpeciesData(name, p["z"], r, rab, betas, dij, p)
+    # the GTH local potential tabulated on the mesh, Hartree -> Ry
+    from scipy.special import erf
+
+    rl = p["rloc"]
+    vloc = 2.0 * (-p["z"] / r * erf(r / (math.sqrt(2.0) * rl)) + np.exp(-0.5 * (r / rl) ** 2) * (p["c1"] + p["c2"] * (r / rl) ** 2))
+    return SpeciesData(name, p["z"], r, rab, betas, dij, p, vloc)
 
 
 @dataclass
@@ -316,25 +327,54 @@ def projector_derivatives(sp: SpeciesData, kpg: np.ndarray, tables) -> np.ndarra
     return np.array(rows)
 
 
+def local_form_factor(sp: SpeciesData, q: np.ndarray) -> np.ndarray:
+    """The reference's local form factor in its default short_range mode (local_vq_short_range,
+    pseudopotential/form_factor.zig:223-262), Ry: 4 pi sum_j r_j^2 [V_loc(r_j) + 2 Z / r_j]
+    sinc(q r_j) rab_j w_j - 8 pi Z / q^2, the Coulomb term left out at q < 1e-10 (so V(0) is epsatm)."""
+    r, rab, vloc, z = sp.mesh
+    n = r.size
+    w = np.ones(n)
+    if n >= 10:
+        cw = np.array([23.75, 95.10, 55.20, 79.30, 70.65]) / 72.0
+        w[:5] = cw
+        w[n - 5:] = cw[::-1]
+    vc = np.where(r < 1e-10, 0.0, 2.0 * z / np.where(r < 1e-10, 1.0, r))
+    terms = r * r * (vloc + vc) * rab * w
+    q = np.atleast_1d(np.asarray(q, dtype=np.float64))
+    out = np.empty(q.size)
+    for i0 in range(0, q.size, 4096):  # bounded temporaries
+        x = np.outer(q[i0:i0 + 4096], r)
+        small = np.abs(x) < 1e-12
+        out[i0:i0 + 4096] = 4.0 * math.pi * (np.where(small, 1.0, np.sin(x) / np.where(small, 1.0, x)) @ terms)
+    big = q >= 1e-10
+    out[big] -= 8.0 * math.pi * z / (q[big] * q[big])
+    return out
+
+
+def epsatm(sp: SpeciesData) -> float:
+    """compute_epsatm (form_factor.zig:264-268): the q = 0 value of the short-range form factor."""
+    return float(local_form_factor(sp, np.zeros(1))[0])
+
+
 def local_potential(c: Crystal, dims, ecut: float) -> np.ndarray:
-    """V(r) (Ry) on the x-fastest box from the analytic GTH local form factors, |G|^2 <= 4 ecut, V(0) = 0."""
+    """V(r) (Ry) on the x-fastest box: V(G) = (1/Omega) sum_atoms V_s(|G|) e^{-iG tau} from each
+    species' radial mesh (local_form_factor), zero at |G| < 1e-10 and for |G|^2 >= 4 ecut
+    (build_ionic_potential_grid, scf/potential.zig:279-318, ecutrho = 4 ecut)."""
     nx, ny, nz = dims
     f = [np.fft.fftfreq(n, 1.0 / n) for n in dims]
     hz, hy, hx = np.meshgrid(f[2], f[1], f[0], indexing="ij")
     gv = np.stack([hx.ravel(), hy.ravel(), hz.ravel()], axis=1) @ c.recip
     g2 = (gv * gv).sum(axis=1)
+    q = np.sqrt(g2)
+    keep = (q >= 1e-10) & (g2 < 4.0 * ecut)
+    uq, inv = np.unique(q[keep], return_inverse=True)
     vg = np.zeros(g2.size, complex)
     for s, sp in enumerate(c.species):
-        p = sp.params
-        rl = p["rloc"]
-        e = np.exp(-0.5 * g2 * rl * rl)
-        safe = np.where(g2 > 1e-12, g2, 1.0)
-        ff = np.where(g2 > 1e-12, (-4 * math.pi * p["z"] / safe * e + math.sqrt(8 * math.pi**3) * rl**3 * e * (p["c1"] + p["c2"] * (3 - g2 * rl * rl))), 0.0)
-        sf = np.zeros(g2.size, complex)
+        ff = local_form_factor(sp, uq)[inv]
+        sf = np.zeros(keep.sum(), complex)
         for a in np.where(c.atom_species == s)[0]:
-            sf += np.exp(-1j * (gv @ c.positions[a]))
-        vg += sf * 2.0 * ff / c.volume
-    vg[g2 > 4 * ecut] = 0.0
+            sf += np.exp(-1j * (gv[keep] @ c.positions[a]))
+        vg[keep] += sf * ff / c.volume
     n = nx * ny * nz
     return np.fft.ifftn(vg.reshape(nz, ny, nx) * n).real.ravel().copy()
 

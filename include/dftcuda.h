@@ -14,7 +14,9 @@
  * and copies through its own device buffers when needed.  Every call returns an int
  * status: DFTCUDA_OK (0) or one of the negative codes below, which map one-to-one onto
  * the reference's Zig error set.  All calls are synchronous with respect to the host
- * unless named *_async.
+ * unless named *_async.  The library's streams are ordered after work queued on the legacy default
+ * stream, so device inputs written there need no extra synchronisation; inputs written on other
+ * streams must be complete (synchronise those streams) before a call reads them.
  */
 #ifndef DFTCUDA_H
 #define DFTCUDA_H
@@ -62,6 +64,14 @@ const char* dftcuda_last_error_message(void);
 
 /* Number of CUDA devices visible (0 on a host without a GPU; never fails). */
 int dftcuda_device_count(void);
+
+/* Failure injection for tests of the timeout path (no reference counterpart).  Every device-side wait
+ * in the library is bounded: the subspace eigensolver's grid barrier polls about a second, then sets
+ * an error flag, its blocks return, and the call reports DFTCUDA_ERR_TIMEOUT with the context still
+ * usable.  polls > 0 sets that barrier's poll budget (0 restores the default); unreachable != 0 raises
+ * every barrier's target by one arrival that no block makes, so each wait runs out its budget.
+ * Process-wide; applies to launches made after the call. */
+int dftcuda_debug_set_wait_limits(long polls, int unreachable);
 
 /* ------------------------------------------------------------------------------------------
  * Per-k-point context: replaces the ApplyContext + KpointApplyCache pair
@@ -235,13 +245,29 @@ int dftcuda_accumulate_density(dftcuda_kctx* ctx, const double* vectors, size_t 
  * the library holds until exit.  vectors [n x nbands], weights[nbands] and rho[N] must all be device
  * pointers (host pointers are rejected), nbands may not exceed DFTCUDA_NOALLOC_MAX_BANDS, and rho is
  * ADDED to exactly as in dftcuda_accumulate_density (bands with weight <= 0 contribute nothing).
- * The first call on each device looks up the scratch address; make that first call before any
- * stream capture.  All calls share the one scratch array, so calls that overlap on the GPU (from
- * two host threads, or two contexts whose streams run concurrently) race; serialise them. */
+ * The call runs on the device the context was created on and is ordered after all work queued on
+ * the legacy default stream; inputs written on any other stream must be complete (synchronise that
+ * stream) before the call.  It returns after its work on the context's stream has finished.
+ * The first call on each device looks up the scratch address, so make that first call before any
+ * stream capture begins.  All calls share the one scratch array, whose contents persist from call to
+ * call, so calls that overlap on the GPU (from two host threads, or two contexts whose streams run
+ * concurrently) race; serialise them. */
 #define DFTCUDA_NOALLOC_SCRATCH_BYTES ((size_t)48 << 20)
 #define DFTCUDA_NOALLOC_MAX_BANDS 4096
 int dftcuda_accumulate_density_noalloc(dftcuda_kctx* ctx, const double* vectors, size_t n, size_t nbands,
                                        const double* weights, double* rho);
+
+/* Fermi level and occupations of an eigenvalue table, FP64 on the device: find_fermi_level_spin with
+ * smearing_occ / smearing_entropy (src/features/scf/fermi_level.zig:7-124), Fermi-Dirac smearing.
+ * values[nk*nbands] (one row of nbands per k-point), kweights[nk] (summing to 1), spin_factor 2 for
+ * unpolarised bands.  The bracket [min e - pad, max e + pad], pad = max(10 sigma, 1e-3), doubles up
+ * to 12 times until it holds nelec; then up to 80 bisections, stopping once |N(mu) - nelec| < 1e-8.
+ * mu_out: the Fermi level; occ (may be NULL): [nk*nbands] 1/(1 + exp((e - mu)/sigma)) (a step at mu
+ * when sigma <= 0); sums (may be NULL): sums[0] = sum_kb spin w_k occ_kb e_kb (band energy),
+ * sums[1] = sum_kb spin w_k S(occ_kb), S(f) = -(f ln f + (1-f) ln(1-f)) (0 within 1e-12 of 0 or 1),
+ * the entropy that enters the energy as -sigma * sums[1].  Host or device pointers. */
+int dftcuda_fermi_occupations(size_t nk, size_t nbands, const double* values, const double* kweights, double nelec,
+                              double sigma, double spin_factor, double* mu_out, double* occ, double* sums);
 
 /* ------------------------------------------------------------------------------------------
  * Profiling: the ScfProfile counters (src/features/scf/logging.zig:114-131) measured on the device
@@ -340,6 +366,24 @@ int dftcuda_ionic_potential(dftcuda_pctx* ctx, int nspecies, const double* gth, 
 int dftcuda_local_forces(dftcuda_pctx* ctx, int nspecies, const double* gth, int natoms, const int* atom_species,
                          const double* positions, double g2max, const double* rho_r, double* forces);
 int dftcuda_pulay_reset(dftcuda_pctx* ctx);
+
+/* dftcuda_ionic_potential and dftcuda_local_forces for pseudopotentials given by their radial mesh
+ * (the UPF local part), with the reference's local form factor in its default short_range mode
+ * (local_vq_short_range, src/features/pseudopotential/form_factor.zig:223-262; config/defaults.zig:28),
+ * evaluated at every |G| of the box as the SCF does (ionic_local_potential, hamiltonian.zig):
+ *   V_s(q) = 4 pi sum_j r_j^2 [vloc_j + 2 Z_s / r_j] sinc(q r_j) rab_j w_j - 8 pi Z_s / q^2   (Ry),
+ * w the composite-trapezoid weights of radial_integration.zig:7-13, the 2Z/r term skipped at
+ * r < 1e-10.  Species s uses points [mesh_off[s], mesh_off[s+1]) of r, rab and vloc (Ry; mesh_off[0]
+ * = 0, nspecies + 1 entries, host memory), z_valence[nspecies].  V(G) = (1/vol) sum_atoms V_s(|G|)
+ * e^{-iG.tau} for |G| >= 1e-10 and G^2 < g2max (build_ionic_potential_grid, potential.zig:279-318;
+ * g2max <= 0: no cut); the local forces (local_pseudo_forces, forces/local_force.zig:66-111) from the
+ * same V_s.  Other arguments and outputs as the GTH forms above. */
+int dftcuda_ionic_potential_radial(dftcuda_pctx* ctx, int nspecies, const size_t* mesh_off, const double* r, const double* rab,
+                                   const double* vloc, const double* z_valence, int natoms, const int* atom_species,
+                                   const double* positions, double g2max, double* v_out_g, double* vloc_r);
+int dftcuda_local_forces_radial(dftcuda_pctx* ctx, int nspecies, const size_t* mesh_off, const double* r, const double* rab,
+                                const double* vloc, const double* z_valence, int natoms, const int* atom_species,
+                                const double* positions, double g2max, const double* rho_r, double* forces);
 
 /* Density symmetrisation (symmetrize_density, scf/density_symmetry.zig:27-94), in place on rho_r
  * (N doubles, x fastest, host or device): rho(G) <- (1/nops) sum_op rho(k_rot G) e^{-2 pi i frac(G.t)}

@@ -9,21 +9,20 @@ Cells follow the workloads the hot path is measured on:
   al4    FCC Al conventional cell a = 4.05 A with a seeded symmetric strain in [-1%, 1%]
   sige8  8-atom zincblende-type Si(1-x)Ge(x) cell, a = 5.43 + 0.23 x A, +-2% strain
 
-The local potential V(r) = Re N IFFT(sum_s S_s(G) v_s(|G|)) uses the analytic
-local form factor of the Goedecker-Teter-Hutter functional form (the synthetic
-species of ``pseudo.py``) on |G|^2 <= 4 ecut, with V(G=0) = 0, built like
-build_local_potential_real (src/features/scf/potential.zig:320-334).
+The local potential V(r) = Re N IFFT(sum_s S_s(G) v_s(|G|)) uses the short-range local
+form factor of each species' radial mesh (local_vq_short_range, form_factor.zig:223-262)
+on |G|^2 < 4 ecut, with V(G=0) = 0, built like build_local_potential_real
+(src/features/scf/potential.zig:320-334).
 """
 from __future__ import annotations
 
-import math
 from dataclasses import dataclass
 
 import numpy as np
 
 from . import fft as offt
 from .apply import ApplyContext, Atom
-from .pseudo import Species, build_nonlocal_species, radial_tables, synthetic_species
+from .pseudo import Species, build_nonlocal_species, ionic_potential_radial, radial_tables, synthetic_species
 from .pw import ANGSTROM_TO_BOHR, Grid, auto_grid, build_fft_index_map, cell_volume, generate_basis, index_to_freq, reciprocal
 
 SI8_FRAC = np.array(
@@ -112,39 +111,12 @@ def make_cell(name: str, seed: int = 0) -> Cell:
     raise KeyError(name)
 
 
-def gth_local_form_factor(sp: Species, g2: np.ndarray, volume: float) -> np.ndarray:
-    """Analytic GTH local form factor (Ry), G = 0 term excluded (set to 0)."""
-    p = sp.gth
-    rl = p["rloc"]
-    g = np.sqrt(g2)
-    x2 = g2 * rl * rl
-    e = np.exp(-0.5 * x2)
-    with np.errstate(divide="ignore", invalid="ignore"):
-        coul = np.where(g2 > 1e-12, -4.0 * math.pi * p["z"] / np.where(g2 > 1e-12, g2, 1.0) * e, 0.0)
-    short = math.sqrt(8.0 * math.pi**3) * rl**3 * e * (p["c1"] + p["c2"] * (3.0 - x2))
-    v = (coul + np.where(g2 > 1e-12, short, 0.0)) / volume
-    del g
-    return 2.0 * v  # Hartree -> Ry
-
-
 def local_potential_r(c: Cell, grid: Grid, ecut_ry: float) -> np.ndarray:
-    """V(r) on the FFT-order grid from the analytic local form factors and structure factors."""
-    recip = c.recip
-    fx = np.array([index_to_freq(i, grid.nx) for i in range(grid.nx)])
-    fy = np.array([index_to_freq(i, grid.ny) for i in range(grid.ny)])
-    fz = np.array([index_to_freq(i, grid.nz) for i in range(grid.nz)])
-    zz, yy, xx = np.meshgrid(fz, fy, fx, indexing="ij")
-    hkl = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], axis=1).astype(np.float64)
-    gc = hkl @ recip
-    g2 = (gc * gc).sum(axis=1)
-    vg = np.zeros(grid.count, dtype=np.complex128)
-    for s, sp in enumerate(c.species):
-        sf = np.zeros(grid.count, dtype=np.complex128)
-        for a in c.atoms:
-            if a.species_index == s:
-                sf += np.exp(-1j * (gc @ a.position))
-        vg += sf * gth_local_form_factor(sp, g2, c.volume)
-    vg[g2 > 4.0 * ecut_ry] = 0.0
+    """V(r) on the FFT-order grid: the ionic potential of the species' radial meshes with the
+    reference's short-range form factor (pseudo.ionic_potential_radial), |G|^2 < 4 ecut, V(0) = 0."""
+    meshes = [(sp.r, sp.rab, sp.vloc_r, sp.z_val) for sp in c.species]
+    vg, _ = ionic_potential_radial(meshes, [a.species_index for a in c.atoms], [a.position for a in c.atoms],
+                                   (grid.nx, grid.ny, grid.nz), c.recip, c.volume, 4.0 * ecut_ry)
     vr = offt.fft3d_inverse(vg * grid.count, grid.nx, grid.ny, grid.nz)
     return vr.real.copy()
 

@@ -105,3 +105,26 @@ def ewald_forces(cell, charges, positions, eta, tol=1e-14):
     for i in range(len(z)):
         out[i] += (4.0 * math.pi / vol) * z[i] * (G * (k * np.imag(np.exp(1j * (G @ pos[i])) * np.conj(S)))[:, None]).sum(axis=0)
     return 2.0 * out
+
+
+def local_forces_radial(rho, meshes, atom_species, positions, dims, recip, g2max=0.0):
+    """local_pseudo_forces (forces/local_force.zig:66-111) with the short-range form factor of each
+    species' radial mesh (pseudo.local_vq_short_range, form_factor.zig:223-262): F_a = sum_G V_s(|G|) G
+    Im(e^{iG.tau_a} rho(G)) over |G| >= 1e-10 and G^2 < g2max.  meshes: (r, rab, vloc_Ry, z) per species."""
+    from oracle import pseudo
+
+    G = op.g_vectors_cart(dims, recip)
+    g2 = (G * G).sum(axis=1)
+    q = np.sqrt(g2)
+    keep = q >= 1e-10
+    if g2max > 0.0:
+        keep &= g2 < g2max
+    G, q = G[keep], q[keep]
+    rg = op.to_g(rho, dims)[keep]
+    uq, inv = np.unique(q, return_inverse=True)
+    vq = [pseudo.local_vq_short_range_vec(m[0], m[1], m[2], m[3], uq)[inv] for m in meshes]
+    out = np.zeros((len(atom_species), 3))
+    for a, (s, tau) in enumerate(zip(atom_species, np.asarray(positions, dtype=np.float64))):
+        w = vq[s] * np.imag(np.exp(1j * (G @ tau)) * rg)
+        out[a] = (G * w[:, None]).sum(axis=0)
+    return out

@@ -350,3 +350,64 @@ def expand_dij_m(ns: NonlocalSpecies) -> np.ndarray:
             for mi in range(ns.m_counts[b]):
                 d[ns.m_offsets[b] + mi, ns.m_offsets[j] + mi] = ns.dij[b, j]
     return d
+
+
+# -- local form factor (radial quadrature) ------------------------------------------------------
+
+
+def local_vq_short_range(r: np.ndarray, rab: np.ndarray, vloc: np.ndarray, z_val: float, q: float) -> float:
+    """form_factor.zig:223-262 (the default local_potential mode, config/defaults.zig:28):
+    V(q) = 4 pi sum_i r_i^2 [V_loc(r_i) + 2 Z / r_i] sinc(q r_i) rab_i w_i - 8 pi Z / q^2 (Ry), the
+    Coulomb term skipped at r < 1e-10 and at q < 1e-10 (where the short-range part alone is returned:
+    compute_epsatm, form_factor.zig:264-268)."""
+    n = r.size
+    w = ctrap_weights(n)
+    vc = np.where(r < 1e-10, 0.0, 2.0 * z_val / np.where(r < 1e-10, 1.0, r))
+    x = q * r
+    sinc = np.where(np.abs(x) < 1e-12, 1.0, np.sin(x) / np.where(np.abs(x) < 1e-12, 1.0, x))
+    total = 0.0
+    terms = r * r * (vloc + vc) * sinc * rab * w
+    for t in terms:  # sequential sum, as the reference's loop
+        total += t
+    v = 4.0 * math.pi * total
+    if q < 1e-10:
+        return v
+    return v - 8.0 * math.pi * z_val / (q * q)
+
+
+def local_vq_short_range_vec(r, rab, vloc, z_val, q: np.ndarray) -> np.ndarray:
+    """local_vq_short_range at many q at once (the sum over the mesh as a dot product)."""
+    n = r.size
+    w = ctrap_weights(n)
+    vc = np.where(r < 1e-10, 0.0, 2.0 * z_val / np.where(r < 1e-10, 1.0, r))
+    terms = r * r * (vloc + vc) * rab * w
+    q = np.asarray(q, dtype=np.float64)
+    x = np.outer(q, r)
+    small = np.abs(x) < 1e-12
+    sinc = np.where(small, 1.0, np.sin(x) / np.where(small, 1.0, x))
+    v = 4.0 * math.pi * (sinc @ terms)
+    big = q >= 1e-10
+    v[big] -= 8.0 * math.pi * z_val / (q[big] * q[big])
+    return v
+
+
+def ionic_potential_radial(meshes, atom_species, positions, dims, recip, volume, g2max=0.0):
+    """build_ionic_potential_grid (scf/potential.zig:279-318) with ionic_local_potential
+    (hamiltonian.zig) and the short-range form factor: V(G) = (1 / Omega) sum_atoms V_s(|G|) e^{-i G tau}
+    on the FFT-order box, 0 at |G| < 1e-10 and, with g2max > 0, for |G|^2 >= g2max.  meshes: per
+    species (r, rab, vloc_Ry, z_valence)."""
+    f = [np.fft.fftfreq(n, 1.0 / n) for n in dims]
+    hz, hy, hx = np.meshgrid(f[2], f[1], f[0], indexing="ij")
+    gv = np.stack([hx.ravel(), hy.ravel(), hz.ravel()], axis=1) @ np.asarray(recip)
+    g2 = (gv * gv).sum(axis=1)
+    q = np.sqrt(g2)
+    uq, inv = np.unique(q, return_inverse=True)
+    vq = [local_vq_short_range_vec(m[0], m[1], m[2], m[3], uq)[inv] for m in meshes]
+    vg = np.zeros(g2.size, complex)
+    for a, s in enumerate(atom_species):
+        vg += vq[s] * np.exp(-1j * (gv @ np.asarray(positions[a])))
+    vg /= volume
+    vg[q < 1e-10] = 0.0
+    if g2max > 0.0:
+        vg[g2 >= g2max] = 0.0
+    return vg, vq

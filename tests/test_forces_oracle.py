@@ -57,6 +57,35 @@ def test_local_forces_are_minus_the_energy_gradient():
         assert abs(f[a, d] - fd) < 1e-6 * max(1.0, abs(fd)), (a, d, f[a, d], fd)
 
 
+def test_radial_local_forces_are_minus_the_energy_gradient():
+    """The radial-mesh local forces (local_force.zig:66-111 with local_vq_short_range) are minus the
+    finite-difference gradient of the local energy Omega sum_G Re(V(G)* rho(G)) of the same form."""
+    from oracle import pseudo
+
+    c = system.crystal("si8")
+    ecut = 8.0
+    dims = system.fft_box(ecut, c.recip)
+    meshes = [sp.mesh for sp in c.species]
+    rng = np.random.default_rng(3)
+    N = dims[0] * dims[1] * dims[2]
+    g2 = op.g2_table(dims, c.recip)
+    rho = 0.02 + 0.01 * op.to_r(np.where(g2 < 3.0, op.to_g(rng.normal(size=N), dims), 0.0), dims)
+    pos = np.array(c.positions, dtype=np.float64)
+    f = of.local_forces_radial(rho, meshes, c.atom_species, pos, dims, c.recip, 4 * ecut)
+
+    def energy(p):
+        vg, _ = pseudo.ionic_potential_radial(meshes, c.atom_species, p, dims, c.recip, c.volume, 4 * ecut)
+        return c.volume * float(np.real(np.vdot(vg, op.to_g(rho, dims))))
+
+    h = 1e-5
+    for a, d in [(1, 1), (6, 0)]:
+        pp, pm = pos.copy(), pos.copy()
+        pp[a, d] += h
+        pm[a, d] -= h
+        fd = -(energy(pp) - energy(pm)) / (2 * h)
+        assert abs(f[a, d] - fd) < 1e-6 * max(1.0, abs(fd)), (a, d, f[a, d], fd)
+
+
 def test_nonlocal_forces_are_minus_the_energy_gradient():
     c = system.crystal("si2")
     ecut = 10.0

@@ -1,0 +1,94 @@
+"""The plain FP64 GPU path against the oracle at the benchmark configurations' own sizes.
+
+* Si216 (3x3x3 conventional cell, seed 3, 25 Ry, Gamma): the 108^3 box with 61,565 plane waves and
+  216 atoms of projectors.  H|psi> on 8 columns (FP64 1e-11, FP32 passes 5e-5) and the band density
+  (1e-12) against the oracle, computed here.
+* Si64 at Gamma (30 Ry, 75^3, 160 bands, max_subspace 648): the device Davidson solver from the
+  reference's LCG start against the oracle's serial solver (lobpcg/serial.zig:55-307), eigenvalues
+  within 1e-7 Ry.
+* Config 1's gate: Si2 at 20 Ry on the 4x4x4 mesh (36 k-points after k/-k folding), fixed
+  occupations: total energy per atom within 1e-8 Ry and every eigenvalue within 1e-7 Ry of the oracle
+  SCF driven through the same host driver.
+* Config 3 (Al4, 25 Ry, Fermi-Dirac 0.02 Ry): three points of the 8x8x8 mesh with different basis
+  sizes, the same two bars.
+
+The oracle results of the last three are committed fixtures (tests/golden/config_parity.json, made by
+tests/golden/make_config_parity.py): the numpy oracle needs minutes for them.
+"""
+import importlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from tests.golden.make_config_parity import AL4_KPOINTS, AL4_PARAMS, SI2_PARAMS, SI64_OPTS
+from tests.helpers import kproblem, make_context, random_block, rel_err
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "config_parity.json")))
+
+
+@pytest.fixture(scope="module")
+def si216():
+    return kproblem("si216", 25.0, (0.0, 0.0, 0.0), 3)
+
+
+def test_si216_box_and_basis(si216):
+    assert (si216.grid.nx, si216.grid.ny, si216.grid.nz) == (108, 108, 108)
+    assert si216.ctx.n == 61565
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-11), (1, 5e-5)], ids=["fp64", "fp32-passes"])
+def test_si216_apply_matches_oracle(dz, si216, precision, tol):
+    kc = make_context(dz, si216, precision)
+    x = random_block(si216.ctx.n, 8, 21)
+    assert rel_err(kc.apply_hamiltonian_batched(x), si216.ctx.apply_batch(x)) < tol
+    kc.close()
+
+
+def test_si216_density_matches_oracle(dz, si216):
+    from oracle import density as odens
+
+    kc = make_context(dz, si216)
+    v = random_block(si216.ctx.n, 6, 22)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    w = np.array([2.0, 2.0, 1.5, 1.0, 0.0, 0.5])
+    rho = np.zeros(si216.grid.count)
+    kc.accumulate_band_density(v, w, rho)
+    ref = odens.accumulate_density(si216.grid, si216.ctx.map, v, w, 1.0 / si216.grid.volume)
+    assert rel_err(rho, ref) < 1e-12
+    kc.close()
+
+
+def test_si64_gamma_davidson_matches_oracle(dz):
+    g = GOLDEN["si64_gamma_davidson"]
+    kp = kproblem("si64", 30.0)
+    assert kp.ctx.n == g["n_pw"]
+    kc = make_context(dz, kp)
+    r = kc.hermitian_eigen_decomp_iterative(kp.ctx.basis.kinetic, g["nbands"], dz.Options(**SI64_OPTS))
+    kc.close()
+    assert r.converged
+    assert np.abs(np.asarray(r.values) - np.asarray(g["eigenvalues"])).max() < 1e-7
+
+
+def _scf_vs_golden(dz, name, seed, params, golden):
+    scf = importlib.import_module("dftzig_b200.scf")
+    system = importlib.import_module("dftzig_b200.system")
+    gpu = scf.GpuBackend(dz)
+    r = scf.run_scf(system.crystal(name, seed), scf.ScfParams(**params), gpu)
+    gpu.close()
+    assert r.converged and golden["converged"]
+    assert abs(r.energy_per_atom - golden["energy_per_atom"]) < 1e-8
+    assert len(r.eigenvalues) == len(golden["eigenvalues"])
+    for a, b in zip(r.eigenvalues, golden["eigenvalues"]):
+        assert np.abs(np.asarray(a) - np.asarray(b)).max() < 1e-7
+
+
+def test_config1_si2_444_gate(dz):
+    _scf_vs_golden(dz, "si2", 1, SI2_PARAMS, GOLDEN["si2_444_scf"])
+
+
+def test_config3_al4_three_kpoints(dz):
+    _scf_vs_golden(dz, "al4", 2, dict(AL4_PARAMS, kpoints=AL4_KPOINTS), GOLDEN["al4_888_three_k"])

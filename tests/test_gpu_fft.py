@@ -22,7 +22,9 @@ def test_golden_roundtrips(dz):
         p.close()
 
 
-@pytest.mark.parametrize("dims", [(20, 20, 20), (27, 27, 27), (36, 32, 32), (75, 12, 10), (4, 5, 6), (1, 8, 3)])
+# the configs' boxes: Si2 20^3, Al4 27^3, SiGe8 32^3 and 36^3, Si64 75^3, Si216 108^3; plus odd shapes
+@pytest.mark.parametrize("dims", [(20, 20, 20), (27, 27, 27), (32, 32, 32), (36, 36, 36), (36, 32, 32), (75, 75, 75),
+                                  (108, 108, 108), (75, 12, 10), (4, 5, 6), (1, 8, 3)])
 def test_forward_inverse_match_oracle(dz, dims):
     rng = np.random.default_rng(1)
     n = int(np.prod(dims))

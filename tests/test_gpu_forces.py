@@ -39,6 +39,30 @@ def test_local_forces_match_oracle(dz):
         pc.close()
 
 
+def test_local_forces_radial_match_oracle(dz):
+    """Local forces with the radial-mesh form factor (dftcuda_local_forces_radial) against the oracle,
+    two species, displaced atoms, with and without the |G|^2 cut."""
+    _, system = _mods()
+    c = system.crystal("si8")
+    ecut = 10.0
+    dims = system.fft_box(ecut, c.recip)
+    rng = np.random.default_rng(9)
+    sp = rng.integers(0, 2, len(c.atom_species)).astype(np.int32)
+    pos = np.asarray(c.positions) + rng.normal(scale=0.2, size=np.shape(c.positions))
+    meshes = [system.species("Si").mesh, system.species("Ge").mesh]
+    N = dims[0] * dims[1] * dims[2]
+    g2 = op.g2_table(dims, c.recip)
+    rho = 0.02 + 0.01 * op.to_r(np.where(g2 < 4.0, op.to_g(rng.normal(size=N), dims), 0.0), dims)
+    pc = dz.PotentialContext(dims, c.volume, c.recip, history=1)
+    try:
+        for g2max in (0.0, 4 * ecut):
+            ref = of.local_forces_radial(rho, meshes, sp, pos, dims, c.recip, g2max)
+            got = pc.local_forces_radial(meshes, sp, pos, rho, g2max)
+            assert np.abs(got - ref).max() < 1e-10 * max(1.0, np.abs(ref).max())
+    finally:
+        pc.close()
+
+
 def test_nonlocal_forces_match_oracle(dz):
     scf, system = _mods()
     c = system.crystal("si2")

@@ -108,6 +108,27 @@ def test_local_potential_kat_through_abi(dz):
     kc.close()
 
 
+def test_local_potential_kat2_through_abi(dz):
+    """src/tests.zig:975-1104 through the C ABI: with V(r) = N IFFT(V_G) for V_G = 1 at G = 0 and 0.5 at
+    G = (+-1, 0, 0), H psi for psi = delta(G=0) equals the direct O(N^2) convolution of V_G and psi
+    (expected2 of the fixture) to the reference's 1e-10."""
+    import os
+
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "local_potential_kat.npz"))
+    nx, ny, nz = (int(v) for v in d["dims"])
+    N = nx * ny * nz
+
+    def freq(i, n):
+        return i if i <= (n - 1) // 2 else i - n
+
+    hkl = np.array([[freq(x, nx), freq(y, ny), freq(z, nz)] for z in range(nz) for y in range(ny) for x in range(nx)], dtype=np.int32)
+    kc = dz.KpointContext(nx, ny, nz, 1.0, hkl, np.zeros(N), np.zeros((N, 3)))
+    kc.set_vloc(offt.fft3d_inverse(d["v2"] * N, nx, ny, nz).real.copy())
+    out = kc.apply_hamiltonian(d["psi2"])
+    assert np.abs(out - d["expected2"]).max() < float(d["tol"])
+    kc.close()
+
+
 def test_errors_map_to_reference(dz):
     kp = kproblem("si2", 20.0)
     kc = make_context(dz, kp)
@@ -129,17 +150,21 @@ def test_zero_columns_is_a_noop(dz):
     kc.close()
 
 
-@pytest.mark.parametrize("path", ["generic", "four_step"])
-@pytest.mark.parametrize("name,ecut,k,prec", [("si2", 20.0, (0.25, 0.125, 0.0), 0), ("sige8", 20.0, (0.25, 0.25, 0.25), 0), ("al4", 25.0, (0.1, 0.2, 0.3), 1)])
-def test_both_fft_paths_match_oracle(dz, monkeypatch, path, name, ecut, k, prec):
-    """The four-step register-FFT passes and the stage-by-stage passes (DFTCUDA_FFT_PATH=generic)
-    give the oracle's H|psi> and density."""
+@pytest.mark.parametrize("path", ["generic", "planes", "sticks"])
+@pytest.mark.parametrize("name,ecut,k,prec", [("si2", 20.0, (0.25, 0.125, 0.0), 0), ("sige8", 20.0, (0.25, 0.25, 0.25), 0),
+                                              ("al4", 25.0, (0.1, 0.2, 0.3), 1), ("si8", 20.0, (0.5, 0.0, 0.0), 1)])
+def test_all_fft_paths_match_oracle(dz, monkeypatch, path, name, ecut, k, prec):
+    """The three local-operator paths give the oracle's H|psi> and density: the stick-layout passes
+    (the default where nx = ny), the four-step plane-layout passes (DFTCUDA_LOCAL=planes) and the
+    stage-by-stage passes (DFTCUDA_FFT_PATH=generic)."""
     from oracle import density as odens
 
+    monkeypatch.delenv("DFTCUDA_FFT_PATH", raising=False)
+    monkeypatch.delenv("DFTCUDA_LOCAL", raising=False)
     if path == "generic":
         monkeypatch.setenv("DFTCUDA_FFT_PATH", "generic")
-    else:
-        monkeypatch.delenv("DFTCUDA_FFT_PATH", raising=False)
+    elif path == "planes":
+        monkeypatch.setenv("DFTCUDA_LOCAL", "planes")
     kp = kproblem(name, ecut, k)
     kc = make_context(dz, kp, precision=prec)
     x = random_block(kp.ctx.n, 6, 21)

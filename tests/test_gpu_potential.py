@@ -1,5 +1,6 @@
 """The device potential build and Pulay mixing (dftcuda_pctx_*, csrc/potential.cu) against the oracle
 (oracle/potential.py): host and device buffers, odd and even boxes, a triclinic cell."""
+import importlib
 import math
 
 import numpy as np
@@ -126,6 +127,32 @@ def test_ionic_potential_matches_oracle(dz):
             assert vrd.is_cuda and np.abs(vrd.cpu().numpy() - ref_r).max() < 1e-11 * np.abs(ref_r).max()
         with pytest.raises(dz.DftCudaError):
             pc.ionic(gth, np.array([0, 2], dtype=np.int32), pos[:2])
+    finally:
+        pc.close()
+
+
+def test_ionic_potential_radial_matches_oracle(dz):
+    """The radial-mesh form (dftcuda_ionic_potential_radial: the reference's short-range form factor
+    at every |G| of the box): two species with different meshes, 37 atoms in a triclinic cell, an odd
+    box, with and without the |G|^2 cut."""
+    from oracle import pseudo
+
+    system = importlib.import_module("dftzig_b200.system")
+    dims = (27, 24, 25)
+    rng = np.random.default_rng(12)
+    cell = np.linalg.inv(RECIP).T * 2 * math.pi
+    pos = rng.random((37, 3)) @ cell
+    sp = rng.integers(0, 2, 37).astype(np.int32)
+    si, al = system.species("Si"), system.species("Al")
+    meshes = [si.mesh, (al.r[::2], al.rab[::2] * 2.0, al.vloc[::2], al.z_val)]  # a coarser second mesh
+    pc = dz.PotentialContext(dims, VOL, RECIP, history=1)
+    try:
+        for g2max in (0.0, 30.0):
+            ref_g, _ = pseudo.ionic_potential_radial(meshes, sp, pos, dims, RECIP, VOL, g2max)
+            ref_r = op.to_r(ref_g, dims)
+            vg, vr = pc.ionic_radial(meshes, sp, pos, g2max)
+            assert np.abs(vg - ref_g).max() < 1e-12 * np.abs(ref_g).max()
+            assert np.abs(vr - ref_r).max() < 1e-11 * np.abs(ref_r).max()
     finally:
         pc.close()
 

@@ -82,16 +82,38 @@ def test_pulay_oracle_matches_driver_and_the_scaled_solve_is_scale_free():
 
 
 def test_ionic_potential_oracle_matches_the_input_builder():
-    """The oracle's GTH ionic potential equals the host input builder's V_loc(r) for the synthetic
-    species (C3 = C4 = 0), with the builder's |G|^2 <= 4 ecut cut."""
+    """The oracle's radial-mesh ionic potential (local_vq_short_range, form_factor.zig:223-262, at every
+    |G|) equals the host input builder's V_loc(r), with the builder's |G|^2 < 4 ecut cut; and it stays
+    within 1e-6 of the analytic GTH form the mesh tabulates (the quadrature's only error)."""
+    from oracle import pseudo
+
     system = importlib.import_module("dftzig_b200.system")
-    c = system.crystal("si8")
+    c = system.crystal("sige8", 2)
     ecut = 10.0
     dims = system.fft_box(ecut, c.recip)
-    gth = [[sp.params["z"], sp.params["rloc"], sp.params["c1"], sp.params["c2"], 0.0, 0.0] for sp in c.species]
-    _, vr = op.ionic_potential(gth, c.atom_species, c.positions, dims, c.recip, c.volume, 4 * ecut)
+    meshes = [sp.mesh for sp in c.species]
+    vg, _ = pseudo.ionic_potential_radial(meshes, c.atom_species, c.positions, dims, c.recip, c.volume, 4 * ecut)
+    vr = op.to_r(vg, dims)
     ref = system.local_potential(c, dims, ecut)
     assert np.abs(vr - ref).max() < 1e-11 * np.abs(ref).max()
+    gth = [[sp.params["z"], sp.params["rloc"], sp.params["c1"], sp.params["c2"], 0.0, 0.0] for sp in c.species]
+    _, vr_gth = op.ionic_potential(gth, c.atom_species, c.positions, dims, c.recip, c.volume, 4 * ecut)
+    assert np.abs(vr_gth - ref).max() < 1e-6 * np.abs(ref).max()
+
+
+def test_short_range_form_factor_matches_reference_loop():
+    """The vectorised form factor equals the reference's sequential loop (form_factor.zig:223-262) and
+    the host builder's, and at q = 0 gives epsatm (compute_epsatm, form_factor.zig:264-268)."""
+    from oracle import pseudo
+
+    system = importlib.import_module("dftzig_b200.system")
+    sp = system.species("Si")
+    r, rab, vloc, z = sp.mesh
+    q = np.array([0.0, 1e-11, 0.2, 1.0, 4.5, 9.0])
+    loop = np.array([pseudo.local_vq_short_range(r, rab, vloc, z, float(x)) for x in q])
+    np.testing.assert_allclose(pseudo.local_vq_short_range_vec(r, rab, vloc, z, q), loop, rtol=1e-13)
+    np.testing.assert_allclose(system.local_form_factor(sp, q), loop, rtol=1e-13)
+    assert system.epsatm(sp) == system.local_form_factor(sp, np.zeros(1))[0]
 
 
 def test_pbe_derivatives_match_finite_differences():
