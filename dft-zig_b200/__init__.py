@@ -38,6 +38,7 @@ ABI_SYMBOLS = (
     "dftcuda_debug_set_wait_limits",
     "dftcuda_fermi_occupations",
     "dftcuda_ionic_potential_radial",
+    "dftcuda_nonlocal_stress",
     "dftcuda_local_forces_radial",
     "dftcuda_kctx_create",
     "dftcuda_kctx_destroy",
@@ -254,6 +255,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.dftcuda_complex_gemm.argtypes = [ip, sz, sz, sz, vp, lb, ip, ip, vp, lb, ip, ip, vp, lb, lb, ct.c_double, ct.c_double]
     lib.dftcuda_debug_set_wait_limits.argtypes = [lb, ip]
     lib.dftcuda_fermi_occupations.argtypes = [sz, sz, dp, dp, ct.c_double, ct.c_double, ct.c_double, dp, dp, dp]
+    lib.dftcuda_nonlocal_stress.argtypes = [vp, dp, sz, ct.POINTER(ct.c_void_p), dp, sz, sz, dp, dp]
     lib.dftcuda_ionic_potential_radial.argtypes = [vp, ip, vp, vp, vp, vp, vp, ip, vp, vp, ct.c_double, dp, dp]
     lib.dftcuda_local_forces_radial.argtypes = [vp, ip, vp, vp, vp, vp, vp, ip, vp, vp, ct.c_double, dp, dp]
     _lib = lib
@@ -445,6 +447,21 @@ class KpointContext:
         out = np.zeros((natoms, 3))
         _check(self._lib.dftcuda_nonlocal_forces(self._h, _ptr(vectors), self.n, w.size, w.ctypes.data, out.ctypes.data))
         return out
+
+    def nonlocal_stress(self, kpg, dphi, vectors, weights) -> np.ndarray:
+        """Nonlocal stress (3, 3) in Ry/bohr^3 of the bands (nbands, n) with weights f_n, a <= b filled
+        (dftcuda_nonlocal_stress).  kpg (n, 3) = k + G; dphi: per species (m_total, 3, n) derivative
+        projectors (system.projector_derivatives)."""
+        q = np.ascontiguousarray(kpg, dtype=np.float64).reshape(self.n, 3)
+        tabs = [np.ascontiguousarray(np.transpose(np.asarray(d, dtype=np.float64), (1, 0, 2))) for d in dphi]
+        arr = (ct.c_void_p * max(len(tabs), 1))(*[t.ctypes.data for t in tabs])
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        if isinstance(vectors, np.ndarray):
+            vectors = np.ascontiguousarray(vectors, dtype=np.complex128).reshape(-1, self.n)
+        out = np.zeros(9)
+        _check(self._lib.dftcuda_nonlocal_stress(self._h, q.ctypes.data, len(tabs), arr, _ptr(vectors), self.n, w.size, w.ctypes.data,
+                                                 out.ctypes.data))
+        return out.reshape(3, 3)
 
     def accumulate_band_density_noalloc(self, vectors_dev, weights_dev, rho_dev, nbands=None):
         """Same result as accumulate_band_density for device tensors, without any device allocation

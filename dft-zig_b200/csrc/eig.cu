@@ -19,11 +19,14 @@
 //    project the kept vectors out of V once more and take a second Cholesky pass (CholQR2).  This spans exactly the vectors MGS
 //    keeps, in the same order; only rounding differs.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <thread>
 #include <cstdio>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "kctx.cuh"
@@ -591,14 +594,8 @@ static int chol_drop(KCtxImpl* e, const double2* G, int k, double drop, int* kk_
     }
   }
   const size_t ci_smem = sizeof(double2) * kCiWarps * (size_t)k + sizeof(int) * (size_t)k;
-  static int ci_attr_dev = -1;
-  int dev = 0;
-  DFT_CUDA_TRY(cudaGetDevice(&dev));
-  if (ci_attr_dev != dev) {  // k <= 1024: at most 68 KB
-    DFT_CUDA_TRY(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(sizeof(double2) * kCiWarps * 1024 + sizeof(int) * 1024)));
-    ci_attr_dev = dev;
-  }
+  // k <= 1024: at most 68 KB
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_chol_inv, (int)(sizeof(double2) * kCiWarps * 1024 + sizeof(int) * 1024)));
   k_chol_inv<<<ceil_div(k, kCiWarps), kCiWarps * 32, ci_smem, s>>>(e->R, k, e->kept, kk_dev, e->Z);
   count_launch();
   DFT_CUDA_TRY(cudaGetLastError());
@@ -731,6 +728,8 @@ struct EigRun {
   double* vectors_out = nullptr;
   dftcuda_eig_info* info = nullptr;
   int status = DFTCUDA_OK;
+  size_t index = 0;     // position in the batch
+  std::string err_msg;  // the failure message, recorded on the host thread that issued the failing call
 };
 
 static int run_init(EigRun& r, const double* diag, const double* init_vecs, size_t init_cols) {
@@ -940,6 +939,47 @@ static double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// Host threads that issue the runs' kernels in each phase: many small runs (k-points, cells) spend
+// most of their time in the host's launch calls, and the runs are independent (each has its own
+// context, stream and workspace), so their issue spreads over threads.  DFTCUDA_ISSUE_THREADS
+// overrides the default (up to 8 threads, one per 8 runs; 1 = issue serially).
+static int issue_threads(size_t nruns) {
+  static const int env = [] {
+    const char* e = std::getenv("DFTCUDA_ISSUE_THREADS");
+    return e ? std::max(1, std::atoi(e)) : 0;
+  }();
+  if (env > 0) return (int)std::min<size_t>(env, std::max<size_t>(nruns, 1));
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  return (int)std::max<size_t>(1, std::min<size_t>({(size_t)8, (size_t)hw, nruns / 8}));
+}
+
+// fn(run) for every run, on up to issue_threads() host threads (dynamic assignment).
+template <typename F>
+static void for_each_run(std::vector<EigRun>& runs, F&& fn) {
+  const int nt = issue_threads(runs.size());
+  if (nt <= 1) {
+    for (EigRun& r : runs) fn(r);
+    return;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::atomic<size_t> next{0};
+  auto work = [&]() {
+    cudaSetDevice(dev);  // the runtime's current device is per host thread
+    for (size_t i; (i = next.fetch_add(1)) < runs.size();) {
+      EigRun& r = runs[i];
+      const int before = r.status;
+      fn(r);
+      if (before == DFTCUDA_OK && r.status != DFTCUDA_OK) r.err_msg = dftcuda_last_error_message();
+    }
+  };
+  std::vector<std::thread> th;
+  th.reserve(nt - 1);
+  for (int t = 1; t < nt; ++t) th.emplace_back(work);
+  work();
+  for (std::thread& t : th) t.join();
+}
+
 // Lockstep driver: every active run does RR; one synchronisation; every run decides (and launches
 // phase A of a chunk); one synchronisation; phase B for those with a chunk (repeated while chunks
 // remain); loop.
@@ -947,35 +987,32 @@ static int eig_solve_runs(std::vector<EigRun>& runs, const std::vector<const dou
                           const std::vector<const double*>& inits, const std::vector<size_t>& icols) {
   EigTimers tm;
   double t0 = now_s();
-  for (size_t i = 0; i < runs.size(); ++i) {
-    runs[i].status = run_init(runs[i], diags[i], inits[i], icols[i]);
-    if (runs[i].status != DFTCUDA_OK) runs[i].done = true;
-  }
+  for (size_t i = 0; i < runs.size(); ++i) runs[i].index = i;
+  for_each_run(runs, [&](EigRun& r) {
+    r.status = run_init(r, diags[r.index], inits[r.index], icols[r.index]);
+    if (r.status != DFTCUDA_OK) r.done = true;
+  });
   double t1 = now_s();
   tm.t[0] += t1 - t0;
   for (;;) {
-    bool any = false;
     t0 = now_s();
-    for (EigRun& r : runs) {
-      if (r.done || r.status != DFTCUDA_OK) continue;
-      if (r.it >= r.opts.max_iter) {
-        r.done = true;
-        continue;
-      }
-      r.status = run_rr(r);
-      any = true;
-    }
+    for (EigRun& r : runs)
+      if (!r.done && r.status == DFTCUDA_OK && r.it >= r.opts.max_iter) r.done = true;
+    bool any = false;
+    for (EigRun& r : runs) any |= (!r.done && r.status == DFTCUDA_OK);
+    if (!any) break;
+    for_each_run(runs, [](EigRun& r) {
+      if (!r.done && r.status == DFTCUDA_OK) r.status = run_rr(r);
+    });
     t1 = now_s();
     tm.t[1] += t1 - t0;
-    if (!any) break;
     sync_runs(runs, false);
     ++tm.syncs;
     t0 = now_s();
     tm.t[2] += t0 - t1;
-    for (EigRun& r : runs) {
-      if (r.done || r.status != DFTCUDA_OK) continue;
-      r.status = run_decide(r);
-    }
+    for_each_run(runs, [](EigRun& r) {
+      if (!r.done && r.status == DFTCUDA_OK) r.status = run_decide(r);
+    });
     t1 = now_s();
     tm.t[3] += t1 - t0;
     for (;;) {
@@ -987,10 +1024,9 @@ static int eig_solve_runs(std::vector<EigRun>& runs, const std::vector<const dou
       ++tm.syncs;
       t1 = now_s();
       tm.t[4] += t1 - t0;
-      for (EigRun& r : runs) {
-        if (r.done || r.status != DFTCUDA_OK || !r.orth_pending) continue;
-        r.status = run_orth_b(r);
-      }
+      for_each_run(runs, [](EigRun& r) {
+        if (!r.done && r.status == DFTCUDA_OK && r.orth_pending) r.status = run_orth_b(r);
+      });
       tm.t[5] += now_s() - t1;
     }
   }
@@ -1000,10 +1036,18 @@ static int eig_solve_runs(std::vector<EigRun>& runs, const std::vector<const dou
                  "%.1f (%ld syncs)\n",
                  1e3 * tm.t[0], 1e3 * tm.t[1], 1e3 * tm.t[2], 1e3 * tm.t[3], 1e3 * tm.t[4], 1e3 * tm.t[5], tm.syncs);
   int first = DFTCUDA_OK;
+  std::string first_msg;
   for (EigRun& r : runs) {
-    if (r.status == DFTCUDA_OK) r.status = run_finish(r);
-    if (first == DFTCUDA_OK && r.status != DFTCUDA_OK) first = r.status;
+    if (r.status == DFTCUDA_OK) {
+      r.status = run_finish(r);
+      if (r.status != DFTCUDA_OK) r.err_msg = dftcuda_last_error_message();
+    }
+    if (first == DFTCUDA_OK && r.status != DFTCUDA_OK) {
+      first = r.status;
+      first_msg = r.err_msg;
+    }
   }
+  if (first != DFTCUDA_OK && !first_msg.empty()) set_last_error(first, first_msg);  // on the caller's thread
   return first;
 }
 

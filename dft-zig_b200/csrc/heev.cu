@@ -18,6 +18,8 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 #include <string>
 
 #include "kctx.cuh"
@@ -864,8 +866,6 @@ int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde,
                 cudaStream_t s) {
   if (m < 1 || m > 2048 || nev < 1 || nev > m || m > (int)w.m_cap || nev > (int)w.nev_cap)
     return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "heev: size outside the workspace");
-  static int attr_dev = -1;
-  static int n_sm = 0, per_sm = 0;
   int dev = 0;
   DFT_CUDA_TRY(cudaGetDevice(&dev));
   // DFTCUDA_HETRD=2barrier selects the two-barrier tridiagonalisation (A/B measurements)
@@ -876,14 +876,24 @@ int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde,
   const void* hetrd_fn = two_barrier ? (const void*)k_hetrd : (const void*)k_hetrd1;
   const int hetrd_bufs = two_barrier ? 2 : 3;  // shared-memory vectors of m entries
   const size_t smem_tr = sizeof(double2) * hetrd_bufs * 2048;
-  if (attr_dev != dev) {
-    DFT_CUDA_TRY(cudaFuncSetAttribute(hetrd_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tr));
-    DFT_CUDA_TRY(cudaFuncSetAttribute(k_hetrd_back, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(sizeof(double2) * BT_WARPS * 2048)));
-    DFT_CUDA_TRY(cudaFuncSetAttribute(k_wy_t_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWyTSmem));
-    DFT_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-    DFT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_fn, HT_THREADS, smem_tr));
-    attr_dev = dev;
+  DFT_TRY(ensure_max_dynamic_smem(hetrd_fn, (int)smem_tr));
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_hetrd_back, (int)(sizeof(double2) * BT_WARPS * 2048)));
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_wy_t_all, (int)kWyTSmem));
+  // SM count and the reduction kernel's occupancy, per device (several host threads may ask at once)
+  static std::mutex occ_mu;
+  static std::map<int, std::pair<int, int>> occ;
+  int n_sm = 0, per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lock(occ_mu);
+    auto it = occ.find(dev);
+    if (it == occ.end()) {
+      DFT_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+      DFT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_fn, HT_THREADS, smem_tr));
+      occ[dev] = {n_sm, per_sm};
+    } else {
+      n_sm = it->second.first;
+      per_sm = it->second.second;
+    }
   }
   if (per_sm < 1) return fail(DFTCUDA_ERR_UNSUPPORTED, "heev: tridiagonalisation kernel does not fit an SM");
   DFT_CUDA_TRY(cudaMemsetAsync(w.bar, 0, 2 * sizeof(unsigned), s));

@@ -257,9 +257,11 @@ static bool use_sticks(const dftcuda_kctx* c) {
 
 // Workspace bytes per column of the local passes (apply = H|psi>, else the density passes, which
 // keep the plane layout).
+static bool use_sticks_density(const dftcuda_kctx* c) { return use_sticks(c) && kctx_sticks_density_ok(c, c->precision); }
+
 static size_t box_col_bytes(const dftcuda_kctx* c, bool apply) {
   const size_t cs = c->precision != DFTCUDA_PRECISION_FP64 ? sizeof(float2) : sizeof(double2);
-  if (apply && use_sticks(c)) return sticks_bytes_per_col(c, cs);
+  if (apply ? use_sticks(c) : use_sticks_density(c)) return sticks_bytes_per_col(c, cs);
   return cs * (size_t)c->n_act * c->P;
 }
 
@@ -449,9 +451,15 @@ int kctx_density_dev(dftcuda_kctx* c, const double2* vecs, size_t nbands, const 
   if (nbands == 0) return DFTCUDA_OK;
   const size_t ch = chunk_cols(c, nbands, false);
   DFT_TRY(ensure_box(c, ch, false));
+  const bool sticks = use_sticks_density(c);
   for (size_t c0 = 0; c0 < nbands; c0 += ch) {
     const size_t nc = std::min(ch, nbands - c0);
-    if (c->precision != DFTCUDA_PRECISION_FP64) {
+    if (sticks) {
+      if (c->precision != DFTCUDA_PRECISION_FP64)
+        DFT_TRY(density_block_sticks<float>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
+      else
+        DFT_TRY(density_block_sticks<double>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
+    } else if (c->precision != DFTCUDA_PRECISION_FP64) {
       if (c->fast32 && !c->fft_generic)
         DFT_TRY(density_block4<float>(c, vecs + c0 * c->npw, nc, w_dev + c0, rho_dev, s));
       else
@@ -655,6 +663,9 @@ extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const d
   c->natoms = 0;
   c->atom_row.clear();
   c->atom_mt.clear();
+  c->atom_species.clear();
+  c->atom_pos.clear();
+  c->species_mt.clear();
   if (n_species == 0 || n_atoms == 0) return DFTCUDA_OK;
   if (!species || !atom_species || !atom_pos) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_projectors: null array");
   // Projector order follows apply.zig:1454-1482: species in order, then that species' atoms in order.
@@ -689,6 +700,10 @@ extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const d
   c->natoms = (int)n_atoms;
   c->atom_row.assign(n_atoms, 0);
   c->atom_mt.assign(n_atoms, 0);
+  c->atom_species.assign(atom_species, atom_species + n_atoms);
+  c->atom_pos.assign(atom_pos, atom_pos + 3 * n_atoms);
+  c->species_mt.resize(n_species);
+  for (size_t s = 0; s < n_species; ++s) c->species_mt[s] = species[s].m_total;
   int p = 0;
   for (size_t s = 0; s < n_species; ++s) {
     const dftcuda_species& sp = species[s];
@@ -912,6 +927,163 @@ extern "C" int dftcuda_nonlocal_forces(dftcuda_kctx* c, const double* vectors, s
     return DFTCUDA_OK;
   };
   st = run();
+  cleanup();
+  return st;
+}
+
+// ---- nonlocal stress (stress/nonlocal_stress.zig:108-558, norm-conserving) -----------------------
+// y = (k+G)_b x per column.
+__global__ void k_scale_q(const double2* __restrict__ x, const double* __restrict__ kpg, int b, long npw, long ncols,
+                          double2* __restrict__ y) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= npw * ncols) return;
+  const double q = kpg[3 * (i % npw) + b];
+  const double2 v = x[i];
+  y[i] = make_double2(q * v.x, q * v.y);
+}
+
+// *out_u += scale sum_{p, n} w_n Re(conj(dp_pn) u_pn)   (accumulate_nonlocal_sigma_for_band), when u
+// *out_t += sum_{p, n} w_n Re(conj(t_pn) dp_pn)          (compute_enl_for_band, times Omega), when t
+// dp, u, t: [nproj][ncols] complex.  One block-sum per block, then an atomic add.
+__global__ void k_stress_reduce(const double2* __restrict__ dp, const double2* __restrict__ u, const double2* __restrict__ t,
+                                const double* __restrict__ w, long nproj, long ncols, double scale, double* __restrict__ out_u,
+                                double* __restrict__ out_t) {
+  __shared__ double red[2][8];
+  double s0 = 0.0, s1 = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nproj * ncols; i += (long)gridDim.x * blockDim.x) {
+    const double wn = w[i % ncols];
+    if (wn <= 0.0) continue;
+    const double2 d = dp[i];
+    if (u) {
+      const double2 v = u[i];
+      s0 += wn * (d.x * v.x + d.y * v.y);
+    }
+    if (t) {
+      const double2 v = t[i];
+      s1 += wn * (v.x * d.x + v.y * d.y);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+  }
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][wp] = s0;
+    red[1][wp] = s1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+      a += red[0][i];
+      b += red[1][i];
+    }
+    if (u) atomicAdd(out_u, scale * a);
+    if (t) atomicAdd(out_t, b);
+  }
+}
+
+extern "C" int dftcuda_nonlocal_stress(dftcuda_kctx* c, const double* kpg, size_t n_species, const double* const* dphi,
+                                       const double* vectors, size_t n, size_t nbands, const double* weights, double* sigma) {
+  if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_stress: null context");
+  if (n != c->npw) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "nonlocal_stress: n != n_pw");
+  if (!sigma || !kpg || (nbands && (!vectors || !weights))) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_stress: null buffer");
+  double hs[9] = {0.0};
+  const int nproj = c->nl.nproj;
+  if (nproj == 0 || nbands == 0) {
+    std::memcpy(sigma, hs, sizeof(hs));
+    return DFTCUDA_OK;
+  }
+  if (n_species != c->species_mt.size() || !dphi) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_stress: one derivative table per species");
+  for (size_t sp = 0; sp < n_species; ++sp)
+    if (!dphi[sp]) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_stress: null derivative table");
+  cudaStream_t s = c->stream;
+  auto packed = [](int a, int b) { return a * 3 + b - (a * (a + 1)) / 2; };  // (a <= b) -> 0..5
+  const size_t nch = std::min<size_t>(nbands, 256);
+  DFT_TRY(kctx_stage(c, nch));
+  DFT_TRY(kctx_ensure_coef(c, nch));
+  // derivative projectors of all atoms, per direction a: DP_a[(atom, m)][G] = dphi_m,a(G) e^{i G . tau}
+  double2* DP = nullptr;
+  double* d_tab = nullptr;
+  double* d_kpg = nullptr;
+  double* d_w = nullptr;
+  double* d_acc = nullptr;  // sigma_ab for a <= b (packed, 6), then sum_n f_n Omega E_nl,n
+  double2* d_u = nullptr;
+  auto cleanup = [&] {
+    for (void* p : {(void*)DP, (void*)d_tab, (void*)d_kpg, (void*)d_w, (void*)d_acc, (void*)d_u})
+      if (p) cudaFree(p);
+  };
+  size_t max_mt = 0;
+  for (size_t mt : c->species_mt) max_mt = std::max(max_mt, mt);
+  if (cudaMalloc(&DP, sizeof(double2) * 3 * (size_t)nproj * n) != cudaSuccess ||
+      cudaMalloc(&d_tab, sizeof(double) * 3 * max_mt * n) != cudaSuccess || cudaMalloc(&d_kpg, sizeof(double) * 3 * n) != cudaSuccess ||
+      cudaMalloc(&d_w, sizeof(double) * nbands) != cudaSuccess || cudaMalloc(&d_acc, sizeof(double) * 7) != cudaSuccess ||
+      cudaMalloc(&d_u, sizeof(double2) * (size_t)nproj * nch) != cudaSuccess) {
+    cleanup();
+    return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "nonlocal_stress: buffers");
+  }
+  auto run = [&]() -> int {
+    DFT_CUDA_TRY(cudaMemcpyAsync(d_kpg, kpg, sizeof(double) * 3 * n, cudaMemcpyDefault, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(d_w, weights, sizeof(double) * nbands, cudaMemcpyDefault, s));
+    DFT_CUDA_TRY(cudaMemsetAsync(d_acc, 0, sizeof(double) * 7, s));
+    for (size_t sp = 0; sp < n_species; ++sp) {
+      const size_t mt = c->species_mt[sp];
+      DFT_CUDA_TRY(cudaMemcpyAsync(d_tab, dphi[sp], sizeof(double) * 3 * mt * n, cudaMemcpyDefault, s));
+      for (int a = 0; a < c->natoms; ++a) {
+        if (c->atom_species[a] != (int)sp) continue;
+        const double* tau = c->atom_pos.data() + 3 * a;
+        for (int d = 0; d < 3; ++d) {
+          k_build_projectors<<<ceil_div(n, 256), 256, 0, s>>>(DP + ((size_t)d * nproj + c->atom_row[a]) * n, d_tab + (size_t)d * mt * n,
+                                                             (int)mt, (long)n, c->d_gcart, tau[0], tau[1], tau[2]);
+          count_launch();
+        }
+      }
+    }
+    const bool dv = is_device_pointer(vectors);
+    for (size_t c0 = 0; c0 < nbands; c0 += nch) {
+      const size_t nc = std::min(nch, nbands - c0);
+      const double2* x = (const double2*)vectors + c0 * n;
+      if (!dv) {
+        DFT_CUDA_TRY(cudaMemcpyAsync(c->d_x, x, sizeof(double2) * n * nc, cudaMemcpyHostToDevice, s));
+        x = c->d_x;
+      }
+      DFT_TRY(kctx_project(c, x, nc, s));  // p
+      const long tot = (long)nproj * nc;
+      k_apply_dij<<<ceil_div(tot, 256), 256, 0, s>>>(c->d_coef, c->d_coef2, c->nl.D, c->nl.proj_off, c->nl.proj_mt, c->nl.maxm,
+                                                   nproj, (int)nc); count_launch();  // Dp
+      const unsigned rb = std::min<unsigned>(ceil_div(tot, 256), 1024);
+      k_stress_reduce<<<rb, 256, 0, s>>>(c->d_coef2, nullptr, c->d_coef, d_w + c0, nproj, (long)nc, 0.0, nullptr, d_acc + 6);
+      count_launch();
+      for (int b = 0; b < 3; ++b) {
+        k_scale_q<<<ceil_div((long)n * nc, 256), 256, 0, s>>>(x, d_kpg, b, (long)n, (long)nc, c->d_y); count_launch();
+        for (int a = 0; a <= b; ++a) {
+          GemmArgs g{};
+          g.M = nproj; g.N = (int)nc; g.K = (int)n;
+          g.A = DP + (size_t)a * nproj * n; g.lda = (long)n; g.a_kc = true; g.conj_a = false;
+          g.B = c->d_y; g.ldb = (long)n; g.b_kc = true; g.conj_b = false;
+          g.O = d_u; g.ldo_r = (long)nc; g.ldo_c = 1;
+          g.alpha = 1.0; g.beta = 0.0;
+          DFT_TRY(zgemm(g, s, c->d_gemm_ws, c->gemm_ws_elems));
+          k_stress_reduce<<<rb, 256, 0, s>>>(c->d_coef2, d_u, nullptr, d_w + c0, nproj, (long)nc,
+                                             -2.0 / (c->volume * c->volume), d_acc + packed(a, b), nullptr);
+          count_launch();
+        }
+      }
+    }
+    double acc[7];
+    DFT_CUDA_TRY(cudaMemcpyAsync(acc, d_acc, sizeof(acc), cudaMemcpyDeviceToHost, s));
+    DFT_CUDA_TRY(cudaStreamSynchronize(s));
+    // sigma_ab (a <= b, as the reference fills it) and the diagonal -sum_n f_n E_nl,n / Omega
+    const double enl = acc[6] / c->volume;
+    for (int a = 0; a < 3; ++a)
+      for (int b = a; b < 3; ++b) hs[3 * a + b] = acc[packed(a, b)];
+    for (int a = 0; a < 3; ++a) hs[4 * a] -= enl / c->volume;
+    if (is_device_pointer(sigma)) DFT_CUDA_TRY(cudaMemcpy(sigma, hs, sizeof(hs), cudaMemcpyHostToDevice));
+    else std::memcpy(sigma, hs, sizeof(hs));
+    return DFTCUDA_OK;
+  };
+  const int st = run();
   cleanup();
   return st;
 }

@@ -121,6 +121,9 @@ struct dftcuda_kctx {
   dftcuda::NonlocalDev nl;
   int natoms = 0;                   // atoms given to set_projectors
   std::vector<int> atom_row, atom_mt;  // per atom (set_projectors order): first projector row, row count
+  std::vector<int> atom_species;       // per atom: species index
+  std::vector<double> atom_pos;        // per atom: Cartesian position (bohr), 3 doubles
+  std::vector<size_t> species_mt;      // per species: m_total
   double2* d_coef = nullptr;   // [nproj][cols] projector coefficients
   double2* d_coef2 = nullptr;
   size_t coef_cols = 0;
@@ -193,6 +196,9 @@ bool kctx_sticks_ok(const dftcuda_kctx* c, int precision);
 int kctx_setup_sticks(dftcuda_kctx* c, const std::vector<int>& slot_of_x, const std::vector<int>& xpos, const int32_t* hkl);
 size_t sticks_bytes_per_col(const dftcuda_kctx* c, size_t cs);
 template <typename T> int local_block_sticks(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols, cudaStream_t s);
+bool kctx_sticks_density_ok(const dftcuda_kctx* c, int precision);
+template <typename T>
+int density_block_sticks(dftcuda_kctx* c, const double2* x, size_t ncols, const double* w, double* rho, cudaStream_t s);
 template <typename T>
 int density_block4(dftcuda_kctx* c, const double2* x, size_t ncols, const double* w, double* rho, cudaStream_t s);
 

@@ -454,13 +454,7 @@ static int mlp_upload(MlpData& d, size_t nbands, size_t npw, const int* off, con
 }
 
 static int mlp_loss_grad_dev(MlpData& d, cudaStream_t s) {
-  static int attr_dev = -1;
-  int dev = 0;
-  DFT_CUDA_TRY(cudaGetDevice(&dev));
-  if (attr_dev != dev) {
-    DFT_CUDA_TRY(cudaFuncSetAttribute(k_mlp_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBackwardSmem));
-    attr_dev = dev;
-  }
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_mlp_backward, (int)kBackwardSmem));
   k_mlp_band_sums<<<d.nb, 256, 0, s>>>(d.off, d.feat, d.cc, d.w, d.params, d.sums); count_launch();
   k_mlp_loss<<<1, 256, 0, s>>>(d.sums, d.dn, d.nb, d.loss); count_launch();
   DFT_CUDA_TRY(cudaMemsetAsync(d.grad, 0, sizeof(float) * MLP_NPARAM, s));
@@ -571,12 +565,7 @@ int precondition_launch(dftcuda_kctx* c, double2* Q, const double2* res, const d
       int dev = 0, nsm = 148;
       DFT_CUDA_TRY(cudaGetDevice(&dev));
       DFT_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-      static int attr_dev = -1;
-      if (attr_dev != dev) {
-        DFT_CUDA_TRY(cudaFuncSetAttribute(k_precondition_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)sizeof(MlpInferSmem)));
-        attr_dev = dev;
-      }
+      DFT_TRY(ensure_max_dynamic_smem((const void*)k_precondition_mlp, (int)sizeof(MlpInferSmem)));
       const size_t tiles = ((size_t)take * n + MLP_TE - 1) / MLP_TE;
       const unsigned g = (unsigned)std::min<size_t>(tiles, (size_t)nsm * 8);
       k_precondition_mlp<<<g, MLP_IT, sizeof(MlpInferSmem), s>>>(Q, res, kin, ekin_ws, norms, band, take, n, t, c->d_mlp);

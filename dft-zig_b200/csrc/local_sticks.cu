@@ -341,6 +341,116 @@ __global__ void __launch_bounds__(plane_max_warps<T>() * 32, 1) k_zplane(cplx<T>
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Band density on the stick layout, pass 2: per z-plane, the inverse y and x transforms of each of
+// the CTA's columns and rho(x, y, z) += w_c |psi_c|^2 / Omega accumulated in a shared-memory plane,
+// added to the global density once at the end (several CTAs share a plane: atomics).
+// ------------------------------------------------------------------------------------------
+template <typename T, int N>
+__global__ void __launch_bounds__(256, 1) k_zplane_density(const cplx<T>* __restrict__ S, int n_st, const int* __restrict__ st_sy,
+                                                           int n_act, const int* __restrict__ slot_of_x, int n1z, int n2z, int ncols,
+                                                           int cols_per_cta, const cplx<T>* __restrict__ tw,
+                                                           const double* __restrict__ wgt, double inv_vol, double* __restrict__ rho) {
+  using C = cplx<T>;
+  using G = PlaneXGeom<N>;
+  constexpr int N1 = G::N1, N2 = G::N2, LW = G::LW, QR = G::Q, SX = G::S;
+  constexpr int QS = N + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double* R = reinterpret_cast<double*>(smraw);               // [N][N] density plane, x fastest
+  C* Q = reinterpret_cast<C*>(R + (size_t)N * N);              // [n_act][QS]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  C* Bw = Q + (size_t)n_act * QS + (size_t)warp * LW * SX;
+  const int z = blockIdx.x;
+  const int r = (z % n1z) * n2z + z / n1z;
+  const int c0 = blockIdx.y * cols_per_cta;
+  const int c1 = min(ncols, c0 + cols_per_cta);
+  const int nq = n_act * QS;
+  const int L = lane / N2, t = lane - L * N2;
+  const bool lane_ok = L < LW;
+  C* B = Bw + (lane_ok ? L : 0) * SX;
+  for (int i = threadIdx.x; i < N * N; i += blockDim.x) R[i] = 0.0;
+  for (int c = c0; c < c1; ++c) {
+    const C* Srow = S + ((long)c * gridDim.x + r) * n_st;
+    const double wc = __ldg(wgt + c) * inv_vol;
+    __syncthreads();
+    for (int i = threadIdx.x; i < nq; i += blockDim.x) Q[i] = mk<C>(0.0, 0.0);
+    __syncthreads();
+    for (int g = threadIdx.x; g < n_st; g += blockDim.x) {
+      const int sy = __ldg(st_sy + g);
+      Q[(sy >> 16) * QS + (sy & 0xffff)] = Srow[g];
+    }
+    __syncthreads();
+    for (int w = threadIdx.x; w < N2 * n_act; w += blockDim.x) {
+      const int sl = w % n_act, tt = w / n_act;
+      C* q = Q + sl * QS;
+      C v[N1];
+#pragma unroll
+      for (int j = 0; j < N1; ++j) v[j] = q[j * N2 + tt];
+      RegDft<T, N1>::run(v, (T)1);
+#pragma unroll
+      for (int k1 = 1; k1 < N1; ++k1)
+        if (tt) v[k1] = cmul(v[k1], twl<T>(tw, (tt * k1) % N, (T)1));
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) q[k1 * N2 + tt] = v[k1];
+    }
+    __syncthreads();
+    for (int w = threadIdx.x; w < N1 * n_act; w += blockDim.x) {
+      const int sl = w % n_act, k1 = w / n_act;
+      C* q = Q + sl * QS + k1 * N2;
+      C u[N2];
+#pragma unroll
+      for (int j = 0; j < N2; ++j) u[j] = q[j];
+      RegDft<T, N2>::run(u, (T)1);
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) q[k2] = u[k2];
+    }
+    __syncthreads();
+    for (int lt = warp; lt * LW < N; lt += nwarp) {
+      const int yl = lt * LW + L;
+      const bool lv = lane_ok && yl < N;
+      const int col = lv ? (yl % N1) * N2 + yl / N1 : 0;
+      {
+        C v[N1];
+#pragma unroll
+        for (int m = 0; m < N1; ++m) {
+          const int sm = lv ? __ldg(slot_of_x + t + N2 * m) : -1;
+          v[m] = sm >= 0 ? Q[sm * QS + col] : mk<C>(0.0, 0.0);
+        }
+        RegDft<T, N1>::run(v, (T)1);
+#pragma unroll
+        for (int k1 = 1; k1 < N1; ++k1)
+          if (t) v[k1] = cmul(v[k1], twl<T>(tw, (t * k1) % N, (T)1));
+        if (lane_ok) {
+#pragma unroll
+          for (int k1 = 0; k1 < N1; ++k1) B[k1 * N2 + t] = v[k1];
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < QR; ++q) {  // inverse step B: x = k1 + N1 k2, then the density
+        const int k1 = t + N2 * q;
+        if (lv && k1 < N1) {
+          C u[N2];
+#pragma unroll
+          for (int j = 0; j < N2; ++j) u[j] = B[k1 * N2 + j];
+          RegDft<T, N2>::run(u, (T)1);
+          double* Ry = R + (size_t)yl * N;
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2)
+            Ry[k1 + N1 * k2] += wc * ((double)u[k2].x * (double)u[k2].x + (double)u[k2].y * (double)u[k2].y);
+        }
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  double* rz = rho + (long)z * N * N;
+  for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
+    const double v = R[i];
+    if (v != 0.0) atomicAdd(rz + i, v);
+  }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------------------------
@@ -439,6 +549,62 @@ static int launch_zplane(dftcuda_kctx* c, cplx<T>* S, size_t ncols, cudaStream_t
   return DFTCUDA_OK;
 }
 
+static constexpr int kDensityWarps = 8;
+
+template <int N> static size_t density_plane_smem(size_t cs, int n_act) {
+  using G = PlaneXGeom<N>;
+  return sizeof(double) * (size_t)N * N + cs * ((size_t)n_act * (N + 1) + (size_t)kDensityWarps * G::LW * G::S);
+}
+
+template <typename T, int N>
+static int launch_zplane_density(dftcuda_kctx* c, const cplx<T>* S, size_t ncols, const double* w, double* rho, cudaStream_t s) {
+  const size_t smem = density_plane_smem<N>(sizeof(cplx<T>), c->n_act);
+  if (smem > (size_t)kSmemSticks) return fail(DFTCUDA_ERR_UNSUPPORTED, "z-plane density pass does not fit shared memory");
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_zplane_density<T, N>, (int)smem));
+  const cplx<T>* tw = std::is_same<T, double>::value ? (const cplx<T>*)c->d_twx64 : (const cplx<T>*)c->d_twx32;
+  // columns per CTA: every CTA sums its columns in shared memory before one atomic pass over its plane
+  const int cpc = std::max(1, (int)((ncols * c->nz + 295) / 296));
+  dim3 g((unsigned)c->nz, ceil_div(ncols, cpc));
+  int n1z = 0, n2z = 0;
+  switch (c->nz) {
+#define X(L)            \
+  case L:               \
+    n1z = Split<L>::N1; \
+    n2z = Split<L>::N2; \
+    break;
+    DFTCUDA_FOUR_STEP_LENGTHS(X)
+#undef X
+    default: return fail(DFTCUDA_ERR_UNSUPPORTED, "z length without a four-step split");
+  }
+  k_zplane_density<T, N><<<g, kDensityWarps * 32, smem, s>>>(S, c->n_st, c->d_st_sy, c->n_act, c->d_st_sox, n1z, n2z, (int)ncols, cpc, tw,
+                                                              w, 1.0 / c->volume, rho);
+  count_launch();
+  return DFTCUDA_OK;
+}
+
+template <typename T>
+static int dispatch_zplane_density(dftcuda_kctx* c, const cplx<T>* S, size_t ncols, const double* w, double* rho, cudaStream_t s) {
+  switch (c->nx) {
+#define X(N) \
+  case N: return launch_zplane_density<T, N>(c, S, ncols, w, rho, s);
+    DFTCUDA_FOUR_STEP_LENGTHS(X)
+#undef X
+    default: return fail(DFTCUDA_ERR_UNSUPPORTED, "x length without a four-step kernel");
+  }
+}
+
+bool kctx_sticks_density_ok(const dftcuda_kctx* c, int precision) {
+  if (!(precision == DFTCUDA_PRECISION_FP64 ? c->sticks64 : c->sticks32)) return false;
+  const size_t cs = precision == DFTCUDA_PRECISION_FP64 ? sizeof(double2) : sizeof(float2);
+  switch (c->nx) {
+#define X(N) \
+  case N: return density_plane_smem<N>(cs, c->n_act) <= (size_t)kSmemSticks;
+    DFTCUDA_FOUR_STEP_LENGTHS(X)
+#undef X
+    default: return false;
+  }
+}
+
 template <typename T>
 static int dispatch_stick_inv(dftcuda_kctx* c, const double2* x, cplx<T>* S, size_t ncols, cudaStream_t s) {
   switch (c->nz) {
@@ -490,6 +656,19 @@ int local_block_sticks(dftcuda_kctx* c, const double2* x, double2* y, size_t nco
 }
 template int local_block_sticks<double>(dftcuda_kctx*, const double2*, double2*, size_t, cudaStream_t);
 template int local_block_sticks<float>(dftcuda_kctx*, const double2*, double2*, size_t, cudaStream_t);
+
+template <typename T>
+int density_block_sticks(dftcuda_kctx* c, const double2* x, size_t ncols, const double* w, double* rho, cudaStream_t s) {
+  cplx<T>* S = reinterpret_cast<cplx<T>*>(c->d_box);
+  ProfScope ps(c, P_DENSITY, s);
+  DFT_TRY(dispatch_stick_inv<T>(c, x, S, ncols, s));
+  DFT_TRY(dispatch_zplane_density<T>(c, S, ncols, w, rho, s));
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}
+
+template int density_block_sticks<double>(dftcuda_kctx*, const double2*, size_t, const double*, double*, cudaStream_t);
+template int density_block_sticks<float>(dftcuda_kctx*, const double2*, size_t, const double*, double*, cudaStream_t);
 
 // Stick tables: sticks in slot order (y ascending within a slot), the packed (slot, y) of each, the
 // plane-wave index of every (stick, z) (or -1), and the z and x/y twiddle tables.

@@ -1051,13 +1051,7 @@ size_t cgemm_tf32_workspace_elems(int M, int N, int K) {
 
 template <bool AKC, bool BKC, bool CJA, bool CJB, bool SPLIT>
 static void tc_launch(const GemmArgs& g, dim3 grid, int kps, double2* part, int* err, cudaStream_t s) {
-  static int attr_dev = -1;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (attr_dev != dev) {
-    cudaFuncSetAttribute(k_cgemm_tf32<AKC, BKC, CJA, CJB, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(SPLIT));
-    attr_dev = dev;
-  }
+  ensure_max_dynamic_smem((const void*)k_cgemm_tf32<AKC, BKC, CJA, CJB, SPLIT>, tc_smem(SPLIT));
   k_cgemm_tf32<AKC, BKC, CJA, CJB, SPLIT><<<grid, TC_THREADS, tc_smem(SPLIT), s>>>(
       g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r, g.ldo_c, g.alpha, g.beta, kps, part, err);
   count_launch();
@@ -1065,13 +1059,7 @@ static void tc_launch(const GemmArgs& g, dim3 grid, int kps, double2* part, int*
 
 template <bool AKC, bool BKC, bool CJA, bool CJB, bool SPLIT>
 static void tc2_launch(const GemmArgs& g, dim3 grid, int kps, double2* part, int* err, cudaStream_t s) {
-  static int attr_dev = -1;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (attr_dev != dev) {
-    cudaFuncSetAttribute(k_cgemm_tc2<AKC, BKC, CJA, CJB, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, t2_smem(SPLIT));
-    attr_dev = dev;
-  }
+  ensure_max_dynamic_smem((const void*)k_cgemm_tc2<AKC, BKC, CJA, CJB, SPLIT>, t2_smem(SPLIT));
   k_cgemm_tc2<AKC, BKC, CJA, CJB, SPLIT><<<grid, T2_THREADS, t2_smem(SPLIT), s>>>(
       g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r, g.ldo_c, g.alpha, g.beta, kps, part, err);
   count_launch();
@@ -1079,13 +1067,7 @@ static void tc2_launch(const GemmArgs& g, dim3 grid, int kps, double2* part, int
 
 template <bool AKC, bool BKC, bool CJA, bool CJB, bool SPLIT>
 static void tc3_launch(const GemmArgs& g, dim3 grid, int kps, double2* part, int* err, cudaStream_t s) {
-  static int attr_dev = -1;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (attr_dev != dev) {
-    cudaFuncSetAttribute(k_cgemm_tc3<AKC, BKC, CJA, CJB, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, t3_smem(SPLIT));
-    attr_dev = dev;
-  }
+  ensure_max_dynamic_smem((const void*)k_cgemm_tc3<AKC, BKC, CJA, CJB, SPLIT>, t3_smem(SPLIT));
   k_cgemm_tc3<AKC, BKC, CJA, CJB, SPLIT><<<grid, T3_THREADS, t3_smem(SPLIT), s>>>(
       g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r, g.ldo_c, g.alpha, g.beta, kps, part, err, t3_chunk());
   count_launch();

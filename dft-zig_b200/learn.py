@@ -3,10 +3,12 @@
 Learned preconditioner (``precond``): a per-plane-wave MLP that refines the Teter-Payne-Allan
 diagonal of the Davidson correction step (m = K_TPA(x) exp(z_theta); the reference's own form is
 r / (|k+G|^2 - lambda), lobpcg/common.zig:214-226).  Training pairs come from TPA-preconditioned
-runs of the device solver on seeded strained and displaced Si8 cells (``si8d``): the solver is
-deterministic (LCG start, serial.zig:75-95), so the run stopped after t iterations reproduces the
-Ritz vectors psi_b^t of the full run; the target is the correction from psi_b^t to its converged
-eigenspace.  The network is trained on the GPU by
+runs of the device solver on 200 seeded Si cells of 8 to 64 atoms (``sitrain``: supercells of the
+cubic cell with strain and displacements; the strained Si8 set ``si8d`` of the first weights stays
+selectable): the solver is deterministic (LCG start, serial.zig:75-95), so the run stopped after t
+iterations reproduces the Ritz vectors psi_b^t of the full run; the target is the correction from
+psi_b^t to its converged eigenspace.  The trained network is judged against TPA on the Si216 cell:
+Davidson iterations, H applications and wall time to the same residual (evaluate_si216).  The network is trained on the GPU by
 the library's own CUDA forward/backward kernels (dftcuda_precond_mlp_train, Adam).
 
 Learned first density (``fno``): a Fourier neural operator (csrc/fno.cu) maps the superposition of
@@ -49,26 +51,34 @@ def _features(kin, ekin, rabs, rms, t):
     return np.stack([np.log(x + 0.05), np.log(rabs / max(rms, 1e-300) + 1e-6), np.full_like(x, min(t / 20.0, 2.0))], axis=1)
 
 
-def precond_samples(dz, cells, ecut: float, nbands: int, t_max: int = 20, kfrac=(0.0, 0.0, 0.0), cluster_tol: float = 1e-4,
-                    min_overlap: float = 0.5):
+def precond_samples(dz, cells, ecut: float, nbands, t_max: int = 20, kfrac=(0.0, 0.0, 0.0), cluster_tol: float = 1e-4,
+                    min_overlap: float = 0.5, t_list=None, bands_per_t=None, seed: int = 0):
     """Residual -> correction samples along Davidson trajectories preconditioned by TPA (the form
     the network refines).  Target of band b at iteration t: delta_b = y - psi_b <psi_b|y>, y the
     normalised projection of psi_b^t on the converged eigenspace of its group of (near-)degenerate
-    bands (gaps < cluster_tol Ry), kept when that projection has norm >= min_overlap."""
+    bands (gaps < cluster_tol Ry), kept when that projection has norm >= min_overlap.
+    nbands: a number, or a function of the cell (e.g. its occupied bands); t_list: the iterations
+    sampled (default 1..t_max); bands_per_t: keep at most this many bands per (cell, t), drawn with
+    a seeded generator (bounds the data of large cells)."""
     off = [0]
     feats, ccs, ws, dns, kins, lams = [], [], [], [], [], []
+    rng = np.random.default_rng(seed)
     for c in cells:
+        nb = int(nbands(c)) if callable(nbands) else int(nbands)
         inp = sysm.kpoint_inputs(c, ecut, kfrac)
         kc = _context(dz, inp)
         kc.set_preconditioner(dz.PRECOND_TPA)
         kin = inp.basis.kinetic
-        conv = kc.hermitian_eigen_decomp_iterative(kin, nbands + 4, dz.Options(max_iter=400, tol=1e-10))
-        for t in range(1, t_max + 1):
-            r = kc.hermitian_eigen_decomp_iterative(kin, nbands, dz.Options(max_iter=t, tol=1e-14))
+        conv = kc.hermitian_eigen_decomp_iterative(kin, nb + 4, dz.Options(max_iter=400, tol=1e-10))
+        for t in (t_list if t_list is not None else range(1, t_max + 1)):
+            r = kc.hermitian_eigen_decomp_iterative(kin, nb, dz.Options(max_iter=t, tol=1e-14))
             psi = r.vectors
             hpsi = kc.apply_hamiltonian_batched(psi)
             res = hpsi - r.values[:, None] * psi
-            for b in range(nbands):
+            bands = range(nb)
+            if bands_per_t is not None and nb > bands_per_t:
+                bands = sorted(rng.choice(nb, size=bands_per_t, replace=False).tolist())
+            for b in bands:
                 rn = float(np.linalg.norm(res[b]))
                 if rn < 1e-7:
                     continue
@@ -156,10 +166,11 @@ def evaluate_precond(dz, cells, ecut: float, nbands: int, params, tol: float = 1
     out = {"reference": [], "tpa": [], "mlp": []}
     for c in cells:
         inp = sysm.kpoint_inputs(c, ecut, kfrac)
+        nb = int(nbands(c)) if callable(nbands) else int(nbands)
         for kind, key in ((dz.PRECOND_REFERENCE, "reference"), (dz.PRECOND_TPA, "tpa"), (dz.PRECOND_MLP, "mlp")):
             kc = _context(dz, inp)
             kc.set_preconditioner(kind, params if kind == dz.PRECOND_MLP else None)
-            r = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, nbands, dz.Options(max_iter=300, tol=tol))
+            r = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, nb, dz.Options(max_iter=300, tol=tol))
             out[key].append({"iterations": r.iterations, "h_applies": r.h_applies, "converged": r.converged})
             kc.close()
     summ = {}
@@ -170,6 +181,29 @@ def evaluate_precond(dz, cells, ecut: float, nbands: int, params, tol: float = 1
             "all_converged": all(r["converged"] for r in rs),
         }
     return summ
+
+
+def evaluate_si216(dz, params, tol: float = 1e-6, max_iter: int = 400) -> dict:
+    """north_star's judge of the learned preconditioner: one Davidson solve of the Si216 cell (3x3x3
+    conventional, seed 3, 25 Ry, Gamma, 448 bands, the reference's defaults otherwise) from the
+    random start to the same residual tol, per preconditioner: iterations, H applications and the
+    solve's wall time (FP64 contexts, device-resident)."""
+    import torch
+
+    c = sysm.crystal("si216", 3)
+    inp = sysm.kpoint_inputs(c, 25.0, (0.0, 0.0, 0.0))
+    out = {}
+    for kind, key in ((dz.PRECOND_REFERENCE, "reference"), (dz.PRECOND_TPA, "tpa"), (dz.PRECOND_MLP, "mlp")):
+        kc = _context(dz, inp)
+        kc.set_preconditioner(kind, params if kind == dz.PRECOND_MLP else None)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, 448, dz.Options(max_iter=max_iter, tol=tol))
+        torch.cuda.synchronize()
+        out[key] = {"iterations": r.iterations, "h_applies": r.h_applies, "wall_s": round(time.perf_counter() - t0, 3),
+                    "converged": bool(r.converged), "max_residual": float(r.max_residual), "lowest_eigenvalue": float(r.values[0])}
+        kc.close()
+    return out
 
 
 def load_precond_weights(path: str = PRECOND_WEIGHTS) -> np.ndarray:
@@ -276,9 +310,11 @@ def main(argv=None):
     import importlib
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=("precond", "fno"))
-    ap.add_argument("--train-cells", type=int, default=48)
-    ap.add_argument("--eval-cells", type=int, default=8)
+    ap.add_argument("what", choices=("precond", "fno", "precond-eval"))
+    ap.add_argument("--cells", choices=("sitrain", "si8d"), default="sitrain",
+                    help="sitrain: 200 seeded Si cells of 8-64 atoms (seeds 1000..), si8d: strained Si8 cells")
+    ap.add_argument("--train-cells", type=int, default=200)
+    ap.add_argument("--eval-cells", type=int, default=16)
     ap.add_argument("--ecut", type=float, default=12.0)
     ap.add_argument("--nbands", type=int, default=16)
     ap.add_argument("--steps", type=int, default=1500)
@@ -293,15 +329,33 @@ def main(argv=None):
     dz = importlib.import_module(__package__)
     if a.what == "fno":
         return main_fno(dz, a)
+    if a.what == "precond-eval":
+        print(json.dumps({"si216": evaluate_si216(dz, load_precond_weights(a.out))}), flush=True)
+        return
     t0 = time.perf_counter()
-    train_cells = [sysm.crystal("si8d", 1000 + i) for i in range(a.train_cells)]
-    eval_cells = [sysm.crystal("si8d", 1200 + i) for i in range(a.eval_cells)]
-    tr = precond_samples(dz, train_cells, a.ecut, a.nbands)
-    ev = precond_samples(dz, eval_cells, a.ecut, a.nbands)
+    if a.cells == "sitrain":
+        # the occupied bands of each cell; a few Davidson iterations of each trajectory and at most
+        # 12 bands of each iteration keep the 200 cells' data under ~1 GB
+        train_cells = [sysm.crystal("sitrain", 1000 + i) for i in range(a.train_cells)]
+        eval_cells = [sysm.crystal("sitrain", 1200 + i) for i in range(a.eval_cells)]
+        nb = lambda c: int(round(c.nelec / 2.0))
+        kw = dict(t_list=(1, 2, 4, 7, 11, 16), bands_per_t=12)
+        tr = precond_samples(dz, train_cells, a.ecut, nb, seed=1, **kw)
+        ev = precond_samples(dz, eval_cells, a.ecut, nb, seed=2, **kw)
+        dav_cells, dav_nb = eval_cells[: min(6, len(eval_cells))], nb
+    else:
+        train_cells = [sysm.crystal("si8d", 1000 + i) for i in range(a.train_cells)]
+        eval_cells = [sysm.crystal("si8d", 1200 + i) for i in range(a.eval_cells)]
+        tr = precond_samples(dz, train_cells, a.ecut, a.nbands)
+        ev = precond_samples(dz, eval_cells, a.ecut, a.nbands)
+        dav_cells, dav_nb = eval_cells, a.nbands
     t1 = time.perf_counter()
     p, hist = train_precond(dz, tr, a.steps, a.lr)
     t2 = time.perf_counter()
     report = {
+        "cells": a.cells,
+        "train_cells": len(train_cells),
+        "train_atoms": sorted({len(c.atom_species) for c in train_cells}),
         "train_bands": int(len(tr["off"]) - 1),
         "train_plane_waves": int(tr["feat"].shape[0]),
         "data_seconds": round(t1 - t0, 2),
@@ -312,8 +366,10 @@ def main(argv=None):
         "heldout_loss_initial_weights_tpa": eval_loss(dz, init_params(0), ev),
         "heldout_loss_reference_diagonal": fixed_loss(ev, "reference"),
         "heldout_loss_tpa": fixed_loss(ev, "tpa"),
-        "heldout_davidson": evaluate_precond(dz, eval_cells, a.ecut, a.nbands, p),
+        "heldout_davidson": evaluate_precond(dz, dav_cells, a.ecut, dav_nb, p),
     }
+    if a.cells == "sitrain":
+        report["si216"] = evaluate_si216(dz, p)
     os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
     np.savez(a.out, params=p, loss_history=hist.astype(np.float32), report=json.dumps(report))
     print(json.dumps(report), flush=True)

@@ -129,6 +129,19 @@ int dftcuda_nonlocal_energies(dftcuda_kctx* ctx, const double* psi, size_t n, si
 int dftcuda_nonlocal_forces(dftcuda_kctx* ctx, const double* vectors, size_t n, size_t nbands, const double* weights,
                             double* forces);
 
+/* Nonlocal (Kleinman-Bylander) stress of nbands bands at this k-point (stress/nonlocal_stress.zig:108-558,
+ * norm-conserving): sigma_ab = -(2/Omega^2) sum_n f_n sum_(atom,m) Re[conj(Dp_mn) sum_G dphi_m/dq_a(G)
+ * e^{iG.tau} q_b c_n(G)] - delta_ab sum_n f_n E_nl,n / Omega, with p = <beta|psi> of the context's
+ * projectors, Dp the D_ij contraction, E_nl,n = Re sum conj(p) Dp / Omega, q = k + G.  Like the reference,
+ * only the components a <= b are filled (the rest of sigma[9], row-major, is 0).  kpg[n*3]: k + G of the
+ * basis; dphi[s] (one per species given to dftcuda_set_projectors): [3][m_total][n] derivative
+ * projectors d phi_bm / d q_a = 4 pi (R_b'(|q|) q_a/|q| Y_lm + R_b dY_lm/dq_a) (project_p_and_dp,
+ * nonlocal_stress.zig:108-165); vectors (nbands, n) complex128; weights f_n (occupation x k weight x
+ * spin; bands with f_n <= 0 skipped); sigma in Ry/bohr^3.  Host or device pointers (dphi entries too).
+ * The six strain projections run through the library's FP64 complex GEMM.  Sum over k-points. */
+int dftcuda_nonlocal_stress(dftcuda_kctx* ctx, const double* kpg, size_t n_species, const double* const* dphi,
+                            const double* vectors, size_t n, size_t nbands, const double* weights, double* sigma);
+
 /* Autotuner: times candidate launch configurations of this context's H|psi> on ncols trial
  * columns (FFT pass variant, column-chunk workspace budget, split-K of the two projector GEMMs)
  * with CUDA events and keeps the fastest for all later calls.  report may be NULL. */

@@ -106,3 +106,37 @@ def test_scf_forces_match_energy_finite_difference(dz):
     assert abs(r0.forces[1, 0] - fd) < 2e-4 + 1e-3 * abs(fd), (r0.forces[1, 0], fd)
     assert abs(r0.forces[1, 0]) > 1e-3  # the displacement produces a real force
     assert np.abs(r0.forces.sum(axis=0)).max() < 1e-3  # no net force beyond grid effects
+
+
+@pytest.mark.parametrize("name,k", [("si8", (0.13, -0.07, 0.21)), ("sige8", (0.0, 0.25, 0.0))])
+def test_nonlocal_stress_matches_oracle(dz, name, k):
+    """dftcuda_nonlocal_stress (derivative-projector GEMMs on the device) against the oracle's
+    restatement of stress/nonlocal_stress.zig (oracle/stress.py, itself checked as the strain
+    derivative of the nonlocal energy): the components a <= b, 1e-10 of the largest."""
+    from oracle import stress as ost
+
+    _, system = _mods()
+    c = system.crystal(name, 1)
+    ecut = 12.0
+    tables = [[system.radial_table(sp, i, ecut) for i in range(len(sp.betas))] for sp in c.species]
+    inp = system.kpoint_inputs(c, ecut, k, tables=tables)
+    kc = dz.KpointContext(*inp.dims, inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart)
+    kc.set_vloc(inp.local_r)
+    kc.set_projectors([dz.SpeciesProjectors(l, d, p) for (l, d, p) in inp.species_phi], inp.atom_species, inp.positions)
+    rng = np.random.default_rng(5)
+    nb = 6
+    vecs = rng.normal(size=(nb, kc.n)) + 1j * rng.normal(size=(nb, kc.n))
+    vecs /= np.linalg.norm(vecs, axis=1, keepdims=True)
+    w = np.array([0.5, 0.5, 0.25, 0.0, 0.125, -0.1])
+    kpg = inp.basis.kpg
+    dphi = [system.projector_derivatives(sp, kpg, tables[s]) for s, sp in enumerate(c.species)]
+    got = kc.nonlocal_stress(kpg, dphi, vecs, w)
+    species = []
+    for s, sp in enumerate(c.species):
+        t = tables[s]
+        species.append(([l for l, _ in sp.betas], sp.dij, lambda b, q, t=t: system._interp(t[b], q),
+                        lambda b, q, t=t: system._interp_deriv(t[b], q)))
+    ref = ost.nonlocal_stress(kpg, inp.basis.gcart, species, inp.atom_species, inp.positions, vecs, w, inp.volume)
+    kc.close()
+    assert np.all(np.tril(got, -1) == 0.0)
+    assert np.abs(got - ref).max() < 1e-10 * np.abs(ref).max()
