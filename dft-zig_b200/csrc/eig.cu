@@ -461,6 +461,7 @@ struct KCtxImpl {
   HeevWork hw;
   bool rr_tc = false;  // Rayleigh-Ritz products on the tensor cores (3xTF32), TF32/TF32X3 contexts
   int* err = nullptr;  // the context's tensor-core error flag
+  TcScratch* tcs = nullptr;  // the context's pre-split operand buffer
   // pinned host mirrors of the per-iteration read-backs
   void* pinned = nullptr;
   double *h_ev = nullptr, *h_nr = nullptr;
@@ -542,7 +543,7 @@ static int eig_alloc(dftcuda_kctx* c, size_t n, size_t max_sub, size_t nb) {
 // form (FP32-class accuracy); the Cholesky factorisations, the subspace eigensolver and the residual
 // norms stay FP64.  FP64 and FP32 contexts use the FP64 GEMM throughout.
 static int gemm_dispatch(KCtxImpl* e, const GemmArgs& g, bool /*rr*/, cudaStream_t s) {
-  if (e->rr_tc) return cgemm_tf32(g, s, e->ws, e->ws_elems, e->err, true);
+  if (e->rr_tc) return cgemm_tf32(g, s, e->ws, e->ws_elems, e->err, true, e->tcs);
   return zgemm(g, s, e->ws, e->ws_elems);
 }
 
@@ -757,6 +758,7 @@ static int run_init(EigRun& r, const double* diag, const double* init_vecs, size
     DFT_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
   }
   e->err = c->d_err;
+  e->tcs = &c->tc_scratch;
   const char* gram_mode = std::getenv("DFTCUDA_GRAM");
   r.gram_full = gram_mode && std::strcmp(gram_mode, "full") == 0;
   DFT_CUDA_TRY(cudaMemcpyAsync(e->diag, diag, sizeof(double) * n,

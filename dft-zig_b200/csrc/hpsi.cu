@@ -357,8 +357,9 @@ int kctx_project(dftcuda_kctx* c, const double2* x, size_t ncols, cudaStream_t s
   g.O = c->d_coef; g.ldo_r = (long)ncols; g.ldo_c = 1;
   g.alpha = 1.0; g.beta = 0.0;
   g.splits = c->split_proj;
+  g.a_cache = &c->tc_ptiles_proj;
   if (precision_uses_tc(c->precision))
-    return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err, c->precision == DFTCUDA_PRECISION_TF32X3);
+    return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err, c->precision == DFTCUDA_PRECISION_TF32X3, &c->tc_scratch);
   return zgemm(g, s, c->d_gemm_ws, c->gemm_ws_elems);
 }
 
@@ -382,8 +383,9 @@ static int nonlocal_block(dftcuda_kctx* c, const double2* x, double2* y, size_t 
   g.O = y; g.ldo_r = (long)c->npw; g.ldo_c = 1;
   g.alpha = 1.0 / c->volume; g.beta = 1.0;
   g.splits = c->split_back;
+  g.b_cache = &c->tc_ptiles_back;
   if (precision_uses_tc(c->precision))
-    return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err, c->precision == DFTCUDA_PRECISION_TF32X3);
+    return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err, c->precision == DFTCUDA_PRECISION_TF32X3, &c->tc_scratch);
   return zgemm(g, s, c->d_gemm_ws, c->gemm_ws_elems);
 }
 
@@ -529,6 +531,9 @@ extern "C" int dftcuda_kctx_destroy(dftcuda_kctx* c) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   c->fx.destroy(); c->fy.destroy(); c->fz.destroy();
+  c->tc_scratch.release();
+  c->tc_ptiles_proj.release();
+  c->tc_ptiles_back.release();
   if (c->ev_order) cudaEventDestroy(c->ev_order);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -660,6 +665,8 @@ extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const d
   if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_projectors: null context");
   cudaStreamSynchronize(c->stream);
   free_nonlocal(c);
+  c->tc_ptiles_proj.release();  // the split copies of the old projector matrix
+  c->tc_ptiles_back.release();
   c->natoms = 0;
   c->atom_row.clear();
   c->atom_mt.clear();

@@ -7,6 +7,18 @@
 
 namespace dftcuda {
 
+// Device buffer of the tensor-core GEMM's pre-split operands (grown on demand, owned by a context).
+// As the cache of a constant operand (the projector matrix) it also records what it holds: valid
+// and the key of the layout it was split for.
+struct TcScratch {
+  void* p = nullptr;
+  size_t bytes = 0;
+  bool valid = false;
+  unsigned long long key = 0;
+  int ensure(size_t need);
+  void release();
+};
+
 // Complex GEMM over strided operands (zgemm.cu):
 //   out(r, c) = alpha * sum_k opA(A(r, k)) * opB(B(c, k)) + beta * out(r, c)
 //   A(r, k) = a_kc ? A[r*lda + k] : A[k*lda + r]      B(c, k) = b_kc ? B[c*ldb + k] : B[k*ldb + c]
@@ -18,13 +30,18 @@ struct GemmArgs {
   double2* O; long ldo_r; long ldo_c;
   double alpha, beta;
   int splits = 0;  // split-K count; 0 = the kernel's wave-filling heuristic
+  // Constant operands whose TF32 split the tensor-core GEMM may keep between calls (null: split per call).
+  TcScratch* a_cache = nullptr;
+  TcScratch* b_cache = nullptr;
 };
 int zgemm(const GemmArgs& g, cudaStream_t s, double2* workspace, size_t workspace_elems);
 size_t zgemm_workspace_elems(int M, int N, int K);
 // The same contraction on the tensor cores (tc_gemm.cu): TF32 inputs, FP32 accumulation.  err_dev
 // receives 1 if a bounded wait gave up.
-// split = true: 3xTF32 (hi + lo operand parts), FP32-class accuracy.
-int cgemm_tf32(const GemmArgs& g, cudaStream_t s, double2* workspace, size_t workspace_elems, int* err_dev, bool split);
+// split = true: 3xTF32 (hi + lo operand parts), FP32-class accuracy.  scratch (may be null): where the
+// products with both output dimensions >= 128 keep their operands split into TF32 tiles.
+int cgemm_tf32(const GemmArgs& g, cudaStream_t s, double2* workspace, size_t workspace_elems, int* err_dev, bool split,
+               TcScratch* scratch = nullptr);
 inline bool precision_uses_tc(int p) { return p == DFTCUDA_PRECISION_TF32 || p == DFTCUDA_PRECISION_TF32X3; }
 size_t cgemm_tf32_workspace_elems(int M, int N, int K);
 
@@ -119,6 +136,8 @@ struct dftcuda_kctx {
   size_t box_bytes = 0;
 
   dftcuda::NonlocalDev nl;
+  dftcuda::TcScratch tc_scratch;  // pre-split tensor-core GEMM operands (TF32 and TF32X3 contexts)
+  dftcuda::TcScratch tc_ptiles_proj, tc_ptiles_back;  // the projector matrix split for the two projector GEMMs
   int natoms = 0;                   // atoms given to set_projectors
   std::vector<int> atom_row, atom_mt;  // per atom (set_projectors order): first projector row, row count
   std::vector<int> atom_species;       // per atom: species index

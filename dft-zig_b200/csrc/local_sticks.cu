@@ -341,6 +341,10 @@ __global__ void __launch_bounds__(plane_max_warps<T>() * 32, 1) k_zplane(cplx<T>
   }
 }
 
+// Doubles reserved for the density kernel's N x N plane: rounded up to an even count, so the complex
+// plane after it starts on a 16-byte boundary (N^2 is odd for odd N).
+template <int N> __host__ __device__ constexpr int density_plane_words() { return (N * N + 1) & ~1; }
+
 // ------------------------------------------------------------------------------------------
 // Band density on the stick layout, pass 2: per z-plane, the inverse y and x transforms of each of
 // the CTA's columns and rho(x, y, z) += w_c |psi_c|^2 / Omega accumulated in a shared-memory plane,
@@ -357,7 +361,7 @@ __global__ void __launch_bounds__(256, 1) k_zplane_density(const cplx<T>* __rest
   constexpr int QS = N + 1;
   extern __shared__ __align__(16) unsigned char smraw[];
   double* R = reinterpret_cast<double*>(smraw);               // [N][N] density plane, x fastest
-  C* Q = reinterpret_cast<C*>(R + (size_t)N * N);              // [n_act][QS]
+  C* Q = reinterpret_cast<C*>(R + density_plane_words<N>());  // [n_act][QS], 16-byte aligned
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   C* Bw = Q + (size_t)n_act * QS + (size_t)warp * LW * SX;
   const int z = blockIdx.x;
@@ -480,11 +484,10 @@ static int plane_warps_rt(size_t cs, int n, int n_act) {
   }
 }
 
-// DFTCUDA_LOCAL=planes keeps a new context on the plane-layout passes (A/B measurements and tests);
-// read at context creation.
+// The stick-layout passes are opt-in: DFTCUDA_LOCAL=sticks, read at context creation.
 static bool sticks_disabled() {
   const char* e = std::getenv("DFTCUDA_LOCAL");
-  return e && std::string(e) == "planes";
+  return !(e && std::string(e) == "sticks");
 }
 
 bool kctx_sticks_ok(const dftcuda_kctx* c, int precision) {
@@ -553,7 +556,7 @@ static constexpr int kDensityWarps = 8;
 
 template <int N> static size_t density_plane_smem(size_t cs, int n_act) {
   using G = PlaneXGeom<N>;
-  return sizeof(double) * (size_t)N * N + cs * ((size_t)n_act * (N + 1) + (size_t)kDensityWarps * G::LW * G::S);
+  return sizeof(double) * (size_t)density_plane_words<N>() + cs * ((size_t)n_act * (N + 1) + (size_t)kDensityWarps * G::LW * G::S);
 }
 
 template <typename T, int N>

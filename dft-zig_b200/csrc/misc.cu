@@ -1,9 +1,9 @@
 // Status strings, per-thread last-error message, pointer classification.
 #include <atomic>
 #include <mutex>
-#include <set>
+#include <map>
 #include <string>
-#include <tuple>
+#include <utility>
 
 #include "kctx.cuh"
 
@@ -66,17 +66,19 @@ bool is_device_pointer(const void* p) {
 }
 
 int ensure_max_dynamic_smem(const void* kernel, int bytes) {
+  // the limit only ever rises: a later, smaller request must not undercut a launch that needs more
   static std::mutex mu;
-  static std::set<std::tuple<int, const void*, int>> done;
+  static std::map<std::pair<int, const void*>, int> set_to;
   int dev = 0;
   DFT_CUDA_TRY(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lock(mu);
-  const auto key = std::make_tuple(dev, kernel, bytes);
-  if (done.count(key)) return DFTCUDA_OK;
+  const auto key = std::make_pair(dev, kernel);
+  auto it = set_to.find(key);
+  if (it != set_to.end() && it->second >= bytes) return DFTCUDA_OK;
   const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess)
     return fail(DFTCUDA_ERR_CUDA, std::string("cudaFuncSetAttribute(MaxDynamicSharedMemorySize): ") + cudaGetErrorString(e));
-  done.insert(key);
+  set_to[key] = bytes;
   return DFTCUDA_OK;
 }
 
@@ -194,8 +196,11 @@ extern "C" int dftcuda_complex_gemm(int precision, size_t M, size_t N, size_t K,
   cudaStream_t s = nullptr;
   double2* ws = nullptr;
   int* err = nullptr;
+  TcScratch tiles;  // the pre-split operands of the wide tensor-core kernel
   int rc = DFTCUDA_OK;
   auto cleanup = [&] {
+    if (s) cudaStreamSynchronize(s);
+    tiles.release();
     if (s) cudaStreamDestroy(s);
     if (ws) cudaFree(ws);
     if (err) cudaFree(err);
@@ -206,7 +211,7 @@ extern "C" int dftcuda_complex_gemm(int precision, size_t M, size_t N, size_t K,
     cleanup();
     return fail(DFTCUDA_ERR_CUDA, "complex_gemm: stream or workspace allocation failed");
   }
-  rc = tc ? cgemm_tf32(g, s, ws, ws_elems, err, precision == DFTCUDA_PRECISION_TF32X3) : zgemm(g, s, ws, ws_elems);
+  rc = tc ? cgemm_tf32(g, s, ws, ws_elems, err, precision == DFTCUDA_PRECISION_TF32X3, &tiles) : zgemm(g, s, ws, ws_elems);
   int herr = 0;
   if (rc == DFTCUDA_OK) {
     const cudaError_t e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);

@@ -910,6 +910,225 @@ __global__ void __launch_bounds__(T3_THREADS, 1) k_cgemm_tc3(int M, int N, int K
   if (warp == T3_CONV_WARPS) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(T3_TMEM_COLS));
 }
 
+// ---- k_cgemm_tc4: the 128 x 256 kernel on pre-split operands -----------------------------------
+// The converter warps of k_cgemm_tc3 bound it (a TF32 product runs nearly as slowly as the 3xTF32
+// one).  Here every operand is split once, by k_tf32_tiles, into the MMA's own shared-memory image:
+// for each 8-deep K step and each plane (real hi, imaginary hi, then for 3xTF32 real lo, imaginary
+// lo) the operand's 8-row groups, 256 bytes each (two 8 x 4 core matrices, the layout of t3_off), one
+// after another.  A slot plane of a 128-row (256-row) tile is then one contiguous 4 KB (8 KB) block
+// of global memory, fetched by one bulk copy (cp.async.bulk) that completes on the slot's mbarrier.
+// Rows are padded to a multiple of 256 and K to a multiple of 8 with zeros, so no copy needs a bound.
+// Warp 8 lane 0 issues the copies, warp 9 lane 0 the MMAs, warps 0-7 drain the accumulators (the
+// same chunked FP64 drains as k_cgemm_tc3).  Every wait is bounded; on a timeout each role winds down
+// and the producer waits (bounded) for the copies it issued before the CTA exits.
+constexpr int T4_THREADS = 32 * (T3_CONV_WARPS + 2);
+constexpr int T4_PRODUCER = T3_CONV_WARPS, T4_MMA = T3_CONV_WARPS + 1;
+__host__ __device__ constexpr int t4_planes(bool split) { return split ? 4 : 2; }
+__host__ __device__ constexpr int t4_slot(bool split) { return t4_planes(split) * (T3_APL + T3_BPL); }
+__host__ __device__ constexpr int t4_stages(bool split) { return split ? 4 : 8; }
+__host__ __device__ constexpr int t4_smem(bool split) { return t4_stages(split) * t4_slot(split) + 256; }
+
+// Split of one operand into TF32 tiles: out[((ks * planes + p) * RG + rg) * 64 + w] (32-bit words),
+// rg = row / 8, the word of (row, k) within its 256-byte group at t3_off(row % 8, k % 8) / 4.
+// X(r, k) = X[r * ld + k] when kc, else X[k * ld + r]; conj conjugates.  hi = tf32(x) and
+// lo = tf32(x - hi), the difference taken in FP64.  One thread per (row, 4-k group).
+template <bool SPLIT>
+__global__ void k_tf32_tiles(const double2* __restrict__ X, long ld, bool kc, bool conj, int R, int K, int RG, int KS,
+                             float* __restrict__ out) {
+  constexpr int NP = t4_planes(SPLIT);
+  const long u = blockIdx.x * (long)blockDim.x + threadIdx.x;  // unit = ((ks * 2 + kg) * RG + rg) * 8 + r8
+  const long nunits = (long)KS * 2 * RG * 8;
+  if (u >= nunits) return;
+  const int r8 = (int)(u & 7);
+  const long v = u >> 3;
+  const int rg = (int)(v % RG);
+  const long w = v / RG;
+  const int kg = (int)(w & 1), ks = (int)(w >> 1);
+  const int row = rg * 8 + r8, k0 = ks * 8 + kg * 4;
+  float hr[4], hi[4], lr[4], li[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    double2 x = make_double2(0.0, 0.0);
+    if (row < R && k0 + j < K) x = kc ? X[(long)row * ld + k0 + j] : X[(long)(k0 + j) * ld + row];
+    const double xr = x.x, xi = conj ? -x.y : x.y;
+    hr[j] = tf32_rna((float)xr);
+    hi[j] = tf32_rna((float)xi);
+    lr[j] = SPLIT ? tf32_rna((float)(xr - (double)hr[j])) : 0.f;
+    li[j] = SPLIT ? tf32_rna((float)(xi - (double)hi[j])) : 0.f;
+  }
+  const long base = (((long)ks * NP) * RG + rg) * 64 + (kg * 128 + r8 * 16) / 4;  // words
+  const long pstride = (long)RG * 64;
+  *reinterpret_cast<float4*>(out + base) = make_float4(hr[0], hr[1], hr[2], hr[3]);
+  *reinterpret_cast<float4*>(out + base + pstride) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+  if (SPLIT) {
+    *reinterpret_cast<float4*>(out + base + 2 * pstride) = make_float4(lr[0], lr[1], lr[2], lr[3]);
+    *reinterpret_cast<float4*>(out + base + 3 * pstride) = make_float4(li[0], li[1], li[2], li[3]);
+  }
+}
+
+__device__ __forceinline__ void t4_bulk(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst), "l"(src),
+               "r"(bytes), "r"(mbar)
+               : "memory");
+}
+__device__ __forceinline__ void t4_expect(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(T4_THREADS, 1) k_cgemm_tc4(int M, int N, const float* __restrict__ At, int RGA,
+                                                             const float* __restrict__ Bt, int RGB, int KS,
+                                                             double2* __restrict__ O, long ldo_r, long ldo_c, double alpha,
+                                                             double beta, int kps, double2* __restrict__ part,
+                                                             int* __restrict__ err, int chunk) {
+  extern __shared__ __align__(1024) unsigned char tsm4[];
+  constexpr int NS = t4_stages(SPLIT);
+  constexpr int SL = t4_slot(SPLIT);
+  constexpr int NP = t4_planes(SPLIT);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm4 + NS * SL);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2 * NS + 3);
+  __shared__ volatile int s_abort;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int r0 = blockIdx.y * TC_M, c0 = blockIdx.x * T3_N;
+  const int kbeg = blockIdx.z * kps;  // in K steps of 8
+  const int kend = min(KS, kbeg + kps);
+  const int ntiles = max(0, kend - kbeg);
+  const int nchunks = (ntiles + chunk - 1) / chunk;
+  const uint32_t ring = (uint32_t)__cvta_generic_to_shared(tsm4);
+  const uint32_t mb = (uint32_t)__cvta_generic_to_shared(mbar);
+  const uint32_t mb_chunk = mb + 16 * NS, mb_drained = mb_chunk + 8, mb_fin = mb_chunk + 16;
+  if (tid == 0) {
+    s_abort = 0;
+    for (int q = 0; q < NS; ++q) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb + 8 * q));         // full: the producer's expect_tx
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb + 8 * (NS + q)));  // empty: the MMA commit
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb_chunk));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mb_drained), "r"(T3_CONV_WARPS));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb_fin));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+  }
+  if (warp == T4_MMA) {
+    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(tmem_slot);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(slot), "r"(T3_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t d_re = tmem, d_im = tmem + T3_N;
+  if (warp < T3_CONV_WARPS) {
+    // ---- drains ----
+    for (int ch = 0; ch < nchunks; ++ch) {
+      int ok = 1;
+      if (lane == 0) ok = tc_wait(mb_chunk, (uint32_t)(ch & 1)) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        if (lane == 0) atomicExch(err, 1);
+        s_abort = 1;
+      }
+      if (__shfl_sync(0xffffffffu, s_abort, 0)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      t3_drain(d_re, d_im, warp, lane, true, ch == 0, M, N, r0, c0, O, ldo_r, ldo_c, alpha, beta, part, blockIdx.z);
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+      __syncwarp();
+      if (lane == 0) t3_arrive(mb_drained);
+    }
+  } else if (warp == T4_PRODUCER) {
+    // ---- bulk copies ----
+    if (lane == 0) {
+      const long a_plane = (long)RGA * 64, b_plane = (long)RGB * 64;  // words per plane of a K step
+      const float* a0 = At + (long)(r0 / 8) * 64;
+      const float* b0 = Bt + (long)(c0 / 8) * 64;
+      int issued = 0;
+      for (int t = 0; t < ntiles; ++t) {
+        const int q = t % NS;
+        if (t >= NS && !tc_wait(mb + 8 * (NS + q), (uint32_t)((t / NS - 1) & 1))) {
+          atomicExch(err, 1);
+          s_abort = 1;
+        }
+        if (s_abort) break;
+        const uint32_t full = mb + 8 * q;
+        t4_expect(full, (uint32_t)SL);
+        const uint32_t dst = ring + q * SL;
+        const long ks = kbeg + t;
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          t4_bulk(dst + p * T3_APL, a0 + (ks * NP + p) * a_plane, T3_APL, full);
+          t4_bulk(dst + NP * T3_APL + p * T3_BPL, b0 + (ks * NP + p) * b_plane, T3_BPL, full);
+        }
+        ++issued;
+      }
+      // no copy may be in flight when the CTA exits: wait for the last full phase of every slot used
+      for (int t = max(0, issued - NS); t < issued; ++t) {
+        if (!tc_wait(mb + 8 * (t % NS), (uint32_t)((t / NS) & 1))) atomicExch(err, 1);
+      }
+    }
+  } else if (lane == 0) {
+    // ---- MMA issuer ----
+    const uint32_t id_pos = t3_idesc(false), id_neg = t3_idesc(true);
+    int issued = 0;
+    for (int t = 0; t < ntiles; ++t) {
+      const int q = t % NS;
+      const int tc = t % chunk;
+      if (tc == 0 && t > 0) {
+        if (!tc_wait(mb_drained, (uint32_t)((t / chunk - 1) & 1))) {
+          atomicExch(err, 1);
+          s_abort = 1;
+        }
+      }
+      if (!s_abort && !tc_wait(mb + 8 * q, (uint32_t)((t / NS) & 1))) {
+        atomicExch(err, 1);
+        s_abort = 1;
+      }
+      if (s_abort) break;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      // slot image: A planes (hi re, hi im[, lo re, lo im]) then the B planes in the same order
+      const uint32_t sa = ring + q * SL, sb = sa + NP * T3_APL;
+      const uint32_t sar = sa, sai = sa + T3_APL, sbr = sb, sbi = sb + T3_BPL;
+      const bool acc = tc > 0;
+      if (SPLIT) {
+        const uint32_t arl = sa + 2 * T3_APL, ail = sa + 3 * T3_APL, brl = sb + 2 * T3_BPL, bil = sb + 3 * T3_BPL;
+        tc_mma(d_re, t3_desc(sar), t3_desc(brl), id_pos, acc);
+        tc_mma(d_re, t3_desc(arl), t3_desc(sbr), id_pos, true);
+        tc_mma(d_re, t3_desc(sai), t3_desc(bil), id_neg, true);
+        tc_mma(d_re, t3_desc(ail), t3_desc(sbi), id_neg, true);
+        tc_mma(d_re, t3_desc(sar), t3_desc(sbr), id_pos, true);
+        tc_mma(d_re, t3_desc(sai), t3_desc(sbi), id_neg, true);
+        tc_mma(d_im, t3_desc(sar), t3_desc(bil), id_pos, acc);
+        tc_mma(d_im, t3_desc(arl), t3_desc(sbi), id_pos, true);
+        tc_mma(d_im, t3_desc(sai), t3_desc(brl), id_pos, true);
+        tc_mma(d_im, t3_desc(ail), t3_desc(sbr), id_pos, true);
+        tc_mma(d_im, t3_desc(sar), t3_desc(sbi), id_pos, true);
+        tc_mma(d_im, t3_desc(sai), t3_desc(sbr), id_pos, true);
+      } else {
+        tc_mma(d_re, t3_desc(sar), t3_desc(sbr), id_pos, acc);
+        tc_mma(d_re, t3_desc(sai), t3_desc(sbi), id_neg, true);
+        tc_mma(d_im, t3_desc(sar), t3_desc(sbi), id_pos, acc);
+        tc_mma(d_im, t3_desc(sai), t3_desc(sbr), id_pos, true);
+      }
+      tc_commit(mb + 8 * (NS + q));
+      ++issued;
+      if (tc == chunk - 1 || t == ntiles - 1) tc_commit(mb_chunk);
+    }
+    if (issued > 0) {
+      tc_commit(mb_fin);
+      if (!tc_wait(mb_fin, 0u)) {
+        atomicExch(err, 1);
+        s_abort = 1;
+      }
+    }
+  }
+  __syncwarp();
+  __syncthreads();
+  if (!s_abort && ntiles == 0 && warp < T3_CONV_WARPS)
+    t3_drain(d_re, d_im, warp, lane, false, true, M, N, r0, c0, O, ldo_r, ldo_c, alpha, beta, part, blockIdx.z);
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == T4_MMA) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(T3_TMEM_COLS));
+}
+
 // Sum of the column-major split-K partials of k_cgemm_tc3 into the output.
 __global__ void k_cgemm_reduce_cm(int M, int N, int splits, const double2* __restrict__ part, double2* __restrict__ O,
                                   long ldo_r, long ldo_c, double alpha, double beta) {
@@ -1023,6 +1242,7 @@ static TcPlan tc_plan(const GemmArgs& g0) {
     g.A = a.B; g.lda = a.ldb; g.a_kc = a.b_kc; g.conj_a = a.conj_b;
     g.B = a.A; g.ldb = a.lda; g.b_kc = a.a_kc; g.conj_b = a.conj_a;
     g.ldo_r = a.ldo_c; g.ldo_c = a.ldo_r;
+    g.a_cache = a.b_cache; g.b_cache = a.a_cache;
     return g;
   };
   TcPlan p{g0, false, 1};
@@ -1097,11 +1317,108 @@ static int tc_dispatch(const GemmArgs& g, bool wide, dim3 grid, int kps, double2
   return DFTCUDA_OK;
 }
 
-int cgemm_tf32(const GemmArgs& g0, cudaStream_t s, double2* ws, size_t ws_elems, int* err_dev, bool split) {
+// DFTCUDA_TC=v3 keeps the wide products on k_cgemm_tc3 (operands converted inside the GEMM) for A/B
+// measurements; otherwise, with a scratch buffer, they run on pre-split operands (k_cgemm_tc4).
+static bool tc4_enabled() {
+  static const bool v = [] {
+    const char* e = std::getenv("DFTCUDA_TC");
+    return !(e && (std::string(e) == "v1" || std::string(e) == "v2" || std::string(e) == "v3"));
+  }();
+  return v;
+}
+
+static int tc4_run(const GemmArgs& g, cudaStream_t s, double2* ws, size_t ws_elems, int* err_dev, bool split, TcScratch* scratch) {
+  const int np = t4_planes(split);
+  const int RGA = (int)(((size_t)g.M + 255) / 256 * 32), RGB = (int)(((size_t)g.N + 255) / 256 * 32);
+  const int KS = (g.K + 7) / 8;
+  const size_t a_bytes = (size_t)KS * np * RGA * 256, b_bytes = (size_t)KS * np * RGB * 256;
+  // an operand goes to its cache (split once while the cache holds it) or to the per-call scratch
+  auto key_of = [&](const double2* X, long ld, bool kc, bool cj, int R) {
+    unsigned long long h = (unsigned long long)(uintptr_t)X;
+    for (unsigned long long v : {(unsigned long long)ld, (unsigned long long)kc, (unsigned long long)cj, (unsigned long long)R,
+                                 (unsigned long long)g.K, (unsigned long long)split})
+      h = h * 1000003ULL ^ v;
+    return h;
+  };
+  DFT_TRY(scratch->ensure((g.a_cache ? 0 : a_bytes) + (g.b_cache ? 0 : b_bytes)));
+  unsigned char* sp = static_cast<unsigned char*>(scratch->p);
+  auto place = [&](TcScratch* cache, size_t bytes, const double2* X, long ld, bool kc, bool cj, int R, int RG,
+                   float** out) -> int {
+    bool convert = true;
+    if (cache) {
+      const unsigned long long key = key_of(X, ld, kc, cj, R);
+      if (cache->valid && cache->key == key && cache->bytes >= bytes) convert = false;
+      else {
+        cache->valid = false;
+        DFT_TRY(cache->ensure(bytes));
+        cache->key = key;
+        cache->valid = true;
+      }
+      *out = reinterpret_cast<float*>(cache->p);
+    } else {
+      *out = reinterpret_cast<float*>(sp);
+      sp += bytes;
+    }
+    if (convert) {
+      const long units = (long)KS * 2 * RG * 8;
+      if (split) k_tf32_tiles<true><<<ceil_div(units, 256), 256, 0, s>>>(X, ld, kc, cj, R, g.K, RG, KS, *out);
+      else k_tf32_tiles<false><<<ceil_div(units, 256), 256, 0, s>>>(X, ld, kc, cj, R, g.K, RG, KS, *out);
+      count_launch();
+    }
+    return DFTCUDA_OK;
+  };
+  float *At = nullptr, *Bt = nullptr;
+  DFT_TRY(place(g.a_cache, a_bytes, g.A, g.lda, g.a_kc, g.conj_a, g.M, RGA, &At));
+  DFT_TRY(place(g.b_cache, b_bytes, g.B, g.ldb, g.b_kc, g.conj_b, g.N, RGB, &Bt));
+  int splits = g.splits > 0 ? std::min(g.splits, std::max(1, KS / 4)) : t3_splits(g.M, g.N, g.K);
+  if (splits > 1) splits = (int)std::max<size_t>(1, std::min<size_t>(splits, ws_elems / ((size_t)g.M * g.N)));
+  const int kps = (KS + splits - 1) / splits;  // K steps per split
+  splits = (KS + kps - 1) / kps;
+  const dim3 grid(ceil_div(g.N, T3_N), ceil_div(g.M, TC_M), splits);
+  double2* part = splits > 1 ? ws : nullptr;
+  if (split) {
+    DFT_TRY(ensure_max_dynamic_smem((const void*)k_cgemm_tc4<true>, t4_smem(true)));
+    k_cgemm_tc4<true><<<grid, T4_THREADS, t4_smem(true), s>>>(g.M, g.N, At, RGA, Bt, RGB, KS, g.O, g.ldo_r, g.ldo_c, g.alpha, g.beta,
+                                                              kps, part, err_dev, t3_chunk());
+  } else {
+    DFT_TRY(ensure_max_dynamic_smem((const void*)k_cgemm_tc4<false>, t4_smem(false)));
+    k_cgemm_tc4<false><<<grid, T4_THREADS, t4_smem(false), s>>>(g.M, g.N, At, RGA, Bt, RGB, KS, g.O, g.ldo_r, g.ldo_c, g.alpha, g.beta,
+                                                                kps, part, err_dev, t3_chunk());
+  }
+  count_launch();
+  if (part) {
+    const long tot = (long)g.M * g.N;
+    k_cgemm_reduce_cm<<<ceil_div(tot, 256), 256, 0, s>>>(g.M, g.N, splits, part, g.O, g.ldo_r, g.ldo_c, g.alpha, g.beta);
+    count_launch();
+  }
+  DFT_CUDA_TRY(cudaGetLastError());
+  return DFTCUDA_OK;
+}
+
+int TcScratch::ensure(size_t need) {
+  if (need <= bytes) return DFTCUDA_OK;
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+  valid = false;
+  if (cudaMalloc(&p, need) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "tensor-core operand tiles");
+  bytes = need;
+  return DFTCUDA_OK;
+}
+
+void TcScratch::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+  valid = false;
+}
+
+int cgemm_tf32(const GemmArgs& g0, cudaStream_t s, double2* ws, size_t ws_elems, int* err_dev, bool split, TcScratch* scratch) {
   if (g0.M <= 0 || g0.N <= 0) return DFTCUDA_OK;
   if (g0.K <= 0) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "cgemm_tf32: K must be positive");
   const TcPlan p = tc_plan(g0);
   const GemmArgs& g = p.g;
+  if (p.wide && scratch && tc4_enabled()) return tc4_run(g, s, ws, ws_elems, err_dev, split, scratch);
   int splits = g.splits > 0 ? std::min(g.splits, std::max(1, g.K / 32)) : p.splits;
   if (splits > 1) splits = (int)std::max<size_t>(1, std::min<size_t>(splits, ws_elems / ((size_t)g.M * g.N)));  // what fits the workspace
   int kps = (g.K + splits - 1) / splits;

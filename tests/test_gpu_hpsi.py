@@ -154,17 +154,17 @@ def test_zero_columns_is_a_noop(dz):
 @pytest.mark.parametrize("name,ecut,k,prec", [("si2", 20.0, (0.25, 0.125, 0.0), 0), ("sige8", 20.0, (0.25, 0.25, 0.25), 0),
                                               ("al4", 25.0, (0.1, 0.2, 0.3), 1), ("si8", 20.0, (0.5, 0.0, 0.0), 1)])
 def test_all_fft_paths_match_oracle(dz, monkeypatch, path, name, ecut, k, prec):
-    """The three local-operator paths give the oracle's H|psi> and density: the stick-layout passes
-    (the default where nx = ny), the four-step plane-layout passes (DFTCUDA_LOCAL=planes) and the
-    stage-by-stage passes (DFTCUDA_FFT_PATH=generic)."""
+    """The three local-operator paths give the oracle's H|psi> and density: the four-step
+    plane-layout passes (the default), the stick-layout passes (DFTCUDA_LOCAL=sticks, where nx = ny)
+    and the stage-by-stage passes (DFTCUDA_FFT_PATH=generic)."""
     from oracle import density as odens
 
     monkeypatch.delenv("DFTCUDA_FFT_PATH", raising=False)
     monkeypatch.delenv("DFTCUDA_LOCAL", raising=False)
     if path == "generic":
         monkeypatch.setenv("DFTCUDA_FFT_PATH", "generic")
-    elif path == "planes":
-        monkeypatch.setenv("DFTCUDA_LOCAL", "planes")
+    elif path == "sticks":
+        monkeypatch.setenv("DFTCUDA_LOCAL", "sticks")
     kp = kproblem(name, ecut, k)
     kc = make_context(dz, kp, precision=prec)
     x = random_block(kp.ctx.n, 6, 21)
