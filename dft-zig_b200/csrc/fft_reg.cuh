@@ -12,6 +12,10 @@
 // from a per-length global table (L1-cached).
 #pragma once
 
+#include <cmath>
+#include <mutex>
+#include <vector>
+
 #include "common.cuh"
 
 namespace dftcuda {
@@ -25,13 +29,37 @@ __host__ __device__ constexpr int root_off(int L) {
 }
 constexpr int kRootTotal = root_off(16) + 16;
 
-// Defined here (not extern): only local4.cu includes this header, and the library is compiled
-// without relocatable device code.
+// Defined here (not extern): the library is compiled without relocatable device code, so every
+// translation unit that includes this header has its own copy of the tables, and must fill it with
+// init_root_tables_here() (idempotent per device) before its first kernel that uses RegDft runs.
 static __constant__ double2 c_roots64[kRootTotal];
 static __constant__ float2 c_roots32[kRootTotal];
 
-// Loads the root tables into constant memory on the current device (idempotent per device).
-int init_root_tables();
+// Loads this translation unit's root tables into constant memory on the current device.
+static int init_root_tables_here() {
+  static std::mutex mu;
+  static bool done[128] = {};
+  int dev = 0;
+  DFT_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return fail(DFTCUDA_ERR_UNSUPPORTED, "device ordinal above 127");
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev]) return DFTCUDA_OK;
+  std::vector<double2> r64(kRootTotal);
+  std::vector<float2> r32(kRootTotal);
+  for (int i = 0; i < kNumRootLens; ++i) {
+    const int L = kRootLens[i], off = root_off(L);
+    for (int e = 0; e < L; ++e) {
+      const double a = 2.0 * M_PI * (double)e / (double)L;
+      r64[off + e] = make_double2(std::cos(a), std::sin(a));
+      r32[off + e] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+  }
+  DFT_CUDA_TRY(cudaMemcpyToSymbol(c_roots64, r64.data(), sizeof(double2) * kRootTotal));
+  DFT_CUDA_TRY(cudaMemcpyToSymbol(c_roots32, r32.data(), sizeof(float2) * kRootTotal));
+  DFT_CUDA_TRY(cudaDeviceSynchronize());
+  done[dev] = true;
+  return DFTCUDA_OK;
+}
 
 template <typename T> __device__ __forceinline__ cplx<T> root(int idx);
 template <> __device__ __forceinline__ double2 root<double>(int idx) { return c_roots64[idx]; }

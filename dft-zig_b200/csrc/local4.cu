@@ -24,31 +24,6 @@
 
 namespace dftcuda {
 
-int init_root_tables() {
-  static std::mutex mu;
-  static bool done[128] = {};
-  int dev = 0;
-  DFT_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 128) return fail(DFTCUDA_ERR_UNSUPPORTED, "device ordinal above 127");
-  std::lock_guard<std::mutex> lock(mu);
-  if (done[dev]) return DFTCUDA_OK;
-  std::vector<double2> r64(kRootTotal);
-  std::vector<float2> r32(kRootTotal);
-  for (int i = 0; i < kNumRootLens; ++i) {
-    const int L = kRootLens[i], off = root_off(L);
-    for (int e = 0; e < L; ++e) {
-      const double a = 2.0 * M_PI * (double)e / (double)L;
-      r64[off + e] = make_double2(std::cos(a), std::sin(a));
-      r32[off + e] = make_float2((float)std::cos(a), (float)std::sin(a));
-    }
-  }
-  DFT_CUDA_TRY(cudaMemcpyToSymbol(c_roots64, r64.data(), sizeof(double2) * kRootTotal));
-  DFT_CUDA_TRY(cudaMemcpyToSymbol(c_roots32, r32.data(), sizeof(float2) * kRootTotal));
-  DFT_CUDA_TRY(cudaDeviceSynchronize());
-  done[dev] = true;
-  return DFTCUDA_OK;
-}
-
 bool four_step_supported(int n) {
   switch (n) {
 #define X(N) case N:
@@ -833,7 +808,7 @@ int kctx_setup_fast_path(dftcuda_kctx* c, const std::vector<int>& slot_of_x, con
   c->fast64 = kctx_fast_path_ok(c, DFTCUDA_PRECISION_FP64);
   c->fast32 = kctx_fast_path_ok(c, DFTCUDA_PRECISION_FP32);
   if (!c->fast64 && !c->fast32) return DFTCUDA_OK;
-  DFT_TRY(init_root_tables());
+  DFT_TRY(init_root_tables_here());
   const int nx = c->nx, ny = c->ny, nz = c->nz, P = c->P, n_act = c->n_act;
   std::vector<int> pwmap((size_t)n_act * P, -1);
   std::vector<std::vector<int>> sticks(n_act);

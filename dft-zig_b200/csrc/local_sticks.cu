@@ -679,6 +679,7 @@ int kctx_setup_sticks(dftcuda_kctx* c, const std::vector<int>& slot_of_x, const 
   c->sticks64 = kctx_sticks_ok(c, DFTCUDA_PRECISION_FP64);
   c->sticks32 = kctx_sticks_ok(c, DFTCUDA_PRECISION_FP32);
   if (!c->sticks64 && !c->sticks32) return DFTCUDA_OK;
+  DFT_TRY(init_root_tables_here());  // this file's copy of the sub-DFT roots
   const int ny = c->ny, nz = c->nz, n_act = c->n_act;
   std::vector<std::vector<int>> ys(n_act);
   std::vector<std::vector<char>> has(n_act, std::vector<char>(ny, 0));
