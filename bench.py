@@ -48,10 +48,62 @@ WORKLOADS = {
 }
 CELL, SEED, ECUT, KMESH, NBANDS = "si64", 1, 30.0, (2, 2, 2), 160  # the Si64 cell of the profiling cases
 S = 16  # bytes per FP64 complex
+# The three local passes of each layout (the library's profile reports which ran: 0 generic, 1 plane
+# layout, 2 stick layout).
+LOCAL_KERNELS = {0: ("k_plane_inv", "k_xline", "k_plane_fwd"), 1: ("k_plane_inv5", "k_xline5", "k_plane_fwd5"),
+                 2: ("k_stick_inv", "k_zplane", "k_stick_fwd")}
 # Measured DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum) of the three local passes
-# per column, FP64: Si64 (75^3) from one 32-column application at Gamma; Si216 (108^3) from one
-# 16-column application at Gamma (profiles/local_kernels_dram_traffic_*.md).
-LOCAL_DRAM_BYTES_PER_COLUMN = {"si64": 315.0e6 / 32, "si216": None}
+# per column, FP64, keyed by (cell, layout): from one application of a small Gamma case of the cell
+# (Si64: 32 columns, Si216: 16 columns), scaled to a block by the columns processed.
+LOCAL_DRAM_BYTES_PER_COLUMN = {("si64", 1): 315.0e6 / 32}
+DRAM_SOURCE = {("si64", 1): "profiles/local_kernels_dram_traffic_si64_fp64.md"}
+
+
+# Complex GEMM shapes of the Si216 Davidson step (n_pw = 61,565, 448 bands, subspace up to 1,800):
+# M, N, K, conj_a, description.  out(r, c) = sum_k op(A(r, k)) B(c, k), A and B row-major [rows][K].
+GEMM_SHAPES = {
+    "gram1344": (1344, 1344, 120000, True, "Gram V^H W, 1344 x 1344, K = 120,000"),
+    "t448x1344": (1344, 448, 61565, True, "new Rayleigh-Ritz columns V^H W_new, 1344 x 448, K = n_pw"),
+    "rot448": (61565, 448, 1344, False, "Ritz rotation V C, n_pw x 448, K = 1344"),
+    "proj864": (864, 452, 61565, True, "projections <beta|psi>, 864 projectors x 452 columns, K = n_pw"),
+}
+
+
+def run_gemm_workload(args):
+    """The library's complex GEMM (dftcuda_complex_gemm) on the Si216 Davidson shapes: seeded
+    complex128 operands resident on the device, one warm-up call, then the fastest of three calls
+    (host clock around the synchronous call: kernels plus one stream sync, no allocation after the
+    first call).  Error = max |out - out_FP64| / max |out_FP64|."""
+    import torch
+
+    import dftzig_loader
+
+    dz = dftzig_loader.load()
+    prec_of = {"fp64": dz.PRECISION_FP64, "tf32x3": dz.PRECISION_TF32X3, "tf32": dz.PRECISION_TF32}
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    out = {}
+    for name in [s for s in args.gemm_shapes.split(",") if s]:
+        M, N, K, conj_a, desc = GEMM_SHAPES[name]
+        a = torch.randn(M, K, dtype=torch.complex128, device="cuda", generator=gen)
+        b = torch.randn(N, K, dtype=torch.complex128, device="cuda", generator=gen)
+        o = torch.zeros(N, M, dtype=torch.complex128, device="cuda").T
+        ref = torch.zeros_like(o)
+        dz.complex_gemm(a, b, ref, conj_a=conj_a, precision=dz.PRECISION_FP64)
+        row = {"shape": desc}
+        for pn in [p for p in args.gemm_precisions.split(",") if p]:
+            dz.complex_gemm(a, b, o, conj_a=conj_a, precision=prec_of[pn])
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                dz.complex_gemm(a, b, o, conj_a=conj_a, precision=prec_of[pn])
+                ts.append(time.perf_counter() - t0)
+            err = float((o - ref).abs().max() / ref.abs().max())
+            row[pn] = {"ms": round(1e3 * min(ts), 3), "useful_tflops": round(8.0 * M * N * K / min(ts) / 1e12, 1), "rel_err": err}
+        out[name] = row
+        del a, b, o, ref
+        torch.cuda.empty_cache()
+    print(json.dumps({"workload": "complex GEMM, Si216 Davidson shapes", "useful_flops": "8 M N K", "shapes": out}), flush=True)
 
 
 def bytes_per_column(npw: int, N: int, nb: int) -> float:
@@ -69,13 +121,17 @@ def parse():
     ap.add_argument("--no-variants", action="store_true", help="skip the FP32 / TF32 variants of the H|psi> step")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile-case", action="store_true", help="small single-k case for ncu captures: Gamma, 32 columns, 2 applications")
-    ap.add_argument("--workload", choices=("hpsi", "scf", "scf64", "scf216", "al4", "cells", "eig", "heev"), default="hpsi",
+    ap.add_argument("--workload", choices=("hpsi", "scf", "scf64", "scf216", "al4", "cells", "eig", "heev", "gemm"), default="hpsi",
                     help="hpsi: H|psi> GB/s (default); scf: time-to-SCF Si2; scf64: time-to-SCF Si64, mixed vs FP64; "
                          "scf216: time-to-SCF Si216 (Gamma, 448 bands), FP64 vs learned+mixed; "
                          "al4: time-to-SCF Al4 8x8x8 (260 k-points, batched), FP64 vs mixed; "
                          "cells: many-cell SiGe8 SCF throughput, atomic vs learned start; "
                          "eig: one Si64 Gamma Davidson solve (profiling case); "
-                         "heev: the subspace eigensolver on a seeded Hermitian matrix (--heev-m, lowest m/3 pairs)")
+                         "heev: the subspace eigensolver on a seeded Hermitian matrix (--heev-m, lowest m/3 pairs); "
+                         "gemm: the library's complex GEMM on the Si216 Davidson shapes (--gemm-shapes), FP64 / 3xTF32 / TF32")
+    ap.add_argument("--gemm-shapes", default="gram1344,t448x1344,rot448,proj864",
+                    help="comma list of --workload gemm shapes: " + ", ".join(f"{k} ({v[4]})" for k, v in GEMM_SHAPES.items()))
+    ap.add_argument("--gemm-precisions", default="fp64,tf32x3,tf32", help="comma list of --workload gemm precisions")
     ap.add_argument("--heev-m", type=int, default=1344, help="matrix size of --workload heev")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="scf216: instead of time-to-SCF, run N SCF steps of each arm and print its kernel-time "
@@ -276,6 +332,8 @@ def run_ours(args):
 
     # roofline: the fused local operator (three passes) is the dominant work
     tot = {k: sum(p[k] for p in profs) for k in profs[0]}
+    layout = int(profs[0]["local_layout"])
+    local_kernels = LOCAL_KERNELS[layout]
     launches = int(tot["kernel_launches"])
     local_ns = tot["apply_local_ns"]
     npw_avg = float(np.mean([kc.n for kc in ctxs]))
@@ -285,8 +343,10 @@ def run_ours(args):
     value = world * algo_bytes_step / (ms * 1e-3) / 1e9
     e2e_value = world * algo_bytes_step / (e2e_ms * 1e-3) / 1e9
     h2d = sum(x.numel() * 16 for x in hx)
+    names = dict(zip(("local_plane_inv_ns", "local_xline_ns", "local_plane_fwd_ns"), local_kernels))
+    names.update(nl_project_ns="projection GEMM", nl_dij_ns="D_ij", nl_backproject_ns="back-projection GEMM")
     kern = {
-        k: {"ms_per_step": tot[k] / 1e6 / args.steps, "share": tot[k] / max(tot["apply_h_ns"], 1)}
+        k: {"kernel": names[k], "ms_per_step": tot[k] / 1e6 / args.steps, "share": tot[k] / max(tot["apply_h_ns"], 1)}
         for k in ("local_plane_inv_ns", "local_xline_ns", "local_plane_fwd_ns", "nl_project_ns", "nl_dij_ns", "nl_backproject_ns")
     }
     # The same workload with the FP32 FFT passes (FP64 projector GEMMs) and in TF32 mode (FP32 FFT
@@ -316,7 +376,7 @@ def run_ours(args):
         for kc in vctx:
             kc.close()
 
-    dram = LOCAL_DRAM_BYTES_PER_COLUMN[args.cell]
+    dram = LOCAL_DRAM_BYTES_PER_COLUMN.get((args.cell, layout))
     line = {
         "metric": "H|psi> HBM GB/s (algorithmic)",
         "value": round(value, 2),
@@ -343,7 +403,7 @@ def run_ours(args):
         "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d, "timer": "host wall clock around synchronous C-ABI calls", "matches_device_result": ok},
         "gpu_launches": launches,
         "roofline": {
-            "kernel": f"local H|psi>: k_plane_inv5 + k_xline5 + k_plane_fwd5 (one {NCOLS}-column block)",
+            "kernel": f"local H|psi>: {' + '.join(local_kernels)} (one {NCOLS}-column block)",
             "bound": "hbm",
             "achieved": round(achieved, 1) if achieved else None,
             "peak": peak,
@@ -353,6 +413,7 @@ def run_ours(args):
             # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the three passes per column,
             # from one ncu capture of a small Gamma case of the same cell, scaled to one block
             "traffic": round(dram * NCOLS) if dram else None,
+            "traffic_source": DRAM_SOURCE.get((args.cell, layout)) if dram else None,
             "algorithmic_bytes": round(bytes_per_column(int(npw_avg), N, NCOLS) * NCOLS),
             "per": f"one {NCOLS}-column application of the local operator at one k-point",
         },
@@ -950,6 +1011,8 @@ def run_scf216_kernel_table(args):
 
 def main():
     args = parse()
+    if args.workload == "gemm":
+        return run_gemm_workload(args)
     if args.workload == "heev":
         run_heev_workload(args)
         return

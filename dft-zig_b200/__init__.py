@@ -179,6 +179,7 @@ PROFILE_FIELDS = (
     "nl_dij_ns",
     "nl_backproject_ns",
     "kernel_launches",
+    "local_layout",
 )
 
 

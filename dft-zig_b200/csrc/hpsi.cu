@@ -251,7 +251,7 @@ static size_t box_bytes_per_col(const dftcuda_kctx* c) {
 
 // The local passes of this context's precision use the stick layout (local_sticks.cu).
 static bool use_sticks(const dftcuda_kctx* c) {
-  if (c->fft_generic) return false;
+  if (c->fft_generic || c->sticks_off) return false;
   return c->precision == DFTCUDA_PRECISION_FP64 ? c->sticks64 : c->sticks32;
 }
 
@@ -399,6 +399,7 @@ int kctx_apply_h_dev(dftcuda_kctx* c, const double2* x, double2* y, size_t ncols
   const size_t ch = chunk_cols(c, ncols, true);
   DFT_TRY(ensure_box(c, ch, true));
   const bool sticks = use_sticks(c);
+  c->last_layout = sticks ? 2 : ((c->precision == DFTCUDA_PRECISION_FP64 ? c->fast64 : c->fast32) && !c->fft_generic ? 1 : 0);
   for (size_t c0 = 0; c0 < ncols; c0 += ch) {
     const size_t nc = std::min(ch, ncols - c0);
     const double2* xc = x + c0 * c->npw;

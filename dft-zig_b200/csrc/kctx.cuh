@@ -100,6 +100,8 @@ struct dftcuda_kctx {
   // Four-step path tables (local4.cu): used when fast64 / fast32 is set for the precision.
   bool fast64 = false, fast32 = false;
   bool fft_generic = false;  // autotuner choice: the generic shared-memory FFT passes even where the four-step path exists
+  bool sticks_off = false;   // autotuner choice: the plane layout even where the stick layout exists
+  int last_layout = -1;      // layout of the last H|psi>: 0 generic passes, 1 plane layout, 2 stick layout
   int split_proj = 0, split_back = 0;  // autotuner choices for the projector GEMMs (0 = heuristic)
   int precond_kind = 0;                // DFTCUDA_PRECOND_* of the Davidson correction step
   float* d_mlp = nullptr;              // learned preconditioner weights (DFTCUDA_PRECOND_MLP_PARAMS)

@@ -484,10 +484,11 @@ static int plane_warps_rt(size_t cs, int n, int n_act) {
   }
 }
 
-// The stick-layout passes are opt-in: DFTCUDA_LOCAL=sticks, read at context creation.
+// The stick layout is the default where it applies; DFTCUDA_LOCAL=planes (read at context
+// creation) keeps the plane layout.
 static bool sticks_disabled() {
   const char* e = std::getenv("DFTCUDA_LOCAL");
-  return !(e && std::string(e) == "sticks");
+  return e && std::string(e) == "planes";
 }
 
 bool kctx_sticks_ok(const dftcuda_kctx* c, int precision) {

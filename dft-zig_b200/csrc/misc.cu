@@ -170,6 +170,7 @@ extern "C" int dftcuda_kctx_get_profile(dftcuda_kctx* c, dftcuda_profile* out) {
   uint64_t l = 0;
   for (int i = 0; i < P_NCAT; ++i) l += p.launches[i];
   r.kernel_launches = l;
+  r.local_layout = c->last_layout < 0 ? 0 : (uint64_t)c->last_layout;
   *out = r;
   return DFTCUDA_OK;
 }
@@ -193,32 +194,52 @@ extern "C" int dftcuda_complex_gemm(int precision, size_t M, size_t N, size_t K,
   g.alpha = alpha; g.beta = beta;
   const bool tc = precision_uses_tc(precision);
   const size_t ws_elems = tc ? cgemm_tf32_workspace_elems(g.M, g.N, g.K) : zgemm_workspace_elems(g.M, g.N, g.K);
-  cudaStream_t s = nullptr;
-  double2* ws = nullptr;
-  int* err = nullptr;
-  TcScratch tiles;  // the pre-split operands of the wide tensor-core kernel
-  int rc = DFTCUDA_OK;
-  auto cleanup = [&] {
-    if (s) cudaStreamSynchronize(s);
-    tiles.release();
-    if (s) cudaStreamDestroy(s);
-    if (ws) cudaFree(ws);
-    if (err) cudaFree(err);
+  int dev = 0;
+  DFT_CUDA_TRY(cudaGetDevice(&dev));
+  // One engine per device (stream, split-K workspace, error flag, pre-split operand tiles), kept for
+  // the life of the process and grown on demand, so that a call costs its kernels and one sync.
+  struct Engine {
+    cudaStream_t s = nullptr;
+    double2* ws = nullptr;
+    size_t ws_cap = 0;
+    int* err = nullptr;
+    TcScratch tiles;
+    std::mutex mu;
   };
-  if (cudaStreamCreateWithFlags(&s, cudaStreamDefault) != cudaSuccess ||
-      (ws_elems && cudaMalloc(&ws, sizeof(double2) * ws_elems) != cudaSuccess) || cudaMalloc(&err, sizeof(int)) != cudaSuccess ||
-      cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) {
-    cleanup();
-    return fail(DFTCUDA_ERR_CUDA, "complex_gemm: stream or workspace allocation failed");
+  static std::mutex map_mu;
+  static std::map<int, Engine*> engines;
+  Engine* en = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(map_mu);
+    Engine*& slot = engines[dev];
+    if (!slot) slot = new Engine();  // never freed: device memory is released at context teardown
+    en = slot;
   }
-  rc = tc ? cgemm_tf32(g, s, ws, ws_elems, err, precision == DFTCUDA_PRECISION_TF32X3, &tiles) : zgemm(g, s, ws, ws_elems);
+  std::lock_guard<std::mutex> lock(en->mu);
+  if (!en->s && (cudaStreamCreateWithFlags(&en->s, cudaStreamDefault) != cudaSuccess || cudaMalloc(&en->err, sizeof(int)) != cudaSuccess)) {
+    if (en->s) cudaStreamDestroy(en->s);
+    en->s = nullptr;
+    en->err = nullptr;
+    return fail(DFTCUDA_ERR_CUDA, "complex_gemm: stream or error-flag allocation failed");
+  }
+  if (ws_elems > en->ws_cap) {
+    cudaStreamSynchronize(en->s);
+    if (en->ws) cudaFree(en->ws);
+    en->ws = nullptr;
+    en->ws_cap = 0;
+    if (cudaMalloc(&en->ws, sizeof(double2) * ws_elems) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "complex_gemm: workspace");
+    en->ws_cap = ws_elems;
+  }
+  DFT_CUDA_TRY(cudaMemsetAsync(en->err, 0, sizeof(int), en->s));
+  en->tiles.valid = false;  // operands differ from call to call
+  int rc = tc ? cgemm_tf32(g, en->s, en->ws, en->ws_cap, en->err, precision == DFTCUDA_PRECISION_TF32X3, &en->tiles)
+              : zgemm(g, en->s, en->ws, en->ws_cap);
   int herr = 0;
+  const cudaError_t e = rc == DFTCUDA_OK ? cudaMemcpyAsync(&herr, en->err, sizeof(int), cudaMemcpyDeviceToHost, en->s) : cudaSuccess;
+  const cudaError_t e2 = cudaStreamSynchronize(en->s);
   if (rc == DFTCUDA_OK) {
-    const cudaError_t e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
-    const cudaError_t e2 = cudaStreamSynchronize(s);
     if (e != cudaSuccess || e2 != cudaSuccess) rc = fail(DFTCUDA_ERR_CUDA, std::string("complex_gemm: ") + cudaGetErrorString(e2));
     else if (herr) rc = fail(DFTCUDA_ERR_TIMEOUT, "complex_gemm: a tensor-core pipeline wait timed out");
   }
-  cleanup();
   return rc;
 }

@@ -76,15 +76,29 @@ extern "C" int dftcuda_kctx_autotune(dftcuda_kctx* c, size_t ncols, dftcuda_tune
   double best = 0.0;
   st = measure(&best);
   const double default_ms = best;
-  // 1. FFT path
+  // 1. local-operator layout: stick layout, plane layout (four-step passes), generic passes
   const bool fast_avail = (c->precision == DFTCUDA_PRECISION_FP64) ? c->fast64 : c->fast32;
-  if (st == DFTCUDA_OK && fast_avail) {
-    const bool keep = c->fft_generic;
-    c->fft_generic = !keep;
-    double t = 0.0;
-    st = measure(&t);
-    if (st == DFTCUDA_OK && t < best) best = t;
-    else c->fft_generic = keep;
+  const bool sticks_avail = (c->precision == DFTCUDA_PRECISION_FP64) ? c->sticks64 : c->sticks32;
+  if (st == DFTCUDA_OK && (fast_avail || sticks_avail)) {
+    const bool keep_generic = c->fft_generic, keep_off = c->sticks_off;
+    bool pick_generic = keep_generic, pick_off = keep_off;
+    const bool cand[3][2] = {{false, false}, {false, true}, {true, true}};  // {generic, sticks_off}
+    for (int i = 0; i < 3 && st == DFTCUDA_OK; ++i) {
+      if (cand[i][0] == keep_generic && cand[i][1] == keep_off) continue;  // the default, timed above
+      if (!cand[i][0] && !cand[i][1] && !sticks_avail) continue;
+      if (!cand[i][0] && cand[i][1] && !fast_avail) continue;
+      c->fft_generic = cand[i][0];
+      c->sticks_off = cand[i][1];
+      double t = 0.0;
+      st = measure(&t);
+      if (st == DFTCUDA_OK && t < best) {
+        best = t;
+        pick_generic = cand[i][0];
+        pick_off = cand[i][1];
+      }
+    }
+    c->fft_generic = pick_generic;
+    c->sticks_off = pick_off;
   }
   // 2. box workspace budget
   if (st == DFTCUDA_OK) {
@@ -129,7 +143,7 @@ extern "C" int dftcuda_kctx_autotune(dftcuda_kctx* c, size_t ncols, dftcuda_tune
   if (st != DFTCUDA_OK) return st;
   DFT_TRY(kctx_check_error(c));
   if (report) {
-    report->fft_path = c->fft_generic ? 0 : (fast_avail ? 1 : 0);
+    report->fft_path = c->fft_generic ? 0 : (sticks_avail && !c->sticks_off ? 2 : (fast_avail ? 1 : 0));
     report->box_budget_mb = c->w_budget_bytes / (1024.0 * 1024.0);
     report->proj_splits = c->split_proj;
     report->back_splits = c->split_back;

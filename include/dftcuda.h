@@ -146,7 +146,7 @@ int dftcuda_nonlocal_stress(dftcuda_kctx* ctx, const double* kpg, size_t n_speci
  * columns (FFT pass variant, column-chunk workspace budget, split-K of the two projector GEMMs)
  * with CUDA events and keeps the fastest for all later calls.  report may be NULL. */
 typedef struct dftcuda_tune_report {
-  int fft_path;          /* 1 four-step register FFT passes, 0 generic shared-memory passes */
+  int fft_path;          /* 2 stick layout, 1 plane layout (four-step register FFT passes), 0 generic passes */
   double box_budget_mb;  /* active-plane workspace budget per column chunk */
   int proj_splits;       /* split-K of the projection GEMM (0 = built-in heuristic) */
   int back_splits;       /* split-K of the back-projection GEMM (0 = built-in heuristic) */
@@ -306,6 +306,9 @@ typedef struct dftcuda_profile {
   uint64_t nl_dij_ns;           /* D_ij                                                            */
   uint64_t nl_backproject_ns;   /* sum |beta> D <beta|psi> GEMM                                    */
   uint64_t kernel_launches;     /* libdftcuda kernels launched on this context while profiling     */
+  uint64_t local_layout;        /* passes of the last H|psi>: 0 generic, 1 plane layout (three passes
+                                   k_plane_inv5, k_xline5, k_plane_fwd5), 2 stick layout (k_stick_inv,
+                                   k_zplane, k_stick_fwd: the three counters above in that order)  */
 } dftcuda_profile;
 
 int dftcuda_kctx_set_profiling(dftcuda_kctx* ctx, int enable);

@@ -154,22 +154,29 @@ def test_zero_columns_is_a_noop(dz):
 @pytest.mark.parametrize("name,ecut,k,prec", [("si2", 20.0, (0.25, 0.125, 0.0), 0), ("sige8", 20.0, (0.25, 0.25, 0.25), 0),
                                               ("al4", 25.0, (0.1, 0.2, 0.3), 1), ("si8", 20.0, (0.5, 0.0, 0.0), 1)])
 def test_all_fft_paths_match_oracle(dz, monkeypatch, path, name, ecut, k, prec):
-    """The three local-operator paths give the oracle's H|psi> and density: the four-step
-    plane-layout passes (the default), the stick-layout passes (DFTCUDA_LOCAL=sticks, where nx = ny)
-    and the stage-by-stage passes (DFTCUDA_FFT_PATH=generic)."""
+    """The three local-operator paths give the oracle's H|psi> and density: the stick-layout passes
+    (the default where nx = ny), the four-step plane-layout passes (DFTCUDA_LOCAL=planes) and the
+    stage-by-stage passes (DFTCUDA_FFT_PATH=generic).  The profile reports the layout that ran."""
     from oracle import density as odens
 
     monkeypatch.delenv("DFTCUDA_FFT_PATH", raising=False)
     monkeypatch.delenv("DFTCUDA_LOCAL", raising=False)
     if path == "generic":
         monkeypatch.setenv("DFTCUDA_FFT_PATH", "generic")
-    elif path == "sticks":
-        monkeypatch.setenv("DFTCUDA_LOCAL", "sticks")
+    elif path == "planes":
+        monkeypatch.setenv("DFTCUDA_LOCAL", "planes")
     kp = kproblem(name, ecut, k)
     kc = make_context(dz, kp, precision=prec)
     x = random_block(kp.ctx.n, 6, 21)
     tol = 1e-11 if prec == 0 else 5e-5
     assert rel_err(kc.apply_hamiltonian_batched(x), kp.ctx.apply_batch(x)) < tol
+    layout = kc.profile()["local_layout"]
+    if path == "generic":
+        assert layout == 0
+    elif path == "planes":
+        assert layout == 1
+    elif kp.grid.nx == kp.grid.ny:
+        assert layout == 2
     w = np.array([2.0, 1.0, 0.5, 0.25, 0.0, 1.5])
     rho = np.zeros(kp.grid.count)
     kc.accumulate_band_density(x, w, rho)
@@ -185,7 +192,7 @@ def test_autotune_keeps_results(dz):
     kc = make_context(dz, kp)
     rep = kc.autotune(48)
     assert rep["candidates"] >= 4 and rep["tuned_ms"] <= rep["default_ms"] + 1e-9
-    assert rep["fft_path"] in (0, 1) and rep["box_budget_mb"] > 0
+    assert rep["fft_path"] in (0, 1, 2) and rep["box_budget_mb"] > 0
     x = random_block(kp.ctx.n, 48, 5)
     assert rel_err(kc.apply_hamiltonian_batched(x), kp.ctx.apply_batch(x)) < 1e-11
     kc.close()
