@@ -462,6 +462,7 @@ struct KCtxImpl {
   bool rr_tc = false;  // Rayleigh-Ritz products on the tensor cores (3xTF32), TF32/TF32X3 contexts
   int* err = nullptr;  // the context's tensor-core error flag
   TcScratch* tcs = nullptr;  // the context's pre-split operand buffer
+  double tc_min_flops = 0.0;  // smaller products take the FP64 GEMM (dftcuda_kctx::tc_min_flops)
   // pinned host mirrors of the per-iteration read-backs
   void* pinned = nullptr;
   double *h_ev = nullptr, *h_nr = nullptr;
@@ -543,7 +544,7 @@ static int eig_alloc(dftcuda_kctx* c, size_t n, size_t max_sub, size_t nb) {
 // form (FP32-class accuracy); the Cholesky factorisations, the subspace eigensolver and the residual
 // norms stay FP64.  FP64 and FP32 contexts use the FP64 GEMM throughout.
 static int gemm_dispatch(KCtxImpl* e, const GemmArgs& g, bool /*rr*/, cudaStream_t s) {
-  if (e->rr_tc) return cgemm_tf32(g, s, e->ws, e->ws_elems, e->err, true, e->tcs);
+  if (e->rr_tc && tc_worthwhile(g.M, g.N, g.K, e->tc_min_flops)) return cgemm_tf32(g, s, e->ws, e->ws_elems, e->err, true, e->tcs);
   return zgemm(g, s, e->ws, e->ws_elems);
 }
 
@@ -759,6 +760,7 @@ static int run_init(EigRun& r, const double* diag, const double* init_vecs, size
   }
   e->err = c->d_err;
   e->tcs = &c->tc_scratch;
+  e->tc_min_flops = c->tc_min_flops;
   const char* gram_mode = std::getenv("DFTCUDA_GRAM");
   r.gram_full = gram_mode && std::strcmp(gram_mode, "full") == 0;
   DFT_CUDA_TRY(cudaMemcpyAsync(e->diag, diag, sizeof(double) * n,

@@ -358,7 +358,7 @@ int kctx_project(dftcuda_kctx* c, const double2* x, size_t ncols, cudaStream_t s
   g.alpha = 1.0; g.beta = 0.0;
   g.splits = c->split_proj;
   g.a_cache = &c->tc_ptiles_proj;
-  if (precision_uses_tc(c->precision))
+  if (precision_uses_tc(c->precision) && tc_worthwhile(g.M, g.N, g.K, c->tc_min_flops))
     return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err, c->precision == DFTCUDA_PRECISION_TF32X3, &c->tc_scratch);
   return zgemm(g, s, c->d_gemm_ws, c->gemm_ws_elems);
 }
@@ -384,7 +384,7 @@ static int nonlocal_block(dftcuda_kctx* c, const double2* x, double2* y, size_t 
   g.alpha = 1.0 / c->volume; g.beta = 1.0;
   g.splits = c->split_back;
   g.b_cache = &c->tc_ptiles_back;
-  if (precision_uses_tc(c->precision))
+  if (precision_uses_tc(c->precision) && tc_worthwhile(g.M, g.N, g.K, c->tc_min_flops))
     return cgemm_tf32(g, s, c->d_gemm_ws, c->gemm_ws_elems, c->d_err, c->precision == DFTCUDA_PRECISION_TF32X3, &c->tc_scratch);
   return zgemm(g, s, c->d_gemm_ws, c->gemm_ws_elems);
 }
@@ -630,6 +630,7 @@ extern "C" int dftcuda_kctx_create(dftcuda_kctx** out, int nx, int ny, int nz, d
     dftcuda_kctx_destroy(c);
     return fail(DFTCUDA_ERR_CUDA, "kctx_create: upload");
   }
+  if (const char* e = std::getenv("DFTCUDA_TC_MIN_FLOP")) c->tc_min_flops = std::atof(e);
   // The four-step register-FFT passes, unless DFTCUDA_FFT_PATH=generic asks for the stage-by-stage ones.
   const char* path = std::getenv("DFTCUDA_FFT_PATH");
   if (!(path && std::string(path) == "generic")) {

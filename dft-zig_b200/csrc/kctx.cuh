@@ -43,6 +43,7 @@ size_t zgemm_workspace_elems(int M, int N, int K);
 int cgemm_tf32(const GemmArgs& g, cudaStream_t s, double2* workspace, size_t workspace_elems, int* err_dev, bool split,
                TcScratch* scratch = nullptr);
 inline bool precision_uses_tc(int p) { return p == DFTCUDA_PRECISION_TF32 || p == DFTCUDA_PRECISION_TF32X3; }
+inline bool tc_worthwhile(int M, int N, int K, double min_flops) { return 8.0 * M * (double)N * K >= min_flops; }
 size_t cgemm_tf32_workspace_elems(int M, int N, int K);
 
 struct NonlocalDev {
@@ -101,6 +102,10 @@ struct dftcuda_kctx {
   bool fast64 = false, fast32 = false;
   bool fft_generic = false;  // autotuner choice: the generic shared-memory FFT passes even where the four-step path exists
   bool sticks_off = false;   // autotuner choice: the plane layout even where the stick layout exists
+  // TF32 / TF32X3 contexts: contractions of fewer useful FLOPs (8 M N K) than this run on the FP64
+  // GEMM, where the operand split and its extra launches would cost more than the tensor cores save
+  // (the FP64 result is within every mode's error bound).  DFTCUDA_TC_MIN_FLOP at creation overrides.
+  double tc_min_flops = 5e8;
   int last_layout = -1;      // layout of the last H|psi>: 0 generic passes, 1 plane layout, 2 stick layout
   int split_proj = 0, split_back = 0;  // autotuner choices for the projector GEMMs (0 = heuristic)
   int precond_kind = 0;                // DFTCUDA_PRECOND_* of the Davidson correction step
