@@ -55,8 +55,9 @@ LOCAL_KERNELS = {0: ("k_plane_inv", "k_xline", "k_plane_fwd"), 1: ("k_plane_inv5
 # Measured DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum) of the three local passes
 # per column, FP64, keyed by (cell, layout): from one application of a small Gamma case of the cell
 # (Si64: 32 columns, Si216: 16 columns), scaled to a block by the columns processed.
-LOCAL_DRAM_BYTES_PER_COLUMN = {("si64", 1): 315.0e6 / 32}
-DRAM_SOURCE = {("si64", 1): "profiles/local_kernels_dram_traffic_si64_fp64.md"}
+LOCAL_DRAM_BYTES_PER_COLUMN = {("si64", 1): 315.0e6 / 32, ("si216", 2): 149.0e6 / 16}
+DRAM_SOURCE = {("si64", 1): "profiles/local_kernels_dram_traffic_si64_fp64.md",
+               ("si216", 2): "profiles/local_kernels_dram_traffic_si216_sticks_fp64.md"}
 
 
 # Complex GEMM shapes of the Si216 Davidson step (n_pw = 61,565, 448 bands, subspace up to 1,800):

@@ -54,9 +54,11 @@ def _features(kin, ekin, rabs, rms, t):
 def precond_samples(dz, cells, ecut: float, nbands, t_max: int = 20, kfrac=(0.0, 0.0, 0.0), cluster_tol: float = 1e-4,
                     min_overlap: float = 0.5, t_list=None, bands_per_t=None, seed: int = 0):
     """Residual -> correction samples along Davidson trajectories preconditioned by TPA (the form
-    the network refines).  Target of band b at iteration t: delta_b = y - psi_b <psi_b|y>, y the
+    the network refines).  Target of band b at iteration t: delta_b = (1 - Psi Psi^H) y, y the
     normalised projection of psi_b^t on the converged eigenspace of its group of (near-)degenerate
-    bands (gaps < cluster_tol Ry), kept when that projection has norm >= min_overlap.
+    bands (gaps < cluster_tol Ry), kept when that projection has norm >= min_overlap, and Psi all nb
+    Ritz vectors of iteration t: the part of the correction that the subspace does not hold yet
+    (whatever lies in span(Psi) the Rayleigh-Ritz step finds without a new direction).
     nbands: a number, or a function of the cell (e.g. its occupied bands); t_list: the iterations
     sampled (default 1..t_max); bands_per_t: keep at most this many bands per (cell, t), drawn with
     a seeded generator (bounds the data of large cells)."""
@@ -89,7 +91,7 @@ def precond_samples(dz, cells, ecut: float, nbands, t_max: int = 20, kfrac=(0.0,
                 if ny < min_overlap:
                     continue
                 y /= ny
-                delta = y - psi[b] * np.vdot(psi[b], y)
+                delta = y - psi.T @ (psi.conj() @ y)
                 dn = float(np.vdot(delta, delta).real)
                 if dn < 1e-24:
                     continue
