@@ -159,6 +159,57 @@ def train_precond(dz, samples, steps: int = 1500, lr: float = 2e-3, seed: int = 
     return p, hist
 
 
+def scale_output(params, alpha: float) -> np.ndarray:
+    """The network with its output layer (w3, b3) scaled by alpha: m = K_TPA exp(alpha z_theta).
+    alpha = 0 is exactly Teter-Payne-Allan, alpha = 1 the trained network."""
+    H = 64
+    p = np.array(params, dtype=np.float32)
+    o = 3 * H + H + H * H + H
+    p[o:o + H + 1] *= np.float32(alpha)
+    return p
+
+
+def davidson_h_applies(dz, cells, ecut: float, nbands, kind, params=None, tol: float = 1e-6) -> float:
+    """Mean H applications of the device Davidson solver (random start, to tol) over the cells."""
+    n = []
+    for c in cells:
+        inp = sysm.kpoint_inputs(c, ecut, (0.0, 0.0, 0.0))
+        nb = int(nbands(c)) if callable(nbands) else int(nbands)
+        kc = _context(dz, inp)
+        kc.set_preconditioner(kind, params)
+        r = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, nb, dz.Options(max_iter=300, tol=tol))
+        n.append(r.h_applies if r.converged else 10 * r.h_applies)
+        kc.close()
+    return float(np.mean(n))
+
+
+def train_and_select(dz, samples, val_cells, ecut: float, nbands, steps: int, lr: float, chunks: int = 4,
+                     alphas=(0.25, 0.5, 0.75, 1.0)):
+    """The loss (1 - cos^2 against the projected correction) does not rank preconditioners by what
+    the solver needs, so the model is selected on the solver itself: the network is trained in
+    `chunks` segments of steps/chunks Adam steps, and every snapshot, with its output layer scaled by
+    each alpha, is scored by the mean H applications of Davidson solves on the validation cells.
+    Returns (params of the best snapshot and scale, loss history, selection table); the table holds
+    TPA (alpha = 0) for comparison, and the best entry can be TPA itself."""
+    p = init_params(0)
+    hist = []
+    tpa = davidson_h_applies(dz, val_cells, ecut, nbands, dz.PRECOND_TPA)
+    table = [{"steps": 0, "alpha": 0.0, "h_applies": tpa}]
+    best = (tpa, scale_output(p, 0.0), 0, 0.0)
+    per = max(1, steps // chunks)
+    for k in range(chunks):
+        p, h = dz.precond_mlp_train(p, samples["off"], samples["feat"], samples["cc"], samples["w"], samples["dnorm"], per, lr)
+        hist.append(h)
+        for a in alphas:
+            q = scale_output(p, a)
+            ha = davidson_h_applies(dz, val_cells, ecut, nbands, dz.PRECOND_MLP, q)
+            table.append({"steps": per * (k + 1), "alpha": a, "h_applies": ha})
+            if ha < best[0]:
+                best = (ha, q, per * (k + 1), a)
+    return best[1], np.concatenate(hist), {"table": table, "chosen": {"steps": best[2], "alpha": best[3], "h_applies": best[0]},
+                                           "tpa_h_applies": tpa}
+
+
 def eval_loss(dz, params, samples) -> float:
     return dz.precond_mlp_loss_grad(params, samples["off"], samples["feat"], samples["cc"], samples["w"], samples["dnorm"])[0]
 
@@ -344,7 +395,9 @@ def main(argv=None):
         kw = dict(t_list=(1, 2, 4, 7, 11, 16), bands_per_t=12)
         tr = precond_samples(dz, train_cells, a.ecut, nb, seed=1, **kw)
         ev = precond_samples(dz, eval_cells, a.ecut, nb, seed=2, **kw)
-        dav_cells, dav_nb = eval_cells[: min(6, len(eval_cells))], nb
+        # selection on six validation cells, the Davidson comparison on the other held-out cells
+        val_cells = eval_cells[: min(6, len(eval_cells))]
+        dav_cells, dav_nb = eval_cells[len(val_cells):] or val_cells, nb
     else:
         train_cells = [sysm.crystal("si8d", 1000 + i) for i in range(a.train_cells)]
         eval_cells = [sysm.crystal("si8d", 1200 + i) for i in range(a.eval_cells)]
@@ -352,7 +405,11 @@ def main(argv=None):
         ev = precond_samples(dz, eval_cells, a.ecut, a.nbands)
         dav_cells, dav_nb = eval_cells, a.nbands
     t1 = time.perf_counter()
-    p, hist = train_precond(dz, tr, a.steps, a.lr)
+    selection = None
+    if a.cells == "sitrain":
+        p, hist, selection = train_and_select(dz, tr, val_cells, a.ecut, nb, a.steps, a.lr)
+    else:
+        p, hist = train_precond(dz, tr, a.steps, a.lr)
     t2 = time.perf_counter()
     report = {
         "cells": a.cells,
@@ -370,6 +427,8 @@ def main(argv=None):
         "heldout_loss_tpa": fixed_loss(ev, "tpa"),
         "heldout_davidson": evaluate_precond(dz, dav_cells, a.ecut, dav_nb, p),
     }
+    if selection is not None:
+        report["selection"] = selection
     if a.cells == "sitrain":
         report["si216"] = evaluate_si216(dz, p)
     os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
