@@ -78,6 +78,8 @@ ABI_SYMBOLS = (
     "dftcuda_local_forces",
     "dftcuda_nonlocal_forces",
     "dftcuda_radial_table",
+    "dftcuda_plane_wave_basis",
+    "dftcuda_projector_phi",
     "dftcuda_symmetrize_density",
 )
 
@@ -251,6 +253,8 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.dftcuda_local_forces.argtypes = [vp, ip, vp, ip, vp, vp, ct.c_double, dp, dp]
     lib.dftcuda_nonlocal_forces.argtypes = [vp, dp, sz, sz, dp, dp]
     lib.dftcuda_radial_table.argtypes = [ip, sz, dp, dp, dp, sz, ct.c_double, dp]
+    lib.dftcuda_plane_wave_basis.argtypes = [dp, ct.c_double, dp, sz, vp, dp, dp, dp, ct.POINTER(ct.c_size_t)]
+    lib.dftcuda_projector_phi.argtypes = [ip, sz, ct.c_double, dp, sz, dp, dp]
     lib.dftcuda_symmetrize_density.argtypes = [vp, ip, vp, vp, vp]
     lb = ct.c_long
     lib.dftcuda_complex_gemm.argtypes = [ip, sz, sz, sz, vp, lb, ip, ip, vp, lb, ip, ip, vp, lb, lb, ct.c_double, ct.c_double]
@@ -858,6 +862,38 @@ def radial_table(l: int, r, rbeta, rab, gmax: float, npts: int = 2048):
     out = np.empty(int(npts))
     _check(lib.dftcuda_radial_table(int(l), r.size, r.ctypes.data, rbeta.ctypes.data, rab.ctypes.data, out.size, float(gmax), out.ctypes.data))
     return out, float(gmax), float(gmax) / (npts - 1)
+
+
+def plane_wave_basis(recip, ecut: float, k_cart):
+    """The plane-wave basis of one k-point built on the device (dftcuda_plane_wave_basis): returns
+    (hkl int32 [n][3], gcart [n][3], kpg [n][3], kinetic [n]) in the reference's order."""
+    lib = load_library()
+    _require_device()
+    recip = np.ascontiguousarray(recip, dtype=np.float64).reshape(9)
+    k = np.ascontiguousarray(k_cart, dtype=np.float64).reshape(3)
+    n = ct.c_size_t(0)
+    _check(lib.dftcuda_plane_wave_basis(recip.ctypes.data, float(ecut), k.ctypes.data, 0, None, None, None, None, ct.byref(n)))
+    m = int(n.value)
+    hkl = np.empty((m, 3), dtype=np.int32)
+    g = np.empty((m, 3))
+    q = np.empty((m, 3))
+    kin = np.empty(m)
+    _check(lib.dftcuda_plane_wave_basis(recip.ctypes.data, float(ecut), k.ctypes.data, max(m, 1), hkl.ctypes.data, g.ctypes.data,
+                                        q.ctypes.data, kin.ctypes.data, ct.byref(n)))
+    return hkl, g, q, kin
+
+
+def projector_phi(l: int, table, kpg):
+    """Projector rows phi[(2l+1)][n] = 4 pi R(|k+G|) Y_lm(k+G) on the device (dftcuda_projector_phi);
+    table = (values, gmax, dq) as radial_table returns."""
+    lib = load_library()
+    _require_device()
+    vals, gmax, _ = table
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    kpg = np.ascontiguousarray(kpg, dtype=np.float64).reshape(-1, 3)
+    out = np.empty((2 * int(l) + 1, kpg.shape[0]))
+    _check(lib.dftcuda_projector_phi(int(l), vals.size, float(gmax), vals.ctypes.data, kpg.shape[0], kpg.ctypes.data, out.ctypes.data))
+    return out
 
 
 def complex_gemm(a, b, out=None, *, conj_a: bool = False, conj_b: bool = False, precision: int = 0, alpha: float = 1.0,

@@ -404,6 +404,11 @@ class ScfParams:
     energy_target: Optional[float] = None
     initial_density: Optional[np.ndarray] = None  # rho(r) on the FFT grid; None = flat N_e / Omega
     kpoints: Optional[list] = None  # explicit [(k_frac, weight)] in place of the kmesh (weights sum to 1)
+    # model dielectric preconditioner of the Pulay residual (apply_model_dielectric_preconditioner,
+    # scf/mixing.zig:319-337; off at diemac = 1, the reference default; its config validation
+    # suggests ~12 for semiconductors at tight convergence)
+    diemac: float = 1.0
+    dielng: float = 1.0
 
 
 @dataclass
@@ -492,6 +497,11 @@ class ScfState:
         if not self.dev:  # the host potential path's G-vector table
             self.g2 = g_vectors(dims, c.recip)
             self.gmask = self.g2 > 1e-12
+        self.dielec = None
+        if p.diemac > 1.0:
+            g2 = self.g2 if not self.dev else g_vectors(dims, c.recip)
+            x = p.dielng * p.dielng * g2
+            self.dielec = np.where(g2 < 1e-12, 1.0 / p.diemac, (x + 1.0 / p.diemac) / (x + 1.0))
         self.nelec = c.nelec
         self.nocc = int(math.ceil(self.nelec / 2.0 - 1e-12))
         self.nbands = max(p.nbands, self.nocc)
@@ -636,6 +646,10 @@ class ScfState:
 
             resid = v_out_d - self.v_hxc
             if self.it >= p.pulay_start:
+                if self.dielec is not None:
+                    if not torch.is_tensor(self.dielec):
+                        self.dielec = torch.from_numpy(self.dielec).to(resid.device)
+                    resid = resid * self.dielec
                 x = torch.view_as_real(self.v_hxc).reshape(-1).clone()
                 self.pot.pulay_mix(x, torch.view_as_real(resid).reshape(-1).contiguous(), p.mixing_beta)
                 self.v_hxc = torch.view_as_complex(x.view(-1, 2))
@@ -644,6 +658,8 @@ class ScfState:
         else:
             resid = self.hxc_g(rho_out) - self.v_hxc
             if self.it >= p.pulay_start:
+                if self.dielec is not None:
+                    resid = resid * self.dielec
                 flat = self.mixer.mix(np.concatenate([self.v_hxc.real, self.v_hxc.imag]), np.concatenate([resid.real, resid.imag]), p.mixing_beta)
                 self.v_hxc = flat[:N] + 1j * flat[N:]
             else:

@@ -417,6 +417,22 @@ int dftcuda_symmetrize_density(dftcuda_pctx* ctx, int nops, const int* k_rot, co
 int dftcuda_radial_table(int l, size_t nr, const double* r, const double* rbeta, const double* rab, size_t nq, double gmax,
                          double* out);
 
+/* Plane-wave basis of one k-point (plane_wave.generate, features/plane_wave/basis.zig:26-74): the
+ * Miller triples of the box [-n, n]^3, n = ceil(sqrt(ecut) / min |b_i|) + 1, in the reference's loop
+ * order (h outer, l inner), kept when |k + G|^2 <= ecut_ry; every value bit-identical to the
+ * reference's arithmetic.  recip: rows b1, b2, b3 (9 doubles, 1/bohr, 2 pi included); k_cart: 3
+ * doubles.  capacity == 0 is a size query (*n_out = basis size); otherwise hkl [n][3], gcart [n][3],
+ * kpg [n][3] and kinetic [n] receive the basis (host or device arrays; InvalidMatrixSize when
+ * capacity < size). */
+int dftcuda_plane_wave_basis(const double* recip, double ecut_ry, const double* k_cart, size_t capacity, int32_t* hkl,
+                             double* gcart, double* kpg, double* kinetic, size_t* n_out);
+
+/* Projector table rows of one radial projector (fill_nonlocal_phi, scf/nonlocal_context.zig:524-549):
+ * phi[m + l][i] = 4 pi R(|kpg_i|) Y_lm(kpg_i), m = -l..l, R by RadialTable.eval on the uniform table
+ * (nq values over [0, gmax], pseudopotential/nonlocal.zig:250-300), Y_lm the real harmonics of
+ * nonlocal.zig:152-241 (l <= 4).  kpg: [n][3]; phi: [(2l+1)][n].  Host or device pointers. */
+int dftcuda_projector_phi(int l, size_t nq, double gmax, const double* table, size_t n, const double* kpg, double* phi);
+
 /* ------------------------------------------------------------------------------------------
  * The library's complex GEMM (no counterpart in the reference; the contraction its projector and
  * Rayleigh-Ritz code paths run), exposed for tests and benchmarks:

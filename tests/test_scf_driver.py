@@ -98,3 +98,15 @@ def test_scf_converges_with_oracle_backend():
     assert math.isfinite(r.energy) and -9.0 < r.energy_per_atom < -7.0
     g = r.eigenvalues[0]
     assert abs(g[1] - g[3]) < 1e-6 and g[4] - g[3] > 0.02  # occupied triplet, gap above it
+
+
+def test_model_dielectric_preconditioner_keeps_the_fixed_point():
+    """The Pulay residual scaled by P(G) = (l^2 G^2 + 1/eps) / (l^2 G^2 + 1) (the reference's
+    apply_model_dielectric_preconditioner, mixing.zig:319-337) changes the path, not the answer: Si2
+    with diemac = 12 converges to the energy of the plain run."""
+    c = system.crystal("si2")
+    base = dict(ecut=8.0, kmesh=(2, 2, 2), nbands=8, convergence=1e-9, iterative_max_iter=100, iterative_tol=1e-10, warmup_steps=0)
+    plain = scf.run_scf(c, scf.ScfParams(**base), OracleBackend())
+    diel = scf.run_scf(c, scf.ScfParams(**base, diemac=12.0, dielng=1.0), OracleBackend())
+    assert plain.converged and diel.converged
+    assert abs(plain.energy_per_atom - diel.energy_per_atom) < 1e-8
