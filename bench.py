@@ -122,14 +122,18 @@ def parse():
     ap.add_argument("--no-variants", action="store_true", help="skip the FP32 / TF32 variants of the H|psi> step")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile-case", action="store_true", help="small single-k case for ncu captures: Gamma, 32 columns, 2 applications")
-    ap.add_argument("--workload", choices=("hpsi", "scf", "scf64", "scf216", "al4", "cells", "eig", "heev", "gemm"), default="hpsi",
+    ap.add_argument("--workload", choices=("hpsi", "scf", "scf64", "scf216", "al4", "cells", "eig", "heev", "gemm", "potential"),
+                    default="hpsi",
                     help="hpsi: H|psi> GB/s (default); scf: time-to-SCF Si2; scf64: time-to-SCF Si64, mixed vs FP64; "
                          "scf216: time-to-SCF Si216 (Gamma, 448 bands), FP64 vs learned+mixed; "
                          "al4: time-to-SCF Al4 8x8x8 (260 k-points, batched), FP64 vs mixed; "
                          "cells: many-cell SiGe8 SCF throughput, atomic vs learned start; "
                          "eig: one Si64 Gamma Davidson solve (profiling case); "
                          "heev: the subspace eigensolver on a seeded Hermitian matrix (--heev-m, lowest m/3 pairs); "
-                         "gemm: the library's complex GEMM on the Si216 Davidson shapes (--gemm-shapes), FP64 / 3xTF32 / TF32")
+                         "gemm: the library's complex GEMM on the Si216 Davidson shapes (--gemm-shapes), FP64 / 3xTF32 / TF32; "
+                         "potential: the Si216 box's potential build, Pulay step and standalone 3D FFTs")
+    ap.add_argument("--eig-precond", choices=("reference", "tpa", "mlp"), default="reference",
+                    help="preconditioner of --workload eig (mlp: the shipped trained weights)")
     ap.add_argument("--gemm-shapes", default="gram1344,t448x1344,rot448,proj864",
                     help="comma list of --workload gemm shapes: " + ", ".join(f"{k} ({v[4]})" for k, v in GEMM_SHAPES.items()))
     ap.add_argument("--gemm-precisions", default="fp64,tf32x3,tf32", help="comma list of --workload gemm precisions")
@@ -600,9 +604,9 @@ def time_to_scf_si216(dz, args, device_index: int):
 
 
 def run_profile_case(precision: str = "fp64", cell: str = "si64"):
-    """One k-point (Gamma) of a benchmark cell, a few columns, H|psi> twice: a small case for ncu
-    captures of single kernels (Si64: 32 columns, a few hundred MB on the device; Si216: 16 columns,
-    under 1 GB)."""
+    """One k-point (Gamma) of a benchmark cell, a few columns, H|psi> twice and one band-density
+    accumulation of the same columns: a small case for ncu captures of single kernels (Si64: 32
+    columns, a few hundred MB on the device; Si216: 16 columns, under 1 GB)."""
     import torch
 
     import dftzig_loader
@@ -626,6 +630,9 @@ def run_profile_case(precision: str = "fp64", cell: str = "si64"):
     torch.cuda.synchronize()
     for _ in range(2):
         kc.apply_hamiltonian_async(x, y, ncols, s.cuda_stream)
+    torch.cuda.synchronize()
+    rho = torch.zeros(dims[0] * dims[1] * dims[2], dtype=torch.float64, device="cuda")
+    kc.accumulate_band_density(x, np.full(ncols, 2.0), rho)
     torch.cuda.synchronize()
     kc.close()
     print("profile case done", flush=True)
@@ -928,6 +935,10 @@ def run_eig_workload(args):
     kc = dz.KpointContext(*inp.dims, inp.volume, inp.basis.hkl, inp.basis.kinetic, inp.basis.gcart, prec)
     kc.set_vloc(inp.local_r)
     kc.set_projectors([dz.SpeciesProjectors(l, d, p) for (l, d, p) in inp.species_phi], inp.atom_species, inp.positions)
+    if args.eig_precond == "tpa":
+        kc.set_preconditioner(dz.PRECOND_TPA)
+    elif args.eig_precond == "mlp":
+        kc.set_preconditioner(dz.PRECOND_MLP, importlib.import_module("dftzig_b200.learn").load_precond_weights())
     kc.set_profiling(True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -939,6 +950,63 @@ def run_eig_workload(args):
     print(json.dumps({"metric": f"Davidson solve wall time, {cell} Gamma {ecut:g} Ry {nb} bands ({args.precision})", "value": round(wall * 1e3, 2), "unit": "ms",
                       "iterations": r.iterations, "h_applies": r.h_applies, "apply_h_ms": round(pr["apply_h_ns"] / 1e6, 2),
                       "subspace_ms": round(pr["subspace_ns"] / 1e6, 2)}), flush=True)
+
+
+def run_potential_workload(args):
+    """The SCF potential kernels on the Si216 box (108^3, 1,259,712 points): the Hartree + LDA-PZ
+    build from a seeded density (dftcuda_hxc_potential), V(r) = V_loc + FFT^-1 V(G)
+    (dftcuda_potential_real), one Pulay step on the complex V(G) with a full 8-deep history
+    (dftcuda_pulay_mix), and the standalone forward + inverse 3D FFT (dftcuda_fft3d).  Device-resident
+    torch tensors; CUDA-event time of each call after warm-up, median of five.  Bytes per call are
+    the arrays each call must read and write once (N points: density 8 B, V(G) 16 B, V(r) 8 B)."""
+    import importlib
+
+    import torch
+
+    import dftzig_loader
+
+    dz = dftzig_loader.load()
+    system = importlib.import_module("dftzig_b200.system")
+    c = system.crystal("si216", 3)
+    dims = system.fft_box(25.0, c.recip)
+    N = dims[0] * dims[1] * dims[2]
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    rho = (c.nelec / c.volume) * (1.0 + 0.1 * torch.rand(N, dtype=torch.float64, device="cuda", generator=gen))
+    vloc = torch.randn(N, dtype=torch.float64, device="cuda", generator=gen)
+    pot = dz.PotentialContext(dims, c.volume, c.recip, history=8, functional="lda")
+    plan = dz.Fft3dPlan(*dims)
+    vg, _ = pot.hxc(rho)
+    x = torch.view_as_real(vg).reshape(-1).clone()
+    for _ in range(8):  # fill the history
+        pot.pulay_mix(x, 1e-3 * torch.randn(2 * N, dtype=torch.float64, device="cuda", generator=gen), 0.3)
+    box = torch.randn(N, dtype=torch.complex128, device="cuda", generator=gen)
+    resid = 1e-3 * torch.randn(2 * N, dtype=torch.float64, device="cuda", generator=gen)
+
+    def timed(fn):
+        fn()
+        ts = []
+        for _ in range(5):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return float(np.median(ts))
+
+    rows = {}
+    for name, fn, nbytes in (
+            ("hxc_lda", lambda: pot.hxc(rho, v_in=vg, out=vg), N * (8 + 16 + 16)),
+            ("potential_real", lambda: pot.real(vg, vloc=vloc), N * (16 + 8 + 8)),
+            ("pulay_mix_h8", lambda: pot.pulay_mix(x, resid, 0.3), N * 16 * (2 * 8 + 3)),
+            ("fft3d_fwd_inv", lambda: (plan.forward(box), plan.inverse(box)), N * 16 * 4)):
+        ms = timed(fn)
+        rows[name] = {"ms": round(ms, 4), "bytes": int(nbytes), "gbs": round(nbytes / (ms * 1e-3) / 1e9, 1)}
+    pot.close()
+    plan.close()
+    print(json.dumps({"workload": f"Si216 box {dims[0]}x{dims[1]}x{dims[2]}, potential kernels", "calls": rows}), flush=True)
 
 
 def run_heev_workload(args):
@@ -1014,6 +1082,8 @@ def main():
     args = parse()
     if args.workload == "gemm":
         return run_gemm_workload(args)
+    if args.workload == "potential":
+        return run_potential_workload(args)
     if args.workload == "heev":
         run_heev_workload(args)
         return

@@ -47,17 +47,6 @@ template <typename T> __device__ __forceinline__ cplx<T> twl(const cplx<T>* tw, 
   return w;
 }
 
-// Asynchronous copy of one V(r) value (8 or 4 bytes, naturally aligned) from global into shared
-// memory; the copies of a lane complete at cp_async_wait_all(), and a __syncwarp() after it makes
-// them visible to the warp.
-template <typename T> __device__ __forceinline__ void cp_async_value(T* sdst, const T* gsrc) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
-  if (sizeof(T) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gsrc) : "memory");
-  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
 // ------------------------------------------------------------------------------------------
 // Pass 1: gather + inverse z transform per stick.
 // ------------------------------------------------------------------------------------------
@@ -207,13 +196,9 @@ __global__ void __launch_bounds__(plane_max_warps<T>() * 32, 1) k_zplane(cplx<T>
   constexpr int N1 = G::N1, N2 = G::N2, LW = G::LW, QR = G::Q, SX = G::S;
   constexpr int QS = N + 1;  // Q row stride: odd, so lanes over slots hit distinct banks
   extern __shared__ __align__(16) unsigned char smraw[];
-  // shared memory: Q [n_act][QS] | twiddles [N] | exchange [nwarp][LW][SX] | V rows [nwarp][LW][N] | slots [N]
+  C* Q = reinterpret_cast<C*>(smraw);  // [n_act][QS]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  C* Q = reinterpret_cast<C*>(smraw);
-  C* tws = Q + (size_t)n_act * QS;
-  C* Bw = tws + N + (size_t)warp * LW * SX;  // this warp's exchange buffer [LW][SX]
-  T* Vw = reinterpret_cast<T*>(tws + N + (size_t)nwarp * LW * SX) + (size_t)warp * LW * N;  // this warp's V rows [LW][N]
-  int* sox = reinterpret_cast<int*>(reinterpret_cast<T*>(tws + N + (size_t)nwarp * LW * SX) + (size_t)nwarp * LW * N);
+  C* Bw = Q + (size_t)n_act * QS + (size_t)warp * LW * SX;  // this warp's exchange buffer [LW][SX]
   const int z = blockIdx.x;
   const int r = (z % n1z) * n2z + z / n1z;  // storage row of z in S
   const int c0 = blockIdx.y * cols_per_cta;
@@ -223,11 +208,6 @@ __global__ void __launch_bounds__(plane_max_warps<T>() * 32, 1) k_zplane(cplx<T>
   const int L = lane / N2, t = lane - L * N2;
   const bool lane_ok = L < LW;
   C* B = Bw + (lane_ok ? L : 0) * SX;
-  const T* Vl = Vw + (lane_ok ? L : 0) * N;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    tws[i] = tw[i];
-    sox[i] = __ldg(slot_of_x + i);
-  }
   for (int c = c0; c < c1; ++c) {
     C* Srow = S + ((long)c * gridDim.x + r) * n_st;
     __syncthreads();  // the previous column's gather has read Q
@@ -248,7 +228,7 @@ __global__ void __launch_bounds__(plane_max_warps<T>() * 32, 1) k_zplane(cplx<T>
       RegDft<T, N1>::run(v, (T)1);
 #pragma unroll
       for (int k1 = 1; k1 < N1; ++k1)
-        if (tt) v[k1] = cmul(v[k1], twl<T>(tws, (tt * k1) % N, (T)1));
+        if (tt) v[k1] = cmul(v[k1], twl<T>(tw, (tt * k1) % N, (T)1));
 #pragma unroll
       for (int k1 = 0; k1 < N1; ++k1) q[k1 * N2 + tt] = v[k1];
     }
@@ -270,23 +250,17 @@ __global__ void __launch_bounds__(plane_max_warps<T>() * 32, 1) k_zplane(cplx<T>
       const int yl = lt * LW + L;
       const bool lv = lane_ok && yl < N;
       const int col = lv ? (yl % N1) * N2 + yl / N1 : 0;
-      // the V(r) rows of this warp's lines, in flight while the inverse transform runs
-      for (int i = lane; i < LW * N; i += 32) {
-        const int li = i / N, yi = lt * LW + li;
-        if (yi < N) cp_async_value<T>(Vw + i, Vz + (long)yi * N + (i - li * N));
-      }
-      cp_async_commit();
       {  // inverse step A over x = t + N2 m
         C v[N1];
 #pragma unroll
         for (int m = 0; m < N1; ++m) {
-          const int sm = lv ? sox[t + N2 * m] : -1;
+          const int sm = lv ? __ldg(slot_of_x + t + N2 * m) : -1;
           v[m] = sm >= 0 ? Q[sm * QS + col] : mk<C>(0.0, 0.0);
         }
         RegDft<T, N1>::run(v, (T)1);
 #pragma unroll
         for (int k1 = 1; k1 < N1; ++k1)
-          if (t) v[k1] = cmul(v[k1], twl<T>(tws, (t * k1) % N, (T)1));
+          if (t) v[k1] = cmul(v[k1], twl<T>(tw, (t * k1) % N, (T)1));
         if (lane_ok) {
 #pragma unroll
           for (int k1 = 0; k1 < N1; ++k1) B[k1 * N2 + t] = v[k1];
@@ -302,7 +276,6 @@ __global__ void __launch_bounds__(plane_max_warps<T>() * 32, 1) k_zplane(cplx<T>
           for (int j = 0; j < N2; ++j) u[q][j] = B[k1 * N2 + j];
         }
       }
-      cp_async_wait_all();
       __syncwarp();
 #pragma unroll
       for (int q = 0; q < QR; ++q) {  // inverse step B, x V(r), forward step A (split swapped)
@@ -310,11 +283,11 @@ __global__ void __launch_bounds__(plane_max_warps<T>() * 32, 1) k_zplane(cplx<T>
         if (lane_ok && k1 < N1) {
           RegDft<T, N2>::run(u[q], (T)1);
 #pragma unroll
-          for (int k2 = 0; k2 < N2; ++k2) u[q][k2] = cscale(u[q][k2], lv ? Vl[k1 + N1 * k2] : (T)0);
+          for (int k2 = 0; k2 < N2; ++k2) u[q][k2] = cscale(u[q][k2], lv ? __ldg(Vz + (long)yl * N + k1 + N1 * k2) : (T)0);
           RegDft<T, N2>::run(u[q], (T)-1);
 #pragma unroll
           for (int kf = 1; kf < N2; ++kf)
-            if (k1) u[q][kf] = cmul(u[q][kf], twl<T>(tws, (k1 * kf) % N, (T)-1));
+            if (k1) u[q][kf] = cmul(u[q][kf], twl<T>(tw, (k1 * kf) % N, (T)-1));
 #pragma unroll
           for (int kf = 0; kf < N2; ++kf) B[kf * N1 + k1] = u[q][kf];
         }
@@ -327,7 +300,7 @@ __global__ void __launch_bounds__(plane_max_warps<T>() * 32, 1) k_zplane(cplx<T>
         RegDft<T, N1>::run(v, (T)-1);
 #pragma unroll
         for (int m = 0; m < N1; ++m) {
-          const int sm = lv ? sox[t + N2 * m] : -1;
+          const int sm = lv ? __ldg(slot_of_x + t + N2 * m) : -1;
           if (sm >= 0) Q[sm * QS + col] = v[m];
         }
       }
@@ -344,7 +317,7 @@ __global__ void __launch_bounds__(plane_max_warps<T>() * 32, 1) k_zplane(cplx<T>
       RegDft<T, N2>::run(v, (T)-1);
 #pragma unroll
       for (int k = 1; k < N2; ++k)
-        if (tt) v[k] = cmul(v[k], twl<T>(tws, (tt * k) % N, (T)-1));
+        if (tt) v[k] = cmul(v[k], twl<T>(tw, (tt * k) % N, (T)-1));
 #pragma unroll
       for (int k = 0; k < N2; ++k) q[k] = v[k];
     }
@@ -492,17 +465,10 @@ static constexpr int kSmemSticks = 227 * 1024;
 
 static size_t stick_smem(size_t cs, int nz) { return cs * (size_t)nz * kStickPad; }
 
-// Shared memory of the z-plane pass: Q and the twiddle and slot tables, then per warp the exchange
-// buffer and the staged V(r) rows of its lines.
-template <int N> static size_t plane_fixed_smem(size_t cs, int n_act) { return cs * ((size_t)n_act * (N + 1) + N) + sizeof(int) * N; }
-template <int N> static size_t plane_warp_smem(size_t cs) {
-  using G = PlaneXGeom<N>;
-  return cs * (size_t)G::LW * G::S + (cs / 2) * (size_t)G::LW * N;
-}
-
 template <int N> static int plane_warps(size_t cs, int n_act) {
-  const size_t q = plane_fixed_smem<N>(cs, n_act);
-  const size_t per_warp = plane_warp_smem<N>(cs);
+  using G = PlaneXGeom<N>;
+  const size_t q = cs * (size_t)n_act * (N + 1);
+  const size_t per_warp = cs * (size_t)G::LW * G::S;
   const int maxw = cs == sizeof(double2) ? plane_max_warps<double>() : plane_max_warps<float>();
   if (q + per_warp > (size_t)kSmemSticks) return 0;
   return (int)std::min<size_t>(maxw, ((size_t)kSmemSticks - q) / per_warp);
@@ -564,7 +530,7 @@ static int launch_zplane(dftcuda_kctx* c, cplx<T>* S, size_t ncols, cudaStream_t
   const size_t cs = sizeof(cplx<T>);
   const int nw = plane_warps<N>(cs, c->n_act);
   if (nw < 1) return fail(DFTCUDA_ERR_UNSUPPORTED, "z-plane pass does not fit shared memory");
-  const size_t smem = plane_fixed_smem<N>(cs, c->n_act) + (size_t)nw * plane_warp_smem<N>(cs);
+  const size_t smem = cs * ((size_t)c->n_act * (N + 1) + (size_t)nw * G::LW * G::S);
   DFT_TRY(ensure_max_dynamic_smem((const void*)k_zplane<T, N>, (int)smem));
   const T* vn = std::is_same<T, double>::value ? (const T*)c->d_vn : (const T*)c->d_vn32;
   const cplx<T>* tw = std::is_same<T, double>::value ? (const cplx<T>*)c->d_twx64 : (const cplx<T>*)c->d_twx32;

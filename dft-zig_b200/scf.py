@@ -489,7 +489,11 @@ class ScfState:
                 raise ValueError("ScfParams.xc = 'pbe' needs the resident driver (GpuBackend(resident=True))")
             self.vloc_r = sysm.local_potential(c, dims, p.ecut)
         tm["local_potential"], t = time.perf_counter() - t, time.perf_counter()
-        self.kin = [sysm.kpoint_inputs(c, p.ecut, kpts[k][0], dims=dims, local_r=self.vloc_r, tables=tables) for k in self.kglobal]
+        if self.dev:  # basis and projector rows on the device too (dftcuda_plane_wave_basis, dftcuda_projector_phi)
+            self.kin = [sysm.kpoint_inputs_device(backend.dz, c, p.ecut, kpts[k][0], dims=dims, local_r=self.vloc_r, tables=tables)
+                        for k in self.kglobal]
+        else:
+            self.kin = [sysm.kpoint_inputs(c, p.ecut, kpts[k][0], dims=dims, local_r=self.vloc_r, tables=tables) for k in self.kglobal]
         self.kweights = [w for _, w in kpts]
         tm["kpoint_inputs"], t = time.perf_counter() - t, time.perf_counter()
         backend.setup(self.kin)

@@ -416,6 +416,24 @@ def kpoint_inputs(c: Crystal, ecut: float, k_frac, dims=None, local_r=None, tabl
     return KpointInputs(dims, c.volume, b, local_r, sph, c.atom_species, c.positions)
 
 
+def kpoint_inputs_device(dz, c: Crystal, ecut: float, k_frac, dims=None, local_r=None, tables=None) -> KpointInputs:
+    """kpoint_inputs with the basis (dftcuda_plane_wave_basis, the reference's order and arithmetic)
+    and the projector rows 4 pi R(|k+G|) Y_lm (dftcuda_projector_phi) built on the device; tables:
+    per species, per beta, (values, gmax, dq) radial tables."""
+    dims = dims or fft_box(ecut, c.recip)
+    hkl, g, q, kin = dz.plane_wave_basis(c.recip, ecut, np.asarray(k_frac, float) @ c.recip)
+    b = PwBasis(hkl, g, q, kin)
+    if tables is None:
+        tables = [[radial_table(sp, i, ecut) for i in range(len(sp.betas))] for sp in c.species]
+    sph = []
+    for s, sp in enumerate(c.species):
+        rows = [dz.projector_phi(l, tables[s][i], q) for i, (l, _) in enumerate(sp.betas)]
+        sph.append(([l for l, _ in sp.betas], sp.dij, np.concatenate(rows, axis=0) if rows else np.zeros((0, len(kin)))))
+    if local_r is None:
+        local_r = local_potential(c, dims, ecut)
+    return KpointInputs(dims, c.volume, b, local_r, sph, c.atom_species, c.positions)
+
+
 def monkhorst_pack(mesh):
     """Gamma-centred MP mesh, k and -k folded (time reversal).  [(k_frac, weight)]."""
     n1, n2, n3 = mesh

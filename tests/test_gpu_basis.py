@@ -67,3 +67,20 @@ def test_projector_phi_matches_oracle(dz, l):
     ref = np.array([4.0 * math.pi * tab.eval(gm) * pseudo.real_ylm(l, m, q[:, 0], q[:, 1], q[:, 2]) for m in range(-l, l + 1)])
     assert phi.shape == ref.shape
     assert np.abs(phi - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_device_kpoint_inputs_match_host(dz):
+    """The resident driver's per-k inputs (basis and projector rows from the device) equal the host
+    builder's: identical basis, projector rows to 1e-13."""
+    import importlib
+
+    system = importlib.import_module("dftzig_b200.system")
+    c = system.crystal("si8", 1)
+    tables = [[system.radial_table(sp, i, 20.0) for i in range(len(sp.betas))] for sp in c.species]
+    k = (0.25, 0.0, 0.125)
+    a = system.kpoint_inputs(c, 20.0, k, tables=tables)
+    b = system.kpoint_inputs_device(dz, c, 20.0, k, local_r=a.local_r, tables=tables)
+    assert np.array_equal(a.basis.hkl, b.basis.hkl) and np.array_equal(a.basis.kinetic, b.basis.kinetic)
+    for (la, da, pa), (lb, db, pb) in zip(a.species_phi, b.species_phi):
+        assert la == lb and np.array_equal(da, db)
+        assert np.abs(pa - pb).max() <= 1e-13 * np.abs(pa).max()
