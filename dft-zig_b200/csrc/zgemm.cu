@@ -1,8 +1,9 @@
 // FP64 complex GEMM over strided operands, used for the Kleinman-Bylander projections
 // (apply.zig:1143-1183, 1278-1336) and the Rayleigh-Ritz contractions V^H W and V C
 // (lobpcg/common.zig:113-143, 231-259).  B200 has no FP64 tcgen05 kind, so the FP64 path runs on
-// the FP64 tensor cores through mma.sync m8n8k4 .f64 (k_zgemm_dmma, the default) or on the FP64
-// FMA pipe (k_zgemm, DFTCUDA_ZGEMM=fma): 64x64 output tiles per 256-thread CTA, K staged through
+// the FP64 tensor cores through mma.sync m16n8k8 .f64 (k_zgemm_dmma16, the default) or m8n8k4 .f64
+// (k_zgemm_dmma, DFTCUDA_ZGEMM=dmma8), or on the FP64 FMA pipe (k_zgemm, DFTCUDA_ZGEMM=fma):
+// 64x64 output tiles per 256-thread CTA, K staged through
 // shared memory in slices of 16 with cp.async double buffering, and split-K with a deterministic
 // second-pass reduction when the output has too few tiles to fill the 148 SMs.
 #include <algorithm>
@@ -224,6 +225,89 @@ __global__ void __launch_bounds__(256, 2) k_zgemm_dmma(int M, int N, int K, cons
       }
 }
 
+// The same tiling on the m16n8k8 FP64 MMA (one instruction = 1,024 FMAs, four times the m8n8k4's,
+// for the same operands).  Fragments of mma.m16n8k8.row.col.f64, lane = 4 g + t:
+//   A (16 x 8): a0 = A[g][t], a1 = A[g + 8][t], a2 = A[g][t + 4], a3 = A[g + 8][t + 4];
+//   B (8 x 8):  b0 = B[t][g], b1 = B[t + 4][g];
+//   C (16 x 8): c0 = C[g][2t], c1 = C[g][2t + 1], c2 = C[g + 8][2t], c3 = C[g + 8][2t + 1].
+// Each warp owns 16 x 32 outputs (four 16 x 8 tiles); a complex product is four real MMAs.
+__device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[4], double b0, double b1) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+               : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b0), "d"(b1));
+}
+
+template <bool AKC, bool BKC, bool CJA, bool CJB>
+__global__ void __launch_bounds__(256, 2) k_zgemm_dmma16(int M, int N, int K, const double2* __restrict__ A, long lda,
+                                                         const double2* __restrict__ B, long ldb, double2* __restrict__ O,
+                                                         long ldo_r, long ldo_c, double alpha, double beta, int kps,
+                                                         double2* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char zsm[];
+  double2(*As)[BK][BM + kZmPad] = reinterpret_cast<double2(*)[BK][BM + kZmPad]>(zsm);
+  double2(*Bs)[BK][BN + kZmPad] = reinterpret_cast<double2(*)[BK][BN + kZmPad]>(zsm + 2 * sizeof(double2) * BK * (BM + kZmPad));
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wr = warp >> 1, wc = warp & 1;  // warp block: rows 16 wr .., columns 32 wc ..
+  const int r0 = blockIdx.y * BM, c0 = blockIdx.x * BN;
+  const int kbeg = blockIdx.z * kps;
+  const int kend = min(K, kbeg + kps);
+  const double sa = CJA ? -1.0 : 1.0, sb = CJB ? -1.0 : 1.0;
+  double cre[4][4], cim[4][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) cre[j][e] = cim[j][e] = 0.0;
+  if (kbeg < kend) zgemm_fetch<AKC, BKC, kZmPad>(As[0], Bs[0], M, N, kend, r0, c0, kbeg, A, lda, B, ldb, tid);
+  int buf = 0;
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
+    cp_async_wait_all();
+    __syncthreads();
+    if (k0 + BK < kend) zgemm_fetch<AKC, BKC, kZmPad>(As[buf ^ 1], Bs[buf ^ 1], M, N, kend, r0, c0, k0 + BK, A, lda, B, ldb, tid);
+#pragma unroll
+    for (int k8 = 0; k8 < BK; k8 += 8) {
+      double ar[4], ai[4], nai[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const double2 v = As[buf][k8 + t + 4 * (e >> 1)][wr * 16 + g + 8 * (e & 1)];
+        ar[e] = v.x;
+        ai[e] = sa * v.y;
+        nai[e] = -ai[e];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double2 u0 = Bs[buf][k8 + t][wc * 32 + j * 8 + g];
+        const double2 u1 = Bs[buf][k8 + t + 4][wc * 32 + j * 8 + g];
+        const double bi0 = sb * u0.y, bi1 = sb * u1.y;
+        dmma16(cre[j], ar, u0.x, u1.x);
+        dmma16(cre[j], nai, bi0, bi1);
+        dmma16(cim[j], ar, bi0, bi1);
+        dmma16(cim[j], ai, u0.x, u1.x);
+      }
+    }
+    buf ^= 1;
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int r = r0 + wr * 16 + g + 8 * (e >> 1), c = c0 + wc * 32 + j * 8 + 2 * t + (e & 1);
+      if (r >= M || c >= N) continue;
+      const double2 acc = make_double2(cre[j][e], cim[j][e]);
+      if (part) {
+        part[((long)blockIdx.z * M + r) * N + c] = acc;
+      } else {
+        double2* o = O + (long)r * ldo_r + (long)c * ldo_c;
+        double2 v = make_double2(alpha * acc.x, alpha * acc.y);
+        if (beta != 0.0) {
+          const double2 old = *o;
+          v.x += beta * old.x;
+          v.y += beta * old.y;
+        }
+        *o = v;
+      }
+    }
+}
+
 __global__ void k_zgemm_reduce(int M, int N, int splits, const double2* __restrict__ part, double2* __restrict__ O,
                                long ldo_r, long ldo_c, double alpha, double beta) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -270,18 +354,28 @@ size_t zgemm_workspace_elems(int M, int N, int K) {
   return s > 1 ? (size_t)s * M * N : 0;
 }
 
-// DFTCUDA_ZGEMM=fma selects the FMA-pipe kernel (A/B measurements); the FP64 tensor-core kernel is the default.
-static bool zgemm_fma() {
-  static const bool v = [] {
+// DFTCUDA_ZGEMM=fma selects the FMA-pipe kernel, =dmma8 the m8n8k4 tensor-core kernel (A/B
+// measurements); the m16n8k8 FP64 tensor-core kernel is the default.
+static int zgemm_kind() {
+  static const int v = [] {
     const char* e = std::getenv("DFTCUDA_ZGEMM");
-    return e && std::string(e) == "fma";
+    if (e && std::string(e) == "fma") return 0;
+    if (e && std::string(e) == "dmma8") return 1;
+    return 2;
   }();
   return v;
 }
 
 template <bool AKC, bool BKC, bool CJA, bool CJB>
 static void launch(const GemmArgs& g, dim3 grid, int kps, double2* part, cudaStream_t s) {
-  if (!zgemm_fma()) {
+  if (zgemm_kind() == 2) {
+    ensure_max_dynamic_smem((const void*)k_zgemm_dmma16<AKC, BKC, CJA, CJB>, (int)kZgemmDmmaSmem);
+    k_zgemm_dmma16<AKC, BKC, CJA, CJB><<<grid, 256, kZgemmDmmaSmem, s>>>(g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r,
+                                                                        g.ldo_c, g.alpha, g.beta, kps, part);
+    count_launch();
+    return;
+  }
+  if (zgemm_kind() == 1) {
     ensure_max_dynamic_smem((const void*)k_zgemm_dmma<AKC, BKC, CJA, CJB>, (int)kZgemmDmmaSmem);
     k_zgemm_dmma<AKC, BKC, CJA, CJB><<<grid, 256, kZgemmDmmaSmem, s>>>(g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r,
                                                                       g.ldo_c, g.alpha, g.beta, kps, part);
