@@ -1,8 +1,9 @@
 // FP64 complex GEMM over strided operands, used for the Kleinman-Bylander projections
 // (apply.zig:1143-1183, 1278-1336) and the Rayleigh-Ritz contractions V^H W and V C
 // (lobpcg/common.zig:113-143, 231-259).  B200 has no FP64 tcgen05 kind, so the FP64 path runs on
-// the FP64 tensor cores through mma.sync m16n8k8 .f64 (k_zgemm_dmma16, the default) or m8n8k4 .f64
-// (k_zgemm_dmma, DFTCUDA_ZGEMM=dmma8), or on the FP64 FMA pipe (k_zgemm, DFTCUDA_ZGEMM=fma):
+// the FP64 tensor cores through mma.sync m8n8k4 .f64 (k_zgemm_dmma, the default) or m16n8k8 .f64
+// (k_zgemm_dmma16, DFTCUDA_ZGEMM=dmma16: the same FP64 tensor throughput, measured 1-2 % slower),
+// or on the FP64 FMA pipe (k_zgemm, DFTCUDA_ZGEMM=fma):
 // 64x64 output tiles per 256-thread CTA, K staged through
 // shared memory in slices of 16 with cp.async double buffering, and split-K with a deterministic
 // second-pass reduction when the output has too few tiles to fill the 148 SMs.
@@ -354,14 +355,14 @@ size_t zgemm_workspace_elems(int M, int N, int K) {
   return s > 1 ? (size_t)s * M * N : 0;
 }
 
-// DFTCUDA_ZGEMM=fma selects the FMA-pipe kernel, =dmma8 the m8n8k4 tensor-core kernel (A/B
-// measurements); the m16n8k8 FP64 tensor-core kernel is the default.
+// DFTCUDA_ZGEMM=fma selects the FMA-pipe kernel, =dmma16 the m16n8k8 tensor-core kernel (A/B
+// measurements); the m8n8k4 FP64 tensor-core kernel is the default.
 static int zgemm_kind() {
   static const int v = [] {
     const char* e = std::getenv("DFTCUDA_ZGEMM");
     if (e && std::string(e) == "fma") return 0;
-    if (e && std::string(e) == "dmma8") return 1;
-    return 2;
+    if (e && std::string(e) == "dmma16") return 2;
+    return 1;
   }();
   return v;
 }
