@@ -95,28 +95,31 @@ def test_fno_training_reduces_loss(dz):
 # ---- the shipped trained weights on held-out cells ------------------------------------------------
 
 
-def test_trained_preconditioner_gain(dz):
-    """The committed MLP preconditioner on a held-out strained/displaced Si8 cell: converges to the
-    reference eigenvalues in far fewer H applications than the reference diagonal and within 10% of
-    Teter-Payne-Allan (the form it refines)."""
+@pytest.mark.parametrize("seed", [1290, 1291])
+def test_trained_preconditioner_gain(dz, seed):
+    """The committed MLP preconditioner on held-out cells of its training family (Si cells of 8 to 64
+    atoms, strained and displaced): converges to the reference eigenvalues in far fewer H
+    applications than the reference diagonal, and in fewer than Teter-Payne-Allan, the form it
+    refines -- the test fails if the network stops beating its base."""
     import importlib
 
     learn = importlib.import_module("dftzig_b200.learn")
     system = importlib.import_module("dftzig_b200.system")
     params = learn.load_precond_weights()
-    c = system.crystal("si8d", 1290)
-    inp = system.kpoint_inputs(c, 12.0, (0.0, 0.0, 0.0))
+    c = system.crystal("sitrain", seed)
+    nb = int(round(c.nelec / 2))
+    inp = system.kpoint_inputs(c, 25.0, (0.0, 0.0, 0.0))
     out = {}
     for kind in (dz.PRECOND_REFERENCE, dz.PRECOND_TPA, dz.PRECOND_MLP):
         kc = learn._context(dz, inp)
         kc.set_preconditioner(kind, params if kind == dz.PRECOND_MLP else None)
-        out[kind] = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, 16, dz.Options(max_iter=400, tol=1e-6))
+        out[kind] = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, nb, dz.Options(max_iter=400, tol=1e-6))
         kc.close()
     ref, tpa, mlp = out[dz.PRECOND_REFERENCE], out[dz.PRECOND_TPA], out[dz.PRECOND_MLP]
     assert ref.converged and tpa.converged and mlp.converged
     assert np.abs(mlp.values - ref.values).max() < 1e-7
     assert mlp.h_applies < 0.5 * ref.h_applies
-    assert mlp.h_applies <= 1.1 * tpa.h_applies
+    assert mlp.h_applies < tpa.h_applies
 
 
 def test_trained_fno_start_beats_atomic_superposition(dz):
@@ -139,3 +142,27 @@ def test_trained_fno_start_beats_atomic_superposition(dz):
     err_fno = np.sqrt(np.mean((rho_fno - r.rho) ** 2))
     err_at = np.sqrt(np.mean((rho_atomic - r.rho) ** 2))
     assert err_fno < 0.2 * err_at
+
+
+def test_trained_preconditioner_scf_gain(dz):
+    """The committed MLP preconditioner inside a whole SCF run (warm-started Davidson every step, the
+    reference's mixing and eigensolver defaults) on a held-out 32-atom cell of its training family:
+    the same converged energy in fewer H applications than Teter-Payne-Allan."""
+    import importlib
+
+    learn = importlib.import_module("dftzig_b200.learn")
+    scf = importlib.import_module("dftzig_b200.scf")
+    system = importlib.import_module("dftzig_b200.system")
+    c = system.crystal("sitrain", 1207)
+    assert len(c.atom_species) == 32
+    nb = int(round(c.nelec / 2.0)) + 8
+    out = {}
+    for key, pre in (("tpa", (dz.PRECOND_TPA, None)), ("mlp", (dz.PRECOND_MLP, learn.load_precond_weights()))):
+        b = scf.GpuBackend(dz, "fp64", precond=pre, resident=True)
+        r = scf.run_scf(c, scf.ScfParams(ecut=25.0, kmesh=(1, 1, 1), nbands=nb, convergence=1e-7, max_iter=60), b)
+        b.close()
+        out[key] = (r, sum(s[2] for s in b.solves))
+    (rt, ht), (rm, hm) = out["tpa"], out["mlp"]
+    assert rt.converged and rm.converged
+    assert abs(rt.energy_per_atom - rm.energy_per_atom) < 1e-6
+    assert hm < ht
