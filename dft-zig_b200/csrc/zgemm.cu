@@ -1,9 +1,11 @@
 // FP64 complex GEMM over strided operands, used for the Kleinman-Bylander projections
 // (apply.zig:1143-1183, 1278-1336) and the Rayleigh-Ritz contractions V^H W and V C
 // (lobpcg/common.zig:113-143, 231-259).  B200 has no FP64 tcgen05 kind, so the FP64 path runs on
-// the FP64 tensor cores through mma.sync m8n8k4 .f64 (k_zgemm_dmma, the default) or m16n8k8 .f64
-// (k_zgemm_dmma16, DFTCUDA_ZGEMM=dmma16: the same FP64 tensor throughput, measured 1-2 % slower),
-// or on the FP64 FMA pipe (k_zgemm, DFTCUDA_ZGEMM=fma):
+// the FP64 tensor cores through mma.sync m8n8k4 .f64 with three real products per complex one
+// (k_zgemm_dmma3m, the default: the FP64 MMA pipe is the bound, and it does a quarter less work),
+// with the plain four products (k_zgemm_dmma, DFTCUDA_ZGEMM=dmma8) or on the m16n8k8 shape
+// (k_zgemm_dmma16, DFTCUDA_ZGEMM=dmma16: the same throughput as m8n8k4), or on the FP64 FMA pipe
+// (k_zgemm, DFTCUDA_ZGEMM=fma):
 // 64x64 output tiles per 256-thread CTA, K staged through
 // shared memory in slices of 16 with cp.async double buffering, and split-K with a deterministic
 // second-pass reduction when the output has too few tiles to fill the 148 SMs.
@@ -309,6 +311,91 @@ __global__ void __launch_bounds__(256, 2) k_zgemm_dmma16(int M, int N, int K, co
     }
 }
 
+// Three real MMAs per complex product (Gauss): with a = ar + i ai, b = br + i bi,
+//   T1 = ar (br + bi),  T2 = (ar + ai) bi,  T3 = (ai - ar) br;   Re = T1 - T2,  Im = T1 + T3.
+// The m8n8k4 kernel's tiling and fragments with a third accumulator per 8 x 8 tile: a quarter
+// fewer FP64 MMAs, the FP64 tensor pipe being the bound of the four-product form.
+template <bool AKC, bool BKC, bool CJA, bool CJB>
+__global__ void __launch_bounds__(256, 2) k_zgemm_dmma3m(int M, int N, int K, const double2* __restrict__ A, long lda,
+                                                         const double2* __restrict__ B, long ldb, double2* __restrict__ O,
+                                                         long ldo_r, long ldo_c, double alpha, double beta, int kps,
+                                                         double2* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char zsm[];
+  double2(*As)[BK][BM + kZmPad] = reinterpret_cast<double2(*)[BK][BM + kZmPad]>(zsm);
+  double2(*Bs)[BK][BN + kZmPad] = reinterpret_cast<double2(*)[BK][BN + kZmPad]>(zsm + 2 * sizeof(double2) * BK * (BM + kZmPad));
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wr = warp >> 1, wc = warp & 1;
+  const int r0 = blockIdx.y * BM, c0 = blockIdx.x * BN;
+  const int kbeg = blockIdx.z * kps;
+  const int kend = min(K, kbeg + kps);
+  const double sa = CJA ? -1.0 : 1.0, sb = CJB ? -1.0 : 1.0;
+  double t1[2][4][2], t2[2][4][2], t3[2][4][2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) t1[i][j][h] = t2[i][j][h] = t3[i][j][h] = 0.0;
+  if (kbeg < kend) zgemm_fetch<AKC, BKC, kZmPad>(As[0], Bs[0], M, N, kend, r0, c0, kbeg, A, lda, B, ldb, tid);
+  int buf = 0;
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
+    cp_async_wait_all();
+    __syncthreads();
+    if (k0 + BK < kend) zgemm_fetch<AKC, BKC, kZmPad>(As[buf ^ 1], Bs[buf ^ 1], M, N, kend, r0, c0, k0 + BK, A, lda, B, ldb, tid);
+#pragma unroll
+    for (int k4 = 0; k4 < BK; k4 += 4) {
+      double ar[2], as_[2], ad[2], bs[4], bi[4], br[4];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const double2 v = As[buf][k4 + t][wr * 16 + i * 8 + g];
+        const double ai = sa * v.y;
+        ar[i] = v.x;
+        as_[i] = v.x + ai;
+        ad[i] = ai - v.x;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double2 v = Bs[buf][k4 + t][wc * 32 + j * 8 + g];
+        br[j] = v.x;
+        bi[j] = sb * v.y;
+        bs[j] = v.x + bi[j];
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          dmma(t1[i][j][0], t1[i][j][1], ar[i], bs[j]);
+          dmma(t2[i][j][0], t2[i][j][1], as_[i], bi[j]);
+          dmma(t3[i][j][0], t3[i][j][1], ad[i], br[j]);
+        }
+    }
+    buf ^= 1;
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = r0 + wr * 16 + i * 8 + g, c = c0 + wc * 32 + j * 8 + 2 * t + h;
+        if (r >= M || c >= N) continue;
+        const double2 acc = make_double2(t1[i][j][h] - t2[i][j][h], t1[i][j][h] + t3[i][j][h]);
+        if (part) {
+          part[((long)blockIdx.z * M + r) * N + c] = acc;
+        } else {
+          double2* o = O + (long)r * ldo_r + (long)c * ldo_c;
+          double2 v = make_double2(alpha * acc.x, alpha * acc.y);
+          if (beta != 0.0) {
+            const double2 old = *o;
+            v.x += beta * old.x;
+            v.y += beta * old.y;
+          }
+          *o = v;
+        }
+      }
+}
+
 __global__ void k_zgemm_reduce(int M, int N, int splits, const double2* __restrict__ part, double2* __restrict__ O,
                                long ldo_r, long ldo_c, double alpha, double beta) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -355,20 +442,28 @@ size_t zgemm_workspace_elems(int M, int N, int K) {
   return s > 1 ? (size_t)s * M * N : 0;
 }
 
-// DFTCUDA_ZGEMM=fma selects the FMA-pipe kernel, =dmma16 the m16n8k8 tensor-core kernel (A/B
-// measurements); the m8n8k4 FP64 tensor-core kernel is the default.
+// DFTCUDA_ZGEMM=fma / dmma8 / dmma16 select the other kernels (A/B measurements); the
+// three-product m8n8k4 kernel is the default.
 static int zgemm_kind() {
   static const int v = [] {
     const char* e = std::getenv("DFTCUDA_ZGEMM");
     if (e && std::string(e) == "fma") return 0;
+    if (e && std::string(e) == "dmma8") return 1;
     if (e && std::string(e) == "dmma16") return 2;
-    return 1;
+    return 3;
   }();
   return v;
 }
 
 template <bool AKC, bool BKC, bool CJA, bool CJB>
 static void launch(const GemmArgs& g, dim3 grid, int kps, double2* part, cudaStream_t s) {
+  if (zgemm_kind() == 3) {
+    ensure_max_dynamic_smem((const void*)k_zgemm_dmma3m<AKC, BKC, CJA, CJB>, (int)kZgemmDmmaSmem);
+    k_zgemm_dmma3m<AKC, BKC, CJA, CJB><<<grid, 256, kZgemmDmmaSmem, s>>>(g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r,
+                                                                        g.ldo_c, g.alpha, g.beta, kps, part);
+    count_launch();
+    return;
+  }
   if (zgemm_kind() == 2) {
     ensure_max_dynamic_smem((const void*)k_zgemm_dmma16<AKC, BKC, CJA, CJB>, (int)kZgemmDmmaSmem);
     k_zgemm_dmma16<AKC, BKC, CJA, CJB><<<grid, 256, kZgemmDmmaSmem, s>>>(g.M, g.N, g.K, g.A, g.lda, g.B, g.ldb, g.O, g.ldo_r,
