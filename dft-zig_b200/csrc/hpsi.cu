@@ -438,6 +438,7 @@ static int density_block(dftcuda_kctx* c, const double2* x, size_t ncols, const 
   ProfScope ps(c, P_DENSITY, s);
   cplx<T>* W = reinterpret_cast<cplx<T>*>(c->d_box);
   const size_t smem_plane = sizeof(cplx<T>) * (size_t)c->P;
+  if (smem_plane > kSmemMax) return fail(DFTCUDA_ERR_UNSUPPORTED, "y-z plane does not fit shared memory");
   dim3 gp(c->n_act, (unsigned)ncols);
   k_plane_inv<T><<<gp, 512, smem_plane, s>>>(x, (long)c->npw, W, c->n_act, c->d_plane_off, c->d_pw_idx, c->d_pw_spos,
                                              c->fy.dev, c->fz.dev, c->ny, c->nz); count_launch();

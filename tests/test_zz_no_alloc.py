@@ -96,3 +96,22 @@ def test_noalloc_density_rejects_too_many_bands_and_host_pointers(dz):
     st = lib.dftcuda_accumulate_density_noalloc(kc.handle, ct.c_void_p(v_dev.data_ptr()), kc.n, 1, ct.c_void_p(w_dev.data_ptr()), host_rho.ctypes.data)
     assert st == -6
     kc.close()
+
+
+def test_noalloc_rejects_a_plane_beyond_shared_memory(dz):
+    """A y-z plane of 128 x 128 FP64 complex values (256 KB) does not fit one CTA's shared memory:
+    the allocation-free entry reports Unsupported instead of failing its launch."""
+    import torch
+
+    dims = (20, 128, 128)
+    hkl = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], dtype=np.int32)
+    kin = np.array([0.0, 1.0, 1.0, 1.0])
+    gcart = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]])
+    kc = dz.KpointContext(*dims, 1000.0, hkl, kin, gcart, 0)
+    v = torch.ones((2, 4), dtype=torch.complex128, device="cuda")
+    w = torch.ones(2, dtype=torch.float64, device="cuda")
+    rho = torch.zeros(dims[0] * dims[1] * dims[2], dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    with pytest.raises(dz.Unsupported):
+        kc.accumulate_band_density_noalloc(v, w, rho)
+    kc.close()
