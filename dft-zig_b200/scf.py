@@ -645,11 +645,14 @@ class ScfState:
             self.converged = self.done = True
             self.rho = rho_out
             return True
+        # Pulay from the reference's 0-based iteration index pulay_start on (scf.zig:164, 495: the
+        # loop counter starts at 0); self.it counts from 1
+        pulay = self.it - 1 >= p.pulay_start
         if self.dev:
             import torch
 
             resid = v_out_d - self.v_hxc
-            if self.it >= p.pulay_start:
+            if pulay:
                 if self.dielec is not None:
                     if not torch.is_tensor(self.dielec):
                         self.dielec = torch.from_numpy(self.dielec).to(resid.device)
@@ -661,7 +664,7 @@ class ScfState:
                 self.v_hxc = self.v_hxc + p.mixing_beta * resid
         else:
             resid = self.hxc_g(rho_out) - self.v_hxc
-            if self.it >= p.pulay_start:
+            if pulay:
                 if self.dielec is not None:
                     resid = resid * self.dielec
                 flat = self.mixer.mix(np.concatenate([self.v_hxc.real, self.v_hxc.imag]), np.concatenate([resid.real, resid.imag]), p.mixing_beta)
