@@ -591,6 +591,7 @@ def time_to_scf_si216(dz, args, device_index: int):
     return {
         "workload": "Si216 3x3x3 conventional, sigma 0.05 A (seed 3), 25 Ry, 108^3, Gamma, 448 bands, LDA-PZ, fixed occupations",
         "criterion": "|E - E_target| < 1e-6 Ry/atom, E_target = plain FP64 run to density RMS residual 1e-8",
+        "target_energy_per_atom": ref.energy / natom,
         "fp64": {"seconds": round(fp64_s, 3), "scf_iterations": int(hit[0]),
                  "dE_per_atom": (hit[1] - ref.energy) / natom, "run_to_target_seconds": round(ref.wall_s, 3),
                  "run_to_target_iterations": ref.iterations},
