@@ -67,12 +67,14 @@ def test_many_cell_scf_matches_single_runs(dz):
 ], ids=["si2", "al4-smeared"])
 def test_resident_scf_matches_host_driver(dz, cell, kw):
     """The resident driver (eigenvectors, density, Hartree-XC potential and Pulay history on the
-    device: csrc/potential.cu) against the host-side potential and mixing with the same eigensolver:
-    same iterations, energy per atom within 1e-10 Ry, density within 1e-9 relative."""
+    device: csrc/potential.cu; the per-k inputs built on the device too) against the host-side
+    inputs, potential and mixing with the same eigensolver: iterations within two, energy per atom
+    within 1e-10 Ry, density within 1e-9 relative.  Converged to 1e-10 so that the two paths, whose
+    inputs differ in the last bits (device and host Y_lm), meet at the same fixed point."""
     scf = importlib.import_module("dftzig_b200.scf")
     system = importlib.import_module("dftzig_b200.system")
     c = system.crystal(cell)
-    p = scf.ScfParams(**kw, convergence=1e-8, iterative_max_iter=200, iterative_tol=1e-10, warmup_steps=0, max_iter=40)
+    p = scf.ScfParams(**kw, convergence=1e-10, iterative_max_iter=200, iterative_tol=1e-11, warmup_steps=0, max_iter=60)
     host = scf.GpuBackend(dz)
     r_host = scf.run_scf(c, p, host)
     host.close()
@@ -80,7 +82,7 @@ def test_resident_scf_matches_host_driver(dz, cell, kw):
     r_dev = scf.run_scf(c, p, dev)
     dev.close()
     assert r_host.converged and r_dev.converged
-    assert abs(r_dev.iterations - r_host.iterations) <= 1
+    assert abs(r_dev.iterations - r_host.iterations) <= 2
     assert abs(r_dev.energy_per_atom - r_host.energy_per_atom) < 1e-10
     assert np.abs(r_dev.rho - r_host.rho).max() < 1e-9 * np.abs(r_host.rho).max()
     for a, b in zip(r_dev.eigenvalues, r_host.eigenvalues):

@@ -98,20 +98,26 @@ def test_noalloc_density_rejects_too_many_bands_and_host_pointers(dz):
     kc.close()
 
 
-def test_noalloc_rejects_a_plane_beyond_shared_memory(dz):
-    """A y-z plane of 128 x 128 FP64 complex values (256 KB) does not fit one CTA's shared memory:
-    the allocation-free entry reports Unsupported instead of failing its launch."""
+def test_plane_beyond_shared_memory_is_rejected(dz):
+    """A y-z plane of 128 x 128 FP64 complex values (256 KB) does not fit one CTA's shared memory.
+    Context creation already refuses it (Unsupported), so no entry point, the allocation-free
+    density included (which checks again), can launch an oversized plane; the FP32 context of the
+    same box (128 KB planes) is accepted and its allocation-free density runs."""
     import torch
 
     dims = (20, 128, 128)
     hkl = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], dtype=np.int32)
     kin = np.array([0.0, 1.0, 1.0, 1.0])
     gcart = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]])
-    kc = dz.KpointContext(*dims, 1000.0, hkl, kin, gcart, 0)
+    with pytest.raises(dz.Unsupported):
+        dz.KpointContext(*dims, 1000.0, hkl, kin, gcart, 0)
+    kc = dz.KpointContext(*dims, 1000.0, hkl, kin, gcart, 1)
     v = torch.ones((2, 4), dtype=torch.complex128, device="cuda")
     w = torch.ones(2, dtype=torch.float64, device="cuda")
     rho = torch.zeros(dims[0] * dims[1] * dims[2], dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
-    with pytest.raises(dz.Unsupported):
-        kc.accumulate_band_density_noalloc(v, w, rho)
+    kc.accumulate_band_density_noalloc(v, w, rho)
+    torch.cuda.synchronize()
+    # Parseval: the density integrates to sum_b w_b sum_G |c_G|^2 = 2 bands x 4 plane waves
+    assert abs(float(rho.sum()) * 1000.0 / rho.numel() - 8.0) < 1e-4
     kc.close()
