@@ -109,3 +109,26 @@ def test_pbe_scf_converges_and_differs_from_lda(dz):
     dims = system.fft_box(20.0, c.recip)
     _, _, e_xc, _ = op.hxc_potential(out["pbe"].rho, dims, c.recip, c.volume, functional="pbe")
     assert abs(out["pbe"].terms["xc"] - e_xc) < 1e-9 * abs(e_xc)
+
+
+@pytest.mark.parametrize("min_pw", [0, 4096], ids=["tf32x3-contexts", "small-kpoints-fp64"])
+def test_mixed_precision_scf_reaches_the_fp64_energy(dz, min_pw):
+    """GpuBackend("mixed"): TF32X3 contexts (FP32 FFT passes, split-TF32 tensor-core GEMMs) while the
+    density residual is large, FP64 contexts after the switch; the converged energy per atom equals
+    the plain FP64 run's within 1e-8 Ry and the switch happened.  With the default threshold Si8's
+    k-points (~1,500 plane waves) stay FP64 throughout (no second context), which must also agree."""
+    scf = importlib.import_module("dftzig_b200.scf")
+    system = importlib.import_module("dftzig_b200.system")
+    c = system.crystal("si8")
+    p = scf.ScfParams(ecut=20.0, kmesh=(1, 1, 1), nbands=20, convergence=1e-9, max_iter=60)
+    b = scf.GpuBackend(dz, resident=True)
+    ref = scf.run_scf(c, p, b)
+    b.close()
+    m = scf.GpuBackend(dz, "mixed", resident=True, min_pw_reduced=min_pw)
+    r = scf.run_scf(c, p, m)
+    m.close()
+    assert ref.converged and r.converged
+    assert abs(r.energy_per_atom - ref.energy_per_atom) < 1e-8
+    assert m.switched_at is not None
+    if min_pw == 0:
+        assert any(s[0] == "tf32x3" for s in m.solves)
