@@ -14,6 +14,8 @@
 //                           interpolation, R(0) at q <= 0, the last value in the last interval, 0 at
 //                           q >= g_max), Y_lm the real harmonics of nonlocal.zig:152-241 (l <= 4).
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -224,6 +226,41 @@ __global__ void k_projector_phi(int l, const double* __restrict__ tab, int nq, d
   for (int mi = 0; mi <= 2 * l; ++mi) phi[(long)mi * n + i] = rad * real_ylm(l, mi - l, x, y, z);
 }
 
+// One stream and one growable device buffer per device, kept for the life of the process: a
+// per-k-point setup calls these entry points a few times for each of hundreds of k-points, and a
+// stream plus allocations per call cost more than the kernels.
+struct SetupEngine {
+  std::mutex mu;
+  cudaStream_t s = nullptr;
+  char* buf = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (!s && cudaStreamCreateWithFlags(&s, cudaStreamDefault) != cudaSuccess) {
+      s = nullptr;
+      return fail(DFTCUDA_ERR_CUDA, "setup engine: stream creation failed");
+    }
+    if (bytes <= cap) return DFTCUDA_OK;
+    cudaStreamSynchronize(s);
+    if (buf) cudaFree(buf);
+    buf = nullptr;
+    cap = 0;
+    if (cudaMalloc(&buf, bytes) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "setup engine: buffer");
+    cap = bytes;
+    return DFTCUDA_OK;
+  }
+};
+
+SetupEngine* setup_engine() {
+  static std::mutex map_mu;
+  static std::map<int, SetupEngine*> engines;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lock(map_mu);
+  SetupEngine*& e = engines[dev];
+  if (!e) e = new SetupEngine();  // lives as long as the process
+  return e;
+}
+
 }  // namespace
 }  // namespace dftcuda
 
@@ -254,55 +291,55 @@ extern "C" int dftcuda_plane_wave_basis(const double* recip, double ecut_ry, con
   const long D = 2L * a.n + 1;
   a.ncand = D * D * D;
   const int nblocks = (int)((a.ncand + kBasisTile - 1) / kBasisTile);
-  cudaStream_t s = nullptr;
-  int* dcount = nullptr;
-  long* dtotal = nullptr;
-  char* dout = nullptr;
-  auto run = [&]() -> int {
-    DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamDefault));
-    DFT_CUDA_TRY(cudaMalloc(&dcount, sizeof(int) * nblocks));
-    DFT_CUDA_TRY(cudaMalloc(&dtotal, sizeof(long)));
+  SetupEngine* en = setup_engine();
+  if (!en) return fail(DFTCUDA_ERR_CUDA, "plane_wave_basis: no device");
+  std::lock_guard<std::mutex> lock(en->mu);
+  // buffer: block counts, the total, then (when the outputs are host arrays) the staged basis
+  const size_t off_total = ((sizeof(int) * (size_t)nblocks + 15) / 16) * 16;
+  const size_t off_out = off_total + 16;
+  DFT_TRY(en->ensure(off_out));
+  cudaStream_t s = en->s;
+  int* dcount = reinterpret_cast<int*>(en->buf);
+  long* dtotal = reinterpret_cast<long*>(en->buf + off_total);
+  k_basis_count<<<nblocks, kBasisThreads, 0, s>>>(a, dcount);
+  count_launch();
+  k_basis_scan<<<1, 1024, 0, s>>>(dcount, nblocks, dtotal);
+  count_launch();
+  long total = 0;
+  DFT_CUDA_TRY(cudaMemcpyAsync(&total, dtotal, sizeof(long), cudaMemcpyDeviceToHost, s));
+  DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  *n_out = (size_t)total;
+  if (capacity == 0) return DFTCUDA_OK;  // size query
+  if ((size_t)total > capacity) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "plane_wave_basis: capacity below the basis size");
+  // outputs: straight into device arrays, else through the engine's buffer
+  const bool dev = is_device_pointer(hkl) && is_device_pointer(gcart) && is_device_pointer(kpg) && is_device_pointer(kinetic);
+  int* oh = hkl;
+  double *og = gcart, *oq = kpg, *ok = kinetic;
+  const size_t nb_h = sizeof(int32_t) * 3 * total, nb_v = sizeof(double) * 3 * total, nb_k = sizeof(double) * total;
+  if (!dev) {
+    DFT_TRY(en->ensure(off_out + 2 * nb_v + nb_k + nb_h + 64));
+    dcount = reinterpret_cast<int*>(en->buf);  // the buffer may have moved; the counts are recomputed below
+    char* o = en->buf + off_out;
+    og = reinterpret_cast<double*>(o);
+    oq = reinterpret_cast<double*>(o + nb_v);
+    ok = reinterpret_cast<double*>(o + 2 * nb_v);
+    oh = reinterpret_cast<int*>(o + 2 * nb_v + nb_k);
     k_basis_count<<<nblocks, kBasisThreads, 0, s>>>(a, dcount);
     count_launch();
-    k_basis_scan<<<1, 1024, 0, s>>>(dcount, nblocks, dtotal);
+    k_basis_scan<<<1, 1024, 0, s>>>(dcount, nblocks, reinterpret_cast<long*>(en->buf + off_total));
     count_launch();
-    long total = 0;
-    DFT_CUDA_TRY(cudaMemcpyAsync(&total, dtotal, sizeof(long), cudaMemcpyDeviceToHost, s));
-    DFT_CUDA_TRY(cudaStreamSynchronize(s));
-    *n_out = (size_t)total;
-    if (capacity == 0) return DFTCUDA_OK;  // size query
-    if ((size_t)total > capacity) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "plane_wave_basis: capacity below the basis size");
-    // outputs: straight into device arrays, else through one staging buffer
-    const bool dev = is_device_pointer(hkl) && is_device_pointer(gcart) && is_device_pointer(kpg) && is_device_pointer(kinetic);
-    int* oh = hkl;
-    double *og = gcart, *oq = kpg, *ok = kinetic;
-    const size_t nb_h = sizeof(int32_t) * 3 * total, nb_v = sizeof(double) * 3 * total, nb_k = sizeof(double) * total;
-    if (!dev) {
-      DFT_CUDA_TRY(cudaMalloc(&dout, nb_h + 2 * nb_v + nb_k + 64));
-      og = reinterpret_cast<double*>(dout);
-      oq = reinterpret_cast<double*>(dout + nb_v);
-      ok = reinterpret_cast<double*>(dout + 2 * nb_v);
-      oh = reinterpret_cast<int*>(dout + 2 * nb_v + nb_k);
-    }
-    k_basis_write<<<nblocks, kBasisThreads, 0, s>>>(a, dcount, total, oh, og, oq, ok);
-    count_launch();
-    DFT_CUDA_TRY(cudaGetLastError());
-    if (!dev) {
-      DFT_CUDA_TRY(cudaMemcpyAsync(hkl, oh, nb_h, cudaMemcpyDeviceToHost, s));
-      DFT_CUDA_TRY(cudaMemcpyAsync(gcart, og, nb_v, cudaMemcpyDeviceToHost, s));
-      DFT_CUDA_TRY(cudaMemcpyAsync(kpg, oq, nb_v, cudaMemcpyDeviceToHost, s));
-      DFT_CUDA_TRY(cudaMemcpyAsync(kinetic, ok, nb_k, cudaMemcpyDeviceToHost, s));
-    }
-    DFT_CUDA_TRY(cudaStreamSynchronize(s));
-    return DFTCUDA_OK;
-  };
-  const int st = run();
-  if (s) cudaStreamSynchronize(s);
-  if (dout) cudaFree(dout);
-  if (dcount) cudaFree(dcount);
-  if (dtotal) cudaFree(dtotal);
-  if (s) cudaStreamDestroy(s);
-  return st;
+  }
+  k_basis_write<<<nblocks, kBasisThreads, 0, s>>>(a, dcount, total, oh, og, oq, ok);
+  count_launch();
+  DFT_CUDA_TRY(cudaGetLastError());
+  if (!dev) {
+    DFT_CUDA_TRY(cudaMemcpyAsync(hkl, oh, nb_h, cudaMemcpyDeviceToHost, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(gcart, og, nb_v, cudaMemcpyDeviceToHost, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(kpg, oq, nb_v, cudaMemcpyDeviceToHost, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(kinetic, ok, nb_k, cudaMemcpyDeviceToHost, s));
+  }
+  DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  return DFTCUDA_OK;
 }
 
 extern "C" int dftcuda_projector_phi(int l, size_t nq, double gmax, const double* table, size_t n, const double* kpg, double* phi) {
@@ -313,35 +350,29 @@ extern "C" int dftcuda_projector_phi(int l, size_t nq, double gmax, const double
   const size_t mt = 2 * (size_t)l + 1;
   const bool dev_in = is_device_pointer(table) && is_device_pointer(kpg);
   const bool dev_out = is_device_pointer(phi);
-  cudaStream_t s = nullptr;
-  char* buf = nullptr;
-  auto run = [&]() -> int {
-    DFT_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamDefault));
-    const double* dt = table;
-    const double* dq = kpg;
-    double* dp = phi;
-    const size_t bt = sizeof(double) * nq, bq = sizeof(double) * 3 * n, bp = sizeof(double) * mt * n;
-    const size_t need = (dev_in ? 0 : bt + bq) + (dev_out ? 0 : bp);
-    if (need) DFT_CUDA_TRY(cudaMalloc(&buf, need));
-    size_t off = 0;
-    if (!dev_in) {
-      DFT_CUDA_TRY(cudaMemcpyAsync(buf, table, bt, cudaMemcpyDefault, s));
-      DFT_CUDA_TRY(cudaMemcpyAsync(buf + bt, kpg, bq, cudaMemcpyDefault, s));
-      dt = reinterpret_cast<const double*>(buf);
-      dq = reinterpret_cast<const double*>(buf + bt);
-      off = bt + bq;
-    }
-    if (!dev_out) dp = reinterpret_cast<double*>(buf + off);
-    k_projector_phi<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(l, dt, (int)nq, gmax, dq, (long)n, dp);
-    count_launch();
-    DFT_CUDA_TRY(cudaGetLastError());
-    if (!dev_out) DFT_CUDA_TRY(cudaMemcpyAsync(phi, dp, bp, cudaMemcpyDeviceToHost, s));
-    DFT_CUDA_TRY(cudaStreamSynchronize(s));
-    return DFTCUDA_OK;
-  };
-  const int st = run();
-  if (s) cudaStreamSynchronize(s);
-  if (buf) cudaFree(buf);
-  if (s) cudaStreamDestroy(s);
-  return st;
+  SetupEngine* en = setup_engine();
+  if (!en) return fail(DFTCUDA_ERR_CUDA, "projector_phi: no device");
+  std::lock_guard<std::mutex> lock(en->mu);
+  const size_t bt = ((sizeof(double) * nq + 15) / 16) * 16, bq = sizeof(double) * 3 * n, bp = sizeof(double) * mt * n;
+  const size_t need = (dev_in ? 0 : bt + bq) + (dev_out ? 0 : bp);
+  if (need) DFT_TRY(en->ensure(need));
+  cudaStream_t s = en->s;
+  const double* dt = table;
+  const double* dq = kpg;
+  double* dp = phi;
+  size_t off = 0;
+  if (!dev_in) {
+    DFT_CUDA_TRY(cudaMemcpyAsync(en->buf, table, sizeof(double) * nq, cudaMemcpyDefault, s));
+    DFT_CUDA_TRY(cudaMemcpyAsync(en->buf + bt, kpg, bq, cudaMemcpyDefault, s));
+    dt = reinterpret_cast<const double*>(en->buf);
+    dq = reinterpret_cast<const double*>(en->buf + bt);
+    off = bt + bq;
+  }
+  if (!dev_out) dp = reinterpret_cast<double*>(en->buf + off);
+  k_projector_phi<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(l, dt, (int)nq, gmax, dq, (long)n, dp);
+  count_launch();
+  DFT_CUDA_TRY(cudaGetLastError());
+  if (!dev_out) DFT_CUDA_TRY(cudaMemcpyAsync(phi, dp, bp, cudaMemcpyDeviceToHost, s));
+  DFT_CUDA_TRY(cudaStreamSynchronize(s));
+  return DFTCUDA_OK;
 }
