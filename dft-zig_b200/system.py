@@ -131,13 +131,14 @@ def crystal(name: str, seed: int = 1) -> Crystal:
         cell = (np.eye(3) * 5.431 * BOHR_PER_ANGSTROM) @ (np.eye(3) + e)
         pos = DIAMOND8 @ cell + rng.normal(0.0, 0.05 * BOHR_PER_ANGSTROM, size=(8, 3))
         return Crystal(cell, [si], np.zeros(8, int), pos)
-    if name == "sitrain":
+    if name in ("sitrain", "sival"):
         # the learned preconditioner's training and held-out cells: 8 to 64 Si atoms (supercells
         # of the 8-atom cubic cell, shape drawn from the seed), a seeded symmetric strain in
-        # [-1%, 1%] and N(0, 0.05 A) displacements
+        # [-1%, 1%] and N(0, 0.05 A) displacements; "sival": its 128-atom (4 x 2 x 2) validation cells
         rng = np.random.default_rng(seed)
         shapes = [(1, 1, 1), (2, 1, 1), (3, 1, 1), (2, 2, 1), (3, 2, 1), (2, 2, 2)]
-        reps = np.array(shapes[int(rng.integers(0, len(shapes)))])
+        pick = int(rng.integers(0, len(shapes)))
+        reps = np.array(shapes[pick] if name == "sitrain" else (4, 2, 2))
         e = rng.uniform(-0.01, 0.01, size=(3, 3))
         e = 0.5 * (e + e.T)
         a = 5.431 * BOHR_PER_ANGSTROM
