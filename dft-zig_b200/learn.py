@@ -280,7 +280,7 @@ def evaluate_precond(dz, cells, ecut: float, nbands: int, params, tol: float = 1
 
 
 def evaluate_si216(dz, params, tol: float = 1e-6, max_iter: int = 400) -> dict:
-    """north_star's judge of the learned preconditioner: one Davidson solve of the Si216 cell (3x3x3
+    """The learned preconditioner on the benchmark cell: one Davidson solve of the Si216 cell (3x3x3
     conventional, seed 3, 25 Ry, Gamma, 448 bands, the reference's defaults otherwise) from the
     random start to the same residual tol, per preconditioner: iterations, H applications and the
     solve's wall time (FP64 contexts, device-resident)."""
