@@ -440,7 +440,7 @@ def main(argv=None):
         kw = dict(t_list=(1, 2, 4, 7, 11, 16), bands_per_t=12)
         tr = precond_samples(dz, train_cells, a.ecut, nb, seed=1, **kw)
         ev = precond_samples(dz, eval_cells, a.ecut, nb, seed=2, **kw)
-        # selection by a whole SCF run on a 128-atom validation cell (4 x 2 x 2, the family's recipe;
+        # selection by a whole SCF run on a 144-atom validation cell (3 x 3 x 2, the family's recipe;
         # SCF runs of 48-64-atom cells did not rank the networks as the 216-atom SCF does), the
         # Davidson comparison on the held-out cells of the training family
         first = eval_cells[: min(6, len(eval_cells))]

@@ -134,11 +134,11 @@ def crystal(name: str, seed: int = 1) -> Crystal:
     if name in ("sitrain", "sival"):
         # the learned preconditioner's training and held-out cells: 8 to 64 Si atoms (supercells
         # of the 8-atom cubic cell, shape drawn from the seed), a seeded symmetric strain in
-        # [-1%, 1%] and N(0, 0.05 A) displacements; "sival": its 128-atom (4 x 2 x 2) validation cells
+        # [-1%, 1%] and N(0, 0.05 A) displacements; "sival": its 144-atom (3 x 3 x 2) validation cells
         rng = np.random.default_rng(seed)
         shapes = [(1, 1, 1), (2, 1, 1), (3, 1, 1), (2, 2, 1), (3, 2, 1), (2, 2, 2)]
         pick = int(rng.integers(0, len(shapes)))
-        reps = np.array(shapes[pick] if name == "sitrain" else (4, 2, 2))
+        reps = np.array(shapes[pick] if name == "sitrain" else (3, 3, 2))
         e = rng.uniform(-0.01, 0.01, size=(3, 3))
         e = 0.5 * (e + e.T)
         a = 5.431 * BOHR_PER_ANGSTROM
