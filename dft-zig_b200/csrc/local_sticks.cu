@@ -484,15 +484,19 @@ static int plane_warps_rt(size_t cs, int n, int n_act) {
   }
 }
 
-// The stick layout is the default where it applies; DFTCUDA_LOCAL=planes (read at context
-// creation) keeps the plane layout.
-static bool sticks_disabled() {
+// Layout choice at context creation: DFTCUDA_LOCAL=planes or =sticks forces one; by default the
+// stick layout serves boxes from 96 points along x on (Si216, 108^3: 12.0 against 14.2 ms per
+// 452-column FP64 block) and the plane layout smaller ones (Si64, 75^3: the stick z-plane pass took
+// 18.1 against 11.3 ms per step).  The autotuner times both either way.
+static int local_layout_env() {
   const char* e = std::getenv("DFTCUDA_LOCAL");
-  return e && std::string(e) == "planes";
+  if (e && std::string(e) == "planes") return 1;
+  if (e && std::string(e) == "sticks") return 2;
+  return 0;
 }
 
 bool kctx_sticks_ok(const dftcuda_kctx* c, int precision) {
-  if (sticks_disabled()) return false;
+  if (local_layout_env() == 1) return false;
   if (!four_step_supported(c->nx) || !four_step_supported(c->nz) || c->nx != c->ny) return false;
   if (c->n_act > 0xffff || c->ny > 0xffff) return false;
   const size_t cs = precision == DFTCUDA_PRECISION_FP64 ? sizeof(double2) : sizeof(float2);
@@ -680,6 +684,7 @@ int kctx_setup_sticks(dftcuda_kctx* c, const std::vector<int>& slot_of_x, const 
   c->sticks64 = kctx_sticks_ok(c, DFTCUDA_PRECISION_FP64);
   c->sticks32 = kctx_sticks_ok(c, DFTCUDA_PRECISION_FP32);
   if (!c->sticks64 && !c->sticks32) return DFTCUDA_OK;
+  c->sticks_off = local_layout_env() != 2 && c->nx < 96;
   DFT_TRY(init_root_tables_here());  // this file's copy of the sub-DFT roots
   const int ny = c->ny, nz = c->nz, n_act = c->n_act;
   std::vector<std::vector<int>> ys(n_act);

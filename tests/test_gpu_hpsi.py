@@ -155,8 +155,9 @@ def test_zero_columns_is_a_noop(dz):
                                               ("al4", 25.0, (0.1, 0.2, 0.3), 1), ("si8", 20.0, (0.5, 0.0, 0.0), 1)])
 def test_all_fft_paths_match_oracle(dz, monkeypatch, path, name, ecut, k, prec):
     """The three local-operator paths give the oracle's H|psi> and density: the stick-layout passes
-    (the default where nx = ny), the four-step plane-layout passes (DFTCUDA_LOCAL=planes) and the
-    stage-by-stage passes (DFTCUDA_FFT_PATH=generic).  The profile reports the layout that ran."""
+    (DFTCUDA_LOCAL=sticks, where nx = ny; the default from 96 points along x), the four-step
+    plane-layout passes (DFTCUDA_LOCAL=planes, the default below) and the stage-by-stage passes
+    (DFTCUDA_FFT_PATH=generic).  The profile reports the layout that ran."""
     from oracle import density as odens
 
     monkeypatch.delenv("DFTCUDA_FFT_PATH", raising=False)
@@ -165,6 +166,8 @@ def test_all_fft_paths_match_oracle(dz, monkeypatch, path, name, ecut, k, prec):
         monkeypatch.setenv("DFTCUDA_FFT_PATH", "generic")
     elif path == "planes":
         monkeypatch.setenv("DFTCUDA_LOCAL", "planes")
+    else:
+        monkeypatch.setenv("DFTCUDA_LOCAL", "sticks")
     kp = kproblem(name, ecut, k)
     kc = make_context(dz, kp, precision=prec)
     x = random_block(kp.ctx.n, 6, 21)
