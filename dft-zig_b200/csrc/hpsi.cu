@@ -537,6 +537,12 @@ extern "C" int dftcuda_kctx_destroy(dftcuda_kctx* c) {
   c->tc_ptiles_proj.release();
   c->tc_ptiles_back.release();
   if (c->ev_order) cudaEventDestroy(c->ev_order);
+  for (int i = 0; i < kPipeChunks; ++i) {
+    if (c->ev_in[i]) cudaEventDestroy(c->ev_in[i]);
+    if (c->ev_done[i]) cudaEventDestroy(c->ev_done[i]);
+  }
+  if (c->s_in) cudaStreamDestroy(c->s_in);
+  if (c->s_out) cudaStreamDestroy(c->s_out);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return DFTCUDA_OK;
@@ -784,6 +790,42 @@ extern "C" int dftcuda_apply_h_batch(dftcuda_kctx* c, const double* x, double* y
   const double2* xd = (const double2*)x;
   double2* yd = (double2*)y;
   if (!dx || !dy) DFT_TRY(kctx_stage(c, ncols));
+  if (!dx && !dy && ncols >= 64) {
+    // host buffers: kPipeChunks column chunks, chunk j's copy in (s_in) ahead of its compute
+    // (context stream), its copy out (s_out) behind it, so the transfers hide under the compute
+    // of the neighbouring chunks; every wait is an event, every stream is drained before return
+    if (!c->s_in) {
+      DFT_CUDA_TRY(cudaStreamCreateWithFlags(&c->s_in, cudaStreamDefault));
+      DFT_CUDA_TRY(cudaStreamCreateWithFlags(&c->s_out, cudaStreamDefault));
+      for (int i = 0; i < kPipeChunks; ++i) {
+        DFT_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_in[i], cudaEventDisableTiming));
+        DFT_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming));
+      }
+    }
+    const size_t per = (ncols + kPipeChunks - 1) / kPipeChunks;
+    int st = DFTCUDA_OK;
+    for (int j = 0; j < kPipeChunks && st == DFTCUDA_OK; ++j) {
+      const size_t c0 = (size_t)j * per;
+      if (c0 >= ncols) break;
+      const size_t nc = std::min(per, ncols - c0);
+      const size_t off = c0 * n, cb = sizeof(double2) * n * nc;
+      if (cudaMemcpyAsync(c->d_x + off, (const double2*)x + off, cb, cudaMemcpyHostToDevice, c->s_in) != cudaSuccess ||
+          cudaEventRecord(c->ev_in[j], c->s_in) != cudaSuccess || cudaStreamWaitEvent(c->stream, c->ev_in[j], 0) != cudaSuccess) {
+        st = fail(DFTCUDA_ERR_CUDA, "apply_h_batch: staging copy");
+        break;
+      }
+      st = kctx_apply_h_dev(c, c->d_x + off, c->d_y + off, nc, c->stream);
+      if (st != DFTCUDA_OK) break;
+      if (cudaEventRecord(c->ev_done[j], c->stream) != cudaSuccess || cudaStreamWaitEvent(c->s_out, c->ev_done[j], 0) != cudaSuccess ||
+          cudaMemcpyAsync((double2*)y + off, c->d_y + off, cb, cudaMemcpyDeviceToHost, c->s_out) != cudaSuccess)
+        st = fail(DFTCUDA_ERR_CUDA, "apply_h_batch: result copy");
+    }
+    const cudaError_t e1 = cudaStreamSynchronize(c->s_in), e2 = cudaStreamSynchronize(c->stream), e3 = cudaStreamSynchronize(c->s_out);
+    if (st != DFTCUDA_OK) return st;
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) return fail(DFTCUDA_ERR_CUDA, "apply_h_batch: pipelined copies");
+    DFT_TRY(kctx_check_error(c));
+    return DFTCUDA_OK;
+  }
   if (!dx) {
     DFT_CUDA_TRY(cudaMemcpyAsync(c->d_x, x, bytes, cudaMemcpyHostToDevice, c->stream));
     xd = c->d_x;

@@ -76,6 +76,9 @@ struct Profiler {
 
 }  // namespace dftcuda
 
+// Column chunks of a host-buffer H|psi> call (copy in, compute, copy out overlapped).
+constexpr int kPipeChunks = 4;
+
 struct dftcuda_kctx {
   int nx, ny, nz;
   long N;        // nx*ny*nz
@@ -86,6 +89,10 @@ struct dftcuda_kctx {
   cudaStream_t stream = nullptr;
   int device = -1;                  // the CUDA device current when the context was created
   cudaEvent_t ev_order = nullptr;   // orders the context's stream after the caller's legacy-stream work
+  // host-buffer H|psi>: the copies of a column chunk run on their own streams, overlapped with the
+  // compute of the neighbouring chunks (created on first use)
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaEvent_t ev_in[kPipeChunks] = {}, ev_done[kPipeChunks] = {};
   dftcuda::Fft1dPlan fx, fy, fz;
 
   // G-sphere grouped by active x-plane ("slot").
