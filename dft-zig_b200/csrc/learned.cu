@@ -49,7 +49,8 @@ __device__ __forceinline__ double mlp_multiplier(float u0, float z) {
   return tpa_k(fmax(exp((double)u0) - 0.05, 0.0)) * exp((double)zclamp(z));
 }
 
-// Forward for one input with the parameters in shared memory; returns z (before softplus) and
+// Forward for one input with the parameters in shared memory; returns z (the log of the multiplier
+// relative to TPA) and
 // optionally the two hidden layers.
 __device__ __forceinline__ float mlp_forward(const float* __restrict__ p, const float u[3], float* h1, float* h2) {
   float a1[MLP_H];

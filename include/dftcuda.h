@@ -195,8 +195,9 @@ int dftcuda_eig_solve_batch(size_t nk, dftcuda_kctx* const* ctxs, const double* 
 /* Preconditioner of the Davidson correction step for this context's solves:
  *  REFERENCE  q_i = r_i / (diag_i - lambda_b), |den| >= 1e-8 (lobpcg/common.zig:214-226), the default;
  *  TPA        Teter-Payne-Allan K(|k+G_i|^2 / E_kin,b) r_i;
- *  MLP        a learned per-plane-wave multiplier m(|k+G|^2 / E_kin, |r_i| / rms(r), iteration) r_i:
- *             a 3-64-64-1 tanh MLP with softplus output, FP32, params[DFTCUDA_PRECOND_MLP_PARAMS] in
+ *  MLP        a learned per-plane-wave multiplier m = K_TPA(x) exp(z(u)) r_i, z a 3-64-64-1 tanh MLP
+ *             (FP32) of u = (log(x + 0.05), log(|r_i| / rms(r) + 1e-6), iteration / 20), x = |k+G|^2 / E_kin:
+ *             a refinement of TPA (zero output weights give TPA); params[DFTCUDA_PRECOND_MLP_PARAMS] in
  *             the order W1[64][3], b1[64], W2[64][64], b2[64], w3[64], b3 (host or device).
  * diag passed to dftcuda_eig_solve must be the kinetic energies |k+G|^2 for TPA and MLP. */
 #define DFTCUDA_PRECOND_REFERENCE 0
