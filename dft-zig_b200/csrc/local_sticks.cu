@@ -179,11 +179,48 @@ __global__ void __launch_bounds__(kStickThreads) k_stick_fwd(const cplx<T>* __re
 // ------------------------------------------------------------------------------------------
 // Pass 2: one z-plane per CTA.
 // ------------------------------------------------------------------------------------------
+// Exchange layout of the H|psi> z-plane pass's x lines.  The inverse half keeps the [N1][N2] layout
+// (stride N2); the forward half stores its [N2][N1] intermediate with row stride R and each line's
+// buffer spans SF entries, chosen per length so that the 16-byte accesses of a quarter warp fall on
+// distinct bank groups (for 108: 222 wavefronts per line group against 330 with R = N1, S = 113; the
+// forward read with stride N1 = 12 was 3.25-way conflicted).
+struct XStrides {
+  int R, SF;
+};
+constexpr XStrides xline_strides(int n) {
+  switch (n) {
+    case 20: return {5, 20};
+    case 24: return {6, 27};
+    case 27: return {9, 27};
+    case 30: return {9, 45};
+    case 32: return {9, 36};
+    case 36: return {9, 54};
+    case 40: return {9, 45};
+    case 45: return {9, 45};
+    case 48: return {9, 54};
+    case 60: return {17, 85};
+    case 64: return {9, 72};
+    case 72: return {9, 72};
+    case 75: return {17, 85};
+    case 80: return {11, 88};
+    case 90: return {17, 153};
+    case 96: return {13, 104};
+    case 100: return {13, 130};
+    case 108: return {17, 153};
+    case 120: return {13, 130};
+    case 128: return {17, 136};
+    default: return {0, 0};
+  }
+}
+
 template <int NX> struct PlaneXGeom {
   static constexpr int N1 = Split<NX>::N1, N2 = Split<NX>::N2;
   static constexpr int LW = 32 / N2;                                 // lines per warp
   static constexpr int Q = (N1 + N2 - 1) / N2;                       // phase-2 rows per lane
   static constexpr int S = NX + ((N2 - NX) % 8 + 8) % 8;             // exchange stride per line
+  static constexpr int R = xline_strides(NX).R;    // forward row stride (H|psi> pass)
+  static constexpr int SF = xline_strides(NX).SF;  // per-line exchange entries (H|psi> pass)
+  static_assert(R >= N1 && SF >= N2 * R && SF >= NX, "x-line exchange strides");
 };
 
 template <typename T, int N>
@@ -193,7 +230,7 @@ __global__ void __launch_bounds__(plane_max_warps<T>() * 32, 1) k_zplane(cplx<T>
                                                                      int cols_per_cta, const cplx<T>* __restrict__ tw) {
   using C = cplx<T>;
   using G = PlaneXGeom<N>;
-  constexpr int N1 = G::N1, N2 = G::N2, LW = G::LW, QR = G::Q, SX = G::S;
+  constexpr int N1 = G::N1, N2 = G::N2, LW = G::LW, QR = G::Q, SX = G::SF, RF = G::R;
   constexpr int QS = N + 1;  // Q row stride: odd, so lanes over slots hit distinct banks
   extern __shared__ __align__(16) unsigned char smraw[];
   C* Q = reinterpret_cast<C*>(smraw);  // [n_act][QS]
@@ -289,14 +326,14 @@ __global__ void __launch_bounds__(plane_max_warps<T>() * 32, 1) k_zplane(cplx<T>
           for (int kf = 1; kf < N2; ++kf)
             if (k1) u[q][kf] = cmul(u[q][kf], twl<T>(tw, (k1 * kf) % N, (T)-1));
 #pragma unroll
-          for (int kf = 0; kf < N2; ++kf) B[kf * N1 + k1] = u[q][kf];
+          for (int kf = 0; kf < N2; ++kf) B[kf * RF + k1] = u[q][kf];
         }
       }
       __syncwarp();
       {  // forward step B for frequency index t: outputs x = t + N2 m
         C v[N1];
 #pragma unroll
-        for (int tf = 0; tf < N1; ++tf) v[tf] = lane_ok ? B[t * N1 + tf] : mk<C>(0.0, 0.0);
+        for (int tf = 0; tf < N1; ++tf) v[tf] = lane_ok ? B[t * RF + tf] : mk<C>(0.0, 0.0);
         RegDft<T, N1>::run(v, (T)-1);
 #pragma unroll
         for (int m = 0; m < N1; ++m) {
@@ -468,7 +505,7 @@ static size_t stick_smem(size_t cs, int nz) { return cs * (size_t)nz * kStickPad
 template <int N> static int plane_warps(size_t cs, int n_act) {
   using G = PlaneXGeom<N>;
   const size_t q = cs * (size_t)n_act * (N + 1);
-  const size_t per_warp = cs * (size_t)G::LW * G::S;
+  const size_t per_warp = cs * (size_t)G::LW * G::SF;
   const int maxw = cs == sizeof(double2) ? plane_max_warps<double>() : plane_max_warps<float>();
   if (q + per_warp > (size_t)kSmemSticks) return 0;
   return (int)std::min<size_t>(maxw, ((size_t)kSmemSticks - q) / per_warp);
@@ -534,7 +571,7 @@ static int launch_zplane(dftcuda_kctx* c, cplx<T>* S, size_t ncols, cudaStream_t
   const size_t cs = sizeof(cplx<T>);
   const int nw = plane_warps<N>(cs, c->n_act);
   if (nw < 1) return fail(DFTCUDA_ERR_UNSUPPORTED, "z-plane pass does not fit shared memory");
-  const size_t smem = cs * ((size_t)c->n_act * (N + 1) + (size_t)nw * G::LW * G::S);
+  const size_t smem = cs * ((size_t)c->n_act * (N + 1) + (size_t)nw * G::LW * G::SF);
   DFT_TRY(ensure_max_dynamic_smem((const void*)k_zplane<T, N>, (int)smem));
   const T* vn = std::is_same<T, double>::value ? (const T*)c->d_vn : (const T*)c->d_vn32;
   const cplx<T>* tw = std::is_same<T, double>::value ? (const cplx<T>*)c->d_twx64 : (const cplx<T>*)c->d_twx32;
