@@ -9,8 +9,9 @@
 //   2. The nev lowest eigenvalues of T by Sturm-count multisection: one warp per eigenvalue, its
 //      32 lanes evaluate the count at 32 interior points, so the bracket shrinks 33x per round.
 //   3. Eigenvectors of T by inverse iteration on a row-pivoted LU of T - lambda I (three sweeps
-//      from a hashed start vector).  Eigenvalues closer than 1e-5 ||T|| form a group whose vectors
-//      one thread computes in order, re-orthogonalising (modified Gram-Schmidt) after each solve.
+//      from a hashed start vector), one warp per group of eigenvalues closer than 1e-5 ||T||: its
+//      vectors are computed in order, re-orthogonalised (modified Gram-Schmidt, all lanes) after
+//      each solve; one lane runs the recurrences out of shared memory.
 //   4. Back-transformation E = H_0 H_1 ... H_{m-2} Z with the stored reflectors.  Small problems:
 //      one warp per eigenvector, the vector held in shared memory.  From m = 192 and nev = 32 on:
 //      blocks of 64 reflectors in compact WY form (I - V T V^H, as LAPACK's zlarft/zlarfb), each
@@ -87,6 +88,22 @@ __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
+}
+
+// block_sum2 without its leading barrier, for callers in which a block barrier separates every
+// thread's last read of red from this call.
+__device__ double2 block_sum2_free(double2 v, double2* red) {
+  v.x = warp_sum(v.x);
+  v.y = warp_sum(v.y);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double2 t = make_double2(0.0, 0.0);
+  for (int i = 0; i < HT_WARPS; ++i) {
+    t.x += red[i].x;
+    t.y += red[i].y;
+  }
+  return t;
 }
 
 // Sum over the block (HT_THREADS threads), returned to every thread.
@@ -235,6 +252,29 @@ __device__ void block_reflector(double2* x, int n, double2* red, double2& t, dou
   __syncthreads();
 }
 
+// block_reflector with two block barriers instead of four, for callers that wrote x before a block
+// barrier and in which a barrier separates every thread's last read of red from this call: alpha is
+// read before the reduction, so x[0] may be overwritten without a barrier in between.
+__device__ void block_reflector_free(double2* x, int n, double2* red, double2& t, double& beta) {
+  const int tid = threadIdx.x;
+  const double2 alpha = x[0];
+  double2 part = make_double2(0.0, 0.0);
+  for (int i = tid + 1; i < n; i += HT_THREADS) part.x += x[i].x * x[i].x + x[i].y * x[i].y;
+  const double xnorm2 = block_sum2_free(part, red).x;
+  t = make_double2(0.0, 0.0);
+  beta = alpha.x;
+  if (!(xnorm2 == 0.0 && alpha.y == 0.0)) {
+    beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2), alpha.x);
+    t = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+  }
+  const bool active = !(t.x == 0.0 && t.y == 0.0);
+  const double2 den = make_double2(alpha.x - beta, alpha.y);  // v = x / (alpha - beta)
+  const double dn2 = den.x * den.x + den.y * den.y;
+  const double2 sc = active ? make_double2(den.x / dn2, -den.y / dn2) : make_double2(0.0, 0.0);
+  for (int i = tid; i < n; i += HT_THREADS) x[i] = i == 0 ? make_double2(1.0, 0.0) : cmul(x[i], sc);
+  __syncthreads();
+}
+
 // Step 1 with one grid barrier per column.  The update of step k and the matrix-vector product of
 // step k+1 share one sweep over the trailing matrix: every block first applies step k's rank-2
 // update to column k+1 alone (redundantly, from the unmodified global copy) and forms reflector
@@ -308,8 +348,15 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
         colr[q] = i < n1 ? __ldcg(col + i) : make_double2(0.0, 0.0);
       }
     }
-    // (1) y = tau A22 v from the partial products; w = y + alpha v, alpha = -tau (y^H v) / 2
+    // (1) y = tau A22 v from the partial products; w = y + alpha v, alpha = -tau (y^H v) / 2.  Every
+    // thread also forms w_0 itself (the same sums in the same order as the thread that owns entry
+    // 0), so step (2) needs no barrier after the w entries are written; the per-column barriers
+    // are the reduction's, the one before reflector k+1, the reflector's two and the grid's.
+    double2 w0;
     {
+      double2 acc0 = make_double2(0.0, 0.0);
+#pragma unroll 8
+      for (int q = 0; q < S_prev; ++q) acc0 = cadd(acc0, __ldcg(yk + (long)q * m + k + 1));
       double2 p2 = make_double2(0.0, 0.0);
       for (int i = tid; i < n1; i += HT_THREADS) {
         double2 acc = make_double2(0.0, 0.0);
@@ -320,27 +367,27 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
         p2.x += yi.x * vi.x + yi.y * vi.y;
         p2.y += yi.x * vi.y - yi.y * vi.x;
       }
-      const double2 sdot = block_sum2(p2, red);
+      const double2 sdot = block_sum2_free(p2, red);
       const double2 al = cscale(cmul(t, sdot), -0.5);
       for (int i = tid; i < n1; i += HT_THREADS) sw[i] = cadd(sw[i], cmul(al, sv[i]));
+      w0 = cadd(cmul(t, acc0), cmul(al, sv[0]));
       if (blockIdx.x == 0) {
         // column k now holds its reflector (no block reads column k any more)
         double2* cw = A + (long)k * m + (k + 1);
         for (int i = tid; i < n1; i += HT_THREADS) cw[i] = i == 0 ? make_double2(beta, 0.0) : sv[i];
       }
-      __syncthreads();
     }
     // (2) column k+1 after step k's update (rows k+1 .. m-1), its diagonal, and reflector k+1
     const bool next = k + 2 < m;  // a reflector k+1 exists
     double2 tn = make_double2(0.0, 0.0);
     double betan = 0.0;
     {
-      const double2 w0c = cconj(sw[0]);  // v_0 = 1
+      const double2 w0c = cconj(w0);  // v_0 = 1
 #pragma unroll
       for (int q = 0; q < kHtColRegs; ++q) {
         const int i = tid + q * HT_THREADS;
         if (i >= n1) break;
-        const double2 x = csub(colr[q], cadd(cmul(sv[i], w0c), sw[i]));
+        const double2 x = csub(colr[q], cadd(cmul(sv[i], w0c), sw[i]));  // sw[i]: this thread's entry
         if (i == 0) {
           if (blockIdx.x == 0) dd[k + 1] = x.x;
         } else {
@@ -349,7 +396,7 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
       }
       __syncthreads();
       if (next) {
-        block_reflector(sn, n1 - 1, red, tn, betan);
+        block_reflector_free(sn, n1 - 1, red, tn, betan);
         if (blockIdx.x == 0 && tid == 0) {
           ee[k + 1] = betan;
           tau[k + 1] = tn;
@@ -488,142 +535,178 @@ __device__ __forceinline__ double hashed_unit(uint64_t a, uint64_t b) {
   return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;  // [-1, 1)
 }
 
-// Step 3.  Z[:, j] (m x nev, column-major, real) = unit eigenvector of T for w[j].  Thread j works
-// when j starts a group (w[j] - w[j-1] > kGroupTol ||T||) and computes the whole group.  lu holds
-// six arrays of m entries per thread (U's diagonal and two superdiagonals, the multipliers, the
-// row-swap flags, the working vector), interleaved across threads, entry (q, i) of thread j at
-// lu[(q m + i) nev + j], so a warp's accesses at one i are one coalesced transaction.  The sweeps
-// load kIvChunk entries ahead of the recurrence that consumes them.
-__global__ void k_tridiag_invit(const double* __restrict__ dd, const double* __restrict__ ee, int m, int nev,
-                                const double* __restrict__ w, const double* __restrict__ tnorm_p,
-                                double* __restrict__ Z, double* __restrict__ lu) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+// Step 3.  Z[:, j] (m x nev, column-major, real) = unit eigenvector of T for w[j].  One warp (one
+// block) per group of eigenvalues closer than kGroupTol ||T|| to their neighbour (a singleton is a
+// group of one), run by the block whose j starts the group.  The group's vectors are computed in
+// order; after every solve each is re-orthogonalised (modified Gram-Schmidt) against the group's
+// earlier vectors, the 32 lanes sharing the dot products, the updates and the norm.  Lane 0 runs the
+// three recurrences (row-pivoted elimination of T - lambda I, the forward and the back substitution)
+// out of shared memory, which holds, m entries each: the reciprocal pivots, U's two superdiagonals,
+// the multipliers, the working vector (doubles) and the row-swap flags (bytes).  Every sweep loads
+// kIvChunk entries ahead of the recurrence that consumes them.
+constexpr size_t invit_smem(int m) { return (size_t)m * (5 * sizeof(double) + 1); }
+
+__global__ void __launch_bounds__(32) k_tridiag_invit(const double* __restrict__ dd, const double* __restrict__ ee, int m,
+                                                      int nev, const double* __restrict__ w,
+                                                      const double* __restrict__ tnorm_p, double* __restrict__ Z) {
+  extern __shared__ double ism[];
+  const int j = blockIdx.x, lane = threadIdx.x;
   if (j >= nev) return;
   const double tnorm = fmax(*tnorm_p, DBL_MIN);
   const double gtol = kGroupTol * tnorm;
   if (j > 0 && !(w[j] - w[j - 1] > gtol)) return;
   int jend = j + 1;
   while (jend < nev && !(w[jend] - w[jend - 1] > gtol)) ++jend;
-  const size_t st = (size_t)nev;
-  double* const u0 = lu + j;
-  double* const u1 = u0 + (size_t)m * st;
-  double* const u2 = u1 + (size_t)m * st;
-  double* const lm = u2 + (size_t)m * st;
-  double* const sw = lm + (size_t)m * st;
-  double* const zz = sw + (size_t)m * st;
+  double* const rp = ism;      // 1 / U's diagonal
+  double* const u1 = rp + m;   // U's first superdiagonal
+  double* const u2 = u1 + m;   // U's second superdiagonal (nonzero after a row swap)
+  double* const lm = u2 + m;   // elimination multipliers
+  double* const zz = lm + m;   // working vector
+  unsigned char* const swp = reinterpret_cast<unsigned char*>(zz + m);  // row i swapped with i+1
   const double tiny = DBL_EPSILON * tnorm;
   for (int p = j; p < jend; ++p) {
     const double lam = w[p];
-    // Row-pivoted elimination of T - lam I.  cur = (a, b): the running row at columns (i, i+1).
-    double a = dd[0] - lam, b = m > 1 ? ee[0] : 0.0;
-    for (int i = 0; i + 1 < m; ++i) {
-      const double sub = ee[i], dn = dd[i + 1] - lam, up = i + 2 < m ? ee[i + 1] : 0.0;
-      const size_t o = (size_t)i * st;
-      if (fabs(a) >= fabs(sub)) {
-        const double piv = fabs(a) < tiny ? (a < 0.0 ? -tiny : tiny) : a;
-        const double l = sub / piv;
-        u0[o] = piv; u1[o] = b; u2[o] = 0.0; lm[o] = l; sw[o] = 0.0;
-        a = dn - l * b;
-        b = up;
-      } else {
-        const double l = a / sub;
-        u0[o] = sub; u1[o] = dn; u2[o] = up; lm[o] = l; sw[o] = 1.0;
-        a = b - l * dn;
-        b = -l * up;
-      }
-    }
-    u0[(size_t)(m - 1) * st] = fabs(a) < tiny ? (a < 0.0 ? -tiny : tiny) : a;
-    u1[(size_t)(m - 1) * st] = 0.0;  // the back substitution reads row m-1's superdiagonals
-    u2[(size_t)(m - 1) * st] = 0.0;
-    // zz holds the vector up to the factor scl (the previous sweep's normalisation, applied as the
-    // next sweep reads it); the first sweep starts from a hashed vector
-    double scl = 1.0;
-    for (int sweep = 0; sweep < 3; ++sweep) {
-      auto rhs = [&](int i) { return sweep == 0 ? hashed_unit((uint64_t)p, (uint64_t)i) : zz[(size_t)i * st] * scl; };
-      // forward: the same row operations on the right-hand side (entry i+1 is read before
-      // entry i is written, so a chunk's loads may all precede its stores)
-      double cb = rhs(0);
+    if (lane == 0) {
+      // Row-pivoted elimination of T - lam I.  (a, b): the running row at columns (i, i+1).
+      double a = dd[0] - lam, b = m > 1 ? ee[0] : 0.0;
       for (int i0 = 0; i0 + 1 < m; i0 += kIvChunk) {
         const int n = min(kIvChunk, m - 1 - i0);
-        double zn[kIvChunk], lv[kIvChunk], sv[kIvChunk];
+        double sb[kIvChunk], dn[kIvChunk], up[kIvChunk];
 #pragma unroll
         for (int c = 0; c < kIvChunk; ++c) {
           if (c < n) {
-            const size_t o = (size_t)(i0 + c) * st;
-            zn[c] = rhs(i0 + c + 1);
-            lv[c] = lm[o];
-            sv[c] = sw[o];
+            const int i = i0 + c;
+            sb[c] = __ldg(ee + i);
+            dn[c] = __ldg(dd + i + 1) - lam;
+            up[c] = i + 2 < m ? __ldg(ee + i + 1) : 0.0;
           }
         }
 #pragma unroll
         for (int c = 0; c < kIvChunk; ++c) {
           if (c < n) {
-            const size_t o = (size_t)(i0 + c) * st;
-            if (sv[c] == 0.0) {
-              zz[o] = cb;
-              cb = zn[c] - lv[c] * cb;
+            const int i = i0 + c;
+            if (fabs(a) >= fabs(sb[c])) {
+              const double piv = fabs(a) < tiny ? (a < 0.0 ? -tiny : tiny) : a;
+              const double l = sb[c] / piv;
+              rp[i] = 1.0 / piv; u1[i] = b; u2[i] = 0.0; lm[i] = l; swp[i] = 0;
+              a = dn[c] - l * b;
+              b = up[c];
             } else {
-              zz[o] = zn[c];
-              cb = cb - lv[c] * zn[c];
+              const double l = a / sb[c];
+              rp[i] = 1.0 / sb[c]; u1[i] = dn[c]; u2[i] = up[c]; lm[i] = l; swp[i] = 1;
+              a = b - l * dn[c];
+              b = -l * up[c];
             }
           }
         }
       }
-      zz[(size_t)(m - 1) * st] = cb;
-      // back substitution with U (diagonal + two superdiagonals), z[i+1], z[i+2] carried; the
-      // squared norm and the entry of largest magnitude (first in index order) on the way
-      double zp1 = 0.0, zp2 = 0.0, nrm = 0.0, big = -1.0, bigv = 0.0;
-      for (int i1 = m; i1 > 0; i1 -= kIvChunk) {
-        const int n = min(kIvChunk, i1);
-        double zr[kIvChunk], d0[kIvChunk], d1[kIvChunk], d2[kIvChunk];
+      rp[m - 1] = 1.0 / (fabs(a) < tiny ? (a < 0.0 ? -tiny : tiny) : a);
+      u1[m - 1] = 0.0;  // the back substitution reads row m-1's superdiagonals
+      u2[m - 1] = 0.0;
+    }
+    // zz holds the vector up to the factor scl (the previous sweep's normalisation, applied as the
+    // next sweep reads it); the first sweep starts from a hashed vector
+    double scl = 1.0;
+    for (int sweep = 0; sweep < 3; ++sweep) {
+      double nrm = 0.0, bigv = 0.0;
+      if (lane == 0) {
+        auto rhs = [&](int i) { return sweep == 0 ? hashed_unit((uint64_t)p, (uint64_t)i) : zz[i] * scl; };
+        // forward: the same row operations on the right-hand side (entry i+1 is read before entry
+        // i is written, so a chunk's loads may all precede its stores)
+        double cb = rhs(0);
+        for (int i0 = 0; i0 + 1 < m; i0 += kIvChunk) {
+          const int n = min(kIvChunk, m - 1 - i0);
+          double zn[kIvChunk], lv[kIvChunk];
+          unsigned char sv[kIvChunk];
 #pragma unroll
-        for (int c = 0; c < kIvChunk; ++c) {
-          if (c < n) {
-            const size_t o = (size_t)(i1 - 1 - c) * st;
-            zr[c] = zz[o];
-            d0[c] = u0[o];
-            d1[c] = u1[o];
-            d2[c] = u2[o];
+          for (int c = 0; c < kIvChunk; ++c) {
+            if (c < n) {
+              zn[c] = rhs(i0 + c + 1);
+              lv[c] = lm[i0 + c];
+              sv[c] = swp[i0 + c];
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < kIvChunk; ++c) {
+            if (c < n) {
+              if (sv[c] == 0) {
+                zz[i0 + c] = cb;
+                cb = zn[c] - lv[c] * cb;
+              } else {
+                zz[i0 + c] = zn[c];
+                cb = cb - lv[c] * zn[c];
+              }
+            }
           }
         }
+        zz[m - 1] = cb;
+        // back substitution with U (diagonal + two superdiagonals), z[i+1], z[i+2] carried; the
+        // squared norm and the entry of largest magnitude (first in index order) on the way
+        double zp1 = 0.0, zp2 = 0.0, big = -1.0;
+        for (int i1 = m; i1 > 0; i1 -= kIvChunk) {
+          const int n = min(kIvChunk, i1);
+          double zr[kIvChunk], r0[kIvChunk], d1[kIvChunk], d2[kIvChunk];
 #pragma unroll
-        for (int c = 0; c < kIvChunk; ++c) {
-          if (c < n) {
-            const double x = (zr[c] - d1[c] * zp1 - d2[c] * zp2) / d0[c];
-            zz[(size_t)(i1 - 1 - c) * st] = x;
-            nrm += x * x;
-            if (fabs(x) >= big) { big = fabs(x); bigv = x; }
-            zp2 = zp1;
-            zp1 = x;
+          for (int c = 0; c < kIvChunk; ++c) {
+            if (c < n) {
+              const int i = i1 - 1 - c;
+              zr[c] = zz[i];
+              r0[c] = rp[i];
+              d1[c] = u1[i];
+              d2[c] = u2[i];
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < kIvChunk; ++c) {
+            if (c < n) {
+              const double x = (zr[c] - d1[c] * zp1 - d2[c] * zp2) * r0[c];
+              zz[i1 - 1 - c] = x;
+              nrm += x * x;
+              if (fabs(x) >= big) { big = fabs(x); bigv = x; }
+              zp2 = zp1;
+              zp1 = x;
+            }
           }
         }
       }
+      __syncwarp();
       if (p > j) {
-        // modified Gram-Schmidt against the group's earlier vectors, then the norm again
+        // modified Gram-Schmidt against the group's earlier vectors (written by this warp), then the
+        // norm and the first entry of largest magnitude again
         for (int q = j; q < p; ++q) {
           const double* zq = Z + (size_t)q * m;
           double dot = 0.0;
-#pragma unroll 8
-          for (int i = 0; i < m; ++i) dot += zq[i] * zz[(size_t)i * st];
-#pragma unroll 8
-          for (int i = 0; i < m; ++i) zz[(size_t)i * st] -= dot * zq[i];
+          for (int i = lane; i < m; i += 32) dot += zq[i] * zz[i];
+          dot = warp_sum(dot);
+          for (int i = lane; i < m; i += 32) zz[i] -= dot * zq[i];
+          __syncwarp();
         }
+        double big = -1.0;
+        int bi = m;
         nrm = 0.0;
-        big = -1.0;
         bigv = 0.0;
-#pragma unroll 8
-        for (int i = 0; i < m; ++i) {
-          const double zi = zz[(size_t)i * st];
+        for (int i = lane; i < m; i += 32) {
+          const double zi = zz[i];
           nrm += zi * zi;
-          if (fabs(zi) > big) { big = fabs(zi); bigv = zi; }
+          if (fabs(zi) > big) { big = fabs(zi); bigv = zi; bi = i; }
         }
+        nrm = warp_sum(nrm);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ob = __shfl_xor_sync(0xffffffffu, big, o), ov = __shfl_xor_sync(0xffffffffu, bigv, o);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+          if (ob > big || (ob == big && oi < bi)) { big = ob; bigv = ov; bi = oi; }
+        }
+      } else {
+        nrm = __shfl_sync(0xffffffffu, nrm, 0);
+        bigv = __shfl_sync(0xffffffffu, bigv, 0);
       }
       scl = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
       if (bigv < 0.0) scl = -scl;
     }
     double* z = Z + (size_t)p * m;
-#pragma unroll 8
-    for (int i = 0; i < m; ++i) z[i] = zz[(size_t)i * st] * scl;
+    for (int i = lane; i < m; i += 32) z[i] = zz[i] * scl;
+    __syncwarp();
   }
 }
 
@@ -840,8 +923,8 @@ static size_t wy_elems(int m, int nev) {
 
 size_t heev_work_bytes(int m, int nev) {
   const size_t mm = (size_t)m;
-  return 256 * 9 + sizeof(double) * (3 * mm + 1) + sizeof(double2) * (1 + 2 * kHtMaxSplit) * mm + sizeof(double) * mm * nev +
-         sizeof(double) * 6 * mm * nev + sizeof(double2) * wy_elems(m, nev);
+  return 256 * 8 + sizeof(double) * (3 * mm + 1) + sizeof(double2) * (1 + 2 * kHtMaxSplit) * mm + sizeof(double) * mm * nev +
+         sizeof(double2) * wy_elems(m, nev);
 }
 
 void heev_bind(HeevWork& w, void* base, int m, int nev) {
@@ -855,7 +938,6 @@ void heev_bind(HeevWork& w, void* base, int m, int nev) {
   w.tau = (double2*)take(sizeof(double2) * m);
   w.y = (double2*)take(sizeof(double2) * m * 2 * kHtMaxSplit);  // two halves for the one-barrier form
   w.z = (double*)take(sizeof(double) * (size_t)m * nev);
-  w.lu = (double*)take(sizeof(double) * 6 * (size_t)m * nev);
   w.wy_ws_elems = wy_ws_elems(nev);
   w.wy = (double2*)take(sizeof(double2) * wy_elems(m, nev));
   w.m_cap = m;
@@ -879,6 +961,7 @@ int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde,
   DFT_TRY(ensure_max_dynamic_smem(hetrd_fn, (int)smem_tr));
   DFT_TRY(ensure_max_dynamic_smem((const void*)k_hetrd_back, (int)(sizeof(double2) * BT_WARPS * 2048)));
   DFT_TRY(ensure_max_dynamic_smem((const void*)k_wy_t_all, (int)kWyTSmem));
+  DFT_TRY(ensure_max_dynamic_smem((const void*)k_tridiag_invit, (int)invit_smem(2048)));
   // SM count and the reduction kernel's occupancy, per device (several host threads may ask at once)
   static std::mutex occ_mu;
   static std::map<int, std::pair<int, int>> occ;
@@ -927,7 +1010,7 @@ int heev_lowest(double2* A, int m, int nev, double* evals, double2* E, long lde,
   }
   k_tridiag_bisect<<<ceil_div(nev, BS_WARPS), BS_WARPS * 32, sizeof(double) * 2 * m, s>>>(w.d, w.e, m, nev, evals, w.tnorm);
   count_launch();
-  k_tridiag_invit<<<ceil_div(nev, 64), 64, 0, s>>>(w.d, w.e, m, nev, evals, w.tnorm, w.z, w.lu);
+  k_tridiag_invit<<<nev, 32, invit_smem(m), s>>>(w.d, w.e, m, nev, evals, w.tnorm, w.z);
   count_launch();
   if (m >= 192 && nev >= 32) {
     DFT_TRY(heev_back_blocked(A, w.tau, m, nev, w.z, E, lde, w, s));

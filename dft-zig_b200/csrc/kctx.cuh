@@ -206,7 +206,6 @@ struct HeevWork {
   double2* tau = nullptr;   // reflector scalars (m)
   double2* y = nullptr;     // tau A v (m)
   double* z = nullptr;      // eigenvectors of T (m x nev)
-  double* lu = nullptr;     // inverse-iteration factors and working vectors (6 m per eigenvalue)
   double2* wy = nullptr;    // blocked back-transformation: V block, G, T, two W blocks, GEMM split-K space
   size_t wy_ws_elems = 0;   // the split-K part of wy (complex elements)
   size_t m_cap = 0, nev_cap = 0;

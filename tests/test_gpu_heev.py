@@ -54,6 +54,18 @@ def test_degenerate_spectrum(dz):
     _check(a, dz.hermitian_eigen_decomp(a, 45), 45)
 
 
+def test_large_eigenvalue_clusters(dz):
+    """Groups beyond a warp: 40 equal eigenvalues and 12 within 1e-9 of each other, between spread
+    singletons, so the inverse iteration re-orthogonalises long groups."""
+    rng = np.random.default_rng(5)
+    n = 400
+    q, _ = np.linalg.qr(rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n)))
+    d = np.sort(np.r_[np.linspace(-3.0, 8.0, n - 52), np.full(40, 0.5), 2.0 + 1e-9 * np.arange(12)])
+    a = q @ np.diag(d) @ q.conj().T
+    a = (a + a.conj().T) / 2
+    _check(a, dz.hermitian_eigen_decomp(a, 240), 240)
+
+
 def test_diagonal_and_identity(dz):
     a = np.diag(np.r_[np.full(6, 2.0), np.full(5, -1.0), [0.5]]).astype(np.complex128)
     _check(a, dz.hermitian_eigen_decomp(a), 12)
