@@ -90,22 +90,6 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// block_sum2 without its leading barrier, for callers in which a block barrier separates every
-// thread's last read of red from this call.
-__device__ double2 block_sum2_free(double2 v, double2* red) {
-  v.x = warp_sum(v.x);
-  v.y = warp_sum(v.y);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) red[w] = v;
-  __syncthreads();
-  double2 t = make_double2(0.0, 0.0);
-  for (int i = 0; i < HT_WARPS; ++i) {
-    t.x += red[i].x;
-    t.y += red[i].y;
-  }
-  return t;
-}
-
 // Sum over the block (HT_THREADS threads), returned to every thread.
 __device__ double2 block_sum2(double2 v, double2* red) {
   v.x = warp_sum(v.x);
@@ -252,29 +236,6 @@ __device__ void block_reflector(double2* x, int n, double2* red, double2& t, dou
   __syncthreads();
 }
 
-// block_reflector with two block barriers instead of four, for callers that wrote x before a block
-// barrier and in which a barrier separates every thread's last read of red from this call: alpha is
-// read before the reduction, so x[0] may be overwritten without a barrier in between.
-__device__ void block_reflector_free(double2* x, int n, double2* red, double2& t, double& beta) {
-  const int tid = threadIdx.x;
-  const double2 alpha = x[0];
-  double2 part = make_double2(0.0, 0.0);
-  for (int i = tid + 1; i < n; i += HT_THREADS) part.x += x[i].x * x[i].x + x[i].y * x[i].y;
-  const double xnorm2 = block_sum2_free(part, red).x;
-  t = make_double2(0.0, 0.0);
-  beta = alpha.x;
-  if (!(xnorm2 == 0.0 && alpha.y == 0.0)) {
-    beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2), alpha.x);
-    t = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
-  }
-  const bool active = !(t.x == 0.0 && t.y == 0.0);
-  const double2 den = make_double2(alpha.x - beta, alpha.y);  // v = x / (alpha - beta)
-  const double dn2 = den.x * den.x + den.y * den.y;
-  const double2 sc = active ? make_double2(den.x / dn2, -den.y / dn2) : make_double2(0.0, 0.0);
-  for (int i = tid; i < n; i += HT_THREADS) x[i] = i == 0 ? make_double2(1.0, 0.0) : cmul(x[i], sc);
-  __syncthreads();
-}
-
 // Step 1 with one grid barrier per column.  The update of step k and the matrix-vector product of
 // step k+1 share one sweep over the trailing matrix: every block first applies step k's rank-2
 // update to column k+1 alone (redundantly, from the unmodified global copy) and forms reflector
@@ -348,15 +309,8 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
         colr[q] = i < n1 ? __ldcg(col + i) : make_double2(0.0, 0.0);
       }
     }
-    // (1) y = tau A22 v from the partial products; w = y + alpha v, alpha = -tau (y^H v) / 2.  Every
-    // thread also forms w_0 itself (the same sums in the same order as the thread that owns entry
-    // 0), so step (2) needs no barrier after the w entries are written; the per-column barriers
-    // are the reduction's, the one before reflector k+1, the reflector's two and the grid's.
-    double2 w0;
+    // (1) y = tau A22 v from the partial products; w = y + alpha v, alpha = -tau (y^H v) / 2
     {
-      double2 acc0 = make_double2(0.0, 0.0);
-#pragma unroll 8
-      for (int q = 0; q < S_prev; ++q) acc0 = cadd(acc0, __ldcg(yk + (long)q * m + k + 1));
       double2 p2 = make_double2(0.0, 0.0);
       for (int i = tid; i < n1; i += HT_THREADS) {
         double2 acc = make_double2(0.0, 0.0);
@@ -367,27 +321,27 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
         p2.x += yi.x * vi.x + yi.y * vi.y;
         p2.y += yi.x * vi.y - yi.y * vi.x;
       }
-      const double2 sdot = block_sum2_free(p2, red);
+      const double2 sdot = block_sum2(p2, red);
       const double2 al = cscale(cmul(t, sdot), -0.5);
       for (int i = tid; i < n1; i += HT_THREADS) sw[i] = cadd(sw[i], cmul(al, sv[i]));
-      w0 = cadd(cmul(t, acc0), cmul(al, sv[0]));
       if (blockIdx.x == 0) {
         // column k now holds its reflector (no block reads column k any more)
         double2* cw = A + (long)k * m + (k + 1);
         for (int i = tid; i < n1; i += HT_THREADS) cw[i] = i == 0 ? make_double2(beta, 0.0) : sv[i];
       }
+      __syncthreads();
     }
     // (2) column k+1 after step k's update (rows k+1 .. m-1), its diagonal, and reflector k+1
     const bool next = k + 2 < m;  // a reflector k+1 exists
     double2 tn = make_double2(0.0, 0.0);
     double betan = 0.0;
     {
-      const double2 w0c = cconj(w0);  // v_0 = 1
+      const double2 w0c = cconj(sw[0]);  // v_0 = 1
 #pragma unroll
       for (int q = 0; q < kHtColRegs; ++q) {
         const int i = tid + q * HT_THREADS;
         if (i >= n1) break;
-        const double2 x = csub(colr[q], cadd(cmul(sv[i], w0c), sw[i]));  // sw[i]: this thread's entry
+        const double2 x = csub(colr[q], cadd(cmul(sv[i], w0c), sw[i]));
         if (i == 0) {
           if (blockIdx.x == 0) dd[k + 1] = x.x;
         } else {
@@ -396,7 +350,7 @@ __global__ void __launch_bounds__(HT_THREADS) k_hetrd1(double2* __restrict__ A, 
       }
       __syncthreads();
       if (next) {
-        block_reflector_free(sn, n1 - 1, red, tn, betan);
+        block_reflector(sn, n1 - 1, red, tn, betan);
         if (blockIdx.x == 0 && tid == 0) {
           ee[k + 1] = betan;
           tau[k + 1] = tn;

@@ -780,6 +780,30 @@ extern "C" int dftcuda_apply_h_batch_async(dftcuda_kctx* c, const double* x, dou
   return kctx_apply_h_dev(c, (const double2*)x, (double2*)y, ncols, s);
 }
 
+// Column chunks of the host-buffer pipeline (len[0 .. returned count)).  Only the first chunk's copy
+// in and the last chunk's copy out are not hidden under compute, so from 256 columns on the end
+// chunks are 64 columns (one column tile of the projector GEMMs) and the middle ones multiples of 64
+// (the last takes the remainder), at most kPipeChunks in all; below 256 columns, four equal chunks.
+static int pipe_chunks(size_t ncols, size_t* len) {
+  int k = 0;
+  if (ncols < 256) {
+    const size_t per = (ncols + 3) / 4;
+    for (size_t c0 = 0; c0 < ncols; c0 += per) len[k++] = std::min(per, ncols - c0);
+    return k;
+  }
+  const size_t mid = ncols - 128;
+  const size_t nm = std::min<size_t>(kPipeChunks - 2, (mid + 127) / 128);
+  const size_t per = ((mid + nm - 1) / nm + 63) / 64 * 64;
+  len[k++] = 64;
+  for (size_t left = mid; left > 0;) {
+    const size_t t = std::min(per, left);
+    len[k++] = t;
+    left -= t;
+  }
+  len[k++] = 64;
+  return k;
+}
+
 extern "C" int dftcuda_apply_h_batch(dftcuda_kctx* c, const double* x, double* y, size_t n, size_t ncols) {
   if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "apply_h_batch: null context");
   if (n != c->npw) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "apply_h_batch: n != n_pw");  // apply.zig:1591
@@ -802,12 +826,12 @@ extern "C" int dftcuda_apply_h_batch(dftcuda_kctx* c, const double* x, double* y
         DFT_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming));
       }
     }
-    const size_t per = (ncols + kPipeChunks - 1) / kPipeChunks;
+    size_t len[kPipeChunks];
+    const int nchunks = pipe_chunks(ncols, len);
     int st = DFTCUDA_OK;
-    for (int j = 0; j < kPipeChunks && st == DFTCUDA_OK; ++j) {
-      const size_t c0 = (size_t)j * per;
-      if (c0 >= ncols) break;
-      const size_t nc = std::min(per, ncols - c0);
+    size_t c0 = 0;
+    for (int j = 0; j < nchunks && st == DFTCUDA_OK; c0 += len[j], ++j) {
+      const size_t nc = len[j];
       const size_t off = c0 * n, cb = sizeof(double2) * n * nc;
       if (cudaMemcpyAsync(c->d_x + off, (const double2*)x + off, cb, cudaMemcpyHostToDevice, c->s_in) != cudaSuccess ||
           cudaEventRecord(c->ev_in[j], c->s_in) != cudaSuccess || cudaStreamWaitEvent(c->stream, c->ev_in[j], 0) != cudaSuccess) {

@@ -77,7 +77,7 @@ struct Profiler {
 }  // namespace dftcuda
 
 // Column chunks of a host-buffer H|psi> call (copy in, compute, copy out overlapped).
-constexpr int kPipeChunks = 4;
+constexpr int kPipeChunks = 8;
 
 struct dftcuda_kctx {
   int nx, ny, nz;

@@ -111,8 +111,9 @@ int dftcuda_set_projectors(dftcuda_kctx* ctx, size_t n_species, const dftcuda_sp
 
 /* y = H x for ncols columns: Operator.apply_batch = apply_hamiltonian_batched (apply.zig:1584-1618).
  * x, y: [n x ncols] column-major complex128, host or device.  n must equal n_pw.  With host x and y
- * and 64 columns or more the call runs four column chunks whose copies in and out overlap the
- * compute of their neighbours (pinned host memory lets the copies run asynchronously); it returns
+ * and 64 columns or more the call runs column chunks whose copies in and out overlap the compute of
+ * their neighbours (four equal chunks below 256 columns; from 256 on, 64-column chunks at both ends
+ * and up to six in between); pinned host memory lets the copies run asynchronously.  It returns
  * when y is complete. */
 int dftcuda_apply_h_batch(dftcuda_kctx* ctx, const double* x, double* y, size_t n, size_t ncols);
 /* Single column: Operator.apply = apply_hamiltonian (apply.zig:643-658). */

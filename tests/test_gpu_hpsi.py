@@ -54,6 +54,24 @@ def test_apply_many_columns_chunked(dz):
     kc.close()
 
 
+def test_host_pipeline_uneven_chunks(dz):
+    """From 256 host columns the copies run in 64-column end chunks around larger middle chunks
+    (here 64, 128, 44, 64): every column equals the device-pointer path, the end chunks the oracle."""
+    import torch
+
+    kp = kproblem("si8", 20.0)
+    kc = make_context(dz, kp)
+    x = random_block(kp.ctx.n, 300, 4)
+    y = kc.apply_hamiltonian_batched(x)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.empty_like(xd)
+    kc.apply_hamiltonian_batched(xd, yd, kp.ctx.n, 300)
+    assert rel_err(y, yd.cpu().numpy()) < 1e-13
+    for cols in (slice(0, 6), slice(190, 196), slice(294, 300)):
+        assert rel_err(y[cols], kp.ctx.apply_batch(x[cols])) < 1e-11
+    kc.close()
+
+
 @pytest.mark.parametrize("name,ecut,k", CASES[:3])
 def test_apply_batched_fp32_passes(dz, name, ecut, k):
     kp = kproblem(name, ecut, k)
