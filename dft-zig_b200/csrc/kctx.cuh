@@ -116,7 +116,8 @@ struct dftcuda_kctx {
   int last_layout = -1;      // layout of the last H|psi>: 0 generic passes, 1 plane layout, 2 stick layout
   int split_proj = 0, split_back = 0;  // autotuner choices for the projector GEMMs (0 = heuristic)
   int precond_kind = 0;                // DFTCUDA_PRECOND_* of the Davidson correction step
-  float* d_mlp = nullptr;              // learned preconditioner weights (DFTCUDA_PRECOND_MLP_PARAMS)
+  float* d_mlp = nullptr;              // learned preconditioner weights (DFTCUDA_PRECOND_MLP_PARAMS), then its z table
+  double mlp_table_t = -1.0;           // iteration input the z table was built for (-1: none)
   double* d_vstage = nullptr;          // host V(r) staging (N doubles)
   int* d_pwmap = nullptr;      // [n_act][nz][ny] plane-wave index or -1
   int* d_stick_off = nullptr;  // [n_act+1]

@@ -20,6 +20,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "kctx.cuh"
@@ -112,6 +114,73 @@ __global__ void k_precondition_tpa(double2* __restrict__ Q, const double2* __res
   const double f = num / (num + 16.0 * x * x * x * x);
   const double2 v = res[(long)band[j] * n + i];
   Q[idx] = make_double2(v.x * f, v.y * f);
+}
+
+// Inference through a table (the default).  The network's output z depends on the entry only through
+// (u0, u1); u2 = t/20 is fixed within a call.  So each call (or the first call at a new t) tabulates z
+// with the FP32 network of the training kernels (mlp_forward) on a kLutN0 x kLutN1 grid over
+// u0 in [kLutU0, kLutU0Hi] (x from 0 to about 1100) and u1 in [kLutU1, kLutU1Hi] (|r_i| / rms(r) from
+// 0 to about 1100), and every entry interpolates the table bilinearly: for the trained weights
+// |dz| <= 5e-5 over the grid (the tensor-core form below moves z by ~1e-3).  An entry outside the
+// grid evaluates the network itself.  DFTCUDA_MLP_INFER=tc selects the tensor-core form.
+constexpr int kLutN0 = 256, kLutN1 = 512;
+constexpr float kLutU0 = -3.0f, kLutU0Hi = 7.0f, kLutU1 = -13.85f, kLutU1Hi = 7.0f;
+constexpr int kMlpParamPad = (MLP_NPARAM + 63) / 64 * 64;  // the table starts 256-byte aligned
+
+__global__ void __launch_bounds__(128) k_mlp_table(const float* __restrict__ params, double t, float* __restrict__ lut) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= kLutN0 * kLutN1) return;
+  const int a = idx / kLutN1, b = idx - a * kLutN1;
+  float u[3];
+  u[0] = kLutU0 + (kLutU0Hi - kLutU0) * (float)a / (float)(kLutN0 - 1);
+  u[1] = kLutU1 + (kLutU1Hi - kLutU1) * (float)b / (float)(kLutN1 - 1);
+  u[2] = (float)fmin(t / 20.0, 2.0);
+  lut[idx] = mlp_forward(params, u, nullptr, nullptr);
+}
+
+// The network for an entry outside the table, kept out of line so that the table path keeps a small
+// register footprint.
+__device__ __noinline__ float mlp_forward_outside(const float* __restrict__ params, float u0, float u1, float u2) {
+  const float u[3] = {u0, u1, u2};
+  return mlp_forward(params, u, nullptr, nullptr);
+}
+
+__global__ void __launch_bounds__(256, 4) k_precondition_lut(double2* __restrict__ Q, const double2* __restrict__ res,
+                                                          const double* __restrict__ kin, const double* __restrict__ ekin,
+                                                          const double* __restrict__ norms, const int* __restrict__ band,
+                                                          int k, long n, double t, const float* __restrict__ lut,
+                                                          const float* __restrict__ params) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= (long)k * n) return;
+  const int j = (int)(idx / n);
+  const long i = idx - (long)j * n;
+  const int b = band[j];
+  const double2 v = res[(long)b * n + i];
+  float u[3];
+  mlp_features(kin[i], ekin[j], sqrt(v.x * v.x + v.y * v.y), norms[b] / sqrt((double)n), t, u);
+  constexpr float s0 = (float)(kLutN0 - 1) / (kLutU0Hi - kLutU0), s1 = (float)(kLutN1 - 1) / (kLutU1Hi - kLutU1);
+  const float f0 = (u[0] - kLutU0) * s0, f1 = (u[1] - kLutU1) * s1;
+  float z;
+  if (f0 >= 0.f && f0 < (float)(kLutN0 - 1) && f1 >= 0.f && f1 < (float)(kLutN1 - 1)) {
+    const int i0 = (int)f0, i1 = (int)f1;
+    const float a = f0 - (float)i0, c = f1 - (float)i1;
+    const float* r0 = lut + i0 * kLutN1 + i1;
+    const float z0 = fmaf(c, __ldg(r0 + 1) - __ldg(r0), __ldg(r0));
+    const float z1 = fmaf(c, __ldg(r0 + kLutN1 + 1) - __ldg(r0 + kLutN1), __ldg(r0 + kLutN1));
+    z = fmaf(a, z1 - z0, z0);
+  } else {
+    z = mlp_forward_outside(params, u[0], u[1], u[2]);
+  }
+  const double m = mlp_multiplier(u[0], z);
+  Q[idx] = make_double2(v.x * m, v.y * m);
+}
+
+static bool mlp_infer_tc() {
+  static const bool v = [] {
+    const char* e = std::getenv("DFTCUDA_MLP_INFER");
+    return e && std::strcmp(e, "tc") == 0;
+  }();
+  return v;
 }
 
 // Inference (the Davidson preconditioner) over tiles of MLP_TE plane-wave entries.  The first layer
@@ -475,8 +544,9 @@ extern "C" int dftcuda_kctx_set_preconditioner(dftcuda_kctx* c, int kind, const 
   if (kind == DFTCUDA_PRECOND_MLP) {
     if (!params || nparams != (size_t)MLP_NPARAM)
       return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_preconditioner: the MLP needs DFTCUDA_PRECOND_MLP_PARAMS weights");
-    if (!c->d_mlp && cudaMalloc(&c->d_mlp, sizeof(float) * MLP_NPARAM) != cudaSuccess)
+    if (!c->d_mlp && cudaMalloc(&c->d_mlp, sizeof(float) * (kMlpParamPad + (size_t)kLutN0 * kLutN1)) != cudaSuccess)
       return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_preconditioner: weights");
+    c->mlp_table_t = -1.0;
     DFT_CUDA_TRY(cudaMemcpyAsync(c->d_mlp, params, sizeof(float) * MLP_NPARAM,
                                  is_device_pointer(params) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
     DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -561,7 +631,15 @@ int precondition_launch(dftcuda_kctx* c, double2* Q, const double2* res, const d
     count_launch();
     if (c->precond_kind == DFTCUDA_PRECOND_TPA)
       k_precondition_tpa<<<grid, 256, 0, s>>>(Q, res, kin, ekin_ws, band, take, n);
-    else {
+    else if (!mlp_infer_tc()) {
+      float* lut = c->d_mlp + kMlpParamPad;
+      if (c->mlp_table_t != t) {
+        k_mlp_table<<<ceil_div((size_t)kLutN0 * kLutN1, 128), 128, 0, s>>>(c->d_mlp, t, lut);
+        count_launch();
+        c->mlp_table_t = t;
+      }
+      k_precondition_lut<<<grid, 256, 0, s>>>(Q, res, kin, ekin_ws, norms, band, take, n, t, lut, c->d_mlp);
+    } else {
       // tiles of MLP_TE entries, up to eight blocks per SM (about three resident)
       int dev = 0, nsm = 148;
       DFT_CUDA_TRY(cudaGetDevice(&dev));

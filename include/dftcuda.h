@@ -202,7 +202,10 @@ int dftcuda_eig_solve_batch(size_t nk, dftcuda_kctx* const* ctxs, const double* 
  *  MLP        a learned per-plane-wave multiplier m = K_TPA(x) exp(z(u)) r_i, z a 3-64-64-1 tanh MLP
  *             (FP32) of u = (log(x + 0.05), log(|r_i| / rms(r) + 1e-6), iteration / 20), x = |k+G|^2 / E_kin:
  *             a refinement of TPA (zero output weights give TPA); params[DFTCUDA_PRECOND_MLP_PARAMS] in
- *             the order W1[64][3], b1[64], W2[64][64], b2[64], w3[64], b3 (host or device).
+ *             the order W1[64][3], b1[64], W2[64][64], b2[64], w3[64], b3 (host or device).  The
+ *             solver evaluates z through a 256 x 512 table of the network over (u0, u1) per
+ *             iteration (bilinear, |dz| <= 5e-5 for the shipped weights; the network itself outside
+ *             u0 in [-3, 7], u1 in [-13.85, 7]); DFTCUDA_MLP_INFER=tc evaluates it per entry instead.
  * diag passed to dftcuda_eig_solve must be the kinetic energies |k+G|^2 for TPA and MLP. */
 #define DFTCUDA_PRECOND_REFERENCE 0
 #define DFTCUDA_PRECOND_TPA 1

@@ -122,6 +122,53 @@ def test_trained_preconditioner_gain(dz, seed):
     assert mlp.h_applies < tpa.h_applies
 
 
+_INFER_SCRIPT = """
+import json, sys
+import numpy as np
+sys.path.insert(0, {root!r})
+import importlib
+import dftzig_loader
+dz = dftzig_loader.load()
+learn = importlib.import_module("dftzig_b200.learn")
+system = importlib.import_module("dftzig_b200.system")
+c = system.crystal("sitrain", 1290)
+nb = int(round(c.nelec / 2))
+inp = system.kpoint_inputs(c, 25.0, (0.0, 0.0, 0.0))
+kc = learn._context(dz, inp)
+kc.set_preconditioner(dz.PRECOND_MLP, learn.load_precond_weights())
+r = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, nb, dz.Options(max_iter=400, tol=1e-6))
+kc.close()
+print(json.dumps({{"values": list(map(float, r.values)), "h_applies": int(r.h_applies), "converged": bool(r.converged)}}))
+"""
+
+
+def test_mlp_table_inference_matches_tensor_core_form():
+    """The default inference interpolates a table of the FP32 network (|dz| <= 5e-5); the tensor-core
+    form (DFTCUDA_MLP_INFER=tc) evaluates the network per entry with TF32 operands.  Both steer the
+    Davidson solve of a held-out cell to the same eigenvalues in about the same number of H
+    applications."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = {}
+    for mode in ("table", "tc"):
+        env = dict(os.environ)
+        env.pop("DFTCUDA_MLP_INFER", None)
+        if mode == "tc":
+            env["DFTCUDA_MLP_INFER"] = "tc"
+        r = subprocess.run([sys.executable, "-c", _INFER_SCRIPT.format(root=root)], env=env, capture_output=True,
+                           text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[mode] = json.loads(r.stdout.strip().splitlines()[-1])
+    a, b = out["table"], out["tc"]
+    assert a["converged"] and b["converged"]
+    assert np.abs(np.array(a["values"]) - np.array(b["values"])).max() < 1e-7
+    assert abs(a["h_applies"] - b["h_applies"]) <= 0.05 * b["h_applies"]
+
+
 def test_trained_fno_start_beats_atomic_superposition(dz):
     """The committed FNO on a held-out SiGe8 cell: its first density is far closer to the converged
     SCF density than the atomic superposition it starts from."""
