@@ -447,6 +447,8 @@ __global__ void __launch_bounds__(kCiWarps * 32) k_chol_inv(const double2* __res
 
 // ------------------------------------------------------------------------------------------
 
+constexpr size_t kVTileCacheBytes = (size_t)8 << 30;  // both V tile caches of one context
+
 struct KCtxImpl {
   size_t n = 0, max_sub = 0, nb = 0, kmax = 0;
   double2 *V = nullptr, *W = nullptr, *ritz = nullptr, *res = nullptr, *Q = nullptr, *Q2 = nullptr;
@@ -462,6 +464,12 @@ struct KCtxImpl {
   bool rr_tc = false;  // Rayleigh-Ritz products on the tensor cores (3xTF32), TF32/TF32X3 contexts
   int* err = nullptr;  // the context's tensor-core error flag
   TcScratch* tcs = nullptr;  // the context's pre-split operand buffer
+  // Pre-split tiles of V[0:m] in its two roles (the Gram operand V^H, and the combination V C), kept
+  // while V[0:m] is unchanged: the Rayleigh-Ritz products and both orthonormalisation passes of an
+  // iteration read the same V[0:m], so each role is split once per iteration instead of three times.
+  // Used when both fit kVTileCacheBytes; invalidated wherever V's leading columns are rewritten.
+  TcScratch vt_gram, vt_comb;
+  bool v_cache = false;
   double tc_min_flops = 0.0;  // smaller products take the FP64 GEMM (dftcuda_kctx::tc_min_flops)
   // pinned host mirrors of the per-iteration read-backs
   void* pinned = nullptr;
@@ -471,6 +479,8 @@ struct KCtxImpl {
 
 void eig_destroy(KCtxImpl* e) {
   if (!e) return;
+  e->vt_gram.release();
+  e->vt_comb.release();
   if (e->all) cudaFree(e->all);
   if (e->ws) cudaFree(e->ws);
   if (e->heev_mem) cudaFree(e->heev_mem);
@@ -553,6 +563,7 @@ static int gram(KCtxImpl* e, const double2* X, int mx, const double2* Y, int my,
   GemmArgs g{};
   g.M = mx; g.N = my; g.K = (int)e->n;
   g.A = X; g.lda = (long)e->n; g.a_kc = true; g.conj_a = true;
+  if (e->v_cache && X == e->V) g.a_cache = &e->vt_gram;
   g.B = Y; g.ldb = (long)e->n; g.b_kc = true; g.conj_b = false;
   g.O = out; g.ldo_r = 1; g.ldo_c = ldo;
   g.alpha = 1.0; g.beta = 0.0;
@@ -566,6 +577,7 @@ static int combine(KCtxImpl* e, const double2* X, int mx, const double2* C, int 
   g.M = ncols; g.N = (int)e->n; g.K = mx;
   g.A = C; g.lda = ldc; g.a_kc = true; g.conj_a = false;
   g.B = X; g.ldb = (long)e->n; g.b_kc = false; g.conj_b = false;
+  if (e->v_cache && X == e->V) g.b_cache = &e->vt_comb;
   g.O = out; g.ldo_r = (long)e->n; g.ldo_c = 1;
   g.alpha = alpha; g.beta = beta;
   return gemm_dispatch(e, g, rr, s);
@@ -670,10 +682,22 @@ static int small_eig(KCtxImpl* e, int m, int nev, cudaStream_t s) {
   return DFTCUDA_OK;
 }
 
+// V's leading columns were rewritten: the tiles cached from them are stale.
+static void v_changed(KCtxImpl* e) {
+  e->vt_gram.valid = false;
+  e->vt_comb.valid = false;
+}
+
 // orthonormalize_all (common.zig:298-312) for V[0:m]: block Gram-Schmidt; columns that drop are
 // replaced by fresh LCG vectors (the reference's retry) and the block is redone, at most 3 times.
+// Every caller has just written V[0:m] (start, restart), and this rewrites it.
 static int orthonormalize_all(dftcuda_kctx* c, int m, uint64_t& seed, cudaStream_t s) {
   KCtxImpl* e = c->eig;
+  struct Invalidate {
+    KCtxImpl* e;
+    ~Invalidate() { v_changed(e); }
+  } inv{e};
+  v_changed(e);
   const long n = (long)e->n;
   for (int attempt = 0; attempt < 4; ++attempt) {
     DFT_CUDA_TRY(cudaMemcpyAsync(e->Q, e->V, sizeof(double2) * n * m, cudaMemcpyDeviceToDevice, s));
@@ -760,6 +784,16 @@ static int run_init(EigRun& r, const double* diag, const double* init_vecs, size
   }
   e->err = c->d_err;
   e->tcs = &c->tc_scratch;
+  v_changed(e);
+  if (e->rr_tc && !e->v_cache) {
+    const size_t bg = tc4_operand_bytes((int)e->max_sub, (int)n, true), bc = tc4_operand_bytes((int)n, (int)e->max_sub, true);
+    if (bg + bc <= kVTileCacheBytes && e->vt_gram.ensure(bg) == DFTCUDA_OK && e->vt_comb.ensure(bc) == DFTCUDA_OK) {
+      e->v_cache = true;
+    } else {
+      e->vt_gram.release();
+      e->vt_comb.release();
+    }
+  }
   e->tc_min_flops = c->tc_min_flops;
   const char* gram_mode = std::getenv("DFTCUDA_GRAM");
   r.gram_full = gram_mode && std::strcmp(gram_mode, "full") == 0;

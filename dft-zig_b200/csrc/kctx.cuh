@@ -45,6 +45,8 @@ int cgemm_tf32(const GemmArgs& g, cudaStream_t s, double2* workspace, size_t wor
 inline bool precision_uses_tc(int p) { return p == DFTCUDA_PRECISION_TF32 || p == DFTCUDA_PRECISION_TF32X3; }
 inline bool tc_worthwhile(int M, int N, int K, double min_flops) { return 8.0 * M * (double)N * K >= min_flops; }
 size_t cgemm_tf32_workspace_elems(int M, int N, int K);
+// Bytes of one operand's pre-split tiles (R rows of K entries) in the wide tensor-core GEMM.
+size_t tc4_operand_bytes(int R, int K, bool split);
 
 struct NonlocalDev {
   int nproj = 0;                 // sum over atoms of m_total(species)

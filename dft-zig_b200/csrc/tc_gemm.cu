@@ -1257,6 +1257,11 @@ static TcPlan tc_plan(const GemmArgs& g0) {
   return p;
 }
 
+size_t tc4_operand_bytes(int R, int K, bool split) {
+  const size_t KS = ((size_t)K + 7) / 8, RG = ((size_t)R + 255) / 256 * 32;
+  return KS * t4_planes(split) * RG * 256;
+}
+
 size_t cgemm_tf32_workspace_elems(int M, int N, int K) {
   GemmArgs g{};
   g.M = M; g.N = N; g.K = K; g.ldo_r = 1; g.ldo_c = M;
