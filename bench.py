@@ -142,6 +142,7 @@ def parse():
                     help="scf216: instead of time-to-SCF, run N SCF steps of each arm and print its kernel-time "
                          "table (CUPTI activity records through torch.profiler)")
     ap.add_argument("--eig-iters", type=int, default=6, help="Davidson iterations of --workload eig")
+    ap.add_argument("--eig-tol", type=float, default=1e-9, help="residual tolerance of --workload eig")
     ap.add_argument("--eig-cell", choices=("si64", "si216"), default="si64", help="cell of --workload eig")
     ap.add_argument("--cells", type=int, default=16, help="cells of the many-cell workload")
     ap.add_argument("--cells-starts", default="atomic,fno", help="starting densities of the many-cell workload (comma list)")
@@ -947,12 +948,13 @@ def run_eig_workload(args):
     kc.set_profiling(True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    r = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, nb, dz.Options(max_iter=args.eig_iters, tol=1e-9))
+    r = kc.hermitian_eigen_decomp_iterative(inp.basis.kinetic, nb, dz.Options(max_iter=args.eig_iters, tol=args.eig_tol))
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     pr = kc.profile()
     kc.close()
     print(json.dumps({"metric": f"Davidson solve wall time, {cell} Gamma {ecut:g} Ry {nb} bands ({args.precision})", "value": round(wall * 1e3, 2), "unit": "ms",
+                      "preconditioner": args.eig_precond, "tol": args.eig_tol, "converged": bool(r.converged),
                       "iterations": r.iterations, "h_applies": r.h_applies, "apply_h_ms": round(pr["apply_h_ns"] / 1e6, 2),
                       "subspace_ms": round(pr["subspace_ns"] / 1e6, 2)}), flush=True)
 
