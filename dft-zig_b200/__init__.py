@@ -36,6 +36,7 @@ ABI_SYMBOLS = (
     "dftcuda_last_error_message",
     "dftcuda_device_count",
     "dftcuda_debug_set_wait_limits",
+    "dftcuda_debug_fail_alloc",
     "dftcuda_fermi_occupations",
     "dftcuda_ionic_potential_radial",
     "dftcuda_nonlocal_stress",
@@ -259,6 +260,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lb = ct.c_long
     lib.dftcuda_complex_gemm.argtypes = [ip, sz, sz, sz, vp, lb, ip, ip, vp, lb, ip, ip, vp, lb, lb, ct.c_double, ct.c_double]
     lib.dftcuda_debug_set_wait_limits.argtypes = [lb, ip]
+    lib.dftcuda_debug_fail_alloc.argtypes = [lb]
     lib.dftcuda_fermi_occupations.argtypes = [sz, sz, dp, dp, ct.c_double, ct.c_double, ct.c_double, dp, dp, dp]
     lib.dftcuda_nonlocal_stress.argtypes = [vp, dp, sz, ct.POINTER(ct.c_void_p), dp, sz, sz, dp, dp]
     lib.dftcuda_ionic_potential_radial.argtypes = [vp, ip, vp, vp, vp, vp, vp, ip, vp, vp, ct.c_double, dp, dp]
@@ -824,6 +826,13 @@ def debug_set_wait_limits(polls: int = 0, unreachable: bool = False):
     the subspace eigensolver's grid-barrier poll budget, unreachable makes every barrier wait run it
     out (the call then raises Timeout).  debug_set_wait_limits() restores the defaults."""
     _check(load_library().dftcuda_debug_set_wait_limits(int(polls), 1 if unreachable else 0))
+
+
+def debug_fail_alloc(after: int = -1):
+    """Failure injection for the out-of-memory path (dftcuda_debug_fail_alloc): after >= 0 makes the
+    after-th following device allocation of the library fail once (the call that makes it raises
+    OutOfMemory); debug_fail_alloc() cancels a planned failure."""
+    _check(load_library().dftcuda_debug_fail_alloc(int(after)))
 
 
 def _is_torch_cuda(a) -> bool:

@@ -244,7 +244,7 @@ struct SetupEngine {
     if (buf) cudaFree(buf);
     buf = nullptr;
     cap = 0;
-    if (cudaMalloc(&buf, bytes) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "setup engine: buffer");
+    if (dev_malloc(&buf, bytes) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "setup engine: buffer");
     cap = bytes;
     return DFTCUDA_OK;
   }

@@ -71,6 +71,18 @@ inline unsigned ceil_div(size_t a, size_t b) { return (unsigned)((a + b - 1) / b
 uint64_t launches_total();
 void count_launch(int n = 1);
 
+// Every device allocation of the library goes through dev_malloc.  dftcuda_debug_fail_alloc(k) makes
+// the k-th following one fail once, as cudaMalloc does when the device is out of memory, so that
+// tests can check that each entry point reports DFTCUDA_ERR_OUT_OF_MEMORY and keeps its context usable.
+bool alloc_should_fail();
+template <typename T> inline cudaError_t dev_malloc(T** p, size_t bytes) {
+  if (alloc_should_fail()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(reinterpret_cast<void**>(p), bytes);
+}
+
 // True when p is device (or managed) memory, false for host memory (pageable or pinned).
 bool is_device_pointer(const void* p);
 

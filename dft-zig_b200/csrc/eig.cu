@@ -507,7 +507,7 @@ static int eig_alloc(dftcuda_kctx* c, size_t n, size_t max_sub, size_t nb) {
   const size_t oev = take(sizeof(double) * max_sub), onr = take(sizeof(double) * nb), odg = take(sizeof(double) * n);
   const size_t oek = take(sizeof(double) * kmax);
   const size_t obd = take(sizeof(int) * kmax), okp = take(sizeof(int) * kmax), ost = take(sizeof(int) * 4);
-  if (cudaMalloc(&e->all, off) != cudaSuccess) {
+  if (dev_malloc(&e->all, off) != cudaSuccess) {
     eig_destroy(e);
     c->eig = nullptr;
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "eigensolver workspace");
@@ -530,15 +530,20 @@ static int eig_alloc(dftcuda_kctx* c, size_t n, size_t max_sub, size_t nb) {
   need = std::max(need, cgemm_tf32_workspace_elems(ms, (int)kmax, (int)n));
   need = std::max(need, cgemm_tf32_workspace_elems((int)kmax, (int)n, ms));
   need = std::max(need, cgemm_tf32_workspace_elems((int)kmax, (int)kmax, (int)n));
+  // a workspace that could not be completed is dropped, so the next call allocates it afresh
+  auto out_of_memory = [&](const char* what) {
+    eig_destroy(e);
+    c->eig = nullptr;
+    return fail(DFTCUDA_ERR_OUT_OF_MEMORY, what);
+  };
   if (need) {
-    if (cudaMalloc(&e->ws, need * sizeof(double2)) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "eig gemm ws");
+    if (dev_malloc(&e->ws, need * sizeof(double2)) != cudaSuccess) return out_of_memory("eig gemm ws");
     e->ws_elems = need;
   }
-  if (cudaMalloc(&e->heev_mem, heev_work_bytes(ms, (int)nb)) != cudaSuccess)
-    return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "eig heev ws");
+  if (dev_malloc(&e->heev_mem, heev_work_bytes(ms, (int)nb)) != cudaSuccess) return out_of_memory("eig heev ws");
   heev_bind(e->hw, e->heev_mem, ms, (int)nb);
   const size_t pin_bytes = sizeof(double) * 2 * nb + sizeof(int) * (8 + kmax);
-  if (cudaMallocHost(&e->pinned, pin_bytes) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "eig pinned host buffers");
+  if (cudaMallocHost(&e->pinned, pin_bytes) != cudaSuccess) return out_of_memory("eig pinned host buffers");
   e->h_ev = (double*)e->pinned;
   e->h_nr = e->h_ev + nb;
   e->h_st = (int*)(e->h_nr + nb);
@@ -779,7 +784,7 @@ static int run_init(EigRun& r, const double* diag, const double* init_vecs, size
   KCtxImpl* e = r.e = c->eig;
   e->rr_tc = precision_uses_tc(c->precision);
   if (e->rr_tc && !c->d_err) {
-    DFT_CUDA_TRY(cudaMalloc(&c->d_err, sizeof(int)));
+    DFT_CUDA_TRY(dev_malloc(&c->d_err, sizeof(int)));
     DFT_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
   }
   e->err = c->d_err;

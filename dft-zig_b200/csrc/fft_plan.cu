@@ -69,7 +69,7 @@ int Fft1dPlan::create(int n) {
   std::vector<float2> tw32(tw.size());
   for (size_t i = 0; i < tw.size(); ++i) tw32[i] = make_float2((float)tw[i].x, (float)tw[i].y);
   const size_t b64 = tw.size() * sizeof(double2), b32 = tw.size() * sizeof(float2), bp = n * sizeof(int);
-  DFT_CUDA_TRY(cudaMalloc(&d_buf, b64 + b32 + bp + 64));
+  DFT_CUDA_TRY(dev_malloc(&d_buf, b64 + b32 + bp + 64));
   char* base = (char*)d_buf;
   // A pageable-host cudaMemcpy may return before its DMA lands; synchronise the device before the
   // tables are used.
@@ -258,7 +258,7 @@ extern "C" int dftcuda_fft3d(dftcuda_fft_plan* pl, double* data, int direction) 
   const bool dev = is_device_pointer(data);
   double2* d = (double2*)data;
   if (!dev) {
-    if (!pl->staging) DFT_CUDA_TRY(cudaMalloc(&pl->staging, N * sizeof(double2)));
+    if (!pl->staging) DFT_CUDA_TRY(dev_malloc(&pl->staging, N * sizeof(double2)));
     d = pl->staging;
     DFT_CUDA_TRY(cudaMemcpyAsync(d, data, N * sizeof(double2), cudaMemcpyHostToDevice, pl->stream));
   }

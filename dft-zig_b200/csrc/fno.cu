@@ -253,7 +253,7 @@ static int fno_alloc(FnoWork& w, long nmax, int dmax) {
   const size_t oca = take(sizeof(float2) * FNO_W * (size_t)dmax * dmax * FNO_M), ocb = take(sizeof(float2) * FNO_W * (size_t)dmax * FNO_M * FNO_M),
                owh = take(sizeof(float2) * FNO_W * FNO_K), og = take(sizeof(float) * FNO_W * nmax), og2 = take(sizeof(float) * FNO_W * nmax),
                oo = take(sizeof(float) * nmax), ot = take(sizeof(float2) * FNO_M * 3 * dmax);
-  if (cudaMalloc(&w.mem, o) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "fno workspace");
+  if (dev_malloc(&w.mem, o) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "fno workspace");
   char* b = (char*)w.mem;
   for (int l = 0; l <= FNO_L; ++l) w.v[l] = (float*)(b + ov[l]);
   for (int l = 0; l < FNO_L; ++l) {
@@ -389,7 +389,7 @@ static int fno_upload(FnoSet& d, size_t ns, const int* dims, const size_t* offs,
   const size_t ou = take(sizeof(float) * FNO_IN * tot), ot = t ? take(sizeof(float) * tot) : 0, oP = take(sizeof(float) * FNO_NPARAM),
                odP = take(sizeof(float) * FNO_NPARAM), o1 = take(sizeof(float) * FNO_NPARAM), o2 = take(sizeof(float) * FNO_NPARAM),
                ol = take(sizeof(double));
-  if (cudaMalloc(&d.mem, o) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "fno data");
+  if (dev_malloc(&d.mem, o) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "fno data");
   char* b = (char*)d.mem;
   d.u = (float*)(b + ou); d.t = t ? (float*)(b + ot) : nullptr; d.P = (float*)(b + oP); d.dP = (float*)(b + odP);
   d.m1 = (float*)(b + o1); d.m2 = (float*)(b + o2); d.loss = (double*)(b + ol);
@@ -490,7 +490,7 @@ extern "C" int dftcuda_fno_train(size_t nsamples, const int* dims, const size_t*
     double* dh = nullptr;
     st = fno_upload(d, nsamples, dims, offs, u, target, params, s);
     if (st == DFTCUDA_OK) st = fno_alloc(w, d.nmax, d.dmax);
-    if (st == DFTCUDA_OK && steps && cudaMalloc(&dh, sizeof(double) * steps) != cudaSuccess)
+    if (st == DFTCUDA_OK && steps && dev_malloc(&dh, sizeof(double) * steps) != cudaSuccess)
       st = fail(DFTCUDA_ERR_OUT_OF_MEMORY, "fno_train: history");
     for (size_t it = 0; it < steps && st == DFTCUDA_OK; ++it) {
       st = fno_loss_grad(d, w, s);

@@ -1006,10 +1006,10 @@ extern "C" int dftcuda_hermitian_eigen_decomp(size_t n, const double* a, size_t 
     }
   } g{s};
   const size_t mat = sizeof(double2) * n * n;
-  DFT_CUDA_TRY(cudaMalloc(&g.p[0], mat));
-  DFT_CUDA_TRY(cudaMalloc(&g.p[1], mat + sizeof(double2) * n * nev + sizeof(double) * nev + 256));
-  DFT_CUDA_TRY(cudaMalloc(&g.p[2], heev_work_bytes(m, k)));
-  DFT_CUDA_TRY(cudaMalloc(&g.p[3], 256));
+  DFT_CUDA_TRY(dev_malloc(&g.p[0], mat));
+  DFT_CUDA_TRY(dev_malloc(&g.p[1], mat + sizeof(double2) * n * nev + sizeof(double) * nev + 256));
+  DFT_CUDA_TRY(dev_malloc(&g.p[2], heev_work_bytes(m, k)));
+  DFT_CUDA_TRY(dev_malloc(&g.p[3], 256));
   double2* src = (double2*)g.p[0];
   double2* A = (double2*)g.p[1];
   double2* E = A + n * n;

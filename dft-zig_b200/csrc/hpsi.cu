@@ -276,7 +276,7 @@ static int ensure_box(dftcuda_kctx* c, size_t cols, bool apply) {
   if (c->d_box) cudaFree(c->d_box);
   c->d_box = nullptr;
   c->box_bytes = 0;
-  if (cudaMalloc(&c->d_box, bytes) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "box workspace");
+  if (dev_malloc(&c->d_box, bytes) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "box workspace");
   c->box_bytes = bytes;
   return DFTCUDA_OK;
 }
@@ -320,7 +320,7 @@ int kctx_ensure_coef(dftcuda_kctx* c, size_t cols) {
     c->d_coef = c->d_coef2 = nullptr;
     c->coef_cols = 0;
     const size_t b = sizeof(double2) * (size_t)c->nl.nproj * cols;
-    if (cudaMalloc(&c->d_coef, b) != cudaSuccess || cudaMalloc(&c->d_coef2, b) != cudaSuccess)
+    if (dev_malloc(&c->d_coef, b) != cudaSuccess || dev_malloc(&c->d_coef2, b) != cudaSuccess)
       return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "projector coefficients");
     c->coef_cols = cols;
   }
@@ -330,7 +330,7 @@ int kctx_ensure_coef(dftcuda_kctx* c, size_t cols) {
     need = std::max(need, cgemm_tf32_workspace_elems(c->nl.nproj, (int)cols, (int)c->npw));
     need = std::max(need, cgemm_tf32_workspace_elems((int)cols, (int)c->npw, c->nl.nproj));
     if (!c->d_err) {
-      if (cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "error flag");
+      if (dev_malloc(&c->d_err, sizeof(int)) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "error flag");
       DFT_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
       DFT_CUDA_TRY(cudaStreamSynchronize(c->stream));
     }
@@ -342,7 +342,7 @@ int kctx_ensure_coef(dftcuda_kctx* c, size_t cols) {
     if (c->d_gemm_ws) cudaFree(c->d_gemm_ws);
     c->d_gemm_ws = nullptr;
     c->gemm_ws_elems = 0;
-    if (cudaMalloc(&c->d_gemm_ws, need * sizeof(double2)) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "gemm workspace");
+    if (dev_malloc(&c->d_gemm_ws, need * sizeof(double2)) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "gemm workspace");
     c->gemm_ws_elems = need;
   }
   return DFTCUDA_OK;
@@ -497,7 +497,7 @@ int kctx_stage(dftcuda_kctx* c, size_t cols) {
   c->d_x = c->d_y = nullptr;
   c->stage_cols = 0;
   const size_t b = sizeof(double2) * c->npw * cols;
-  if (cudaMalloc(&c->d_x, b) != cudaSuccess || cudaMalloc(&c->d_y, b) != cudaSuccess)
+  if (dev_malloc(&c->d_x, b) != cudaSuccess || dev_malloc(&c->d_y, b) != cudaSuccess)
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "staging buffers");
   c->stage_cols = cols;
   return DFTCUDA_OK;
@@ -612,14 +612,14 @@ extern "C" int dftcuda_kctx_create(dftcuda_kctx** out, int nx, int ny, int nz, d
   std::vector<int> slot_xpos(c->n_act);
   for (int sidx = 0; sidx < c->n_act; ++sidx) slot_xpos[sidx] = c->fx.pinv[xs[sidx]];
   c->h_kinetic.assign(kinetic, kinetic + n_pw);
-  bool ok = cudaMalloc(&c->d_plane_off, sizeof(int) * (c->n_act + 1)) == cudaSuccess &&
-            cudaMalloc(&c->d_pw_idx, sizeof(int) * n_pw) == cudaSuccess &&
-            cudaMalloc(&c->d_pw_spos, sizeof(int) * n_pw) == cudaSuccess &&
-            cudaMalloc(&c->d_slot_xpos, sizeof(int) * c->n_act) == cudaSuccess &&
-            cudaMalloc(&c->d_kinetic, sizeof(double) * n_pw) == cudaSuccess &&
-            cudaMalloc(&c->d_gcart, sizeof(double) * 3 * n_pw) == cudaSuccess &&
-            cudaMalloc(&c->d_vt, sizeof(double) * c->N) == cudaSuccess &&
-            cudaMalloc(&c->d_vt32, sizeof(float) * c->N) == cudaSuccess;
+  bool ok = dev_malloc(&c->d_plane_off, sizeof(int) * (c->n_act + 1)) == cudaSuccess &&
+            dev_malloc(&c->d_pw_idx, sizeof(int) * n_pw) == cudaSuccess &&
+            dev_malloc(&c->d_pw_spos, sizeof(int) * n_pw) == cudaSuccess &&
+            dev_malloc(&c->d_slot_xpos, sizeof(int) * c->n_act) == cudaSuccess &&
+            dev_malloc(&c->d_kinetic, sizeof(double) * n_pw) == cudaSuccess &&
+            dev_malloc(&c->d_gcart, sizeof(double) * 3 * n_pw) == cudaSuccess &&
+            dev_malloc(&c->d_vt, sizeof(double) * c->N) == cudaSuccess &&
+            dev_malloc(&c->d_vt32, sizeof(float) * c->N) == cudaSuccess;
   if (!ok) {
     dftcuda_kctx_destroy(c);
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "kctx_create: device tables");
@@ -658,7 +658,7 @@ extern "C" int dftcuda_set_vloc(dftcuda_kctx* c, const double* v) {
   const bool dev = is_device_pointer(v);
   // A staging buffer kept in the context: cudaFree would synchronise the whole device (every other
   // k-point's stream) on each SCF iteration.
-  if (!dev && !c->d_vstage && cudaMalloc(&c->d_vstage, sizeof(double) * c->N) != cudaSuccess)
+  if (!dev && !c->d_vstage && dev_malloc(&c->d_vstage, sizeof(double) * c->N) != cudaSuccess)
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_vloc staging");
   if (!dev) DFT_CUDA_TRY(cudaMemcpyAsync(c->d_vstage, v, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
   k_transpose_vloc<<<ceil_div(c->N, 256), 256, 0, c->stream>>>(dev ? v : c->d_vstage, c->d_vt, c->d_vt32, c->nx, c->ny, c->nz,
@@ -708,7 +708,7 @@ extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const d
   nl.maxm = maxm;
   std::vector<double> D((size_t)nproj * maxm, 0.0);
   std::vector<int> poff(nproj), pmt(nproj);
-  if (cudaMalloc(&nl.P, sizeof(double2) * (size_t)nproj * c->npw) != cudaSuccess) {
+  if (dev_malloc(&nl.P, sizeof(double2) * (size_t)nproj * c->npw) != cudaSuccess) {
     free_nonlocal(c);
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_projectors: projector matrix");
   }
@@ -736,7 +736,7 @@ extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const d
         const double d = sp.dij[b * sp.beta_count + j];
         for (int mi = 0; mi < 2 * sp.l_list[b] + 1; ++mi) dm[(size_t)(moff[b] + mi) * mt + moff[j] + mi] = d;
       }
-    if (cudaMalloc(&dphi, sizeof(double) * (size_t)mt * c->npw) != cudaSuccess) {
+    if (dev_malloc(&dphi, sizeof(double) * (size_t)mt * c->npw) != cudaSuccess) {
       free_nonlocal(c);
       return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_projectors: phi");
     }
@@ -759,9 +759,9 @@ extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const d
     cudaFree(dphi);
     dphi = nullptr;
   }
-  bool ok = cudaMalloc(&nl.D, sizeof(double) * D.size()) == cudaSuccess &&
-            cudaMalloc(&nl.proj_off, sizeof(int) * nproj) == cudaSuccess &&
-            cudaMalloc(&nl.proj_mt, sizeof(int) * nproj) == cudaSuccess;
+  bool ok = dev_malloc(&nl.D, sizeof(double) * D.size()) == cudaSuccess &&
+            dev_malloc(&nl.proj_off, sizeof(int) * nproj) == cudaSuccess &&
+            dev_malloc(&nl.proj_mt, sizeof(int) * nproj) == cudaSuccess;
   if (!ok) {
     free_nonlocal(c);
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_projectors: tables");
@@ -966,8 +966,8 @@ extern "C" int dftcuda_nonlocal_forces(dftcuda_kctx* c, const double* vectors, s
     if (d_w) cudaFree(d_w);
     if (d_F) cudaFree(d_F);
   };
-  if (cudaMalloc(&d_row, sizeof(int) * 2 * (size_t)natoms) != cudaSuccess || cudaMalloc(&d_w, sizeof(double) * nbands) != cudaSuccess ||
-      cudaMalloc(&d_F, sizeof(double) * 3 * (size_t)natoms) != cudaSuccess) {
+  if (dev_malloc(&d_row, sizeof(int) * 2 * (size_t)natoms) != cudaSuccess || dev_malloc(&d_w, sizeof(double) * nbands) != cudaSuccess ||
+      dev_malloc(&d_F, sizeof(double) * 3 * (size_t)natoms) != cudaSuccess) {
     cleanup();
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "nonlocal_forces: buffers");
   }
@@ -1092,10 +1092,10 @@ extern "C" int dftcuda_nonlocal_stress(dftcuda_kctx* c, const double* kpg, size_
   };
   size_t max_mt = 0;
   for (size_t mt : c->species_mt) max_mt = std::max(max_mt, mt);
-  if (cudaMalloc(&DP, sizeof(double2) * 3 * (size_t)nproj * n) != cudaSuccess ||
-      cudaMalloc(&d_tab, sizeof(double) * 3 * max_mt * n) != cudaSuccess || cudaMalloc(&d_kpg, sizeof(double) * 3 * n) != cudaSuccess ||
-      cudaMalloc(&d_w, sizeof(double) * nbands) != cudaSuccess || cudaMalloc(&d_acc, sizeof(double) * 7) != cudaSuccess ||
-      cudaMalloc(&d_u, sizeof(double2) * (size_t)nproj * nch) != cudaSuccess) {
+  if (dev_malloc(&DP, sizeof(double2) * 3 * (size_t)nproj * n) != cudaSuccess ||
+      dev_malloc(&d_tab, sizeof(double) * 3 * max_mt * n) != cudaSuccess || dev_malloc(&d_kpg, sizeof(double) * 3 * n) != cudaSuccess ||
+      dev_malloc(&d_w, sizeof(double) * nbands) != cudaSuccess || dev_malloc(&d_acc, sizeof(double) * 7) != cudaSuccess ||
+      dev_malloc(&d_u, sizeof(double2) * (size_t)nproj * nch) != cudaSuccess) {
     cleanup();
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "nonlocal_stress: buffers");
   }
@@ -1192,13 +1192,13 @@ extern "C" int dftcuda_accumulate_density(dftcuda_kctx* c, const double* vectors
   for (size_t i = 0; i < keep.size(); ++i) kw[i] = hw[keep[i]];
   if (keep.size() > c->w_cap) {
     if (c->d_w) cudaFree(c->d_w);
-    if (cudaMalloc(&c->d_w, sizeof(double) * keep.size()) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "weights");
+    if (dev_malloc(&c->d_w, sizeof(double) * keep.size()) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "weights");
     c->w_cap = keep.size();
   }
   DFT_CUDA_TRY(cudaMemcpyAsync(c->d_w, kw.data(), sizeof(double) * kw.size(), cudaMemcpyHostToDevice, c->stream));
   double* rd = rho;
   if (!dr) {
-    if (!c->d_rho && cudaMalloc(&c->d_rho, sizeof(double) * c->N) != cudaSuccess)
+    if (!c->d_rho && dev_malloc(&c->d_rho, sizeof(double) * c->N) != cudaSuccess)
       return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "rho staging");
     DFT_CUDA_TRY(cudaMemcpyAsync(c->d_rho, rho, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
     rd = c->d_rho;

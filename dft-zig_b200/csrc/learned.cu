@@ -504,7 +504,7 @@ static int mlp_upload(MlpData& d, size_t nbands, size_t npw, const int* off, con
                ow = take(sizeof(float) * npw), od = take(sizeof(float) * nbands), os = take(sizeof(double) * 3 * nbands),
                ol = take(sizeof(double)), op = take(sizeof(float) * MLP_NPARAM), og = take(sizeof(float) * MLP_NPARAM),
                o1 = take(sizeof(float) * MLP_NPARAM), o2 = take(sizeof(float) * MLP_NPARAM);
-  if (cudaMalloc(&d.mem, o) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "precond_mlp: training data");
+  if (dev_malloc(&d.mem, o) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "precond_mlp: training data");
   char* b = (char*)d.mem;
   d.off = (int*)(b + oo); d.feat = (float*)(b + of); d.cc = (float2*)(b + oc); d.w = (float*)(b + ow);
   d.dn = (float*)(b + od); d.sums = (double*)(b + os); d.loss = (double*)(b + ol); d.params = (float*)(b + op);
@@ -544,7 +544,7 @@ extern "C" int dftcuda_kctx_set_preconditioner(dftcuda_kctx* c, int kind, const 
   if (kind == DFTCUDA_PRECOND_MLP) {
     if (!params || nparams != (size_t)MLP_NPARAM)
       return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_preconditioner: the MLP needs DFTCUDA_PRECOND_MLP_PARAMS weights");
-    if (!c->d_mlp && cudaMalloc(&c->d_mlp, sizeof(float) * (kMlpParamPad + (size_t)kLutN0 * kLutN1)) != cudaSuccess)
+    if (!c->d_mlp && dev_malloc(&c->d_mlp, sizeof(float) * (kMlpParamPad + (size_t)kLutN0 * kLutN1)) != cudaSuccess)
       return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "set_preconditioner: weights");
     c->mlp_table_t = -1.0;
     DFT_CUDA_TRY(cudaMemcpyAsync(c->d_mlp, params, sizeof(float) * MLP_NPARAM,
@@ -592,7 +592,7 @@ extern "C" int dftcuda_precond_mlp_train(size_t nbands, size_t npw, const int* b
     st = mlp_upload(d, nbands, npw, band_off, feat, cc, w, dnorm, params, s);
     std::vector<double> hist(steps, 0.0);
     double* dhist = nullptr;
-    if (st == DFTCUDA_OK && steps && cudaMalloc(&dhist, sizeof(double) * steps) != cudaSuccess)
+    if (st == DFTCUDA_OK && steps && dev_malloc(&dhist, sizeof(double) * steps) != cudaSuccess)
       st = fail(DFTCUDA_ERR_OUT_OF_MEMORY, "precond_mlp_train: history");
     for (size_t it = 0; it < steps && st == DFTCUDA_OK; ++it) {
       st = mlp_loss_grad_dev(d, s);

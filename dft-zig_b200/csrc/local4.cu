@@ -843,14 +843,14 @@ int kctx_setup_fast_path(dftcuda_kctx* c, const std::vector<int>& slot_of_x, con
   std::vector<float2> tx32, tp32;
   roots(nx, tx64, tx32);
   roots(ny, tp64, tp32);
-  bool ok = cudaMalloc(&c->d_pwmap, sizeof(int) * pwmap.size()) == cudaSuccess &&
-            cudaMalloc(&c->d_stick_off, sizeof(int) * soff.size()) == cudaSuccess &&
-            cudaMalloc(&c->d_stick_y, sizeof(int) * std::max<size_t>(sy.size(), 1)) == cudaSuccess &&
-            cudaMalloc(&c->d_slot_of_x, sizeof(int) * nx) == cudaSuccess &&
-            cudaMalloc(&c->d_tw4x64, sizeof(double2) * nx) == cudaSuccess &&
-            cudaMalloc(&c->d_tw4x32, sizeof(float2) * nx) == cudaSuccess &&
-            cudaMalloc(&c->d_tw4p64, sizeof(double2) * ny) == cudaSuccess &&
-            cudaMalloc(&c->d_tw4p32, sizeof(float2) * ny) == cudaSuccess;
+  bool ok = dev_malloc(&c->d_pwmap, sizeof(int) * pwmap.size()) == cudaSuccess &&
+            dev_malloc(&c->d_stick_off, sizeof(int) * soff.size()) == cudaSuccess &&
+            dev_malloc(&c->d_stick_y, sizeof(int) * std::max<size_t>(sy.size(), 1)) == cudaSuccess &&
+            dev_malloc(&c->d_slot_of_x, sizeof(int) * nx) == cudaSuccess &&
+            dev_malloc(&c->d_tw4x64, sizeof(double2) * nx) == cudaSuccess &&
+            dev_malloc(&c->d_tw4x32, sizeof(float2) * nx) == cudaSuccess &&
+            dev_malloc(&c->d_tw4p64, sizeof(double2) * ny) == cudaSuccess &&
+            dev_malloc(&c->d_tw4p32, sizeof(float2) * ny) == cudaSuccess;
   if (!ok) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "four-step tables");
   cudaStream_t st = c->stream;
   cudaMemcpyAsync(c->d_pwmap, pwmap.data(), sizeof(int) * pwmap.size(), cudaMemcpyHostToDevice, st);

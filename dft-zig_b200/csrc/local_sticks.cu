@@ -766,15 +766,15 @@ int kctx_setup_sticks(dftcuda_kctx* c, const std::vector<int>& slot_of_x, const 
   roots(nz, tz64, tz32);
   roots(c->nx, tx64, tx32);
   std::vector<int> sox(slot_of_x.begin(), slot_of_x.end());
-  bool ok = cudaMalloc(&c->d_st_sy, sizeof(int) * std::max<size_t>(sy.size(), 1)) == cudaSuccess &&
-            cudaMalloc(&c->d_st_map, sizeof(int) * std::max<size_t>(map.size(), 1)) == cudaSuccess &&
-            cudaMalloc(&c->d_st_sox, sizeof(int) * c->nx) == cudaSuccess &&
-            cudaMalloc(&c->d_twz64, sizeof(double2) * nz) == cudaSuccess &&
-            cudaMalloc(&c->d_twz32, sizeof(float2) * nz) == cudaSuccess &&
-            cudaMalloc(&c->d_twx64, sizeof(double2) * c->nx) == cudaSuccess &&
-            cudaMalloc(&c->d_twx32, sizeof(float2) * c->nx) == cudaSuccess &&
-            cudaMalloc(&c->d_vn, sizeof(double) * c->N) == cudaSuccess &&
-            cudaMalloc(&c->d_vn32, sizeof(float) * c->N) == cudaSuccess;
+  bool ok = dev_malloc(&c->d_st_sy, sizeof(int) * std::max<size_t>(sy.size(), 1)) == cudaSuccess &&
+            dev_malloc(&c->d_st_map, sizeof(int) * std::max<size_t>(map.size(), 1)) == cudaSuccess &&
+            dev_malloc(&c->d_st_sox, sizeof(int) * c->nx) == cudaSuccess &&
+            dev_malloc(&c->d_twz64, sizeof(double2) * nz) == cudaSuccess &&
+            dev_malloc(&c->d_twz32, sizeof(float2) * nz) == cudaSuccess &&
+            dev_malloc(&c->d_twx64, sizeof(double2) * c->nx) == cudaSuccess &&
+            dev_malloc(&c->d_twx32, sizeof(float2) * c->nx) == cudaSuccess &&
+            dev_malloc(&c->d_vn, sizeof(double) * c->N) == cudaSuccess &&
+            dev_malloc(&c->d_vn32, sizeof(float) * c->N) == cudaSuccess;
   if (!ok) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "stick tables");
   cudaStream_t st = c->stream;
   if (!sy.empty()) DFT_CUDA_TRY(cudaMemcpyAsync(c->d_st_sy, sy.data(), sizeof(int) * sy.size(), cudaMemcpyHostToDevice, st));

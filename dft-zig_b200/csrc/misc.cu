@@ -86,6 +86,16 @@ static std::atomic<long> g_wait_polls{0};
 static std::atomic<bool> g_wait_unreachable{false};
 WaitLimits wait_limits() { return WaitLimits{g_wait_polls.load(), g_wait_unreachable.load()}; }
 
+// -1: no failure planned; k >= 0: the k-th following allocation fails (then -1 again).
+static std::atomic<long> g_fail_alloc{-1};
+bool alloc_should_fail() {
+  long v = g_fail_alloc.load(std::memory_order_relaxed);
+  while (v >= 0) {
+    if (g_fail_alloc.compare_exchange_weak(v, v - 1)) return v == 0;
+  }
+  return false;
+}
+
 DeviceGuard::DeviceGuard(int dev) {
   if (cudaGetDevice(&prev) != cudaSuccess) {
     cudaGetLastError();
@@ -106,6 +116,11 @@ extern "C" int dftcuda_debug_set_wait_limits(long polls, int unreachable) {
   if (polls < 0) return dftcuda::fail(DFTCUDA_ERR_INVALID_ARGUMENT, "debug_set_wait_limits: polls < 0");
   dftcuda::g_wait_polls.store(polls);
   dftcuda::g_wait_unreachable.store(unreachable != 0);
+  return DFTCUDA_OK;
+}
+
+extern "C" int dftcuda_debug_fail_alloc(long after) {
+  dftcuda::g_fail_alloc.store(after < 0 ? -1 : after);
   return DFTCUDA_OK;
 }
 
@@ -216,7 +231,7 @@ extern "C" int dftcuda_complex_gemm(int precision, size_t M, size_t N, size_t K,
     en = slot;
   }
   std::lock_guard<std::mutex> lock(en->mu);
-  if (!en->s && (cudaStreamCreateWithFlags(&en->s, cudaStreamDefault) != cudaSuccess || cudaMalloc(&en->err, sizeof(int)) != cudaSuccess)) {
+  if (!en->s && (cudaStreamCreateWithFlags(&en->s, cudaStreamDefault) != cudaSuccess || dev_malloc(&en->err, sizeof(int)) != cudaSuccess)) {
     if (en->s) cudaStreamDestroy(en->s);
     en->s = nullptr;
     en->err = nullptr;
@@ -227,7 +242,7 @@ extern "C" int dftcuda_complex_gemm(int precision, size_t M, size_t N, size_t K,
     if (en->ws) cudaFree(en->ws);
     en->ws = nullptr;
     en->ws_cap = 0;
-    if (cudaMalloc(&en->ws, sizeof(double2) * ws_elems) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "complex_gemm: workspace");
+    if (dev_malloc(&en->ws, sizeof(double2) * ws_elems) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "complex_gemm: workspace");
     en->ws_cap = ws_elems;
   }
   DFT_CUDA_TRY(cudaMemsetAsync(en->err, 0, sizeof(int), en->s));

@@ -162,7 +162,7 @@ extern "C" int dftcuda_fermi_occupations(size_t nk, size_t nbands, const double*
   } g{s};
   // device staging: values, weights, occupations, mu and the two sums
   const size_t bytes = sizeof(double) * (2 * n + nk + 3);
-  DFT_CUDA_TRY(cudaMalloc(&g.p, bytes));
+  DFT_CUDA_TRY(dev_malloc(&g.p, bytes));
   double* d_e = static_cast<double*>(g.p);
   double* d_w = d_e + n;
   double* d_occ = d_w + nk;

@@ -683,12 +683,12 @@ extern "C" int dftcuda_pctx_create(dftcuda_pctx** out, int nx, int ny, int nz, d
   const long N = c->N;
   const int nparts = std::max(2, pulay_history);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault) != cudaSuccess ||
-      cudaMalloc(&c->g2, sizeof(double) * N) != cudaSuccess || cudaMalloc(&c->a, sizeof(double2) * N) != cudaSuccess ||
-      cudaMalloc(&c->b, sizeof(double2) * N) != cudaSuccess || cudaMalloc(&c->rho, sizeof(double) * N) != cudaSuccess ||
-      cudaMalloc(&c->vin, sizeof(double2) * N) != cudaSuccess || cudaMalloc(&c->vout, sizeof(double2) * N) != cudaSuccess ||
-      cudaMalloc(&c->part, sizeof(double) * kPotBlocks * nparts) != cudaSuccess ||
+      dev_malloc(&c->g2, sizeof(double) * N) != cudaSuccess || dev_malloc(&c->a, sizeof(double2) * N) != cudaSuccess ||
+      dev_malloc(&c->b, sizeof(double2) * N) != cudaSuccess || dev_malloc(&c->rho, sizeof(double) * N) != cudaSuccess ||
+      dev_malloc(&c->vin, sizeof(double2) * N) != cudaSuccess || dev_malloc(&c->vout, sizeof(double2) * N) != cudaSuccess ||
+      dev_malloc(&c->part, sizeof(double) * kPotBlocks * nparts) != cudaSuccess ||
       cudaMallocHost(&c->h_part, sizeof(double) * kPotBlocks * nparts) != cudaSuccess ||
-      cudaMalloc(&c->d_slots, sizeof(int) * 64) != cudaSuccess || cudaMalloc(&c->d_coef, sizeof(double) * 65) != cudaSuccess)
+      dev_malloc(&c->d_slots, sizeof(int) * 64) != cudaSuccess || dev_malloc(&c->d_coef, sizeof(double) * 65) != cudaSuccess)
     return pctx_fail_free(c, fail(DFTCUDA_ERR_CUDA, "pctx_create: device allocation failed"));
   const double* r = recip;
   k_pot_g2<<<kPotBlocks, kPotThreads, 0, c->stream>>>(nx, ny, nz, r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8], c->g2);
@@ -733,8 +733,8 @@ extern "C" int dftcuda_pctx_set_functional(dftcuda_pctx* c, int functional) {
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "pctx_set_functional: LDA-PZ (0) or PBE (1)");
   if (functional == DFTCUDA_XC_PBE && !c->w) {
     const long N = c->N;
-    if (cudaMalloc(&c->w, sizeof(double2) * N) != cudaSuccess || cudaMalloc(&c->gr, sizeof(double) * 3 * N) != cudaSuccess ||
-        cudaMalloc(&c->vr, sizeof(double) * N) != cudaSuccess) {
+    if (dev_malloc(&c->w, sizeof(double2) * N) != cudaSuccess || dev_malloc(&c->gr, sizeof(double) * 3 * N) != cudaSuccess ||
+        dev_malloc(&c->vr, sizeof(double) * N) != cudaSuccess) {
       for (void** p : {(void**)&c->w, (void**)&c->gr, (void**)&c->vr})
         if (*p) {
           cudaFree(*p);
@@ -854,8 +854,8 @@ extern "C" int dftcuda_symmetrize_density(dftcuda_pctx* c, int nops, const int* 
   const long N = c->N;
   cudaStream_t s = c->stream;
   if (!c->sym_kr) {
-    if (cudaMalloc(&c->sym_kr, sizeof(int) * 9 * kSymMaxOps) != cudaSuccess ||
-        cudaMalloc(&c->sym_t, sizeof(double) * 3 * kSymMaxOps) != cudaSuccess)
+    if (dev_malloc(&c->sym_kr, sizeof(int) * 9 * kSymMaxOps) != cudaSuccess ||
+        dev_malloc(&c->sym_t, sizeof(double) * 3 * kSymMaxOps) != cudaSuccess)
       return fail(DFTCUDA_ERR_CUDA, "symmetrize_density: allocation failed");
   }
   DFT_CUDA_TRY(cudaMemcpyAsync(c->sym_kr, k_rot, sizeof(int) * 9 * nops, cudaMemcpyDefault, s));
@@ -897,7 +897,7 @@ struct FFDevice {
   }
   int init(const FFArgs& a, int nspecies, const double* g2, long N, cudaStream_t s) {
     if (a.gth) {
-      if (cudaMalloc(&buf, sizeof(double) * 6 * nspecies) != cudaSuccess) return fail(DFTCUDA_ERR_CUDA, "form factors: allocation failed");
+      if (dev_malloc(&buf, sizeof(double) * 6 * nspecies) != cudaSuccess) return fail(DFTCUDA_ERR_CUDA, "form factors: allocation failed");
       DFT_CUDA_TRY(cudaMemcpyAsync(buf, a.gth, sizeof(double) * 6 * nspecies, cudaMemcpyDefault, s));
       ff.gth = buf;
       return DFTCUDA_OK;
@@ -910,8 +910,8 @@ struct FFDevice {
     }
     const size_t nr = (size_t)ho[nspecies] - ho[0];
     if (ho[0] != 0 || nr == 0) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "radial form factors: empty mesh");
-    if (cudaMalloc(&buf, sizeof(double) * (3 * nr + nspecies + (size_t)nspecies * N)) != cudaSuccess ||
-        cudaMalloc(&off, sizeof(int) * (nspecies + 1)) != cudaSuccess)
+    if (dev_malloc(&buf, sizeof(double) * (3 * nr + nspecies + (size_t)nspecies * N)) != cudaSuccess ||
+        dev_malloc(&off, sizeof(int) * (nspecies + 1)) != cudaSuccess)
       return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "radial form factors: allocation failed");
     double *dr = buf, *drab = buf + nr, *dv = buf + 2 * nr, *dz = buf + 3 * nr, *vq = dz + nspecies;
     DFT_CUDA_TRY(cudaMemcpyAsync(dr, a.r, sizeof(double) * nr, cudaMemcpyDefault, s));
@@ -947,8 +947,8 @@ static int ionic_impl(dftcuda_pctx* c, int nspecies, const FFArgs& ffa, int nato
   };
   FFDevice ffd;
   DFT_TRY(ffd.init(ffa, nspecies, c->g2, N, s));
-  if (cudaMalloc(&d_pos, sizeof(double) * 3 * std::max(natoms, 1)) != cudaSuccess ||
-      cudaMalloc(&d_sp, sizeof(int) * std::max(natoms, 1)) != cudaSuccess) {
+  if (dev_malloc(&d_pos, sizeof(double) * 3 * std::max(natoms, 1)) != cudaSuccess ||
+      dev_malloc(&d_sp, sizeof(int) * std::max(natoms, 1)) != cudaSuccess) {
     cleanup();
     return fail(DFTCUDA_ERR_CUDA, "ionic_potential: allocation failed");
   }
@@ -1001,8 +1001,8 @@ static int local_forces_impl(dftcuda_pctx* c, int nspecies, const FFArgs& ffa, i
   const size_t npart = (size_t)natoms * kLfChunks * 3;
   FFDevice ffd;
   DFT_TRY(ffd.init(ffa, nspecies, c->g2, N, s));
-  if (cudaMalloc(&d_pos, sizeof(double) * 3 * natoms) != cudaSuccess ||
-      cudaMalloc(&d_sp, sizeof(int) * natoms) != cudaSuccess || cudaMalloc(&d_part, sizeof(double) * npart) != cudaSuccess) {
+  if (dev_malloc(&d_pos, sizeof(double) * 3 * natoms) != cudaSuccess ||
+      dev_malloc(&d_sp, sizeof(int) * natoms) != cudaSuccess || dev_malloc(&d_part, sizeof(double) * npart) != cudaSuccess) {
     cleanup();
     return fail(DFTCUDA_ERR_CUDA, "local_forces: allocation failed");
   }
@@ -1083,7 +1083,7 @@ extern "C" int dftcuda_radial_table(int l, size_t nr, const double* r, const dou
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "radial_table: bad arguments (nq 2..65535)");
   double* d = nullptr;
   const size_t bytes = sizeof(double) * (3 * nr + nq);
-  if (cudaMalloc(&d, bytes) != cudaSuccess) return fail(DFTCUDA_ERR_CUDA, "radial_table: allocation failed");
+  if (dev_malloc(&d, bytes) != cudaSuccess) return fail(DFTCUDA_ERR_CUDA, "radial_table: allocation failed");
   cudaStream_t s = nullptr;
   int st = DFTCUDA_OK;
   auto run = [&]() -> int {
@@ -1121,8 +1121,8 @@ extern "C" int dftcuda_pulay_mix(dftcuda_pctx* c, double* x, const double* resid
         cudaFree(*p);
         *p = nullptr;
       }
-    if (cudaMalloc(&c->hx, sizeof(double) * n * H) != cudaSuccess || cudaMalloc(&c->hr, sizeof(double) * n * H) != cudaSuccess ||
-        cudaMalloc(&c->px, sizeof(double) * n) != cudaSuccess || cudaMalloc(&c->pr, sizeof(double) * n) != cudaSuccess) {
+    if (dev_malloc(&c->hx, sizeof(double) * n * H) != cudaSuccess || dev_malloc(&c->hr, sizeof(double) * n * H) != cudaSuccess ||
+        dev_malloc(&c->px, sizeof(double) * n) != cudaSuccess || dev_malloc(&c->pr, sizeof(double) * n) != cudaSuccess) {
       c->pn = 0;
       return fail(DFTCUDA_ERR_CUDA, "pulay_mix: history allocation failed");
     }

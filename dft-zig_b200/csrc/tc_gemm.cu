@@ -1406,7 +1406,7 @@ int TcScratch::ensure(size_t need) {
   p = nullptr;
   bytes = 0;
   valid = false;
-  if (cudaMalloc(&p, need) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "tensor-core operand tiles");
+  if (dev_malloc(&p, need) != cudaSuccess) return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "tensor-core operand tiles");
   bytes = need;
   return DFTCUDA_OK;
 }

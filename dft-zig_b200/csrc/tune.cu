@@ -47,7 +47,7 @@ extern "C" int dftcuda_kctx_autotune(dftcuda_kctx* c, size_t ncols, dftcuda_tune
   cudaStream_t s = c->stream;
   const size_t n = c->npw;
   double2* xy = nullptr;
-  if (cudaMalloc(&xy, sizeof(double2) * n * ncols * 2) != cudaSuccess)
+  if (dev_malloc(&xy, sizeof(double2) * n * ncols * 2) != cudaSuccess)
     return fail(DFTCUDA_ERR_OUT_OF_MEMORY, "kctx_autotune: trial columns");
   double2* x = xy;
   double2* y = xy + n * ncols;

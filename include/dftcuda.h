@@ -73,6 +73,12 @@ int dftcuda_device_count(void);
  * Process-wide; applies to launches made after the call. */
 int dftcuda_debug_set_wait_limits(long polls, int unreachable);
 
+/* Failure injection for tests of the out-of-memory path (no reference counterpart): after >= 0 makes
+ * the after-th following device allocation of the library fail once, as cudaMalloc does when the
+ * device is full; the entry point that made it returns DFTCUDA_ERR_OUT_OF_MEMORY and its context
+ * stays usable.  after < 0 cancels a planned failure.  Process-wide. */
+int dftcuda_debug_fail_alloc(long after);
+
 /* ------------------------------------------------------------------------------------------
  * Per-k-point context: replaces the ApplyContext + KpointApplyCache pair
  * (src/features/scf/apply.zig:45-169, 554-573) and PwGridMap (src/features/scf/pw_grid_map.zig:8-56).
