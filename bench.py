@@ -120,6 +120,8 @@ def parse():
     ap.add_argument("--cell", choices=tuple(WORKLOADS), default="si216", help="cell of the H|psi> workload")
     ap.add_argument("--no-scf", action="store_true", help="skip the Si216 time-to-SCF object of the default line")
     ap.add_argument("--no-variants", action="store_true", help="skip the FP32 / TF32 variants of the H|psi> step")
+    ap.add_argument("--autotune", action="store_true",
+                    help="run the context autotuner (layout, workspace budget, projector split-K) before timing")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile-case", action="store_true", help="small single-k case for ncu captures: Gamma, 32 columns, 2 applications")
     ap.add_argument("--workload", choices=("hpsi", "scf", "scf64", "scf216", "al4", "cells", "eig", "heev", "gemm", "potential"),
@@ -264,6 +266,7 @@ def run_ours(args):
         kc.set_vloc(inp.local_r)
         kc.set_projectors([dz.SpeciesProjectors(l, d, p) for (l, d, p) in inp.species_phi], inp.atom_species, inp.positions)
         ctxs.append(kc)
+    tuned = [kc.autotune(NCOLS) for kc in ctxs] if args.autotune else None
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
     xs, ys = [], []
     for kc in ctxs:
@@ -425,6 +428,7 @@ def run_ours(args):
             "per": f"one {NCOLS}-column application of the local operator at one k-point",
         },
         "kernels": kern,
+        "autotune": tuned,
         "variants": variants,
     }
     if rank == 0 and world == 1:
