@@ -334,62 +334,75 @@ __global__ void __launch_bounds__(1024) k_chol_right(const double2* __restrict__
   if (tid == 0) *kk_out = s_nk;
 }
 
-// Blocked form of the same factorisation for larger blocks: one CTA factors the rows of a panel of
-// kChPanel columns (pivots, drops, row scaling and the updates among the panel's own rows, over all
-// columns); the panel's rank-kChPanel update of the trailing triangle is an FP64 GEMM.  Dropped rows
-// are zeroed so they add nothing to the GEMM.  Launch j0 = 0 first: it copies G and resets *kk.
-constexpr int kChPanel = 32;
-__global__ void __launch_bounds__(1024) k_chol_panel(const double2* __restrict__ G, int k, double drop,
-                                                     double2* __restrict__ A, int* __restrict__ kept, int* __restrict__ kk,
-                                                     int j0, int j1) {
+// Blocked form of the same factorisation for larger blocks.  k_chol_init copies G's upper triangle
+// into A (row-major) over the whole grid and resets the kept count; then per panel of rows
+// [j0, j1) one CTA loads the panel's rows (columns j0 .. k-1) into shared memory, factors them there
+// (pivots, drops, row scaling and the updates among the panel's own rows), and writes them back;
+// the panel's rank-(j1 - j0) update of the trailing triangle is an FP64 GEMM.  Dropped rows are
+// zeroed so they add nothing to the GEMM.  The panel width keeps its rows within kChPanelSmem.
+constexpr int kChPanelMax = 32;
+constexpr size_t kChPanelSmem = 200 * 1024;
+
+__global__ void k_chol_init(const double2* __restrict__ G, int k, double2* __restrict__ A, int* __restrict__ kk) {
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx == 0) *kk = 0;
+  if (idx >= (long)k * k) return;
+  const int j = (int)(idx / k), l = (int)(idx - (long)j * k);
+  if (l >= j) A[idx] = G[j + (long)l * k];
+}
+
+__global__ void __launch_bounds__(1024) k_chol_panel(double2* __restrict__ A, int k, double drop, int* __restrict__ kept,
+                                                     int* __restrict__ kk, int j0, int j1) {
+  extern __shared__ double2 cps[];  // [j1 - j0][k - j0]: row j0 + r, column j0 + c at cps[r * nc + c]
   __shared__ double s_piv;
   __shared__ int s_nk;
   const int tid = threadIdx.x, nt = blockDim.x;
-  if (j0 == 0) {
-    for (long idx = tid; idx < (long)k * k; idx += nt) {
-      const int j = (int)(idx / k), l = (int)(idx - (long)j * k);
-      if (l >= j) A[idx] = G[j + (long)l * k];
-    }
-    if (tid == 0) *kk = 0;
-    __syncthreads();
+  const int nc = k - j0, rows = j1 - j0;
+  for (long idx = tid; idx < (long)rows * nc; idx += nt) {
+    const int r = (int)(idx / nc), c = (int)(idx - (long)r * nc);
+    cps[idx] = A[(long)(j0 + r) * k + j0 + c];
   }
   if (tid == 0) s_nk = *kk;
   __syncthreads();
-  for (int j = j0; j < j1; ++j) {
+  for (int jl = 0; jl < rows; ++jl) {  // row j = j0 + jl; its diagonal at column jl
+    double2* rj = cps + (long)jl * nc;
     if (tid == 0) {
-      const double d = A[(long)j * k + j].x;
+      const double d = rj[jl].x;
       s_piv = d > 0.0 ? sqrt(d) : 0.0;
     }
     __syncthreads();
     const double piv = s_piv;
-    double2* rj = A + (long)j * k;
     if (!(piv >= drop) || piv == 0.0) {
-      for (int l = j + tid; l < k; l += nt) rj[l] = make_double2(0.0, 0.0);
+      for (int c = jl + tid; c < nc; c += nt) rj[c] = make_double2(0.0, 0.0);
       __syncthreads();
       continue;
     }
     const double inv = 1.0 / piv;
-    for (int l = j + 1 + tid; l < k; l += nt) rj[l] = make_double2(rj[l].x * inv, rj[l].y * inv);
+    for (int c = jl + 1 + tid; c < nc; c += nt) rj[c] = make_double2(rj[c].x * inv, rj[c].y * inv);
     if (tid == 0) {
-      rj[j] = make_double2(piv, 0.0);
-      kept[s_nk] = j;
+      rj[jl] = make_double2(piv, 0.0);
+      kept[s_nk] = j0 + jl;
       s_nk = s_nk + 1;
     }
     __syncthreads();
-    // rows j' of the panel after j: A[j'][l] -= conj(R[j][j']) R[j][l] for l >= j'
-    const int nr = j1 - j - 1, nc = k - j - 1;
-    for (long idx = tid; idx < (long)nr * nc; idx += nt) {
-      const int a = (int)(idx / nc), b = (int)(idx - (long)a * nc);
-      const int jr = j + 1 + a, l = j + 1 + b;
-      if (l < jr) continue;
-      const double2 x = rj[jr], y = rj[l];
-      double2* t = A + (long)jr * k + l;
+    // the panel's rows after j: A[j'][l] -= conj(R[j][j']) R[j][l] for l >= j'
+    const int nr = rows - jl - 1, nu = nc - jl - 1;
+    for (long idx = tid; idx < (long)nr * nu; idx += nt) {
+      const int a = (int)(idx / nu), b = (int)(idx - (long)a * nu);
+      const int rr = jl + 1 + a, c = jl + 1 + b;
+      if (c < rr) continue;
+      const double2 x = rj[rr], y = rj[c];
+      double2* t = cps + (long)rr * nc + c;
       double2 v = *t;
       v.x -= x.x * y.x + x.y * y.y;
       v.y -= x.x * y.y - x.y * y.x;
       *t = v;
     }
     __syncthreads();
+  }
+  for (long idx = tid; idx < (long)rows * nc; idx += nt) {
+    const int r = (int)(idx / nc), c = (int)(idx - (long)r * nc);
+    A[(long)(j0 + r) * k + j0 + c] = cps[idx];
   }
   if (tid == 0) *kk = s_nk;
 }
@@ -595,9 +608,13 @@ static int chol_drop(KCtxImpl* e, const double2* G, int k, double drop, int* kk_
     k_chol_right<<<1, 1024, 0, s>>>(G, k, drop, e->R, e->kept, kk_dev);
     count_launch();
   } else {
-    for (int j0 = 0; j0 < k; j0 += kChPanel) {
-      const int j1 = std::min(k, j0 + kChPanel);
-      k_chol_panel<<<1, 1024, 0, s>>>(G, k, drop, e->R, e->kept, kk_dev, j0, j1);
+    k_chol_init<<<ceil_div((size_t)k * k, 256), 256, 0, s>>>(G, k, e->R, kk_dev);
+    count_launch();
+    DFT_TRY(ensure_max_dynamic_smem((const void*)k_chol_panel, (int)kChPanelSmem));
+    for (int j0 = 0; j0 < k;) {
+      const int w = (int)std::max<size_t>(1, std::min<size_t>(kChPanelMax, kChPanelSmem / (sizeof(double2) * (size_t)(k - j0))));
+      const int j1 = std::min(k, j0 + w);
+      k_chol_panel<<<1, 1024, sizeof(double2) * (size_t)(j1 - j0) * (k - j0), s>>>(e->R, k, drop, e->kept, kk_dev, j0, j1);
       count_launch();
       if (j1 < k) {
         // A[l1][l2] -= sum_{j in panel} conj(R[j][l1]) R[j][l2], l1, l2 >= j1 (the lower triangle
@@ -610,6 +627,7 @@ static int chol_drop(KCtxImpl* e, const double2* G, int k, double drop, int* kk_
         g.alpha = -1.0; g.beta = 1.0;
         DFT_TRY(zgemm(g, s, e->ws, e->ws_elems));
       }
+      j0 = j1;
     }
   }
   const size_t ci_smem = sizeof(double2) * kCiWarps * (size_t)k + sizeof(int) * (size_t)k;
