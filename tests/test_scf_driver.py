@@ -110,3 +110,28 @@ def test_model_dielectric_preconditioner_keeps_the_fixed_point():
     diel = scf.run_scf(c, scf.ScfParams(**base, diemac=12.0, dielng=1.0), OracleBackend())
     assert plain.converged and diel.converged
     assert abs(plain.energy_per_atom - diel.energy_per_atom) < 1e-8
+
+
+def test_mixed_backend_switch_rule():
+    """GpuBackend("mixed") leaves the reduced-precision contexts when the density residual falls below
+    switch_drho, or when it has stopped reaching a new minimum for `stall` observations once it is
+    below 10 x switch_drho; a residual that rises above that band is the mixing's own transient and
+    does not count."""
+    b = scf.GpuBackend(None, "mixed", switch_drho=1e-4, stall=3)
+    for d in (1e-2, 3e-2, 5e-2, 2e-3):  # rises above the band: no stall counted
+        b.observe(d)
+    assert b.use32 and b.since_best == 0
+    for d in (9e-4, 9.5e-4, 9.6e-4):
+        b.observe(d)
+    assert b.use32 and b.since_best == 2
+    b.observe(9.7e-4)  # the third observation without a new minimum inside the band
+    assert not b.use32 and b.switched_at == 8
+
+    b = scf.GpuBackend(None, "mixed", switch_drho=1e-4, stall=3)
+    b.observe(5e-3)
+    b.observe(8e-5)  # below the threshold: switch at once
+    assert not b.use32 and b.switched_at == 2
+
+    b = scf.GpuBackend(None, "fp64")
+    b.observe(1e-9)
+    assert not b.use32 and b.switched_at is None
