@@ -54,3 +54,22 @@ def test_monkhorst_pack_weights():
     assert len(k) == 8 and abs(sum(w for _, w in k) - 1.0) < 1e-15
     k4 = system.monkhorst_pack((4, 4, 4))
     assert abs(sum(w for _, w in k4) - 1.0) < 1e-15 and len(k4) == 36
+
+
+@pytest.mark.parametrize("name,ecut,box", [("si2", 20.0, (20, 20, 20)), ("si2", 30.0, (24, 24, 24)), ("al4", 25.0, (27, 27, 27)),
+                                           ("si64", 30.0, (75, 75, 75)), ("si216", 25.0, (108, 108, 108)),
+                                           ("sige8", 20.0, (36, 32, 32)), ("sival", 25.0, (108, 100, 72))])
+def test_every_cell_box_has_a_register_fft_split(name, ecut, box):
+    """The FFT box of each cell the tests and the bench run (fft_box: 2-3-5-smooth, >= 2 G_max + 1)
+    is one the fused register-FFT passes implement (DFTCUDA_FOUR_STEP_LENGTHS in csrc/fft_reg.cuh),
+    so none of them falls back to the generic passes."""
+    import os
+    import re
+
+    src = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "dft-zig_b200", "csrc", "fft_reg.cuh")).read()
+    macro = src[src.index("#define DFTCUDA_FOUR_STEP_LENGTHS"):].split("\n\n")[0]
+    lengths = {int(v) for v in re.findall(r"X\((\d+)\)", macro)}
+    c = system.crystal(name, 1)
+    dims = system.fft_box(ecut, c.recip)
+    assert tuple(dims) == box
+    assert set(dims) <= lengths
