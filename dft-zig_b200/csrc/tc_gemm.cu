@@ -562,7 +562,6 @@ constexpr int T3_APL = TC_M * T3_K * 4;  // one TF32 plane of the A slot (4 KB)
 constexpr int T3_BPL = T3_N * T3_K * 4;  // one TF32 plane of the B slot (8 KB)
 constexpr int T3_SLOT = 2 * T3_APL + 2 * T3_BPL;  // Ar, Ai, Br, Bi
 constexpr int T3_ACM = (TC_M / 8) * (T3_K / 4);   // 32 core matrices of A per slot
-constexpr int T3_BCM = (T3_N / 8) * (T3_K / 4);   // 64 of B
 constexpr uint32_t T3_TMEM_COLS = 512;
 __host__ __device__ constexpr int t3_slot(bool split) { return split ? 2 * T3_SLOT : T3_SLOT; }
 __host__ __device__ constexpr int t3_stages(bool split) { return split ? 3 : 6; }
