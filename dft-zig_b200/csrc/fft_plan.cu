@@ -198,7 +198,7 @@ struct dftcuda_fft_plan {
   cudaStream_t stream = nullptr;
 };
 
-static int run_axis(dftcuda_fft_plan* pl, double2* d, const Fft1d& p, int es, int ninner, int nouter, long os, int dir,
+static int run_axis(dftcuda_fft_plan* /*pl*/, double2* d, const Fft1d& p, int es, int ninner, int nouter, long os, int dir,
                     double scale, cudaStream_t stream) {
   const int lines = ninner >= 16 ? 16 : ninner;
   dim3 block(16, lines);

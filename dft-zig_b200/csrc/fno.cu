@@ -121,8 +121,10 @@ __global__ void k_fno_mix(const float2* __restrict__ Vh, const float2* __restric
 }
 
 // dR[k][o][i] += G[o][k] conj(Vhat[i][k]);  dVhat[i][k] = sum_o conj(R[k][o][i]) G[o][k]
-__global__ void k_fno_mix_bwd(const float2* __restrict__ G, const float2* __restrict__ Vh, const float2* __restrict__ R,
-                              float2* __restrict__ dR, float2* __restrict__ dVh) {
+// Vh and dVh may be the same buffer (the backward pass writes dVh over Vh): each thread reads its own
+// Vh entry before it writes the same dVh entry, so neither pointer is restrict-qualified.
+__global__ void k_fno_mix_bwd(const float2* __restrict__ G, const float2* Vh, const float2* __restrict__ R,
+                              float2* __restrict__ dR, float2* dVh) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= FNO_W * FNO_K) return;
   const int i = idx / FNO_K, k = idx - i * FNO_K;
