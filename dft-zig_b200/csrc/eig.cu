@@ -1153,5 +1153,11 @@ extern "C" int dftcuda_eig_solve_batch(size_t nk, dftcuda_kctx* const* ctxs, con
       ic[i] = init_cols ? init_cols[i] : 0;
     }
   }
+  // every run's kernels go to its context's stream on that context's device: one device per batch
+  for (size_t i = 1; i < nk; ++i)
+    if (ctxs[i]->device != ctxs[0]->device)
+      return fail(DFTCUDA_ERR_UNSUPPORTED, "eig_solve_batch: contexts of different devices in one batch");
+  DeviceGuard guard(ctxs[0]->device);  // the contexts' device, whatever the caller has current
+  DFT_TRY(guard.status);
   return eig_solve_runs(runs, dg, iv, ic);
 }

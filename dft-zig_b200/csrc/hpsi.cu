@@ -521,6 +521,9 @@ static void free_nonlocal(dftcuda_kctx* c) {
 
 extern "C" int dftcuda_kctx_destroy(dftcuda_kctx* c) {
   if (!c) return DFTCUDA_OK;
+  // the context's device, whatever the caller has current; the release goes ahead even if switching
+  // fails (at process exit the runtime may already be unloading)
+  DeviceGuard dg(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   eig_destroy(c->eig);
   c->prof.destroy();
@@ -655,6 +658,8 @@ extern "C" size_t dftcuda_kctx_npw(const dftcuda_kctx* c) { return c ? c->npw : 
 
 extern "C" int dftcuda_set_vloc(dftcuda_kctx* c, const double* v) {
   if (!c || !v) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_vloc: null argument");
+  DeviceGuard dg(c->device);  // the context's device, whatever the caller has current
+  DFT_TRY(dg.status);
   const bool dev = is_device_pointer(v);
   // A staging buffer kept in the context: cudaFree would synchronise the whole device (every other
   // k-point's stream) on each SCF iteration.
@@ -672,6 +677,8 @@ extern "C" int dftcuda_set_vloc(dftcuda_kctx* c, const double* v) {
 extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const dftcuda_species* species, size_t n_atoms,
                                       const int32_t* atom_species, const double* atom_pos) {
   if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_projectors: null context");
+  DeviceGuard dg(c->device);  // the context's device, whatever the caller has current
+  DFT_TRY(dg.status);
   cudaStreamSynchronize(c->stream);
   free_nonlocal(c);
   c->tc_ptiles_proj.release();  // the split copies of the old projector matrix
@@ -776,6 +783,8 @@ extern "C" int dftcuda_set_projectors(dftcuda_kctx* c, size_t n_species, const d
 
 extern "C" int dftcuda_apply_h_batch_async(dftcuda_kctx* c, const double* x, double* y, size_t ncols, void* stream) {
   if (!c || (!x && ncols) || (!y && ncols)) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "apply_h_batch_async: null argument");
+  DeviceGuard dg(c->device);  // the context's device, whatever the caller has current
+  DFT_TRY(dg.status);
   cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
   return kctx_apply_h_dev(c, (const double2*)x, (double2*)y, ncols, s);
 }
@@ -806,6 +815,8 @@ static int pipe_chunks(size_t ncols, size_t* len) {
 
 extern "C" int dftcuda_apply_h_batch(dftcuda_kctx* c, const double* x, double* y, size_t n, size_t ncols) {
   if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "apply_h_batch: null context");
+  DeviceGuard dg(c->device);  // the context's device, whatever the caller has current
+  DFT_TRY(dg.status);
   if (n != c->npw) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "apply_h_batch: n != n_pw");  // apply.zig:1591
   if (ncols == 0) return DFTCUDA_OK;
   if (!x || !y) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "apply_h_batch: null buffer");
@@ -868,6 +879,8 @@ extern "C" int dftcuda_apply_h(dftcuda_kctx* c, const double* x, double* y, size
 
 extern "C" int dftcuda_nonlocal_energies(dftcuda_kctx* c, const double* psi, size_t n, size_t nbands, double* e_out) {
   if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_energies: null context");
+  DeviceGuard dg(c->device);  // the context's device, whatever the caller has current
+  DFT_TRY(dg.status);
   if (n != c->npw) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "nonlocal_energies: n != n_pw");
   if (nbands == 0) return DFTCUDA_OK;
   if (!psi || !e_out) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_energies: null buffer");
@@ -942,6 +955,8 @@ __global__ void k_nl_force(const double2* __restrict__ t, const double2* __restr
 extern "C" int dftcuda_nonlocal_forces(dftcuda_kctx* c, const double* vectors, size_t n, size_t nbands, const double* weights,
                                        double* forces) {
   if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_forces: null context");
+  DeviceGuard dg(c->device);  // the context's device, whatever the caller has current
+  DFT_TRY(dg.status);
   if (n != c->npw) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "nonlocal_forces: n != n_pw");
   if (!forces || (nbands && (!vectors || !weights))) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_forces: null buffer");
   const int nproj = c->nl.nproj;
@@ -1063,6 +1078,8 @@ __global__ void k_stress_reduce(const double2* __restrict__ dp, const double2* _
 extern "C" int dftcuda_nonlocal_stress(dftcuda_kctx* c, const double* kpg, size_t n_species, const double* const* dphi,
                                        const double* vectors, size_t n, size_t nbands, const double* weights, double* sigma) {
   if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_stress: null context");
+  DeviceGuard dg(c->device);  // the context's device, whatever the caller has current
+  DFT_TRY(dg.status);
   if (n != c->npw) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "nonlocal_stress: n != n_pw");
   if (!sigma || !kpg || (nbands && (!vectors || !weights))) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "nonlocal_stress: null buffer");
   double hs[9] = {0.0};
@@ -1167,6 +1184,8 @@ extern "C" int dftcuda_nonlocal_stress(dftcuda_kctx* c, const double* kpg, size_
 extern "C" int dftcuda_accumulate_density(dftcuda_kctx* c, const double* vectors, size_t n, size_t nbands,
                                           const double* weights, double* rho) {
   if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "accumulate_density: null context");
+  DeviceGuard dg(c->device);  // the context's device, whatever the caller has current
+  DFT_TRY(dg.status);
   if (n != c->npw) return fail(DFTCUDA_ERR_INVALID_MATRIX_SIZE, "accumulate_density: n != n_pw");
   if (nbands == 0) return DFTCUDA_OK;
   if (!vectors || !weights || !rho) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "accumulate_density: null buffer");

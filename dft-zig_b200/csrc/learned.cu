@@ -539,6 +539,8 @@ using namespace dftcuda;
 
 extern "C" int dftcuda_kctx_set_preconditioner(dftcuda_kctx* c, int kind, const float* params, size_t nparams) {
   if (!c) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_preconditioner: null context");
+  DeviceGuard dg(c->device);  // the context's device, whatever the caller has current
+  DFT_TRY(dg.status);
   if (kind < DFTCUDA_PRECOND_REFERENCE || kind > DFTCUDA_PRECOND_MLP)
     return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "set_preconditioner: unknown kind");
   if (kind == DFTCUDA_PRECOND_MLP) {

@@ -43,6 +43,8 @@ using namespace dftcuda;
 
 extern "C" int dftcuda_kctx_autotune(dftcuda_kctx* c, size_t ncols, dftcuda_tune_report* report) {
   if (!c || ncols == 0) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "kctx_autotune: null context or no columns");
+  DeviceGuard dg(c->device);  // the context's device, whatever the caller has current
+  DFT_TRY(dg.status);
   if (!c->has_vloc) return fail(DFTCUDA_ERR_INVALID_ARGUMENT, "kctx_autotune: local potential not set (dftcuda_set_vloc)");
   cudaStream_t s = c->stream;
   const size_t n = c->npw;
