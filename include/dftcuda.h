@@ -197,7 +197,8 @@ int dftcuda_eig_solve(dftcuda_kctx* ctx, const double* diag, size_t nbands, cons
  * the runs advance in lockstep, each on its own context's stream, with one host synchronisation per
  * phase for all of them, so the GPU overlaps the k-points' kernels.  Per-k arrays of length nk:
  * diags[k] (n_k), init_vecs (NULL, or per-k pointers that may be NULL) with init_cols, values_out[k]
- * (nbands), vectors_out[k] (n_k x nbands); infos: NULL or nk entries.  Each context at most once. */
+ * (nbands), vectors_out[k] (n_k x nbands); infos: NULL or nk entries.  Each context at most once,
+ * all created on one device (DFTCUDA_ERR_UNSUPPORTED otherwise; one batch per device). */
 int dftcuda_eig_solve_batch(size_t nk, dftcuda_kctx* const* ctxs, const double* const* diags, size_t nbands,
                             const dftcuda_eig_opts* opts, const double* const* init_vecs, const size_t* init_cols,
                             double* const* values_out, double* const* vectors_out, dftcuda_eig_info* infos);
